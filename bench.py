@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark: Yee FDTD throughput (MCells/s) and fraction of the HBM roofline.
+
+Workload (default): cpml_boxes_256 -- 256^3 uniform 1 mm grid, 8-cell CPML
+on all faces (m = 3, R0 = 1e-6), 40 seeded dielectric boxes (eps_r U[1,10],
+sigma U[0,0.1] S/m), soft Gaussian Ez 0-10 GHz at the centre, FP32 fields and
+coefficients.  The full run is 10000 timesteps.
+
+A bench "step" is one EngineBatch of 1000 timesteps (the reference's GPU
+batch size, src/fdtd/simulation.rs:219); --steps 10 is the full 10000-step
+run.  Working set 1.2 GB >> 126 MB L2, so no L2 flush is needed between steps.
+
+  value  device-resident throughput: CUDA events on the engine's stream around
+         K batches (fields, coefficients and CPML state stay in HBM).
+  e2e    the same metric through the public API with host buffers: operator
+         upload (H2D), K batches with their sampled waveforms (H2D) and energy
+         samples / probe traces (D2H), and the final read_fields (D2H).
+  roofline  the H and E update kernels (each ~half the step): 60 algorithmic
+         bytes per cell per launch (120 B per cell-step), timed with CUDA
+         events around every launch on the engine's stream in a profiling
+         batch of the same workload run after the timed region.
+  cpu_baseline  the oracle's C++ restatement of the reference's Rayon engine
+         (OpenMP over x-planes, same arithmetic) on the host cores, on a
+         bounded sample of timesteps of the same workload.
+
+--impl reference times that CPU restatement alone (the reference is Rust and
+cannot be built here) with all host threads.
+
+Multi-GPU: one grid does not shard without a halo exchange, and the target is
+one GPU, so --gpus N runs N independent replicas (weak scaling); value is the
+cells*steps of all ranks over the max time across ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL_STEP = 120.0       # uncompressed FP32 Yee step (H 60 B + E 60 B)
+BYTES_PER_CELL_KERNEL = 60.0      # one half-step kernel
+STEPS_PER_BENCH_STEP = 1000
+METRIC = "MCells/s (Yee FDTD throughput, % of HBM roofline)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--n", type=int, default=256, help="grid edge (default 256)")
+    p.add_argument("--timesteps-per-step", type=int, default=STEPS_PER_BENCH_STEP)
+    p.add_argument("--compressed", action="store_true", help="material-id coefficient storage")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_engine(oe, wl, compressed=False):
+    op = wl.operator()
+    eng = oe.Engine(op, compressed=compressed)
+    if wl.cpml_layers:
+        eng.add_cpml(wl.cpml())
+    for comp, pos in wl.probes:
+        eng.add_point_probe(comp, pos)
+    return op, eng
+
+
+def batch_for(oe, wl, dt, start, n):
+    sched = [oe.ScheduledExcitation.from_excitation(wl.excitation(), start, n, dt)]
+    return oe.EngineBatch(num_steps=n, excitations=sched,
+                          termination=oe.TerminationConfig(max_timesteps=n, check_interval=100),
+                          energy_monitoring=oe.EnergyMonitorConfig(sample_interval=100,
+                                                                   track_peak=True))
+
+
+def run_device(oe, wl, args, torch, dist):
+    """value: device-resident batches timed with CUDA events (engine stream)."""
+    op, eng = build_engine(oe, wl, args.compressed)
+    dt = op.timestep()
+    T = args.timesteps_per_step
+    t = 0
+    for _ in range(args.warmup):
+        eng.run_batch(batch_for(oe, wl, dt, t, T))
+        t += T
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    dev_s, launches = 0.0, 0
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            eng.run_batch(batch_for(oe, wl, dt, t, T))
+            n, s = eng.last_batch_stats()
+            dev_s += s
+            launches += n
+            t += T
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+    if dist is not None:
+        dist.barrier()
+    # per-kernel timing of the same workload (events around every launch)
+    eng.set_kernel_profiling(True)
+    eng.run_batch(batch_for(oe, wl, dt, t, 200))
+    hs, hn, es, en = eng.kernel_profile()
+    eng.set_kernel_profiling(False)
+    eng.close()
+    return {"device_s": dev_s, "wall_s": wall, "launches": launches, "clocks": clk.summary(),
+            "h_avg_s": hs / max(hn, 1), "e_avg_s": es / max(en, 1)}
+
+
+def run_e2e(oe, wl, args, torch):
+    """e2e: public API from host buffers, copies inside the timed region."""
+    T = args.timesteps_per_step
+    # warm-up on a separate engine (context, kernels, autotune cache)
+    op, eng = build_engine(oe, wl, args.compressed)
+    dt = op.timestep()
+    for w in range(max(1, args.warmup)):
+        eng.run_batch(batch_for(oe, wl, dt, w * T, T))
+    eng.close()
+    del op
+    torch.cuda.synchronize()
+    nprobe = len(wl.probes)
+    t0 = time.perf_counter()
+    op = wl.operator()                       # host-side operator (12 host arrays)
+    eng = oe.Engine(op, compressed=args.compressed)  # H2D of the coefficients
+    if wl.cpml_layers:
+        eng.add_cpml(wl.cpml())
+    for comp, pos in wl.probes:
+        eng.add_point_probe(comp, pos)
+    h2d = 12 * wl.cells * 4
+    d2h = 0
+    for k in range(args.steps):
+        res = eng.run_batch(batch_for(oe, wl, dt, k * T, T))  # H2D samples, D2H energy
+        h2d += T * 4
+        d2h += len(res.energy_samples) * 32
+        tr = eng.probe_traces()                                 # D2H probe traces
+        d2h += tr.nbytes
+    e, h = eng.read_fields()                                    # D2H final fields
+    d2h += e.nbytes + h.nbytes
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    eng.close()
+    steps = args.steps * T
+    return {"mcells": wl.cells * steps / wall / 1e6, "h2d": h2d / args.steps,
+            "d2h": d2h / args.steps, "wall_s": wall, "nprobe": nprobe}
+
+
+def cpu_oracle(wl, threads):
+    """The oracle's restatement of the reference's parallel CPU engine for the
+    workload (FP32, OpenMP over x-planes)."""
+    import oracle
+    lines = [oracle.uniform_lines(n, wl.delta) for n in wl.dims]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*wl.dims, dt, delta, precision=32, threads=threads)
+    for b in wl.boxes:
+        s.set_material(*b)
+    if wl.cpml_layers:
+        s.enable_cpml((wl.cpml_layers,) * 6)
+    x = wl.excitation()
+    s.add_excitation_analytic(x.position, x.direction, True, 0, list(x.params), 1.0, 0, 100000)
+    return s
+
+
+def cpu_sample(wl, target_s=12.0, threads=None, max_steps=400):
+    """A bounded sample of timesteps of the same workload on the host cores."""
+    threads = threads or os.cpu_count() or 1
+    s = cpu_oracle(wl, threads)
+    t0 = time.perf_counter()
+    s.run_batch(2)
+    per = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(max_steps, target_s / max(per, 1e-9))))
+    t0 = time.perf_counter()
+    s.run_batch(n)
+    el = time.perf_counter() - t0
+    return {"value": wl.cells * n / el / 1e6, "steps": n, "threads": threads, "seconds": el}
+
+
+def main():
+    args = parse()
+    from openems_b200 import workloads
+    wl = workloads.cpml_boxes(args.n, 10000)
+    hbm, peak_src = peaks()
+    config = {"workload": f"{wl.name}: {args.n}^3 1 mm, CPML 8 (m=3, R0=1e-6), 40 dielectric boxes "
+                          "(default_rng(2)), Gaussian Ez 0-10 GHz, FP32, 10000 timesteps",
+              "timesteps_per_step": args.timesteps_per_step, "cells": wl.cells,
+              "coefficients": "compressed (material id + table)" if args.compressed else "full arrays",
+              "l2": "working set 1.2 GB > 126 MB L2; no flush", "parallelism": "replicas"}
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = os.cpu_count() or 1
+        sim = cpu_oracle(wl, cores)
+        t0 = time.perf_counter()
+        sim.run_batch(1)
+        per = time.perf_counter() - t0
+        # timesteps per bench step: about 2 s of CPU work, at most the GPU's step
+        T = int(max(1, min(args.timesteps_per_step, 2.0 / max(per, 1e-9))))
+        times = []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            sim.run_batch(T)
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        value = wl.cells * T * len(times) / sum(times) / 1e6
+        sample = (f"{T} timesteps of {wl.name} per step, OpenMP restatement of the reference "
+                  f"ParallelEngine on {cores} threads (the Rust reference is not buildable here)")
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "MCells/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": value, "unit": "MCells/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "MCells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import openems_b200 as oe
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = dist_
+    else:
+        torch.cuda.set_device(0)
+    torch.cuda.init()
+
+    d = run_device(oe, wl, args, torch, dist)
+    steps_total = args.steps * args.timesteps_per_step
+    t_dev = d["device_s"]
+    if dist is not None:
+        t = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t.item())
+    value = world * wl.cells * steps_total / t_dev / 1e6
+    e2e = None if args.no_e2e else run_e2e(oe, wl, args, torch)
+    if dist is not None:
+        if e2e is not None:
+            t = torch.tensor([e2e["wall_s"]], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e["mcells"] = world * wl.cells * steps_total / float(t.item()) / 1e6
+        dist.barrier()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    kernel_avg = max(d["h_avg_s"], d["e_avg_s"])
+    dominant = "k_update_h" if d["h_avg_s"] >= d["e_avg_s"] else "k_update_e"
+    achieved = BYTES_PER_CELL_KERNEL * wl.cells / kernel_avg / 1e9
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_path):
+        try:
+            with open(prof_path) as f:
+                tj = json.load(f)
+            traffic = tj.get(dominant, {}).get("bytes_per_cell")
+            traffic = traffic * wl.cells if traffic else None
+        except Exception:
+            traffic = None
+    cpu = None if args.no_cpu_baseline else cpu_sample(wl)
+    step_gbs = BYTES_PER_CELL_STEP * wl.cells * steps_total / t_dev / 1e9 / world
+    line = {
+        "metric": METRIC, "value": value, "unit": "MCells/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+        "hbm_fraction_step": step_gbs / hbm,
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": BYTES_PER_CELL_KERNEL * wl.cells,
+                     "h_kernel_ms": d["h_avg_s"] * 1e3, "e_kernel_ms": d["e_avg_s"] * 1e3},
+        "gpu_launches": d["launches"],
+        "clocks": d["clocks"],
+        "wall_s_timed": d["wall_s"],
+    }
+    if e2e is not None:
+        line["e2e"] = {"value": e2e["mcells"], "unit": "MCells/s",
+                       "h2d_bytes_per_step": int(e2e["h2d"]), "d2h_bytes_per_step": int(e2e["d2h"])}
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": "MCells/s", "cores": cpu["threads"],
+                                "kind": "port",
+                                "sample": f"{cpu['steps']} timesteps of {wl.name} "
+                                          f"({cpu['seconds']:.1f} s), OpenMP restatement of the "
+                                          "reference ParallelEngine"}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

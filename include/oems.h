@@ -1,0 +1,222 @@
+/*
+ * oems.h -- C ABI of the B200 FDTD engine (liboems_b200.so).
+ *
+ * This is the drop-in boundary for the Rust openEMS rewrite's engine
+ * interface.  Each entry point names the reference item it replaces
+ * (paths relative to the reference project):
+ *
+ *   EngineImpl::new(&Operator)          src/fdtd/engine_impl.rs:32   -> oems_engine_create
+ *   EngineImpl::run_batch(EngineBatch)  src/fdtd/engine_impl.rs:48   -> oems_engine_run_batch
+ *   EngineImpl::current_timestep()      src/fdtd/engine_impl.rs:53   -> oems_engine_current_timestep
+ *   EngineImpl::read_fields()           src/fdtd/engine_impl.rs:59   -> oems_engine_read_fields
+ *   EngineImpl::write_fields()          src/fdtd/engine_impl.rs:65   -> oems_engine_write_fields
+ *   EngineImpl::reset()                 src/fdtd/engine_impl.rs:70   -> oems_engine_reset
+ *   drop(Engine)                        src/fdtd/new_engine.rs:20    -> oems_engine_destroy
+ *   crate::Error variants               src/lib.rs:60-85             -> oems_status
+ *
+ * Extensions are attached to the engine once and stay resident on the GPU
+ * (the reference passes them per batch as `EngineBatch::extensions`,
+ * src/fdtd/batch.rs:25, and calls per-cell hooks; here they are fused into the
+ * update kernels):
+ *
+ *   Cpml::new           src/extensions/cpml.rs:235     -> oems_engine_add_cpml
+ *   FieldProbe::sample  src/processing/probes.rs:289   -> oems_engine_add_point_probe
+ *
+ * Conventions
+ *   - Arrays are float32, one array per component, z fastest:
+ *     idx = (i*ny + j)*nz + k  (src/arrays/mod.rs:61-64).
+ *   - Host pointers passed in are borrowed for the duration of the call only.
+ *   - No call throws or aborts.  Every failure returns a status;
+ *     oems_last_error_message() gives the detail for the calling thread.
+ *   - A handle is thread-compatible, not thread-safe (the reference trait is
+ *     Send but not Sync): one thread drives a handle at a time.  Each handle
+ *     owns one CUDA stream on its device.
+ */
+#ifndef OEMS_H
+#define OEMS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OEMS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define OEMS_API __attribute__((visibility("default")))
+#else
+#define OEMS_API
+#endif
+
+/* Status codes.  1..6 map one to one onto crate::Error (src/lib.rs:60-85). */
+typedef enum oems_status {
+  OEMS_OK = 0,
+  OEMS_ERR_CONFIG = 1,    /* Error::Config    */
+  OEMS_ERR_IO = 2,        /* Error::Io        */
+  OEMS_ERR_GRID = 3,      /* Error::Grid      */
+  OEMS_ERR_MATERIAL = 4,  /* Error::Material  */
+  OEMS_ERR_NUMERICAL = 5, /* Error::Numerical: a field became NaN or infinite */
+  OEMS_ERR_XML = 6,       /* Error::Xml       */
+  OEMS_ERR_CUDA = 7,      /* CUDA runtime failure (maps to Error::Numerical on the Rust side) */
+  OEMS_ERR_NO_DEVICE = 8, /* no usable CUDA device */
+  OEMS_ERR_TIMEOUT = 9,   /* a bounded device-side wait gave up */
+  OEMS_ERR_INVALID_ARGUMENT = 10
+} oems_status;
+
+typedef struct oems_engine oems_engine;
+
+/* Engine creation flags. */
+#define OEMS_ENGINE_COMPRESSED 0x1u /* store a per-cell material id + table of unique
+                                       coefficient sets instead of 12 arrays
+                                       (replaces CompressedCoefficients,
+                                       src/fdtd/compressed.rs:125-192) */
+#define OEMS_ENGINE_NO_AUTOTUNE 0x2u /* keep the default launch shape */
+#define OEMS_ENGINE_NO_GRAPHS 0x4u   /* launch kernels one by one instead of
+                                        replaying captured CUDA graphs */
+
+/* What Operator hands to EngineImpl::new: dimensions, dt, cell sizes and the
+ * 12 per-cell coefficient arrays (src/fdtd/operator.rs:21-38, :145-185). */
+typedef struct oems_operator_desc {
+  uint64_t nx, ny, nz;
+  double dt;
+  double delta[3];    /* cell size per axis (Grid::cell_size), used by extensions */
+  const float* ca[3]; /* E: E = ca*E + cb*curl(H) */
+  const float* cb[3];
+  const float* da[3]; /* H: H = da*H + db*curl(E) (db carries the minus sign) */
+  const float* db[3];
+  int32_t device;     /* CUDA device ordinal, -1 = the calling thread's current device */
+  uint32_t flags;     /* OEMS_ENGINE_* */
+} oems_operator_desc;
+
+/* ScheduledExcitation with a Sampled waveform (src/fdtd/batch.rs:71-100).
+ * samples[s] is applied after the E update of batch step s; steps beyond
+ * num_samples inject nothing (src/fdtd/basic_engine.rs:319-325). */
+typedef struct oems_scheduled_excitation {
+  uint64_t position[3];
+  uint32_t direction;   /* 0 = x, 1 = y, 2 = z */
+  uint32_t soft_source; /* 1: E += v, 0: E = v */
+  const float* samples;
+  uint64_t num_samples;
+} oems_scheduled_excitation;
+
+/* EngineBatch without the extension list (src/fdtd/batch.rs:17-32), with
+ * TerminationConfig (:150-170) and EnergyMonitorConfig (:173-193) inlined. */
+typedef struct oems_batch {
+  uint64_t num_steps;
+  const oems_scheduled_excitation* excitations;
+  uint32_t num_excitations;
+  int32_t has_energy_decay_db;
+  double energy_decay_db;
+  uint64_t check_interval;   /* 0 disables the termination check */
+  uint64_t sample_interval;  /* 0 disables energy sampling */
+  int32_t track_peak;
+  int32_t reserved0;
+  double initial_peak_energy; /* peak carried in from earlier batches; 0 reproduces the
+                                 reference, whose peak restarts at 0 every batch
+                                 (src/fdtd/basic_engine.rs:62) */
+} oems_batch;
+
+/* EnergySample (src/fdtd/batch.rs:197-220): unweighted sums of squares. */
+typedef struct oems_energy_sample {
+  uint64_t timestep;
+  double e_energy;
+  double h_energy;
+  double total_energy;
+} oems_energy_sample;
+
+/* TerminationReason (src/fdtd/batch.rs:52-67). */
+#define OEMS_TERMINATION_STEPS_COMPLETED 0
+#define OEMS_TERMINATION_ENERGY_DECAY 1
+#define OEMS_TERMINATION_EXTENSION_STOP 2
+
+/* BatchResult (src/fdtd/batch.rs:36-48). energy_samples is caller-owned and
+ * may be NULL; num_energy_samples reports how many were produced even when
+ * that exceeds energy_capacity. */
+typedef struct oems_batch_result {
+  uint64_t timesteps_executed;
+  int32_t termination_reason;
+  int32_t reserved0;
+  double final_decay_db;
+  oems_energy_sample* energy_samples;
+  uint64_t energy_capacity;
+  uint64_t num_energy_samples;
+  double peak_energy;
+  double elapsed_seconds;
+} oems_batch_result;
+
+/* CpmlBoundaries (src/extensions/cpml.rs:27-51).  layers: xmin xmax ymin ymax
+ * zmin zmax, 0 disables a face.  The profile follows cpml.rs:68-177; the field
+ * correction is the standard Roden-Gedney recursive convolution (the
+ * reference computes psi but never applies it, cpml.rs:344-350). */
+typedef struct oems_cpml_desc {
+  int32_t layers[6];
+  double grading_order;    /* default 3    */
+  double reflection_coeff; /* default 1e-6 */
+  double alpha_max;        /* default 0    */
+  double kappa_max;        /* default 1    */
+} oems_cpml_desc;
+
+/* Field components for probes: 0..2 = Ex Ey Ez, 3..5 = Hx Hy Hz. */
+#define OEMS_COMPONENT_EX 0
+#define OEMS_COMPONENT_HX 3
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+OEMS_API oems_status oems_engine_create(const oems_operator_desc* desc, oems_engine** out);
+OEMS_API void oems_engine_destroy(oems_engine* engine);
+
+/* ---- EngineImpl --------------------------------------------------------- */
+
+OEMS_API oems_status oems_engine_run_batch(oems_engine* engine, const oems_batch* batch,
+                                  oems_batch_result* result);
+OEMS_API oems_status oems_engine_current_timestep(const oems_engine* engine, uint64_t* timestep);
+/* e[c], h[c]: host buffers of nx*ny*nz floats each. */
+OEMS_API oems_status oems_engine_read_fields(oems_engine* engine, float* const e[3], float* const h[3]);
+OEMS_API oems_status oems_engine_write_fields(oems_engine* engine, const float* const e[3],
+                                     const float* const h[3]);
+/* Clears fields, extension state and the timestep counter. */
+OEMS_API oems_status oems_engine_reset(oems_engine* engine);
+
+/* ---- extensions ---------------------------------------------------------- */
+
+OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);
+
+/* ---- probes ---------------------------------------------------------------- */
+
+/* A point probe records one value per executed step (after the excitation). */
+OEMS_API oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component,
+                                        const uint64_t position[3], int32_t* probe_id);
+/* Traces of the most recent batch, layout [step][probe]; *steps_out receives
+ * the number of steps recorded (at most max_steps are copied). */
+OEMS_API oems_status oems_engine_read_probe_traces(oems_engine* engine, float* out, uint64_t max_steps,
+                                          uint64_t* steps_out);
+
+/* Unweighted field energies sum(E^2), sum(H^2) in f64 over the whole grid
+ * (VectorField3D::energy, src/arrays/field.rs:314-316), computed on the GPU. */
+OEMS_API oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_energy);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Per-kernel timing: while enabled, run_batch launches the update kernels one
+ * by one (no graphs) with CUDA events around every H and E launch on the
+ * engine's stream, and accumulates their device time.  Enabling resets the
+ * totals. */
+OEMS_API oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable);
+OEMS_API oems_status oems_engine_kernel_profile(const oems_engine* engine, double* h_seconds,
+                                                uint64_t* h_launches, double* e_seconds,
+                                                uint64_t* e_launches);
+
+OEMS_API const char* oems_status_string(oems_status status);
+/* Detail of the last failure on the calling thread ("" if none). */
+OEMS_API const char* oems_last_error_message(void);
+OEMS_API int32_t oems_abi_version(void);
+/* Launch statistics of the most recent batch: kernels launched on the GPU
+ * (each graph node counts) and the device time of the batch in seconds. */
+OEMS_API oems_status oems_engine_last_batch_stats(const oems_engine* engine, uint64_t* kernel_launches,
+                                         double* device_seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OEMS_H */

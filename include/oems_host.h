@@ -1,0 +1,126 @@
+/*
+ * oems_host.h -- C ABI of the host-side mirror of the reference's
+ * Operator / Excitation / Simulation surface (liboems_b200.so).
+ *
+ * The Rust openEMS rewrite keeps these types in Rust (its FFI would bind only
+ * include/oems.h).  Without a Rust toolchain, the same surface is provided in
+ * C++ so that C, C++ and Python callers can build an operator, sample
+ * excitations and run a simulation exactly as the reference does:
+ *
+ *   Grid::uniform / Grid::cartesian   src/geometry/mod.rs:60-71     -> oems_operator_create*
+ *   Operator::new                     src/fdtd/operator.rs:59-77    -> oems_operator_create*
+ *   Operator::set_material            src/fdtd/operator.rs:187-244  -> oems_operator_set_material
+ *   Operator::set_pec                 src/fdtd/operator.rs:249-263  -> oems_operator_set_pec
+ *   Operator::timestep/dimensions     src/fdtd/operator.rs:145-159  -> oems_operator_info
+ *   Operator::e/h_coefficients        src/fdtd/operator.rs:163-171  -> oems_operator_coefficients
+ *   Excitation::gaussian & co.        src/fdtd/excitation.rs:67-147 -> oems_excitation_*
+ *   Excitation::evaluate              src/fdtd/excitation.rs:150-200 -> oems_excitation_evaluate
+ *   ScheduledExcitation::from_excitation src/fdtd/batch.rs:110-129  -> oems_excitation_sample
+ *   Simulation::new/setup/run         src/fdtd/simulation.rs:96-360 -> oems_simulation_*
+ */
+#ifndef OEMS_HOST_H
+#define OEMS_HOST_H
+
+#include <stdint.h>
+
+#include "oems.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oems_operator oems_operator;
+typedef struct oems_simulation oems_simulation;
+
+/* ---- Operator ----------------------------------------------------------- */
+
+/* Cartesian grid from mesh lines (cells = lines - 1 per axis), scaled by unit. */
+OEMS_API oems_status oems_operator_create(const double* x_lines, uint64_t nxl, const double* y_lines,
+                                 uint64_t nyl, const double* z_lines, uint64_t nzl, double unit,
+                                 oems_operator** out);
+/* Grid::uniform(nx, ny, nz, delta). */
+OEMS_API oems_status oems_operator_create_uniform(uint64_t nx, uint64_t ny, uint64_t nz, double delta,
+                                         oems_operator** out);
+OEMS_API void oems_operator_destroy(oems_operator* op);
+/* region = i0, i1, j0, j1, k0, k1 (half-open, clipped to the grid). */
+OEMS_API oems_status oems_operator_set_material(oems_operator* op, double eps_r, double mu_r,
+                                       double sigma_e, double sigma_m, const uint64_t region[6]);
+OEMS_API oems_status oems_operator_set_pec(oems_operator* op, const uint64_t region[6]);
+OEMS_API oems_status oems_operator_info(const oems_operator* op, uint64_t dims[3], double* dt,
+                               double delta[3]);
+/* Borrowed pointers to the 12 coefficient arrays (ca0 ca1 ca2 cb0 cb1 cb2 da0
+ * da1 da2 db0 db1 db2), valid until the operator is modified or destroyed. */
+OEMS_API oems_status oems_operator_coefficients(const oems_operator* op, const float* out[12]);
+/* Fills an engine descriptor that borrows the operator's arrays. */
+OEMS_API oems_status oems_operator_engine_desc(const oems_operator* op, int32_t device, uint32_t flags,
+                                      oems_operator_desc* out);
+
+/* ---- Excitation ---------------------------------------------------------- */
+
+/* ExcitationType (src/fdtd/excitation.rs:9-42). */
+#define OEMS_EXC_GAUSSIAN 0           /* params: t0, tau            */
+#define OEMS_EXC_SINUSOIDAL 1         /* params: frequency          */
+#define OEMS_EXC_GAUSSIAN_MODULATED 2 /* params: frequency, t0, tau */
+#define OEMS_EXC_DIRAC 3
+#define OEMS_EXC_STEP 4
+
+typedef struct oems_excitation {
+  int32_t kind;
+  uint32_t direction;
+  uint64_t position[3];
+  double params[3];
+  double amplitude;
+  int32_t soft_source;
+  int32_t reserved0;
+} oems_excitation;
+
+OEMS_API oems_status oems_excitation_gaussian(double center_freq, double bandwidth, uint32_t direction,
+                                     const uint64_t position[3], oems_excitation* out);
+OEMS_API oems_status oems_excitation_gaussian_modulated(double center_freq, double bandwidth,
+                                               uint32_t direction, const uint64_t position[3],
+                                               oems_excitation* out);
+OEMS_API oems_status oems_excitation_sinusoidal(double frequency, uint32_t direction,
+                                       const uint64_t position[3], oems_excitation* out);
+OEMS_API oems_status oems_excitation_dirac(double amplitude, uint32_t direction, const uint64_t position[3],
+                                  oems_excitation* out);
+OEMS_API double oems_excitation_evaluate(const oems_excitation* exc, double t);
+/* out[s] = (float) evaluate((start_timestep + s) * dt), s < n. */
+OEMS_API oems_status oems_excitation_sample(const oems_excitation* exc, uint64_t start_timestep, uint64_t n,
+                                   double dt, float* out);
+
+/* ---- Simulation ---------------------------------------------------------- */
+
+/* EndCondition (src/fdtd/simulation.rs:36-43). */
+#define OEMS_END_TIMESTEPS 0
+#define OEMS_END_ENERGY_DECAY 1
+#define OEMS_END_SIMULATION_TIME 2
+
+/* SimulationStats (src/fdtd/simulation.rs:53-66). */
+typedef struct oems_simulation_stats {
+  uint64_t timesteps;
+  double sim_time;
+  double wall_time;
+  double peak_energy;
+  double final_energy;
+  double speed_mcells_per_sec;
+} oems_simulation_stats;
+
+/* Simulation over a copy of `op` (materials included).  The engine is
+ * created in setup (first run), on `device` (-1 = current) with `flags`. */
+OEMS_API oems_status oems_simulation_create(const oems_operator* op, int32_t device, uint32_t flags,
+                                   oems_simulation** out);
+OEMS_API void oems_simulation_destroy(oems_simulation* sim);
+OEMS_API oems_status oems_simulation_add_excitation(oems_simulation* sim, const oems_excitation* exc);
+OEMS_API oems_status oems_simulation_set_end_condition(oems_simulation* sim, int32_t kind, double value);
+/* 0 = automatic (1000 steps per batch, the reference's GPU batch size). */
+OEMS_API oems_status oems_simulation_set_batch_size(oems_simulation* sim, uint64_t batch_size);
+OEMS_API oems_status oems_simulation_set_cpml(oems_simulation* sim, const oems_cpml_desc* cpml);
+OEMS_API oems_status oems_simulation_setup(oems_simulation* sim);
+OEMS_API oems_status oems_simulation_run(oems_simulation* sim, oems_simulation_stats* stats);
+/* Borrowed engine handle (NULL before setup). */
+OEMS_API oems_engine* oems_simulation_engine(oems_simulation* sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OEMS_HOST_H */

@@ -1,0 +1,212 @@
+"""ctypes binding of liboems_b200.so (include/oems.h, include/oems_host.h).
+
+The library is required: there is no CPU fallback.  Importing this module
+without the built library raises immediately with the build command.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboems_b200.so")
+
+c_u64, c_i64, c_i32, c_u32, c_f64, c_f32 = (ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
+                                              ctypes.c_uint32, ctypes.c_double, ctypes.c_float)
+P = ctypes.c_void_p
+PF = ctypes.POINTER(c_f32)
+
+# status codes (include/oems.h)
+OK, ERR_CONFIG, ERR_IO, ERR_GRID, ERR_MATERIAL, ERR_NUMERICAL, ERR_XML, ERR_CUDA, \
+    ERR_NO_DEVICE, ERR_TIMEOUT, ERR_INVALID_ARGUMENT = range(11)
+
+ENGINE_COMPRESSED = 0x1
+ENGINE_NO_AUTOTUNE = 0x2
+ENGINE_NO_GRAPHS = 0x4
+
+
+class OpenEMSError(Exception):
+    """crate::Error (src/lib.rs:60-85); `status` is the C status code."""
+
+    status = -1
+
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        if status is not None:
+            self.status = status
+
+
+class ConfigError(OpenEMSError):
+    status = ERR_CONFIG
+
+
+class IoError(OpenEMSError):
+    status = ERR_IO
+
+
+class GridError(OpenEMSError):
+    status = ERR_GRID
+
+
+class MaterialError(OpenEMSError):
+    status = ERR_MATERIAL
+
+
+class NumericalError(OpenEMSError):
+    status = ERR_NUMERICAL
+
+
+class XmlError(OpenEMSError):
+    status = ERR_XML
+
+
+class CudaError(OpenEMSError):
+    status = ERR_CUDA
+
+
+class NoDeviceError(OpenEMSError):
+    status = ERR_NO_DEVICE
+
+
+class DeviceTimeoutError(OpenEMSError):
+    status = ERR_TIMEOUT
+
+
+class InvalidArgumentError(OpenEMSError):
+    status = ERR_INVALID_ARGUMENT
+
+
+_ERRORS = {c.status: c for c in (ConfigError, IoError, GridError, MaterialError, NumericalError,
+                                 XmlError, CudaError, NoDeviceError, DeviceTimeoutError,
+                                 InvalidArgumentError)}
+
+
+class OperatorDesc(ctypes.Structure):
+    _fields_ = [("nx", c_u64), ("ny", c_u64), ("nz", c_u64), ("dt", c_f64), ("delta", c_f64 * 3),
+                ("ca", PF * 3), ("cb", PF * 3), ("da", PF * 3), ("db", PF * 3),
+                ("device", c_i32), ("flags", c_u32)]
+
+
+class ScheduledExcitationC(ctypes.Structure):
+    _fields_ = [("position", c_u64 * 3), ("direction", c_u32), ("soft_source", c_u32),
+                ("samples", PF), ("num_samples", c_u64)]
+
+
+class BatchC(ctypes.Structure):
+    _fields_ = [("num_steps", c_u64), ("excitations", ctypes.POINTER(ScheduledExcitationC)),
+                ("num_excitations", c_u32), ("has_energy_decay_db", c_i32),
+                ("energy_decay_db", c_f64), ("check_interval", c_u64), ("sample_interval", c_u64),
+                ("track_peak", c_i32), ("reserved0", c_i32), ("initial_peak_energy", c_f64)]
+
+
+class EnergySampleC(ctypes.Structure):
+    _fields_ = [("timestep", c_u64), ("e_energy", c_f64), ("h_energy", c_f64),
+                ("total_energy", c_f64)]
+
+
+class BatchResultC(ctypes.Structure):
+    _fields_ = [("timesteps_executed", c_u64), ("termination_reason", c_i32),
+                ("reserved0", c_i32), ("final_decay_db", c_f64),
+                ("energy_samples", ctypes.POINTER(EnergySampleC)), ("energy_capacity", c_u64),
+                ("num_energy_samples", c_u64), ("peak_energy", c_f64),
+                ("elapsed_seconds", c_f64)]
+
+
+class CpmlDescC(ctypes.Structure):
+    _fields_ = [("layers", c_i32 * 6), ("grading_order", c_f64), ("reflection_coeff", c_f64),
+                ("alpha_max", c_f64), ("kappa_max", c_f64)]
+
+
+class ExcitationC(ctypes.Structure):
+    _fields_ = [("kind", c_i32), ("direction", c_u32), ("position", c_u64 * 3),
+                ("params", c_f64 * 3), ("amplitude", c_f64), ("soft_source", c_i32),
+                ("reserved0", c_i32)]
+
+
+class SimulationStatsC(ctypes.Structure):
+    _fields_ = [("timesteps", c_u64), ("sim_time", c_f64), ("wall_time", c_f64),
+                ("peak_energy", c_f64), ("final_energy", c_f64),
+                ("speed_mcells_per_sec", c_f64)]
+
+
+# name -> (restype, argtypes); every symbol the headers declare
+SIGNATURES = {
+    # include/oems.h
+    "oems_engine_create": (c_i32, [ctypes.POINTER(OperatorDesc), ctypes.POINTER(P)]),
+    "oems_engine_destroy": (None, [P]),
+    "oems_engine_run_batch": (c_i32, [P, ctypes.POINTER(BatchC), ctypes.POINTER(BatchResultC)]),
+    "oems_engine_current_timestep": (c_i32, [P, ctypes.POINTER(c_u64)]),
+    "oems_engine_read_fields": (c_i32, [P, PF * 3, PF * 3]),
+    "oems_engine_write_fields": (c_i32, [P, PF * 3, PF * 3]),
+    "oems_engine_reset": (c_i32, [P]),
+    "oems_engine_add_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
+    "oems_engine_add_point_probe": (c_i32, [P, c_i32, c_u64 * 3, ctypes.POINTER(c_i32)]),
+    "oems_engine_read_probe_traces": (c_i32, [P, PF, c_u64, ctypes.POINTER(c_u64)]),
+    "oems_engine_energy": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
+    "oems_status_string": (ctypes.c_char_p, [c_i32]),
+    "oems_last_error_message": (ctypes.c_char_p, []),
+    "oems_abi_version": (c_i32, []),
+    "oems_engine_last_batch_stats": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_f64)]),
+    "oems_engine_set_kernel_profiling": (c_i32, [P, c_i32]),
+    "oems_engine_kernel_profile": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_u64),
+                                           ctypes.POINTER(c_f64), ctypes.POINTER(c_u64)]),
+    # include/oems_host.h
+    "oems_operator_create": (c_i32, [P, c_u64, P, c_u64, P, c_u64, c_f64, ctypes.POINTER(P)]),
+    "oems_operator_create_uniform": (c_i32, [c_u64, c_u64, c_u64, c_f64, ctypes.POINTER(P)]),
+    "oems_operator_destroy": (None, [P]),
+    "oems_operator_set_material": (c_i32, [P, c_f64, c_f64, c_f64, c_f64, c_u64 * 6]),
+    "oems_operator_set_pec": (c_i32, [P, c_u64 * 6]),
+    "oems_operator_info": (c_i32, [P, c_u64 * 3, ctypes.POINTER(c_f64), c_f64 * 3]),
+    "oems_operator_coefficients": (c_i32, [P, PF * 12]),
+    "oems_operator_engine_desc": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(OperatorDesc)]),
+    "oems_excitation_gaussian": (c_i32, [c_f64, c_f64, c_u32, c_u64 * 3, ctypes.POINTER(ExcitationC)]),
+    "oems_excitation_gaussian_modulated": (c_i32, [c_f64, c_f64, c_u32, c_u64 * 3,
+                                                   ctypes.POINTER(ExcitationC)]),
+    "oems_excitation_sinusoidal": (c_i32, [c_f64, c_u32, c_u64 * 3, ctypes.POINTER(ExcitationC)]),
+    "oems_excitation_dirac": (c_i32, [c_f64, c_u32, c_u64 * 3, ctypes.POINTER(ExcitationC)]),
+    "oems_excitation_evaluate": (c_f64, [ctypes.POINTER(ExcitationC), c_f64]),
+    "oems_excitation_sample": (c_i32, [ctypes.POINTER(ExcitationC), c_u64, c_u64, c_f64, PF]),
+    "oems_simulation_create": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(P)]),
+    "oems_simulation_destroy": (None, [P]),
+    "oems_simulation_add_excitation": (c_i32, [P, ctypes.POINTER(ExcitationC)]),
+    "oems_simulation_set_end_condition": (c_i32, [P, c_i32, c_f64]),
+    "oems_simulation_set_batch_size": (c_i32, [P, c_u64]),
+    "oems_simulation_set_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
+    "oems_simulation_setup": (c_i32, [P]),
+    "oems_simulation_run": (c_i32, [P, ctypes.POINTER(SimulationStatsC)]),
+    "oems_simulation_engine": (P, [P]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python openems_b200/build.py` "
+                "(the engine has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    """Raise the OpenEMSError subclass matching a non-zero status."""
+    if status == OK:
+        return
+    msg = lib().oems_last_error_message().decode(errors="replace")
+    name = lib().oems_status_string(status).decode(errors="replace")
+    cls = _ERRORS.get(status, OpenEMSError)
+    raise cls(f"{name}: {msg}" if msg else name, status)
+
+
+def fptr(a) -> "ctypes._Pointer":
+    """float* to the data of a C-contiguous float32 numpy array."""
+    return a.ctypes.data_as(PF)

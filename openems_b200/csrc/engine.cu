@@ -1,0 +1,1184 @@
+// engine.cu -- the B200 FDTD engine behind the C ABI in include/oems.h.
+//
+// One engine = one grid on one GPU.  All state (fields, coefficients, CPML psi,
+// probe traces, energy samples, excitation waveforms) stays resident in HBM;
+// the host only uploads the operator once, the sampled waveforms per batch, and
+// reads back small results.  A batch is planned on the host into spans of
+// timesteps between energy samples / termination checks; each span replays a
+// captured CUDA graph (H kernel, E kernel, post-step kernel per timestep), so
+// the per-step launch cost is that of graph nodes.
+//
+// Step order per timestep (src/fdtd/basic_engine.rs:83-147):
+//   H update -> E update -> excitations -> probes -> timestep += 1 ->
+//   energy sample if cur % sample_interval == 0 ->
+//   energy-decay check if cur > 0 && cur % check_interval == 0.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/oems.h"
+#include "yee_kernels.cuh"
+
+namespace oems {
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+
+thread_local std::string g_last_error;
+
+static oems_status fail(oems_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+#define OEMS_CUDA(call)                                                                        \
+  do {                                                                                         \
+    cudaError_t err_ = (call);                                                                 \
+    if (err_ != cudaSuccess) {                                                                 \
+      return fail(OEMS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_));       \
+    }                                                                                          \
+  } while (0)
+
+#define OEMS_TRY(expr)              \
+  do {                              \
+    oems_status st_ = (expr);       \
+    if (st_ != OEMS_OK) return st_; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// small device kernels
+// ---------------------------------------------------------------------------
+
+// Post-step work of one timestep: excitations (serially, in list order, so
+// duplicate positions behave like the reference's sequential loop,
+// basic_engine.rs:318-394), then point probes.
+struct PostArgs {
+  float* e[3];
+  const float* h[3];
+  int nexc;
+  const long long* exc_idx;    // device linear index (padded layout)
+  const int* exc_meta;         // dir | soft << 2
+  const long long* exc_off;    // offset into exc_samples
+  const long long* exc_count;  // number of samples
+  const float* exc_samples;
+  int nprobe;
+  const long long* probe_idx;
+  const int* probe_comp;
+  float* traces;               // [batch step][probe]
+  const long long* d_base;     // batch step of local step 0
+  int local;
+};
+
+__global__ void k_post_step(const PostArgs a) {
+  const long long s = *a.d_base + a.local;
+  if (threadIdx.x == 0) {
+    for (int x = 0; x < a.nexc; ++x) {
+      if (s >= a.exc_count[x]) continue;
+      const float v = a.exc_samples[a.exc_off[x] + s];
+      const int meta = a.exc_meta[x];
+      float* p = a.e[meta & 3] + a.exc_idx[x];
+      *p = (meta >> 2) ? __fadd_rn(*p, v) : v;
+    }
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < a.nprobe; p += blockDim.x) {
+    const int comp = a.probe_comp[p];
+    const float* f = comp < 3 ? a.e[comp] : a.h[comp - 3];
+    a.traces[s * a.nprobe + p] = f[a.probe_idx[p]];
+  }
+}
+
+__global__ void k_set_i64(long long* p, long long v) { *p = v; }
+
+// Energy: per-block partial sums of x^2 in f64 over one array (blockIdx.y),
+// then a fixed-order final sum (deterministic run to run).
+constexpr int kEnergyBlocks = 296;
+constexpr int kEnergyThreads = 256;
+
+struct EnergyArgs {
+  const float* arr[6];
+  long long n4;          // float4 count per array
+  double* partials;      // [6][kEnergyBlocks]
+};
+
+__global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyArgs a) {
+  const float4* p = reinterpret_cast<const float4*>(a.arr[blockIdx.y]);
+  double s = 0.0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.n4;
+       t += (long long)gridDim.x * blockDim.x) {
+    const float4 v = __ldcs(p + t);
+    s += (double)v.x * (double)v.x + (double)v.y * (double)v.y + (double)v.z * (double)v.z +
+         (double)v.w * (double)v.w;
+  }
+  __shared__ double red[kEnergyThreads];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kEnergyThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.partials[blockIdx.y * kEnergyBlocks + blockIdx.x] = red[0];
+}
+
+// out[0] = E energy, out[1] = H energy (each the sum over its 3 components in
+// component order, like VectorField3D::energy, src/arrays/field.rs:314-316).
+__global__ void k_energy_final(const double* partials, double* out) {
+  __shared__ double comp[6];
+  const int c = threadIdx.x;
+  if (c < 6) {
+    double s = 0.0;
+    for (int b = 0; b < kEnergyBlocks; ++b) s += partials[c * kEnergyBlocks + b];
+    comp[c] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[0] = comp[0] + comp[1] + comp[2];
+    out[1] = comp[3] + comp[4] + comp[5];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+
+struct LaunchShape {
+  int block = 256;
+  int ichunk = 8;
+  int grid_h = 0;
+  int grid_e = 0;
+};
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t ensure(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) n = std::max<size_t>(count, 1);
+    return e;
+  }
+};
+
+struct CpmlHost {
+  bool on = false;
+  oems_cpml_desc desc{};
+  CpmlArgs args{};
+  DevBuf<float> prof;
+  DevBuf<float> psi;  // one allocation holding every psi array
+  std::vector<size_t> psi_sizes;
+};
+
+}  // namespace oems
+
+struct oems_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t flags = 0;
+  oems::Geom g{};
+  int nx = 0, ny = 0, nz = 0;
+  double dt = 0.0;
+  double delta[3] = {0, 0, 0};
+  uint64_t timestep = 0;
+  long long ncells_padded = 0;
+
+  // fields and coefficients (one allocation each)
+  float* fields = nullptr;  // 6 * ncells_padded
+  float* coeffs = nullptr;  // 12 * ncells_padded (full mode)
+  void* ids = nullptr;      // compressed mode
+  int id_bytes = 0;         // 0 full, 1 uint8, 2 uint16
+  float* table = nullptr;
+  int ntable = 0;
+
+  oems::CpmlHost cpml;
+
+  // probes
+  std::vector<long long> probe_idx;
+  std::vector<int> probe_comp;
+  oems::DevBuf<long long> d_probe_idx;
+  oems::DevBuf<int> d_probe_comp;
+  oems::DevBuf<float> d_traces;
+  uint64_t traces_steps = 0;
+
+  // excitations for the current batch
+  oems::DevBuf<long long> d_exc_idx, d_exc_off, d_exc_count;
+  oems::DevBuf<int> d_exc_meta;
+  oems::DevBuf<float> d_exc_samples;
+  int nexc = 0;
+
+  // energy
+  oems::DevBuf<double> d_partials;
+  oems::DevBuf<double> d_energy;  // [sample][2]
+  double* h_energy = nullptr;     // pinned mirror
+  size_t h_energy_cap = 0;
+
+  oems::DevBuf<long long> d_base;
+
+  oems::LaunchShape shape;
+  bool tuned = false;
+
+  // graphs keyed by span length; invalidated when any baked pointer changes
+  std::map<int, cudaGraphExec_t> graphs;
+  uint64_t graph_epoch = 0, built_epoch = ~0ull;
+
+  // per-kernel profiling
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;  // 4 per step: h0 h1 e0 e1
+  double prof_h_s = 0.0, prof_e_s = 0.0;
+  uint64_t prof_h_n = 0, prof_e_n = 0;
+
+  uint64_t last_launches = 0;
+  double last_device_seconds = 0.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  float* E(int c) { return fields + (size_t)c * ncells_padded; }
+  float* H(int c) { return fields + (size_t)(3 + c) * ncells_padded; }
+  float* C(int a) { return coeffs + (size_t)a * ncells_padded; }
+};
+
+namespace oems {
+
+static void drop_graphs(oems_engine* en) {
+  for (auto& kv : en->graphs) cudaGraphExecDestroy(kv.second);
+  en->graphs.clear();
+}
+
+static Geom make_geom(const oems_engine* en, int block, int ichunk) {
+  Geom g{};
+  g.nx = en->nx;
+  g.ny = en->ny;
+  g.nz = en->nz;
+  g.nzp = (en->nz + 3) / 4 * 4;
+  g.nzq = g.nzp / 4;
+  g.plane = (long long)g.ny * g.nzp;
+  g.plane4 = g.ny * g.nzq;
+  g.tiles = (g.plane4 + block - 1) / block;
+  g.ichunk = ichunk;
+  g.nchunks = (g.nx + ichunk - 1) / ichunk;
+  g.work = g.tiles * g.nchunks;
+  return g;
+}
+
+static HArgs h_args(oems_engine* en) {
+  HArgs a{};
+  a.g = en->g;
+  a.ex = en->E(0);
+  a.ey = en->E(1);
+  a.ez = en->E(2);
+  a.hx = en->H(0);
+  a.hy = en->H(1);
+  a.hz = en->H(2);
+  if (en->id_bytes == 0) {
+    for (int c = 0; c < 3; ++c) {
+      a.da[c] = en->C(6 + c);
+      a.db[c] = en->C(9 + c);
+    }
+  }
+  a.ids = en->ids;
+  a.table = en->table;
+  a.ntable = en->ntable;
+  a.cp = en->cpml.args;
+  return a;
+}
+
+static EArgs e_args(oems_engine* en) {
+  EArgs a{};
+  a.g = en->g;
+  a.ex = en->E(0);
+  a.ey = en->E(1);
+  a.ez = en->E(2);
+  a.hx = en->H(0);
+  a.hy = en->H(1);
+  a.hz = en->H(2);
+  if (en->id_bytes == 0) {
+    for (int c = 0; c < 3; ++c) {
+      a.ca[c] = en->C(c);
+      a.cb[c] = en->C(3 + c);
+    }
+  }
+  a.ids = en->ids;
+  a.table = en->table;
+  a.ntable = en->ntable;
+  a.cp = en->cpml.args;
+  return a;
+}
+
+using HKernel = void (*)(HArgs);
+using EKernel = void (*)(EArgs);
+
+static HKernel pick_h(int id_bytes, bool cpml) {
+  if (id_bytes == 0) return cpml ? k_update_h<0, true> : k_update_h<0, false>;
+  if (id_bytes == 1) return cpml ? k_update_h<1, true> : k_update_h<1, false>;
+  return cpml ? k_update_h<2, true> : k_update_h<2, false>;
+}
+static EKernel pick_e(int id_bytes, bool cpml) {
+  if (id_bytes == 0) return cpml ? k_update_e<0, true> : k_update_e<0, false>;
+  if (id_bytes == 1) return cpml ? k_update_e<1, true> : k_update_e<1, false>;
+  return cpml ? k_update_e<2, true> : k_update_e<2, false>;
+}
+
+static size_t table_smem(const oems_engine* en) {
+  return en->id_bytes == 1 ? (size_t)en->ntable * 12 * sizeof(float) : 0;
+}
+
+// Grid = resident CTAs (occupancy x SMs), capped by the work item count.
+static oems_status size_grid(oems_engine* en, LaunchShape& s) {
+  int sms = 0;
+  OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, en->device));
+  const size_t smem = table_smem(en);
+  int occ_h = 0, occ_e = 0;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ_h, (const void*)pick_h(en->id_bytes, en->cpml.on), s.block, smem));
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ_e, (const void*)pick_e(en->id_bytes, en->cpml.on), s.block, smem));
+  const Geom g = make_geom(en, s.block, s.ichunk);
+  s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h) * sms));
+  s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e) * sms));
+  return OEMS_OK;
+}
+
+static void apply_shape(oems_engine* en, const LaunchShape& s) {
+  en->shape = s;
+  en->g = make_geom(en, s.block, s.ichunk);
+  en->graph_epoch++;
+}
+
+static cudaError_t launch_h(oems_engine* en) {
+  HArgs a = h_args(en);
+  pick_h(en->id_bytes, en->cpml.on)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
+  return cudaGetLastError();
+}
+static cudaError_t launch_e(oems_engine* en) {
+  EArgs a = e_args(en);
+  pick_e(en->id_bytes, en->cpml.on)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
+  return cudaGetLastError();
+}
+
+static bool need_post(const oems_engine* en) { return en->nexc > 0 || !en->probe_idx.empty(); }
+
+static cudaError_t launch_post(oems_engine* en, int local) {
+  PostArgs a{};
+  for (int c = 0; c < 3; ++c) {
+    a.e[c] = en->E(c);
+    a.h[c] = en->H(c);
+  }
+  a.nexc = en->nexc;
+  a.exc_idx = en->d_exc_idx.p;
+  a.exc_meta = en->d_exc_meta.p;
+  a.exc_off = en->d_exc_off.p;
+  a.exc_count = en->d_exc_count.p;
+  a.exc_samples = en->d_exc_samples.p;
+  a.nprobe = (int)en->probe_idx.size();
+  a.probe_idx = en->d_probe_idx.p;
+  a.probe_comp = en->d_probe_comp.p;
+  a.traces = en->d_traces.p;
+  a.d_base = en->d_base.p;
+  a.local = local;
+  k_post_step<<<1, 128, 0, en->stream>>>(a);
+  return cudaGetLastError();
+}
+
+static int kernels_per_step(const oems_engine* en) { return 2 + (need_post(en) ? 1 : 0); }
+
+// Launches `steps` timesteps directly (no graph).
+static oems_status launch_steps_direct(oems_engine* en, int steps) {
+  for (int s = 0; s < steps; ++s) {
+    OEMS_CUDA(launch_h(en));
+    OEMS_CUDA(launch_e(en));
+    if (need_post(en)) OEMS_CUDA(launch_post(en, s));
+  }
+  return OEMS_OK;
+}
+
+// Direct launches with an event pair around every H and E kernel; the span is
+// processed in chunks of at most 64 steps, reading the events after each.
+static oems_status launch_steps_profiled(oems_engine* en, int steps) {
+  constexpr int kChunk = 64;
+  if (en->prof_ev.empty()) {
+    en->prof_ev.resize(4 * kChunk, nullptr);
+    for (auto& e : en->prof_ev) OEMS_CUDA(cudaEventCreate(&e));
+  }
+  for (int s0 = 0; s0 < steps; s0 += kChunk) {
+    const int n = std::min(kChunk, steps - s0);
+    for (int s = 0; s < n; ++s) {
+      cudaEvent_t* ev = &en->prof_ev[4 * s];
+      OEMS_CUDA(cudaEventRecord(ev[0], en->stream));
+      OEMS_CUDA(launch_h(en));
+      OEMS_CUDA(cudaEventRecord(ev[1], en->stream));
+      OEMS_CUDA(cudaEventRecord(ev[2], en->stream));
+      OEMS_CUDA(launch_e(en));
+      OEMS_CUDA(cudaEventRecord(ev[3], en->stream));
+      if (need_post(en)) OEMS_CUDA(launch_post(en, s0 + s));
+    }
+    OEMS_CUDA(cudaEventSynchronize(en->prof_ev[4 * (n - 1) + 3]));
+    for (int s = 0; s < n; ++s) {
+      float h = 0.f, e = 0.f;
+      OEMS_CUDA(cudaEventElapsedTime(&h, en->prof_ev[4 * s], en->prof_ev[4 * s + 1]));
+      OEMS_CUDA(cudaEventElapsedTime(&e, en->prof_ev[4 * s + 2], en->prof_ev[4 * s + 3]));
+      en->prof_h_s += h * 1e-3;
+      en->prof_e_s += e * 1e-3;
+    }
+    en->prof_h_n += n;
+    en->prof_e_n += n;
+  }
+  return OEMS_OK;
+}
+
+static oems_status get_graph(oems_engine* en, int steps, cudaGraphExec_t* out) {
+  if (en->built_epoch != en->graph_epoch) {
+    drop_graphs(en);
+    en->built_epoch = en->graph_epoch;
+  }
+  auto it = en->graphs.find(steps);
+  if (it != en->graphs.end()) {
+    *out = it->second;
+    return OEMS_OK;
+  }
+  if (en->graphs.size() >= 8) drop_graphs(en);
+  cudaGraph_t graph = nullptr;
+  OEMS_CUDA(cudaStreamBeginCapture(en->stream, cudaStreamCaptureModeThreadLocal));
+  oems_status st = launch_steps_direct(en, steps);
+  cudaError_t ce = cudaStreamEndCapture(en->stream, &graph);
+  if (st != OEMS_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (ce != cudaSuccess) return fail(OEMS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  cudaGraphExec_t exec = nullptr;
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return fail(OEMS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+  en->graphs[steps] = exec;
+  *out = exec;
+  return OEMS_OK;
+}
+
+// Runs batch steps [base, base + steps).
+static oems_status run_span(oems_engine* en, long long base, int steps) {
+  if (need_post(en)) {
+    k_set_i64<<<1, 1, 0, en->stream>>>(en->d_base.p, base);
+    OEMS_CUDA(cudaGetLastError());
+    en->last_launches += 1;
+  }
+  if (en->profiling) {
+    OEMS_TRY(launch_steps_profiled(en, steps));
+  } else if (en->flags & OEMS_ENGINE_NO_GRAPHS) {
+    OEMS_TRY(launch_steps_direct(en, steps));
+  } else {
+    cudaGraphExec_t exec = nullptr;
+    OEMS_TRY(get_graph(en, steps, &exec));
+    OEMS_CUDA(cudaGraphLaunch(exec, en->stream));
+  }
+  en->last_launches += (uint64_t)steps * kernels_per_step(en);
+  return OEMS_OK;
+}
+
+static oems_status launch_energy(oems_engine* en, double* out2) {
+  EnergyArgs a{};
+  for (int c = 0; c < 6; ++c) a.arr[c] = en->fields + (size_t)c * en->ncells_padded;
+  a.n4 = en->ncells_padded / 4;
+  a.partials = en->d_partials.p;
+  k_energy_partial<<<dim3(kEnergyBlocks, 6), kEnergyThreads, 0, en->stream>>>(a);
+  OEMS_CUDA(cudaGetLastError());
+  k_energy_final<<<1, 32, 0, en->stream>>>(en->d_partials.p, out2);
+  OEMS_CUDA(cudaGetLastError());
+  en->last_launches += 2;
+  return OEMS_OK;
+}
+
+static oems_status ensure_host_energy(oems_engine* en, size_t samples) {
+  if (samples <= en->h_energy_cap) return OEMS_OK;
+  if (en->h_energy) cudaFreeHost(en->h_energy);
+  for (cudaEvent_t e : en->prof_ev) cudaEventDestroy(e);
+  en->h_energy = nullptr;
+  en->h_energy_cap = 0;
+  OEMS_CUDA(cudaMallocHost(&en->h_energy, std::max<size_t>(samples, 16) * 2 * sizeof(double)));
+  en->h_energy_cap = std::max<size_t>(samples, 16);
+  return OEMS_OK;
+}
+
+// Times `reps` H+E pairs with the current shape (device time in ms).
+static oems_status time_shape(oems_engine* en, int reps, float* ms) {
+  OEMS_CUDA(launch_h(en));
+  OEMS_CUDA(launch_e(en));
+  OEMS_CUDA(cudaEventRecord(en->ev0, en->stream));
+  for (int r = 0; r < reps; ++r) {
+    OEMS_CUDA(launch_h(en));
+    OEMS_CUDA(launch_e(en));
+  }
+  OEMS_CUDA(cudaEventRecord(en->ev1, en->stream));
+  OEMS_CUDA(cudaEventSynchronize(en->ev1));
+  OEMS_CUDA(cudaEventElapsedTime(ms, en->ev0, en->ev1));
+  return OEMS_OK;
+}
+
+// Launch shapes already tuned in this process, keyed by grid, device and
+// kernel variant (like a cuDNN benchmark cache).
+struct TuneKey {
+  int dev, nx, ny, nz, id_bytes, cpml;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, nx, ny, nz, id_bytes, cpml) < std::tie(o.dev, o.nx, o.ny, o.nz, o.id_bytes, o.cpml);
+  }
+};
+static std::map<TuneKey, LaunchShape>& tune_cache() {
+  static std::map<TuneKey, LaunchShape> m;
+  return m;
+}
+
+// Project autotuner: tries CTA sizes and x-chunk depths on scratch copies of
+// the state (fields and psi are saved and restored), keeps the fastest.
+static oems_status autotune(oems_engine* en) {
+  en->tuned = true;
+  if (en->flags & OEMS_ENGINE_NO_AUTOTUNE) return OEMS_OK;
+  const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes, en->cpml.on ? 1 : 0};
+  auto hit = tune_cache().find(key);
+  if (hit != tune_cache().end()) {
+    apply_shape(en, hit->second);
+    return OEMS_OK;
+  }
+  const size_t fbytes = (size_t)6 * en->ncells_padded * sizeof(float);
+  const size_t pbytes = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
+  float* save = nullptr;
+  OEMS_CUDA(cudaMalloc(&save, fbytes + pbytes));
+  OEMS_CUDA(cudaMemcpyAsync(save, en->fields, fbytes, cudaMemcpyDeviceToDevice, en->stream));
+  if (pbytes)
+    OEMS_CUDA(cudaMemcpyAsync((char*)save + fbytes, en->cpml.psi.p, pbytes, cudaMemcpyDeviceToDevice,
+                              en->stream));
+  const long long cells = (long long)en->nx * en->ny * en->nz;
+  const int reps = (int)std::max<long long>(2, std::min<long long>(20, 200000000LL / std::max(1LL, cells)));
+  LaunchShape best = en->shape;
+  float best_ms = 1e30f;
+  const int blocks[] = {128, 256, 512};
+  const int chunks[] = {4, 8, 16, 32, 64};
+  oems_status st = OEMS_OK;
+  for (int b : blocks) {
+    for (int c : chunks) {
+      if (c > 2 * en->nx && c != 4) continue;
+      LaunchShape s;
+      s.block = b;
+      s.ichunk = c;
+      st = size_grid(en, s);
+      if (st != OEMS_OK) break;
+      apply_shape(en, s);
+      float ms = 0.f;
+      st = time_shape(en, reps, &ms);
+      if (st != OEMS_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = s;
+      }
+    }
+    if (st != OEMS_OK) break;
+  }
+  apply_shape(en, best);
+  if (st == OEMS_OK) tune_cache()[key] = best;
+  cudaMemcpyAsync(en->fields, save, fbytes, cudaMemcpyDeviceToDevice, en->stream);
+  if (pbytes) cudaMemcpyAsync(en->cpml.psi.p, (char*)save + fbytes, pbytes, cudaMemcpyDeviceToDevice, en->stream);
+  cudaStreamSynchronize(en->stream);
+  cudaFree(save);
+  return st;
+}
+
+struct CoefKey {
+  float v[12];
+  bool operator==(const CoefKey& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
+};
+struct CoefKeyHash {
+  size_t operator()(const CoefKey& k) const {
+    uint64_t h = 1469598103934665603ull;
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(k.v);
+    for (size_t i = 0; i < sizeof(k.v); ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return (size_t)h;
+  }
+};
+
+static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc* d) {
+  const size_t nzp = en->g.nzp;
+  const size_t rows = (size_t)en->nx * en->ny;
+  const float* src[12] = {d->ca[0], d->ca[1], d->ca[2], d->cb[0], d->cb[1], d->cb[2],
+                          d->da[0], d->da[1], d->da[2], d->db[0], d->db[1], d->db[2]};
+  for (int a = 0; a < 12; ++a)
+    if (!src[a]) return fail(OEMS_ERR_INVALID_ARGUMENT, "coefficient array pointer is NULL");
+  if (!(en->flags & OEMS_ENGINE_COMPRESSED)) {
+    OEMS_CUDA(cudaMalloc(&en->coeffs, (size_t)12 * en->ncells_padded * sizeof(float)));
+    OEMS_CUDA(cudaMemsetAsync(en->coeffs, 0, (size_t)12 * en->ncells_padded * sizeof(float), en->stream));
+    for (int a = 0; a < 12; ++a)
+      OEMS_CUDA(cudaMemcpy2DAsync(en->C(a), nzp * sizeof(float), src[a], en->nz * sizeof(float),
+                                  en->nz * sizeof(float), rows, cudaMemcpyHostToDevice, en->stream));
+    OEMS_CUDA(cudaStreamSynchronize(en->stream));
+    return OEMS_OK;
+  }
+  // Compressed: exact (bitwise) deduplication of the 12 coefficients of each
+  // cell into a table; the reference quantises at 1e-10
+  // (src/fdtd/compressed.rs:11-31), which is below one f32 ulp for every
+  // coefficient magnitude the operator produces, so the two agree.
+  std::unordered_map<CoefKey, uint32_t, CoefKeyHash> map;
+  std::vector<float> table;
+  std::vector<uint16_t> ids16((size_t)en->ncells_padded, 0);
+  const size_t n = (size_t)en->nx * en->ny * en->nz;
+  for (size_t r = 0; r < rows; ++r) {
+    for (int k = 0; k < en->nz; ++k) {
+      const size_t q = r * en->nz + k;
+      CoefKey key;
+      for (int a = 0; a < 12; ++a) key.v[a] = src[a][q];
+      auto it = map.find(key);
+      uint32_t id;
+      if (it == map.end()) {
+        id = (uint32_t)map.size();
+        if (id >= 65536) return fail(OEMS_ERR_MATERIAL, "more than 65536 unique coefficient sets; compressed storage refused");
+        map.emplace(key, id);
+        table.insert(table.end(), key.v, key.v + 12);
+      } else {
+        id = it->second;
+      }
+      ids16[r * nzp + k] = (uint16_t)id;
+    }
+  }
+  (void)n;
+  en->ntable = (int)map.size();
+  OEMS_CUDA(cudaMalloc(&en->table, table.size() * sizeof(float)));
+  OEMS_CUDA(cudaMemcpy(en->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice));
+  if (en->ntable <= 256) {
+    en->id_bytes = 1;
+    std::vector<uint8_t> ids8(ids16.size());
+    for (size_t q = 0; q < ids16.size(); ++q) ids8[q] = (uint8_t)ids16[q];
+    OEMS_CUDA(cudaMalloc(&en->ids, ids8.size()));
+    OEMS_CUDA(cudaMemcpy(en->ids, ids8.data(), ids8.size(), cudaMemcpyHostToDevice));
+  } else {
+    en->id_bytes = 2;
+    OEMS_CUDA(cudaMalloc(&en->ids, ids16.size() * sizeof(uint16_t)));
+    OEMS_CUDA(cudaMemcpy(en->ids, ids16.data(), ids16.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  }
+  return OEMS_OK;
+}
+
+static void destroy(oems_engine* en) {
+  if (!en) return;
+  if (en->stream) cudaStreamSynchronize(en->stream);
+  drop_graphs(en);
+  if (en->fields) cudaFree(en->fields);
+  if (en->coeffs) cudaFree(en->coeffs);
+  if (en->ids) cudaFree(en->ids);
+  if (en->table) cudaFree(en->table);
+  if (en->h_energy) cudaFreeHost(en->h_energy);
+  if (en->ev0) cudaEventDestroy(en->ev0);
+  if (en->ev1) cudaEventDestroy(en->ev1);
+  if (en->stream) cudaStreamDestroy(en->stream);
+  delete en;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+static oems_status create(const oems_operator_desc* d, oems_engine** out) {
+  if (!d || !out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL descriptor or output pointer");
+  *out = nullptr;
+  if (d->nx == 0 || d->ny == 0 || d->nz == 0) return fail(OEMS_ERR_GRID, "grid dimensions must be positive");
+  if (d->nx > (1u << 30) || d->ny > (1u << 30) || d->nz > (1u << 30))
+    return fail(OEMS_ERR_GRID, "grid dimension too large");
+  const uint64_t nzp = (d->nz + 3) / 4 * 4;
+  if ((double)d->ny * (double)nzp / 4.0 > 2.0e9) return fail(OEMS_ERR_GRID, "x-plane too large");
+  if (!(d->dt > 0.0) || !std::isfinite(d->dt)) return fail(OEMS_ERR_CONFIG, "dt must be positive and finite");
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(OEMS_ERR_NO_DEVICE, cudaGetErrorString(ce));
+  }
+  int dev = d->device;
+  if (dev < 0) OEMS_CUDA(cudaGetDevice(&dev));
+  if (dev >= ndev) return fail(OEMS_ERR_NO_DEVICE, "device ordinal out of range");
+  DeviceGuard guard(dev);
+  std::unique_ptr<oems_engine, void (*)(oems_engine*)> en(new oems_engine, destroy);
+  en->device = dev;
+  en->flags = d->flags;
+  en->nx = (int)d->nx;
+  en->ny = (int)d->ny;
+  en->nz = (int)d->nz;
+  en->dt = d->dt;
+  for (int a = 0; a < 3; ++a) en->delta[a] = d->delta[a];
+  OEMS_CUDA(cudaStreamCreateWithFlags(&en->stream, cudaStreamNonBlocking));
+  OEMS_CUDA(cudaEventCreate(&en->ev0));
+  OEMS_CUDA(cudaEventCreate(&en->ev1));
+  en->g = make_geom(en.get(), 256, 8);
+  en->ncells_padded = (long long)en->nx * en->ny * en->g.nzp;
+  OEMS_CUDA(cudaMalloc(&en->fields, (size_t)6 * en->ncells_padded * sizeof(float)));
+  OEMS_CUDA(cudaMemsetAsync(en->fields, 0, (size_t)6 * en->ncells_padded * sizeof(float), en->stream));
+  OEMS_TRY(upload_coefficients(en.get(), d));
+  OEMS_CUDA(cudaMalloc(&en->d_partials.p, 6 * kEnergyBlocks * sizeof(double)));
+  en->d_partials.n = 6 * kEnergyBlocks;
+  OEMS_CUDA(en->d_base.ensure(1));
+  LaunchShape s;
+  OEMS_TRY(size_grid(en.get(), s));
+  apply_shape(en.get(), s);
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  *out = en.release();
+  return OEMS_OK;
+}
+
+static oems_status upload_excitations(oems_engine* en, const oems_batch* b) {
+  en->nexc = (int)b->num_excitations;
+  if (en->nexc == 0) return OEMS_OK;
+  if (!b->excitations) return fail(OEMS_ERR_INVALID_ARGUMENT, "excitation list is NULL");
+  std::vector<long long> idx(en->nexc), off(en->nexc), cnt(en->nexc);
+  std::vector<int> meta(en->nexc);
+  long long total = 0;
+  for (int x = 0; x < en->nexc; ++x) {
+    const oems_scheduled_excitation& e = b->excitations[x];
+    if (e.position[0] >= (uint64_t)en->nx || e.position[1] >= (uint64_t)en->ny || e.position[2] >= (uint64_t)en->nz)
+      return fail(OEMS_ERR_CONFIG, "excitation position outside the grid");
+    if (e.direction > 2) return fail(OEMS_ERR_CONFIG, "excitation direction must be 0, 1 or 2");
+    if (e.num_samples > 0 && !e.samples) return fail(OEMS_ERR_INVALID_ARGUMENT, "excitation samples are NULL");
+    idx[x] = ((long long)e.position[0] * en->ny + (long long)e.position[1]) * en->g.nzp + (long long)e.position[2];
+    meta[x] = (int)e.direction | ((e.soft_source ? 1 : 0) << 2);
+    // only the samples this batch can use are uploaded
+    cnt[x] = (long long)std::min<uint64_t>(e.num_samples, b->num_steps);
+    off[x] = total;
+    total += cnt[x];
+  }
+  bool realloc = false;
+  realloc |= en->d_exc_idx.n < (size_t)en->nexc || en->d_exc_samples.n < (size_t)std::max(total, 1LL);
+  OEMS_CUDA(en->d_exc_idx.ensure(en->nexc));
+  OEMS_CUDA(en->d_exc_off.ensure(en->nexc));
+  OEMS_CUDA(en->d_exc_count.ensure(en->nexc));
+  OEMS_CUDA(en->d_exc_meta.ensure(en->nexc));
+  OEMS_CUDA(en->d_exc_samples.ensure(std::max(total, 1LL)));
+  if (realloc) en->graph_epoch++;
+  OEMS_CUDA(cudaMemcpyAsync(en->d_exc_idx.p, idx.data(), en->nexc * sizeof(long long), cudaMemcpyHostToDevice, en->stream));
+  OEMS_CUDA(cudaMemcpyAsync(en->d_exc_off.p, off.data(), en->nexc * sizeof(long long), cudaMemcpyHostToDevice, en->stream));
+  OEMS_CUDA(cudaMemcpyAsync(en->d_exc_count.p, cnt.data(), en->nexc * sizeof(long long), cudaMemcpyHostToDevice, en->stream));
+  OEMS_CUDA(cudaMemcpyAsync(en->d_exc_meta.p, meta.data(), en->nexc * sizeof(int), cudaMemcpyHostToDevice, en->stream));
+  for (int x = 0; x < en->nexc; ++x)
+    if (cnt[x] > 0)
+      OEMS_CUDA(cudaMemcpyAsync(en->d_exc_samples.p + off[x], b->excitations[x].samples, cnt[x] * sizeof(float),
+                                cudaMemcpyHostToDevice, en->stream));
+  // the host buffers are borrowed only for this call
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  return OEMS_OK;
+}
+
+static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_result* r) {
+  if (!b || !r) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL batch or result");
+  DeviceGuard guard(en->device);
+  const auto t_start = std::chrono::steady_clock::now();
+  en->last_launches = 0;
+  if (!en->tuned) OEMS_TRY(autotune(en));
+  const int prev_nexc = en->nexc;
+  OEMS_TRY(upload_excitations(en, b));
+  if (prev_nexc != en->nexc) en->graph_epoch++;  // nexc is baked into captured graphs
+  const uint64_t steps = b->num_steps;
+  const int nprobe = (int)en->probe_idx.size();
+  if (nprobe > 0) {
+    const size_t need = (size_t)std::max<uint64_t>(steps, 1) * nprobe;
+    if (en->d_traces.n < need) {
+      OEMS_CUDA(en->d_traces.ensure(need));
+      en->graph_epoch++;
+    }
+  }
+  const uint64_t si = b->sample_interval, ci = b->check_interval;
+  const bool has_decay = b->has_energy_decay_db != 0;
+  // worst-case number of energy samples this batch can take
+  const uint64_t t0 = en->timestep;
+  uint64_t max_samples = 0;
+  if (si > 0 && steps > 0) {
+    const uint64_t first = (t0 + si - 1) / si * si;  // first multiple of si >= t0
+    const uint64_t last_step = t0 + steps - 1;
+    max_samples = first > last_step ? 0 : (last_step - first) / si + 1;
+  }
+  OEMS_CUDA(en->d_energy.ensure(2 * (max_samples + 1)));
+  OEMS_TRY(ensure_host_energy(en, max_samples + 1));
+  double* d_check = en->d_energy.p + 2 * max_samples;  // scratch slot for checks
+
+  std::vector<uint64_t> sample_steps;
+  double peak = b->initial_peak_energy;
+  size_t peaked = 0;  // samples already folded into `peak`
+  uint64_t executed = 0;
+  int reason = OEMS_TERMINATION_STEPS_COMPLETED;
+  double final_db = 0.0;
+  bool numerical = false;
+  OEMS_CUDA(cudaEventRecord(en->ev0, en->stream));
+  uint64_t s = 0;
+  while (s < steps) {
+    const uint64_t cur = t0 + s;
+    // next event step >= cur
+    uint64_t ev = UINT64_MAX;
+    if (si > 0) ev = std::min(ev, (cur + si - 1) / si * si);
+    if (has_decay && ci > 0) {
+      uint64_t c = (cur + ci - 1) / ci * ci;
+      if (c == 0) c = ci;
+      ev = std::min(ev, c);
+    }
+    uint64_t span = steps - s;
+    if (ev != UINT64_MAX && ev - cur + 1 < span) span = ev - cur + 1;
+    span = std::min<uint64_t>(span, 1u << 20);
+    OEMS_TRY(run_span(en, (long long)s, (int)span));
+    s += span;
+    executed = s;
+    const uint64_t last = t0 + s - 1;  // `cur` of the last executed step
+    const bool do_sample = si > 0 && last % si == 0;
+    const bool do_check = has_decay && ci > 0 && last > 0 && last % ci == 0;
+    if (do_sample) {
+      OEMS_TRY(launch_energy(en, en->d_energy.p + 2 * sample_steps.size()));
+      sample_steps.push_back(last);
+    }
+    if (do_check) {
+      double* src = do_sample ? en->d_energy.p + 2 * (sample_steps.size() - 1) : d_check;
+      if (!do_sample) OEMS_TRY(launch_energy(en, d_check));
+      // bring back every sample taken since the last check, plus this energy
+      const size_t ns = sample_steps.size();
+      if (ns > peaked)
+        OEMS_CUDA(cudaMemcpyAsync(en->h_energy + 2 * peaked, en->d_energy.p + 2 * peaked,
+                                  (ns - peaked) * 2 * sizeof(double), cudaMemcpyDeviceToHost, en->stream));
+      double curE[2];
+      OEMS_CUDA(cudaMemcpyAsync(en->h_energy + 2 * max_samples, src, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                en->stream));
+      OEMS_CUDA(cudaStreamSynchronize(en->stream));
+      curE[0] = en->h_energy[2 * max_samples];
+      curE[1] = en->h_energy[2 * max_samples + 1];
+      for (; peaked < ns; ++peaked) {
+        const double tot = en->h_energy[2 * peaked] + en->h_energy[2 * peaked + 1];
+        if (!std::isfinite(tot)) numerical = true;
+        if (b->track_peak) peak = std::max(peak, tot);
+      }
+      const double tot = curE[0] + curE[1];
+      if (!std::isfinite(tot)) numerical = true;
+      if (numerical) break;
+      if (peak > 0.0 && tot > 0.0) {
+        const double d = 10.0 * std::log10(tot / peak);
+        if (d < -std::fabs(b->energy_decay_db)) {
+          reason = OEMS_TERMINATION_ENERGY_DECAY;
+          final_db = d;
+          break;
+        }
+      }
+    }
+  }
+  OEMS_CUDA(cudaEventRecord(en->ev1, en->stream));
+  const size_t ns = sample_steps.size();
+  if (ns > peaked)
+    OEMS_CUDA(cudaMemcpyAsync(en->h_energy + 2 * peaked, en->d_energy.p + 2 * peaked,
+                              (ns - peaked) * 2 * sizeof(double), cudaMemcpyDeviceToHost, en->stream));
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  for (; peaked < ns; ++peaked) {
+    const double tot = en->h_energy[2 * peaked] + en->h_energy[2 * peaked + 1];
+    if (!std::isfinite(tot)) numerical = true;
+    if (b->track_peak) peak = std::max(peak, tot);
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, en->ev0, en->ev1);
+  en->last_device_seconds = ms * 1e-3;
+  en->timestep = t0 + executed;
+  en->traces_steps = executed;
+  r->timesteps_executed = executed;
+  r->termination_reason = reason;
+  r->reserved0 = 0;
+  r->final_decay_db = final_db;
+  r->num_energy_samples = ns;
+  r->peak_energy = peak;
+  for (size_t q = 0; q < ns && r->energy_samples && q < r->energy_capacity; ++q) {
+    r->energy_samples[q].timestep = sample_steps[q];
+    r->energy_samples[q].e_energy = en->h_energy[2 * q];
+    r->energy_samples[q].h_energy = en->h_energy[2 * q + 1];
+    r->energy_samples[q].total_energy = en->h_energy[2 * q] + en->h_energy[2 * q + 1];
+  }
+  r->elapsed_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (numerical) return fail(OEMS_ERR_NUMERICAL, "field energy became NaN or infinite");
+  return OEMS_OK;
+}
+
+static oems_status copy_fields(oems_engine* en, float* const* host6, bool to_host) {
+  DeviceGuard guard(en->device);
+  const size_t rows = (size_t)en->nx * en->ny;
+  for (int c = 0; c < 6; ++c) {
+    if (!host6[c]) return fail(OEMS_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+    float* dev = en->fields + (size_t)c * en->ncells_padded;
+    if (to_host)
+      OEMS_CUDA(cudaMemcpy2DAsync(host6[c], en->nz * sizeof(float), dev, en->g.nzp * sizeof(float),
+                                  en->nz * sizeof(float), rows, cudaMemcpyDeviceToHost, en->stream));
+    else
+      OEMS_CUDA(cudaMemcpy2DAsync(dev, en->g.nzp * sizeof(float), host6[c], en->nz * sizeof(float),
+                                  en->nz * sizeof(float), rows, cudaMemcpyHostToDevice, en->stream));
+  }
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  return OEMS_OK;
+}
+
+static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
+  if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL CPML descriptor");
+  if (en->cpml.on) return fail(OEMS_ERR_CONFIG, "CPML already attached");
+  DeviceGuard guard(en->device);
+  const int ext[3] = {en->nx, en->ny, en->nz};
+  int L[6];
+  int lmax = 0;
+  for (int f = 0; f < 6; ++f) {
+    if (d->layers[f] < 0) return fail(OEMS_ERR_CONFIG, "negative CPML layer count");
+    // src/extensions/cpml.rs:262,283: a face is active if 0 < layers < n
+    L[f] = (d->layers[f] > 0 && d->layers[f] < ext[f / 2]) ? d->layers[f] : 0;
+    lmax = std::max(lmax, d->layers[f]);
+  }
+  for (int a = 0; a < 3; ++a)
+    if (L[2 * a] + L[2 * a + 1] > ext[a]) return fail(OEMS_ERR_CONFIG, "CPML slabs overlap");
+  if (lmax <= 0) return fail(OEMS_ERR_CONFIG, "CPML needs at least one face with layers > 0");
+  if (!(d->reflection_coeff > 0.0 && d->reflection_coeff < 1.0))
+    return fail(OEMS_ERR_CONFIG, "CPML reflection coefficient must be in (0, 1)");
+  // src/extensions/cpml.rs:68-72 and :236: sigma_max from the largest layer
+  // count and the smallest cell size
+  const double kEps0 = 8.854187817e-12, kZ0 = 376.730313668;
+  const double dmin = std::min(en->delta[0], std::min(en->delta[1], en->delta[2]));
+  const double sigma_max = -(d->grading_order + 1.0) * std::log(d->reflection_coeff) / (2.0 * kZ0 * (double)lmax * dmin);
+  std::vector<float> prof;
+  CpmlArgs& A = en->cpml.args;
+  std::memset(&A, 0, sizeof(A));
+  for (int f = 0; f < 6; ++f) {
+    const int a = f / 2;
+    const bool is_min = (f % 2) == 0;
+    A.L[f] = L[f];
+    A.start[f] = is_min ? 0 : ext[a] - L[f];
+    A.prof_off[f] = (int)prof.size();
+    if (L[f] == 0) continue;
+    const double width = (double)L[f] * en->delta[a];
+    std::vector<float> rows(6 * L[f]);
+    for (int l = 0; l < L[f]; ++l) {
+      // src/extensions/cpml.rs:114-124
+      const double depth_e = is_min ? (double)(L[f] - l) * en->delta[a] : (double)(l + 1) * en->delta[a];
+      const double depth_h = depth_e - 0.5 * en->delta[a];
+      for (int w = 0; w < 2; ++w) {
+        const double depth = w == 0 ? depth_e : depth_h;
+        const double rho = std::min(1.0, std::max(0.0, depth / width));
+        const double sigma = sigma_max * std::pow(rho, d->grading_order);
+        const double alpha = d->alpha_max * (1.0 - rho);
+        const double kappa = 1.0 + (d->kappa_max - 1.0) * std::pow(rho, d->grading_order);
+        const double bb = std::exp(-(sigma / kappa / kEps0 + alpha / kEps0) * en->dt);
+        const double sn = sigma / (kEps0 * kappa), an = alpha / kEps0, den = sn + an;
+        const double a_ref = std::fabs(den) > 1e-20 ? sn / den * (1.0 - bb) : 0.0;
+        // Roden-Gedney a = sigma/(sigma*kappa + kappa^2*alpha)*(b - 1) = -a_ref/kappa
+        rows[(3 * w + 0) * L[f] + l] = (float)bb;
+        rows[(3 * w + 1) * L[f] + l] = (float)(-a_ref / kappa);
+        rows[(3 * w + 2) * L[f] + l] = (float)(1.0 / kappa);
+      }
+    }
+    prof.insert(prof.end(), rows.begin(), rows.end());
+  }
+  OEMS_CUDA(en->cpml.prof.ensure(prof.size()));
+  OEMS_CUDA(cudaMemcpy(en->cpml.prof.p, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice));
+  A.prof = en->cpml.prof.p;
+  // psi arrays: per face 2 for H and 2 for E
+  const size_t nzp = en->g.nzp;
+  size_t face_sz[6];
+  size_t total = 0;
+  for (int f = 0; f < 6; ++f) {
+    const int a = f / 2;
+    if (L[f] == 0) {
+      face_sz[f] = 0;
+      continue;
+    }
+    if (a == 0) face_sz[f] = (size_t)L[f] * en->ny * nzp;
+    else if (a == 1) face_sz[f] = (size_t)en->nx * L[f] * nzp;
+    else face_sz[f] = (size_t)en->nx * en->ny * L[f];
+    face_sz[f] = (face_sz[f] + 3) / 4 * 4;  // keep every array 16-byte aligned
+    total += 4 * face_sz[f];
+  }
+  OEMS_CUDA(en->cpml.psi.ensure(total));
+  OEMS_CUDA(cudaMemsetAsync(en->cpml.psi.p, 0, total * sizeof(float), en->stream));
+  size_t off = 0;
+  for (int f = 0; f < 6; ++f) {
+    for (int s = 0; s < 2; ++s) {
+      A.psi_h[f][s] = face_sz[f] ? en->cpml.psi.p + off : nullptr;
+      off += face_sz[f];
+      A.psi_e[f][s] = face_sz[f] ? en->cpml.psi.p + off : nullptr;
+      off += face_sz[f];
+    }
+  }
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  en->cpml.on = true;
+  en->cpml.desc = *d;
+  en->tuned = false;  // the CPML kernels get their own launch shape
+  LaunchShape s = en->shape;
+  OEMS_TRY(size_grid(en, s));
+  apply_shape(en, s);
+  return OEMS_OK;
+}
+
+}  // namespace oems
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+using namespace oems;
+
+extern "C" {
+
+oems_status oems_engine_create(const oems_operator_desc* desc, oems_engine** out) {
+  g_last_error.clear();
+  return create(desc, out);
+}
+
+void oems_engine_destroy(oems_engine* engine) {
+  if (!engine) return;
+  DeviceGuard guard(engine->device);
+  destroy(engine);
+}
+
+oems_status oems_engine_run_batch(oems_engine* engine, const oems_batch* batch, oems_batch_result* result) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  g_last_error.clear();
+  return run_batch(engine, batch, result);
+}
+
+oems_status oems_engine_current_timestep(const oems_engine* engine, uint64_t* timestep) {
+  if (!engine || !timestep) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  *timestep = engine->timestep;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_fields(oems_engine* engine, float* const e[3], float* const h[3]) {
+  if (!engine || !e || !h) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  float* all[6] = {e[0], e[1], e[2], h[0], h[1], h[2]};
+  return copy_fields(engine, all, true);
+}
+
+oems_status oems_engine_write_fields(oems_engine* engine, const float* const e[3], const float* const h[3]) {
+  if (!engine || !e || !h) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  float* all[6] = {const_cast<float*>(e[0]), const_cast<float*>(e[1]), const_cast<float*>(e[2]),
+                   const_cast<float*>(h[0]), const_cast<float*>(h[1]), const_cast<float*>(h[2])};
+  return copy_fields(engine, all, false);
+}
+
+oems_status oems_engine_reset(oems_engine* engine) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  DeviceGuard guard(engine->device);
+  OEMS_CUDA(cudaMemsetAsync(engine->fields, 0, (size_t)6 * engine->ncells_padded * sizeof(float), engine->stream));
+  if (engine->cpml.on)
+    OEMS_CUDA(cudaMemsetAsync(engine->cpml.psi.p, 0, engine->cpml.psi.n * sizeof(float), engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  engine->timestep = 0;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  return add_cpml(engine, desc);
+}
+
+oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component, const uint64_t position[3],
+                                        int32_t* probe_id) {
+  if (!engine || !position) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (component < 0 || component > 5) return fail(OEMS_ERR_CONFIG, "probe component must be 0..5");
+  if (position[0] >= (uint64_t)engine->nx || position[1] >= (uint64_t)engine->ny ||
+      position[2] >= (uint64_t)engine->nz)
+    return fail(OEMS_ERR_CONFIG, "probe position outside the grid");
+  DeviceGuard guard(engine->device);
+  engine->probe_idx.push_back(((long long)position[0] * engine->ny + (long long)position[1]) * engine->g.nzp +
+                              (long long)position[2]);
+  engine->probe_comp.push_back(component);
+  const size_t np = engine->probe_idx.size();
+  OEMS_CUDA(engine->d_probe_idx.ensure(np + 16));
+  OEMS_CUDA(engine->d_probe_comp.ensure(np + 16));
+  OEMS_CUDA(cudaMemcpy(engine->d_probe_idx.p, engine->probe_idx.data(), np * sizeof(long long), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_probe_comp.p, engine->probe_comp.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  engine->d_traces.ensure(0);
+  engine->graph_epoch++;
+  if (probe_id) *probe_id = (int32_t)(np - 1);
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_probe_traces(oems_engine* engine, float* out, uint64_t max_steps, uint64_t* steps_out) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  const uint64_t steps = std::min<uint64_t>(engine->traces_steps, max_steps);
+  if (steps_out) *steps_out = engine->traces_steps;
+  const size_t np = engine->probe_idx.size();
+  if (steps == 0 || np == 0) return OEMS_OK;
+  if (!out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL output buffer");
+  DeviceGuard guard(engine->device);
+  OEMS_CUDA(cudaMemcpy(out, engine->d_traces.p, steps * np * sizeof(float), cudaMemcpyDeviceToHost));
+  return OEMS_OK;
+}
+
+oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_energy) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  DeviceGuard guard(engine->device);
+  OEMS_CUDA(engine->d_energy.ensure(2));
+  OEMS_TRY(launch_energy(engine, engine->d_energy.p));
+  double out[2];
+  OEMS_CUDA(cudaMemcpyAsync(out, engine->d_energy.p, sizeof(out), cudaMemcpyDeviceToHost, engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  if (e_energy) *e_energy = out[0];
+  if (h_energy) *h_energy = out[1];
+  return OEMS_OK;
+}
+
+oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  engine->profiling = enable != 0;
+  engine->prof_h_s = engine->prof_e_s = 0.0;
+  engine->prof_h_n = engine->prof_e_n = 0;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_kernel_profile(const oems_engine* engine, double* h_seconds, uint64_t* h_launches,
+                                       double* e_seconds, uint64_t* e_launches) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  if (h_seconds) *h_seconds = engine->prof_h_s;
+  if (h_launches) *h_launches = engine->prof_h_n;
+  if (e_seconds) *e_seconds = engine->prof_e_s;
+  if (e_launches) *e_launches = engine->prof_e_n;
+  return OEMS_OK;
+}
+
+const char* oems_status_string(oems_status st) {
+  switch (st) {
+    case OEMS_OK: return "ok";
+    case OEMS_ERR_CONFIG: return "configuration error";
+    case OEMS_ERR_IO: return "I/O error";
+    case OEMS_ERR_GRID: return "grid error";
+    case OEMS_ERR_MATERIAL: return "material error";
+    case OEMS_ERR_NUMERICAL: return "numerical error";
+    case OEMS_ERR_XML: return "XML error";
+    case OEMS_ERR_CUDA: return "CUDA error";
+    case OEMS_ERR_NO_DEVICE: return "no CUDA device";
+    case OEMS_ERR_TIMEOUT: return "device wait timed out";
+    case OEMS_ERR_INVALID_ARGUMENT: return "invalid argument";
+  }
+  return "unknown status";
+}
+
+const char* oems_last_error_message(void) { return g_last_error.c_str(); }
+
+int32_t oems_abi_version(void) { return OEMS_ABI_VERSION; }
+
+oems_status oems_engine_last_batch_stats(const oems_engine* engine, uint64_t* kernel_launches, double* device_seconds) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  if (kernel_launches) *kernel_launches = engine->last_launches;
+  if (device_seconds) *device_seconds = engine->last_device_seconds;
+  return OEMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,431 @@
+// yee_kernels.cuh -- sm_100a Yee update kernels (H and E half-steps).
+//
+// Semantics follow the reference scalar engine:
+//   H: src/fdtd/basic_engine.rs:191-254  (every cell; a forward difference that
+//      would reach index n is 0)
+//   E: src/fdtd/basic_engine.rs:262-306  (only i, j, k >= 1 are written)
+// Every product and sum is rounded separately (__fmul_rn / __fadd_rn /
+// __fsub_rn, no FMA contraction) in the reference's order, so an FP32 run is
+// bit-identical to the unfused Rust arithmetic.  The stencil is HBM-bound; the
+// rounding mode costs nothing.
+//
+// Data layout in HBM: one array per component, z fastest, rows padded to
+// nzp = round_up(nz, 4) floats so every (i, j) row starts 16-byte aligned.
+// Thread mapping: one thread owns one float4 chunk (4 consecutive k) of an
+// x-plane; a warp covers 32 consecutive chunks of the flattened (j, k) plane,
+// so every load is a fully coalesced 128-bit access whatever nz is.  Each CTA
+// marches its tile of chunks through `ichunk` consecutive x-planes, carrying
+// the x-neighbour plane in registers (register-blocked marching along x).
+// z-neighbours come from the adjacent lane by warp shuffle; y-neighbours are
+// the same tile one row over and hit L1.  CTAs loop over (tile, x-chunk) work
+// items, so the grid is sized to the number of resident CTAs.
+//
+// CPML (standard Roden-Gedney recursive convolution with the profile of
+// src/extensions/cpml.rs:68-177) is fused: in a slab cell the difference d
+// along the slab normal becomes d*inv_kappa + psi with psi = b*psi + c*d.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace oems {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+struct Geom {
+  int nx, ny, nz, nzp, nzq;  // nzq = nzp / 4 float4 chunks per row
+  long long plane;           // floats per x-plane = ny * nzp
+  int plane4;                // float4 chunks per x-plane = ny * nzq
+  int tiles;                 // CTA tiles per x-plane
+  int ichunk;                // x-planes per work item
+  int nchunks;               // ceil(nx / ichunk)
+  int work;                  // tiles * nchunks
+};
+
+// CPML state on the device.  Faces: 0 xmin 1 xmax 2 ymin 3 ymax 4 zmin 5 zmax.
+// psi layout per face: x faces [l][j][k] (k pitch nzp), y faces [i][l][k],
+// z faces [i][j][l].  Slot per axis: x: H {Hy, Hz} E {Ey, Ez};
+// y: H {Hx, Hz} E {Ex, Ez}; z: H {Hx, Hy} E {Ex, Ey}.
+struct CpmlArgs {
+  int L[6];
+  int start[6];       // first global index of the slab along its axis
+  int prof_off[6];    // offset of face f in prof: 6 rows of L: b_e c_e ik_e b_h c_h ik_h
+  const float* prof;
+  float* psi_h[6][2];
+  float* psi_e[6][2];
+};
+
+struct HArgs {
+  Geom g;
+  const float* ex;
+  const float* ey;
+  const float* ez;
+  float* hx;
+  float* hy;
+  float* hz;
+  const float* da[3];
+  const float* db[3];
+  const void* ids;     // compressed: per-cell material id (uint8 or uint16)
+  const float* table;  // compressed: [ntable][12] = ca0..2 cb0..2 da0..2 db0..2
+  int ntable;
+  CpmlArgs cp;
+};
+
+struct EArgs {
+  Geom g;
+  float* ex;
+  float* ey;
+  float* ez;
+  const float* hx;
+  const float* hy;
+  const float* hz;
+  const float* ca[3];
+  const float* cb[3];
+  const void* ids;
+  const float* table;
+  int ntable;
+  CpmlArgs cp;
+};
+
+__device__ __forceinline__ float4 ld_nc4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 ld_cs4(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+__device__ __forceinline__ void to_arr(float4 v, float (&a)[4]) {
+  a[0] = v.x;
+  a[1] = v.y;
+  a[2] = v.z;
+  a[3] = v.w;
+}
+__device__ __forceinline__ float4 to_f4(const float (&a)[4]) { return make_float4(a[0], a[1], a[2], a[3]); }
+
+// psi <- b*psi + c*d ; return d*ik + psi (each operation rounded).
+__device__ __forceinline__ float cpml_stretch(float d, float& psi, float b, float c, float ik) {
+  psi = __fadd_rn(__fmul_rn(b, psi), __fmul_rn(c, d));
+  return __fadd_rn(__fmul_rn(d, ik), psi);
+}
+
+// Slab lookup along one axis: returns face (or -1) and layer.
+__device__ __forceinline__ int cpml_face(const CpmlArgs& cp, int axis, int g, int& l) {
+  const int fmin = 2 * axis, fmax = 2 * axis + 1;
+  if (g < cp.L[fmin]) {
+    l = g;
+    return fmin;
+  }
+  if (cp.L[fmax] > 0 && g >= cp.start[fmax]) {
+    l = g - cp.start[fmax];
+    return fmax;
+  }
+  return -1;
+}
+
+// x- or y-slab: the same (face, layer) for all 4 elements of the chunk, psi is
+// a float4 at a 16-byte aligned address.
+__device__ __forceinline__ void cpml_vec(const CpmlArgs& cp, int f, int l, long long pidx, int slot,
+                                         bool is_h, float (&d)[4]) {
+  float* base = is_h ? cp.psi_h[f][slot] : cp.psi_e[f][slot];
+  const int L = cp.L[f];
+  const float* pr = cp.prof + cp.prof_off[f] + (is_h ? 3 * L : 0);
+  const float b = __ldg(pr + l), c = __ldg(pr + L + l), ik = __ldg(pr + 2 * L + l);
+  float4 p4 = ld4(base + pidx);
+  float p[4];
+  to_arr(p4, p);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) d[e] = cpml_stretch(d[e], p[e], b, c, ik);
+  st4(base + pidx, to_f4(p));
+}
+
+// z-slab: per element.  zrow = (i*ny + j).
+// Elements with k < kmin (E: k = 0 is never updated) keep their psi untouched.
+__device__ __forceinline__ void cpml_z(const CpmlArgs& cp, int k0, int kmin, int nz, long long zrow,
+                                       int slot, bool is_h, float (&d)[4]) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = k0 + e;
+    if (k >= nz || k < kmin) continue;
+    int l;
+    const int f = cpml_face(cp, 2, k, l);
+    if (f < 0) continue;
+    const int L = cp.L[f];
+    float* psi = (is_h ? cp.psi_h[f][slot] : cp.psi_e[f][slot]) + zrow * L + l;
+    const float* pr = cp.prof + cp.prof_off[f] + (is_h ? 3 * L : 0);
+    float p = *psi;
+    d[e] = cpml_stretch(d[e], p, __ldg(pr + l), __ldg(pr + L + l), __ldg(pr + 2 * L + l));
+    *psi = p;
+  }
+}
+
+__device__ __forceinline__ bool z_chunk_in_cpml(const CpmlArgs& cp, int k0, int nz) {
+  return (k0 < cp.L[4]) || (cp.L[5] > 0 && k0 + 3 >= cp.start[5] && k0 < nz);
+}
+
+// Per-chunk coefficient fetch: full arrays or compressed table.
+template <int kIdBytes>
+struct Coef {
+  // kIdBytes == 0: full arrays
+  __device__ __forceinline__ static void load(const float* const (&arr)[3], const void* ids, const float* tab,
+                                              int off, long long q, float (&c)[3][4]) {
+    if constexpr (kIdBytes == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        float4 v = ld_cs4(arr[a] + q);
+        to_arr(v, c[a]);
+      }
+    } else if constexpr (kIdBytes == 1) {
+      const uint32_t w = __ldcs(reinterpret_cast<const unsigned int*>(static_cast<const uint8_t*>(ids) + q));
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int id = (w >> (8 * e)) & 0xff;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) c[a][e] = tab[id * 12 + off + a];
+      }
+    } else {
+      const uint2 w = __ldcs(reinterpret_cast<const uint2*>(static_cast<const uint16_t*>(ids) + q));
+      const uint32_t ws[2] = {w.x, w.y};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int id = (ws[e >> 1] >> (16 * (e & 1))) & 0xffff;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) c[a][e] = __ldg(tab + id * 12 + off + a);
+      }
+    }
+  }
+};
+
+// Loads the compressed table into shared memory (uint8 ids only).
+template <int kIdBytes>
+__device__ __forceinline__ const float* stage_table(const float* table, int ntable, float* smem) {
+  if constexpr (kIdBytes == 1) {
+    for (int t = threadIdx.x; t < ntable * 12; t += blockDim.x) smem[t] = __ldg(table + t);
+    __syncthreads();
+    return smem;
+  } else {
+    return table;
+  }
+}
+
+// H half-step: H = da*H + db*curl(E).
+template <int kIdBytes, bool kCpml>
+__global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
+  extern __shared__ float s_table[];
+  const Geom& g = a.g;
+  const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
+  const int lane = threadIdx.x & 31;
+  for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
+    const int tile = w % g.tiles;
+    const int chunk = w / g.tiles;
+    int c = tile * blockDim.x + threadIdx.x;
+    const bool valid = c < g.plane4;
+    if (!valid) c = g.plane4 - 1;
+    const int j = c / g.nzq;
+    const int k0 = (c - j * g.nzq) * 4;
+    const int i0 = chunk * g.ichunk;
+    const int i1 = min(i0 + g.ichunk, g.nx);
+    const bool has_jp = j + 1 < g.ny;
+    const long long row = (long long)j * g.nzp + k0;
+    long long q = (long long)i0 * g.plane + row;
+    float4 ey4 = ld_nc4(a.ey + q);
+    float4 ez4 = ld_nc4(a.ez + q);
+    for (int i = i0; i < i1; ++i, q += g.plane) {
+      const bool has_ip = i + 1 < g.nx;
+      const float4 ex4 = ld_nc4(a.ex + q);
+      const float4 ey1 = has_ip ? ld_nc4(a.ey + q + g.plane) : ey4;
+      const float4 ez1 = has_ip ? ld_nc4(a.ez + q + g.plane) : ez4;
+      const float4 exj = has_jp ? ld_nc4(a.ex + q + g.nzp) : ex4;
+      const float4 ezj = has_jp ? ld_nc4(a.ez + q + g.nzp) : ez4;
+      // first element of the next chunk (k0 + 4)
+      float exn = __shfl_down_sync(kFullMask, ex4.x, 1);
+      float eyn = __shfl_down_sync(kFullMask, ey4.x, 1);
+      if (lane == 31 && k0 + 4 < g.nz) {
+        exn = __ldg(a.ex + q + 4);
+        eyn = __ldg(a.ey + q + 4);
+      }
+      float ex[4], ey[4], ez[4], eyp[4], ezp[4], exjv[4], ezjv[4];
+      to_arr(ex4, ex);
+      to_arr(ey4, ey);
+      to_arr(ez4, ez);
+      to_arr(ey1, eyp);
+      to_arr(ez1, ezp);
+      to_arr(exj, exjv);
+      to_arr(ezj, ezjv);
+      const float exk[4] = {ex[1], ex[2], ex[3], exn};
+      const float eyk[4] = {ey[1], ey[2], ey[3], eyn};
+      float dez_dy[4], dey_dz[4], dex_dz[4], dez_dx[4], dey_dx[4], dex_dy[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool has_kp = k0 + e + 1 < g.nz;
+        dez_dy[e] = has_jp ? __fsub_rn(ezjv[e], ez[e]) : 0.f;
+        dey_dz[e] = has_kp ? __fsub_rn(eyk[e], ey[e]) : 0.f;
+        dex_dz[e] = has_kp ? __fsub_rn(exk[e], ex[e]) : 0.f;
+        dez_dx[e] = has_ip ? __fsub_rn(ezp[e], ez[e]) : 0.f;
+        dey_dx[e] = has_ip ? __fsub_rn(eyp[e], ey[e]) : 0.f;
+        dex_dy[e] = has_jp ? __fsub_rn(exjv[e], ex[e]) : 0.f;
+      }
+      if constexpr (kCpml) {
+        int l;
+        // y-slab: Hx (dEz/dy, slot 0), Hz (dEx/dy, slot 1)
+        int f = cpml_face(a.cp, 1, j, l);
+        if (f >= 0) {
+          const long long p = ((long long)i * a.cp.L[f] + l) * g.nzp + k0;
+          cpml_vec(a.cp, f, l, p, 0, true, dez_dy);
+          cpml_vec(a.cp, f, l, p, 1, true, dex_dy);
+        }
+        // z-slab: Hx (dEy/dz, slot 0), Hy (dEx/dz, slot 1)
+        if (z_chunk_in_cpml(a.cp, k0, g.nz)) {
+          const long long zrow = (long long)i * g.ny + j;
+          cpml_z(a.cp, k0, 0, g.nz, zrow, 0, true, dey_dz);
+          cpml_z(a.cp, k0, 0, g.nz, zrow, 1, true, dex_dz);
+        }
+        // x-slab: Hy (dEz/dx, slot 0), Hz (dEy/dx, slot 1)
+        f = cpml_face(a.cp, 0, i, l);
+        if (f >= 0) {
+          const long long p = ((long long)l * g.ny + j) * g.nzp + k0;
+          cpml_vec(a.cp, f, l, p, 0, true, dez_dx);
+          cpml_vec(a.cp, f, l, p, 1, true, dey_dx);
+        }
+      }
+      float co_a[3][4], co_b[3][4];
+      Coef<kIdBytes>::load(a.da, a.ids, tab, 6, q, co_a);
+      Coef<kIdBytes>::load(a.db, a.ids, tab, 9, q, co_b);
+      float h[3][4];
+      to_arr(ld4(a.hx + q), h[0]);
+      to_arr(ld4(a.hy + q), h[1]);
+      to_arr(ld4(a.hz + q), h[2]);
+      float out[3][4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float curl[3] = {__fsub_rn(dez_dy[e], dey_dz[e]), __fsub_rn(dex_dz[e], dez_dx[e]),
+                               __fsub_rn(dey_dx[e], dex_dy[e])};
+        const bool live = k0 + e < g.nz;
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const float v = __fadd_rn(__fmul_rn(co_a[cc][e], h[cc][e]), __fmul_rn(co_b[cc][e], curl[cc]));
+          out[cc][e] = live ? v : h[cc][e];
+        }
+      }
+      if (valid) {
+        st4(a.hx + q, to_f4(out[0]));
+        st4(a.hy + q, to_f4(out[1]));
+        st4(a.hz + q, to_f4(out[2]));
+      }
+      ey4 = ey1;
+      ez4 = ez1;
+    }
+  }
+}
+
+// E half-step: E = ca*E + cb*curl(H), cells with i, j, k >= 1 only.
+template <int kIdBytes, bool kCpml>
+__global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
+  extern __shared__ float s_table[];
+  const Geom& g = a.g;
+  const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
+  const int lane = threadIdx.x & 31;
+  for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
+    const int tile = w % g.tiles;
+    const int chunk = w / g.tiles;
+    int c = tile * blockDim.x + threadIdx.x;
+    const bool valid = c < g.plane4;
+    if (!valid) c = g.plane4 - 1;
+    const int j = c / g.nzq;
+    const int k0 = (c - j * g.nzq) * 4;
+    const int i0 = chunk * g.ichunk;
+    const int i1 = min(i0 + g.ichunk, g.nx);
+    const bool has_jm = j >= 1;
+    const long long row = (long long)j * g.nzp + k0;
+    long long q = (long long)i0 * g.plane + row;
+    float4 hym4 = make_float4(0.f, 0.f, 0.f, 0.f), hzm4 = hym4;  // H at i-1
+    if (i0 > 0) {
+      hym4 = ld_nc4(a.hy + q - g.plane);
+      hzm4 = ld_nc4(a.hz + q - g.plane);
+    }
+    for (int i = i0; i < i1; ++i, q += g.plane) {
+      const float4 hx4 = ld_nc4(a.hx + q);
+      const float4 hy4 = ld_nc4(a.hy + q);
+      const float4 hz4 = ld_nc4(a.hz + q);
+      // last element of the previous chunk (k0 - 1)
+      float hxm = __shfl_up_sync(kFullMask, hx4.w, 1);
+      float hym = __shfl_up_sync(kFullMask, hy4.w, 1);
+      if (lane == 0 && k0 >= 4) {
+        hxm = __ldg(a.hx + q - 1);
+        hym = __ldg(a.hy + q - 1);
+      }
+      if (i >= 1 && has_jm) {
+        const float4 hxj4 = ld_nc4(a.hx + q - g.nzp);
+        const float4 hzj4 = ld_nc4(a.hz + q - g.nzp);
+        float hx[4], hy[4], hz[4], hxj[4], hzj[4], hyi[4], hzi[4];
+        to_arr(hx4, hx);
+        to_arr(hy4, hy);
+        to_arr(hz4, hz);
+        to_arr(hxj4, hxj);
+        to_arr(hzj4, hzj);
+        to_arr(hym4, hyi);
+        to_arr(hzm4, hzi);
+        const float hxk[4] = {hxm, hx[0], hx[1], hx[2]};
+        const float hyk[4] = {hym, hy[0], hy[1], hy[2]};
+        float dhz_dy[4], dhy_dz[4], dhx_dz[4], dhz_dx[4], dhy_dx[4], dhx_dy[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          dhz_dy[e] = __fsub_rn(hz[e], hzj[e]);
+          dhy_dz[e] = __fsub_rn(hy[e], hyk[e]);
+          dhx_dz[e] = __fsub_rn(hx[e], hxk[e]);
+          dhz_dx[e] = __fsub_rn(hz[e], hzi[e]);
+          dhy_dx[e] = __fsub_rn(hy[e], hyi[e]);
+          dhx_dy[e] = __fsub_rn(hx[e], hxj[e]);
+        }
+        if constexpr (kCpml) {
+          int l;
+          // y-slab: Ex (dHz/dy, slot 0), Ez (dHx/dy, slot 1)
+          int f = cpml_face(a.cp, 1, j, l);
+          if (f >= 0) {
+            const long long p = ((long long)i * a.cp.L[f] + l) * g.nzp + k0;
+            cpml_vec(a.cp, f, l, p, 0, false, dhz_dy);
+            cpml_vec(a.cp, f, l, p, 1, false, dhx_dy);
+          }
+          // z-slab: Ex (dHy/dz, slot 0), Ey (dHx/dz, slot 1); k = 0 is never updated
+          if (z_chunk_in_cpml(a.cp, k0, g.nz)) {
+            const long long zrow = (long long)i * g.ny + j;
+            cpml_z(a.cp, k0, 1, g.nz, zrow, 0, false, dhy_dz);
+            cpml_z(a.cp, k0, 1, g.nz, zrow, 1, false, dhx_dz);
+          }
+          // x-slab: Ey (dHz/dx, slot 0), Ez (dHy/dx, slot 1)
+          f = cpml_face(a.cp, 0, i, l);
+          if (f >= 0) {
+            const long long p = ((long long)l * g.ny + j) * g.nzp + k0;
+            cpml_vec(a.cp, f, l, p, 0, false, dhz_dx);
+            cpml_vec(a.cp, f, l, p, 1, false, dhy_dx);
+          }
+        }
+        float co_a[3][4], co_b[3][4];
+        Coef<kIdBytes>::load(a.ca, a.ids, tab, 0, q, co_a);
+        Coef<kIdBytes>::load(a.cb, a.ids, tab, 3, q, co_b);
+        float ev[3][4];
+        to_arr(ld4(a.ex + q), ev[0]);
+        to_arr(ld4(a.ey + q), ev[1]);
+        to_arr(ld4(a.ez + q), ev[2]);
+        float out[3][4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float curl[3] = {__fsub_rn(dhz_dy[e], dhy_dz[e]), __fsub_rn(dhx_dz[e], dhz_dx[e]),
+                                 __fsub_rn(dhy_dx[e], dhx_dy[e])};
+          const bool live = (k0 + e >= 1) && (k0 + e < g.nz);
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const float v = __fadd_rn(__fmul_rn(co_a[cc][e], ev[cc][e]), __fmul_rn(co_b[cc][e], curl[cc]));
+            out[cc][e] = live ? v : ev[cc][e];
+          }
+        }
+        if (valid) {
+          st4(a.ex + q, to_f4(out[0]));
+          st4(a.ey + q, to_f4(out[1]));
+          st4(a.ez + q, to_f4(out[2]));
+        }
+      }
+      hym4 = hy4;
+      hzm4 = hz4;
+    }
+  }
+}
+
+}  // namespace oems

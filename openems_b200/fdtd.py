@@ -1,0 +1,689 @@
+"""Python mirror of the reference's src/fdtd surface, over liboems_b200.so.
+
+Names and argument meanings follow the Rust openEMS rewrite:
+
+  Grid                       src/geometry/mod.rs:20-255
+  Operator                   src/fdtd/operator.rs:42-263
+  Excitation/ExcitationType  src/fdtd/excitation.rs:9-200
+  ScheduledExcitation        src/fdtd/batch.rs:71-147
+  EngineBatch, TerminationConfig, EnergyMonitorConfig,
+  BatchResult, TerminationReason, EnergySample
+                             src/fdtd/batch.rs:17-228
+  Engine / EngineType        src/fdtd/new_engine.rs:20-153, src/fdtd/mod.rs:69-79
+  BoundaryConditions         src/fdtd/mod.rs:82-167
+  Simulation, EndCondition, SimulationStats
+                             src/fdtd/simulation.rs:36-360
+
+The engine is CUDA only (one GPU, no CPU fallback).  Fields are returned as
+numpy float32 arrays of shape (3, nx, ny, nz), z fastest.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .constants import PI
+
+# ---------------------------------------------------------------------------
+# geometry
+# ---------------------------------------------------------------------------
+
+
+class Grid:
+    """Cartesian mesh lines per axis (cells = lines - 1), scaled by `unit`."""
+
+    def __init__(self, x_lines, y_lines, z_lines, unit: float = 1.0):
+        self.x_lines = np.asarray(x_lines, dtype=np.float64)
+        self.y_lines = np.asarray(y_lines, dtype=np.float64)
+        self.z_lines = np.asarray(z_lines, dtype=np.float64)
+        self.unit = float(unit)
+
+    @classmethod
+    def uniform(cls, nx: int, ny: int, nz: int, delta: float) -> "Grid":
+        """Grid::uniform (src/geometry/mod.rs:60-66): lines = i * delta."""
+        return cls(np.arange(nx + 1) * delta, np.arange(ny + 1) * delta,
+                   np.arange(nz + 1) * delta)
+
+    @classmethod
+    def cartesian(cls, x_lines, y_lines, z_lines) -> "Grid":
+        return cls(x_lines, y_lines, z_lines)
+
+    def dimensions(self) -> Tuple[int, int, int]:
+        return tuple(max(len(v) - 1, 1) for v in (self.x_lines, self.y_lines, self.z_lines))
+
+    @staticmethod
+    def _min_delta(lines) -> float:
+        if len(lines) < 2:
+            return 1.0
+        d = np.diff(lines)
+        d = d[d > 0]
+        return float(d.min())
+
+    def cell_size(self) -> Tuple[float, float, float]:
+        """Minimum line spacing per axis (src/geometry/mod.rs:113-119)."""
+        return tuple(self._min_delta(v) * self.unit
+                     for v in (self.x_lines, self.y_lines, self.z_lines))
+
+
+# ---------------------------------------------------------------------------
+# boundaries
+# ---------------------------------------------------------------------------
+
+
+@dataclass(frozen=True)
+class BoundaryCondition:
+    """One face: kind in {'pec', 'pmc', 'mur', 'pml', 'periodic'}; layers for 'pml'."""
+
+    kind: str = "pec"
+    layers: int = 0
+
+    @staticmethod
+    def pec():
+        return BoundaryCondition("pec")
+
+    @staticmethod
+    def pml(layers: int = 8):
+        return BoundaryCondition("pml", layers)
+
+
+@dataclass
+class BoundaryConditions:
+    """Six faces xmin xmax ymin ymax zmin zmax (src/fdtd/mod.rs:102-167).
+
+    The reference's default is PML with 8 layers on every face
+    (src/fdtd/mod.rs:117-128); its Operator stores but never applies it.  Here
+    a 'pml' face attaches a CPML with that many layers; 'pec' faces keep the
+    reference's stencil truncation.
+    """
+
+    faces: Tuple[BoundaryCondition, ...] = field(
+        default_factory=lambda: tuple(BoundaryCondition.pml(8) for _ in range(6)))
+
+    @classmethod
+    def all_pec(cls):
+        return cls(tuple(BoundaryCondition.pec() for _ in range(6)))
+
+    @classmethod
+    def all_pml(cls, layers: int):
+        return cls(tuple(BoundaryCondition.pml(layers) for _ in range(6)))
+
+    @classmethod
+    def from_array(cls, bc: Sequence[BoundaryCondition]):
+        return cls(tuple(bc))
+
+    def cpml_layers(self) -> Tuple[int, ...]:
+        return tuple(f.layers if f.kind == "pml" else 0 for f in self.faces)
+
+
+@dataclass
+class CpmlBoundaries:
+    """CpmlBoundaries (src/extensions/cpml.rs:27-73); defaults of :41-51."""
+
+    layers: Tuple[int, ...] = (8, 8, 8, 8, 8, 8)
+    grading_order: float = 3.0
+    reflection_coeff: float = 1e-6
+    alpha_max: float = 0.0
+    kappa_max: float = 1.0
+
+    @classmethod
+    def uniform(cls, layers: int):
+        return cls(layers=(layers,) * 6)
+
+    def to_c(self) -> N.CpmlDescC:
+        d = N.CpmlDescC()
+        for f in range(6):
+            d.layers[f] = int(self.layers[f])
+        d.grading_order = self.grading_order
+        d.reflection_coeff = self.reflection_coeff
+        d.alpha_max = self.alpha_max
+        d.kappa_max = self.kappa_max
+        return d
+
+
+# ---------------------------------------------------------------------------
+# operator
+# ---------------------------------------------------------------------------
+
+
+class Operator:
+    """Coefficient precompute (src/fdtd/operator.rs:42-263), in the native library."""
+
+    def __init__(self, grid: Grid, boundaries: Optional[BoundaryConditions] = None):
+        self.grid = grid
+        self.boundaries = boundaries if boundaries is not None else BoundaryConditions()
+        h = ctypes.c_void_p()
+        xl, yl, zl = (np.ascontiguousarray(v, dtype=np.float64)
+                      for v in (grid.x_lines, grid.y_lines, grid.z_lines))
+        N.check(N.lib().oems_operator_create(xl.ctypes.data, len(xl), yl.ctypes.data, len(yl),
+                                             zl.ctypes.data, len(zl), grid.unit, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().oems_operator_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _info(self):
+        dims = (N.c_u64 * 3)()
+        dt = N.c_f64()
+        delta = (N.c_f64 * 3)()
+        N.check(N.lib().oems_operator_info(self._h, dims, ctypes.byref(dt), delta))
+        return tuple(dims), dt.value, tuple(delta)
+
+    def timestep(self) -> float:
+        return self._info()[1]
+
+    def dimensions(self) -> Tuple[int, int, int]:
+        return tuple(int(v) for v in self._info()[0])
+
+    def cell_size(self) -> Tuple[float, float, float]:
+        return self._info()[2]
+
+    @staticmethod
+    def _region(region):
+        r = (N.c_u64 * 6)()
+        for a in range(6):
+            r[a] = int(region[a])
+        return r
+
+    def set_material(self, eps_r, mu_r, sigma_e, sigma_m, region):
+        """region = (i0, i1, j0, j1, k0, k1), half-open."""
+        N.check(N.lib().oems_operator_set_material(self._h, eps_r, mu_r, sigma_e, sigma_m,
+                                                   self._region(region)))
+
+    def set_pec(self, region):
+        N.check(N.lib().oems_operator_set_pec(self._h, self._region(region)))
+
+    def coefficients(self) -> np.ndarray:
+        """Copy of the 12 arrays: (12, nx, ny, nz) = ca0..2, cb0..2, da0..2, db0..2."""
+        ptrs = (N.PF * 12)()
+        N.check(N.lib().oems_operator_coefficients(self._h, ptrs))
+        nx, ny, nz = self.dimensions()
+        n = nx * ny * nz
+        out = np.empty((12, nx, ny, nz), dtype=np.float32)
+        for a in range(12):
+            out[a] = np.ctypeslib.as_array(ptrs[a], shape=(n,)).reshape(nx, ny, nz)
+        return out
+
+    def e_coefficients(self):
+        c = self.coefficients()
+        return c[0:3], c[3:6]
+
+    def h_coefficients(self):
+        c = self.coefficients()
+        return c[6:9], c[9:12]
+
+    def nyquist_timesteps(self, freq: float) -> int:
+        """src/fdtd/operator.rs:266-270."""
+        return int(np.ceil((1.0 / freq) / self.timestep()))
+
+
+# ---------------------------------------------------------------------------
+# excitation
+# ---------------------------------------------------------------------------
+
+
+class ExcitationType(enum.IntEnum):
+    Gaussian = 0
+    Sinusoidal = 1
+    GaussianModulated = 2
+    Dirac = 3
+    Step = 4
+
+
+@dataclass
+class Excitation:
+    """Excitation (src/fdtd/excitation.rs:46-226).
+
+    params: Gaussian (t0, tau); Sinusoidal (frequency,); GaussianModulated
+    (frequency, t0, tau); Dirac / Step ().
+    """
+
+    excitation_type: ExcitationType
+    params: Tuple[float, ...]
+    direction: int
+    position: Tuple[int, int, int]
+    amplitude: float = 1.0
+    soft_source: bool = True
+
+    @classmethod
+    def _from_c(cls, c: N.ExcitationC):
+        kind = ExcitationType(c.kind)
+        npar = {0: 2, 1: 1, 2: 3, 3: 0, 4: 0}[int(kind)]
+        return cls(kind, tuple(c.params[:npar]), int(c.direction), tuple(int(v) for v in c.position),
+                   float(c.amplitude), bool(c.soft_source))
+
+    @staticmethod
+    def _pos(position):
+        p = (N.c_u64 * 3)()
+        for a in range(3):
+            p[a] = int(position[a])
+        return p
+
+    @classmethod
+    def gaussian(cls, center_freq, bandwidth, direction, position):
+        c = N.ExcitationC()
+        N.check(N.lib().oems_excitation_gaussian(center_freq, bandwidth, direction,
+                                                 cls._pos(position), ctypes.byref(c)))
+        return cls._from_c(c)
+
+    @classmethod
+    def gaussian_pulse(cls, tau, t0, direction, position, amplitude=1.0):
+        """ExcitationType::Gaussian { t0, tau } built directly."""
+        return cls(ExcitationType.Gaussian, (t0, tau), direction, tuple(position), amplitude, True)
+
+    @classmethod
+    def gaussian_modulated(cls, center_freq, bandwidth, direction, position):
+        c = N.ExcitationC()
+        N.check(N.lib().oems_excitation_gaussian_modulated(center_freq, bandwidth, direction,
+                                                           cls._pos(position), ctypes.byref(c)))
+        return cls._from_c(c)
+
+    @classmethod
+    def sinusoidal(cls, frequency, direction, position):
+        c = N.ExcitationC()
+        N.check(N.lib().oems_excitation_sinusoidal(frequency, direction, cls._pos(position),
+                                                   ctypes.byref(c)))
+        return cls._from_c(c)
+
+    @classmethod
+    def dirac(cls, amplitude, direction, position):
+        c = N.ExcitationC()
+        N.check(N.lib().oems_excitation_dirac(amplitude, direction, cls._pos(position),
+                                              ctypes.byref(c)))
+        return cls._from_c(c)
+
+    def with_amplitude(self, amplitude):
+        self.amplitude = float(amplitude)
+        return self
+
+    def hard_source(self):
+        self.soft_source = False
+        return self
+
+    def to_c(self) -> N.ExcitationC:
+        c = N.ExcitationC()
+        c.kind = int(self.excitation_type)
+        c.direction = int(self.direction)
+        for a in range(3):
+            c.position[a] = int(self.position[a])
+        for a, v in enumerate(self.params):
+            c.params[a] = float(v)
+        c.amplitude = float(self.amplitude)
+        c.soft_source = int(bool(self.soft_source))
+        return c
+
+    def evaluate(self, t: float) -> float:
+        c = self.to_c()
+        return N.lib().oems_excitation_evaluate(ctypes.byref(c), t)
+
+    def sample(self, start_timestep: int, num_timesteps: int, dt: float) -> np.ndarray:
+        out = np.empty(num_timesteps, dtype=np.float32)
+        c = self.to_c()
+        N.check(N.lib().oems_excitation_sample(ctypes.byref(c), start_timestep, num_timesteps, dt,
+                                               N.fptr(out)))
+        return out
+
+    def duration(self) -> float:
+        """src/fdtd/excitation.rs:203-213."""
+        if self.excitation_type in (ExcitationType.Gaussian, ExcitationType.GaussianModulated):
+            t0, tau = self.params[-2], self.params[-1]
+            return t0 + 6.0 * tau
+        return float("inf")
+
+
+@dataclass
+class ScheduledExcitation:
+    """ScheduledExcitation with a Sampled waveform (src/fdtd/batch.rs:71-129)."""
+
+    position: Tuple[int, int, int]
+    direction: int
+    soft_source: bool
+    samples: np.ndarray
+
+    @classmethod
+    def from_excitation(cls, exc: Excitation, start_timestep: int, num_timesteps: int, dt: float):
+        return cls(tuple(exc.position), exc.direction, exc.soft_source,
+                   exc.sample(start_timestep, num_timesteps, dt))
+
+
+# ---------------------------------------------------------------------------
+# batch protocol
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class TerminationConfig:
+    max_timesteps: Optional[int] = None
+    energy_decay_db: Optional[float] = None
+    check_interval: int = 100
+
+
+@dataclass
+class EnergyMonitorConfig:
+    sample_interval: int = 0
+    track_peak: bool = False
+    decay_threshold: Optional[float] = None
+
+
+@dataclass
+class EngineBatch:
+    """EngineBatch (src/fdtd/batch.rs:17-32).  Extensions are attached to the
+    engine (Engine.add_cpml) instead of being passed per batch."""
+
+    num_steps: Optional[int] = None
+    excitations: List[ScheduledExcitation] = field(default_factory=list)
+    termination: TerminationConfig = field(default_factory=TerminationConfig)
+    energy_monitoring: EnergyMonitorConfig = field(default_factory=EnergyMonitorConfig)
+    initial_peak_energy: float = 0.0
+
+
+class TerminationReason(enum.IntEnum):
+    StepsCompleted = 0
+    EnergyDecay = 1
+    ExtensionStop = 2
+
+
+@dataclass
+class EnergySample:
+    timestep: int
+    e_energy: float
+    h_energy: float
+    total_energy: float
+
+
+@dataclass
+class BatchResult:
+    timesteps_executed: int
+    termination_reason: TerminationReason
+    final_decay_db: float
+    energy_samples: List[EnergySample]
+    peak_energy: float
+    elapsed_time: float
+
+
+# ---------------------------------------------------------------------------
+# engine
+# ---------------------------------------------------------------------------
+
+
+class EngineType(enum.Enum):
+    """The engine is CUDA-only; `Cuda` is the single implementation."""
+
+    Cuda = "cuda"
+
+
+class Engine:
+    """CUDA engine (EngineImpl, src/fdtd/engine_impl.rs:24-71) on one GPU."""
+
+    def __init__(self, operator: Operator, engine_type: EngineType = EngineType.Cuda, *,
+                 device: int = -1, compressed: bool = False, autotune: bool = True,
+                 graphs: bool = True):
+        if engine_type is not EngineType.Cuda:
+            raise N.ConfigError("only the CUDA engine exists")
+        flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
+            | (0 if graphs else N.ENGINE_NO_GRAPHS)
+        desc = N.OperatorDesc()
+        N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_engine_create(ctypes.byref(desc), ctypes.byref(h)))
+        self._h = h
+        self.dims = operator.dimensions()
+        self.dt = operator.timestep()
+        self.num_probes = 0
+        layers = operator.boundaries.cpml_layers() if operator.boundaries else (0,) * 6
+        if any(layers):
+            self.add_cpml(CpmlBoundaries(layers=layers))
+
+    @classmethod
+    def from_descriptor(cls, desc: N.OperatorDesc):
+        self = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_engine_create(ctypes.byref(desc), ctypes.byref(h)))
+        self._h = h
+        self.dims = (int(desc.nx), int(desc.ny), int(desc.nz))
+        self.dt = float(desc.dt)
+        self.num_probes = 0
+        return self
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().oems_engine_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def add_cpml(self, cpml: CpmlBoundaries):
+        d = cpml.to_c()
+        N.check(N.lib().oems_engine_add_cpml(self._h, ctypes.byref(d)))
+
+    def add_point_probe(self, component: int, position) -> int:
+        p = (N.c_u64 * 3)(*[int(v) for v in position])
+        pid = N.c_i32()
+        N.check(N.lib().oems_engine_add_point_probe(self._h, component, p, ctypes.byref(pid)))
+        self.num_probes += 1
+        return pid.value
+
+    def probe_traces(self) -> np.ndarray:
+        steps = N.c_u64()
+        N.check(N.lib().oems_engine_read_probe_traces(self._h, None, 0, ctypes.byref(steps)))
+        out = np.zeros((steps.value, self.num_probes), dtype=np.float32)
+        if out.size:
+            N.check(N.lib().oems_engine_read_probe_traces(self._h, N.fptr(out), steps.value, None))
+        return out
+
+    def run_batch(self, batch: EngineBatch) -> BatchResult:
+        num_steps = batch.num_steps
+        if num_steps is None:
+            num_steps = batch.termination.max_timesteps
+        if num_steps is None:
+            raise N.ConfigError("EngineBatch needs num_steps or termination.max_timesteps")
+        keep = []
+        arr = (N.ScheduledExcitationC * max(1, len(batch.excitations)))()
+        for x, e in enumerate(batch.excitations):
+            s = np.ascontiguousarray(e.samples, dtype=np.float32)
+            keep.append(s)
+            for a in range(3):
+                arr[x].position[a] = int(e.position[a])
+            arr[x].direction = int(e.direction)
+            arr[x].soft_source = int(bool(e.soft_source))
+            arr[x].samples = N.fptr(s)
+            arr[x].num_samples = len(s)
+        b = N.BatchC()
+        b.num_steps = int(num_steps)
+        b.excitations = arr
+        b.num_excitations = len(batch.excitations)
+        b.has_energy_decay_db = int(batch.termination.energy_decay_db is not None)
+        b.energy_decay_db = float(batch.termination.energy_decay_db or 0.0)
+        b.check_interval = int(batch.termination.check_interval)
+        b.sample_interval = int(batch.energy_monitoring.sample_interval)
+        b.track_peak = int(bool(batch.energy_monitoring.track_peak))
+        b.initial_peak_energy = float(batch.initial_peak_energy)
+        si = batch.energy_monitoring.sample_interval
+        cap = (int(num_steps) // si + 2) if si > 0 else 1
+        samples = (N.EnergySampleC * cap)()
+        r = N.BatchResultC()
+        r.energy_samples = samples
+        r.energy_capacity = cap
+        N.check(N.lib().oems_engine_run_batch(self._h, ctypes.byref(b), ctypes.byref(r)))
+        es = [EnergySample(int(s.timestep), s.e_energy, s.h_energy, s.total_energy)
+              for s in samples[:min(cap, r.num_energy_samples)]]
+        return BatchResult(int(r.timesteps_executed), TerminationReason(r.termination_reason),
+                           float(r.final_decay_db), es, float(r.peak_energy),
+                           float(r.elapsed_seconds))
+
+    def current_timestep(self) -> int:
+        t = N.c_u64()
+        N.check(N.lib().oems_engine_current_timestep(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    timestep = current_timestep
+
+    def read_fields(self) -> Tuple[np.ndarray, np.ndarray]:
+        e = np.empty((3,) + tuple(self.dims), dtype=np.float32)
+        h = np.empty_like(e)
+        ep = (N.PF * 3)(*[N.fptr(e[c]) for c in range(3)])
+        hp = (N.PF * 3)(*[N.fptr(h[c]) for c in range(3)])
+        N.check(N.lib().oems_engine_read_fields(self._h, ep, hp))
+        return e, h
+
+    def write_fields(self, e: np.ndarray, h: np.ndarray) -> None:
+        e = np.ascontiguousarray(e, dtype=np.float32)
+        h = np.ascontiguousarray(h, dtype=np.float32)
+        if e.shape != (3,) + tuple(self.dims) or h.shape != e.shape:
+            raise N.InvalidArgumentError("fields must have shape (3, nx, ny, nz)")
+        ep = (N.PF * 3)(*[N.fptr(e[c]) for c in range(3)])
+        hp = (N.PF * 3)(*[N.fptr(h[c]) for c in range(3)])
+        N.check(N.lib().oems_engine_write_fields(self._h, ep, hp))
+
+    def reset(self) -> None:
+        N.check(N.lib().oems_engine_reset(self._h))
+
+    def energy(self) -> Tuple[float, float]:
+        e, h = N.c_f64(), N.c_f64()
+        N.check(N.lib().oems_engine_energy(self._h, ctypes.byref(e), ctypes.byref(h)))
+        return e.value, h.value
+
+    def set_kernel_profiling(self, enable: bool) -> None:
+        N.check(N.lib().oems_engine_set_kernel_profiling(self._h, int(bool(enable))))
+
+    def kernel_profile(self):
+        """(H seconds, H launches, E seconds, E launches) since profiling was enabled."""
+        hs, hn, es, en = N.c_f64(), N.c_u64(), N.c_f64(), N.c_u64()
+        N.check(N.lib().oems_engine_kernel_profile(self._h, ctypes.byref(hs), ctypes.byref(hn),
+                                                   ctypes.byref(es), ctypes.byref(en)))
+        return hs.value, int(hn.value), es.value, int(en.value)
+
+    def last_batch_stats(self) -> Tuple[int, float]:
+        n, s = N.c_u64(), N.c_f64()
+        N.check(N.lib().oems_engine_last_batch_stats(self._h, ctypes.byref(n), ctypes.byref(s)))
+        return int(n.value), float(s.value)
+
+
+# ---------------------------------------------------------------------------
+# simulation
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class EndCondition:
+    """EndCondition (src/fdtd/simulation.rs:36-49): kind 0 Timesteps(n),
+    1 EnergyDecay(dB), 2 SimulationTime(s)."""
+
+    kind: int = 0
+    value: float = 10000.0
+
+    @classmethod
+    def timesteps(cls, n: int):
+        return cls(0, float(n))
+
+    @classmethod
+    def energy_decay(cls, db: float):
+        return cls(1, float(db))
+
+    @classmethod
+    def simulation_time(cls, t: float):
+        return cls(2, float(t))
+
+
+@dataclass
+class SimulationStats:
+    timesteps: int
+    sim_time: float
+    wall_time: float
+    peak_energy: float
+    final_energy: float
+    speed_mcells_per_sec: float
+
+
+class Simulation:
+    """Simulation (src/fdtd/simulation.rs:69-360) driving the CUDA engine.
+
+    Unlike the reference, whose Simulation cannot carry materials, the
+    operator is exposed as `sim.operator` for set_material / set_pec before
+    the first run.
+    """
+
+    def __init__(self, grid: Grid, boundaries: Optional[BoundaryConditions] = None, *,
+                 device: int = -1, compressed: bool = False):
+        self.grid = grid
+        self.boundaries = boundaries if boundaries is not None else BoundaryConditions()
+        self.operator = Operator(grid, self.boundaries)
+        self.excitations: List[Excitation] = []
+        self.end_condition = EndCondition()
+        self.batch_size: Optional[int] = None
+        self.device = device
+        self.flags = N.ENGINE_COMPRESSED if compressed else 0
+        self._sim = None
+
+    def __del__(self):
+        s = getattr(self, "_sim", None)
+        if s:
+            N.lib().oems_simulation_destroy(s)
+            self._sim = None
+
+    def set_boundaries(self, boundaries: BoundaryConditions):
+        self.boundaries = boundaries
+        self.operator.boundaries = boundaries
+        return self
+
+    def add_excitation(self, exc: Excitation):
+        self.excitations.append(exc)
+        return self
+
+    def set_end_condition(self, cond: EndCondition):
+        self.end_condition = cond
+        return self
+
+    def set_batch_size(self, n: Optional[int]):
+        self.batch_size = n
+        return self
+
+    def timestep(self) -> float:
+        return self.operator.timestep()
+
+    def setup(self):
+        if self._sim is not None:
+            raise N.ConfigError("Simulation already set up")
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_simulation_create(self.operator.handle, self.device, self.flags,
+                                               ctypes.byref(h)))
+        self._sim = h
+        for e in self.excitations:
+            c = e.to_c()
+            N.check(N.lib().oems_simulation_add_excitation(h, ctypes.byref(c)))
+        N.check(N.lib().oems_simulation_set_end_condition(h, self.end_condition.kind,
+                                                          self.end_condition.value))
+        N.check(N.lib().oems_simulation_set_batch_size(h, int(self.batch_size or 0)))
+        layers = self.boundaries.cpml_layers()
+        if any(layers):
+            d = CpmlBoundaries(layers=layers).to_c()
+            N.check(N.lib().oems_simulation_set_cpml(h, ctypes.byref(d)))
+        N.check(N.lib().oems_simulation_setup(h))
+
+    def run(self) -> SimulationStats:
+        if self._sim is None:
+            self.setup()
+        st = N.SimulationStatsC()
+        N.check(N.lib().oems_simulation_run(self._sim, ctypes.byref(st)))
+        return SimulationStats(int(st.timesteps), st.sim_time, st.wall_time, st.peak_energy,
+                               st.final_energy, st.speed_mcells_per_sec)
+
+    def engine_handle(self):
+        return N.lib().oems_simulation_engine(self._sim) if self._sim else None

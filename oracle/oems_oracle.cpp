@@ -1,0 +1,665 @@
+// oems_oracle.cpp -- CPU oracle for the Yee FDTD hot path (TEST INFRASTRUCTURE).
+//
+// Only tests/, the smoke check and bench.py's CPU-baseline leg use this file;
+// the product path never links it.  See oems_oracle.h for the reference
+// files each part restates.  Build: oracle/Makefile (-O2 -ffp-contract=off).
+#include "oems_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// src/constants.rs:8-18
+constexpr double kC0 = 299792458.0;
+constexpr double kEps0 = 8.854187817e-12;
+constexpr double kMu0 = 1.256637062e-6;
+constexpr double kZ0 = 376.730313668;
+constexpr double kPi = 3.14159265358979323846;
+
+// src/geometry/mod.rs:242-255 (min positive spacing; 1.0 if fewer than 2 lines)
+double min_delta(const double* l, int64_t n) {
+  if (n < 2) return 1.0;
+  double m = std::numeric_limits<double>::max();
+  for (int64_t i = 0; i + 1 < n; ++i) {
+    double d = l[i + 1] - l[i];
+    if (d > 0.0 && d < m) m = d;
+  }
+  return m;
+}
+
+// src/fdtd/excitation.rs:150-200
+double eval_excitation(int kind, const double* p, double amplitude, double t) {
+  double v = 0.0;
+  switch (kind) {
+    case ORC_EXC_GAUSSIAN: {
+      double arg = (t - p[0]) / p[1];
+      v = std::exp(-arg * arg);
+      break;
+    }
+    case ORC_EXC_SINUSOIDAL:
+      v = std::sin(2.0 * kPi * p[0] * t);
+      break;
+    case ORC_EXC_GAUSSIAN_MODULATED: {
+      double arg = (t - p[1]) / p[2];
+      double env = std::exp(-arg * arg);
+      double car = std::sin(2.0 * kPi * p[0] * t);
+      v = env * car;
+      break;
+    }
+    case ORC_EXC_DIRAC:
+      v = std::fabs(t) < 1e-15 ? 1.0 : 0.0;
+      break;
+    case ORC_EXC_STEP:
+      v = t >= 0.0 ? 1.0 : 0.0;
+      break;
+    default:
+      v = 0.0;
+  }
+  return amplitude * v;
+}
+
+struct CpmlFace {
+  int layers = 0;
+  // per layer: b, c (standard Roden-Gedney a), 1/kappa for E and H positions
+  std::vector<double> b_e, c_e, ik_e, b_h, c_h, ik_h;
+};
+
+template <typename T>
+struct Sim {
+  int64_t nx, ny, nz, n;
+  double dt;
+  double delta[3];
+  int threads = 1;
+  uint64_t timestep = 0;
+  std::vector<T> E[3], H[3], ca[3], cb[3], da[3], db[3];
+
+  struct Exc {
+    int64_t i, j, k;
+    int dir;
+    bool soft;
+    std::vector<T> samples;
+  };
+  std::vector<Exc> excs;
+
+  struct Probe {
+    int comp;
+    int64_t i, j, k;
+  };
+  std::vector<Probe> probes;
+  std::vector<T> traces;  // [step][probe]
+
+  std::vector<orc_energy_sample> energy;
+
+  // CPML state
+  bool cpml = false;
+  CpmlFace face[6];
+  // per axis, per index: side (-1 none, 0 min, 1 max) and layer
+  std::vector<int> side[3], layer[3];
+  // psi arrays, full size (only slab cells used): H: hx_y hx_z hy_z hy_x hz_x hz_y
+  // E: ex_y ex_z ey_z ey_x ez_x ez_y
+  std::vector<T> psi_h[6], psi_e[6];
+
+  Sim(int64_t nx_, int64_t ny_, int64_t nz_, double dt_, double dx, double dy, double dz)
+      : nx(nx_), ny(ny_), nz(nz_), n(nx_ * ny_ * nz_), dt(dt_) {
+    delta[0] = dx;
+    delta[1] = dy;
+    delta[2] = dz;
+    for (int c = 0; c < 3; ++c) {
+      E[c].assign(n, T(0));
+      H[c].assign(n, T(0));
+    }
+    init_vacuum();
+  }
+
+  int64_t idx(int64_t i, int64_t j, int64_t k) const { return (i * ny + j) * nz + k; }
+
+  // src/fdtd/operator.rs:92-141
+  void init_vacuum() {
+    for (int c = 0; c < 3; ++c) {
+      ca[c].assign(n, T(1));
+      da[c].assign(n, T(1));
+    }
+    T cbv[3] = {T(dt / (kEps0 * delta[0])), T(dt / (kEps0 * delta[1])), T(dt / (kEps0 * delta[2]))};
+    T dbv[3] = {T(-(dt / (kMu0 * delta[0]))), T(-(dt / (kMu0 * delta[1]))),
+                T(-(dt / (kMu0 * delta[2])))};
+    for (int c = 0; c < 3; ++c) {
+      cb[c].assign(n, cbv[c]);
+      db[c].assign(n, dbv[c]);
+    }
+  }
+
+  // src/fdtd/operator.rs:187-244
+  void set_material(double eps_r, double mu_r, double sigma_e, double sigma_m, const int64_t* r) {
+    double eps = eps_r * kEps0;
+    double loss_e = sigma_e * dt / (2.0 * eps);
+    T ca_mat = T((1.0 - loss_e) / (1.0 + loss_e));
+    double cb_factor = (dt / eps) / (1.0 + loss_e);
+    T cbv[3] = {T(cb_factor / delta[0]), T(cb_factor / delta[1]), T(cb_factor / delta[2])};
+    double mu = mu_r * kMu0;
+    double loss_m = sigma_m * dt / (2.0 * mu);
+    T da_mat = T((1.0 - loss_m) / (1.0 + loss_m));
+    double db_factor = -(dt / mu) / (1.0 + loss_m);
+    T dbv[3] = {T(db_factor / delta[0]), T(db_factor / delta[1]), T(db_factor / delta[2])};
+    for (int64_t i = r[0]; i < r[1]; ++i)
+      for (int64_t j = r[2]; j < r[3]; ++j)
+        for (int64_t k = r[4]; k < r[5]; ++k) {
+          int64_t q = idx(i, j, k);
+          for (int c = 0; c < 3; ++c) {
+            ca[c][q] = ca_mat;
+            cb[c][q] = cbv[c];
+            da[c][q] = da_mat;
+            db[c][q] = dbv[c];
+          }
+        }
+  }
+
+  // src/fdtd/operator.rs:249-263
+  void set_pec(const int64_t* r) {
+    for (int64_t i = r[0]; i < r[1]; ++i)
+      for (int64_t j = r[2]; j < r[3]; ++j)
+        for (int64_t k = r[4]; k < r[5]; ++k) {
+          int64_t q = idx(i, j, k);
+          for (int c = 0; c < 3; ++c) {
+            ca[c][q] = T(0);
+            cb[c][q] = T(0);
+          }
+        }
+  }
+
+  // Profile: src/extensions/cpml.rs:68-72 (sigma_max from the largest layer
+  // count and the smallest cell size) and :98-177 (per-layer b and a).
+  int enable_cpml(const int32_t* layers6, double m, double R, double alpha_max, double kappa_max) {
+    int lmax = 0;
+    for (int f = 0; f < 6; ++f) lmax = std::max(lmax, (int)layers6[f]);
+    if (lmax <= 0) return -1;
+    double dmin = std::min(delta[0], std::min(delta[1], delta[2]));
+    double d = (double)lmax * dmin;
+    double sigma_max = -(m + 1.0) * std::log(R) / (2.0 * kZ0 * d);
+    int64_t ext[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+      side[a].assign(ext[a], -1);
+      layer[a].assign(ext[a], 0);
+      int lmin_ = layers6[2 * a], lmax_ = layers6[2 * a + 1];
+      bool use_min = lmin_ > 0 && lmin_ < ext[a];
+      bool use_max = lmax_ > 0 && lmax_ < ext[a];
+      if ((use_min ? lmin_ : 0) + (use_max ? lmax_ : 0) > ext[a]) return -2;
+      for (int s = 0; s < 2; ++s) {
+        int L = s == 0 ? lmin_ : lmax_;
+        bool use = s == 0 ? use_min : use_max;
+        CpmlFace& F = face[2 * a + s];
+        F.layers = use ? L : 0;
+        if (!use) continue;
+        double width = (double)L * delta[a];
+        F.b_e.resize(L);
+        F.c_e.resize(L);
+        F.ik_e.resize(L);
+        F.b_h.resize(L);
+        F.c_h.resize(L);
+        F.ik_h.resize(L);
+        for (int l = 0; l < L; ++l) {
+          double depth_e = s == 0 ? (double)(L - l) * delta[a] : (double)(l + 1) * delta[a];
+          double depth_h = depth_e - 0.5 * delta[a];
+          for (int w = 0; w < 2; ++w) {
+            double depth = w == 0 ? depth_e : depth_h;
+            double rho = std::min(1.0, std::max(0.0, depth / width));
+            double sigma = sigma_max * std::pow(rho, m);
+            double alpha = alpha_max * (1.0 - rho);
+            double kappa = 1.0 + (kappa_max - 1.0) * std::pow(rho, m);
+            double b = std::exp(-(sigma / kappa / kEps0 + alpha / kEps0) * dt);
+            double sn = sigma / (kEps0 * kappa);
+            double an = alpha / kEps0;
+            double den = sn + an;
+            double a_ref = std::fabs(den) > 1e-20 ? sn / den * (1.0 - b) : 0.0;
+            // Standard Roden-Gedney a = sigma/(sigma*kappa + kappa^2*alpha)*(b-1),
+            // which equals -a_ref/kappa.
+            double c = -a_ref / kappa;
+            double ik = 1.0 / kappa;
+            // round to the sim precision so the profile matches the kernels
+            if (w == 0) {
+              F.b_e[l] = (double)T(b);
+              F.c_e[l] = (double)T(c);
+              F.ik_e[l] = (double)T(ik);
+            } else {
+              F.b_h[l] = (double)T(b);
+              F.c_h[l] = (double)T(c);
+              F.ik_h[l] = (double)T(ik);
+            }
+          }
+        }
+        for (int l = 0; l < L; ++l) {
+          int64_t g = s == 0 ? l : ext[a] - L + l;
+          side[a][g] = s;
+          layer[a][g] = l;
+        }
+      }
+    }
+    for (int q = 0; q < 6; ++q) {
+      psi_h[q].assign(n, T(0));
+      psi_e[q].assign(n, T(0));
+    }
+    cpml = true;
+    return 0;
+  }
+
+  // psi <- b*psi + c*d ; d <- d*ik + psi   (each product and sum rounded)
+  static inline T stretch(T d, T& psi, T b, T c, T ik) {
+    T t1 = b * psi;
+    T t2 = c * d;
+    psi = t1 + t2;
+    T t3 = d * ik;
+    return t3 + psi;
+  }
+
+  inline void cpml_h(int axis, int64_t g, int64_t q, T& d, int which) {
+    int s = side[axis][g];
+    if (s < 0) return;
+    const CpmlFace& F = face[2 * axis + s];
+    int l = layer[axis][g];
+    d = stretch(d, psi_h[which][q], T(F.b_h[l]), T(F.c_h[l]), T(F.ik_h[l]));
+  }
+  inline void cpml_e(int axis, int64_t g, int64_t q, T& d, int which) {
+    int s = side[axis][g];
+    if (s < 0) return;
+    const CpmlFace& F = face[2 * axis + s];
+    int l = layer[axis][g];
+    d = stretch(d, psi_e[which][q], T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
+  }
+
+  // src/fdtd/basic_engine.rs:191-254
+  void update_h() {
+    const T* ex = E[0].data();
+    const T* ey = E[1].data();
+    const T* ez = E[2].data();
+#pragma omp parallel for num_threads(threads) if (threads > 1) schedule(static)
+    for (int64_t i = 0; i < nx; ++i)
+      for (int64_t j = 0; j < ny; ++j)
+        for (int64_t k = 0; k < nz; ++k) {
+          int64_t q = idx(i, j, k);
+          T dez_dy = j + 1 < ny ? ez[q + nz] - ez[q] : T(0);
+          T dey_dz = k + 1 < nz ? ey[q + 1] - ey[q] : T(0);
+          T dex_dz = k + 1 < nz ? ex[q + 1] - ex[q] : T(0);
+          T dez_dx = i + 1 < nx ? ez[q + ny * nz] - ez[q] : T(0);
+          T dey_dx = i + 1 < nx ? ey[q + ny * nz] - ey[q] : T(0);
+          T dex_dy = j + 1 < ny ? ex[q + nz] - ex[q] : T(0);
+          if (cpml) {
+            cpml_h(1, j, q, dez_dy, 0);  // Hx, y-slab
+            cpml_h(2, k, q, dey_dz, 1);  // Hx, z-slab
+            cpml_h(2, k, q, dex_dz, 2);  // Hy, z-slab
+            cpml_h(0, i, q, dez_dx, 3);  // Hy, x-slab
+            cpml_h(0, i, q, dey_dx, 4);  // Hz, x-slab
+            cpml_h(1, j, q, dex_dy, 5);  // Hz, y-slab
+          }
+          T curl_x = dez_dy - dey_dz;
+          T curl_y = dex_dz - dez_dx;
+          T curl_z = dey_dx - dex_dy;
+          T a0 = da[0][q] * H[0][q];
+          T b0 = db[0][q] * curl_x;
+          H[0][q] = a0 + b0;
+          T a1 = da[1][q] * H[1][q];
+          T b1 = db[1][q] * curl_y;
+          H[1][q] = a1 + b1;
+          T a2 = da[2][q] * H[2][q];
+          T b2 = db[2][q] * curl_z;
+          H[2][q] = a2 + b2;
+        }
+  }
+
+  // src/fdtd/basic_engine.rs:262-306 (only i, j, k >= 1 are updated)
+  void update_e() {
+    const T* hx = H[0].data();
+    const T* hy = H[1].data();
+    const T* hz = H[2].data();
+#pragma omp parallel for num_threads(threads) if (threads > 1) schedule(static)
+    for (int64_t i = 1; i < nx; ++i)
+      for (int64_t j = 1; j < ny; ++j)
+        for (int64_t k = 1; k < nz; ++k) {
+          int64_t q = idx(i, j, k);
+          T dhz_dy = hz[q] - hz[q - nz];
+          T dhy_dz = hy[q] - hy[q - 1];
+          T dhx_dz = hx[q] - hx[q - 1];
+          T dhz_dx = hz[q] - hz[q - ny * nz];
+          T dhy_dx = hy[q] - hy[q - ny * nz];
+          T dhx_dy = hx[q] - hx[q - nz];
+          if (cpml) {
+            cpml_e(1, j, q, dhz_dy, 0);  // Ex, y-slab
+            cpml_e(2, k, q, dhy_dz, 1);  // Ex, z-slab
+            cpml_e(2, k, q, dhx_dz, 2);  // Ey, z-slab
+            cpml_e(0, i, q, dhz_dx, 3);  // Ey, x-slab
+            cpml_e(0, i, q, dhy_dx, 4);  // Ez, x-slab
+            cpml_e(1, j, q, dhx_dy, 5);  // Ez, y-slab
+          }
+          T curl_x = dhz_dy - dhy_dz;
+          T curl_y = dhx_dz - dhz_dx;
+          T curl_z = dhy_dx - dhx_dy;
+          T a0 = ca[0][q] * E[0][q];
+          T b0 = cb[0][q] * curl_x;
+          E[0][q] = a0 + b0;
+          T a1 = ca[1][q] * E[1][q];
+          T b1 = cb[1][q] * curl_y;
+          E[1][q] = a1 + b1;
+          T a2 = ca[2][q] * E[2][q];
+          T b2 = cb[2][q] * curl_z;
+          E[2][q] = a2 + b2;
+        }
+  }
+
+  // src/fdtd/basic_engine.rs:313-395 (samples beyond the vector are skipped)
+  void apply_excitations(uint64_t step) {
+    for (const Exc& x : excs) {
+      if (step >= x.samples.size()) continue;
+      T v = x.samples[step];
+      int64_t q = idx(x.i, x.j, x.k);
+      if (x.soft)
+        E[x.dir][q] += v;
+      else
+        E[x.dir][q] = v;
+    }
+  }
+
+  void record_probes() {
+    for (const Probe& p : probes) {
+      int64_t q = idx(p.i, p.j, p.k);
+      traces.push_back(p.comp < 3 ? E[p.comp][q] : H[p.comp - 3][q]);
+    }
+  }
+
+  // src/arrays/field.rs:219-221, :314-316
+  static double sumsq(const std::vector<T>& a) {
+    double s = 0.0;
+    for (T v : a) s += (double)v * (double)v;
+    return s;
+  }
+  void energies(double* e, double* h) const {
+    *e = sumsq(E[0]) + sumsq(E[1]) + sumsq(E[2]);
+    *h = sumsq(H[0]) + sumsq(H[1]) + sumsq(H[2]);
+  }
+
+  // src/fdtd/basic_engine.rs:56-163
+  int run_batch(uint64_t num_steps, uint64_t sample_interval, bool track_peak,
+                uint64_t check_interval, bool has_decay, double decay_db, double peak0,
+                orc_batch_result* res) {
+    double peak = peak0;
+    uint64_t executed = 0;
+    int reason = 0;
+    double final_db = 0.0;
+    energy.clear();
+    traces.clear();
+    for (uint64_t step = 0; step < num_steps; ++step) {
+      uint64_t cur = timestep;
+      update_h();
+      update_e();
+      apply_excitations(step);
+      record_probes();
+      timestep += 1;
+      executed += 1;
+      if (sample_interval > 0 && cur % sample_interval == 0) {
+        orc_energy_sample smp;
+        smp.timestep = cur;
+        energies(&smp.e_energy, &smp.h_energy);
+        smp.total_energy = smp.e_energy + smp.h_energy;
+        if (track_peak) peak = std::max(peak, smp.total_energy);
+        energy.push_back(smp);
+      }
+      if (check_interval > 0 && cur > 0 && cur % check_interval == 0) {
+        if (has_decay) {
+          double e, h;
+          energies(&e, &h);
+          double curE = e + h;
+          if (peak > 0.0 && curE > 0.0) {
+            double d = 10.0 * std::log10(curE / peak);
+            if (d < -std::fabs(decay_db)) {
+              reason = 1;
+              final_db = d;
+              break;
+            }
+          }
+        }
+      }
+    }
+    res->timesteps_executed = executed;
+    res->termination_reason = reason;
+    res->pad_ = 0;
+    res->final_decay_db = final_db;
+    res->num_energy_samples = energy.size();
+    res->peak_energy = peak;
+    return 0;
+  }
+};
+
+struct Any {
+  int precision;
+  Sim<float>* f = nullptr;
+  Sim<double>* d = nullptr;
+};
+
+}  // namespace
+
+struct orc_sim {
+  Any a;
+};
+
+#define DISPATCH(s, ...)             \
+  do {                               \
+    if ((s)->a.precision == 32) {    \
+      auto* S = (s)->a.f;            \
+      __VA_ARGS__;                   \
+    } else {                         \
+      auto* S = (s)->a.d;            \
+      __VA_ARGS__;                   \
+    }                                \
+  } while (0)
+
+extern "C" {
+
+void orc_grid_timestep(const double* xl, int64_t nxl, const double* yl, int64_t nyl,
+                       const double* zl, int64_t nzl, double unit, double* dt_out,
+                       double* delta_out3) {
+  double dx = min_delta(xl, nxl) * unit;
+  double dy = min_delta(yl, nyl) * unit;
+  double dz = min_delta(zl, nzl) * unit;
+  double inv_sum = 1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz);
+  double dt_max = 1.0 / (kC0 * std::sqrt(inv_sum));
+  *dt_out = 0.99 * dt_max;
+  delta_out3[0] = dx;
+  delta_out3[1] = dy;
+  delta_out3[2] = dz;
+}
+
+double orc_excitation_eval(int32_t kind, const double* params, double amplitude, double t) {
+  return eval_excitation(kind, params, amplitude, t);
+}
+
+orc_sim* orc_new(int32_t precision, int64_t nx, int64_t ny, int64_t nz, double dt, double dx,
+                 double dy, double dz) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return nullptr;
+  orc_sim* s = new orc_sim;
+  s->a.precision = precision == 64 ? 64 : 32;
+  if (s->a.precision == 32)
+    s->a.f = new Sim<float>(nx, ny, nz, dt, dx, dy, dz);
+  else
+    s->a.d = new Sim<double>(nx, ny, nz, dt, dx, dy, dz);
+  return s;
+}
+
+void orc_free(orc_sim* s) {
+  if (!s) return;
+  delete s->a.f;
+  delete s->a.d;
+  delete s;
+}
+
+void orc_set_threads(orc_sim* s, int32_t threads) { DISPATCH(s, S->threads = threads < 1 ? 1 : threads); }
+
+void orc_set_material(orc_sim* s, double eps_r, double mu_r, double sigma_e, double sigma_m,
+                      const int64_t* r) {
+  DISPATCH(s, S->set_material(eps_r, mu_r, sigma_e, sigma_m, r));
+}
+
+void orc_set_pec(orc_sim* s, const int64_t* r) { DISPATCH(s, S->set_pec(r)); }
+
+void orc_get_coefficients(const orc_sim* s, void* out12) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    T* o = (T*)out12;
+    const std::vector<T>* arr[12] = {&S->ca[0], &S->ca[1], &S->ca[2], &S->cb[0], &S->cb[1], &S->cb[2],
+                                     &S->da[0], &S->da[1], &S->da[2], &S->db[0], &S->db[1], &S->db[2]};
+    for (int a = 0; a < 12; ++a) std::memcpy(o + a * S->n, arr[a]->data(), sizeof(T) * S->n);
+  });
+}
+
+void orc_set_coefficients(orc_sim* s, const void* in12) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    const T* p = (const T*)in12;
+    std::vector<T>* arr[12] = {&S->ca[0], &S->ca[1], &S->ca[2], &S->cb[0], &S->cb[1], &S->cb[2],
+                               &S->da[0], &S->da[1], &S->da[2], &S->db[0], &S->db[1], &S->db[2]};
+    for (int a = 0; a < 12; ++a) std::memcpy(arr[a]->data(), p + a * S->n, sizeof(T) * S->n);
+  });
+}
+
+void orc_get_fields(const orc_sim* s, void* out6) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    T* o = (T*)out6;
+    for (int c = 0; c < 3; ++c) {
+      std::memcpy(o + c * S->n, S->E[c].data(), sizeof(T) * S->n);
+      std::memcpy(o + (3 + c) * S->n, S->H[c].data(), sizeof(T) * S->n);
+    }
+  });
+}
+
+void orc_set_fields(orc_sim* s, const void* in6) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    const T* p = (const T*)in6;
+    for (int c = 0; c < 3; ++c) {
+      std::memcpy(S->E[c].data(), p + c * S->n, sizeof(T) * S->n);
+      std::memcpy(S->H[c].data(), p + (3 + c) * S->n, sizeof(T) * S->n);
+    }
+  });
+}
+
+void orc_reset(orc_sim* s) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    for (int c = 0; c < 3; ++c) {
+      std::fill(S->E[c].begin(), S->E[c].end(), T(0));
+      std::fill(S->H[c].begin(), S->H[c].end(), T(0));
+    }
+    for (int q = 0; q < 6; ++q) {
+      std::fill(S->psi_h[q].begin(), S->psi_h[q].end(), T(0));
+      std::fill(S->psi_e[q].begin(), S->psi_e[q].end(), T(0));
+    }
+    S->timestep = 0;
+  });
+}
+
+uint64_t orc_timestep(const orc_sim* s) {
+  uint64_t t = 0;
+  DISPATCH(s, t = S->timestep);
+  return t;
+}
+
+void orc_clear_excitations(orc_sim* s) { DISPATCH(s, S->excs.clear()); }
+
+void orc_add_excitation_sampled(orc_sim* s, const int64_t* pos3, int32_t dir, int32_t soft,
+                                const void* samples, int64_t n) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    typename std::remove_reference_t<decltype(*S)>::Exc x;
+    x.i = pos3[0];
+    x.j = pos3[1];
+    x.k = pos3[2];
+    x.dir = dir;
+    x.soft = soft != 0;
+    x.samples.assign((const T*)samples, (const T*)samples + n);
+    S->excs.push_back(x);
+  });
+}
+
+// src/fdtd/batch.rs:110-129: t = (start + step) * dt, value = evaluate(t)
+// rounded to the sim precision.
+void orc_add_excitation_analytic(orc_sim* s, const int64_t* pos3, int32_t dir, int32_t soft,
+                                 int32_t kind, const double* params, double amplitude,
+                                 uint64_t start_timestep, int64_t n) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    typename std::remove_reference_t<decltype(*S)>::Exc x;
+    x.i = pos3[0];
+    x.j = pos3[1];
+    x.k = pos3[2];
+    x.dir = dir;
+    x.soft = soft != 0;
+    x.samples.resize(n);
+    for (int64_t st = 0; st < n; ++st) {
+      double t = (double)(start_timestep + (uint64_t)st) * S->dt;
+      x.samples[st] = T(eval_excitation(kind, params, amplitude, t));
+    }
+    S->excs.push_back(x);
+  });
+}
+
+void orc_add_point_probe(orc_sim* s, int32_t comp, const int64_t* pos3) {
+  DISPATCH(s, S->probes.push_back({comp, pos3[0], pos3[1], pos3[2]}));
+}
+
+void orc_get_probe_traces(const orc_sim* s, void* out, int64_t max_steps) {
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    int64_t cnt = std::min<int64_t>((int64_t)S->traces.size(), max_steps * (int64_t)S->probes.size());
+    std::memcpy(out, S->traces.data(), sizeof(T) * cnt);
+  });
+}
+
+int32_t orc_enable_cpml(orc_sim* s, const int32_t* layers6, double m, double R, double alpha_max,
+                        double kappa_max) {
+  int rc = 0;
+  DISPATCH(s, rc = S->enable_cpml(layers6, m, R, alpha_max, kappa_max));
+  return rc;
+}
+
+int32_t orc_cpml_profile(const orc_sim* s, int32_t f, double* out) {
+  int L = 0;
+  DISPATCH(s, {
+    if (!S->cpml || f < 0 || f >= 6) return 0;
+    const CpmlFace& F = S->face[f];
+    L = F.layers;
+    for (int l = 0; l < L; ++l) {
+      out[0 * L + l] = F.b_e[l];
+      out[1 * L + l] = F.c_e[l];
+      out[2 * L + l] = F.ik_e[l];
+      out[3 * L + l] = F.b_h[l];
+      out[4 * L + l] = F.c_h[l];
+      out[5 * L + l] = F.ik_h[l];
+    }
+  });
+  return L;
+}
+
+int32_t orc_run_batch(orc_sim* s, uint64_t num_steps, uint64_t sample_interval, int32_t track_peak,
+                      uint64_t check_interval, int32_t has_decay, double decay_db,
+                      double initial_peak, orc_batch_result* res) {
+  int rc = 0;
+  DISPATCH(s, rc = S->run_batch(num_steps, sample_interval, track_peak != 0, check_interval,
+                                has_decay != 0, decay_db, initial_peak, res));
+  return rc;
+}
+
+void orc_get_energy_samples(const orc_sim* s, orc_energy_sample* out, uint64_t cap) {
+  DISPATCH(s, {
+    uint64_t cnt = std::min<uint64_t>(cap, S->energy.size());
+    std::memcpy(out, S->energy.data(), sizeof(orc_energy_sample) * cnt);
+  });
+}
+
+void orc_energy(const orc_sim* s, double* e, double* h) { DISPATCH(s, S->energies(e, h)); }
+
+}  // extern "C"

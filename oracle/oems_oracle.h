@@ -1,0 +1,137 @@
+/*
+ * oems_oracle.h -- CPU oracle for the Yee FDTD hot path (TEST INFRASTRUCTURE).
+ *
+ * This library is the checker, never the product: only tests/, the smoke
+ * check in __graft_entry__.py and the CPU-baseline leg of bench.py load it.
+ * It restates, in plain C++, the semantics of the Rust openEMS rewrite's
+ * scalar reference engine and its operator:
+ *
+ *   - src/fdtd/basic_engine.rs:56-163   run_batch step order, energy sampling,
+ *                                       energy-decay termination
+ *   - src/fdtd/basic_engine.rs:191-306  H / E update loops, loop bounds and the
+ *                                       zero-derivative rule at the max faces
+ *   - src/fdtd/basic_engine.rs:313-395  soft / hard excitation injection
+ *   - src/fdtd/operator.rs:82-263       dt and the Ca/Cb/Da/Db coefficients
+ *   - src/fdtd/excitation.rs:67-200     waveforms (evaluated in f64)
+ *   - src/fdtd/batch.rs:110-129         pre-sampling f64 -> f32
+ *   - src/arrays/field.rs:219-221       energy = sum of squares in f64
+ *   - src/extensions/cpml.rs:68-177     CPML profile coefficients (the update
+ *                                       itself is the standard Roden-Gedney
+ *                                       recursive convolution; the reference
+ *                                       leaves its correction disabled)
+ *
+ * Parity status: pinned to the reference's known-answer unit tests (operator
+ * coefficients, excitation waveforms, probe sums, CPML coefficient ranges,
+ * energy arithmetic) and to the physics checks of its scenario tests.  The
+ * reference stores no golden field arrays and cannot be compiled here (no Rust
+ * toolchain), so field-level parity rests on this restatement plus a second,
+ * independent numpy restatement that must agree with it bit for bit.
+ *
+ * Arithmetic: compiled with -ffp-contract=off and no fast-math, so every
+ * `a*b + c*d` rounds each product and the sum separately, like the Rust code.
+ * The oracle exists in two precisions: FP32 (bit-faithful to the reference)
+ * and FP64 (the accuracy oracle: same formulas, coefficients never rounded to
+ * f32).
+ */
+#ifndef OEMS_ORACLE_H
+#define OEMS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_sim orc_sim;
+
+/* Excitation kinds, same order as ExcitationType (src/fdtd/excitation.rs:9-42). */
+enum {
+  ORC_EXC_GAUSSIAN = 0,          /* params: t0, tau            */
+  ORC_EXC_SINUSOIDAL = 1,        /* params: frequency          */
+  ORC_EXC_GAUSSIAN_MODULATED = 2,/* params: frequency, t0, tau */
+  ORC_EXC_DIRAC = 3,
+  ORC_EXC_STEP = 4
+};
+
+typedef struct {
+  uint64_t timestep;
+  double e_energy;
+  double h_energy;
+  double total_energy;
+} orc_energy_sample;
+
+typedef struct {
+  uint64_t timesteps_executed;
+  int32_t termination_reason; /* 0 steps completed, 1 energy decay */
+  int32_t pad_;
+  double final_decay_db;
+  uint64_t num_energy_samples;
+  double peak_energy;
+} orc_batch_result;
+
+/* dt = 0.99 * CFL limit from the minimum line spacing per axis
+ * (src/fdtd/operator.rs:82-89, src/geometry/mod.rs:113-119,242-255). */
+void orc_grid_timestep(const double* xl, int64_t nxl, const double* yl, int64_t nyl,
+                       const double* zl, int64_t nzl, double unit, double* dt_out,
+                       double* delta_out3);
+
+/* Reference evaluate(t) in f64 (src/fdtd/excitation.rs:150-200). */
+double orc_excitation_eval(int32_t kind, const double* params, double amplitude, double t);
+
+/* precision: 32 or 64. Coefficients start as vacuum (operator.rs:92-141). */
+orc_sim* orc_new(int32_t precision, int64_t nx, int64_t ny, int64_t nz, double dt,
+                 double dx, double dy, double dz);
+void orc_free(orc_sim* s);
+void orc_set_threads(orc_sim* s, int32_t threads);
+
+/* Operator::set_material / set_pec (src/fdtd/operator.rs:187-263). region =
+ * i0,i1,j0,j1,k0,k1 (half-open). */
+void orc_set_material(orc_sim* s, double eps_r, double mu_r, double sigma_e, double sigma_m,
+                      const int64_t* region6);
+void orc_set_pec(orc_sim* s, const int64_t* region6);
+/* 12 arrays of n values each in the order ca0 ca1 ca2 cb0 cb1 cb2 da0 da1 da2
+ * db0 db1 db2; element type float (precision 32) or double (64). */
+void orc_get_coefficients(const orc_sim* s, void* out12);
+void orc_set_coefficients(orc_sim* s, const void* in12);
+
+/* Fields: 6 arrays Ex Ey Ez Hx Hy Hz, z fastest, element type per precision. */
+void orc_get_fields(const orc_sim* s, void* out6);
+void orc_set_fields(orc_sim* s, const void* in6);
+void orc_reset(orc_sim* s);
+uint64_t orc_timestep(const orc_sim* s);
+
+/* Sampled excitation: samples[step] is applied after the E update of batch
+ * step `step` (basic_engine.rs:313-395). Samples are f32 for precision 32 and
+ * f64 for precision 64. */
+void orc_clear_excitations(orc_sim* s);
+void orc_add_excitation_sampled(orc_sim* s, const int64_t* pos3, int32_t dir, int32_t soft,
+                                const void* samples, int64_t n);
+/* Analytic excitation sampled by the oracle itself in its own precision. */
+void orc_add_excitation_analytic(orc_sim* s, const int64_t* pos3, int32_t dir, int32_t soft,
+                                 int32_t kind, const double* params, double amplitude,
+                                 uint64_t start_timestep, int64_t n);
+
+/* Point probes: comp 0..5 = Ex Ey Ez Hx Hy Hz. One value per executed step,
+ * taken after the excitation. Traces are float / double per precision. */
+void orc_add_point_probe(orc_sim* s, int32_t comp, const int64_t* pos3);
+void orc_get_probe_traces(const orc_sim* s, void* out, int64_t max_steps);
+
+/* CPML on the faces with layers[f] > 0 (f = xmin,xmax,ymin,ymax,zmin,zmax).
+ * Profile: src/extensions/cpml.rs:68-177; update: Roden-Gedney. */
+int32_t orc_enable_cpml(orc_sim* s, const int32_t* layers6, double grading_order,
+                        double reflection_coeff, double alpha_max, double kappa_max);
+/* Per-face profile arrays for tests: out has 6 rows (b_e, c_e, ik_e, b_h, c_h,
+ * ik_h) of `layers` doubles for face f (values after rounding to the sim's
+ * precision). Returns the layer count, 0 if the face is disabled. */
+int32_t orc_cpml_profile(const orc_sim* s, int32_t face, double* out);
+
+int32_t orc_run_batch(orc_sim* s, uint64_t num_steps, uint64_t sample_interval,
+                      int32_t track_peak, uint64_t check_interval, int32_t has_decay,
+                      double decay_db, double initial_peak, orc_batch_result* res);
+void orc_get_energy_samples(const orc_sim* s, orc_energy_sample* out, uint64_t cap);
+void orc_energy(const orc_sim* s, double* e_energy, double* h_energy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,214 @@
+"""Scenario descriptions run identically on the CUDA engine and on the oracle.
+
+A Scenario mirrors the reference's SimulationSetup
+(src/fdtd/engine_testing.rs:38-66): grid, material boxes, PEC boxes,
+excitations, steps, energy monitoring, plus CPML and point probes.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+import oracle
+import openems_b200 as oe
+
+
+@dataclass
+class Scenario:
+    name: str
+    dims: Tuple[int, int, int]
+    delta: float
+    materials: List[Tuple] = field(default_factory=list)  # (eps_r, mu_r, sig_e, sig_m, region6)
+    pec: List[Tuple] = field(default_factory=list)        # region6
+    excitations: List[oe.Excitation] = field(default_factory=list)
+    num_steps: int = 100
+    sample_interval: int = 0
+    track_peak: bool = False
+    cpml: Optional[oe.CpmlBoundaries] = None
+    probes: List[Tuple[int, Tuple[int, int, int]]] = field(default_factory=list)
+    batches: Sequence[int] = ()  # split num_steps into these batch sizes (default: one batch)
+
+    def batch_sizes(self):
+        return list(self.batches) if self.batches else [self.num_steps]
+
+
+def make_operator(sc: Scenario) -> oe.Operator:
+    grid = oe.Grid.uniform(*sc.dims, sc.delta)
+    op = oe.Operator(grid, oe.BoundaryConditions.all_pec())
+    for eps_r, mu_r, se, sm, reg in sc.materials:
+        op.set_material(eps_r, mu_r, se, sm, reg)
+    for reg in sc.pec:
+        op.set_pec(reg)
+    return op
+
+
+def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True):
+    """Runs the scenario on the CUDA engine; returns dict of results."""
+    op = make_operator(sc)
+    eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune)
+    if sc.cpml is not None:
+        eng.add_cpml(sc.cpml)
+    for comp, pos in sc.probes:
+        eng.add_point_probe(comp, pos)
+    dt = op.timestep()
+    energy, traces, start = [], [], 0
+    for n in sc.batch_sizes():
+        sched = [oe.ScheduledExcitation.from_excitation(x, start, n, dt) for x in sc.excitations]
+        res = eng.run_batch(oe.EngineBatch(
+            num_steps=n, excitations=sched,
+            termination=oe.TerminationConfig(max_timesteps=n, check_interval=100),
+            energy_monitoring=oe.EnergyMonitorConfig(sample_interval=sc.sample_interval,
+                                                     track_peak=sc.track_peak)))
+        energy += [(s.timestep, s.e_energy, s.h_energy, s.total_energy) for s in res.energy_samples]
+        if sc.probes:
+            traces.append(eng.probe_traces())
+        start += n
+    e, h = eng.read_fields()
+    return {"fields": np.concatenate([e, h]), "energy": energy,
+            "traces": np.concatenate(traces) if traces else None,
+            "timestep": eng.current_timestep(), "engine": eng, "operator": op}
+
+
+def run_oracle(sc: Scenario, precision=32, threads=1):
+    """Runs the scenario on the oracle (BasicEngine semantics)."""
+    lines = [oracle.uniform_lines(n, sc.delta) for n in sc.dims]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*sc.dims, dt, delta, precision=precision, threads=threads)
+    for eps_r, mu_r, se, sm, reg in sc.materials:
+        s.set_material(eps_r, mu_r, se, sm, reg)
+    for reg in sc.pec:
+        s.set_pec(reg)
+    if sc.cpml is not None:
+        c = sc.cpml
+        s.enable_cpml(c.layers, c.grading_order, c.reflection_coeff, c.alpha_max, c.kappa_max)
+    for comp, pos in sc.probes:
+        s.add_point_probe(comp, pos)
+    energy, traces, start = [], [], 0
+    for n in sc.batch_sizes():
+        s.clear_excitations()
+        for x in sc.excitations:
+            s.add_excitation_analytic(x.position, x.direction, x.soft_source,
+                                      int(x.excitation_type), list(x.params), x.amplitude, start, n)
+        r = s.run_batch(n, sample_interval=sc.sample_interval, track_peak=sc.track_peak,
+                        check_interval=100)
+        energy += r["energy_samples"]
+        if sc.probes:
+            traces.append(s.probe_traces())
+        start += n
+    return {"fields": s.fields(), "energy": energy,
+            "traces": np.concatenate(traces) if traces else None,
+            "timestep": s.timestep, "sim": s}
+
+
+def config1_scenario(num_steps=2000) -> Scenario:
+    """64^3, 1 mm, vacuum, PEC faces, soft Gaussian Ez at the centre
+    (tau = 1/(pi*20 GHz), t0 = 4 tau), Ez/Hy probes at 4 fixed cells."""
+    tau = 1.0 / (np.pi * 20e9)
+    exc = oe.Excitation.gaussian_pulse(tau, 4.0 * tau, 2, (32, 32, 32))
+    cells = [(16, 16, 16), (48, 16, 32), (32, 48, 16), (40, 40, 48)]
+    probes = [(2, c) for c in cells] + [(4, c) for c in cells]
+    return Scenario("config1_64_pec", (64, 64, 64), 1e-3, excitations=[exc], num_steps=num_steps,
+                    sample_interval=100, track_peak=True, probes=probes)
+
+
+def reference_scenarios() -> List[Scenario]:
+    """The reference's physics scenarios (src/fdtd/engine_testing.rs:782-1700)
+    with their grids, materials, sources and step counts."""
+    E = oe.Excitation
+    return [
+        Scenario("pec_cavity", (20, 20, 20), 0.5e-3, excitations=[E.dirac(1.0, 2, (10, 10, 10))],
+                 num_steps=200, sample_interval=10, track_peak=True),
+        Scenario("free_propagation", (40, 40, 60), 0.5e-3,
+                 excitations=[E.gaussian(5e9, 0.5, 2, (20, 20, 10))], num_steps=150,
+                 sample_interval=20, track_peak=True),
+        Scenario("dielectric_slab", (30, 30, 60), 0.3e-3,
+                 materials=[(4.0, 1.0, 0.0, 0.0, (0, 30, 0, 30, 25, 35))],
+                 excitations=[E.gaussian(3e9, 0.5, 2, (15, 15, 10))], num_steps=200,
+                 sample_interval=20, track_peak=True),
+        Scenario("resonant_cavity", (20, 20, 40), 0.5e-3,
+                 excitations=[E.sinusoidal(3e9, 2, (10, 10, 20))], num_steps=300,
+                 sample_interval=20, track_peak=True),
+        Scenario("small_grid", (10, 10, 10), 1.0e-3,
+                 excitations=[E.gaussian(2e9, 0.5, 0, (5, 5, 5))], num_steps=100,
+                 sample_interval=10, track_peak=True),
+        Scenario("multi_direction", (25, 25, 25), 0.5e-3,
+                 excitations=[E.gaussian(3e9, 0.5, 0, (12, 12, 12)),
+                              E.gaussian(3e9, 0.5, 1, (13, 13, 13)),
+                              E.gaussian(3e9, 0.5, 2, (14, 14, 14))],
+                 num_steps=150, sample_interval=15, track_peak=True),
+        Scenario("hard_soft_source", (30, 30, 30), 0.5e-3,
+                 excitations=[E.gaussian(3e9, 0.5, 2, (15, 15, 15)),
+                              E.gaussian(3e9, 0.5, 0, (20, 20, 20)).hard_source()],
+                 num_steps=100, sample_interval=10, track_peak=True),
+        Scenario("long_simulation", (15, 15, 15), 1.0e-3,
+                 excitations=[E.dirac(1.0, 1, (7, 7, 7))], num_steps=1000, sample_interval=100,
+                 track_peak=True),
+        Scenario("zero_excitation", (20, 20, 20), 0.5e-3, num_steps=100, sample_interval=10,
+                 track_peak=True),
+        Scenario("batch_consistency", (15, 15, 15), 0.8e-3,
+                 excitations=[E.gaussian(4e9, 0.5, 2, (7, 7, 7))], num_steps=200,
+                 sample_interval=10, track_peak=True, batches=(50, 70, 80)),
+        Scenario("high_permittivity", (30, 30, 60), 0.3e-3,
+                 materials=[(100.0, 1.0, 0.0, 0.0, (0, 30, 0, 30, 25, 35))],
+                 excitations=[E.gaussian(1e9, 0.5, 2, (15, 15, 10))], num_steps=300,
+                 sample_interval=20, track_peak=True),
+        Scenario("extreme_permittivity", (25, 25, 50), 0.4e-3,
+                 materials=[(1000.0, 1.0, 0.0, 0.0, (0, 25, 0, 25, 20, 30))],
+                 excitations=[E.gaussian(0.5e9, 0.5, 2, (12, 12, 8))], num_steps=400,
+                 sample_interval=20, track_peak=True),
+        Scenario("lossy_material", (30, 30, 60), 0.3e-3,
+                 materials=[(4.0, 1.0, 0.1, 0.0, (0, 30, 0, 30, 20, 40))],
+                 excitations=[E.gaussian(3e9, 0.5, 2, (15, 15, 10))], num_steps=300,
+                 sample_interval=20, track_peak=True),
+        Scenario("magnetic_material", (25, 25, 50), 0.4e-3,
+                 materials=[(1.0, 10.0, 0.0, 0.0, (0, 25, 0, 25, 18, 32))],
+                 excitations=[E.gaussian(2e9, 0.5, 2, (12, 12, 8))], num_steps=300,
+                 sample_interval=20, track_peak=True),
+    ]
+
+
+def odd_scenarios() -> List[Scenario]:
+    """Bounds cases: odd sizes, nz not a multiple of 4, one-cell-thick grids,
+    sources on faces, overlapping material / PEC boxes."""
+    E = oe.Excitation
+    tau = 1.0 / (np.pi * 30e9)
+    g = lambda d, p: E.gaussian_pulse(tau, 4 * tau, d, p)  # noqa: E731
+    return [
+        Scenario("odd_5x7x9", (5, 7, 9), 1e-3, excitations=[g(2, (2, 3, 4)), g(0, (4, 6, 8))],
+                 num_steps=60, sample_interval=7, track_peak=True,
+                 probes=[(0, (4, 6, 8)), (5, (0, 0, 0)), (3, (2, 3, 4))]),
+        Scenario("nz1", (6, 5, 1), 1e-3, excitations=[g(2, (3, 2, 0))], num_steps=40),
+        Scenario("nx1", (1, 9, 10), 1e-3, excitations=[g(1, (0, 4, 5))], num_steps=40),
+        Scenario("ny1", (7, 1, 6), 1e-3, excitations=[g(0, (3, 0, 3))], num_steps=40),
+        Scenario("nz_odd_33", (11, 13, 33), 0.7e-3,
+                 materials=[(3.0, 1.5, 0.02, 0.0, (2, 9, 0, 13, 5, 30)),
+                            (6.0, 1.0, 0.0, 2e2, (4, 11, 3, 8, 0, 12))],
+                 pec=[(5, 7, 5, 7, 10, 20)],
+                 excitations=[g(2, (5, 6, 16)), g(1, (10, 12, 32)).hard_source(),
+                              g(0, (0, 0, 0))],
+                 num_steps=120, sample_interval=10, track_peak=True,
+                 probes=[(2, (5, 6, 16)), (1, (10, 12, 32)), (4, (3, 3, 31))]),
+        Scenario("wide_z_130", (6, 9, 130), 1e-3, excitations=[g(2, (3, 4, 65))], num_steps=80,
+                 probes=[(2, (3, 4, 64)), (3, (1, 1, 129))]),
+    ]
+
+
+def cpml_scenarios() -> List[Scenario]:
+    E = oe.Excitation
+    tau = 1.0 / (np.pi * 20e9)
+    return [
+        Scenario("cpml_cube_24", (24, 24, 24), 1e-3,
+                 excitations=[E.gaussian_pulse(tau, 4 * tau, 2, (12, 12, 12))], num_steps=200,
+                 sample_interval=20, track_peak=True, cpml=oe.CpmlBoundaries.uniform(6),
+                 probes=[(2, (12, 12, 12)), (2, (2, 12, 12))]),
+        Scenario("cpml_odd_asym", (19, 23, 29), 0.8e-3,
+                 materials=[(4.0, 1.0, 0.05, 0.0, (5, 14, 6, 17, 8, 21))],
+                 excitations=[E.gaussian_pulse(tau, 4 * tau, 1, (9, 11, 14)),
+                              E.gaussian_pulse(tau, 4 * tau, 0, (10, 12, 15))],
+                 num_steps=150, sample_interval=25, track_peak=True,
+                 cpml=oe.CpmlBoundaries(layers=(4, 5, 0, 6, 7, 3), grading_order=4.0,
+                                        reflection_coeff=1e-5, alpha_max=0.05, kappa_max=3.0),
+                 probes=[(1, (9, 11, 14)), (5, (1, 1, 1))]),
+    ]
