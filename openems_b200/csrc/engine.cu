@@ -952,7 +952,8 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
   // count and the smallest cell size
   const double kEps0 = 8.854187817e-12, kZ0 = 376.730313668;
   const double dmin = std::min(en->delta[0], std::min(en->delta[1], en->delta[2]));
-  const double sigma_max = -(d->grading_order + 1.0) * std::log(d->reflection_coeff) / (2.0 * kZ0 * (double)lmax * dmin);
+  const double width_max = (double)lmax * dmin;
+  const double sigma_max = -(d->grading_order + 1.0) * std::log(d->reflection_coeff) / (2.0 * kZ0 * width_max);
   std::vector<float> prof;
   CpmlArgs& A = en->cpml.args;
   std::memset(&A, 0, sizeof(A));
@@ -989,6 +990,11 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
   OEMS_CUDA(en->cpml.prof.ensure(prof.size()));
   OEMS_CUDA(cudaMemcpy(en->cpml.prof.p, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice));
   A.prof = en->cpml.prof.p;
+  // z faces: psi rows start at a multiple of 4 in k so chunks map to aligned float4s
+  A.zbase[0] = 0;
+  A.zw[0] = (L[4] + 3) / 4 * 4;
+  A.zbase[1] = L[5] > 0 ? (en->nz - L[5]) / 4 * 4 : 0;
+  A.zw[1] = L[5] > 0 ? en->g.nzp - A.zbase[1] : 0;
   // psi arrays: per face 2 for H and 2 for E
   const size_t nzp = en->g.nzp;
   size_t face_sz[6];
@@ -1001,7 +1007,7 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
     }
     if (a == 0) face_sz[f] = (size_t)L[f] * en->ny * nzp;
     else if (a == 1) face_sz[f] = (size_t)en->nx * L[f] * nzp;
-    else face_sz[f] = (size_t)en->nx * en->ny * L[f];
+    else face_sz[f] = (size_t)en->nx * en->ny * A.zw[f - 4];
     face_sz[f] = (face_sz[f] + 3) / 4 * 4;  // keep every array 16-byte aligned
     total += 4 * face_sz[f];
   }

@@ -13,12 +13,16 @@
 // nzp = round_up(nz, 4) floats so every (i, j) row starts 16-byte aligned.
 // Thread mapping: one thread owns one float4 chunk (4 consecutive k) of an
 // x-plane; a warp covers 32 consecutive chunks of the flattened (j, k) plane,
-// so every load is a fully coalesced 128-bit access whatever nz is.  Each CTA
-// marches its tile of chunks through `ichunk` consecutive x-planes, carrying
-// the x-neighbour plane in registers (register-blocked marching along x).
-// z-neighbours come from the adjacent lane by warp shuffle; y-neighbours are
-// the same tile one row over and hit L1.  CTAs loop over (tile, x-chunk) work
-// items, so the grid is sized to the number of resident CTAs.
+// so every access is a fully coalesced 128-bit load or store whatever nz is.
+// Each CTA marches its tile of chunks through `ichunk` consecutive x-planes,
+// carrying the x-neighbour plane in registers (register-blocked marching along
+// x).  z-neighbours come from the adjacent lane by warp shuffle; y-neighbours
+// are the same tile one row over and hit L1.  CTAs loop over (tile, x-chunk)
+// work items, so the grid is sized to the number of resident CTAs.
+//
+// Per plane, a thread first issues every load it needs (fields, neighbours,
+// coefficients and, in CPML slabs, the psi values) and only then shuffles and
+// computes, so all of its memory requests are in flight together.
 //
 // CPML (standard Roden-Gedney recursive convolution with the profile of
 // src/extensions/cpml.rs:68-177) is fused: in a slab cell the difference d
@@ -43,13 +47,19 @@ struct Geom {
 };
 
 // CPML state on the device.  Faces: 0 xmin 1 xmax 2 ymin 3 ymax 4 zmin 5 zmax.
-// psi layout per face: x faces [l][j][k] (k pitch nzp), y faces [i][l][k],
-// z faces [i][j][l].  Slot per axis: x: H {Hy, Hz} E {Ey, Ez};
-// y: H {Hx, Hz} E {Ex, Ez}; z: H {Hx, Hy} E {Ex, Ey}.
+// psi layout per face:
+//   x faces [l][j][k]  (k pitch nzp)
+//   y faces [i][l][k]  (k pitch nzp)
+//   z faces [i][j][w]  w = k - zbase[f], width zw[f] (multiple of 4) so that a
+//                      float4 chunk of k maps to an aligned float4 of psi.
+// Slot per axis: x: H {Hy, Hz} E {Ey, Ez}; y: H {Hx, Hz} E {Ex, Ez};
+// z: H {Hx, Hy} E {Ex, Ey}.
 struct CpmlArgs {
   int L[6];
   int start[6];       // first global index of the slab along its axis
   int prof_off[6];    // offset of face f in prof: 6 rows of L: b_e c_e ik_e b_h c_h ik_h
+  int zbase[2];       // z faces: first k of the psi row (multiple of 4)
+  int zw[2];          // z faces: psi row width (multiple of 4)
   const float* prof;
   float* psi_h[6][2];
   float* psi_e[6][2];
@@ -99,6 +109,7 @@ __device__ __forceinline__ void to_arr(float4 v, float (&a)[4]) {
   a[3] = v.w;
 }
 __device__ __forceinline__ float4 to_f4(const float (&a)[4]) { return make_float4(a[0], a[1], a[2], a[3]); }
+__device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
 // psi <- b*psi + c*d ; return d*ik + psi (each operation rounded).
 __device__ __forceinline__ float cpml_stretch(float d, float& psi, float b, float c, float ik) {
@@ -109,6 +120,7 @@ __device__ __forceinline__ float cpml_stretch(float d, float& psi, float b, floa
 // Slab lookup along one axis: returns face (or -1) and layer.
 __device__ __forceinline__ int cpml_face(const CpmlArgs& cp, int axis, int g, int& l) {
   const int fmin = 2 * axis, fmax = 2 * axis + 1;
+  l = 0;
   if (g < cp.L[fmin]) {
     l = g;
     return fmin;
@@ -120,58 +132,60 @@ __device__ __forceinline__ int cpml_face(const CpmlArgs& cp, int axis, int g, in
   return -1;
 }
 
-// x- or y-slab: the same (face, layer) for all 4 elements of the chunk, psi is
-// a float4 at a 16-byte aligned address.
-__device__ __forceinline__ void cpml_vec(const CpmlArgs& cp, int f, int l, long long pidx, int slot,
-                                         bool is_h, float (&d)[4]) {
-  float* base = is_h ? cp.psi_h[f][slot] : cp.psi_e[f][slot];
+// Profile row (b, c, ik) of face f, layer l, for H (is_h) or E positions.
+__device__ __forceinline__ void cpml_prof(const CpmlArgs& cp, int f, int l, bool is_h, float& b, float& c,
+                                          float& ik) {
   const int L = cp.L[f];
   const float* pr = cp.prof + cp.prof_off[f] + (is_h ? 3 * L : 0);
-  const float b = __ldg(pr + l), c = __ldg(pr + L + l), ik = __ldg(pr + 2 * L + l);
-  float4 p4 = ld4(base + pidx);
+  b = __ldg(pr + l);
+  c = __ldg(pr + L + l);
+  ik = __ldg(pr + 2 * L + l);
+}
+
+// One slab (x or y): psi float4s already loaded; stretch the 4 elements whose
+// `live` bit is set, same layer for all.
+__device__ __forceinline__ void stretch_vec(float (&d)[4], float4& p4, float b, float c, float ik, unsigned live) {
   float p[4];
   to_arr(p4, p);
 #pragma unroll
-  for (int e = 0; e < 4; ++e) d[e] = cpml_stretch(d[e], p[e], b, c, ik);
-  st4(base + pidx, to_f4(p));
+  for (int e = 0; e < 4; ++e) {
+    if (live & (1u << e)) {
+      float pe = p[e];
+      d[e] = cpml_stretch(d[e], pe, b, c, ik);
+      p[e] = pe;
+    }
+  }
+  p4 = to_f4(p);
 }
 
-// z-slab: per element.  zrow = (i*ny + j).
-// Elements with k < kmin (E: k = 0 is never updated) keep their psi untouched.
-__device__ __forceinline__ void cpml_z(const CpmlArgs& cp, int k0, int kmin, int nz, long long zrow,
-                                       int slot, bool is_h, float (&d)[4]) {
+// z slab: per element, layer = k - start of the face.
+__device__ __forceinline__ void stretch_z(const CpmlArgs& cp, int f, int k0, bool is_h, float (&d)[4], float4& p4,
+                                          unsigned live) {
+  float p[4];
+  to_arr(p4, p);
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int k = k0 + e;
-    if (k >= nz || k < kmin) continue;
-    int l;
-    const int f = cpml_face(cp, 2, k, l);
-    if (f < 0) continue;
-    const int L = cp.L[f];
-    float* psi = (is_h ? cp.psi_h[f][slot] : cp.psi_e[f][slot]) + zrow * L + l;
-    const float* pr = cp.prof + cp.prof_off[f] + (is_h ? 3 * L : 0);
-    float p = *psi;
-    d[e] = cpml_stretch(d[e], p, __ldg(pr + l), __ldg(pr + L + l), __ldg(pr + 2 * L + l));
-    *psi = p;
+    const int l = k - cp.start[f];
+    if ((live & (1u << e)) && l >= 0 && l < cp.L[f]) {
+      float b, c, ik;
+      cpml_prof(cp, f, l, is_h, b, c, ik);
+      float pe = p[e];
+      d[e] = cpml_stretch(d[e], pe, b, c, ik);
+      p[e] = pe;
+    }
   }
-}
-
-__device__ __forceinline__ bool z_chunk_in_cpml(const CpmlArgs& cp, int k0, int nz) {
-  return (k0 < cp.L[4]) || (cp.L[5] > 0 && k0 + 3 >= cp.start[5] && k0 < nz);
+  p4 = to_f4(p);
 }
 
 // Per-chunk coefficient fetch: full arrays or compressed table.
 template <int kIdBytes>
 struct Coef {
-  // kIdBytes == 0: full arrays
   __device__ __forceinline__ static void load(const float* const (&arr)[3], const void* ids, const float* tab,
                                               int off, long long q, float (&c)[3][4]) {
     if constexpr (kIdBytes == 0) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        float4 v = ld_cs4(arr[a] + q);
-        to_arr(v, c[a]);
-      }
+      for (int a = 0; a < 3; ++a) to_arr(ld_cs4(arr[a] + q), c[a]);
     } else if constexpr (kIdBytes == 1) {
       const uint32_t w = __ldcs(reinterpret_cast<const unsigned int*>(static_cast<const uint8_t*>(ids) + q));
 #pragma unroll
@@ -205,6 +219,28 @@ __device__ __forceinline__ const float* stage_table(const float* table, int ntab
   }
 }
 
+// Which CPML slabs a chunk touches, and where its psi float4s live.
+struct SlabInfo {
+  int fx, lx, fy, ly;      // x / y face and layer (-1 if none)
+  bool zmin, zmax;         // chunk overlaps the z faces
+  long long px, py;        // psi offsets (float4 aligned)
+  long long pz0, pz1;
+};
+
+__device__ __forceinline__ SlabInfo slab_info(const CpmlArgs& cp, const Geom& g, int i, int j, int k0) {
+  SlabInfo s;
+  s.fx = cpml_face(cp, 0, i, s.lx);
+  s.fy = cpml_face(cp, 1, j, s.ly);
+  s.px = ((long long)s.lx * g.ny + j) * g.nzp + k0;
+  s.py = s.fy >= 0 ? ((long long)i * cp.L[s.fy] + s.ly) * g.nzp + k0 : 0;
+  s.zmin = cp.L[4] > 0 && k0 < cp.L[4];
+  s.zmax = cp.L[5] > 0 && k0 + 3 >= cp.start[5] && k0 < g.nz;
+  const long long zrow = (long long)i * g.ny + j;
+  s.pz0 = zrow * cp.zw[0] + k0 - cp.zbase[0];
+  s.pz1 = zrow * cp.zw[1] + k0 - cp.zbase[1];
+  return s;
+}
+
 // H half-step: H = da*H + db*curl(E).
 template <int kIdBytes, bool kCpml>
 __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
@@ -223,23 +259,48 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
     const int i0 = chunk * g.ichunk;
     const int i1 = min(i0 + g.ichunk, g.nx);
     const bool has_jp = j + 1 < g.ny;
-    const long long row = (long long)j * g.nzp + k0;
-    long long q = (long long)i0 * g.plane + row;
+    const bool need_kn = lane == 31 && k0 + 4 < g.nz;
+    unsigned live = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) live |= (k0 + e < g.nz ? 1u : 0u) << e;
+    long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
     float4 ey4 = ld_nc4(a.ey + q);
     float4 ez4 = ld_nc4(a.ez + q);
     for (int i = i0; i < i1; ++i, q += g.plane) {
       const bool has_ip = i + 1 < g.nx;
+      // ---- every load of this plane first
       const float4 ex4 = ld_nc4(a.ex + q);
       const float4 ey1 = has_ip ? ld_nc4(a.ey + q + g.plane) : ey4;
       const float4 ez1 = has_ip ? ld_nc4(a.ez + q + g.plane) : ez4;
       const float4 exj = has_jp ? ld_nc4(a.ex + q + g.nzp) : ex4;
       const float4 ezj = has_jp ? ld_nc4(a.ez + q + g.nzp) : ez4;
-      // first element of the next chunk (k0 + 4)
+      const float exn_m = need_kn ? __ldg(a.ex + q + 4) : 0.f;
+      const float eyn_m = need_kn ? __ldg(a.ey + q + 4) : 0.f;
+      float co_a[3][4], co_b[3][4], h[3][4];
+      Coef<kIdBytes>::load(a.da, a.ids, tab, 6, q, co_a);
+      Coef<kIdBytes>::load(a.db, a.ids, tab, 9, q, co_b);
+      to_arr(ld4(a.hx + q), h[0]);
+      to_arr(ld4(a.hy + q), h[1]);
+      to_arr(ld4(a.hz + q), h[2]);
+      SlabInfo sl;
+      float4 px0, px1, py0, py1, pzn0, pzn1, pzx0, pzx1;
+      if constexpr (kCpml) {
+        sl = slab_info(a.cp, g, i, j, k0);
+        px0 = sl.fx >= 0 ? ld4(a.cp.psi_h[sl.fx][0] + sl.px) : zero4();
+        px1 = sl.fx >= 0 ? ld4(a.cp.psi_h[sl.fx][1] + sl.px) : zero4();
+        py0 = sl.fy >= 0 ? ld4(a.cp.psi_h[sl.fy][0] + sl.py) : zero4();
+        py1 = sl.fy >= 0 ? ld4(a.cp.psi_h[sl.fy][1] + sl.py) : zero4();
+        pzn0 = sl.zmin ? ld4(a.cp.psi_h[4][0] + sl.pz0) : zero4();
+        pzn1 = sl.zmin ? ld4(a.cp.psi_h[4][1] + sl.pz0) : zero4();
+        pzx0 = sl.zmax ? ld4(a.cp.psi_h[5][0] + sl.pz1) : zero4();
+        pzx1 = sl.zmax ? ld4(a.cp.psi_h[5][1] + sl.pz1) : zero4();
+      }
+      // ---- neighbours along z: first element of the next chunk (k0 + 4)
       float exn = __shfl_down_sync(kFullMask, ex4.x, 1);
       float eyn = __shfl_down_sync(kFullMask, ey4.x, 1);
-      if (lane == 31 && k0 + 4 < g.nz) {
-        exn = __ldg(a.ex + q + 4);
-        eyn = __ldg(a.ey + q + 4);
+      if (need_kn) {
+        exn = exn_m;
+        eyn = eyn_m;
       }
       float ex[4], ey[4], ez[4], eyp[4], ezp[4], exjv[4], ezjv[4];
       to_arr(ex4, ex);
@@ -263,51 +324,63 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
         dex_dy[e] = has_jp ? __fsub_rn(exjv[e], ex[e]) : 0.f;
       }
       if constexpr (kCpml) {
-        int l;
+        float b, cc, ik;
         // y-slab: Hx (dEz/dy, slot 0), Hz (dEx/dy, slot 1)
-        int f = cpml_face(a.cp, 1, j, l);
-        if (f >= 0) {
-          const long long p = ((long long)i * a.cp.L[f] + l) * g.nzp + k0;
-          cpml_vec(a.cp, f, l, p, 0, true, dez_dy);
-          cpml_vec(a.cp, f, l, p, 1, true, dex_dy);
+        if (sl.fy >= 0) {
+          cpml_prof(a.cp, sl.fy, sl.ly, true, b, cc, ik);
+          stretch_vec(dez_dy, py0, b, cc, ik, live);
+          stretch_vec(dex_dy, py1, b, cc, ik, live);
         }
         // z-slab: Hx (dEy/dz, slot 0), Hy (dEx/dz, slot 1)
-        if (z_chunk_in_cpml(a.cp, k0, g.nz)) {
-          const long long zrow = (long long)i * g.ny + j;
-          cpml_z(a.cp, k0, 0, g.nz, zrow, 0, true, dey_dz);
-          cpml_z(a.cp, k0, 0, g.nz, zrow, 1, true, dex_dz);
+        if (sl.zmin) {
+          stretch_z(a.cp, 4, k0, true, dey_dz, pzn0, live);
+          stretch_z(a.cp, 4, k0, true, dex_dz, pzn1, live);
+        }
+        if (sl.zmax) {
+          stretch_z(a.cp, 5, k0, true, dey_dz, pzx0, live);
+          stretch_z(a.cp, 5, k0, true, dex_dz, pzx1, live);
         }
         // x-slab: Hy (dEz/dx, slot 0), Hz (dEy/dx, slot 1)
-        f = cpml_face(a.cp, 0, i, l);
-        if (f >= 0) {
-          const long long p = ((long long)l * g.ny + j) * g.nzp + k0;
-          cpml_vec(a.cp, f, l, p, 0, true, dez_dx);
-          cpml_vec(a.cp, f, l, p, 1, true, dey_dx);
+        if (sl.fx >= 0) {
+          cpml_prof(a.cp, sl.fx, sl.lx, true, b, cc, ik);
+          stretch_vec(dez_dx, px0, b, cc, ik, live);
+          stretch_vec(dey_dx, px1, b, cc, ik, live);
         }
       }
-      float co_a[3][4], co_b[3][4];
-      Coef<kIdBytes>::load(a.da, a.ids, tab, 6, q, co_a);
-      Coef<kIdBytes>::load(a.db, a.ids, tab, 9, q, co_b);
-      float h[3][4];
-      to_arr(ld4(a.hx + q), h[0]);
-      to_arr(ld4(a.hy + q), h[1]);
-      to_arr(ld4(a.hz + q), h[2]);
       float out[3][4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const float curl[3] = {__fsub_rn(dez_dy[e], dey_dz[e]), __fsub_rn(dex_dz[e], dez_dx[e]),
                                __fsub_rn(dey_dx[e], dex_dy[e])};
-        const bool live = k0 + e < g.nz;
+        const bool lv = (live >> e) & 1u;
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const float v = __fadd_rn(__fmul_rn(co_a[cc][e], h[cc][e]), __fmul_rn(co_b[cc][e], curl[cc]));
-          out[cc][e] = live ? v : h[cc][e];
+          out[cc][e] = lv ? v : h[cc][e];
         }
       }
       if (valid) {
         st4(a.hx + q, to_f4(out[0]));
         st4(a.hy + q, to_f4(out[1]));
         st4(a.hz + q, to_f4(out[2]));
+        if constexpr (kCpml) {
+          if (sl.fy >= 0) {
+            st4(a.cp.psi_h[sl.fy][0] + sl.py, py0);
+            st4(a.cp.psi_h[sl.fy][1] + sl.py, py1);
+          }
+          if (sl.zmin) {
+            st4(a.cp.psi_h[4][0] + sl.pz0, pzn0);
+            st4(a.cp.psi_h[4][1] + sl.pz0, pzn1);
+          }
+          if (sl.zmax) {
+            st4(a.cp.psi_h[5][0] + sl.pz1, pzx0);
+            st4(a.cp.psi_h[5][1] + sl.pz1, pzx1);
+          }
+          if (sl.fx >= 0) {
+            st4(a.cp.psi_h[sl.fx][0] + sl.px, px0);
+            st4(a.cp.psi_h[sl.fx][1] + sl.px, px1);
+          }
+        }
       }
       ey4 = ey1;
       ez4 = ez1;
@@ -333,27 +406,61 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
     const int i0 = chunk * g.ichunk;
     const int i1 = min(i0 + g.ichunk, g.nx);
     const bool has_jm = j >= 1;
-    const long long row = (long long)j * g.nzp + k0;
-    long long q = (long long)i0 * g.plane + row;
-    float4 hym4 = make_float4(0.f, 0.f, 0.f, 0.f), hzm4 = hym4;  // H at i-1
+    const bool need_km = lane == 0 && k0 >= 4;
+    // elements that are updated: 1 <= k < nz (i >= 1 and j >= 1 checked per plane)
+    unsigned live_k = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) live_k |= (k0 + e >= 1 && k0 + e < g.nz ? 1u : 0u) << e;
+    long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
+    float4 hym4 = zero4(), hzm4 = zero4();  // H at i-1
     if (i0 > 0) {
       hym4 = ld_nc4(a.hy + q - g.plane);
       hzm4 = ld_nc4(a.hz + q - g.plane);
     }
     for (int i = i0; i < i1; ++i, q += g.plane) {
+      const bool upd = i >= 1 && has_jm;
+      const unsigned live = upd ? live_k : 0u;
+      // ---- every load of this plane first
       const float4 hx4 = ld_nc4(a.hx + q);
       const float4 hy4 = ld_nc4(a.hy + q);
       const float4 hz4 = ld_nc4(a.hz + q);
-      // last element of the previous chunk (k0 - 1)
+      const float4 hxj4 = upd ? ld_nc4(a.hx + q - g.nzp) : zero4();
+      const float4 hzj4 = upd ? ld_nc4(a.hz + q - g.nzp) : zero4();
+      const float hxm_m = need_km ? __ldg(a.hx + q - 1) : 0.f;
+      const float hym_m = need_km ? __ldg(a.hy + q - 1) : 0.f;
+      float co_a[3][4], co_b[3][4], ev[3][4];
+      if (upd) {
+        Coef<kIdBytes>::load(a.ca, a.ids, tab, 0, q, co_a);
+        Coef<kIdBytes>::load(a.cb, a.ids, tab, 3, q, co_b);
+        to_arr(ld4(a.ex + q), ev[0]);
+        to_arr(ld4(a.ey + q), ev[1]);
+        to_arr(ld4(a.ez + q), ev[2]);
+      }
+      SlabInfo sl;
+      float4 px0, px1, py0, py1, pzn0, pzn1, pzx0, pzx1;
+      if constexpr (kCpml) {
+        sl = slab_info(a.cp, g, i, j, k0);
+        if (!upd) {
+          sl.fx = sl.fy = -1;
+          sl.zmin = sl.zmax = false;
+        }
+        px0 = sl.fx >= 0 ? ld4(a.cp.psi_e[sl.fx][0] + sl.px) : zero4();
+        px1 = sl.fx >= 0 ? ld4(a.cp.psi_e[sl.fx][1] + sl.px) : zero4();
+        py0 = sl.fy >= 0 ? ld4(a.cp.psi_e[sl.fy][0] + sl.py) : zero4();
+        py1 = sl.fy >= 0 ? ld4(a.cp.psi_e[sl.fy][1] + sl.py) : zero4();
+        pzn0 = sl.zmin ? ld4(a.cp.psi_e[4][0] + sl.pz0) : zero4();
+        pzn1 = sl.zmin ? ld4(a.cp.psi_e[4][1] + sl.pz0) : zero4();
+        pzx0 = sl.zmax ? ld4(a.cp.psi_e[5][0] + sl.pz1) : zero4();
+        pzx1 = sl.zmax ? ld4(a.cp.psi_e[5][1] + sl.pz1) : zero4();
+      }
+      // ---- neighbours along z: last element of the previous chunk (k0 - 1)
       float hxm = __shfl_up_sync(kFullMask, hx4.w, 1);
       float hym = __shfl_up_sync(kFullMask, hy4.w, 1);
-      if (lane == 0 && k0 >= 4) {
-        hxm = __ldg(a.hx + q - 1);
-        hym = __ldg(a.hy + q - 1);
+      if (need_km) {
+        hxm = hxm_m;
+        hym = hym_m;
       }
-      if (i >= 1 && has_jm) {
-        const float4 hxj4 = ld_nc4(a.hx + q - g.nzp);
-        const float4 hzj4 = ld_nc4(a.hz + q - g.nzp);
+      if (upd) {
         float hx[4], hy[4], hz[4], hxj[4], hzj[4], hyi[4], hzi[4];
         to_arr(hx4, hx);
         to_arr(hy4, hy);
@@ -375,51 +482,63 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
           dhx_dy[e] = __fsub_rn(hx[e], hxj[e]);
         }
         if constexpr (kCpml) {
-          int l;
+          float b, cc, ik;
           // y-slab: Ex (dHz/dy, slot 0), Ez (dHx/dy, slot 1)
-          int f = cpml_face(a.cp, 1, j, l);
-          if (f >= 0) {
-            const long long p = ((long long)i * a.cp.L[f] + l) * g.nzp + k0;
-            cpml_vec(a.cp, f, l, p, 0, false, dhz_dy);
-            cpml_vec(a.cp, f, l, p, 1, false, dhx_dy);
+          if (sl.fy >= 0) {
+            cpml_prof(a.cp, sl.fy, sl.ly, false, b, cc, ik);
+            stretch_vec(dhz_dy, py0, b, cc, ik, live);
+            stretch_vec(dhx_dy, py1, b, cc, ik, live);
           }
-          // z-slab: Ex (dHy/dz, slot 0), Ey (dHx/dz, slot 1); k = 0 is never updated
-          if (z_chunk_in_cpml(a.cp, k0, g.nz)) {
-            const long long zrow = (long long)i * g.ny + j;
-            cpml_z(a.cp, k0, 1, g.nz, zrow, 0, false, dhy_dz);
-            cpml_z(a.cp, k0, 1, g.nz, zrow, 1, false, dhx_dz);
+          // z-slab: Ex (dHy/dz, slot 0), Ey (dHx/dz, slot 1)
+          if (sl.zmin) {
+            stretch_z(a.cp, 4, k0, false, dhy_dz, pzn0, live);
+            stretch_z(a.cp, 4, k0, false, dhx_dz, pzn1, live);
+          }
+          if (sl.zmax) {
+            stretch_z(a.cp, 5, k0, false, dhy_dz, pzx0, live);
+            stretch_z(a.cp, 5, k0, false, dhx_dz, pzx1, live);
           }
           // x-slab: Ey (dHz/dx, slot 0), Ez (dHy/dx, slot 1)
-          f = cpml_face(a.cp, 0, i, l);
-          if (f >= 0) {
-            const long long p = ((long long)l * g.ny + j) * g.nzp + k0;
-            cpml_vec(a.cp, f, l, p, 0, false, dhz_dx);
-            cpml_vec(a.cp, f, l, p, 1, false, dhy_dx);
+          if (sl.fx >= 0) {
+            cpml_prof(a.cp, sl.fx, sl.lx, false, b, cc, ik);
+            stretch_vec(dhz_dx, px0, b, cc, ik, live);
+            stretch_vec(dhy_dx, px1, b, cc, ik, live);
           }
         }
-        float co_a[3][4], co_b[3][4];
-        Coef<kIdBytes>::load(a.ca, a.ids, tab, 0, q, co_a);
-        Coef<kIdBytes>::load(a.cb, a.ids, tab, 3, q, co_b);
-        float ev[3][4];
-        to_arr(ld4(a.ex + q), ev[0]);
-        to_arr(ld4(a.ey + q), ev[1]);
-        to_arr(ld4(a.ez + q), ev[2]);
         float out[3][4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const float curl[3] = {__fsub_rn(dhz_dy[e], dhy_dz[e]), __fsub_rn(dhx_dz[e], dhz_dx[e]),
                                  __fsub_rn(dhy_dx[e], dhx_dy[e])};
-          const bool live = (k0 + e >= 1) && (k0 + e < g.nz);
+          const bool lv = (live >> e) & 1u;
 #pragma unroll
           for (int cc = 0; cc < 3; ++cc) {
             const float v = __fadd_rn(__fmul_rn(co_a[cc][e], ev[cc][e]), __fmul_rn(co_b[cc][e], curl[cc]));
-            out[cc][e] = live ? v : ev[cc][e];
+            out[cc][e] = lv ? v : ev[cc][e];
           }
         }
         if (valid) {
           st4(a.ex + q, to_f4(out[0]));
           st4(a.ey + q, to_f4(out[1]));
           st4(a.ez + q, to_f4(out[2]));
+          if constexpr (kCpml) {
+            if (sl.fy >= 0) {
+              st4(a.cp.psi_e[sl.fy][0] + sl.py, py0);
+              st4(a.cp.psi_e[sl.fy][1] + sl.py, py1);
+            }
+            if (sl.zmin) {
+              st4(a.cp.psi_e[4][0] + sl.pz0, pzn0);
+              st4(a.cp.psi_e[4][1] + sl.pz0, pzn1);
+            }
+            if (sl.zmax) {
+              st4(a.cp.psi_e[5][0] + sl.pz1, pzx0);
+              st4(a.cp.psi_e[5][1] + sl.pz1, pzx1);
+            }
+            if (sl.fx >= 0) {
+              st4(a.cp.psi_e[sl.fx][0] + sl.px, px0);
+              st4(a.cp.psi_e[sl.fx][1] + sl.px, px1);
+            }
+          }
         }
       }
       hym4 = hy4;

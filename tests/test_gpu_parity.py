@@ -130,7 +130,7 @@ def test_energy_decay_termination_matches_oracle():
     sc_cpml = oe.CpmlBoundaries.uniform(6)
     from scenarios import Scenario, make_operator
     sc = Scenario("decay", (24, 24, 24), 1e-3,
-                  excitations=[oe.Excitation.gaussian_pulse(tau, 4 * tau, 2, (12, 12, 12))],
+                  excitations=[oe.Excitation.gaussian_modulated(10e9, 0.3, 2, (12, 12, 12))],
                   num_steps=3000, cpml=sc_cpml)
     op = make_operator(sc)
     eng = oe.Engine(op)
@@ -147,7 +147,7 @@ def test_energy_decay_termination_matches_oracle():
     s = oracle.OracleSim(*sc.dims, dt_o, delta)
     s.enable_cpml((6,) * 6)
     x = sc.excitations[0]
-    s.add_excitation_analytic(x.position, 2, True, 0, list(x.params), 1.0, 0, 3000)
+    s.add_excitation_analytic(x.position, 2, True, int(x.excitation_type), list(x.params), 1.0, 0, 3000)
     r = s.run_batch(3000, sample_interval=10, track_peak=True, check_interval=50, energy_decay_db=30.0)
     assert r["termination_reason"] == 1
     assert res.termination_reason == oe.TerminationReason.EnergyDecay
@@ -216,7 +216,7 @@ def test_energy_decay_end_condition_stops_simulation():
     g = oe.Grid.uniform(24, 24, 24, 1e-3)
     sim = oe.Simulation(g, oe.BoundaryConditions.all_pml(6))
     tau = 1.0 / (np.pi * 20e9)
-    sim.add_excitation(oe.Excitation.gaussian_pulse(tau, 4 * tau, 2, (12, 12, 12)))
+    sim.add_excitation(oe.Excitation.gaussian_modulated(10e9, 0.3, 2, (12, 12, 12)))
     sim.set_end_condition(oe.EndCondition.energy_decay(40.0))
     st = sim.run()
     assert 100 < st.timesteps < 1_000_000
