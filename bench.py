@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--compressed", action="store_true", help="material-id coefficient storage")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernels", choices=("auto", "register", "staged"), default="auto")
     return p.parse_args()
 
 
@@ -127,9 +128,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_engine(oe, wl, compressed=False):
+def build_engine(oe, wl, compressed=False, kernels="auto"):
     op = wl.operator()
-    eng = oe.Engine(op, compressed=compressed)
+    eng = oe.Engine(op, compressed=compressed, kernels=kernels)
     if wl.cpml_layers:
         eng.add_cpml(wl.cpml())
     for comp, pos in wl.probes:
@@ -147,7 +148,7 @@ def batch_for(oe, wl, dt, start, n):
 
 def run_device(oe, wl, args, torch, dist):
     """value: device-resident batches timed with CUDA events (engine stream)."""
-    op, eng = build_engine(oe, wl, args.compressed)
+    op, eng = build_engine(oe, wl, args.compressed, args.kernels)
     dt = op.timestep()
     T = args.timesteps_per_step
     t = 0
@@ -175,16 +176,17 @@ def run_device(oe, wl, args, torch, dist):
     eng.run_batch(batch_for(oe, wl, dt, t, 200))
     hs, hn, es, en = eng.kernel_profile()
     eng.set_kernel_profiling(False)
+    info = eng.launch_info()
     eng.close()
     return {"device_s": dev_s, "wall_s": wall, "launches": launches, "clocks": clk.summary(),
-            "h_avg_s": hs / max(hn, 1), "e_avg_s": es / max(en, 1)}
+            "h_avg_s": hs / max(hn, 1), "e_avg_s": es / max(en, 1), "launch": info}
 
 
 def run_e2e(oe, wl, args, torch):
     """e2e: public API from host buffers, copies inside the timed region."""
     T = args.timesteps_per_step
     # warm-up on a separate engine (context, kernels, autotune cache)
-    op, eng = build_engine(oe, wl, args.compressed)
+    op, eng = build_engine(oe, wl, args.compressed, args.kernels)
     dt = op.timestep()
     for w in range(max(1, args.warmup)):
         eng.run_batch(batch_for(oe, wl, dt, w * T, T))
@@ -194,7 +196,7 @@ def run_e2e(oe, wl, args, torch):
     nprobe = len(wl.probes)
     t0 = time.perf_counter()
     op = wl.operator()                       # host-side operator (12 host arrays)
-    eng = oe.Engine(op, compressed=args.compressed)  # H2D of the coefficients
+    eng = oe.Engine(op, compressed=args.compressed, kernels=args.kernels)  # H2D of the coefficients
     if wl.cpml_layers:
         eng.add_cpml(wl.cpml())
     for comp, pos in wl.probes:
@@ -354,6 +356,7 @@ def main():
         "gpu_launches": d["launches"],
         "clocks": d["clocks"],
         "wall_s_timed": d["wall_s"],
+        "launch_shape": d["launch"],
     }
     if e2e is not None:
         line["e2e"] = {"value": e2e["mcells"], "unit": "MCells/s",

@@ -74,6 +74,9 @@ typedef struct oems_engine oems_engine;
 #define OEMS_ENGINE_NO_AUTOTUNE 0x2u /* keep the default launch shape */
 #define OEMS_ENGINE_NO_GRAPHS 0x4u   /* launch kernels one by one instead of
                                         replaying captured CUDA graphs */
+#define OEMS_ENGINE_REGISTER_KERNELS 0x10u /* only the register-blocked update kernels */
+#define OEMS_ENGINE_STAGED_KERNELS 0x20u   /* only the bulk-async (TMA) staged update
+                                              kernels, where their stages fit */
 
 /* What Operator hands to EngineImpl::new: dimensions, dt, cell sizes and the
  * 12 per-cell coefficient arrays (src/fdtd/operator.rs:21-38, :145-185). */
@@ -203,6 +206,13 @@ OEMS_API oems_status oems_engine_energy(oems_engine* engine, double* e_energy, d
  * engine's stream, and accumulates their device time.  Enabling resets the
  * totals. */
 OEMS_API oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable);
+/* Launch shape chosen for the update kernels (valid after the first batch):
+ * staged = 1 for the bulk-async staged kernels, threads per CTA, x-planes per
+ * work item, rows per tile (staged), pipeline stages (staged), CTAs. */
+OEMS_API oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged,
+                                             int32_t* threads, int32_t* ichunk,
+                                             int32_t* rows_per_tile, int32_t* stages,
+                                             int32_t* grid);
 OEMS_API oems_status oems_engine_kernel_profile(const oems_engine* engine, double* h_seconds,
                                                 uint64_t* h_launches, double* e_seconds,
                                                 uint64_t* e_launches);

@@ -23,6 +23,8 @@ OK, ERR_CONFIG, ERR_IO, ERR_GRID, ERR_MATERIAL, ERR_NUMERICAL, ERR_XML, ERR_CUDA
 ENGINE_COMPRESSED = 0x1
 ENGINE_NO_AUTOTUNE = 0x2
 ENGINE_NO_GRAPHS = 0x4
+ENGINE_REGISTER_KERNELS = 0x10
+ENGINE_STAGED_KERNELS = 0x20
 
 
 class OpenEMSError(Exception):
@@ -148,6 +150,7 @@ SIGNATURES = {
     "oems_abi_version": (c_i32, []),
     "oems_engine_last_batch_stats": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_f64)]),
     "oems_engine_set_kernel_profiling": (c_i32, [P, c_i32]),
+    "oems_engine_launch_info": (c_i32, [P] + [ctypes.POINTER(c_i32)] * 6),
     "oems_engine_kernel_profile": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_u64),
                                            ctypes.POINTER(c_f64), ctypes.POINTER(c_u64)]),
     # include/oems_host.h

@@ -28,6 +28,7 @@
 
 #include "../../include/oems.h"
 #include "yee_kernels.cuh"
+#include "yee_tma.cuh"
 
 namespace oems {
 
@@ -152,11 +153,18 @@ __global__ void k_energy_final(const double* partials, double* out) {
 // engine
 // ---------------------------------------------------------------------------
 
+// Launch shape of the update kernels.  tma = false: register kernels
+// (yee_kernels.cuh) with `block` threads; tma = true: bulk-async staged
+// kernels (yee_tma.cuh) with `nconsumer` + 32 threads and `smem` bytes.
 struct LaunchShape {
   int block = 256;
   int ichunk = 8;
   int grid_h = 0;
   int grid_e = 0;
+  bool tma = false;
+  int nconsumer = 256;
+  TmaGeom tg{};
+  size_t smem = 0;
 };
 
 template <typename T>
@@ -230,6 +238,7 @@ struct oems_engine {
   size_t h_energy_cap = 0;
 
   oems::DevBuf<long long> d_base;
+  oems::DevBuf<int> d_err;  // device error word (bounded waits that gave up)
 
   oems::LaunchShape shape;
   bool tuned = false;
@@ -338,10 +347,77 @@ static size_t table_smem(const oems_engine* en) {
   return en->id_bytes == 1 ? (size_t)en->ntable * 12 * sizeof(float) : 0;
 }
 
+// Stage layout of the bulk-staged kernels for tiles of TJ rows.  Returns the
+// dynamic shared memory in bytes, 0 if fewer than 2 stages fit in `limit`.
+static size_t make_tma_geom(const oems_engine* en, int TJ, int ichunk, int nconsumer, size_t limit, int ns_max,
+                            TmaGeom& t) {
+  const int nzp = en->g.nzp;
+  t = TmaGeom{};
+  t.TJ = TJ;
+  t.ntiles = (en->ny + TJ - 1) / TJ;
+  t.ichunk = ichunk;
+  t.nitems = t.ntiles * ((en->nx + ichunk - 1) / ichunk);
+  t.nconsumer = nconsumer;
+  int off = 0;
+  t.off_f = off;
+  off += 3 * (TJ + 1) * nzp;
+  t.off_u = off;
+  off += 3 * TJ * nzp;
+  t.off_c = off;
+  off += 6 * TJ * nzp;
+  t.off_px = t.off_py = t.off_pz = off;
+  if (en->cpml.on) {
+    const CpmlArgs& cp = en->cpml.args;
+    t.zwmax = std::max(cp.zw[0], cp.zw[1]);
+    t.off_px = off;
+    off += 2 * TJ * nzp;
+    t.off_py = off;
+    off += 2 * TJ * nzp;
+    t.off_pz = off;
+    off += 4 * TJ * t.zwmax;
+    t.prof_floats = 0;
+    for (int f = 0; f < 6; ++f) t.prof_floats += 6 * cp.L[f];
+  }
+  t.stage_floats = (off + 31) / 32 * 32;  // 128-byte aligned stages
+  const size_t fixed = (size_t)((t.prof_floats + 3) / 4 * 4) * sizeof(float) + 64;
+  int ns = 0;
+  for (int s = ns_max; s >= 2; --s)
+    if ((size_t)s * t.stage_floats * sizeof(float) + fixed + 2 * s * sizeof(uint64_t) <= limit) {
+      ns = s;
+      break;
+    }
+  if (ns == 0) return 0;
+  t.NS = ns;
+  return (size_t)ns * t.stage_floats * sizeof(float) + fixed + 2 * ns * sizeof(uint64_t);
+}
+
+static oems_status tma_smem_limit(const oems_engine* en, size_t* limit) {
+  int optin = 0;
+  OEMS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en->device));
+  *limit = (size_t)optin;
+  return OEMS_OK;
+}
+
+static oems_status prepare_tma_kernels(size_t smem) {
+  OEMS_CUDA(cudaFuncSetAttribute((const void*)k_update_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  OEMS_CUDA(cudaFuncSetAttribute((const void*)k_update_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  return OEMS_OK;
+}
+
 // Grid = resident CTAs (occupancy x SMs), capped by the work item count.
 static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   int sms = 0;
   OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, en->device));
+  if (s.tma) {
+    OEMS_TRY(prepare_tma_kernels(s.smem));
+    int occ = 0;
+    OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_update_tma<true>,
+                                                            s.nconsumer + 32, s.smem));
+    s.grid_h = s.grid_e = std::max(1, std::min(s.tg.nitems, std::max(1, occ) * sms));
+    return OEMS_OK;
+  }
   const size_t smem = table_smem(en);
   int occ_h = 0, occ_e = 0;
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -360,12 +436,38 @@ static void apply_shape(oems_engine* en, const LaunchShape& s) {
   en->graph_epoch++;
 }
 
+static TmaArgs tma_args(oems_engine* en, bool is_h) {
+  TmaArgs a{};
+  a.g = en->g;
+  a.t = en->shape.tg;
+  for (int c = 0; c < 3; ++c) {
+    a.f[c] = is_h ? en->E(c) : en->H(c);
+    a.u[c] = is_h ? en->H(c) : en->E(c);
+    a.c[c] = en->C(is_h ? 6 + c : c);
+    a.c[3 + c] = en->C(is_h ? 9 + c : 3 + c);
+  }
+  a.cp = en->cpml.args;
+  a.cpml = en->cpml.on;
+  a.err = en->d_err.p;
+  return a;
+}
+
 static cudaError_t launch_h(oems_engine* en) {
+  if (en->shape.tma) {
+    TmaArgs a = tma_args(en, true);
+    k_update_tma<true><<<en->shape.grid_h, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
+    return cudaGetLastError();
+  }
   HArgs a = h_args(en);
   pick_h(en->id_bytes, en->cpml.on)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
 }
 static cudaError_t launch_e(oems_engine* en) {
+  if (en->shape.tma) {
+    TmaArgs a = tma_args(en, false);
+    k_update_tma<false><<<en->shape.grid_e, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
+    return cudaGetLastError();
+  }
   EArgs a = e_args(en);
   pick_e(en->id_bytes, en->cpml.on)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
@@ -546,8 +648,25 @@ static std::map<TuneKey, LaunchShape>& tune_cache() {
 // the state (fields and psi are saved and restored), keeps the fastest.
 static oems_status autotune(oems_engine* en) {
   en->tuned = true;
-  if (en->flags & OEMS_ENGINE_NO_AUTOTUNE) return OEMS_OK;
-  const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes, en->cpml.on ? 1 : 0};
+  const bool want_reg = !(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0;
+  const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0;
+  if (en->flags & OEMS_ENGINE_NO_AUTOTUNE) {
+    LaunchShape s;
+    if (!want_reg) {
+      size_t limit = 0;
+      OEMS_TRY(tma_smem_limit(en, &limit));
+      s.tma = true;
+      s.nconsumer = 256;
+      s.ichunk = 16;
+      s.smem = make_tma_geom(en, std::max(1, std::min(en->ny, 256 / en->g.nzq)), 16, 256, limit, 4, s.tg);
+      if (s.smem == 0) s = LaunchShape{};
+    }
+    OEMS_TRY(size_grid(en, s));
+    apply_shape(en, s);
+    return OEMS_OK;
+  }
+  const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes,
+                    (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0)};
   auto hit = tune_cache().find(key);
   if (hit != tune_cache().end()) {
     apply_shape(en, hit->second);
@@ -565,27 +684,52 @@ static oems_status autotune(oems_engine* en) {
   const int reps = (int)std::max<long long>(2, std::min<long long>(20, 200000000LL / std::max(1LL, cells)));
   LaunchShape best = en->shape;
   float best_ms = 1e30f;
-  const int blocks[] = {128, 256, 512};
-  const int chunks[] = {4, 8, 16, 32, 64};
-  oems_status st = OEMS_OK;
-  for (int b : blocks) {
-    for (int c : chunks) {
+  std::vector<LaunchShape> cands;
+  for (int b : {256, 512})
+    for (int c : {4, 8, 16, 32}) {
       if (c > 2 * en->nx && c != 4) continue;
       LaunchShape s;
       s.block = b;
       s.ichunk = c;
-      st = size_grid(en, s);
-      if (st != OEMS_OK) break;
-      apply_shape(en, s);
-      float ms = 0.f;
-      st = time_shape(en, reps, &ms);
-      if (st != OEMS_OK) break;
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = s;
-      }
+      if (want_reg) cands.push_back(s);
     }
+  if (want_tma) {
+    size_t limit = 0;
+    OEMS_TRY(tma_smem_limit(en, &limit));
+    for (int nc : {128, 256})
+      for (int per : {1, 2}) {
+        const int tj = std::max(1, std::min(en->ny, per * nc / en->g.nzq));
+        for (int c : {8, 16, 32})
+          for (int ns : {4, 3}) {
+            if (c > 2 * en->nx && c != 8) continue;
+            LaunchShape s;
+            s.tma = true;
+            s.nconsumer = nc;
+            s.ichunk = c;
+            s.smem = make_tma_geom(en, tj, c, nc, limit, ns, s.tg);
+            if (s.smem == 0) continue;
+            if (ns == 3 && s.tg.NS < 3) continue;  // same as the ns = 4 candidate
+            cands.push_back(s);
+          }
+      }
+  }
+  oems_status st = OEMS_OK;
+  for (LaunchShape s : cands) {
+    st = size_grid(en, s);
     if (st != OEMS_OK) break;
+    apply_shape(en, s);
+    float ms = 0.f;
+    st = time_shape(en, reps, &ms);
+    if (st != OEMS_OK) break;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = s;
+    }
+  }
+  if (st == OEMS_OK) {
+    int err = 0;
+    cudaMemcpy(&err, en->d_err.p, sizeof(int), cudaMemcpyDeviceToHost);
+    if (err) st = fail(OEMS_ERR_TIMEOUT, "a bounded device wait gave up while tuning");
   }
   apply_shape(en, best);
   if (st == OEMS_OK) tune_cache()[key] = best;
@@ -735,6 +879,8 @@ static oems_status create(const oems_operator_desc* d, oems_engine** out) {
   OEMS_CUDA(cudaMalloc(&en->d_partials.p, 6 * kEnergyBlocks * sizeof(double)));
   en->d_partials.n = 6 * kEnergyBlocks;
   OEMS_CUDA(en->d_base.ensure(1));
+  OEMS_CUDA(en->d_err.ensure(1));
+  OEMS_CUDA(cudaMemsetAsync(en->d_err.p, 0, sizeof(int), en->stream));
   LaunchShape s;
   OEMS_TRY(size_grid(en.get(), s));
   apply_shape(en.get(), s);
@@ -885,7 +1031,14 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
   if (ns > peaked)
     OEMS_CUDA(cudaMemcpyAsync(en->h_energy + 2 * peaked, en->d_energy.p + 2 * peaked,
                               (ns - peaked) * 2 * sizeof(double), cudaMemcpyDeviceToHost, en->stream));
+  int dev_err = 0;
+  OEMS_CUDA(cudaMemcpyAsync(&dev_err, en->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, en->stream));
   OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  if (dev_err != 0) {
+    cudaMemsetAsync(en->d_err.p, 0, sizeof(int), en->stream);
+    cudaStreamSynchronize(en->stream);
+    return fail(OEMS_ERR_TIMEOUT, "a bounded wait in an update kernel gave up; the fields are not valid");
+  }
   for (; peaked < ns; ++peaked) {
     const double tot = en->h_energy[2 * peaked] + en->h_energy[2 * peaked + 1];
     if (!std::isfinite(tot)) numerical = true;
@@ -1146,6 +1299,19 @@ oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable
   engine->profiling = enable != 0;
   engine->prof_h_s = engine->prof_e_s = 0.0;
   engine->prof_h_n = engine->prof_e_n = 0;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged, int32_t* threads, int32_t* ichunk,
+                                    int32_t* rows_per_tile, int32_t* stages, int32_t* grid) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  const LaunchShape& s = engine->shape;
+  if (staged) *staged = s.tma ? 1 : 0;
+  if (threads) *threads = s.tma ? s.nconsumer + 32 : s.block;
+  if (ichunk) *ichunk = s.ichunk;
+  if (rows_per_tile) *rows_per_tile = s.tma ? s.tg.TJ : 0;
+  if (stages) *stages = s.tma ? s.tg.NS : 0;
+  if (grid) *grid = s.grid_h;
   return OEMS_OK;
 }
 

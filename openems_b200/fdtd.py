@@ -428,11 +428,13 @@ class Engine:
 
     def __init__(self, operator: Operator, engine_type: EngineType = EngineType.Cuda, *,
                  device: int = -1, compressed: bool = False, autotune: bool = True,
-                 graphs: bool = True):
+                 graphs: bool = True, kernels: str = "auto"):
+        """kernels: "auto" (tuner picks), "register" or "staged" (bulk-async)."""
         if engine_type is not EngineType.Cuda:
             raise N.ConfigError("only the CUDA engine exists")
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
-            | (0 if graphs else N.ENGINE_NO_GRAPHS)
+            | (0 if graphs else N.ENGINE_NO_GRAPHS) \
+            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS}[kernels]
         desc = N.OperatorDesc()
         N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))
         h = ctypes.c_void_p()
@@ -569,6 +571,12 @@ class Engine:
         N.check(N.lib().oems_engine_kernel_profile(self._h, ctypes.byref(hs), ctypes.byref(hn),
                                                    ctypes.byref(es), ctypes.byref(en)))
         return hs.value, int(hn.value), es.value, int(en.value)
+
+    def launch_info(self) -> dict:
+        v = [N.c_i32() for _ in range(6)]
+        N.check(N.lib().oems_engine_launch_info(self._h, *[ctypes.byref(x) for x in v]))
+        keys = ("staged", "threads", "ichunk", "rows_per_tile", "stages", "grid")
+        return {k: int(x.value) for k, x in zip(keys, v)}
 
     def last_batch_stats(self) -> Tuple[int, float]:
         n, s = N.c_u64(), N.c_f64()

@@ -44,10 +44,10 @@ def make_operator(sc: Scenario) -> oe.Operator:
     return op
 
 
-def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True):
+def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kernels="auto"):
     """Runs the scenario on the CUDA engine; returns dict of results."""
     op = make_operator(sc)
-    eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune)
+    eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune, kernels=kernels)
     if sc.cpml is not None:
         eng.add_cpml(sc.cpml)
     for comp, pos in sc.probes:

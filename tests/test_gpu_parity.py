@@ -43,10 +43,11 @@ def assert_parity(got, ref, bit_exact=True):
         assert h1 == pytest.approx(h2, rel=1e-10, abs=1e-300)
 
 
-def test_config1_64_pec_2000_steps():
+@pytest.mark.parametrize("kernels", ("auto", "register", "staged"))
+def test_config1_64_pec_2000_steps(kernels):
     """64^3 PEC, 2000 steps, soft Gaussian Ez, 4 Ez/Hy probes (bit-exact)."""
     sc = config1_scenario(2000)
-    got = run_engine(sc)
+    got = run_engine(sc, kernels=kernels)
     ref = run_oracle(sc, precision=32, threads=8)
     assert_parity(got, ref)
     # accuracy against the FP64 oracle, reported and bounded
@@ -56,19 +57,32 @@ def test_config1_64_pec_2000_steps():
     assert max(errs) < 1e-3
 
 
+KERNELS = ("register", "staged")
+
+
+@pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("sc", reference_scenarios(), ids=lambda s: s.name)
-def test_reference_scenarios(sc):
-    assert_parity(run_engine(sc), run_oracle(sc))
+def test_reference_scenarios(sc, kernels):
+    assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
 
 
+@pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("sc", odd_scenarios(), ids=lambda s: s.name)
-def test_odd_sizes(sc):
-    assert_parity(run_engine(sc), run_oracle(sc))
+def test_odd_sizes(sc, kernels):
+    assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
 
 
+@pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("sc", cpml_scenarios(), ids=lambda s: s.name)
-def test_cpml(sc):
-    assert_parity(run_engine(sc), run_oracle(sc))
+def test_cpml(sc, kernels):
+    assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
+
+
+def test_staged_kernels_are_used_when_requested():
+    sc = cpml_scenarios()[0]
+    r = run_engine(sc, kernels="staged")
+    info = r["engine"].launch_info()
+    assert info["staged"] == 1 and info["stages"] >= 2, info
 
 
 @pytest.mark.parametrize("sc", [reference_scenarios()[2], odd_scenarios()[4], cpml_scenarios()[1]],
