@@ -411,7 +411,11 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   int sms = 0;
   OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, en->device));
   if (s.tma) {
-    OEMS_TRY(prepare_tma_kernels(s.smem));
+    // allow any stage count up to the opt-in limit (the attribute is per
+    // function, shared by every engine and tuning candidate)
+    size_t limit = 0;
+    OEMS_TRY(tma_smem_limit(en, &limit));
+    OEMS_TRY(prepare_tma_kernels(limit));
     int occ = 0;
     OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_update_tma<true>,
                                                             s.nconsumer + 32, s.smem));
