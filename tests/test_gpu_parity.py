@@ -54,7 +54,10 @@ def test_config1_64_pec_2000_steps(kernels):
     ref64 = run_oracle(sc, precision=64, threads=8)
     errs = [rel_l2(got["fields"][c], ref64["fields"][c]) for c in range(6)]
     print("config1 FP32 vs FP64 rel-L2:", ["%.2e" % e for e in errs])
-    assert max(errs) < 1e-3
+    # per vector field (Hz of an Ez source is ~0 by symmetry: its own relative
+    # error is rounding noise)
+    assert rel_l2(got["fields"][:3], ref64["fields"][:3]) < 1e-4
+    assert rel_l2(got["fields"][3:], ref64["fields"][3:]) < 1e-4
 
 
 KERNELS = ("register", "staged")

@@ -1,0 +1,174 @@
+"""The reference's known-answer unit tests, applied to the oracle (CPU).
+
+These pin the oracle to every known answer the Rust reference's own tests
+hold for this path; the reference ships no golden field arrays.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+
+C0 = 299792458.0
+
+
+def op5(delta=0.001, dt=None, precision=32):
+    """create_test_grid (src/fdtd/operator.rs:278-285): 5 cells of 1 mm per axis."""
+    lines = oracle.uniform_lines(5, delta)
+    dt0, d3 = oracle.grid_timestep(lines, lines, lines)
+    return oracle.OracleSim(5, 5, 5, dt if dt else dt0, d3, precision=precision), dt0
+
+
+# ---- src/fdtd/operator.rs:287-501 -----------------------------------------
+
+def test_timestep_below_cfl():
+    lines = oracle.uniform_lines(2, 0.001)
+    dt, _ = oracle.grid_timestep(lines, lines, lines)
+    assert 0 < dt < 1.0 / (C0 * math.sqrt(3.0) / 0.001)
+
+
+def test_vacuum_coefficients():
+    s, _ = op5()
+    c = s.coefficients()
+    ca, cb, da, db = c[0:3], c[3:6], c[6:9], c[9:12]
+    assert np.all(np.abs(ca[:, 2, 2, 2] - 1.0) < 1e-6) and np.all(cb[:, 2, 2, 2] > 0)
+    assert np.all(np.abs(da[:, 2, 2, 2] - 1.0) < 1e-6) and np.all(db[:, 2, 2, 2] < 0)
+
+
+def test_set_material_eps4_ratio_quarter():
+    s, _ = op5()
+    s.set_material(4.0, 1.0, 0.0, 0.0, (1, 3, 1, 3, 1, 3))
+    c = s.coefficients()
+    assert abs(c[0, 2, 2, 2] - 1.0) < 1e-6
+    assert abs(c[3, 2, 2, 2] / c[3, 0, 0, 0] - 0.25) < 1e-5
+    assert abs(c[6, 2, 2, 2] - 1.0) < 1e-6
+
+
+def test_set_material_lossy():
+    s, _ = op5()
+    s.set_material(2.0, 1.0, 0.01, 0.0, (1, 3, 1, 3, 1, 3))
+    ca = s.coefficients()[0, 2, 2, 2]
+    assert 0.0 < ca < 1.0
+
+
+def test_set_material_magnetic():
+    s, _ = op5()
+    s.set_material(1.0, 4.0, 0.0, 1e6, (1, 3, 1, 3, 1, 3))
+    c = s.coefficients()
+    assert 0.0 < c[6, 2, 2, 2] < 1.0
+    assert abs(c[9, 2, 2, 2]) < abs(c[9, 0, 0, 0])
+
+
+def test_set_pec():
+    s, _ = op5()
+    s.set_pec((1, 3, 1, 3, 1, 3))
+    c = s.coefficients()
+    assert np.all(np.abs(c[0:6, 2, 2, 2]) < 1e-10)
+    assert abs(c[0, 0, 0, 0] - 1.0) < 1e-6 and c[3, 0, 0, 0] > 0
+
+
+def test_anisotropic_timestep():
+    dt, _ = oracle.grid_timestep([0, 0.001, 0.002, 0.003], [0, 0.002, 0.004, 0.006], [0, 0.0005, 0.001])
+    dt_max = 1.0 / (C0 * math.sqrt(1 / 0.001 ** 2 + 1 / 0.002 ** 2 + 1 / 0.0005 ** 2))
+    assert 0.9 * dt_max < dt < dt_max
+
+
+# ---- src/fdtd/excitation.rs:258-400 -----------------------------------------
+
+def gaussian_params(fc, bw):
+    f_max = fc * (1.0 + 0.5 * bw)
+    tau = 1.0 / (math.pi * f_max)
+    return [4.0 * tau, tau]
+
+
+def test_gaussian():
+    p = gaussian_params(1e9, 0.5)
+    assert abs(oracle.excitation_eval(oracle.EXC_GAUSSIAN, p, 1.0, p[0]) - 1.0) < 1e-10
+    assert oracle.excitation_eval(oracle.EXC_GAUSSIAN, p, 1.0, 0.0) < 0.01
+    assert abs(oracle.excitation_eval(oracle.EXC_GAUSSIAN, p, 2.5, p[0]) - 2.5) < 1e-10
+
+
+def test_sinusoidal():
+    f = 1e9
+    v1 = oracle.excitation_eval(oracle.EXC_SINUSOIDAL, [f], 1.0, 0.0)
+    v2 = oracle.excitation_eval(oracle.EXC_SINUSOIDAL, [f], 1.0, 1.0 / f)
+    assert abs(v1 - v2) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_SINUSOIDAL, [f], 1.0, 0.25 / f) - 1.0) < 1e-10
+
+
+def test_gaussian_modulated():
+    fc, bw = 1e9, 0.5
+    tau = 1.0 / (math.pi * fc * bw)
+    p = [fc, 4 * tau, tau]
+    assert abs(oracle.excitation_eval(oracle.EXC_GAUSSIAN_MODULATED, p, 1.0, 0.0)) < 0.01
+    v1 = oracle.excitation_eval(oracle.EXC_GAUSSIAN_MODULATED, p, 1.0, p[1])
+    v2 = oracle.excitation_eval(oracle.EXC_GAUSSIAN_MODULATED, p, 1.0, p[1] + 0.5 / fc)
+    assert v1 * v2 <= 0.0 or abs(v1) < 0.1 or abs(v2) < 0.1
+
+
+def test_dirac_and_step():
+    assert abs(oracle.excitation_eval(oracle.EXC_DIRAC, [], 1.0, 0.0) - 1.0) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_DIRAC, [], 1.0, 1e-9)) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_DIRAC, [], 1.0, -1e-9)) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_STEP, [], 3.0, 0.0) - 3.0) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_STEP, [], 3.0, 1e-9) - 3.0) < 1e-10
+    assert abs(oracle.excitation_eval(oracle.EXC_STEP, [], 3.0, -1e-9)) < 1e-10
+
+
+# ---- src/fdtd/batch.rs:235-294 ----------------------------------------------
+
+def test_scheduled_samples_match_evaluate():
+    """ScheduledExcitation::from_excitation: samples[i] == (f32) evaluate(i*dt)."""
+    p = gaussian_params(1e9, 0.5)
+    s, _ = op5(dt=1e-12)
+    s.add_excitation_analytic((2, 2, 2), 2, True, oracle.EXC_GAUSSIAN, p, 1.0, 0, 100)
+    s.add_point_probe(2, (2, 2, 2))
+    s.run_batch(1)
+    # soft source into a zero field: after step 0 (E update of zero fields is zero)
+    # the cell holds exactly samples[0]
+    got = s.probe_traces()[0, 0]
+    assert abs(got - np.float32(oracle.excitation_eval(oracle.EXC_GAUSSIAN, p, 1.0, 0.0))) < 1e-6
+
+
+def test_energy_sample_arithmetic():
+    s, _ = op5()
+    f = np.zeros((6, 5, 5, 5), np.float32)
+    f[0, 2, 2, 2] = 1.0
+    f[4, 2, 2, 2] = 2.0
+    s.set_fields(f)
+    e, h = s.energy()
+    assert e == 1.0 and h == 4.0
+
+
+# ---- src/extensions/cpml.rs:744-804 ------------------------------------------
+
+def test_cpml_coefficient_ranges():
+    """sigma_max > 0; 0 <= b <= 1; a >= 0 (the reference's a is -c*kappa)."""
+    lines = oracle.uniform_lines(50, 0.001)
+    _, d3 = oracle.grid_timestep(lines, lines, lines)
+    s = oracle.OracleSim(50, 50, 50, 1e-12, d3)
+    s.enable_cpml((8,) * 6)
+    for f in range(6):
+        prof = s.cpml_profile(f)
+        assert len(prof["b_e"]) == 8
+        for k in ("b_e", "b_h"):
+            assert np.all((prof[k] >= 0) & (prof[k] <= 1))
+        for k in ("c_e", "c_h"):
+            assert np.all(-prof[k] >= 0)
+        # graded: deeper layers absorb more (smaller b)
+        b = prof["b_e"] if f % 2 else prof["b_e"][::-1]
+        assert np.all(np.diff(b) <= 0)
+
+
+def test_cpml_regions_count():
+    """Cpml::new with uniform(8) on 50^3 has 6 active regions (cpml.rs:744-759);
+    a face with layers >= n is inactive (cpml.rs:262, 283)."""
+    lines = oracle.uniform_lines(50, 0.001)
+    _, d3 = oracle.grid_timestep(lines, lines, lines)
+    s = oracle.OracleSim(50, 50, 50, 1e-12, d3)
+    s.enable_cpml((8,) * 6)
+    assert sum(1 for f in range(6) if len(s.cpml_profile(f)["b_e"])) == 6
+    s2 = oracle.OracleSim(6, 50, 50, 1e-12, d3)
+    s2.enable_cpml((6, 6, 8, 8, 8, 8))
+    assert [len(s2.cpml_profile(f)["b_e"]) for f in range(6)] == [0, 0, 8, 8, 8, 8]
