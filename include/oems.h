@@ -199,6 +199,21 @@ OEMS_API oems_status oems_engine_read_probe_traces(oems_engine* engine, float* o
  * (VectorField3D::energy, src/arrays/field.rs:314-316), computed on the GPU. */
 OEMS_API oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_energy);
 
+/* Energies without allocation.  No counterpart in the reference.  For callers
+ * that cannot let the library call cudaMalloc (a host that owns all device
+ * memory, a loop that must not stall on an allocation's implicit device
+ * synchronisation): the same sums as oems_engine_energy, computed from six
+ * caller-owned device arrays (Ex Ey Ez Hx Hy Hz, `count` floats each, 16-byte
+ * aligned, count <= 67108864), written to the device pointer `energies`
+ * (energies[0] = sum E^2, energies[1] = sum H^2), on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream), asynchronously.  Partial
+ * sums live in a fixed 192 KB device array inside the library that every call
+ * on a device shares (calls that overlap on the GPU race on it).  The first
+ * call on each device looks up that array's address; make it before any
+ * stream capture. */
+OEMS_API oems_status oems_field_energy_noalloc(const float* const fields[6], uint64_t count,
+                                               double* energies, void* stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Per-kernel timing: while enabled, run_batch launches the update kernels one

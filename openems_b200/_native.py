@@ -149,6 +149,7 @@ SIGNATURES = {
     "oems_last_error_message": (ctypes.c_char_p, []),
     "oems_abi_version": (c_i32, []),
     "oems_engine_last_batch_stats": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_f64)]),
+    "oems_field_energy_noalloc": (c_i32, [ctypes.c_void_p * 6, c_u64, P, P]),
     "oems_engine_set_kernel_profiling": (c_i32, [P, c_i32]),
     "oems_engine_launch_info": (c_i32, [P] + [ctypes.POINTER(c_i32)] * 6),
     "oems_engine_kernel_profile": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_u64),

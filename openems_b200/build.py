@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liboems_b200.so")
-SOURCES = ["csrc/engine.cu", "csrc/host.cpp"]
+SOURCES = ["csrc/engine.cu", "csrc/host.cpp", "csrc/noalloc.cu"]
 HEADERS = ["csrc/yee_kernels.cuh", "../include/oems.h"]
 
 NVCC_FLAGS = [
