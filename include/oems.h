@@ -20,6 +20,7 @@
  * update kernels):
  *
  *   Cpml::new           src/extensions/cpml.rs:235     -> oems_engine_add_cpml
+ *   MurAbc::new         src/extensions/mur_abc.rs:175  -> oems_engine_add_mur
  *   FieldProbe::sample  src/processing/probes.rs:289   -> oems_engine_add_point_probe
  *
  * Conventions
@@ -160,6 +161,20 @@ typedef struct oems_cpml_desc {
   double kappa_max;        /* default 1    */
 } oems_cpml_desc;
 
+/* MurAbcConfig (src/extensions/mur_abc.rs:13-28).  enabled: xmin xmax ymin
+ * ymax zmin zmax.  order 1 restates the reference (mur_abc.rs:88-324): pre
+ * before the E update, post and apply after it, faces applied in order.
+ * order 2 is the second-order Mur condition (no counterpart in the
+ * reference) on face interiors, first order on the two outermost rows and
+ * columns of a face; at a min face its boundary is line 1, the first line the
+ * E update writes. */
+typedef struct oems_mur_desc {
+  int32_t enabled[6];
+  int32_t order;
+  int32_t reserved0;
+  double phase_velocity; /* <= 0: c0 */
+} oems_mur_desc;
+
 /* Field components for probes: 0..2 = Ex Ey Ez, 3..5 = Hx Hy Hz. */
 #define OEMS_COMPONENT_EX 0
 #define OEMS_COMPONENT_HX 3
@@ -184,6 +199,8 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 /* ---- extensions ---------------------------------------------------------- */
 
 OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);
+/* MurAbc::new (src/extensions/mur_abc.rs:175). */
+OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc);
 
 /* ---- probes ---------------------------------------------------------------- */
 

@@ -9,7 +9,7 @@ from ._native import (OpenEMSError, ConfigError, IoError, GridError, MaterialErr
                       NumericalError, XmlError, CudaError, NoDeviceError, DeviceTimeoutError,
                       InvalidArgumentError, LIB_PATH)
 from .constants import C0, EPS0, MU0, Z0  # noqa: F401
-from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, Operator,  # noqa: F401
+from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, MurAbcConfig, Operator,  # noqa: F401
                    Excitation, ExcitationType, ScheduledExcitation, TerminationConfig,
                    EnergyMonitorConfig, EngineBatch, TerminationReason, EnergySample, BatchResult,
                    EngineType, Engine, EndCondition, SimulationStats, Simulation)

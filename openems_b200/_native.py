@@ -119,6 +119,11 @@ class CpmlDescC(ctypes.Structure):
                 ("alpha_max", c_f64), ("kappa_max", c_f64)]
 
 
+class MurDescC(ctypes.Structure):
+    _fields_ = [("enabled", c_i32 * 6), ("order", c_i32), ("reserved0", c_i32),
+                ("phase_velocity", c_f64)]
+
+
 class ExcitationC(ctypes.Structure):
     _fields_ = [("kind", c_i32), ("direction", c_u32), ("position", c_u64 * 3),
                 ("params", c_f64 * 3), ("amplitude", c_f64), ("soft_source", c_i32),
@@ -142,6 +147,7 @@ SIGNATURES = {
     "oems_engine_write_fields": (c_i32, [P, PF * 3, PF * 3]),
     "oems_engine_reset": (c_i32, [P]),
     "oems_engine_add_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
+    "oems_engine_add_mur": (c_i32, [P, ctypes.POINTER(MurDescC)]),
     "oems_engine_add_point_probe": (c_i32, [P, c_i32, c_u64 * 3, ctypes.POINTER(c_i32)]),
     "oems_engine_read_probe_traces": (c_i32, [P, PF, c_u64, ctypes.POINTER(c_u64)]),
     "oems_engine_energy": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),

@@ -29,6 +29,7 @@
 #include "../../include/oems.h"
 #include "yee_kernels.cuh"
 #include "yee_tma.cuh"
+#include "mur.cuh"
 
 namespace oems {
 
@@ -194,6 +195,12 @@ struct CpmlHost {
   std::vector<size_t> psi_sizes;
 };
 
+struct MurHost {
+  bool on = false;
+  MurArgs args{};
+  DevBuf<float> state;  // v, ob, os: 3 x 2 x total
+};
+
 }  // namespace oems
 
 struct oems_engine {
@@ -216,6 +223,7 @@ struct oems_engine {
   int ntable = 0;
 
   oems::CpmlHost cpml;
+  oems::MurHost mur;
 
   // probes
   std::vector<long long> probe_idx;
@@ -501,13 +509,41 @@ static cudaError_t launch_post(oems_engine* en, int local) {
   return cudaGetLastError();
 }
 
-static int kernels_per_step(const oems_engine* en) { return 2 + (need_post(en) ? 1 : 0); }
+// Extension kernels between the H and E updates (Mur pre) and after the E
+// update (Mur post and apply), in the reference's hook order.
+static int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+static cudaError_t launch_pre_e(oems_engine* en) {
+  if (en->mur.on) {
+    k_mur_pre<<<blocks_for(en->mur.args.total, 256), 256, 0, en->stream>>>(en->mur.args);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t launch_post_e(oems_engine* en) {
+  if (en->mur.on) {
+    const int b = blocks_for(en->mur.args.total, 256);
+    k_mur_post<<<b, 256, 0, en->stream>>>(en->mur.args);
+    k_mur_apply<<<b, 256, 0, en->stream>>>(en->mur.args);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static int ext_kernels(const oems_engine* en) { return en->mur.on ? 3 : 0; }
+
+static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + (need_post(en) ? 1 : 0); }
 
 // Launches `steps` timesteps directly (no graph).
 static oems_status launch_steps_direct(oems_engine* en, int steps) {
   for (int s = 0; s < steps; ++s) {
     OEMS_CUDA(launch_h(en));
+    OEMS_CUDA(launch_pre_e(en));
     OEMS_CUDA(launch_e(en));
+    OEMS_CUDA(launch_post_e(en));
     if (need_post(en)) OEMS_CUDA(launch_post(en, s));
   }
   return OEMS_OK;
@@ -528,9 +564,11 @@ static oems_status launch_steps_profiled(oems_engine* en, int steps) {
       OEMS_CUDA(cudaEventRecord(ev[0], en->stream));
       OEMS_CUDA(launch_h(en));
       OEMS_CUDA(cudaEventRecord(ev[1], en->stream));
+      OEMS_CUDA(launch_pre_e(en));
       OEMS_CUDA(cudaEventRecord(ev[2], en->stream));
       OEMS_CUDA(launch_e(en));
       OEMS_CUDA(cudaEventRecord(ev[3], en->stream));
+      OEMS_CUDA(launch_post_e(en));
       if (need_post(en)) OEMS_CUDA(launch_post(en, s0 + s));
     }
     OEMS_CUDA(cudaEventSynchronize(en->prof_ev[4 * (n - 1) + 3]));
@@ -1087,6 +1125,61 @@ static oems_status copy_fields(oems_engine* en, float* const* host6, bool to_hos
   return OEMS_OK;
 }
 
+// MurAbc::new (src/extensions/mur_abc.rs:175-206) and its face set-up
+// (:88-151); second order as described in mur.cuh.
+static oems_status add_mur(oems_engine* en, const oems_mur_desc* d) {
+  if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL Mur descriptor");
+  if (en->mur.on) return fail(OEMS_ERR_CONFIG, "Mur boundary already attached");
+  if (d->order != 1 && d->order != 2) return fail(OEMS_ERR_CONFIG, "Mur order must be 1 or 2");
+  DeviceGuard guard(en->device);
+  const int ext[3] = {en->nx, en->ny, en->nz};
+  const double kC0 = 299792458.0;
+  const double c = d->phase_velocity > 0.0 ? d->phase_velocity : kC0;
+  MurArgs& A = en->mur.args;
+  A = MurArgs{};
+  A.order = d->order;
+  long long off = 0;
+  for (int f = 0; f < 6; ++f) {
+    if (!d->enabled[f]) continue;
+    MurFaceDev F{};
+    F.ny = f / 2;
+    F.nyp = (F.ny + 1) % 3;
+    F.nypp = (F.ny + 2) % 3;
+    const bool is_max = f % 2 == 1;
+    const int o = (d->order == 2 && !is_max) ? 1 : 0;
+    const int n = ext[F.ny];
+    if (n < 2 + o) return fail(OEMS_ERR_CONFIG, "Mur face needs at least two cells along its normal");
+    F.line = is_max ? n - 1 : o;
+    F.shift = is_max ? n - 2 : o + 1;
+    F.size0 = ext[F.nyp];
+    F.size1 = ext[F.nypp];
+    F.lo0 = (d->order == 2 && d->enabled[2 * F.nyp]) ? 1 : 0;
+    F.lo1 = (d->order == 2 && d->enabled[2 * F.nypp]) ? 1 : 0;
+    const double cdt = c * en->dt, dn = en->delta[F.ny];
+    F.coeff = (float)((cdt - dn) / (cdt + dn));
+    F.c2 = (float)(2.0 * dn / (cdt + dn));
+    F.c3p = (float)(cdt * cdt * dn / (2.0 * en->delta[F.nyp] * en->delta[F.nyp] * (cdt + dn)));
+    F.c3q = (float)(cdt * cdt * dn / (2.0 * en->delta[F.nypp] * en->delta[F.nypp] * (cdt + dn)));
+    F.off = off;
+    off += (long long)F.size0 * F.size1;
+    A.f[A.nfaces++] = F;
+  }
+  if (A.nfaces == 0) return fail(OEMS_ERR_CONFIG, "no Mur face enabled");
+  A.total = off;
+  OEMS_CUDA(en->mur.state.ensure((size_t)6 * off));
+  OEMS_CUDA(cudaMemsetAsync(en->mur.state.p, 0, (size_t)6 * off * sizeof(float), en->stream));
+  A.v = en->mur.state.p;
+  A.ob = A.v + 2 * off;
+  A.os = A.ob + 2 * off;
+  for (int c3 = 0; c3 < 3; ++c3) A.e[c3] = en->E(c3);
+  A.ny = en->ny;
+  A.nzp = en->g.nzp;
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  en->mur.on = true;
+  en->graph_epoch++;
+  return OEMS_OK;
+}
+
 static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
   if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL CPML descriptor");
   if (en->cpml.on) return fail(OEMS_ERR_CONFIG, "CPML already attached");
@@ -1241,6 +1334,8 @@ oems_status oems_engine_reset(oems_engine* engine) {
   OEMS_CUDA(cudaMemsetAsync(engine->fields, 0, (size_t)6 * engine->ncells_padded * sizeof(float), engine->stream));
   if (engine->cpml.on)
     OEMS_CUDA(cudaMemsetAsync(engine->cpml.psi.p, 0, engine->cpml.psi.n * sizeof(float), engine->stream));
+  if (engine->mur.on)
+    OEMS_CUDA(cudaMemsetAsync(engine->mur.state.p, 0, engine->mur.state.n * sizeof(float), engine->stream));
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   engine->timestep = 0;
   return OEMS_OK;
@@ -1249,6 +1344,11 @@ oems_status oems_engine_reset(oems_engine* engine) {
 oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   return add_cpml(engine, desc);
+}
+
+oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  return add_mur(engine, desc);
 }
 
 oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component, const uint64_t position[3],

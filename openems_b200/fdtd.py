@@ -145,6 +145,28 @@ class CpmlBoundaries:
         return d
 
 
+@dataclass
+class MurAbcConfig:
+    """MurAbcConfig (src/extensions/mur_abc.rs:13-58); order 2 selects the
+    second-order Mur condition (no counterpart in the reference)."""
+
+    enabled: Tuple[bool, ...] = (True,) * 6
+    phase_velocity: Optional[float] = None
+    order: int = 1
+
+    @classmethod
+    def all(cls, order: int = 1):
+        return cls(order=order)
+
+    def to_c(self) -> N.MurDescC:
+        d = N.MurDescC()
+        for f in range(6):
+            d.enabled[f] = int(bool(self.enabled[f]))
+        d.order = int(self.order)
+        d.phase_velocity = float(self.phase_velocity or 0.0)
+        return d
+
+
 # ---------------------------------------------------------------------------
 # operator
 # ---------------------------------------------------------------------------
@@ -474,6 +496,10 @@ class Engine:
     def add_cpml(self, cpml: CpmlBoundaries):
         d = cpml.to_c()
         N.check(N.lib().oems_engine_add_cpml(self._h, ctypes.byref(d)))
+
+    def add_mur(self, mur: MurAbcConfig):
+        d = mur.to_c()
+        N.check(N.lib().oems_engine_add_mur(self._h, ctypes.byref(d)))
 
     def add_point_probe(self, component: int, position) -> int:
         p = (N.c_u64 * 3)(*[int(v) for v in position])

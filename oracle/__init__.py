@@ -82,6 +82,8 @@ def lib() -> ctypes.CDLL:
         L.orc_enable_cpml.argtypes = [P, P, D, D, D, D]
         L.orc_cpml_profile.restype = I32
         L.orc_cpml_profile.argtypes = [P, I32, P]
+        L.orc_enable_mur.restype = I32
+        L.orc_enable_mur.argtypes = [P, P, I32, D]
         L.orc_run_batch.restype = I32
         L.orc_run_batch.argtypes = [P, U64, U64, I32, U64, I32, D, D, ctypes.POINTER(BatchResult)]
         L.orc_get_energy_samples.argtypes = [P, ctypes.POINTER(EnergySample), U64]
@@ -209,6 +211,12 @@ class OracleSim:
                                    kappa_max)
         if rc != 0:
             raise ValueError(f"invalid CPML configuration ({rc})")
+
+    def enable_mur(self, enabled=(1,) * 6, order=1, phase_velocity=0.0):
+        e = np.ascontiguousarray([int(bool(v)) for v in enabled], dtype=np.int32)
+        rc = lib().orc_enable_mur(self._h, _ptr(e), order, phase_velocity or 0.0)
+        if rc != 0:
+            raise ValueError(f"invalid Mur configuration ({rc})")
 
     def cpml_profile(self, face):
         out = np.zeros((6, 256))

@@ -107,6 +107,23 @@ struct Sim {
   // E: ex_y ex_z ey_z ey_x ez_x ez_y
   std::vector<T> psi_h[6], psi_e[6];
 
+  // Mur state (src/extensions/mur_abc.rs:60-131): per face the normal axis,
+  // its two tangential axes, boundary and shift lines, face size and the
+  // pending boundary values; second order also keeps the time-n-1 values of
+  // both lines.
+  struct MurFace {
+    int ny, nyp, nypp;
+    int64_t line, shift;
+    int64_t size0, size1;
+    int64_t lo0, lo1;               // second order: first live row / column of the face
+    T coeff;                        // (c dt - d) / (c dt + d)
+    T c2, c3p, c3q;                 // second order
+    std::vector<T> v[2];            // pending values for nyp, nypp
+    std::vector<T> ob[2], os[2];    // boundary / shift line at n-1 (second order)
+  };
+  std::vector<MurFace> mur;
+  int mur_order = 0;
+
   Sim(int64_t nx_, int64_t ny_, int64_t nz_, double dt_, double dx, double dy, double dz)
       : nx(nx_), ny(ny_), nz(nz_), n(nx_ * ny_ * nz_), dt(dt_) {
     delta[0] = dx;
@@ -371,6 +388,130 @@ struct Sim {
     }
   }
 
+  int enable_mur(const int32_t* en, int order, double vphase) {
+    const int64_t ext[3] = {nx, ny, nz};
+    const double c = vphase > 0.0 ? vphase : kC0;
+    mur.clear();
+    for (int f = 0; f < 6; ++f) {
+      if (!en[f]) continue;
+      MurFace F;
+      F.ny = f / 2;
+      F.nyp = (F.ny + 1) % 3;
+      F.nypp = (F.ny + 2) % 3;
+      const int64_t n = ext[F.ny];
+      if (n < 2) return -1;
+      const bool is_max = f % 2 == 1;
+      // first order: the reference's lines (mur_abc.rs:93-103).  Second order:
+      // at a min face the plane 0 is never updated by the E loop (not even its
+      // normal component), so the boundary sits on the first updated line.
+      const int64_t off = (order == 2 && !is_max) ? 1 : 0;
+      if (n < 2 + off) return -1;
+      F.line = is_max ? n - 1 : off;
+      F.shift = is_max ? n - 2 : off + 1;
+      F.size0 = ext[F.nyp];
+      F.size1 = ext[F.nypp];
+      // second order: the plane 0 of a tangential axis whose min face is a
+      // second-order Mur face is dead (never updated) and not part of this face
+      F.lo0 = (order == 2 && en[2 * F.nyp]) ? 1 : 0;
+      F.lo1 = (order == 2 && en[2 * F.nypp]) ? 1 : 0;
+      // src/extensions/mur_abc.rs:138-151
+      const double cdt = c * dt, d = delta[F.ny];
+      F.coeff = T((cdt - d) / (cdt + d));
+      F.c2 = T(2.0 * d / (cdt + d));
+      F.c3p = T(cdt * cdt * d / (2.0 * delta[F.nyp] * delta[F.nyp] * (cdt + d)));
+      F.c3q = T(cdt * cdt * d / (2.0 * delta[F.nypp] * delta[F.nypp] * (cdt + d)));
+      const size_t m = (size_t)(F.size0 * F.size1);
+      for (int t = 0; t < 2; ++t) {
+        F.v[t].assign(m, T(0));
+        F.ob[t].assign(m, T(0));
+        F.os[t].assign(m, T(0));
+      }
+      mur.push_back(F);
+    }
+    mur_order = order;
+    return 0;
+  }
+
+  int64_t mur_idx(const MurFace& F, int64_t line, int64_t p, int64_t q) const {
+    int64_t pos[3];
+    pos[F.ny] = line;
+    pos[F.nyp] = p;
+    pos[F.nypp] = q;
+    return idx(pos[0], pos[1], pos[2]);
+  }
+
+  // (W(+1) + W(-1)) - 2 W along one face axis of line `line`
+  T lap(const std::vector<T>& W, const MurFace& F, int64_t line, int64_t p, int64_t q, bool along_p) const {
+    const int64_t a = along_p ? mur_idx(F, line, p + 1, q) : mur_idx(F, line, p, q + 1);
+    const int64_t b = along_p ? mur_idx(F, line, p - 1, q) : mur_idx(F, line, p, q - 1);
+    const T s1 = W[a] + W[b];
+    const T s2 = T(2) * W[mur_idx(F, line, p, q)];
+    return s1 - s2;
+  }
+
+  // Before the E update: src/extensions/mur_abc.rs:213-254 (first order).
+  void mur_pre() {
+    for (MurFace& F : mur) {
+      const int comp[2] = {F.nyp, F.nypp};
+      for (int64_t p = 0; p < F.size0; ++p)
+        for (int64_t q = 0; q < F.size1; ++q) {
+          const size_t m = (size_t)(p * F.size1 + q);
+          if (p < F.lo0 || q < F.lo1) continue;
+          const bool interior =
+              mur_order == 2 && p > F.lo0 + 1 && p + 2 < F.size0 && q > F.lo1 + 1 && q + 2 < F.size1;
+          for (int t = 0; t < 2; ++t) {
+            const std::vector<T>& W = E[comp[t]];
+            const T wb = W[mur_idx(F, F.line, p, q)];
+            const T ws = W[mur_idx(F, F.shift, p, q)];
+            if (!interior) {
+              const T a = F.coeff * wb;
+              F.v[t][m] = ws - a;
+            } else {
+              const T a1 = F.coeff * F.ob[t][m];
+              T acc = a1 - F.os[t][m];
+              const T s = wb + ws;
+              acc = acc + F.c2 * s;
+              const T lp = lap(W, F, F.line, p, q, true) + lap(W, F, F.shift, p, q, true);
+              acc = acc + F.c3p * lp;
+              const T lq = lap(W, F, F.line, p, q, false) + lap(W, F, F.shift, p, q, false);
+              acc = acc + F.c3q * lq;
+              F.v[t][m] = acc;
+            }
+            if (mur_order == 2) {
+              F.ob[t][m] = wb;
+              F.os[t][m] = ws;
+            }
+          }
+        }
+    }
+  }
+
+  // After the E update: post (mur_abc.rs:257-291) for every face, then apply
+  // (mur_abc.rs:294-324) face by face.
+  void mur_post_apply() {
+    for (MurFace& F : mur) {
+      const int comp[2] = {F.nyp, F.nypp};
+      for (int64_t p = 0; p < F.size0; ++p)
+        for (int64_t q = 0; q < F.size1; ++q) {
+          const size_t m = (size_t)(p * F.size1 + q);
+          if (p < F.lo0 || q < F.lo1) continue;
+          for (int t = 0; t < 2; ++t) {
+            const T a = F.coeff * E[comp[t]][mur_idx(F, F.shift, p, q)];
+            F.v[t][m] = F.v[t][m] + a;
+          }
+        }
+    }
+    for (MurFace& F : mur) {
+      const int comp[2] = {F.nyp, F.nypp};
+      for (int64_t p = 0; p < F.size0; ++p)
+        for (int64_t q = 0; q < F.size1; ++q) {
+          const size_t m = (size_t)(p * F.size1 + q);
+          if (p < F.lo0 || q < F.lo1) continue;
+          for (int t = 0; t < 2; ++t) E[comp[t]][mur_idx(F, F.line, p, q)] = F.v[t][m];
+        }
+    }
+  }
+
   // src/arrays/field.rs:219-221, :314-316
   static double sumsq(const std::vector<T>& a) {
     double s = 0.0;
@@ -395,7 +536,9 @@ struct Sim {
     for (uint64_t step = 0; step < num_steps; ++step) {
       uint64_t cur = timestep;
       update_h();
+      if (!mur.empty()) mur_pre();
       update_e();
+      if (!mur.empty()) mur_post_apply();
       apply_excitations(step);
       record_probes();
       timestep += 1;
@@ -558,6 +701,12 @@ void orc_reset(orc_sim* s) {
       std::fill(S->psi_h[q].begin(), S->psi_h[q].end(), T(0));
       std::fill(S->psi_e[q].begin(), S->psi_e[q].end(), T(0));
     }
+    for (auto& F : S->mur)
+      for (int t = 0; t < 2; ++t) {
+        std::fill(F.v[t].begin(), F.v[t].end(), T(0));
+        std::fill(F.ob[t].begin(), F.ob[t].end(), T(0));
+        std::fill(F.os[t].begin(), F.os[t].end(), T(0));
+      }
     S->timestep = 0;
   });
 }
@@ -642,6 +791,13 @@ int32_t orc_cpml_profile(const orc_sim* s, int32_t f, double* out) {
     }
   });
   return L;
+}
+
+int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity) {
+  if (order != 1 && order != 2) return -2;
+  int rc = 0;
+  DISPATCH(s, rc = S->enable_mur(enabled6, order, phase_velocity));
+  return rc;
 }
 
 int32_t orc_run_batch(orc_sim* s, uint64_t num_steps, uint64_t sample_interval, int32_t track_peak,

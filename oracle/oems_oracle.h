@@ -125,6 +125,13 @@ int32_t orc_enable_cpml(orc_sim* s, const int32_t* layers6, double grading_order
  * precision). Returns the layer count, 0 if the face is disabled. */
 int32_t orc_cpml_profile(const orc_sim* s, int32_t face, double* out);
 
+/* Mur absorbing boundary on the faces with enabled[f] != 0.  order 1 restates
+ * src/extensions/mur_abc.rs:88-324 (pre before the E update, post and apply
+ * after it, faces applied in order); order 2 is the second-order Mur
+ * condition (Mur 1981) on face interiors, first order on face edges.
+ * phase_velocity <= 0 means c0.  Returns 0 or a negative error. */
+int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity);
+
 int32_t orc_run_batch(orc_sim* s, uint64_t num_steps, uint64_t sample_interval,
                       int32_t track_peak, uint64_t check_interval, int32_t has_decay,
                       double decay_db, double initial_peak, orc_batch_result* res);

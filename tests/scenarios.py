@@ -27,6 +27,7 @@ class Scenario:
     sample_interval: int = 0
     track_peak: bool = False
     cpml: Optional[oe.CpmlBoundaries] = None
+    mur: Optional[oe.MurAbcConfig] = None
     probes: List[Tuple[int, Tuple[int, int, int]]] = field(default_factory=list)
     batches: Sequence[int] = ()  # split num_steps into these batch sizes (default: one batch)
 
@@ -50,6 +51,8 @@ def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kerne
     eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune, kernels=kernels)
     if sc.cpml is not None:
         eng.add_cpml(sc.cpml)
+    if sc.mur is not None:
+        eng.add_mur(sc.mur)
     for comp, pos in sc.probes:
         eng.add_point_probe(comp, pos)
     dt = op.timestep()
@@ -83,6 +86,8 @@ def run_oracle(sc: Scenario, precision=32, threads=1):
     if sc.cpml is not None:
         c = sc.cpml
         s.enable_cpml(c.layers, c.grading_order, c.reflection_coeff, c.alpha_max, c.kappa_max)
+    if sc.mur is not None:
+        s.enable_mur(sc.mur.enabled, sc.mur.order, sc.mur.phase_velocity or 0.0)
     for comp, pos in sc.probes:
         s.add_point_probe(comp, pos)
     energy, traces, start = [], [], 0
@@ -211,4 +216,23 @@ def cpml_scenarios() -> List[Scenario]:
                  cpml=oe.CpmlBoundaries(layers=(4, 5, 0, 6, 7, 3), grading_order=4.0,
                                         reflection_coeff=1e-5, alpha_max=0.05, kappa_max=3.0),
                  probes=[(1, (9, 11, 14)), (5, (1, 1, 1))]),
+    ]
+
+
+def mur_scenarios() -> List[Scenario]:
+    E = oe.Excitation
+    f0 = 10e9
+    x = E.gaussian_modulated(f0, 0.5, 2, (12, 11, 13))
+    return [
+        Scenario("mur1_all", (25, 22, 27), 1e-3, excitations=[x], num_steps=300, sample_interval=25,
+                 track_peak=True, mur=oe.MurAbcConfig.all(1), probes=[(2, (1, 11, 13)), (1, (24, 5, 5))]),
+        Scenario("mur2_all", (25, 22, 27), 1e-3, excitations=[x], num_steps=300, sample_interval=25,
+                 track_peak=True, mur=oe.MurAbcConfig.all(2), probes=[(2, (1, 11, 13)), (1, (24, 5, 5))]),
+        Scenario("mur1_partial_phase", (18, 9, 14), 0.8e-3,
+                 materials=[(3.0, 1.0, 0.01, 0.0, (0, 18, 0, 9, 0, 7))],
+                 excitations=[E.gaussian_modulated(8e9, 0.5, 1, (9, 4, 7))], num_steps=200,
+                 mur=oe.MurAbcConfig(enabled=(1, 0, 1, 1, 0, 1), phase_velocity=2.0e8, order=1)),
+        Scenario("mur2_partial", (18, 9, 14), 0.8e-3,
+                 excitations=[E.gaussian_modulated(8e9, 0.5, 0, (9, 4, 7))], num_steps=200,
+                 mur=oe.MurAbcConfig(enabled=(0, 1, 1, 0, 1, 1), order=2)),
     ]

@@ -11,8 +11,8 @@ import pytest
 
 import openems_b200 as oe
 from conftest import rel_l2
-from scenarios import (config1_scenario, cpml_scenarios, odd_scenarios, reference_scenarios,
-                       run_engine, run_oracle)
+from scenarios import (config1_scenario, cpml_scenarios, mur_scenarios, odd_scenarios,
+                       reference_scenarios, run_engine, run_oracle)
 
 pytestmark = pytest.mark.gpu
 
@@ -78,6 +78,12 @@ def test_odd_sizes(sc, kernels):
 @pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("sc", cpml_scenarios(), ids=lambda s: s.name)
 def test_cpml(sc, kernels):
+    assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
+
+
+@pytest.mark.parametrize("kernels", KERNELS)
+@pytest.mark.parametrize("sc", mur_scenarios(), ids=lambda s: s.name)
+def test_mur(sc, kernels):
     assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
 
 
