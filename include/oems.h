@@ -204,13 +204,42 @@ OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_des
 
 /* ---- probes ---------------------------------------------------------------- */
 
-/* A point probe records one value per executed step (after the excitation). */
+/* One term of a probe: the value of `component` at `position`, with weight. */
+typedef struct oems_probe_term {
+  int32_t component; /* 0..2 = Ex Ey Ez, 3..5 = Hx Hy Hz */
+  int32_t reserved0;
+  uint64_t position[3];
+  double weight;
+} oems_probe_term;
+
+/* Probe modes.  F32: the term values summed in order in f32, weight +1 adds
+ * and weight -1 subtracts (VoltageProbe::sample / CurrentProbe::sample,
+ * src/processing/probes.rs:98-239).  F64: sum of weight * value in f64
+ * (EngineInterface::calc_voltage_integral / calc_current_integral,
+ * src/fdtd/engine_interface.rs:208-305; port loop integrals). */
+#define OEMS_PROBE_SUM_F32 0
+#define OEMS_PROBE_SUM_F64 1
+
+/* A probe records one value per executed step, after the excitation: E
+ * values belong to t = (n+1) dt, H values to (n+1/2) dt. */
+OEMS_API oems_status oems_engine_add_probe(oems_engine* engine, const oems_probe_term* terms,
+                                           uint64_t nterms, int32_t mode, int32_t* probe_id);
+/* FieldProbe-style single value (src/processing/probes.rs:289-303). */
 OEMS_API oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component,
                                         const uint64_t position[3], int32_t* probe_id);
-/* Traces of the most recent batch, layout [step][probe]; *steps_out receives
- * the number of steps recorded (at most max_steps are copied). */
-OEMS_API oems_status oems_engine_read_probe_traces(oems_engine* engine, float* out, uint64_t max_steps,
+/* Traces of the most recent batch, layout [step][probe], f64; *steps_out
+ * receives the number of steps recorded (at most max_steps are copied). */
+OEMS_API oems_status oems_engine_read_probe_traces(oems_engine* engine, double* out, uint64_t max_steps,
                                           uint64_t* steps_out);
+/* Running DFT of a probe's trace (FrequencyDomainFieldDump::accumulate,
+ * src/processing/fields_fd.rs:149-217, applied to the probe value):
+ * X(f) += x(t) exp(-j 2 pi f t) 2 dt in f64, t = (timestep after the step -
+ * h) dt with h = 1/2 for a probe of H components only, 0 otherwise.
+ * Accumulates over every step run after the call, until reset. */
+OEMS_API oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t probe_id,
+                                               const double* freqs, uint64_t nfreq, int32_t* dft_id);
+/* out: 2 * nfreq doubles (re, im per frequency). */
+OEMS_API oems_status oems_engine_read_probe_dft(oems_engine* engine, int32_t dft_id, double* out);
 
 /* Unweighted field energies sum(E^2), sum(H^2) in f64 over the whole grid
  * (VectorField3D::energy, src/arrays/field.rs:314-316), computed on the GPU. */

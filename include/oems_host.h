@@ -88,6 +88,40 @@ OEMS_API double oems_excitation_evaluate(const oems_excitation* exc, double t);
 OEMS_API oems_status oems_excitation_sample(const oems_excitation* exc, uint64_t start_timestep, uint64_t n,
                                    double dt, float* out);
 
+/* ---- probe term builders --------------------------------------------------
+ * Each fills up to `cap` terms into `out` and the required count into *n
+ * (call with cap = 0 to size the buffer); the terms go to
+ * oems_engine_add_probe with the mode named below. */
+
+/* VoltageProbe::sample (src/processing/probes.rs:98-131): E[direction] summed
+ * over the inclusive line start..end along `direction`; mode F32.  An
+ * invalid direction gives no term (value 0). */
+OEMS_API oems_status oems_probe_voltage_terms(const uint64_t start[3], const uint64_t end[3],
+                                              int32_t direction, oems_probe_term* out, uint64_t cap,
+                                              uint64_t* n);
+/* CurrentProbe::sample (src/processing/probes.rs:193-239): +H and -H of the
+ * two tangential components over the inclusive surface; mode F32. */
+OEMS_API oems_status oems_probe_current_terms(const uint64_t start[3], const uint64_t end[3],
+                                              int32_t normal, oems_probe_term* out, uint64_t cap,
+                                              uint64_t* n);
+/* EngineInterface::calc_voltage_integral (src/fdtd/engine_interface.rs:208-
+ * 247) between cell indices: V = -sum E . dl along x, then y, then z; mode F64. */
+OEMS_API oems_status oems_probe_voltage_integral_terms(const oems_operator* op, const uint64_t start[3],
+                                                       const uint64_t stop[3], oems_probe_term* out,
+                                                       uint64_t cap, uint64_t* n);
+/* EngineInterface::calc_current_integral (src/fdtd/engine_interface.rs:251-
+ * 305) between cell indices; mode F64. */
+OEMS_API oems_status oems_probe_current_integral_terms(const oems_operator* op, const uint64_t start[3],
+                                                       const uint64_t stop[3], int32_t normal,
+                                                       oems_probe_term* out, uint64_t cap, uint64_t* n);
+/* Lumped-port probes on the E edge (position, direction): kind 0 voltage
+ * V = -E . dl over the edge; kind 1 current I = loop integral of H around the
+ * edge (the curl of H that drives that E component, times the cell sides);
+ * mode F64. */
+OEMS_API oems_status oems_probe_port_terms(const oems_operator* op, const uint64_t position[3],
+                                           int32_t direction, int32_t kind, oems_probe_term* out,
+                                           uint64_t cap, uint64_t* n);
+
 /* ---- Simulation ---------------------------------------------------------- */
 
 /* EndCondition (src/fdtd/simulation.rs:36-43). */

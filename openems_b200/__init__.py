@@ -12,6 +12,8 @@ from .constants import C0, EPS0, MU0, Z0  # noqa: F401
 from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, MurAbcConfig, Operator,  # noqa: F401
                    Excitation, ExcitationType, ScheduledExcitation, TerminationConfig,
                    EnergyMonitorConfig, EngineBatch, TerminationReason, EnergySample, BatchResult,
-                   EngineType, Engine, EndCondition, SimulationStats, Simulation)
+                   EngineType, Engine, EndCondition, SimulationStats, Simulation,
+                   ProbeTerms, voltage_probe, current_probe, voltage_integral, current_integral,
+                   port_probe)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -119,6 +119,15 @@ class CpmlDescC(ctypes.Structure):
                 ("alpha_max", c_f64), ("kappa_max", c_f64)]
 
 
+class ProbeTermC(ctypes.Structure):
+    _fields_ = [("component", c_i32), ("reserved0", c_i32), ("position", c_u64 * 3),
+                ("weight", c_f64)]
+
+
+PROBE_SUM_F32 = 0
+PROBE_SUM_F64 = 1
+
+
 class MurDescC(ctypes.Structure):
     _fields_ = [("enabled", c_i32 * 6), ("order", c_i32), ("reserved0", c_i32),
                 ("phase_velocity", c_f64)]
@@ -149,7 +158,10 @@ SIGNATURES = {
     "oems_engine_add_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
     "oems_engine_add_mur": (c_i32, [P, ctypes.POINTER(MurDescC)]),
     "oems_engine_add_point_probe": (c_i32, [P, c_i32, c_u64 * 3, ctypes.POINTER(c_i32)]),
-    "oems_engine_read_probe_traces": (c_i32, [P, PF, c_u64, ctypes.POINTER(c_u64)]),
+    "oems_engine_read_probe_traces": (c_i32, [P, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_u64)]),
+    "oems_engine_add_probe": (c_i32, [P, ctypes.POINTER(ProbeTermC), c_u64, c_i32, ctypes.POINTER(c_i32)]),
+    "oems_engine_add_probe_dft": (c_i32, [P, c_i32, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_i32)]),
+    "oems_engine_read_probe_dft": (c_i32, [P, c_i32, ctypes.POINTER(c_f64)]),
     "oems_engine_energy": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_status_string": (ctypes.c_char_p, [c_i32]),
     "oems_last_error_message": (ctypes.c_char_p, []),
@@ -176,6 +188,16 @@ SIGNATURES = {
     "oems_excitation_dirac": (c_i32, [c_f64, c_u32, c_u64 * 3, ctypes.POINTER(ExcitationC)]),
     "oems_excitation_evaluate": (c_f64, [ctypes.POINTER(ExcitationC), c_f64]),
     "oems_excitation_sample": (c_i32, [ctypes.POINTER(ExcitationC), c_u64, c_u64, c_f64, PF]),
+    "oems_probe_voltage_terms": (c_i32, [c_u64 * 3, c_u64 * 3, c_i32, ctypes.POINTER(ProbeTermC), c_u64,
+                                         ctypes.POINTER(c_u64)]),
+    "oems_probe_current_terms": (c_i32, [c_u64 * 3, c_u64 * 3, c_i32, ctypes.POINTER(ProbeTermC), c_u64,
+                                         ctypes.POINTER(c_u64)]),
+    "oems_probe_voltage_integral_terms": (c_i32, [P, c_u64 * 3, c_u64 * 3, ctypes.POINTER(ProbeTermC), c_u64,
+                                                  ctypes.POINTER(c_u64)]),
+    "oems_probe_current_integral_terms": (c_i32, [P, c_u64 * 3, c_u64 * 3, c_i32, ctypes.POINTER(ProbeTermC),
+                                                  c_u64, ctypes.POINTER(c_u64)]),
+    "oems_probe_port_terms": (c_i32, [P, c_u64 * 3, c_i32, c_i32, ctypes.POINTER(ProbeTermC), c_u64,
+                                      ctypes.POINTER(c_u64)]),
     "oems_simulation_create": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(P)]),
     "oems_simulation_destroy": (None, [P]),
     "oems_simulation_add_excitation": (c_i32, [P, ctypes.POINTER(ExcitationC)]),

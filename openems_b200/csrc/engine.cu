@@ -64,7 +64,11 @@ static oems_status fail(oems_status st, const std::string& msg) {
 
 // Post-step work of one timestep: excitations (serially, in list order, so
 // duplicate positions behave like the reference's sequential loop,
-// basic_engine.rs:318-394), then point probes.
+// basic_engine.rs:318-394), then probes.  A probe is a list of terms
+// (component, cell, weight): mode 0 sums the values in order in f32 with
+// weights +-1 (VoltageProbe / CurrentProbe::sample, src/processing/probes.rs:
+// 98-239), mode 1 sums weight * value in f64 (EngineInterface integrals,
+// src/fdtd/engine_interface.rs:208-305).  Traces are f64.
 struct PostArgs {
   float* e[3];
   const float* h[3];
@@ -75,9 +79,12 @@ struct PostArgs {
   const long long* exc_count;  // number of samples
   const float* exc_samples;
   int nprobe;
-  const long long* probe_idx;
-  const int* probe_comp;
-  float* traces;               // [batch step][probe]
+  const int* probe_off;        // [nprobe + 1] term ranges
+  const int* probe_mode;
+  const long long* term_idx;
+  const int* term_comp;
+  const double* term_w;
+  double* traces;              // [batch step][probe]
   const long long* d_base;     // batch step of local step 0
   int local;
 };
@@ -95,10 +102,61 @@ __global__ void k_post_step(const PostArgs a) {
   }
   __syncthreads();
   for (int p = threadIdx.x; p < a.nprobe; p += blockDim.x) {
-    const int comp = a.probe_comp[p];
-    const float* f = comp < 3 ? a.e[comp] : a.h[comp - 3];
-    a.traces[s * a.nprobe + p] = f[a.probe_idx[p]];
+    double val;
+    if (a.probe_mode[p] == 0) {
+      float acc = 0.0f;
+      for (int t = a.probe_off[p]; t < a.probe_off[p + 1]; ++t) {
+        const int c = a.term_comp[t];
+        const float v = (c < 3 ? a.e[c] : a.h[c - 3])[a.term_idx[t]];
+        acc = a.term_w[t] >= 0.0 ? __fadd_rn(acc, v) : __fsub_rn(acc, v);
+      }
+      val = (double)acc;
+    } else {
+      double acc = 0.0;
+      for (int t = a.probe_off[p]; t < a.probe_off[p + 1]; ++t) {
+        const int c = a.term_comp[t];
+        const float v = (c < 3 ? a.e[c] : a.h[c - 3])[a.term_idx[t]];
+        acc = __dadd_rn(acc, __dmul_rn(a.term_w[t], (double)v));
+      }
+      val = acc;
+    }
+    a.traces[s * a.nprobe + p] = val;
   }
+}
+
+// Running DFT of probe traces over the steps of a batch
+// (src/processing/fields_fd.rs:149-217): X(f) += x(t) exp(-j 2 pi f t) 2 dt,
+// t = (t_after - half) dt.  One thread per (dft, frequency), steps in order.
+struct DftArgs {
+  int nentries;             // total (dft, frequency) pairs
+  const int* entry_probe;   // probe of each pair
+  const double* entry_freq;
+  const double* entry_half;
+  double* acc;              // [nentries][2]
+  const double* traces;
+  int nprobe;
+  long long steps;
+  long long t0;             // timestep before the batch
+  double dt;
+};
+
+__global__ void k_probe_dft(const DftArgs a) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.nentries) return;
+  const int p = a.entry_probe[e];
+  const double f = a.entry_freq[e];
+  const double scale = 2.0 * a.dt;
+  double re = a.acc[2 * e], im = a.acc[2 * e + 1];
+  for (long long s = 0; s < a.steps; ++s) {
+    const double x = a.traces[s * a.nprobe + p];
+    const double t = ((double)(a.t0 + s + 1) - a.entry_half[e]) * a.dt;
+    double sn, cs;
+    sincos(-2.0 * 3.14159265358979323846 * f * t, &sn, &cs);
+    re += x * (cs * scale);
+    im += x * (sn * scale);
+  }
+  a.acc[2 * e] = re;
+  a.acc[2 * e + 1] = im;
 }
 
 __global__ void k_set_i64(long long* p, long long v) { *p = v; }
@@ -225,13 +283,22 @@ struct oems_engine {
   oems::CpmlHost cpml;
   oems::MurHost mur;
 
-  // probes
-  std::vector<long long> probe_idx;
-  std::vector<int> probe_comp;
-  oems::DevBuf<long long> d_probe_idx;
-  oems::DevBuf<int> d_probe_comp;
-  oems::DevBuf<float> d_traces;
+  // probes: term tables (host copies and device mirrors) and f64 traces
+  std::vector<int> probe_off{0}, probe_mode, term_comp;
+  std::vector<long long> term_idx;
+  std::vector<double> term_w, probe_half;
+  oems::DevBuf<int> d_probe_off, d_probe_mode, d_term_comp;
+  oems::DevBuf<long long> d_term_idx;
+  oems::DevBuf<double> d_term_w;
+  oems::DevBuf<double> d_traces;
   uint64_t traces_steps = 0;
+  int nprobe() const { return (int)probe_mode.size(); }
+  // probe DFTs: one entry per (dft, frequency)
+  std::vector<int> dft_first, dft_count;  // entry range of each dft
+  std::vector<int> entry_probe;
+  std::vector<double> entry_freq, entry_half;
+  oems::DevBuf<int> d_entry_probe;
+  oems::DevBuf<double> d_entry_freq, d_entry_half, d_dft_acc;
 
   // excitations for the current batch
   oems::DevBuf<long long> d_exc_idx, d_exc_off, d_exc_count;
@@ -485,7 +552,7 @@ static cudaError_t launch_e(oems_engine* en) {
   return cudaGetLastError();
 }
 
-static bool need_post(const oems_engine* en) { return en->nexc > 0 || !en->probe_idx.empty(); }
+static bool need_post(const oems_engine* en) { return en->nexc > 0 || en->nprobe() > 0; }
 
 static cudaError_t launch_post(oems_engine* en, int local) {
   PostArgs a{};
@@ -499,9 +566,12 @@ static cudaError_t launch_post(oems_engine* en, int local) {
   a.exc_off = en->d_exc_off.p;
   a.exc_count = en->d_exc_count.p;
   a.exc_samples = en->d_exc_samples.p;
-  a.nprobe = (int)en->probe_idx.size();
-  a.probe_idx = en->d_probe_idx.p;
-  a.probe_comp = en->d_probe_comp.p;
+  a.nprobe = en->nprobe();
+  a.probe_off = en->d_probe_off.p;
+  a.probe_mode = en->d_probe_mode.p;
+  a.term_idx = en->d_term_idx.p;
+  a.term_comp = en->d_term_comp.p;
+  a.term_w = en->d_term_w.p;
   a.traces = en->d_traces.p;
   a.d_base = en->d_base.p;
   a.local = local;
@@ -982,7 +1052,7 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
   OEMS_TRY(upload_excitations(en, b));
   if (prev_nexc != en->nexc) en->graph_epoch++;  // nexc is baked into captured graphs
   const uint64_t steps = b->num_steps;
-  const int nprobe = (int)en->probe_idx.size();
+  const int nprobe = en->nprobe();
   if (nprobe > 0) {
     const size_t need = (size_t)std::max<uint64_t>(steps, 1) * nprobe;
     if (en->d_traces.n < need) {
@@ -1067,6 +1137,22 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
         }
       }
     }
+  }
+  if (!en->entry_probe.empty() && executed > 0) {
+    DftArgs da{};
+    da.nentries = (int)en->entry_probe.size();
+    da.entry_probe = en->d_entry_probe.p;
+    da.entry_freq = en->d_entry_freq.p;
+    da.entry_half = en->d_entry_half.p;
+    da.acc = en->d_dft_acc.p;
+    da.traces = en->d_traces.p;
+    da.nprobe = en->nprobe();
+    da.steps = (long long)executed;
+    da.t0 = (long long)t0;
+    da.dt = en->dt;
+    k_probe_dft<<<(da.nentries + 127) / 128, 128, 0, en->stream>>>(da);
+    OEMS_CUDA(cudaGetLastError());
+    en->last_launches += 1;
   }
   OEMS_CUDA(cudaEventRecord(en->ev1, en->stream));
   const size_t ns = sample_steps.size();
@@ -1336,8 +1422,12 @@ oems_status oems_engine_reset(oems_engine* engine) {
     OEMS_CUDA(cudaMemsetAsync(engine->cpml.psi.p, 0, engine->cpml.psi.n * sizeof(float), engine->stream));
   if (engine->mur.on)
     OEMS_CUDA(cudaMemsetAsync(engine->mur.state.p, 0, engine->mur.state.n * sizeof(float), engine->stream));
+  if (!engine->entry_probe.empty())
+    OEMS_CUDA(cudaMemsetAsync(engine->d_dft_acc.p, 0, 2 * engine->entry_probe.size() * sizeof(double),
+                              engine->stream));
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   engine->timestep = 0;
+  engine->traces_steps = 0;
   return OEMS_OK;
 }
 
@@ -1351,39 +1441,117 @@ oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc) 
   return add_mur(engine, desc);
 }
 
-oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component, const uint64_t position[3],
-                                        int32_t* probe_id) {
-  if (!engine || !position) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (component < 0 || component > 5) return fail(OEMS_ERR_CONFIG, "probe component must be 0..5");
-  if (position[0] >= (uint64_t)engine->nx || position[1] >= (uint64_t)engine->ny ||
-      position[2] >= (uint64_t)engine->nz)
-    return fail(OEMS_ERR_CONFIG, "probe position outside the grid");
+oems_status oems_engine_add_probe(oems_engine* engine, const oems_probe_term* terms, uint64_t nterms, int32_t mode,
+                                  int32_t* probe_id) {
+  // no terms is valid: the probe reads 0 (a VoltageProbe with an invalid
+  // direction, src/processing/probes.rs:125)
+  if (!engine || (!terms && nterms)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (mode != OEMS_PROBE_SUM_F32 && mode != OEMS_PROBE_SUM_F64) return fail(OEMS_ERR_CONFIG, "unknown probe mode");
+  if (engine->term_idx.size() + nterms > (size_t)INT32_MAX) return fail(OEMS_ERR_CONFIG, "too many probe terms");
+  bool all_h = nterms > 0;
+  for (uint64_t t = 0; t < nterms; ++t) {
+    const oems_probe_term& q = terms[t];
+    if (q.component < 0 || q.component > 5) return fail(OEMS_ERR_CONFIG, "probe component must be 0..5");
+    if (q.position[0] >= (uint64_t)engine->nx || q.position[1] >= (uint64_t)engine->ny ||
+        q.position[2] >= (uint64_t)engine->nz)
+      return fail(OEMS_ERR_CONFIG, "probe position outside the grid");
+    if (!std::isfinite(q.weight)) return fail(OEMS_ERR_CONFIG, "probe weight must be finite");
+    all_h = all_h && q.component >= 3;
+  }
   DeviceGuard guard(engine->device);
-  engine->probe_idx.push_back(((long long)position[0] * engine->ny + (long long)position[1]) * engine->g.nzp +
-                              (long long)position[2]);
-  engine->probe_comp.push_back(component);
-  const size_t np = engine->probe_idx.size();
-  OEMS_CUDA(engine->d_probe_idx.ensure(np + 16));
-  OEMS_CUDA(engine->d_probe_comp.ensure(np + 16));
-  OEMS_CUDA(cudaMemcpy(engine->d_probe_idx.p, engine->probe_idx.data(), np * sizeof(long long), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_probe_comp.p, engine->probe_comp.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  for (uint64_t t = 0; t < nterms; ++t) {
+    const oems_probe_term& q = terms[t];
+    engine->term_idx.push_back(((long long)q.position[0] * engine->ny + (long long)q.position[1]) * engine->g.nzp +
+                               (long long)q.position[2]);
+    engine->term_comp.push_back(q.component);
+    engine->term_w.push_back(q.weight);
+  }
+  engine->probe_off.push_back((int)engine->term_idx.size());
+  engine->probe_mode.push_back(mode);
+  engine->probe_half.push_back(all_h ? 0.5 : 0.0);
+  const size_t np = engine->probe_mode.size(), nt = engine->term_idx.size();
+  OEMS_CUDA(engine->d_probe_off.ensure(np + 1));
+  OEMS_CUDA(engine->d_probe_mode.ensure(np));
+  OEMS_CUDA(engine->d_term_idx.ensure(nt));
+  OEMS_CUDA(engine->d_term_comp.ensure(nt));
+  OEMS_CUDA(engine->d_term_w.ensure(nt));
+  OEMS_CUDA(cudaMemcpy(engine->d_probe_off.p, engine->probe_off.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_probe_mode.p, engine->probe_mode.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_term_idx.p, engine->term_idx.data(), nt * sizeof(long long), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_term_comp.p, engine->term_comp.data(), nt * sizeof(int), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_term_w.p, engine->term_w.data(), nt * sizeof(double), cudaMemcpyHostToDevice));
   engine->d_traces.ensure(0);
-  engine->graph_epoch++;
+  engine->traces_steps = 0;
+  engine->graph_epoch++;  // device table pointers and the probe count are baked into graphs
   if (probe_id) *probe_id = (int32_t)(np - 1);
   return OEMS_OK;
 }
 
-oems_status oems_engine_read_probe_traces(oems_engine* engine, float* out, uint64_t max_steps, uint64_t* steps_out) {
+oems_status oems_engine_add_point_probe(oems_engine* engine, int32_t component, const uint64_t position[3],
+                                        int32_t* probe_id) {
+  if (!position) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  oems_probe_term t{};
+  t.component = component;
+  for (int a = 0; a < 3; ++a) t.position[a] = position[a];
+  t.weight = 1.0;
+  return oems_engine_add_probe(engine, &t, 1, OEMS_PROBE_SUM_F32, probe_id);
+}
+
+oems_status oems_engine_read_probe_traces(oems_engine* engine, double* out, uint64_t max_steps, uint64_t* steps_out) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   const uint64_t steps = std::min<uint64_t>(engine->traces_steps, max_steps);
   if (steps_out) *steps_out = engine->traces_steps;
-  const size_t np = engine->probe_idx.size();
+  const size_t np = engine->nprobe();
   if (steps == 0 || np == 0) return OEMS_OK;
   if (!out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL output buffer");
   DeviceGuard guard(engine->device);
-  OEMS_CUDA(cudaMemcpy(out, engine->d_traces.p, steps * np * sizeof(float), cudaMemcpyDeviceToHost));
+  OEMS_CUDA(cudaMemcpy(out, engine->d_traces.p, steps * np * sizeof(double), cudaMemcpyDeviceToHost));
   return OEMS_OK;
 }
+
+oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t probe_id, const double* freqs, uint64_t nfreq,
+                                      int32_t* dft_id) {
+  if (!engine || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (probe_id < 0 || probe_id >= engine->nprobe()) return fail(OEMS_ERR_CONFIG, "unknown probe");
+  if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "a DFT needs at least one frequency");
+  DeviceGuard guard(engine->device);
+  engine->dft_first.push_back((int)engine->entry_probe.size());
+  engine->dft_count.push_back((int)nfreq);
+  for (uint64_t f = 0; f < nfreq; ++f) {
+    engine->entry_probe.push_back(probe_id);
+    engine->entry_freq.push_back(freqs[f]);
+    engine->entry_half.push_back(engine->probe_half[probe_id]);
+  }
+  const size_t ne = engine->entry_probe.size();
+  // keep the accumulated values of existing DFTs
+  std::vector<double> acc(2 * ne, 0.0);
+  const size_t old = ne - nfreq;
+  if (old) OEMS_CUDA(cudaMemcpy(acc.data(), engine->d_dft_acc.p, 2 * old * sizeof(double), cudaMemcpyDeviceToHost));
+  OEMS_CUDA(engine->d_entry_probe.ensure(ne));
+  OEMS_CUDA(engine->d_entry_freq.ensure(ne));
+  OEMS_CUDA(engine->d_entry_half.ensure(ne));
+  if (engine->d_dft_acc.n < 2 * ne) {
+    engine->d_dft_acc.ensure(0);
+    OEMS_CUDA(cudaMalloc(&engine->d_dft_acc.p, 2 * ne * sizeof(double)));
+    engine->d_dft_acc.n = 2 * ne;
+  }
+  OEMS_CUDA(cudaMemcpy(engine->d_entry_probe.p, engine->entry_probe.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_entry_freq.p, engine->entry_freq.data(), ne * sizeof(double), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_entry_half.p, engine->entry_half.data(), ne * sizeof(double), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(engine->d_dft_acc.p, acc.data(), 2 * ne * sizeof(double), cudaMemcpyHostToDevice));
+  if (dft_id) *dft_id = (int32_t)engine->dft_first.size() - 1;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_probe_dft(oems_engine* engine, int32_t dft_id, double* out) {
+  if (!engine || !out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (dft_id < 0 || dft_id >= (int32_t)engine->dft_first.size()) return fail(OEMS_ERR_CONFIG, "unknown DFT");
+  DeviceGuard guard(engine->device);
+  OEMS_CUDA(cudaMemcpy(out, engine->d_dft_acc.p + 2 * engine->dft_first[dft_id],
+                       2 * engine->dft_count[dft_id] * sizeof(double), cudaMemcpyDeviceToHost));
+  return OEMS_OK;
+}
+
 
 oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_energy) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");

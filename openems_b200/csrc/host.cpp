@@ -323,6 +323,164 @@ oems_status oems_excitation_sample(const oems_excitation* exc, uint64_t start, u
   return OEMS_OK;
 }
 
+// ---- probe term builders ----------------------------------------------------
+
+namespace {
+
+struct TermList {
+  oems_probe_term* out;
+  uint64_t cap, n = 0;
+  void add(int comp, uint64_t i, uint64_t j, uint64_t k, double w) {
+    if (n < cap) {
+      oems_probe_term& t = out[n];
+      t = oems_probe_term{};
+      t.component = comp;
+      t.position[0] = i;
+      t.position[1] = j;
+      t.position[2] = k;
+      t.weight = w;
+    }
+    ++n;
+  }
+};
+
+// Grid::delta_x/y/z (src/geometry/mod.rs:281-313)
+double grid_delta(const oems_operator* op, int a, uint64_t i) {
+  const auto& l = op->grid.lines[a];
+  if (i + 1 < l.size()) return (l[i + 1] - l[i]) * op->grid.unit;
+  if (i > 0) return (l[i] - l[i - 1]) * op->grid.unit;
+  return op->grid.unit;
+}
+
+oems_status finish(TermList& L, uint64_t* n) {
+  if (n) *n = L.n;
+  return OEMS_OK;
+}
+
+}  // namespace
+
+oems_status oems_probe_voltage_terms(const uint64_t s[3], const uint64_t e[3], int32_t dir, oems_probe_term* out,
+                                     uint64_t cap, uint64_t* n) {
+  if (!s || !e || (!out && cap)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  TermList L{out, cap};
+  // src/processing/probes.rs:107-127: inclusive ranges, value 0 for other directions
+  if (dir == 0)
+    for (uint64_t i = s[0]; i <= e[0]; ++i) L.add(0, i, s[1], s[2], 1.0);
+  else if (dir == 1)
+    for (uint64_t j = s[1]; j <= e[1]; ++j) L.add(1, s[0], j, s[2], 1.0);
+  else if (dir == 2)
+    for (uint64_t k = s[2]; k <= e[2]; ++k) L.add(2, s[0], s[1], k, 1.0);
+  return finish(L, n);
+}
+
+oems_status oems_probe_current_terms(const uint64_t s[3], const uint64_t e[3], int32_t normal, oems_probe_term* out,
+                                     uint64_t cap, uint64_t* n) {
+  if (!s || !e || (!out && cap)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  TermList L{out, cap};
+  // src/processing/probes.rs:204-236: current += H_a; current -= H_b, in loop order
+  if (normal == 0) {
+    for (uint64_t j = s[1]; j <= e[1]; ++j)
+      for (uint64_t k = s[2]; k <= e[2]; ++k) {
+        L.add(4, s[0], j, k, 1.0);
+        L.add(5, s[0], j, k, -1.0);
+      }
+  } else if (normal == 1) {
+    for (uint64_t i = s[0]; i <= e[0]; ++i)
+      for (uint64_t k = s[2]; k <= e[2]; ++k) {
+        L.add(5, i, s[1], k, 1.0);
+        L.add(3, i, s[1], k, -1.0);
+      }
+  } else if (normal == 2) {
+    for (uint64_t i = s[0]; i <= e[0]; ++i)
+      for (uint64_t j = s[1]; j <= e[1]; ++j) {
+        L.add(3, i, j, s[2], 1.0);
+        L.add(4, i, j, s[2], -1.0);
+      }
+  }
+  return finish(L, n);
+}
+
+oems_status oems_probe_voltage_integral_terms(const oems_operator* op, const uint64_t s[3], const uint64_t t[3],
+                                              oems_probe_term* out, uint64_t cap, uint64_t* n) {
+  if (!op || !s || !t || (!out && cap)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  TermList L{out, cap};
+  // src/fdtd/engine_interface.rs:208-247 (x at (j_start, k_start), y at
+  // (i_stop, k_start), z at (i_stop, j_stop); indices clamped to the grid)
+  for (uint64_t i = std::min(s[0], t[0]); i < std::max(s[0], t[0]); ++i) {
+    const uint64_t ic = std::min(i, op->n[0] - 1);
+    L.add(0, ic, s[1], s[2], -grid_delta(op, 0, ic));
+  }
+  for (uint64_t j = std::min(s[1], t[1]); j < std::max(s[1], t[1]); ++j) {
+    const uint64_t jc = std::min(j, op->n[1] - 1);
+    L.add(1, t[0], jc, s[2], -grid_delta(op, 1, jc));
+  }
+  for (uint64_t k = std::min(s[2], t[2]); k < std::max(s[2], t[2]); ++k) {
+    const uint64_t kc = std::min(k, op->n[2] - 1);
+    L.add(2, t[0], t[1], kc, -grid_delta(op, 2, kc));
+  }
+  return finish(L, n);
+}
+
+oems_status oems_probe_current_integral_terms(const oems_operator* op, const uint64_t s[3], const uint64_t t[3],
+                                              int32_t normal, oems_probe_term* out, uint64_t cap, uint64_t* n) {
+  if (!op || !s || !t || (!out && cap)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  TermList L{out, cap};
+  // src/fdtd/engine_interface.rs:251-305
+  const uint64_t a0 = std::min(s[0], t[0]), a1 = std::max(s[0], t[0]);
+  const uint64_t b0 = std::min(s[1], t[1]), b1 = std::max(s[1], t[1]);
+  const uint64_t c0 = std::min(s[2], t[2]), c1 = std::max(s[2], t[2]);
+  if (normal == 0) {
+    for (uint64_t j = b0; j < b1; ++j)
+      for (uint64_t k = c0; k < c1; ++k) {
+        const uint64_t jc = std::min(j, op->n[1] - 1), kc = std::min(k, op->n[2] - 1);
+        L.add(4, s[0], jc, kc, grid_delta(op, 2, kc));
+        L.add(5, s[0], jc, kc, -grid_delta(op, 1, jc));
+      }
+  } else if (normal == 1) {
+    for (uint64_t i = a0; i < a1; ++i)
+      for (uint64_t k = c0; k < c1; ++k) {
+        const uint64_t ic = std::min(i, op->n[0] - 1), kc = std::min(k, op->n[2] - 1);
+        L.add(5, ic, s[1], kc, grid_delta(op, 0, ic));
+        L.add(3, ic, s[1], kc, -grid_delta(op, 2, kc));
+      }
+  } else {
+    for (uint64_t i = a0; i < a1; ++i)
+      for (uint64_t j = b0; j < b1; ++j) {
+        const uint64_t ic = std::min(i, op->n[0] - 1), jc = std::min(j, op->n[1] - 1);
+        L.add(3, ic, jc, s[2], grid_delta(op, 1, jc));
+        L.add(4, ic, jc, s[2], -grid_delta(op, 0, ic));
+      }
+  }
+  return finish(L, n);
+}
+
+oems_status oems_probe_port_terms(const oems_operator* op, const uint64_t p[3], int32_t dir, int32_t kind,
+                                  oems_probe_term* out, uint64_t cap, uint64_t* n) {
+  if (!op || !p || (!out && cap)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (dir < 0 || dir > 2) return hfail(OEMS_ERR_CONFIG, "port direction must be 0, 1 or 2");
+  for (int a = 0; a < 3; ++a)
+    if (p[a] >= op->n[a]) return hfail(OEMS_ERR_CONFIG, "port position outside the grid");
+  TermList L{out, cap};
+  if (kind == 0) {
+    L.add(dir, p[0], p[1], p[2], -grid_delta(op, dir, p[dir]));
+    return finish(L, n);
+  }
+  // the curl of H driving E[dir] at p (the E update's curl, times cell sides)
+  const int a = (dir + 1) % 3, b = (dir + 2) % 3;  // H_b varies along a, H_a along b
+  if (p[a] == 0 || p[b] == 0) return hfail(OEMS_ERR_CONFIG, "port current needs a cell before the edge");
+  uint64_t m[3] = {p[0], p[1], p[2]};
+  // + (H_b(p) - H_b(p - e_a)) * d_b   - (H_a(p) - H_a(p - e_b)) * d_a
+  const double db = grid_delta(op, b, p[b]), da = grid_delta(op, a, p[a]);
+  L.add(3 + b, p[0], p[1], p[2], db);
+  m[a] -= 1;
+  L.add(3 + b, m[0], m[1], m[2], -db);
+  m[a] += 1;
+  L.add(3 + a, p[0], p[1], p[2], -da);
+  m[b] -= 1;
+  L.add(3 + a, m[0], m[1], m[2], da);
+  return finish(L, n);
+}
+
 oems_status oems_simulation_create(const oems_operator* op, int32_t device, uint32_t flags, oems_simulation** out) {
   if (!op || !out) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   std::unique_ptr<oems_simulation> s(new oems_simulation);

@@ -255,6 +255,59 @@ class Operator:
 # ---------------------------------------------------------------------------
 
 
+@dataclass
+class ProbeTerms:
+    """A probe's term list [(component, (i, j, k), weight)] and its mode:
+    0 = f32 ordered sum (VoltageProbe / CurrentProbe::sample), 1 = f64
+    weighted sum (EngineInterface integrals, port V / I)."""
+
+    terms: List[Tuple[int, Tuple[int, int, int], float]]
+    mode: int
+
+
+def _terms_from(fn, *args, mode):
+    n = N.c_u64()
+    N.check(fn(*args, None, 0, ctypes.byref(n)))
+    arr = (N.ProbeTermC * max(1, n.value))()
+    N.check(fn(*args, arr, n.value, ctypes.byref(n)))
+    return ProbeTerms([(arr[i].component, tuple(arr[i].position), arr[i].weight)
+                       for i in range(n.value)], mode)
+
+
+def _u3(v):
+    return (N.c_u64 * 3)(*[int(x) for x in v])
+
+
+def voltage_probe(start, end, direction) -> ProbeTerms:
+    """VoltageProbe (src/processing/probes.rs:63-131)."""
+    return _terms_from(N.lib().oems_probe_voltage_terms, _u3(start), _u3(end), direction,
+                       mode=N.PROBE_SUM_F32)
+
+
+def current_probe(start, end, normal_direction) -> ProbeTerms:
+    """CurrentProbe (src/processing/probes.rs:155-239)."""
+    return _terms_from(N.lib().oems_probe_current_terms, _u3(start), _u3(end), normal_direction,
+                       mode=N.PROBE_SUM_F32)
+
+
+def voltage_integral(op: "Operator", start, stop) -> ProbeTerms:
+    """EngineInterface::calc_voltage_integral between cell indices."""
+    return _terms_from(N.lib().oems_probe_voltage_integral_terms, op.handle, _u3(start), _u3(stop),
+                       mode=N.PROBE_SUM_F64)
+
+
+def current_integral(op: "Operator", start, stop, normal_dir) -> ProbeTerms:
+    """EngineInterface::calc_current_integral between cell indices."""
+    return _terms_from(N.lib().oems_probe_current_integral_terms, op.handle, _u3(start), _u3(stop),
+                       normal_dir, mode=N.PROBE_SUM_F64)
+
+
+def port_probe(op: "Operator", position, direction, kind) -> ProbeTerms:
+    """Lumped-port voltage (kind 0) or loop current (kind 1) at an E edge."""
+    return _terms_from(N.lib().oems_probe_port_terms, op.handle, _u3(position), direction, kind,
+                       mode=N.PROBE_SUM_F64)
+
+
 class ExcitationType(enum.IntEnum):
     Gaussian = 0
     Sinusoidal = 1
@@ -502,19 +555,53 @@ class Engine:
         N.check(N.lib().oems_engine_add_mur(self._h, ctypes.byref(d)))
 
     def add_point_probe(self, component: int, position) -> int:
+        """FieldProbe-style value of one component at one cell."""
         p = (N.c_u64 * 3)(*[int(v) for v in position])
         pid = N.c_i32()
         N.check(N.lib().oems_engine_add_point_probe(self._h, component, p, ctypes.byref(pid)))
         self.num_probes += 1
         return pid.value
 
+    def add_probe(self, terms: "ProbeTerms") -> int:
+        """General probe from a term list (see probe_* builders)."""
+        arr = (N.ProbeTermC * max(1, len(terms.terms)))()
+        for i, (c, pos, w) in enumerate(terms.terms):
+            arr[i].component = int(c)
+            for a in range(3):
+                arr[i].position[a] = int(pos[a])
+            arr[i].weight = float(w)
+        pid = N.c_i32()
+        N.check(N.lib().oems_engine_add_probe(self._h, arr, len(terms.terms), terms.mode,
+                                              ctypes.byref(pid)))
+        self.num_probes += 1
+        return pid.value
+
     def probe_traces(self) -> np.ndarray:
+        """Traces of the most recent batch, shape (steps, probes), float64."""
         steps = N.c_u64()
         N.check(N.lib().oems_engine_read_probe_traces(self._h, None, 0, ctypes.byref(steps)))
-        out = np.zeros((steps.value, self.num_probes), dtype=np.float32)
+        out = np.zeros((steps.value, self.num_probes), dtype=np.float64)
         if out.size:
-            N.check(N.lib().oems_engine_read_probe_traces(self._h, N.fptr(out), steps.value, None))
+            N.check(N.lib().oems_engine_read_probe_traces(
+                self._h, out.ctypes.data_as(ctypes.POINTER(N.c_f64)), steps.value, None))
         return out
+
+    def add_probe_dft(self, probe_id: int, freqs) -> int:
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        did = N.c_i32()
+        N.check(N.lib().oems_engine_add_probe_dft(self._h, probe_id,
+                                                  f.ctypes.data_as(ctypes.POINTER(N.c_f64)), len(f),
+                                                  ctypes.byref(did)))
+        self._dft_sizes = getattr(self, "_dft_sizes", {})
+        self._dft_sizes[did.value] = len(f)
+        return did.value
+
+    def probe_dft(self, dft_id: int) -> np.ndarray:
+        n = self._dft_sizes[dft_id]
+        out = np.zeros(2 * n, dtype=np.float64)
+        N.check(N.lib().oems_engine_read_probe_dft(self._h, dft_id,
+                                                   out.ctypes.data_as(ctypes.POINTER(N.c_f64))))
+        return out[0::2] + 1j * out[1::2]
 
     def run_batch(self, batch: EngineBatch) -> BatchResult:
         num_steps = batch.num_steps

@@ -78,6 +78,12 @@ def lib() -> ctypes.CDLL:
         L.orc_add_excitation_analytic.argtypes = [P, P, I32, I32, I32, P, D, U64, I64]
         L.orc_add_point_probe.argtypes = [P, I32, P]
         L.orc_get_probe_traces.argtypes = [P, P, I64]
+        L.orc_add_probe.restype = I32
+        L.orc_add_probe.argtypes = [P, P, P, P, I64, I32]
+        L.orc_add_probe_dft.restype = I32
+        L.orc_add_probe_dft.argtypes = [P, I32, P, I64]
+        L.orc_get_probe_dft.argtypes = [P, I32, P]
+        L.orc_eval_probes.argtypes = [P, P]
         L.orc_enable_cpml.restype = I32
         L.orc_enable_cpml.argtypes = [P, P, D, D, D, D]
         L.orc_cpml_profile.restype = I32
@@ -199,10 +205,35 @@ class OracleSim:
         lib().orc_add_point_probe(self._h, comp, _ptr(p))
         self.num_probes += 1
 
+    def add_probe(self, terms, mode):
+        """terms: [(component, (i, j, k), weight)]; mode 0 f32 ordered sum, 1 f64."""
+        c = np.ascontiguousarray([t[0] for t in terms] or [0], dtype=np.int32)
+        p = np.ascontiguousarray([list(t[1]) for t in terms] or [[0, 0, 0]], dtype=np.int64)
+        w = np.ascontiguousarray([t[2] for t in terms] or [0.0], dtype=np.float64)
+        pid = lib().orc_add_probe(self._h, _ptr(c), _ptr(p), _ptr(w), len(terms), mode)
+        self.num_probes += 1
+        return pid
+
     def probe_traces(self):
-        out = np.zeros((self._last_steps, self.num_probes), dtype=self.dtype)
+        out = np.zeros((self._last_steps, self.num_probes), dtype=np.float64)
         lib().orc_get_probe_traces(self._h, _ptr(out), self._last_steps)
         return out
+
+    def eval_probes(self):
+        out = np.zeros(max(1, self.num_probes))
+        lib().orc_eval_probes(self._h, _ptr(out))
+        return out[:self.num_probes]
+
+    def add_probe_dft(self, probe, freqs):
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        self._dft_sizes = getattr(self, "_dft_sizes", [])
+        self._dft_sizes.append(len(f))
+        return lib().orc_add_probe_dft(self._h, probe, _ptr(f), len(f))
+
+    def probe_dft(self, dft):
+        out = np.zeros(2 * self._dft_sizes[dft])
+        lib().orc_get_probe_dft(self._h, dft, _ptr(out))
+        return out[0::2] + 1j * out[1::2]
 
     def enable_cpml(self, layers=(8,) * 6, grading_order=3.0, reflection_coeff=1e-6,
                     alpha_max=0.0, kappa_max=1.0):

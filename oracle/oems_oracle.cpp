@@ -90,11 +90,21 @@ struct Sim {
   std::vector<Exc> excs;
 
   struct Probe {
-    int comp;
-    int64_t i, j, k;
+    std::vector<int> comp;
+    std::vector<int64_t> q;   // linear index per term
+    std::vector<double> w;    // weight per term
+    int mode;                 // 0: f32 sum with +-1, 1: f64 weighted sum
+    double half;              // time offset (0.5 for H-only probes)
   };
   std::vector<Probe> probes;
-  std::vector<T> traces;  // [step][probe]
+  std::vector<double> traces;  // [step][probe]
+
+  struct ProbeDft {
+    int probe;
+    std::vector<double> freqs;
+    std::vector<double> re, im;
+  };
+  std::vector<ProbeDft> dfts;
 
   std::vector<orc_energy_sample> energy;
 
@@ -381,10 +391,39 @@ struct Sim {
     }
   }
 
-  void record_probes() {
+  T field_value(int comp, int64_t q) const { return comp < 3 ? E[comp][q] : H[comp - 3][q]; }
+
+  // probe values after the step; DFT accumulation at t = (timestep - half) dt
+  // where `timestep` already counts this step (src/processing/fields_fd.rs:149-217)
+  void record_probes(uint64_t t_after) {
+    const size_t base = traces.size();
     for (const Probe& p : probes) {
-      int64_t q = idx(p.i, p.j, p.k);
-      traces.push_back(p.comp < 3 ? E[p.comp][q] : H[p.comp - 3][q]);
+      double val;
+      if (p.mode == 0) {
+        float acc = 0.0f;
+        for (size_t t = 0; t < p.q.size(); ++t) {
+          const float v = (float)field_value(p.comp[t], p.q[t]);
+          acc = p.w[t] >= 0.0 ? acc + v : acc - v;
+        }
+        val = (double)acc;
+      } else {
+        double acc = 0.0;
+        for (size_t t = 0; t < p.q.size(); ++t) acc += p.w[t] * (double)field_value(p.comp[t], p.q[t]);
+        val = acc;
+      }
+      traces.push_back(val);
+    }
+    for (ProbeDft& d : dfts) {
+      const double x = traces[base + d.probe];
+      const double t = ((double)t_after - probes[d.probe].half) * dt;
+      const double scale = 2.0 * dt;
+      for (size_t f = 0; f < d.freqs.size(); ++f) {
+        // factor = exp(-j 2 pi f t) * 2 dt, then acc += x * factor
+        const double ph = -2.0 * kPi * d.freqs[f] * t;
+        const double fr = std::cos(ph) * scale, fi = std::sin(ph) * scale;
+        d.re[f] += x * fr;
+        d.im[f] += x * fi;
+      }
     }
   }
 
@@ -540,7 +579,7 @@ struct Sim {
       update_e();
       if (!mur.empty()) mur_post_apply();
       apply_excitations(step);
-      record_probes();
+      record_probes(timestep + 1);
       timestep += 1;
       executed += 1;
       if (sample_interval > 0 && cur % sample_interval == 0) {
@@ -757,14 +796,71 @@ void orc_add_excitation_analytic(orc_sim* s, const int64_t* pos3, int32_t dir, i
 }
 
 void orc_add_point_probe(orc_sim* s, int32_t comp, const int64_t* pos3) {
-  DISPATCH(s, S->probes.push_back({comp, pos3[0], pos3[1], pos3[2]}));
+  const double w = 1.0;
+  orc_add_probe(s, &comp, pos3, &w, 1, 0);
 }
 
-void orc_get_probe_traces(const orc_sim* s, void* out, int64_t max_steps) {
+int32_t orc_add_probe(orc_sim* s, const int32_t* comps, const int64_t* pos, const double* weights, int64_t nterms,
+                      int32_t mode) {
+  int32_t id = -1;
   DISPATCH(s, {
-    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    typename std::remove_reference_t<decltype(*S)>::Probe p;
+    p.mode = mode;
+    bool all_h = nterms > 0;
+    for (int64_t t = 0; t < nterms; ++t) {
+      p.comp.push_back(comps[t]);
+      p.q.push_back(S->idx(pos[3 * t], pos[3 * t + 1], pos[3 * t + 2]));
+      p.w.push_back(weights[t]);
+      all_h = all_h && comps[t] >= 3;
+    }
+    p.half = all_h ? 0.5 : 0.0;
+    S->probes.push_back(p);
+    id = (int32_t)S->probes.size() - 1;
+  });
+  return id;
+}
+
+void orc_eval_probes(orc_sim* s, double* out) {
+  DISPATCH(s, {
+    const size_t base = S->traces.size();
+    auto saved = S->dfts;
+    S->dfts.clear();
+    S->record_probes(S->timestep);
+    S->dfts = saved;
+    for (size_t p = 0; p < S->probes.size(); ++p) out[p] = S->traces[base + p];
+    S->traces.resize(base);
+  });
+}
+
+void orc_get_probe_traces(const orc_sim* s, double* out, int64_t max_steps) {
+  DISPATCH(s, {
     int64_t cnt = std::min<int64_t>((int64_t)S->traces.size(), max_steps * (int64_t)S->probes.size());
-    std::memcpy(out, S->traces.data(), sizeof(T) * cnt);
+    std::memcpy(out, S->traces.data(), sizeof(double) * cnt);
+  });
+}
+
+int32_t orc_add_probe_dft(orc_sim* s, int32_t probe, const double* freqs, int64_t nfreq) {
+  int32_t id = -1;
+  DISPATCH(s, {
+    if (probe < 0 || probe >= (int32_t)S->probes.size()) return -1;
+    typename std::remove_reference_t<decltype(*S)>::ProbeDft d;
+    d.probe = probe;
+    d.freqs.assign(freqs, freqs + nfreq);
+    d.re.assign(nfreq, 0.0);
+    d.im.assign(nfreq, 0.0);
+    S->dfts.push_back(d);
+    id = (int32_t)S->dfts.size() - 1;
+  });
+  return id;
+}
+
+void orc_get_probe_dft(const orc_sim* s, int32_t dft, double* out) {
+  DISPATCH(s, {
+    const auto& d = S->dfts[dft];
+    for (size_t f = 0; f < d.freqs.size(); ++f) {
+      out[2 * f] = d.re[f];
+      out[2 * f + 1] = d.im[f];
+    }
   });
 }
 

@@ -111,10 +111,26 @@ void orc_add_excitation_analytic(orc_sim* s, const int64_t* pos3, int32_t dir, i
                                  int32_t kind, const double* params, double amplitude,
                                  uint64_t start_timestep, int64_t n);
 
-/* Point probes: comp 0..5 = Ex Ey Ez Hx Hy Hz. One value per executed step,
- * taken after the excitation. Traces are float / double per precision. */
+/* Probes: one value per executed step, taken after the excitation, recorded
+ * as double.  A point probe (comp 0..5 = Ex Ey Ez Hx Hy Hz) is a one-term
+ * probe.  General probes are term lists (comp, i, j, k, weight):
+ * mode 0 sums the values in order in f32 with weights +-1 (acc = acc + v or
+ * acc = acc - v), as VoltageProbe/CurrentProbe::sample do
+ * (src/processing/probes.rs:98-239); mode 1 sums weight*value in f64, as
+ * EngineInterface::calc_voltage/current_integral do
+ * (src/fdtd/engine_interface.rs:208-305). */
 void orc_add_point_probe(orc_sim* s, int32_t comp, const int64_t* pos3);
-void orc_get_probe_traces(const orc_sim* s, void* out, int64_t max_steps);
+int32_t orc_add_probe(orc_sim* s, const int32_t* comps, const int64_t* pos, const double* weights,
+                      int64_t nterms, int32_t mode);
+void orc_get_probe_traces(const orc_sim* s, double* out, int64_t max_steps);
+/* Evaluates every probe on the current fields (no step); out[probe]. */
+void orc_eval_probes(orc_sim* s, double* out);
+/* Running DFT of a probe trace (src/processing/fields_fd.rs:149-217):
+ * X(f) += x(t) exp(-j 2 pi f t) 2 dt with t = (timestep after the step
+ * - half) dt, half = 0.5 for probes of H components, 0 otherwise.
+ * Accumulates over every step run after the call.  out: re, im per frequency. */
+int32_t orc_add_probe_dft(orc_sim* s, int32_t probe, const double* freqs, int64_t nfreq);
+void orc_get_probe_dft(const orc_sim* s, int32_t dft, double* out);
 
 /* CPML on the faces with layers[f] > 0 (f = xmin,xmax,ymin,ymax,zmin,zmax).
  * Profile: src/extensions/cpml.rs:68-177; update: Roden-Gedney. */

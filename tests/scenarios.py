@@ -236,3 +236,14 @@ def mur_scenarios() -> List[Scenario]:
                  excitations=[E.gaussian_modulated(8e9, 0.5, 0, (9, 4, 7))], num_steps=200,
                  mur=oe.MurAbcConfig(enabled=(0, 1, 1, 0, 1, 1), order=2)),
     ]
+
+
+def probe_scenario() -> Scenario:
+    """Lossy box with CPML, two sources and every probe kind."""
+    E = oe.Excitation
+    return Scenario("probes", (21, 18, 24), 1e-3,
+                    materials=[(2.5, 1.0, 0.02, 0.0, (4, 16, 3, 15, 5, 19))],
+                    excitations=[E.gaussian_modulated(9e9, 0.5, 2, (10, 9, 12)),
+                                 E.gaussian_modulated(6e9, 0.4, 0, (12, 6, 15))],
+                    num_steps=260, cpml=oe.CpmlBoundaries(layers=(4, 4, 4, 4, 4, 4)),
+                    batches=(100, 160))

@@ -244,3 +244,54 @@ def test_energy_decay_end_condition_stops_simulation():
     st = sim.run()
     assert 100 < st.timesteps < 1_000_000
     assert st.final_energy < st.peak_energy * 1e-4
+
+
+def _all_probes(op):
+    return [oe.voltage_probe((3, 9, 12), (17, 9, 12), 0),
+            oe.voltage_probe((10, 9, 6), (10, 9, 18), 2),
+            oe.current_probe((10, 5, 8), (10, 12, 16), 0),
+            oe.current_probe((5, 9, 5), (15, 9, 18), 1),
+            oe.voltage_integral(op, (4, 5, 6), (14, 12, 18)),
+            oe.current_integral(op, (6, 4, 12), (14, 13, 12), 2),
+            oe.port_probe(op, (10, 9, 12), 2, 0),
+            oe.port_probe(op, (10, 9, 12), 2, 1),
+            oe.port_probe(op, (12, 6, 15), 0, 1)]
+
+
+@pytest.mark.parametrize("kernels", KERNELS)
+def test_probes_and_dft_match_oracle(kernels):
+    """f32 probe sums and f64 integrals bit-exact; DFT to 1e-12 (sincos)."""
+    from scenarios import probe_scenario, make_operator
+    import oracle
+    sc = probe_scenario()
+    freqs = np.linspace(1e9, 12e9, 23)
+    op = make_operator(sc)
+    eng = oe.Engine(op, kernels=kernels)
+    eng.add_cpml(sc.cpml)
+    probes = _all_probes(op)
+    pids = [eng.add_probe(p) for p in probes]
+    dfts = [eng.add_probe_dft(p, freqs) for p in pids]
+    lines = [oracle.uniform_lines(n, sc.delta) for n in sc.dims]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*sc.dims, dt, delta)
+    for m in sc.materials:
+        s.set_material(*m)
+    s.enable_cpml(sc.cpml.layers)
+    opids = [s.add_probe(p.terms, p.mode) for p in probes]
+    odfts = [s.add_probe_dft(p, freqs) for p in opids]
+    start = 0
+    for n in sc.batch_sizes():
+        sched = [oe.ScheduledExcitation.from_excitation(x, start, n, dt) for x in sc.excitations]
+        eng.run_batch(oe.EngineBatch(num_steps=n, excitations=sched))
+        s.clear_excitations()
+        for x in sc.excitations:
+            s.add_excitation_analytic(x.position, x.direction, True, int(x.excitation_type),
+                                      list(x.params), 1.0, start, n)
+        s.run_batch(n)
+        got, ref = eng.probe_traces(), s.probe_traces()
+        assert got.shape == ref.shape == (n, len(probes))
+        assert np.array_equal(got, ref)
+        start += n
+    for d, od in zip(dfts, odfts):
+        g, r = eng.probe_dft(d), s.probe_dft(od)
+        assert np.abs(g - r).max() <= 1e-12 * np.abs(r).max() + 1e-300

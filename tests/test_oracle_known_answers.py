@@ -172,3 +172,56 @@ def test_cpml_regions_count():
     s2 = oracle.OracleSim(6, 50, 50, 1e-12, d3)
     s2.enable_cpml((6, 6, 8, 8, 8, 8))
     assert [len(s2.cpml_profile(f)["b_e"]) for f in range(6)] == [0, 0, 8, 8, 8, 8]
+
+
+# ---- src/processing/probes.rs:388-503 (probe sums, via the C++ term builders) --
+
+def _probe_value(terms, fields_fn, dims=(10, 10, 10)):
+    lines = oracle.uniform_lines(dims[0], 1e-3)
+    dt, d3 = oracle.grid_timestep(lines, lines, lines)
+    s = oracle.OracleSim(*dims, dt, d3)
+    f = np.zeros((6,) + dims, np.float32)
+    fields_fn(f)
+    s.set_fields(f)
+    s.add_probe(terms.terms, terms.mode)
+    return s.eval_probes()[0]
+
+
+def test_voltage_probe_sums():
+    import openems_b200 as oe
+    assert abs(_probe_value(oe.voltage_probe((0, 5, 5), (9, 5, 5), 0),
+                            lambda f: f[0].fill(2.0)) - 20.0) < 1e-6
+    assert abs(_probe_value(oe.voltage_probe((5, 0, 5), (5, 9, 5), 1),
+                            lambda f: f[1].fill(3.0)) - 30.0) < 1e-6
+    for val, want in ((1.0, 5.0), (2.0, 10.0), (0.5, 2.5)):
+        assert abs(_probe_value(oe.voltage_probe((5, 5, 0), (5, 5, 4), 2),
+                                lambda f, v=val: f[2].fill(v)) - want) < 1e-6
+
+    def single(f):
+        f[2, 5, 5, 5] = 2.5
+    assert abs(_probe_value(oe.voltage_probe((5, 5, 5), (5, 5, 5), 2), single) - 2.5) < 1e-5
+
+
+def test_current_probe_sums():
+    import openems_b200 as oe
+
+    def yfill(f):
+        f[5].fill(1.0)
+        f[3].fill(0.5)
+    assert abs(_probe_value(oe.current_probe((0, 5, 0), (9, 5, 9), 1), yfill) - 50.0) < 1e-5
+
+    def zfill(f):
+        f[3].fill(2.0)
+        f[4].fill(1.0)
+    assert abs(_probe_value(oe.current_probe((0, 0, 5), (9, 9, 5), 2), zfill) - 100.0) < 1e-5
+    t = oe.current_probe((5, 0, 0), (5, 4, 4), 10)
+    assert t.terms == [] and abs(_probe_value(t, lambda f: f[4].fill(1.0))) < 1e-10
+
+
+def test_voltage_integral_weights_and_sign():
+    """V = -sum E . dl (src/fdtd/engine_interface.rs:206-247)."""
+    import openems_b200 as oe
+    op = oe.Operator(oe.Grid.uniform(10, 10, 10, 1e-3), oe.BoundaryConditions.all_pec())
+    t = oe.voltage_integral(op, (2, 3, 4), (2, 3, 9))
+    assert len(t.terms) == 5 and all(c == 2 and abs(w + 1e-3) < 1e-15 for c, _, w in t.terms)
+    assert abs(_probe_value(t, lambda f: f[2].fill(4.0)) - (-5 * 4.0 * 1e-3)) < 1e-15
