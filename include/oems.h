@@ -175,6 +175,33 @@ typedef struct oems_mur_desc {
   double phase_velocity; /* <= 0: c0 */
 } oems_mur_desc;
 
+/* Dispersive material on a list of cells (src/extensions/dispersive.rs),
+ * applied after the E update to all three components of every cell:
+ *   kind 0 Drude    params (omega_p, gamma)            :476-535
+ *   kind 1 Lorentz  params (omega_0, gamma, delta_eps) :134-196, as the
+ *          reference (first order in J; unstable for usual parameters)
+ *   kind 2 Debye    params (tau, delta_eps)             :570-630
+ *   kind 3 Lorentz, second order: P' = a P + b P_prev + c E,
+ *          E -= (P' - P) / (eps0 eps_inf)  (no counterpart in the reference)
+ * Angular frequencies in rad/s.  eps_inf divides the E correction; 1 gives
+ * the reference's coefficients. */
+typedef struct oems_dispersive_desc {
+  int32_t kind;
+  int32_t reserved0;
+  double params[3];
+  double eps_inf;
+} oems_dispersive_desc;
+
+/* RlcElement (src/extensions/lumped_rlc.rs:20-112); type 0 parallel, 1
+ * series; resistance / inductance / capacitance <= 0 mean absent.  Applied
+ * after the E update as LumpedRlc::post_update_e (:263-286). */
+typedef struct oems_lumped_rlc_desc {
+  uint64_t position[3];
+  uint32_t direction;
+  int32_t type;
+  double resistance, inductance, capacitance;
+} oems_lumped_rlc_desc;
+
 /* Field components for probes: 0..2 = Ex Ey Ez, 3..5 = Hx Hy Hz. */
 #define OEMS_COMPONENT_EX 0
 #define OEMS_COMPONENT_HX 3
@@ -201,6 +228,15 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);
 /* MurAbc::new (src/extensions/mur_abc.rs:175). */
 OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc);
+/* LorentzMaterial / DrudeMaterial / DebyeMaterial::new (src/extensions/
+ * dispersive.rs:134, 476, 570); cells: ncells x (i, j, k). Materials apply in
+ * the order they are added. */
+OEMS_API oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersive_desc* desc,
+                                                const uint64_t* cells, uint64_t ncells);
+/* LumpedRlc::new (src/extensions/lumped_rlc.rs:145-160).  Elements apply in
+ * list order; adding elements restarts every element's integrator at 0. */
+OEMS_API oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rlc_desc* elements,
+                                                uint64_t n);
 
 /* ---- probes ---------------------------------------------------------------- */
 

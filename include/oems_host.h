@@ -51,6 +51,18 @@ OEMS_API oems_status oems_operator_info(const oems_operator* op, uint64_t dims[3
 /* Borrowed pointers to the 12 coefficient arrays (ca0 ca1 ca2 cb0 cb1 cb2 da0
  * da1 da2 db0 db1 db2), valid until the operator is modified or destroyed. */
 OEMS_API oems_status oems_operator_coefficients(const oems_operator* op, const float* out[12]);
+/* Lumped resistor R and/or capacitor C across the E edge (position,
+ * direction), folded into that edge's Ca/Cb (no counterpart in the
+ * reference, whose LumpedRlc leaves a series resistor without effect):
+ * eps = eps_r eps0 + C dl / A, sigma = sigma + dl / (R A) with dl the edge
+ * length and A the cell face normal to it; R or C <= 0 means absent.
+ * *source_scale (may be NULL) receives the factor that turns a voltage
+ * source in series with R into the soft-source sample added to that E
+ * component: dt / (eps (1 + sigma dt / 2 eps) R A). */
+OEMS_API oems_status oems_operator_set_lumped(oems_operator* op, const uint64_t position[3],
+                                              int32_t direction, double resistance,
+                                              double capacitance, double eps_r, double sigma,
+                                              double* source_scale);
 /* Fills an engine descriptor that borrows the operator's arrays. */
 OEMS_API oems_status oems_operator_engine_desc(const oems_operator* op, int32_t device, uint32_t flags,
                                       oems_operator_desc* out);

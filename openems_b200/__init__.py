@@ -14,6 +14,7 @@ from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, 
                    EnergyMonitorConfig, EngineBatch, TerminationReason, EnergySample, BatchResult,
                    EngineType, Engine, EndCondition, SimulationStats, Simulation,
                    ProbeTerms, voltage_probe, current_probe, voltage_integral, current_integral,
-                   port_probe)
+                   port_probe, LumpedPort, DrudeMaterial, LorentzMaterial, DebyeMaterial,
+                   RlcType, RlcElement)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -133,6 +133,15 @@ class MurDescC(ctypes.Structure):
                 ("phase_velocity", c_f64)]
 
 
+class DispersiveDescC(ctypes.Structure):
+    _fields_ = [("kind", c_i32), ("reserved0", c_i32), ("params", c_f64 * 3), ("eps_inf", c_f64)]
+
+
+class LumpedRlcDescC(ctypes.Structure):
+    _fields_ = [("position", c_u64 * 3), ("direction", c_u32), ("type", c_i32),
+                ("resistance", c_f64), ("inductance", c_f64), ("capacitance", c_f64)]
+
+
 class ExcitationC(ctypes.Structure):
     _fields_ = [("kind", c_i32), ("direction", c_u32), ("position", c_u64 * 3),
                 ("params", c_f64 * 3), ("amplitude", c_f64), ("soft_source", c_i32),
@@ -157,6 +166,8 @@ SIGNATURES = {
     "oems_engine_reset": (c_i32, [P]),
     "oems_engine_add_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
     "oems_engine_add_mur": (c_i32, [P, ctypes.POINTER(MurDescC)]),
+    "oems_engine_add_dispersive": (c_i32, [P, ctypes.POINTER(DispersiveDescC), P, c_u64]),
+    "oems_engine_add_lumped_rlc": (c_i32, [P, ctypes.POINTER(LumpedRlcDescC), c_u64]),
     "oems_engine_add_point_probe": (c_i32, [P, c_i32, c_u64 * 3, ctypes.POINTER(c_i32)]),
     "oems_engine_read_probe_traces": (c_i32, [P, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_u64)]),
     "oems_engine_add_probe": (c_i32, [P, ctypes.POINTER(ProbeTermC), c_u64, c_i32, ctypes.POINTER(c_i32)]),
@@ -180,6 +191,8 @@ SIGNATURES = {
     "oems_operator_set_pec": (c_i32, [P, c_u64 * 6]),
     "oems_operator_info": (c_i32, [P, c_u64 * 3, ctypes.POINTER(c_f64), c_f64 * 3]),
     "oems_operator_coefficients": (c_i32, [P, PF * 12]),
+    "oems_operator_set_lumped": (c_i32, [P, c_u64 * 3, c_i32, c_f64, c_f64, c_f64, c_f64,
+                                         ctypes.POINTER(c_f64)]),
     "oems_operator_engine_desc": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(OperatorDesc)]),
     "oems_excitation_gaussian": (c_i32, [c_f64, c_f64, c_u32, c_u64 * 3, ctypes.POINTER(ExcitationC)]),
     "oems_excitation_gaussian_modulated": (c_i32, [c_f64, c_f64, c_u32, c_u64 * 3,

@@ -30,6 +30,7 @@
 #include "yee_kernels.cuh"
 #include "yee_tma.cuh"
 #include "mur.cuh"
+#include "lumped_ade.cuh"
 
 namespace oems {
 
@@ -259,6 +260,21 @@ struct MurHost {
   DevBuf<float> state;  // v, ob, os: 3 x 2 x total
 };
 
+struct DispHost {
+  DispArgs args{};
+  std::unique_ptr<DevBuf<long long>> q{new DevBuf<long long>};
+  std::unique_ptr<DevBuf<float>> state{new DevBuf<float>};  // st then pp
+};
+
+struct RlcHost {
+  std::vector<long long> q;
+  std::vector<int> dir;
+  std::vector<float> v_vv, v_il;
+  DevBuf<long long> d_q;
+  DevBuf<int> d_dir;
+  DevBuf<float> d_vv, d_vil, d_int;
+};
+
 }  // namespace oems
 
 struct oems_engine {
@@ -282,6 +298,8 @@ struct oems_engine {
 
   oems::CpmlHost cpml;
   oems::MurHost mur;
+  std::vector<oems::DispHost> disp;
+  oems::RlcHost rlc;
 
   // probes: term tables (host copies and device mirrors) and f64 traces
   std::vector<int> probe_off{0}, probe_mode, term_comp;
@@ -597,13 +615,27 @@ static cudaError_t launch_post_e(oems_engine* en) {
     const int b = blocks_for(en->mur.args.total, 256);
     k_mur_post<<<b, 256, 0, en->stream>>>(en->mur.args);
     k_mur_apply<<<b, 256, 0, en->stream>>>(en->mur.args);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  // materials one launch each, in the order they were added
+  for (const DispHost& d : en->disp) k_dispersive<<<blocks_for(d.args.n, 256), 256, 0, en->stream>>>(d.args);
+  if (!en->rlc.q.empty()) {
+    RlcArgs r{};
+    r.n = (int)en->rlc.q.size();
+    r.q = en->rlc.d_q.p;
+    r.dir = en->rlc.d_dir.p;
+    r.v_vv = en->rlc.d_vv.p;
+    r.v_il = en->rlc.d_vil.p;
+    r.i_int = en->rlc.d_int.p;
+    r.dtf = (float)en->dt;
+    for (int c = 0; c < 3; ++c) r.e[c] = en->E(c);
+    k_lumped_rlc<<<1, 32, 0, en->stream>>>(r);
+  }
+  return cudaGetLastError();
 }
 
-static int ext_kernels(const oems_engine* en) { return en->mur.on ? 3 : 0; }
+static int ext_kernels(const oems_engine* en) {
+  return (en->mur.on ? 3 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
+}
 
 static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + (need_post(en) ? 1 : 0); }
 
@@ -1425,6 +1457,10 @@ oems_status oems_engine_reset(oems_engine* engine) {
   if (!engine->entry_probe.empty())
     OEMS_CUDA(cudaMemsetAsync(engine->d_dft_acc.p, 0, 2 * engine->entry_probe.size() * sizeof(double),
                               engine->stream));
+  for (auto& d : engine->disp)
+    OEMS_CUDA(cudaMemsetAsync(d.state->p, 0, d.state->n * sizeof(float), engine->stream));
+  if (!engine->rlc.q.empty())
+    OEMS_CUDA(cudaMemsetAsync(engine->rlc.d_int.p, 0, engine->rlc.q.size() * sizeof(float), engine->stream));
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   engine->timestep = 0;
   engine->traces_steps = 0;
@@ -1434,6 +1470,110 @@ oems_status oems_engine_reset(oems_engine* engine) {
 oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   return add_cpml(engine, desc);
+}
+
+oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersive_desc* d, const uint64_t* cells,
+                                       uint64_t ncells) {
+  if (!engine || !d || (!cells && ncells)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (d->kind < 0 || d->kind > 3) return fail(OEMS_ERR_MATERIAL, "unknown dispersive material kind");
+  if (!(d->eps_inf > 0.0)) return fail(OEMS_ERR_MATERIAL, "eps_inf must be positive");
+  if (ncells == 0) return fail(OEMS_ERR_MATERIAL, "a dispersive material needs at least one cell");
+  DeviceGuard guard(engine->device);
+  DispHost h;
+  DispArgs& A = h.args;
+  A.kind = d->kind;
+  const double dt = engine->dt, kEps0 = 8.854187817e-12;
+  const double* p = d->params;
+  if (d->kind == 0) {  // DrudeMaterial::new (src/extensions/dispersive.rs:476-498)
+    const double den = 1.0 + p[1] * dt / 2.0;
+    A.a = (float)((1.0 - p[1] * dt / 2.0) / den);
+    A.b = (float)(kEps0 * p[0] * p[0] * dt / den);
+    A.c = (float)(dt / (kEps0 * d->eps_inf));
+  } else if (d->kind == 1 || d->kind == 3) {  // LorentzMaterial::new (:134-159)
+    const double den = 1.0 + p[1] * dt / 2.0;
+    A.a = (float)((2.0 - p[0] * p[0] * dt * dt) / den);
+    A.b = (float)((p[1] * dt / 2.0 - 1.0) / den);
+    A.c = (float)(kEps0 * p[2] * p[0] * p[0] * dt * dt / den);
+    A.c2 = (float)(1.0 / (kEps0 * d->eps_inf));
+  } else {  // DebyeMaterial::new (:570-592)
+    const double den = 2.0 * p[0] + dt;
+    A.a = (float)((2.0 * p[0] - dt) / den);
+    A.b = (float)(2.0 * kEps0 * p[1] * dt / den);
+    A.c = (float)(dt / (kEps0 * d->eps_inf));
+  }
+  A.dtf = (float)dt;
+  std::vector<long long> q(ncells);
+  for (uint64_t m = 0; m < ncells; ++m) {
+    const uint64_t* c = cells + 3 * m;
+    if (c[0] >= (uint64_t)engine->nx || c[1] >= (uint64_t)engine->ny || c[2] >= (uint64_t)engine->nz)
+      return fail(OEMS_ERR_MATERIAL, "dispersive cell outside the grid");
+    q[m] = ((long long)c[0] * engine->ny + (long long)c[1]) * engine->g.nzp + (long long)c[2];
+  }
+  OEMS_CUDA(h.q->ensure(ncells));
+  OEMS_CUDA(h.state->ensure(6 * ncells));
+  OEMS_CUDA(cudaMemcpy(h.q->p, q.data(), ncells * sizeof(long long), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemset(h.state->p, 0, 6 * ncells * sizeof(float)));
+  A.n = (long long)ncells;
+  A.q = h.q->p;
+  A.st = h.state->p;
+  A.pp = h.state->p + 3 * ncells;
+  for (int c = 0; c < 3; ++c) A.e[c] = engine->E(c);
+  engine->disp.push_back(std::move(h));
+  engine->graph_epoch++;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rlc_desc* elems, uint64_t n) {
+  if (!engine || (!elems && n)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  DeviceGuard guard(engine->device);
+  RlcHost& R = engine->rlc;
+  const double dt = engine->dt, kEps0 = 8.854187817e-12;
+  for (uint64_t m = 0; m < n; ++m) {  // validate the whole list before taking any of it
+    const oems_lumped_rlc_desc& e = elems[m];
+    if (e.direction > 2) return fail(OEMS_ERR_CONFIG, "lumped element direction must be 0, 1 or 2");
+    if (e.position[0] >= (uint64_t)engine->nx || e.position[1] >= (uint64_t)engine->ny ||
+        e.position[2] >= (uint64_t)engine->nz)
+      return fail(OEMS_ERR_CONFIG, "lumped element outside the grid");
+  }
+  for (uint64_t m = 0; m < n; ++m) {
+    const oems_lumped_rlc_desc& e = elems[m];
+    const double dl = engine->delta[e.direction], da = dl * dl;
+    double v_vv, v_il;
+    if (e.type == 0) {  // calc_parallel_coeffs (src/extensions/lumped_rlc.rs:190-216)
+      const double g = e.resistance > 0 ? 1.0 / e.resistance : 0.0;
+      const double inv_l = e.inductance > 0 ? dt / e.inductance : 0.0;
+      const double cc = e.capacitance > 0 ? e.capacitance : 0.0;
+      const double g_eff = g * dl / da, c_eff = cc * dl / da + kEps0 * dl / da;
+      const double den = 2.0 * c_eff + g_eff * dt;
+      v_vv = (2.0 * c_eff - g_eff * dt) / den;
+      v_il = inv_l * dl / da;
+    } else {  // calc_series_coeffs (:219-250): v_vv = 1 always
+      const double rr = e.resistance > 0 ? e.resistance : 0.0, ll = e.inductance > 0 ? e.inductance : 0.0;
+      const double inv_c = e.capacitance > 0 ? dt / e.capacitance : 0.0;
+      const double den = 2.0 * (ll * da / dl) + (rr * da / dl) * dt;
+      v_vv = 1.0;
+      v_il = std::fabs(den) < 1e-20 ? 0.0 : inv_c * da / dl;
+    }
+    R.q.push_back(((long long)e.position[0] * engine->ny + (long long)e.position[1]) * engine->g.nzp +
+                  (long long)e.position[2]);
+    R.dir.push_back((int)e.direction);
+    R.v_vv.push_back((float)v_vv);
+    R.v_il.push_back((float)v_il);
+  }
+  const size_t k = R.q.size();
+  if (k == 0) return OEMS_OK;
+  OEMS_CUDA(R.d_q.ensure(k));
+  OEMS_CUDA(R.d_dir.ensure(k));
+  OEMS_CUDA(R.d_vv.ensure(k));
+  OEMS_CUDA(R.d_vil.ensure(k));
+  OEMS_CUDA(R.d_int.ensure(k));
+  OEMS_CUDA(cudaMemcpy(R.d_q.p, R.q.data(), k * sizeof(long long), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(R.d_dir.p, R.dir.data(), k * sizeof(int), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(R.d_vv.p, R.v_vv.data(), k * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(R.d_vil.p, R.v_il.data(), k * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemset(R.d_int.p, 0, k * sizeof(float)));
+  engine->graph_epoch++;
+  return OEMS_OK;
 }
 
 oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc) {

@@ -237,6 +237,25 @@ oems_status oems_operator_set_pec(oems_operator* op, const uint64_t region[6]) {
   return OEMS_OK;
 }
 
+oems_status oems_operator_set_lumped(oems_operator* op, const uint64_t pos[3], int32_t dir, double r, double c,
+                                     double eps_r, double sigma, double* source_scale) {
+  if (!op || !pos) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (dir < 0 || dir > 2) return hfail(OEMS_ERR_CONFIG, "lumped element direction must be 0, 1 or 2");
+  for (int a = 0; a < 3; ++a)
+    if (pos[a] >= op->n[a]) return hfail(OEMS_ERR_CONFIG, "lumped element outside the grid");
+  if (!(eps_r > 0.0) || sigma < 0.0) return hfail(OEMS_ERR_MATERIAL, "eps_r must be positive, sigma >= 0");
+  const int a = (dir + 1) % 3, b = (dir + 2) % 3;
+  const double dl = op->delta[dir], area = op->delta[a] * op->delta[b], dt = op->dt;
+  const double eps = eps_r * kEps0 + (c > 0 ? c * dl / area : 0.0);
+  const double sig = sigma + (r > 0 ? dl / (r * area) : 0.0);
+  const double loss = sig * dt / (2.0 * eps);
+  const size_t q = op->idx(pos[0], pos[1], pos[2]);
+  op->c[dir][q] = (float)((1.0 - loss) / (1.0 + loss));
+  op->c[3 + dir][q] = (float)((dt / eps) / (1.0 + loss) / dl);
+  if (source_scale) *source_scale = r > 0 ? (dt / eps) / (1.0 + loss) / (r * area) : 0.0;
+  return OEMS_OK;
+}
+
 oems_status oems_operator_info(const oems_operator* op, uint64_t dims[3], double* dt, double delta[3]) {
   if (!op) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL operator");
   for (int a = 0; a < 3; ++a) {

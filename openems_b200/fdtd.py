@@ -167,6 +167,106 @@ class MurAbcConfig:
         return d
 
 
+@dataclass
+class DrudeMaterial:
+    """DrudeMaterial (src/extensions/dispersive.rs:450-535): omega_p, gamma
+    in rad/s; eps_inf divides the E correction (1 = the reference)."""
+
+    plasma_frequency: float
+    collision_frequency: float
+    eps_inf: float = 1.0
+
+    def to_c(self) -> N.DispersiveDescC:
+        return _disp_desc(0, (self.plasma_frequency, self.collision_frequency), self.eps_inf)
+
+
+@dataclass
+class LorentzMaterial:
+    """LorentzMaterial (src/extensions/dispersive.rs:107-196).  second_order
+    False reproduces the reference's update, which keeps no P^{n-1} and
+    grows without bound; True runs the full second-order recursion."""
+
+    resonance_frequency: float
+    damping: float
+    delta_eps: float
+    eps_inf: float = 1.0
+    second_order: bool = False
+
+    def to_c(self) -> N.DispersiveDescC:
+        return _disp_desc(3 if self.second_order else 1,
+                          (self.resonance_frequency, self.damping, self.delta_eps), self.eps_inf)
+
+
+@dataclass
+class DebyeMaterial:
+    """DebyeMaterial (src/extensions/dispersive.rs:545-630): tau in s."""
+
+    relaxation_time: float
+    delta_eps: float
+    eps_inf: float = 1.0
+
+    def to_c(self) -> N.DispersiveDescC:
+        return _disp_desc(2, (self.relaxation_time, self.delta_eps), self.eps_inf)
+
+
+def _disp_desc(kind, params, eps_inf) -> N.DispersiveDescC:
+    d = N.DispersiveDescC()
+    d.kind = kind
+    for a, v in enumerate(params):
+        d.params[a] = float(v)
+    d.eps_inf = float(eps_inf)
+    return d
+
+
+class RlcType(enum.IntEnum):
+    """RlcType (src/extensions/lumped_rlc.rs:10-16)."""
+
+    Parallel = 0
+    Series = 1
+
+
+@dataclass
+class RlcElement:
+    """RlcElement (src/extensions/lumped_rlc.rs:20-112) on one E edge."""
+
+    position: Tuple[int, int, int]
+    direction: int
+    rlc_type: RlcType = RlcType.Parallel
+    resistance: float = 0.0
+    inductance: float = 0.0
+    capacitance: float = 0.0
+
+    @classmethod
+    def resistor(cls, position, direction, r):
+        return cls(tuple(position), direction, RlcType.Parallel, resistance=r)
+
+    @classmethod
+    def capacitor(cls, position, direction, c):
+        return cls(tuple(position), direction, RlcType.Parallel, capacitance=c)
+
+    @classmethod
+    def inductor(cls, position, direction, l):
+        return cls(tuple(position), direction, RlcType.Parallel, inductance=l)
+
+    @classmethod
+    def parallel_rlc(cls, position, direction, r=None, l=None, c=None):
+        return cls(tuple(position), direction, RlcType.Parallel, r or 0.0, l or 0.0, c or 0.0)
+
+    @classmethod
+    def series_rlc(cls, position, direction, r=None, l=None, c=None):
+        return cls(tuple(position), direction, RlcType.Series, r or 0.0, l or 0.0, c or 0.0)
+
+    def to_c(self) -> N.LumpedRlcDescC:
+        d = N.LumpedRlcDescC()
+        for a in range(3):
+            d.position[a] = int(self.position[a])
+        d.direction = int(self.direction)
+        d.type = int(self.rlc_type)
+        d.resistance, d.inductance, d.capacitance = (float(self.resistance), float(self.inductance),
+                                                     float(self.capacitance))
+        return d
+
+
 # ---------------------------------------------------------------------------
 # operator
 # ---------------------------------------------------------------------------
@@ -225,6 +325,17 @@ class Operator:
 
     def set_pec(self, region):
         N.check(N.lib().oems_operator_set_pec(self._h, self._region(region)))
+
+    def set_lumped(self, position, direction, resistance=0.0, capacitance=0.0, eps_r=1.0,
+                   sigma=0.0) -> float:
+        """Lumped R and/or C folded into the Ca/Cb of one E edge; returns the
+        factor that turns a series source voltage into that edge's soft-source
+        sample (0 without R)."""
+        scale = N.c_f64()
+        N.check(N.lib().oems_operator_set_lumped(self._h, _u3(position), int(direction),
+                                                 float(resistance), float(capacitance), float(eps_r),
+                                                 float(sigma), ctypes.byref(scale)))
+        return scale.value
 
     def coefficients(self) -> np.ndarray:
         """Copy of the 12 arrays: (12, nx, ny, nz) = ca0..2, cb0..2, da0..2, db0..2."""
@@ -306,6 +417,86 @@ def port_probe(op: "Operator", position, direction, kind) -> ProbeTerms:
     """Lumped-port voltage (kind 0) or loop current (kind 1) at an E edge."""
     return _terms_from(N.lib().oems_probe_port_terms, op.handle, _u3(position), direction, kind,
                        mode=N.PROBE_SUM_F64)
+
+
+class LumpedPort:
+    """Lumped port on one E edge (python/openEMS/ports.py:155-209).
+
+    A resistor R sits across the edge (folded into its Ca/Cb); with excite
+    != 0 a voltage source excite * waveform drives it in series with R.  The
+    port voltage is u = +E . dl and the port current i is the current the port
+    delivers into the structure (minus the loop integral of H around the
+    edge), so that an open port reads u = excite * waveform and a matched
+    load reads half of it.  calc_port follows Port.CalcPort
+    (python/openEMS/ports.py:115-153) on the engine's running DFTs, which use
+    the single-sided 2 dt scaling of utilities.DFT_time2freq (:21-35).
+    """
+
+    def __init__(self, port_nr: int, R: float, position, direction: int, excite: float = 0.0,
+                 eps_r: float = 1.0):
+        if direction not in (0, 1, 2):
+            raise N.ConfigError("LumpedPort direction must be 0, 1 or 2")
+        if R <= 0:
+            raise N.ConfigError("LumpedPort needs a positive resistance")
+        self.number = port_nr
+        self.R = float(R)
+        self.Z_ref = float(R)
+        self.position = tuple(int(v) for v in position)
+        self.direction = int(direction)
+        self.excite = float(excite)
+        self.eps_r = float(eps_r)
+        self.source_scale = None
+        self.freqs = None
+
+    def apply(self, op: Operator) -> "LumpedPort":
+        """Writes the port resistor into the operator's coefficients."""
+        self.source_scale = op.set_lumped(self.position, self.direction, resistance=self.R,
+                                          eps_r=self.eps_r)
+        self._op = op
+        return self
+
+    def excitation(self, waveform: Excitation) -> Excitation:
+        """waveform's time signal as this port's soft source."""
+        if self.source_scale is None:
+            raise N.ConfigError("LumpedPort.apply(operator) must run first")
+        return Excitation(waveform.excitation_type, tuple(waveform.params), self.direction,
+                          self.position, waveform.amplitude * self.excite * self.source_scale, True)
+
+    def add_probes(self, engine: "Engine", freqs) -> "LumpedPort":
+        """u / i probes and their running DFTs at freqs (Hz)."""
+        u = port_probe(self._op, self.position, self.direction, 0)
+        i = port_probe(self._op, self.position, self.direction, 1)
+        u = ProbeTerms([(c, q, -w) for c, q, w in u.terms], u.mode)
+        i = ProbeTerms([(c, q, -w) for c, q, w in i.terms], i.mode)
+        self.u_probe = engine.add_probe(u)
+        self.i_probe = engine.add_probe(i)
+        self.freqs = np.asarray(freqs, dtype=np.float64)
+        self.u_dft = engine.add_probe_dft(self.u_probe, self.freqs)
+        self.i_dft = engine.add_probe_dft(self.i_probe, self.freqs)
+        return self
+
+    def calc_port(self, engine: "Engine", ref_impedance: Optional[float] = None) -> "LumpedPort":
+        """Port.CalcPort (python/openEMS/ports.py:115-153) without the
+        reference-plane shift, which a lumped port does not support."""
+        if ref_impedance is not None:
+            self.Z_ref = float(ref_impedance)
+        Z = self.Z_ref
+        self.uf_tot = engine.probe_dft(self.u_dft)
+        self.if_tot = engine.probe_dft(self.i_dft)
+        self.uf_inc = 0.5 * (self.uf_tot + self.if_tot * Z)
+        self.if_inc = 0.5 * (self.if_tot + self.uf_tot / Z)
+        self.uf_ref = self.uf_tot - self.uf_inc
+        self.if_ref = self.if_inc - self.if_tot
+        self.P_inc = 0.5 * np.real(self.uf_inc * np.conj(self.if_inc))
+        self.P_ref = 0.5 * np.real(self.uf_ref * np.conj(self.if_ref))
+        self.P_acc = 0.5 * np.real(self.uf_tot * np.conj(self.if_tot))
+        return self
+
+    def s11(self) -> np.ndarray:
+        return self.uf_ref / self.uf_inc
+
+    def z_in(self) -> np.ndarray:
+        return self.uf_tot / self.if_tot
 
 
 class ExcitationType(enum.IntEnum):
@@ -553,6 +744,18 @@ class Engine:
     def add_mur(self, mur: MurAbcConfig):
         d = mur.to_c()
         N.check(N.lib().oems_engine_add_mur(self._h, ctypes.byref(d)))
+
+    def add_dispersive(self, material, cells):
+        """Dispersive material (Drude / Lorentz / Debye) on cells (n, 3)."""
+        c = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1, 3)
+        d = material.to_c()
+        N.check(N.lib().oems_engine_add_dispersive(self._h, ctypes.byref(d), c.ctypes.data, len(c)))
+
+    def add_lumped_rlc(self, elements: Sequence[RlcElement]):
+        arr = (N.LumpedRlcDescC * max(1, len(elements)))()
+        for i, e in enumerate(elements):
+            arr[i] = e.to_c()
+        N.check(N.lib().oems_engine_add_lumped_rlc(self._h, arr, len(elements)))
 
     def add_point_probe(self, component: int, position) -> int:
         """FieldProbe-style value of one component at one cell."""

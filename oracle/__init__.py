@@ -90,6 +90,12 @@ def lib() -> ctypes.CDLL:
         L.orc_cpml_profile.argtypes = [P, I32, P]
         L.orc_enable_mur.restype = I32
         L.orc_enable_mur.argtypes = [P, P, I32, D]
+        L.orc_add_dispersive.restype = I32
+        L.orc_add_dispersive.argtypes = [P, I32, P, D, P, I64]
+        L.orc_add_lumped_rlc.restype = I32
+        L.orc_add_lumped_rlc.argtypes = [P, P, I32, I32, D, D, D]
+        L.orc_set_lumped.restype = D
+        L.orc_set_lumped.argtypes = [P, P, I32, D, D, D, D]
         L.orc_run_batch.restype = I32
         L.orc_run_batch.argtypes = [P, U64, U64, I32, U64, I32, D, D, ctypes.POINTER(BatchResult)]
         L.orc_get_energy_samples.argtypes = [P, ctypes.POINTER(EnergySample), U64]
@@ -248,6 +254,24 @@ class OracleSim:
         rc = lib().orc_enable_mur(self._h, _ptr(e), order, phase_velocity or 0.0)
         if rc != 0:
             raise ValueError(f"invalid Mur configuration ({rc})")
+
+    def add_dispersive(self, kind, params, cells, eps_inf=1.0):
+        p = np.zeros(3)
+        p[:len(params)] = params
+        c = np.ascontiguousarray(cells, dtype=np.int64).reshape(-1, 3)
+        rc = lib().orc_add_dispersive(self._h, int(kind), _ptr(p), float(eps_inf), _ptr(c), len(c))
+        if rc != 0:
+            raise ValueError(f"invalid dispersive material ({rc})")
+
+    def add_lumped_rlc(self, pos, direction, type_, r=0.0, l=0.0, c=0.0):
+        q = np.ascontiguousarray(pos, dtype=np.int64)
+        rc = lib().orc_add_lumped_rlc(self._h, _ptr(q), int(direction), int(type_), r, l, c)
+        if rc != 0:
+            raise ValueError(f"invalid lumped RLC element ({rc})")
+
+    def set_lumped(self, pos, direction, r=0.0, c=0.0, eps_r=1.0, sigma=0.0):
+        q = np.ascontiguousarray(pos, dtype=np.int64)
+        return lib().orc_set_lumped(self._h, _ptr(q), int(direction), r, c, eps_r, sigma)
 
     def cpml_profile(self, face):
         out = np.zeros((6, 256))

@@ -70,3 +70,78 @@ def run(coeffs12: np.ndarray, fields6: np.ndarray, num_steps: int, excitations=(
             else:
                 comps[d][tuple(pos)] = v
     return np.stack([ex, ey, ez, hx, hy, hz])
+
+
+# ---------------------------------------------------------------------------
+# per-cell extensions, written separately from oems_oracle.cpp
+# ---------------------------------------------------------------------------
+
+EPS0 = 8.854187817e-12  # src/constants.rs
+f32 = np.float32
+
+
+def dispersive_coeffs(kind: int, params, dt: float, eps_inf: float = 1.0):
+    """(a, b, c, c2) as float32.  Drude: DrudeMaterial::new
+    (src/extensions/dispersive.rs:476-498); Lorentz: LorentzMaterial::new
+    (:134-159, kind 1 as the reference, kind 3 the same a, b, c with the
+    second-order update); Debye: DebyeMaterial::new (:570-592).  eps_inf = 1
+    gives the reference's c."""
+    p = list(params) + [0.0] * (3 - len(params))
+    c2 = 0.0
+    if kind == 0:
+        den = 1.0 + p[1] * dt / 2.0
+        a, b, c = (1.0 - p[1] * dt / 2.0) / den, EPS0 * p[0] * p[0] * dt / den, dt / (EPS0 * eps_inf)
+    elif kind in (1, 3):
+        den = 1.0 + p[1] * dt / 2.0
+        a = (2.0 - p[0] * p[0] * dt * dt) / den
+        b = (p[1] * dt / 2.0 - 1.0) / den
+        c = EPS0 * p[2] * p[0] * p[0] * dt * dt / den
+        c2 = 1.0 / (EPS0 * eps_inf)
+    else:
+        den = 2.0 * p[0] + dt
+        a, b, c = (2.0 * p[0] - dt) / den, 2.0 * EPS0 * p[1] * dt / den, dt / (EPS0 * eps_inf)
+    return f32(a), f32(b), f32(c), f32(c2)
+
+
+def dispersive_step(kind, coeffs, e, state, prev, dt):
+    """One post_update_e of one field value (float32 scalars); returns
+    (e', state', prev').  Drude :510-535, Lorentz :171-196, Debye :604-630."""
+    a, b, c, c2 = coeffs
+    e, state, prev = f32(e), f32(state), f32(prev)
+    if kind == 0:
+        jn = a * state + b * e
+        return e - c * jn, jn, prev
+    if kind == 1:
+        jn = a * state + c * e
+        return e - b * jn, jn, prev
+    if kind == 2:
+        pn = a * state + b * e
+        return e - c * ((pn - state) / f32(dt)), pn, prev
+    pn = (a * state + b * prev) + c * e
+    return e - c2 * (pn - state), pn, state
+
+
+def rlc_coeffs(rlc_type, r, l, c, dl, dt):
+    """(v_vv, v_il) as float32: calc_parallel_coeffs / calc_series_coeffs
+    (src/extensions/lumped_rlc.rs:190-250)."""
+    da = dl * dl
+    if rlc_type == 0:
+        g = 1.0 / r if r > 0 else 0.0
+        inv_l = dt / l if l > 0 else 0.0
+        cc = c if c > 0 else 0.0
+        g_eff = g * dl / da
+        c_eff = cc * dl / da + EPS0 * dl / da
+        den = 2.0 * c_eff + g_eff * dt
+        return f32((2.0 * c_eff - g_eff * dt) / den), f32(inv_l * dl / da)
+    rr = r if r > 0 else 0.0
+    ll = l if l > 0 else 0.0
+    inv_c = dt / c if c > 0 else 0.0
+    den = 2.0 * (ll * da / dl) + (rr * da / dl) * dt
+    return f32(1.0), f32(0.0 if abs(den) < 1e-20 else inv_c * da / dl)
+
+
+def rlc_step(coeffs, e, i_int, dt):
+    """LumpedRlc::post_update_e for one element (lumped_rlc.rs:263-286)."""
+    v_vv, v_il = coeffs
+    e, i_int = f32(e), f32(i_int)
+    return v_vv * e + v_il * i_int, i_int + e * f32(dt)

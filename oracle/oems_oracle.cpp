@@ -134,6 +134,72 @@ struct Sim {
   std::vector<MurFace> mur;
   int mur_order = 0;
 
+  // dispersive materials (src/extensions/dispersive.rs:75-96: coefficients
+  // a, b, c per material, state per cell and component)
+  struct Dispersive {
+    int kind;
+    float a, b, c, c2;          // as computed by the reference constructors, f32
+    std::vector<int64_t> q;     // cells
+    std::vector<T> j[3], pp[3]; // state (J or P) and P at n-1 (second-order Lorentz)
+  };
+  std::vector<Dispersive> disp;
+
+  // LumpedRlc elements (src/extensions/lumped_rlc.rs:118-139)
+  struct Rlc {
+    int64_t q;
+    int dir;
+    float v_vv, v_il;
+    T i_int;
+  };
+  std::vector<Rlc> rlc;
+
+  // src/extensions/dispersive.rs:171-196, 510-535, 604-630 (+ second-order Lorentz)
+  void apply_dispersive() {
+    const float dtf = (float)dt;
+    for (Dispersive& D : disp) {
+      for (size_t m = 0; m < D.q.size(); ++m)
+        for (int c = 0; c < 3; ++c) {
+          T& ef = E[c][D.q[m]];
+          const T e = ef;
+          const T old = D.j[c][m];
+          if (D.kind == 0) {  // Drude: j = a j + b e; e -= c j
+            const T jn = T(D.a) * old + T(D.b) * e;
+            D.j[c][m] = jn;
+            ef = e - T(D.c) * jn;
+          } else if (D.kind == 1) {  // Lorentz as the reference: j = a j + c e; e -= b j
+            const T jn = T(D.a) * old + T(D.c) * e;
+            D.j[c][m] = jn;
+            ef = e - T(D.b) * jn;
+          } else if (D.kind == 2) {  // Debye: p' = a p + b e; e -= c (p' - p) / dt
+            const T pn = T(D.a) * old + T(D.b) * e;
+            D.j[c][m] = pn;
+            const T dpdt = (pn - old) / T(dtf);
+            ef = e - T(D.c) * dpdt;
+          } else {  // second-order Lorentz
+            const T t1 = T(D.a) * old;
+            const T t2 = T(D.b) * D.pp[c][m];
+            const T t3 = T(D.c) * e;
+            const T pn = (t1 + t2) + t3;
+            D.pp[c][m] = old;
+            D.j[c][m] = pn;
+            ef = e - T(D.c2) * (pn - old);
+          }
+        }
+    }
+  }
+
+  // src/extensions/lumped_rlc.rs:263-286
+  void apply_rlc() {
+    const T dtf = T((float)dt);
+    for (Rlc& r : rlc) {
+      T& ef = E[r.dir][r.q];
+      const T e = ef;
+      const T en = T(r.v_vv) * e + T(r.v_il) * r.i_int;
+      r.i_int = r.i_int + e * dtf;
+      ef = en;
+    }
+  }
+
   Sim(int64_t nx_, int64_t ny_, int64_t nz_, double dt_, double dx, double dy, double dz)
       : nx(nx_), ny(ny_), nz(nz_), n(nx_ * ny_ * nz_), dt(dt_) {
     delta[0] = dx;
@@ -578,6 +644,8 @@ struct Sim {
       if (!mur.empty()) mur_pre();
       update_e();
       if (!mur.empty()) mur_post_apply();
+      if (!disp.empty()) apply_dispersive();
+      if (!rlc.empty()) apply_rlc();
       apply_excitations(step);
       record_probes(timestep + 1);
       timestep += 1;
@@ -740,6 +808,12 @@ void orc_reset(orc_sim* s) {
       std::fill(S->psi_h[q].begin(), S->psi_h[q].end(), T(0));
       std::fill(S->psi_e[q].begin(), S->psi_e[q].end(), T(0));
     }
+    for (auto& D : S->disp)
+      for (int c = 0; c < 3; ++c) {
+        std::fill(D.j[c].begin(), D.j[c].end(), T(0));
+        std::fill(D.pp[c].begin(), D.pp[c].end(), T(0));
+      }
+    for (auto& r : S->rlc) r.i_int = T(0);
     for (auto& F : S->mur)
       for (int t = 0; t < 2; ++t) {
         std::fill(F.v[t].begin(), F.v[t].end(), T(0));
@@ -887,6 +961,91 @@ int32_t orc_cpml_profile(const orc_sim* s, int32_t f, double* out) {
     }
   });
   return L;
+}
+
+int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* p, double eps_inf, const int64_t* cells,
+                           int64_t ncells) {
+  if (kind < 0 || kind > 3 || !(eps_inf > 0.0)) return -1;
+  int32_t rc = 0;
+  DISPATCH(s, {
+    typename std::remove_reference_t<decltype(*S)>::Dispersive D;
+    D.kind = kind;
+    const double dt = S->dt;
+    if (kind == 0) {  // DrudeMaterial::new (dispersive.rs:476-498)
+      const double wp = p[0], g = p[1], den = 1.0 + g * dt / 2.0;
+      D.a = (float)((1.0 - g * dt / 2.0) / den);
+      D.b = (float)(kEps0 * wp * wp * dt / den);
+      D.c = (float)(dt / (kEps0 * eps_inf));
+    } else if (kind == 1 || kind == 3) {  // LorentzMaterial::new (dispersive.rs:134-159)
+      const double w0 = p[0], g = p[1], de = p[2], den = 1.0 + g * dt / 2.0;
+      D.a = (float)((2.0 - w0 * w0 * dt * dt) / den);
+      D.b = (float)((g * dt / 2.0 - 1.0) / den);
+      D.c = (float)(kEps0 * de * w0 * w0 * dt * dt / den);
+      D.c2 = (float)(1.0 / (kEps0 * eps_inf));
+    } else {  // DebyeMaterial::new (dispersive.rs:570-592)
+      const double tau = p[0], de = p[1], den = 2.0 * tau + dt;
+      D.a = (float)((2.0 * tau - dt) / den);
+      D.b = (float)(2.0 * kEps0 * de * dt / den);
+      D.c = (float)(dt / (kEps0 * eps_inf));
+    }
+    for (int64_t m = 0; m < ncells; ++m) D.q.push_back(S->idx(cells[3 * m], cells[3 * m + 1], cells[3 * m + 2]));
+    for (int c = 0; c < 3; ++c) {
+      D.j[c].assign(ncells, 0);
+      D.pp[c].assign(ncells, 0);
+    }
+    S->disp.push_back(D);
+  });
+  return rc;
+}
+
+int32_t orc_add_lumped_rlc(orc_sim* s, const int64_t* pos, int32_t dir, int32_t type, double r, double l,
+                           double c) {
+  DISPATCH(s, {
+    typename std::remove_reference_t<decltype(*S)>::Rlc e;
+    const double dt = S->dt, dl = S->delta[dir], da = dl * dl;
+    double v_vv, v_il;
+    if (type == 0) {  // calc_parallel_coeffs (lumped_rlc.rs:190-216)
+      const double g = r > 0 ? 1.0 / r : 0.0;
+      const double inv_l = l > 0 ? dt / l : 0.0;
+      const double cc = c > 0 ? c : 0.0;
+      const double g_eff = g * dl / da;
+      const double c_eff = cc * dl / da + kEps0 * dl / da;
+      const double den = 2.0 * c_eff + g_eff * dt;
+      v_vv = (2.0 * c_eff - g_eff * dt) / den;
+      v_il = inv_l * dl / da;
+    } else {  // calc_series_coeffs (lumped_rlc.rs:219-250)
+      const double rr = r > 0 ? r : 0.0, ll = l > 0 ? l : 0.0;
+      const double inv_c = c > 0 ? dt / c : 0.0;
+      const double den = 2.0 * (ll * da / dl) + (rr * da / dl) * dt;
+      v_vv = 1.0;
+      v_il = std::fabs(den) < 1e-20 ? 0.0 : inv_c * da / dl;
+    }
+    e.q = S->idx(pos[0], pos[1], pos[2]);
+    e.dir = dir;
+    e.v_vv = (float)v_vv;
+    e.v_il = (float)v_il;
+    e.i_int = 0;
+    S->rlc.push_back(e);
+  });
+  return 0;
+}
+
+double orc_set_lumped(orc_sim* s, const int64_t* pos, int32_t dir, double r, double c, double eps_r,
+                      double sigma) {
+  double scale = 0.0;
+  DISPATCH(s, {
+    using T = std::remove_reference_t<decltype(S->E[0][0])>;
+    const int a = (dir + 1) % 3, b = (dir + 2) % 3;
+    const double dl = S->delta[dir], area = S->delta[a] * S->delta[b], dt = S->dt;
+    const double eps = eps_r * kEps0 + (c > 0 ? c * dl / area : 0.0);
+    const double sig = sigma + (r > 0 ? dl / (r * area) : 0.0);
+    const double loss = sig * dt / (2.0 * eps);
+    const int64_t q = S->idx(pos[0], pos[1], pos[2]);
+    S->ca[dir][q] = T((1.0 - loss) / (1.0 + loss));
+    S->cb[dir][q] = T((dt / eps) / (1.0 + loss) / dl);
+    scale = r > 0 ? (dt / eps) / (1.0 + loss) / (r * area) : 0.0;
+  });
+  return scale;
 }
 
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity) {

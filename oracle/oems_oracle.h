@@ -148,6 +148,28 @@ int32_t orc_cpml_profile(const orc_sim* s, int32_t face, double* out);
  * phase_velocity <= 0 means c0.  Returns 0 or a negative error. */
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity);
 
+/* Dispersive material on a list of cells (src/extensions/dispersive.rs),
+ * applied after the E update, all three components per cell:
+ *   kind 0 Drude  (:476-535)  j = a j + b e;  e = e - c j
+ *   kind 1 Lorentz as the reference (:134-196) j = a j + c e; e = e - b j
+ *   kind 2 Debye  (:570-630)  p' = a p + b e; e = e - c (p' - p) / dt
+ *   kind 3 Lorentz, second order: p' = a p + b p_prev + c e;
+ *          e = e - (p' - p) / (eps0 eps_inf)
+ * params: Drude (omega_p, gamma) rad/s; Lorentz (omega_0, gamma, delta_eps);
+ * Debye (tau, delta_eps).  eps_inf divides the E correction (1 = reference). */
+int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* params, double eps_inf,
+                           const int64_t* cells, int64_t ncells);
+/* LumpedRlc (src/extensions/lumped_rlc.rs:155-286) after the E update:
+ * e' = v_vv e + v_il int; int += e dt.  type 0 parallel, 1 series; r, l, c
+ * <= 0 mean absent. */
+int32_t orc_add_lumped_rlc(orc_sim* s, const int64_t* pos3, int32_t dir, int32_t type, double r,
+                           double l, double c);
+/* Lumped resistor / capacitor across the E edge (pos, dir) folded into Ca/Cb
+ * (eps = eps_r eps0 + C dl / A, sigma = sigma + dl / (R A)); returns the
+ * factor that turns a series source voltage into the soft-source sample. */
+double orc_set_lumped(orc_sim* s, const int64_t* pos3, int32_t dir, double r, double c, double eps_r,
+                      double sigma);
+
 int32_t orc_run_batch(orc_sim* s, uint64_t num_steps, uint64_t sample_interval,
                       int32_t track_peak, uint64_t check_interval, int32_t has_decay,
                       double decay_db, double initial_peak, orc_batch_result* res);

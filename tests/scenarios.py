@@ -30,6 +30,9 @@ class Scenario:
     mur: Optional[oe.MurAbcConfig] = None
     probes: List[Tuple[int, Tuple[int, int, int]]] = field(default_factory=list)
     batches: Sequence[int] = ()  # split num_steps into these batch sizes (default: one batch)
+    dispersive: List[Tuple] = field(default_factory=list)  # (material, cells (n, 3))
+    rlc: List[oe.RlcElement] = field(default_factory=list)
+    lumped: List[Tuple] = field(default_factory=list)      # (pos, dir, R, C, eps_r, sigma)
 
     def batch_sizes(self):
         return list(self.batches) if self.batches else [self.num_steps]
@@ -42,6 +45,8 @@ def make_operator(sc: Scenario) -> oe.Operator:
         op.set_material(eps_r, mu_r, se, sm, reg)
     for reg in sc.pec:
         op.set_pec(reg)
+    for pos, d, r, c, eps_r, sig in sc.lumped:
+        op.set_lumped(pos, d, r, c, eps_r, sig)
     return op
 
 
@@ -53,6 +58,10 @@ def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kerne
         eng.add_cpml(sc.cpml)
     if sc.mur is not None:
         eng.add_mur(sc.mur)
+    for mat, cells in sc.dispersive:
+        eng.add_dispersive(mat, cells)
+    if sc.rlc:
+        eng.add_lumped_rlc(sc.rlc)
     for comp, pos in sc.probes:
         eng.add_point_probe(comp, pos)
     dt = op.timestep()
@@ -88,6 +97,14 @@ def run_oracle(sc: Scenario, precision=32, threads=1):
         s.enable_cpml(c.layers, c.grading_order, c.reflection_coeff, c.alpha_max, c.kappa_max)
     if sc.mur is not None:
         s.enable_mur(sc.mur.enabled, sc.mur.order, sc.mur.phase_velocity or 0.0)
+    for pos, d, r, c, eps_r, sig in sc.lumped:
+        s.set_lumped(pos, d, r, c, eps_r, sig)
+    for mat, cells in sc.dispersive:
+        d = mat.to_c()
+        s.add_dispersive(d.kind, list(d.params), cells, d.eps_inf)
+    for e in sc.rlc:
+        s.add_lumped_rlc(e.position, e.direction, int(e.rlc_type), e.resistance, e.inductance,
+                         e.capacitance)
     for comp, pos in sc.probes:
         s.add_point_probe(comp, pos)
     energy, traces, start = [], [], 0
@@ -247,3 +264,47 @@ def probe_scenario() -> Scenario:
                                  E.gaussian_modulated(6e9, 0.4, 0, (12, 6, 15))],
                     num_steps=260, cpml=oe.CpmlBoundaries(layers=(4, 4, 4, 4, 4, 4)),
                     batches=(100, 160))
+
+
+def _box_cells(i0, i1, j0, j1, k0, k1):
+    g = np.mgrid[i0:i1, j0:j1, k0:k1].reshape(3, -1).T
+    return np.ascontiguousarray(g, dtype=np.int64)
+
+
+def dispersive_scenarios() -> List[Scenario]:
+    """Drude, Debye and second-order Lorentz blocks with sources and CPML;
+    the reference's first-order Lorentz for a few steps (it diverges);
+    lumped RLC elements of both types; a lumped resistor port."""
+    E = oe.Excitation
+    x = E.gaussian_modulated(12e9, 0.5, 2, (8, 9, 10))
+    drude = oe.DrudeMaterial(2 * np.pi * 20e9, 1e10)
+    debye = oe.DebyeMaterial(1e-11, 3.0, eps_inf=2.0)
+    lorentz2 = oe.LorentzMaterial(2 * np.pi * 15e9, 2e9, 2.0, eps_inf=1.5, second_order=True)
+    lorentz = oe.LorentzMaterial(2 * np.pi * 15e9, 2e9, 2.0)
+    rlc = [oe.RlcElement((5, 5, 5), 2, oe.RlcType.Parallel, 50.0, 1e-9, 1e-12),
+           oe.RlcElement((11, 4, 12), 0, oe.RlcType.Parallel, 0.0, 2e-9, 0.0),
+           oe.RlcElement((6, 12, 7), 1, oe.RlcType.Series, 10.0, 1e-9, 0.5e-12),
+           oe.RlcElement((5, 5, 5), 2, oe.RlcType.Parallel, 100.0, 0.0, 0.0)]
+    return [
+        Scenario("drude_debye_cpml", (17, 19, 21), 1e-3, excitations=[x], num_steps=220,
+                 sample_interval=20, track_peak=True, cpml=oe.CpmlBoundaries.uniform(4),
+                 dispersive=[(drude, _box_cells(10, 14, 3, 9, 12, 18)),
+                             (debye, _box_cells(2, 7, 11, 16, 2, 19))],
+                 probes=[(2, (11, 5, 14)), (0, (4, 13, 10))]),
+        Scenario("lorentz2_overlap", (14, 13, 22), 1e-3, excitations=[x], num_steps=200,
+                 dispersive=[(lorentz2, _box_cells(3, 12, 2, 11, 12, 20)),
+                             (drude, _box_cells(6, 9, 5, 8, 14, 17))],
+                 probes=[(2, (7, 6, 15))]),
+        Scenario("lorentz_reference_short", (10, 11, 12), 1e-3,
+                 excitations=[E.gaussian_modulated(12e9, 0.5, 1, (5, 5, 6))], num_steps=30,
+                 dispersive=[(lorentz, _box_cells(2, 8, 2, 9, 3, 10))]),
+        Scenario("lumped_rlc", (16, 15, 18), 1e-3,
+                 excitations=[E.gaussian_modulated(10e9, 0.5, 2, (8, 7, 9))], num_steps=250,
+                 sample_interval=25, track_peak=True, rlc=rlc, mur=oe.MurAbcConfig.all(1),
+                 probes=[(2, (5, 5, 5)), (0, (11, 4, 12)), (1, (6, 12, 7))]),
+        Scenario("lumped_port_r", (16, 16, 20), 1e-3,
+                 excitations=[E.gaussian_modulated(10e9, 0.5, 2, (8, 8, 10)).with_amplitude(7.0)],
+                 num_steps=200, lumped=[((8, 8, 10), 2, 50.0, 0.0, 1.0, 0.0),
+                                        ((4, 9, 6), 0, 0.0, 2e-13, 2.0, 0.01)],
+                 cpml=oe.CpmlBoundaries.uniform(4), probes=[(2, (8, 8, 10)), (0, (4, 9, 6))]),
+    ]
