@@ -202,6 +202,61 @@ typedef struct oems_lumped_rlc_desc {
   double resistance, inductance, capacitance;
 } oems_lumped_rlc_desc;
 
+/* Frequency-domain field dump (FrequencyDomainFieldDump,
+ * src/processing/fields_fd.rs:31-217) over a half-open cell region with
+ * per-axis sub-sampling.  X(f) += x(t) exp(-j 2 pi f t) 2 dt interval at every
+ * timestep count that is a multiple of `interval` (>= 1; the reference
+ * accumulates every call with 2 dt), E at t = n dt and H at (n - 1/2) dt,
+ * in f64.  components: bit c records component c (0..2 Ex Ey Ez, 3..5 Hx Hy
+ * Hz); FdDumpType EField / HField / Both are 0x07 / 0x38 / 0x3F. */
+typedef struct oems_field_dft_desc {
+  uint64_t region[6];
+  uint32_t sub_sample[3];
+  uint32_t components;
+  uint32_t interval;
+  uint32_t reserved0;
+} oems_field_dft_desc;
+
+/* Near-field to far-field recording box on the node planes start..stop
+ * (1 <= start < stop <= n - 1 per axis), faces -x +x -y +y -z +z enabled by
+ * `directions` (the nf2ff box of python/openEMS/nf2ff.py:38-97 with
+ * frequency-domain recording).  Per face it records tangential E on the
+ * face plane and tangential H averaged over the two half-cells around it, in
+ * f64 at the sampled timesteps as above. */
+typedef struct oems_nf2ff_box_desc {
+  uint64_t start[3], stop[3];
+  int32_t directions[6];
+  uint32_t interval;
+  uint32_t reserved0;
+} oems_nf2ff_box_desc;
+
+/* Far-field request (nf2ff.CalcNF2FF, python/openEMS/nf2ff.py:98-165):
+ * angles in radians, observation radius in metres, phase centre, and the
+ * mesh lines in metres per axis (n + 1 values; NULL = uniform delta). */
+typedef struct oems_nf2ff_request {
+  const double* theta;
+  uint64_t ntheta;
+  const double* phi;
+  uint64_t nphi;
+  double radius;
+  double center[3];
+  const double* lines[3];
+} oems_nf2ff_request;
+
+/* Far-field result (nf2ff_results, python/openEMS/nf2ff.py:167-220), caller
+ * owned, theta-major: e_theta / e_phi 2 x ntheta x nphi doubles (re, im) in
+ * V/m at the radius, p_rad ntheta x nphi in W/m^2 (= |E|^2 / (2 Z0)); any
+ * pointer may be NULL.  prad = the integral of p_rad r^2 sin(theta) over the
+ * requested grid (trapezoid rule), dmax = 4 pi r^2 max(p_rad) / prad: both
+ * need a grid covering the whole sphere. */
+typedef struct oems_nf2ff_result {
+  double* e_theta;
+  double* e_phi;
+  double* p_rad;
+  double prad;
+  double dmax;
+} oems_nf2ff_result;
+
 /* Field components for probes: 0..2 = Ex Ey Ez, 3..5 = Hx Hy Hz. */
 #define OEMS_COMPONENT_EX 0
 #define OEMS_COMPONENT_HX 3
@@ -233,6 +288,35 @@ OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_des
  * the order they are added. */
 OEMS_API oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersive_desc* desc,
                                                 const uint64_t* cells, uint64_t ncells);
+/* FrequencyDomainFieldDump::new (src/processing/fields_fd.rs:73-123) with
+ * set_sub_sample (:126-128); recording starts with the next batch. */
+OEMS_API oems_status oems_engine_add_field_dft(oems_engine* engine, const oems_field_dft_desc* desc,
+                                               const double* freqs, uint32_t nfreq, int32_t* dump_id);
+/* get_e_field / get_h_field (src/processing/fields_fd.rs:222-238) for one
+ * component: npoints (re, im) pairs in region order (k fastest) of the
+ * sub-sampled region. */
+OEMS_API oems_status oems_engine_read_field_dft(oems_engine* engine, int32_t dump_id, uint32_t freq_index,
+                                                uint32_t component, double* out, uint64_t npoints);
+/* NF2FF recording box (no counterpart in the reference engine). */
+OEMS_API oems_status oems_engine_add_nf2ff_box(oems_engine* engine, const oems_nf2ff_box_desc* desc,
+                                               const double* freqs, uint32_t nfreq, int32_t* box_id);
+/* Raw accumulators of one face (0..5 = -x +x -y +y -z +z) at one frequency:
+ * 4 arrays Eb, Ec, Hb, Hc (b = a+1, c = a+2 mod 3 for normal axis a) of
+ * nb x nc points (b-major) as (re, im); *npoints receives nb nc; out NULL
+ * only queries the size. */
+OEMS_API oems_status oems_engine_read_nf2ff_face(oems_engine* engine, int32_t box_id, uint32_t face,
+                                                 uint32_t freq_index, double* out, uint64_t cap_doubles,
+                                                 uint64_t* npoints);
+/* Far field of a recorded box at one of its frequencies (Nf2ff::calculate,
+ * src/nf2ff/mod.rs:117-170, with the radiation vectors its
+ * integrate_surfaces leaves at zero computed on the GPU in f64). */
+OEMS_API oems_status oems_engine_nf2ff(oems_engine* engine, int32_t box_id, uint32_t freq_index,
+                                       const oems_nf2ff_request* request, oems_nf2ff_result* result);
+/* The same transform from a host point list: npoints x 16 doubles
+ * (x y z weight, J (re, im) x 3, M (re, im) x 3; J = n x H, M = -n x E,
+ * weight = area).  device -1 = current. */
+OEMS_API oems_status oems_nf2ff_surface(int32_t device, const double* points, uint64_t npoints, double frequency,
+                                        const oems_nf2ff_request* request, oems_nf2ff_result* result);
 /* LumpedRlc::new (src/extensions/lumped_rlc.rs:145-160).  Elements apply in
  * list order; adding elements restarts every element's integrator at 0. */
 OEMS_API oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rlc_desc* elements,

@@ -142,6 +142,27 @@ class LumpedRlcDescC(ctypes.Structure):
                 ("resistance", c_f64), ("inductance", c_f64), ("capacitance", c_f64)]
 
 
+class FieldDftDescC(ctypes.Structure):
+    _fields_ = [("region", c_u64 * 6), ("sub_sample", c_u32 * 3), ("components", c_u32),
+                ("interval", c_u32), ("reserved0", c_u32)]
+
+
+class Nf2ffBoxDescC(ctypes.Structure):
+    _fields_ = [("start", c_u64 * 3), ("stop", c_u64 * 3), ("directions", c_i32 * 6),
+                ("interval", c_u32), ("reserved0", c_u32)]
+
+
+class Nf2ffRequestC(ctypes.Structure):
+    _fields_ = [("theta", ctypes.POINTER(c_f64)), ("ntheta", c_u64),
+                ("phi", ctypes.POINTER(c_f64)), ("nphi", c_u64), ("radius", c_f64),
+                ("center", c_f64 * 3), ("lines", ctypes.POINTER(c_f64) * 3)]
+
+
+class Nf2ffResultC(ctypes.Structure):
+    _fields_ = [("e_theta", ctypes.POINTER(c_f64)), ("e_phi", ctypes.POINTER(c_f64)),
+                ("p_rad", ctypes.POINTER(c_f64)), ("prad", c_f64), ("dmax", c_f64)]
+
+
 class ExcitationC(ctypes.Structure):
     _fields_ = [("kind", c_i32), ("direction", c_u32), ("position", c_u64 * 3),
                 ("params", c_f64 * 3), ("amplitude", c_f64), ("soft_source", c_i32),
@@ -168,6 +189,17 @@ SIGNATURES = {
     "oems_engine_add_mur": (c_i32, [P, ctypes.POINTER(MurDescC)]),
     "oems_engine_add_dispersive": (c_i32, [P, ctypes.POINTER(DispersiveDescC), P, c_u64]),
     "oems_engine_add_lumped_rlc": (c_i32, [P, ctypes.POINTER(LumpedRlcDescC), c_u64]),
+    "oems_engine_add_field_dft": (c_i32, [P, ctypes.POINTER(FieldDftDescC), ctypes.POINTER(c_f64), c_u32,
+                                          ctypes.POINTER(c_i32)]),
+    "oems_engine_read_field_dft": (c_i32, [P, c_i32, c_u32, c_u32, ctypes.POINTER(c_f64), c_u64]),
+    "oems_engine_add_nf2ff_box": (c_i32, [P, ctypes.POINTER(Nf2ffBoxDescC), ctypes.POINTER(c_f64), c_u32,
+                                          ctypes.POINTER(c_i32)]),
+    "oems_engine_read_nf2ff_face": (c_i32, [P, c_i32, c_u32, c_u32, ctypes.POINTER(c_f64), c_u64,
+                                            ctypes.POINTER(c_u64)]),
+    "oems_engine_nf2ff": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(Nf2ffRequestC),
+                                  ctypes.POINTER(Nf2ffResultC)]),
+    "oems_nf2ff_surface": (c_i32, [c_i32, ctypes.POINTER(c_f64), c_u64, c_f64, ctypes.POINTER(Nf2ffRequestC),
+                                   ctypes.POINTER(Nf2ffResultC)]),
     "oems_engine_add_point_probe": (c_i32, [P, c_i32, c_u64 * 3, ctypes.POINTER(c_i32)]),
     "oems_engine_read_probe_traces": (c_i32, [P, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_u64)]),
     "oems_engine_add_probe": (c_i32, [P, ctypes.POINTER(ProbeTermC), c_u64, c_i32, ctypes.POINTER(c_i32)]),

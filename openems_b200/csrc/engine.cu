@@ -31,6 +31,7 @@
 #include "yee_tma.cuh"
 #include "mur.cuh"
 #include "lumped_ade.cuh"
+#include "fd_nf2ff.cuh"
 
 namespace oems {
 
@@ -275,6 +276,34 @@ struct RlcHost {
   DevBuf<float> d_vv, d_vil, d_int;
 };
 
+// Per-batch twiddle table of one frequency-domain recorder: [step][f][4] and
+// the steps that sample.
+struct FdTable {
+  DevBuf<double> tw;
+  DevBuf<int> sampled;
+  std::vector<double> h_tw;
+  std::vector<int> h_sampled;
+};
+
+struct FieldDftHost {
+  FieldDftArgs args{};
+  std::vector<double> freqs;
+  std::vector<int> comps;
+  uint32_t interval = 1;
+  std::unique_ptr<DevBuf<double>> acc{new DevBuf<double>};
+  std::unique_ptr<FdTable> tab{new FdTable};
+};
+
+struct Nf2ffHost {
+  Nf2ffAccArgs args{};
+  long long lo[3], hi[3];
+  int sign[6];
+  std::vector<double> freqs;
+  uint32_t interval = 1;
+  std::unique_ptr<DevBuf<double>> acc{new DevBuf<double>};
+  std::unique_ptr<FdTable> tab{new FdTable};
+};
+
 }  // namespace oems
 
 struct oems_engine {
@@ -300,6 +329,8 @@ struct oems_engine {
   oems::MurHost mur;
   std::vector<oems::DispHost> disp;
   oems::RlcHost rlc;
+  std::vector<oems::FieldDftHost> fdumps;
+  std::vector<oems::Nf2ffHost> boxes;
 
   // probes: term tables (host copies and device mirrors) and f64 traces
   std::vector<int> probe_off{0}, probe_mode, term_comp;
@@ -570,9 +601,33 @@ static cudaError_t launch_e(oems_engine* en) {
   return cudaGetLastError();
 }
 
-static bool need_post(const oems_engine* en) { return en->nexc > 0 || en->nprobe() > 0; }
+static int post_kernels(const oems_engine* en) {
+  return (en->nexc > 0 || en->nprobe() > 0 ? 1 : 0) + (int)en->fdumps.size() + (int)en->boxes.size();
+}
+static bool need_post(const oems_engine* en) { return post_kernels(en) > 0; }
+
+static cudaError_t launch_fd(oems_engine* en, int local) {
+  for (FieldDftHost& d : en->fdumps) {
+    FieldDftArgs a = d.args;
+    a.tw = d.tab->tw.p;
+    a.sampled = d.tab->sampled.p;
+    a.d_base = en->d_base.p;
+    a.local = local;
+    k_field_dft<<<(int)((a.npts + 255) / 256), 256, 0, en->stream>>>(a);
+  }
+  for (Nf2ffHost& b : en->boxes) {
+    Nf2ffAccArgs a = b.args;
+    a.tw = b.tab->tw.p;
+    a.sampled = b.tab->sampled.p;
+    a.d_base = en->d_base.p;
+    a.local = local;
+    k_nf2ff_acc<<<(int)((a.off[a.nfaces] + 255) / 256), 256, 0, en->stream>>>(a);
+  }
+  return cudaGetLastError();
+}
 
 static cudaError_t launch_post(oems_engine* en, int local) {
+  if (en->nexc == 0 && en->nprobe() == 0) return launch_fd(en, local);
   PostArgs a{};
   for (int c = 0; c < 3; ++c) {
     a.e[c] = en->E(c);
@@ -594,7 +649,9 @@ static cudaError_t launch_post(oems_engine* en, int local) {
   a.d_base = en->d_base.p;
   a.local = local;
   k_post_step<<<1, 128, 0, en->stream>>>(a);
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_fd(en, local);
 }
 
 // Extension kernels between the H and E updates (Mur pre) and after the E
@@ -637,7 +694,7 @@ static int ext_kernels(const oems_engine* en) {
   return (en->mur.on ? 3 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
 }
 
-static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + (need_post(en) ? 1 : 0); }
+static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + post_kernels(en); }
 
 // Launches `steps` timesteps directly (no graph).
 static oems_status launch_steps_direct(oems_engine* en, int steps) {
@@ -1074,6 +1131,45 @@ static oems_status upload_excitations(oems_engine* en, const oems_batch* b) {
   return OEMS_OK;
 }
 
+// Twiddles of the steps of the next batch: the sample after batch step s is
+// timestep t = t0 + s + 1; it is taken when t is a multiple of `interval`,
+// with exp(-j 2 pi f t dt) and exp(-j 2 pi f (t - 1/2) dt) times 2 dt interval
+// (src/processing/fields_fd.rs:156-167), evaluated with the host libm.
+static oems_status fill_twiddles(oems_engine* en, FdTable* T, const std::vector<double>& freqs,
+                                 uint32_t interval, uint64_t steps) {
+  const size_t nf = freqs.size(), ns = (size_t)std::max<uint64_t>(steps, 1);
+  if (ns * nf * 4 * sizeof(double) > ((size_t)1 << 30))
+    return fail(OEMS_ERR_CONFIG, "frequency-domain twiddle table above 1 GiB: use shorter batches");
+  T->h_tw.assign(ns * nf * 4, 0.0);
+  T->h_sampled.assign(ns, 0);
+  const double scale = 2.0 * en->dt * (double)interval;
+  for (uint64_t st = 0; st < steps; ++st) {
+    const uint64_t t = en->timestep + st + 1;
+    if (t % interval != 0) continue;
+    T->h_sampled[st] = 1;
+    double* w = T->h_tw.data() + st * nf * 4;
+    for (size_t f = 0; f < nf; ++f) {
+      const double pe = -2.0 * 3.14159265358979323846 * freqs[f] * ((double)t * en->dt);
+      const double ph = -2.0 * 3.14159265358979323846 * freqs[f] * (((double)t - 0.5) * en->dt);
+      w[4 * f] = std::cos(pe) * scale;
+      w[4 * f + 1] = std::sin(pe) * scale;
+      w[4 * f + 2] = std::cos(ph) * scale;
+      w[4 * f + 3] = std::sin(ph) * scale;
+    }
+  }
+  if (T->tw.n < T->h_tw.size() || T->sampled.n < ns) {
+    OEMS_CUDA(T->tw.ensure(T->h_tw.size()));
+    OEMS_CUDA(T->sampled.ensure(ns));
+    en->graph_epoch++;
+  }
+  OEMS_CUDA(cudaMemcpyAsync(T->tw.p, T->h_tw.data(), T->h_tw.size() * sizeof(double), cudaMemcpyHostToDevice,
+                            en->stream));
+  OEMS_CUDA(cudaMemcpyAsync(T->sampled.p, T->h_sampled.data(), ns * sizeof(int), cudaMemcpyHostToDevice,
+                            en->stream));
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  return OEMS_OK;
+}
+
 static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_result* r) {
   if (!b || !r) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL batch or result");
   DeviceGuard guard(en->device);
@@ -1092,6 +1188,8 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
       en->graph_epoch++;
     }
   }
+  for (FieldDftHost& d : en->fdumps) OEMS_TRY(fill_twiddles(en, d.tab.get(), d.freqs, d.interval, steps));
+  for (Nf2ffHost& x : en->boxes) OEMS_TRY(fill_twiddles(en, x.tab.get(), x.freqs, x.interval, steps));
   const uint64_t si = b->sample_interval, ci = b->check_interval;
   const bool has_decay = b->has_energy_decay_db != 0;
   // worst-case number of energy samples this batch can take
@@ -1461,6 +1559,10 @@ oems_status oems_engine_reset(oems_engine* engine) {
     OEMS_CUDA(cudaMemsetAsync(d.state->p, 0, d.state->n * sizeof(float), engine->stream));
   if (!engine->rlc.q.empty())
     OEMS_CUDA(cudaMemsetAsync(engine->rlc.d_int.p, 0, engine->rlc.q.size() * sizeof(float), engine->stream));
+  for (auto& d : engine->fdumps)
+    OEMS_CUDA(cudaMemsetAsync(d.acc->p, 0, d.acc->n * sizeof(double), engine->stream));
+  for (auto& x : engine->boxes)
+    OEMS_CUDA(cudaMemsetAsync(x.acc->p, 0, x.acc->n * sizeof(double), engine->stream));
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   engine->timestep = 0;
   engine->traces_steps = 0;
@@ -1574,6 +1676,323 @@ oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rl
   OEMS_CUDA(cudaMemset(R.d_int.p, 0, k * sizeof(float)));
   engine->graph_epoch++;
   return OEMS_OK;
+}
+
+oems_status oems_engine_add_field_dft(oems_engine* engine, const oems_field_dft_desc* d, const double* freqs,
+                                      uint32_t nfreq, int32_t* dump_id) {
+  if (!engine || !d || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "a field DFT needs at least one frequency");
+  if ((d->components & 0x3Fu) == 0 || (d->components & ~0x3Fu))
+    return fail(OEMS_ERR_CONFIG, "field DFT components must be a non-empty mask of bits 0..5");
+  DeviceGuard guard(engine->device);
+  FieldDftHost h;
+  FieldDftArgs& A = h.args;
+  const long long ext[3] = {engine->nx, engine->ny, engine->nz};
+  long long r[6], ss[3], n[3];
+  A.npts = 1;
+  for (int a = 0; a < 3; ++a) {
+    r[2 * a] = (long long)std::min<uint64_t>(d->region[2 * a], (uint64_t)ext[a]);
+    r[2 * a + 1] = (long long)std::min<uint64_t>(d->region[2 * a + 1], (uint64_t)ext[a]);
+    ss[a] = std::max<uint32_t>(d->sub_sample[a], 1u);
+    const long long len = std::max(r[2 * a + 1] - r[2 * a], 0LL);
+    n[a] = (len + ss[a] - 1) / ss[a];
+    A.npts *= n[a];
+  }
+  if (A.npts == 0) return fail(OEMS_ERR_CONFIG, "field DFT region is empty");
+  for (int c = 0; c < 6; ++c)
+    if (d->components >> c & 1u) {
+      A.f[h.comps.size()] = c < 3 ? engine->E(c) : engine->H(c - 3);
+      if (c >= 3) A.hmask |= 1u << h.comps.size();
+      h.comps.push_back(c);
+    }
+  A.ncomp = (int)h.comps.size();
+  A.nf = (int)nfreq;
+  A.n1 = n[1];
+  A.n2 = n[2];
+  A.r0 = r[0];
+  A.r1 = r[2];
+  A.r2 = r[4];
+  A.s0 = ss[0];
+  A.s1 = ss[1];
+  A.s2 = ss[2];
+  A.ny = engine->ny;
+  A.nzp = engine->g.nzp;
+  h.freqs.assign(freqs, freqs + nfreq);
+  h.interval = std::max<uint32_t>(d->interval, 1u);
+  const size_t nacc = 2 * (size_t)nfreq * A.ncomp * (size_t)A.npts;
+  OEMS_CUDA(h.acc->ensure(nacc));
+  OEMS_CUDA(cudaMemset(h.acc->p, 0, nacc * sizeof(double)));
+  A.acc = reinterpret_cast<double2*>(h.acc->p);
+  if (!engine->d_base.p) OEMS_CUDA(engine->d_base.ensure(1));
+  engine->fdumps.push_back(std::move(h));
+  engine->graph_epoch++;
+  if (dump_id) *dump_id = (int32_t)engine->fdumps.size() - 1;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_field_dft(oems_engine* engine, int32_t id, uint32_t f, uint32_t component,
+                                       double* out, uint64_t npoints) {
+  if (!engine || !out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (id < 0 || id >= (int32_t)engine->fdumps.size()) return fail(OEMS_ERR_CONFIG, "unknown field DFT id");
+  const FieldDftHost& h = engine->fdumps[id];
+  if (f >= h.freqs.size()) return fail(OEMS_ERR_CONFIG, "frequency index out of range");
+  const auto it = std::find(h.comps.begin(), h.comps.end(), (int)component);
+  if (it == h.comps.end()) return fail(OEMS_ERR_CONFIG, "component not recorded by this field DFT");
+  if (npoints < (uint64_t)h.args.npts) return fail(OEMS_ERR_INVALID_ARGUMENT, "output buffer too small");
+  DeviceGuard guard(engine->device);
+  const size_t slot = it - h.comps.begin();
+  const size_t off = 2 * ((size_t)f * h.comps.size() + slot) * (size_t)h.args.npts;
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  OEMS_CUDA(cudaMemcpy(out, h.acc->p + off, 2 * (size_t)h.args.npts * sizeof(double), cudaMemcpyDeviceToHost));
+  return OEMS_OK;
+}
+
+oems_status oems_engine_add_nf2ff_box(oems_engine* engine, const oems_nf2ff_box_desc* d, const double* freqs,
+                                      uint32_t nfreq, int32_t* box_id) {
+  if (!engine || !d || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "an NF2FF box needs at least one frequency");
+  const long long ext[3] = {engine->nx, engine->ny, engine->nz};
+  for (int a = 0; a < 3; ++a)
+    if (d->start[a] < 1 || d->stop[a] <= d->start[a] || d->stop[a] > (uint64_t)ext[a] - 1)
+      return fail(OEMS_ERR_CONFIG, "NF2FF box must satisfy 1 <= start < stop <= n - 1 on every axis");
+  DeviceGuard guard(engine->device);
+  Nf2ffHost h;
+  Nf2ffAccArgs& A = h.args;
+  for (int a = 0; a < 3; ++a) {
+    h.lo[a] = (long long)d->start[a];
+    h.hi[a] = (long long)d->stop[a];
+  }
+  size_t total = 0;
+  A.off[0] = 0;
+  for (int f = 0; f < 6; ++f) {
+    if (!d->directions[f]) continue;
+    Nf2ffFace& F = A.face[A.nfaces];
+    F.a = f / 2;
+    F.b = (F.a + 1) % 3;
+    F.c = (F.a + 2) % 3;
+    F.p = (f & 1) ? h.hi[F.a] : h.lo[F.a];
+    F.lo_b = h.lo[F.b];
+    F.lo_c = h.lo[F.c];
+    F.nb = h.hi[F.b] - h.lo[F.b] + 1;
+    F.nc = h.hi[F.c] - h.lo[F.c] + 1;
+    F.np = F.nb * F.nc;
+    h.sign[A.nfaces] = (f & 1) ? 1 : -1;
+    total += (size_t)F.np;
+    A.nfaces++;
+    A.off[A.nfaces] = (long long)total;
+  }
+  if (A.nfaces == 0) return fail(OEMS_ERR_CONFIG, "NF2FF box has no face enabled");
+  const size_t nacc = 8 * (size_t)nfreq * total;  // 4 complex values per point and frequency
+  OEMS_CUDA(h.acc->ensure(nacc));
+  OEMS_CUDA(cudaMemset(h.acc->p, 0, nacc * sizeof(double)));
+  size_t off = 0;
+  for (int i = 0; i < A.nfaces; ++i) {
+    A.face[i].acc = reinterpret_cast<double2*>(h.acc->p + off);
+    off += 8 * (size_t)nfreq * (size_t)A.face[i].np;
+  }
+  for (int c = 0; c < 3; ++c) {
+    A.e[c] = engine->E(c);
+    A.h[c] = engine->H(c);
+  }
+  A.ny = engine->ny;
+  A.nzp = engine->g.nzp;
+  A.nf = (int)nfreq;
+  h.freqs.assign(freqs, freqs + nfreq);
+  h.interval = std::max<uint32_t>(d->interval, 1u);
+  if (!engine->d_base.p) OEMS_CUDA(engine->d_base.ensure(1));
+  engine->boxes.push_back(std::move(h));
+  engine->graph_epoch++;
+  if (box_id) *box_id = (int32_t)engine->boxes.size() - 1;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_nf2ff_face(oems_engine* engine, int32_t id, uint32_t face, uint32_t f, double* out,
+                                        uint64_t cap_doubles, uint64_t* npoints) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  if (id < 0 || id >= (int32_t)engine->boxes.size()) return fail(OEMS_ERR_CONFIG, "unknown NF2FF box id");
+  const Nf2ffHost& h = engine->boxes[id];
+  if (f >= h.freqs.size() || face > 5) return fail(OEMS_ERR_CONFIG, "face or frequency index out of range");
+  for (int i = 0; i < h.args.nfaces; ++i) {
+    const Nf2ffFace& F = h.args.face[i];
+    if (2 * F.a + (h.sign[i] > 0 ? 1 : 0) != (int)face) continue;
+    if (npoints) *npoints = (uint64_t)F.np;
+    if (!out) return OEMS_OK;
+    if (cap_doubles < 8 * (uint64_t)F.np) return fail(OEMS_ERR_INVALID_ARGUMENT, "output buffer too small");
+    DeviceGuard guard(engine->device);
+    OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+    OEMS_CUDA(cudaMemcpy(out, F.acc + (size_t)f * 4 * F.np, 8 * (size_t)F.np * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    return OEMS_OK;
+  }
+  return fail(OEMS_ERR_CONFIG, "face not recorded by this NF2FF box");
+}
+
+// Far field of a device point list on `stream`: directions over the theta x
+// phi grid, radiation vectors on the GPU, then E_theta / E_phi, P_rad, Prad
+// and Dmax on the host (python/openEMS/nf2ff.py:178-220 result fields).
+static oems_status far_field(cudaStream_t stream, const double* d_pts, long long npts, double freq,
+                             const oems_nf2ff_request* q, oems_nf2ff_result* res) {
+  const long long nt = (long long)q->ntheta, np = (long long)q->nphi, ndir = nt * np;
+  if (ndir > (1LL << 24)) return fail(OEMS_ERR_CONFIG, "too many far-field directions");
+  std::vector<double> dirs(3 * ndir);
+  for (long long i = 0; i < nt; ++i)
+    for (long long j = 0; j < np; ++j) {
+      const double th = q->theta[i], ph = q->phi[j];
+      double* r = dirs.data() + 3 * (i * np + j);
+      r[0] = std::sin(th) * std::cos(ph);
+      r[1] = std::sin(th) * std::sin(ph);
+      r[2] = std::cos(th);
+    }
+  const int dir_blocks = (int)((ndir + kFarThreads - 1) / kFarThreads);
+  long long nchunks = std::max<long long>(1, (4 * 148 + dir_blocks - 1) / dir_blocks);
+  nchunks = std::min<long long>(nchunks, std::max<long long>(1, (npts + kFarTile - 1) / kFarTile));
+  nchunks = std::min<long long>(nchunks, 65535);
+  long long chunk = (npts + nchunks - 1) / nchunks;
+  chunk = (chunk + kFarTile - 1) / kFarTile * kFarTile;
+  nchunks = (npts + chunk - 1) / chunk;
+  DevBuf<double> d_dirs, d_partial, d_nl;
+  OEMS_CUDA(d_dirs.ensure(3 * ndir));
+  OEMS_CUDA(d_partial.ensure((size_t)nchunks * ndir * 12));
+  OEMS_CUDA(d_nl.ensure((size_t)ndir * 12));
+  OEMS_CUDA(cudaMemcpyAsync(d_dirs.p, dirs.data(), dirs.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+  const double k = 2.0 * 3.14159265358979323846 * freq / 299792458.0;
+  Nf2ffFarArgs a{};
+  a.pts = d_pts;
+  a.npts = npts;
+  a.chunk = chunk;
+  a.dirs = d_dirs.p;
+  a.ndir = (int)ndir;
+  a.k = k;
+  a.cx = q->center[0];
+  a.cy = q->center[1];
+  a.cz = q->center[2];
+  a.partial = d_partial.p;
+  k_nf2ff_far<<<dim3(dir_blocks, (unsigned)nchunks), kFarThreads, 0, stream>>>(a);
+  OEMS_CUDA(cudaGetLastError());
+  k_nf2ff_reduce<<<(int)((ndir * 12 + 255) / 256), 256, 0, stream>>>(d_partial.p, (int)nchunks, (int)ndir, d_nl.p);
+  OEMS_CUDA(cudaGetLastError());
+  std::vector<double> nl((size_t)ndir * 12);
+  OEMS_CUDA(cudaMemcpyAsync(nl.data(), d_nl.p, nl.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  OEMS_CUDA(cudaStreamSynchronize(stream));
+  const double eta = 376.730313668, R = q->radius, pi = 3.14159265358979323846;
+  // fac = j k exp(-j k R) / (4 pi R)
+  const double g = k / (4.0 * pi * R);
+  const double fr = g * std::sin(k * R), fi = g * std::cos(k * R);
+  double pmax = 0.0, prad = 0.0;
+  auto trap = [](const double* x, long long n, long long i) {
+    if (n < 2) return 0.0;
+    if (i == 0) return 0.5 * (x[1] - x[0]);
+    if (i == n - 1) return 0.5 * (x[n - 1] - x[n - 2]);
+    return 0.5 * (x[i + 1] - x[i - 1]);
+  };
+  for (long long i = 0; i < nt; ++i)
+    for (long long j = 0; j < np; ++j) {
+      const long long dI = i * np + j;
+      const double th = q->theta[i], ph = q->phi[j];
+      const double tv[3] = {std::cos(th) * std::cos(ph), std::cos(th) * std::sin(ph), -std::sin(th)};
+      const double pv[3] = {-std::sin(ph), std::cos(ph), 0.0};
+      const double* v = nl.data() + 12 * dI;
+      double Nt[2] = {0, 0}, Np[2] = {0, 0}, Lt[2] = {0, 0}, Lp[2] = {0, 0};
+      for (int c = 0; c < 3; ++c) {
+        Nt[0] += v[2 * c] * tv[c];
+        Nt[1] += v[2 * c + 1] * tv[c];
+        Np[0] += v[2 * c] * pv[c];
+        Np[1] += v[2 * c + 1] * pv[c];
+        Lt[0] += v[6 + 2 * c] * tv[c];
+        Lt[1] += v[7 + 2 * c] * tv[c];
+        Lp[0] += v[6 + 2 * c] * pv[c];
+        Lp[1] += v[7 + 2 * c] * pv[c];
+      }
+      // E_theta = -fac (L_phi + eta N_theta); E_phi = fac (L_theta - eta N_phi)
+      const double ar = Lp[0] + eta * Nt[0], ai = Lp[1] + eta * Nt[1];
+      const double br = Lt[0] - eta * Np[0], bi = Lt[1] - eta * Np[1];
+      const double etr = -(fr * ar - fi * ai), eti = -(fr * ai + fi * ar);
+      const double epr = fr * br - fi * bi, epi = fr * bi + fi * br;
+      if (res->e_theta) {
+        res->e_theta[2 * dI] = etr;
+        res->e_theta[2 * dI + 1] = eti;
+      }
+      if (res->e_phi) {
+        res->e_phi[2 * dI] = epr;
+        res->e_phi[2 * dI + 1] = epi;
+      }
+      const double p = (etr * etr + eti * eti + epr * epr + epi * epi) / (2.0 * eta);
+      if (res->p_rad) res->p_rad[dI] = p;
+      pmax = std::max(pmax, p);
+      prad += p * R * R * std::sin(th) * trap(q->theta, nt, i) * trap(q->phi, np, j);
+    }
+  res->prad = prad;
+  res->dmax = prad > 0.0 ? 4.0 * pi * R * R * pmax / prad : 0.0;
+  return OEMS_OK;
+}
+
+static oems_status check_request(const oems_nf2ff_request* q, double freq) {
+  if (!q || !q->theta || !q->phi) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL far-field request");
+  if (q->ntheta == 0 || q->nphi == 0) return fail(OEMS_ERR_CONFIG, "empty theta or phi grid");
+  if (!(q->radius > 0.0)) return fail(OEMS_ERR_CONFIG, "far-field radius must be positive");
+  if (!(freq > 0.0)) return fail(OEMS_ERR_CONFIG, "frequency must be positive");
+  return OEMS_OK;
+}
+
+oems_status oems_engine_nf2ff(oems_engine* engine, int32_t id, uint32_t f, const oems_nf2ff_request* q,
+                              oems_nf2ff_result* res) {
+  if (!engine || !res) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (id < 0 || id >= (int32_t)engine->boxes.size()) return fail(OEMS_ERR_CONFIG, "unknown NF2FF box id");
+  const Nf2ffHost& h = engine->boxes[id];
+  if (f >= h.freqs.size()) return fail(OEMS_ERR_CONFIG, "frequency index out of range");
+  OEMS_TRY(check_request(q, h.freqs[f]));
+  DeviceGuard guard(engine->device);
+  const long long ext[3] = {engine->nx, engine->ny, engine->nz};
+  DevBuf<double> d_lines[3];
+  Nf2ffPointsArgs P{};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> l(ext[a] + 1);
+    for (long long i = 0; i <= ext[a]; ++i) l[i] = q->lines[a] ? q->lines[a][i] : (double)i * engine->delta[a];
+    OEMS_CUDA(d_lines[a].ensure(l.size()));
+    OEMS_CUDA(cudaMemcpy(d_lines[a].p, l.data(), l.size() * sizeof(double), cudaMemcpyHostToDevice));
+    P.lines[a] = d_lines[a].p;
+  }
+  P.nfaces = h.args.nfaces;
+  P.off[0] = 0;
+  for (int i = 0; i < P.nfaces; ++i) {
+    P.face[i] = h.args.face[i];
+    P.sign[i] = h.sign[i];
+    const Nf2ffFace& F = P.face[i];
+    P.off[i + 1] = P.off[i] + F.nb * (F.nc - 1) + (F.nb - 1) * F.nc;
+  }
+  P.f = (int)f;
+  const long long npts = P.off[P.nfaces];
+  DevBuf<double> pts;
+  OEMS_CUDA(pts.ensure((size_t)npts * 16));
+  P.pts = pts.p;
+  k_nf2ff_points<<<(int)((npts + 255) / 256), 256, 0, engine->stream>>>(P);
+  OEMS_CUDA(cudaGetLastError());
+  return far_field(engine->stream, pts.p, npts, h.freqs[f], q, res);
+}
+
+oems_status oems_nf2ff_surface(int32_t device, const double* points, uint64_t npoints, double freq,
+                               const oems_nf2ff_request* q, oems_nf2ff_result* res) {
+  if (!points || !res) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (npoints == 0) return fail(OEMS_ERR_CONFIG, "empty point list");
+  OEMS_TRY(check_request(q, freq));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(OEMS_ERR_NO_DEVICE, "no CUDA device");
+  int dev = device;
+  if (dev < 0) OEMS_CUDA(cudaGetDevice(&dev));
+  DeviceGuard guard(dev);
+  cudaStream_t stream = nullptr;
+  OEMS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  oems_status st = OEMS_OK;
+  {
+    DevBuf<double> pts;
+    cudaError_t e = pts.ensure((size_t)npoints * 16);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(pts.p, points, (size_t)npoints * 16 * sizeof(double), cudaMemcpyHostToDevice);
+    st = e == cudaSuccess ? far_field(stream, pts.p, (long long)npoints, freq, q, res)
+                          : fail(OEMS_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaStreamDestroy(stream);
+  return st;
 }
 
 oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc) {

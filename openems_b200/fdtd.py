@@ -683,6 +683,145 @@ class BatchResult:
 # ---------------------------------------------------------------------------
 
 
+def _request(theta, phi, radius, center, lines, keep):
+    th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+    ph = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+    keep += [th, ph]
+    q = N.Nf2ffRequestC()
+    q.theta = th.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    q.ntheta = len(th)
+    q.phi = ph.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    q.nphi = len(ph)
+    q.radius = float(radius)
+    for a in range(3):
+        q.center[a] = float(center[a])
+        if lines is not None and lines[a] is not None:
+            la = np.ascontiguousarray(lines[a], dtype=np.float64)
+            keep.append(la)
+            q.lines[a] = la.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    return q, len(th), len(ph)
+
+
+def _result(nt, np_, keep):
+    et = np.zeros(2 * nt * np_)
+    ep = np.zeros(2 * nt * np_)
+    pr = np.zeros(nt * np_)
+    keep += [et, ep, pr]
+    r = N.Nf2ffResultC()
+    r.e_theta = et.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    r.e_phi = ep.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    r.p_rad = pr.ctypes.data_as(ctypes.POINTER(N.c_f64))
+    return r, et, ep, pr
+
+
+@dataclass
+class Nf2ffResults:
+    """nf2ff_results (python/openEMS/nf2ff.py:167-220): per frequency
+    E_theta, E_phi, E_norm, E_cprh, E_cplh, P_rad (ntheta x nphi) and Dmax,
+    Prad; theta / phi in radians, r the observation radius (m)."""
+
+    theta: np.ndarray
+    phi: np.ndarray
+    r: float
+    freq: np.ndarray
+    E_theta: List[np.ndarray] = field(default_factory=list)
+    E_phi: List[np.ndarray] = field(default_factory=list)
+    E_norm: List[np.ndarray] = field(default_factory=list)
+    E_cprh: List[np.ndarray] = field(default_factory=list)
+    E_cplh: List[np.ndarray] = field(default_factory=list)
+    P_rad: List[np.ndarray] = field(default_factory=list)
+    Dmax: List[float] = field(default_factory=list)
+    Prad: List[float] = field(default_factory=list)
+
+    def _append(self, et, ep, pr, nt, np_, prad, dmax):
+        Et = (et[0::2] + 1j * et[1::2]).reshape(nt, np_)
+        Ep = (ep[0::2] + 1j * ep[1::2]).reshape(nt, np_)
+        _, PHI = np.meshgrid(self.theta, self.phi, indexing="ij")
+        self.E_theta.append(Et)
+        self.E_phi.append(Ep)
+        self.E_norm.append(np.sqrt(np.abs(Et) ** 2 + np.abs(Ep) ** 2))
+        self.E_cprh.append((np.cos(PHI) + 1j * np.sin(PHI)) * (Et + 1j * Ep) / np.sqrt(2.0))
+        self.E_cplh.append((np.cos(PHI) - 1j * np.sin(PHI)) * (Et - 1j * Ep) / np.sqrt(2.0))
+        self.P_rad.append(pr.reshape(nt, np_))
+        self.Prad.append(prad)
+        self.Dmax.append(dmax)
+
+
+class Nf2ffBox:
+    """nf2ff recording box (python/openEMS/nf2ff.py:26-97) with
+    frequency-domain recording on an engine; start / stop are node planes
+    (cell indices) with 1 <= start < stop <= n - 1."""
+
+    def __init__(self, engine: "Engine", start, stop, frequency, directions=(True,) * 6,
+                 interval: int = 1, name: str = "nf2ff"):
+        self.engine = engine
+        self.name = name
+        self.start = tuple(int(v) for v in start)
+        self.stop = tuple(int(v) for v in stop)
+        self.freq = np.atleast_1d(np.asarray(frequency, dtype=np.float64))
+        self.directions = tuple(bool(v) for v in directions)
+        d = N.Nf2ffBoxDescC()
+        for a in range(3):
+            d.start[a], d.stop[a] = self.start[a], self.stop[a]
+        for f in range(6):
+            d.directions[f] = int(self.directions[f])
+        d.interval = int(interval)
+        bid = N.c_i32()
+        N.check(N.lib().oems_engine_add_nf2ff_box(engine.handle, ctypes.byref(d),
+                                                  self.freq.ctypes.data_as(ctypes.POINTER(N.c_f64)),
+                                                  len(self.freq), ctypes.byref(bid)))
+        self.box_id = bid.value
+
+    def face(self, face: int, freq_index: int) -> np.ndarray:
+        """Raw accumulators (4, nb, nc) = Eb, Ec, Hb, Hc of one face."""
+        a = face // 2
+        b, c = (a + 1) % 3, (a + 2) % 3
+        nb, nc = self.stop[b] - self.start[b] + 1, self.stop[c] - self.start[c] + 1
+        out = np.zeros(8 * nb * nc)
+        N.check(N.lib().oems_engine_read_nf2ff_face(self.engine.handle, self.box_id, face, freq_index,
+                                                    out.ctypes.data_as(ctypes.POINTER(N.c_f64)),
+                                                    len(out), None))
+        return (out[0::2] + 1j * out[1::2]).reshape(4, nb, nc)
+
+    def calc_nf2ff(self, freq, theta, phi, radius=1.0, center=(0.0, 0.0, 0.0), lines=None,
+                   degrees=True) -> Nf2ffResults:
+        """CalcNF2FF (python/openEMS/nf2ff.py:98-165): freq one or several of
+        the recorded frequencies; theta / phi in degrees unless degrees=False;
+        lines: mesh lines in metres per axis (default: uniform cells)."""
+        th = np.deg2rad(theta) if degrees else np.asarray(theta, dtype=np.float64)
+        ph = np.deg2rad(phi) if degrees else np.asarray(phi, dtype=np.float64)
+        th, ph = np.atleast_1d(th).astype(np.float64), np.atleast_1d(ph).astype(np.float64)
+        freqs = np.atleast_1d(np.asarray(freq, dtype=np.float64))
+        res = Nf2ffResults(th, ph, float(radius), freqs)
+        for f in freqs:
+            hit = np.nonzero(np.isclose(self.freq, f, rtol=1e-9, atol=0))[0]
+            if len(hit) == 0:
+                raise N.ConfigError(f"frequency {f} is not recorded by this NF2FF box")
+            keep = []
+            q, nt, np_ = _request(th, ph, radius, center, lines, keep)
+            r, et, ep, pr = _result(nt, np_, keep)
+            N.check(N.lib().oems_engine_nf2ff(self.engine.handle, self.box_id, int(hit[0]),
+                                              ctypes.byref(q), ctypes.byref(r)))
+            res._append(et, ep, pr, nt, np_, r.prad, r.dmax)
+        return res
+
+
+def nf2ff_surface(points: np.ndarray, freq: float, theta, phi, radius=1.0, center=(0.0, 0.0, 0.0),
+                  device: int = -1) -> Nf2ffResults:
+    """Far field of a point list (n, 16): x y z weight, J (re, im) x 3,
+    M (re, im) x 3; theta / phi in radians."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 16)
+    th, ph = np.atleast_1d(theta).astype(np.float64), np.atleast_1d(phi).astype(np.float64)
+    keep = []
+    q, nt, np_ = _request(th, ph, radius, center, None, keep)
+    r, et, ep, pr = _result(nt, np_, keep)
+    N.check(N.lib().oems_nf2ff_surface(device, pts.ctypes.data_as(ctypes.POINTER(N.c_f64)), len(pts),
+                                       float(freq), ctypes.byref(q), ctypes.byref(r)))
+    res = Nf2ffResults(th, ph, float(radius), np.array([freq]))
+    res._append(et, ep, pr, nt, np_, r.prad, r.dmax)
+    return res
+
+
 class EngineType(enum.Enum):
     """The engine is CUDA-only; `Cuda` is the single implementation."""
 
@@ -805,6 +944,43 @@ class Engine:
         N.check(N.lib().oems_engine_read_probe_dft(self._h, dft_id,
                                                    out.ctypes.data_as(ctypes.POINTER(N.c_f64))))
         return out[0::2] + 1j * out[1::2]
+
+    def add_field_dft(self, region, freqs, components=0x3F, sub_sample=(1, 1, 1), interval=1) -> int:
+        """Frequency-domain field dump (FrequencyDomainFieldDump) over the
+        half-open region (i0, i1, j0, j1, k0, k1); components is a bit mask or
+        "E" / "H" / "EH"."""
+        if isinstance(components, str):
+            components = {"E": 0x07, "H": 0x38, "EH": 0x3F, "HE": 0x3F}[components]
+        d = N.FieldDftDescC()
+        for a in range(6):
+            d.region[a] = int(region[a])
+        for a in range(3):
+            d.sub_sample[a] = int(sub_sample[a])
+        d.components = int(components)
+        d.interval = int(interval)
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        did = N.c_i32()
+        N.check(N.lib().oems_engine_add_field_dft(self._h, ctypes.byref(d),
+                                                  f.ctypes.data_as(ctypes.POINTER(N.c_f64)), len(f),
+                                                  ctypes.byref(did)))
+        ext = self.dims
+        shape = []
+        for a in range(3):
+            lo, hi = min(int(region[2 * a]), ext[a]), min(int(region[2 * a + 1]), ext[a])
+            ss = max(int(sub_sample[a]), 1)
+            shape.append((max(hi - lo, 0) + ss - 1) // ss)
+        self._fd_shapes = getattr(self, "_fd_shapes", {})
+        self._fd_shapes[did.value] = tuple(shape)
+        return did.value
+
+    def field_dft(self, dump_id: int, freq_index: int, component: int) -> np.ndarray:
+        """Complex accumulator of one component, shape of the sub-sampled region."""
+        shape = self._fd_shapes[dump_id]
+        n = int(np.prod(shape))
+        out = np.zeros(2 * n, dtype=np.float64)
+        N.check(N.lib().oems_engine_read_field_dft(self._h, dump_id, freq_index, component,
+                                                   out.ctypes.data_as(ctypes.POINTER(N.c_f64)), n))
+        return (out[0::2] + 1j * out[1::2]).reshape(shape)
 
     def run_batch(self, batch: EngineBatch) -> BatchResult:
         num_steps = batch.num_steps

@@ -96,6 +96,15 @@ def lib() -> ctypes.CDLL:
         L.orc_add_lumped_rlc.argtypes = [P, P, I32, I32, D, D, D]
         L.orc_set_lumped.restype = D
         L.orc_set_lumped.argtypes = [P, P, I32, D, D, D, D]
+        L.orc_add_field_dft.restype = I32
+        L.orc_add_field_dft.argtypes = [P, P, P, ctypes.c_uint32, P, I64, U64]
+        L.orc_field_dft_points.restype = I64
+        L.orc_field_dft_points.argtypes = [P, I32]
+        L.orc_get_field_dft.argtypes = [P, I32, I64, I64, P]
+        L.orc_add_nf2ff_box.restype = I32
+        L.orc_add_nf2ff_box.argtypes = [P, P, P, P, P, I64, U64]
+        L.orc_get_nf2ff_face.restype = I64
+        L.orc_get_nf2ff_face.argtypes = [P, I32, I32, I64, P]
         L.orc_run_batch.restype = I32
         L.orc_run_batch.argtypes = [P, U64, U64, I32, U64, I32, D, D, ctypes.POINTER(BatchResult)]
         L.orc_get_energy_samples.argtypes = [P, ctypes.POINTER(EnergySample), U64]
@@ -272,6 +281,44 @@ class OracleSim:
     def set_lumped(self, pos, direction, r=0.0, c=0.0, eps_r=1.0, sigma=0.0):
         q = np.ascontiguousarray(pos, dtype=np.int64)
         return lib().orc_set_lumped(self._h, _ptr(q), int(direction), r, c, eps_r, sigma)
+
+    def add_field_dft(self, region, freqs, comp_mask=0x3F, sub_sample=(1, 1, 1), interval=1):
+        r = np.ascontiguousarray(region, dtype=np.int64)
+        ss = np.ascontiguousarray(sub_sample, dtype=np.int64)
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        did = lib().orc_add_field_dft(self._h, _ptr(r), _ptr(ss), comp_mask, _ptr(f), len(f), interval)
+        self._fd = getattr(self, "_fd", {})
+        self._fd[did] = (len(f), [c for c in range(6) if comp_mask >> c & 1])
+        return did
+
+    def field_dft(self, did, f, comp):
+        """Complex accumulator of component comp (0..5) at frequency index f."""
+        n = lib().orc_field_dft_points(self._h, did)
+        out = np.zeros(2 * n)
+        lib().orc_get_field_dft(self._h, did, f, self._fd[did][1].index(comp), _ptr(out))
+        return out[0::2] + 1j * out[1::2]
+
+    def add_nf2ff_box(self, lo, hi, freqs, directions=(1,) * 6, interval=1):
+        l3 = np.ascontiguousarray(lo, dtype=np.int64)
+        h3 = np.ascontiguousarray(hi, dtype=np.int64)
+        d6 = np.ascontiguousarray([int(bool(v)) for v in directions], dtype=np.int32)
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        bid = lib().orc_add_nf2ff_box(self._h, _ptr(l3), _ptr(h3), _ptr(d6), _ptr(f), len(f), interval)
+        if bid < 0:
+            raise ValueError("invalid NF2FF box")
+        return bid
+
+    def nf2ff_face(self, bid, face, f, lo, hi):
+        """(4, nb, nc) complex: Eb, Ec, Hb, Hc of one face at frequency index f."""
+        a = face // 2
+        b, c = (a + 1) % 3, (a + 2) % 3
+        nb, nc = hi[b] - lo[b] + 1, hi[c] - lo[c] + 1
+        out = np.zeros(8 * nb * nc)
+        n = lib().orc_get_nf2ff_face(self._h, bid, face, f, _ptr(out))
+        if n == 0:
+            return None
+        z = out[0::2] + 1j * out[1::2]
+        return z.reshape(4, nb, nc)
 
     def cpml_profile(self, face):
         out = np.zeros((6, 256))

@@ -106,6 +106,32 @@ struct Sim {
   };
   std::vector<ProbeDft> dfts;
 
+  // Frequency-domain field dump (src/processing/fields_fd.rs:31-217) over a
+  // half-open region with sub-sampling; components in ascending order.
+  // Accumulated when the timestep count is a multiple of `interval`, with
+  // scale 2 dt interval.  acc: [freq][component][point] (re, im).
+  struct FieldDft {
+    int64_t r[6], ss[3], n[3], npts;
+    std::vector<int> comps;
+    uint64_t interval;
+    std::vector<double> freqs, acc;
+  };
+  std::vector<FieldDft> fdumps;
+
+  // NF2FF box: per enabled face (-x +x -y +y -z +z) at node plane p of axis
+  // a, with b = a+1, c = a+2 (mod 3): Eb, Ec at plane p and Hb, Hc averaged
+  // over planes p-1 and p, on the face's node grid (nb x nc, b-major).
+  // acc: [face slot][freq][4][nb * nc] (re, im).
+  struct Nf2ffBox {
+    int64_t lo[3], hi[3];
+    int dirs[6];
+    uint64_t interval;
+    std::vector<double> freqs;
+    std::vector<int> faces;                 // enabled faces in order
+    std::vector<std::vector<double>> acc;   // per enabled face
+  };
+  std::vector<Nf2ffBox> boxes;
+
   std::vector<orc_energy_sample> energy;
 
   // CPML state
@@ -493,6 +519,75 @@ struct Sim {
     }
   }
 
+  // twiddle of one sample: exp(-j 2 pi f t) * scale (fields_fd.rs:163-167)
+  static void twiddle(double f, double t, double scale, double* re, double* im) {
+    const double ph = -2.0 * kPi * f * t;
+    *re = std::cos(ph) * scale;
+    *im = std::sin(ph) * scale;
+  }
+
+  void record_fd(uint64_t t_after) {
+    for (FieldDft& d : fdumps) {
+      if (t_after % d.interval != 0) continue;
+      const double scale = 2.0 * dt * (double)d.interval;
+      const size_t nc = d.comps.size();
+      for (size_t f = 0; f < d.freqs.size(); ++f) {
+        double tw[2][2];
+        twiddle(d.freqs[f], (double)t_after * dt, scale, &tw[0][0], &tw[0][1]);
+        twiddle(d.freqs[f], ((double)t_after - 0.5) * dt, scale, &tw[1][0], &tw[1][1]);
+        for (size_t ci = 0; ci < nc; ++ci) {
+          const int comp = d.comps[ci];
+          const double* w = tw[comp >= 3 ? 1 : 0];
+          double* acc = d.acc.data() + 2 * (f * nc + ci) * (size_t)d.npts;
+          int64_t p = 0;
+          for (int64_t a = 0; a < d.n[0]; ++a)
+            for (int64_t b = 0; b < d.n[1]; ++b)
+              for (int64_t c = 0; c < d.n[2]; ++c, ++p) {
+                const double x = (double)field_value(
+                    comp, idx(d.r[0] + a * d.ss[0], d.r[2] + b * d.ss[1], d.r[4] + c * d.ss[2]));
+                acc[2 * p] = acc[2 * p] + x * w[0];
+                acc[2 * p + 1] = acc[2 * p + 1] + x * w[1];
+              }
+        }
+      }
+    }
+    for (Nf2ffBox& B : boxes) {
+      if (t_after % B.interval != 0) continue;
+      const double scale = 2.0 * dt * (double)B.interval;
+      for (size_t fs = 0; fs < B.faces.size(); ++fs) {
+        const int face = B.faces[fs], a = face / 2, b = (a + 1) % 3, c = (a + 2) % 3;
+        const int64_t p = (face & 1) ? B.hi[a] : B.lo[a];
+        const int64_t nb = B.hi[b] - B.lo[b] + 1, ncc = B.hi[c] - B.lo[c] + 1, np = nb * ncc;
+        for (size_t f = 0; f < B.freqs.size(); ++f) {
+          double te[2], th[2];
+          twiddle(B.freqs[f], (double)t_after * dt, scale, &te[0], &te[1]);
+          twiddle(B.freqs[f], ((double)t_after - 0.5) * dt, scale, &th[0], &th[1]);
+          double* acc = B.acc[fs].data() + f * 8 * (size_t)np;
+          for (int64_t jb = 0; jb < nb; ++jb)
+            for (int64_t kc = 0; kc < ncc; ++kc) {
+              int64_t pos[3];
+              pos[a] = p;
+              pos[b] = B.lo[b] + jb;
+              pos[c] = B.lo[c] + kc;
+              const int64_t q = idx(pos[0], pos[1], pos[2]);
+              pos[a] = p - 1;
+              const int64_t qm = idx(pos[0], pos[1], pos[2]);
+              const double v[4] = {(double)E[b][q], (double)E[c][q],
+                                   0.5 * ((double)H[b][qm] + (double)H[b][q]),
+                                   0.5 * ((double)H[c][qm] + (double)H[c][q])};
+              const int64_t m = jb * ncc + kc;
+              for (int k = 0; k < 4; ++k) {
+                const double* w = k < 2 ? te : th;
+                double* z = acc + 2 * (k * np + m);
+                z[0] = z[0] + v[k] * w[0];
+                z[1] = z[1] + v[k] * w[1];
+              }
+            }
+        }
+      }
+    }
+  }
+
   int enable_mur(const int32_t* en, int order, double vphase) {
     const int64_t ext[3] = {nx, ny, nz};
     const double c = vphase > 0.0 ? vphase : kC0;
@@ -648,6 +743,7 @@ struct Sim {
       if (!rlc.empty()) apply_rlc();
       apply_excitations(step);
       record_probes(timestep + 1);
+      record_fd(timestep + 1);
       timestep += 1;
       executed += 1;
       if (sample_interval > 0 && cur % sample_interval == 0) {
@@ -814,6 +910,9 @@ void orc_reset(orc_sim* s) {
         std::fill(D.pp[c].begin(), D.pp[c].end(), T(0));
       }
     for (auto& r : S->rlc) r.i_int = T(0);
+    for (auto& d : S->fdumps) std::fill(d.acc.begin(), d.acc.end(), 0.0);
+    for (auto& B : S->boxes)
+      for (auto& v : B.acc) std::fill(v.begin(), v.end(), 0.0);
     for (auto& F : S->mur)
       for (int t = 0; t < 2; ++t) {
         std::fill(F.v[t].begin(), F.v[t].end(), T(0));
@@ -936,6 +1035,89 @@ void orc_get_probe_dft(const orc_sim* s, int32_t dft, double* out) {
       out[2 * f + 1] = d.im[f];
     }
   });
+}
+
+int32_t orc_add_field_dft(orc_sim* s, const int64_t* region6, const int64_t* sub3, uint32_t comp_mask,
+                          const double* freqs, int64_t nfreq, uint64_t interval) {
+  int32_t id = -1;
+  DISPATCH(s, {
+    typename std::remove_reference_t<decltype(*S)>::FieldDft d;
+    const int64_t ext[3] = {S->nx, S->ny, S->nz};
+    d.npts = 1;
+    for (int a = 0; a < 3; ++a) {
+      d.r[2 * a] = std::min(region6[2 * a], ext[a]);
+      d.r[2 * a + 1] = std::min(region6[2 * a + 1], ext[a]);
+      d.ss[a] = std::max<int64_t>(sub3[a], 1);
+      const int64_t len = std::max<int64_t>(d.r[2 * a + 1] - d.r[2 * a], 0);
+      d.n[a] = (len + d.ss[a] - 1) / d.ss[a];
+      d.npts *= d.n[a];
+    }
+    for (int c = 0; c < 6; ++c)
+      if (comp_mask & (1u << c)) d.comps.push_back(c);
+    d.interval = std::max<uint64_t>(interval, 1);
+    d.freqs.assign(freqs, freqs + nfreq);
+    d.acc.assign(2 * (size_t)nfreq * d.comps.size() * (size_t)d.npts, 0.0);
+    S->fdumps.push_back(std::move(d));
+    id = (int32_t)S->fdumps.size() - 1;
+  });
+  return id;
+}
+
+int64_t orc_field_dft_points(const orc_sim* s, int32_t id) {
+  int64_t n = 0;
+  DISPATCH(s, n = S->fdumps[id].npts);
+  return n;
+}
+
+void orc_get_field_dft(const orc_sim* s, int32_t id, int64_t f, int64_t comp_slot, double* out) {
+  DISPATCH(s, {
+    const auto& d = S->fdumps[id];
+    const size_t off = 2 * (f * d.comps.size() + comp_slot) * (size_t)d.npts;
+    std::memcpy(out, d.acc.data() + off, 2 * sizeof(double) * d.npts);
+  });
+}
+
+int32_t orc_add_nf2ff_box(orc_sim* s, const int64_t* lo3, const int64_t* hi3, const int32_t* dirs6,
+                          const double* freqs, int64_t nfreq, uint64_t interval) {
+  int32_t id = -1;
+  DISPATCH(s, {
+    typename std::remove_reference_t<decltype(*S)>::Nf2ffBox B;
+    const int64_t ext[3] = {S->nx, S->ny, S->nz};
+    for (int a = 0; a < 3; ++a) {
+      if (lo3[a] < 1 || hi3[a] <= lo3[a] || hi3[a] > ext[a] - 1) return -1;
+      B.lo[a] = lo3[a];
+      B.hi[a] = hi3[a];
+    }
+    B.interval = std::max<uint64_t>(interval, 1);
+    B.freqs.assign(freqs, freqs + nfreq);
+    for (int f = 0; f < 6; ++f) {
+      B.dirs[f] = dirs6[f] != 0;
+      if (!B.dirs[f]) continue;
+      const int a = f / 2, b = (a + 1) % 3, c = (a + 2) % 3;
+      const int64_t np = (B.hi[b] - B.lo[b] + 1) * (B.hi[c] - B.lo[c] + 1);
+      B.faces.push_back(f);
+      B.acc.emplace_back(8 * (size_t)nfreq * (size_t)np, 0.0);
+    }
+    S->boxes.push_back(std::move(B));
+    id = (int32_t)S->boxes.size() - 1;
+  });
+  return id;
+}
+
+/* out: 4 arrays (Eb, Ec, Hb, Hc) of nb * nc (re, im); returns nb * nc, 0 if
+ * the face is not recorded. */
+int64_t orc_get_nf2ff_face(const orc_sim* s, int32_t id, int32_t face, int64_t f, double* out) {
+  int64_t np = 0;
+  DISPATCH(s, {
+    const auto& B = S->boxes[id];
+    for (size_t fs = 0; fs < B.faces.size(); ++fs) {
+      if (B.faces[fs] != face) continue;
+      const int a = face / 2, b = (a + 1) % 3, c = (a + 2) % 3;
+      np = (B.hi[b] - B.lo[b] + 1) * (B.hi[c] - B.lo[c] + 1);
+      std::memcpy(out, B.acc[fs].data() + f * 8 * (size_t)np, 8 * sizeof(double) * np);
+    }
+  });
+  return np;
 }
 
 int32_t orc_enable_cpml(orc_sim* s, const int32_t* layers6, double m, double R, double alpha_max,

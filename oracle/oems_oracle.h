@@ -146,6 +146,23 @@ int32_t orc_cpml_profile(const orc_sim* s, int32_t face, double* out);
  * after it, faces applied in order); order 2 is the second-order Mur
  * condition (Mur 1981) on face interiors, first order on face edges.
  * phase_velocity <= 0 means c0.  Returns 0 or a negative error. */
+/* Frequency-domain field dump (src/processing/fields_fd.rs:31-217): region
+ * i0 i1 j0 j1 k0 k1 half-open, sub-sampling per axis, components by bit mask
+ * (0..2 E, 3..5 H), accumulated at timesteps that are multiples of interval
+ * with factor exp(-j 2 pi f t) 2 dt interval; E at t = n dt, H at
+ * (n - 1/2) dt.  Returns the dump id. */
+int32_t orc_add_field_dft(orc_sim* s, const int64_t* region6, const int64_t* sub3, uint32_t comp_mask,
+                          const double* freqs, int64_t nfreq, uint64_t interval);
+int64_t orc_field_dft_points(const orc_sim* s, int32_t id);
+/* out: npoints (re, im) of frequency f, component slot (ascending order of
+ * the mask), points in region order (k fastest). */
+void orc_get_field_dft(const orc_sim* s, int32_t id, int64_t f, int64_t comp_slot, double* out);
+/* NF2FF recording box on node planes lo..hi (1 <= lo < hi <= n - 1) with
+ * faces -x +x -y +y -z +z enabled by dirs6: tangential E on the face plane and
+ * tangential H averaged over the two half-planes around it. */
+int32_t orc_add_nf2ff_box(orc_sim* s, const int64_t* lo3, const int64_t* hi3, const int32_t* dirs6,
+                          const double* freqs, int64_t nfreq, uint64_t interval);
+int64_t orc_get_nf2ff_face(const orc_sim* s, int32_t id, int32_t face, int64_t f, double* out);
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity);
 
 /* Dispersive material on a list of cells (src/extensions/dispersive.rs),
