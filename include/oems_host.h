@@ -42,6 +42,8 @@ OEMS_API oems_status oems_operator_create(const double* x_lines, uint64_t nxl, c
 OEMS_API oems_status oems_operator_create_uniform(uint64_t nx, uint64_t ny, uint64_t nz, double delta,
                                          oems_operator** out);
 OEMS_API void oems_operator_destroy(oems_operator* op);
+/* Independent copy (grid, dt and all coefficients). */
+OEMS_API oems_status oems_operator_clone(const oems_operator* op, oems_operator** out);
 /* region = i0, i1, j0, j1, k0, k1 (half-open, clipped to the grid). */
 OEMS_API oems_status oems_operator_set_material(oems_operator* op, double eps_r, double mu_r,
                                        double sigma_e, double sigma_m, const uint64_t region[6]);
@@ -165,6 +167,55 @@ OEMS_API oems_status oems_simulation_setup(oems_simulation* sim);
 OEMS_API oems_status oems_simulation_run(oems_simulation* sim, oems_simulation_stats* stats);
 /* Borrowed engine handle (NULL before setup). */
 OEMS_API oems_engine* oems_simulation_engine(oems_simulation* sim);
+
+/* ---- batched port sweep --------------------------------------------------
+ * Many independent lumped-port simulations (no counterpart in the reference)
+ * run to energy decay, each in its own engine and CUDA stream on one device,
+ * `concurrency` of them at a time from host worker threads, so that small
+ * grids together fill the GPU.  Every instance records the port voltage u =
+ * E . dl and current i (into the structure) as f64 running DFTs at the
+ * sweep's frequencies and returns S11 = (u - u_inc) / u_inc with u_inc =
+ * (u + i R) / 2 (Port.CalcPort, python/openEMS/ports.py:136-138). */
+
+typedef struct oems_sweep oems_sweep;
+
+typedef struct oems_sweep_instance {
+  const oems_operator* op;   /* copied by oems_sweep_add */
+  oems_cpml_desc cpml;       /* all layers 0 = no CPML */
+  uint64_t port_position[3]; /* E edge of the port */
+  int32_t port_direction;
+  int32_t reserved0;
+  double port_resistance;    /* > 0 */
+  double port_eps_r;         /* background of the port edge */
+  double port_sigma;
+  oems_excitation waveform;  /* source voltage signal; position / direction ignored */
+  double energy_decay_db;    /* stop below -|value| dB of the peak; 0 = run max_timesteps */
+  uint64_t max_timesteps;
+} oems_sweep_instance;
+
+typedef struct oems_sweep_result {
+  uint64_t timesteps;
+  int32_t termination_reason; /* OEMS_TERMINATION_* */
+  int32_t status;             /* OEMS_OK or the instance's error */
+  double final_decay_db;
+  double device_seconds;      /* sum over the instance's batches */
+  double cells;
+} oems_sweep_result;
+
+/* freqs: the DFT frequencies of every instance (Hz).  engine_flags as for
+ * oems_engine_create; concurrency >= 1. */
+OEMS_API oems_status oems_sweep_create(int32_t device, uint32_t concurrency, uint32_t engine_flags,
+                                       const double* freqs, uint64_t nfreq, oems_sweep** out);
+OEMS_API void oems_sweep_destroy(oems_sweep* sweep);
+OEMS_API oems_status oems_sweep_add(oems_sweep* sweep, const oems_sweep_instance* inst, int32_t* instance_id);
+/* Runs every instance not run yet; batch_steps 0 = 2000.  Returns the first
+ * instance error (the others still run; see oems_sweep_get_result). */
+OEMS_API oems_status oems_sweep_run(oems_sweep* sweep, uint64_t batch_steps);
+/* uf, if_ and s11: 2 x nfreq doubles (re, im) each; any may be NULL. */
+OEMS_API oems_status oems_sweep_get_result(const oems_sweep* sweep, int32_t instance_id, oems_sweep_result* info,
+                                           double* uf, double* if_, double* s11);
+/* Wall time of the last run and the cell x timestep count it executed. */
+OEMS_API oems_status oems_sweep_stats(const oems_sweep* sweep, double* wall_seconds, double* cell_steps);
 
 #ifdef __cplusplus
 }

@@ -175,6 +175,18 @@ class SimulationStatsC(ctypes.Structure):
                 ("speed_mcells_per_sec", c_f64)]
 
 
+class SweepInstanceC(ctypes.Structure):
+    _fields_ = [("op", P), ("cpml", CpmlDescC), ("port_position", c_u64 * 3),
+                ("port_direction", c_i32), ("reserved0", c_i32), ("port_resistance", c_f64),
+                ("port_eps_r", c_f64), ("port_sigma", c_f64), ("waveform", ExcitationC),
+                ("energy_decay_db", c_f64), ("max_timesteps", c_u64)]
+
+
+class SweepResultC(ctypes.Structure):
+    _fields_ = [("timesteps", c_u64), ("termination_reason", c_i32), ("status", c_i32),
+                ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64)]
+
+
 # name -> (restype, argtypes); every symbol the headers declare
 SIGNATURES = {
     # include/oems.h
@@ -223,6 +235,14 @@ SIGNATURES = {
     "oems_operator_set_pec": (c_i32, [P, c_u64 * 6]),
     "oems_operator_info": (c_i32, [P, c_u64 * 3, ctypes.POINTER(c_f64), c_f64 * 3]),
     "oems_operator_coefficients": (c_i32, [P, PF * 12]),
+    "oems_operator_clone": (c_i32, [P, ctypes.POINTER(P)]),
+    "oems_sweep_create": (c_i32, [c_i32, c_u32, c_u32, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(P)]),
+    "oems_sweep_destroy": (None, [P]),
+    "oems_sweep_add": (c_i32, [P, ctypes.POINTER(SweepInstanceC), ctypes.POINTER(c_i32)]),
+    "oems_sweep_run": (c_i32, [P, c_u64]),
+    "oems_sweep_get_result": (c_i32, [P, c_i32, ctypes.POINTER(SweepResultC), ctypes.POINTER(c_f64),
+                                      ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
+    "oems_sweep_stats": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_operator_set_lumped": (c_i32, [P, c_u64 * 3, c_i32, c_f64, c_f64, c_f64, c_f64,
                                          ctypes.POINTER(c_f64)]),
     "oems_operator_engine_desc": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(OperatorDesc)]),

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <unordered_map>
@@ -844,6 +845,11 @@ static std::map<TuneKey, LaunchShape>& tune_cache() {
   static std::map<TuneKey, LaunchShape> m;
   return m;
 }
+// engines may be driven from several host threads (one engine per thread)
+static std::mutex& tune_mutex() {
+  static std::mutex m;
+  return m;
+}
 
 // Project autotuner: tries CTA sizes and x-chunk depths on scratch copies of
 // the state (fields and psi are saved and restored), keeps the fastest.
@@ -868,10 +874,13 @@ static oems_status autotune(oems_engine* en) {
   }
   const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes,
                     (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0)};
-  auto hit = tune_cache().find(key);
-  if (hit != tune_cache().end()) {
-    apply_shape(en, hit->second);
-    return OEMS_OK;
+  {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    auto hit = tune_cache().find(key);
+    if (hit != tune_cache().end()) {
+      apply_shape(en, hit->second);
+      return OEMS_OK;
+    }
   }
   const size_t fbytes = (size_t)6 * en->ncells_padded * sizeof(float);
   const size_t pbytes = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
@@ -933,7 +942,10 @@ static oems_status autotune(oems_engine* en) {
     if (err) st = fail(OEMS_ERR_TIMEOUT, "a bounded device wait gave up while tuning");
   }
   apply_shape(en, best);
-  if (st == OEMS_OK) tune_cache()[key] = best;
+  if (st == OEMS_OK) {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    tune_cache()[key] = best;
+  }
   cudaMemcpyAsync(en->fields, save, fbytes, cudaMemcpyDeviceToDevice, en->stream);
   if (pbytes) cudaMemcpyAsync(en->cpml.psi.p, (char*)save + fbytes, pbytes, cudaMemcpyDeviceToDevice, en->stream);
   cudaStreamSynchronize(en->stream);

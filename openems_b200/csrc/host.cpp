@@ -256,6 +256,12 @@ oems_status oems_operator_set_lumped(oems_operator* op, const uint64_t pos[3], i
   return OEMS_OK;
 }
 
+oems_status oems_operator_clone(const oems_operator* op, oems_operator** out) {
+  if (!op || !out) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  *out = new oems_operator(*op);
+  return OEMS_OK;
+}
+
 oems_status oems_operator_info(const oems_operator* op, uint64_t dims[3], double* dt, double delta[3]) {
   if (!op) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL operator");
   for (int a = 0; a < 3; ++a) {

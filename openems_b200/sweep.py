@@ -1,0 +1,155 @@
+"""Batched lumped-port sweeps: many independent grids run to energy decay on
+one GPU, several at a time, each returning its port DFTs and S11.
+
+The scheduler is native (csrc/sweep.cpp, oems_sweep_* in oems_host.h); this
+module builds its inputs and reads its results.  S11 uses Port.CalcPort's
+arithmetic (python/openEMS/ports.py:136-138).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from .fdtd import CpmlBoundaries, Excitation, Operator
+
+
+@dataclass
+class SweepInstance:
+    """One grid of a sweep: its operator (materials and PEC already set), a
+    lumped port on one E edge with its background material, the source
+    waveform, CPML and the end condition."""
+
+    operator: Operator
+    port_position: tuple
+    port_direction: int
+    waveform: Excitation
+    port_resistance: float = 50.0
+    port_eps_r: float = 1.0
+    port_sigma: float = 0.0
+    cpml: Optional[CpmlBoundaries] = None
+    energy_decay_db: float = 50.0
+    max_timesteps: int = 60000
+
+    def to_c(self) -> N.SweepInstanceC:
+        d = N.SweepInstanceC()
+        d.op = self.operator.handle
+        if self.cpml is not None:
+            d.cpml = self.cpml.to_c()
+        for a in range(3):
+            d.port_position[a] = int(self.port_position[a])
+        d.port_direction = int(self.port_direction)
+        d.port_resistance = float(self.port_resistance)
+        d.port_eps_r = float(self.port_eps_r)
+        d.port_sigma = float(self.port_sigma)
+        d.waveform = self.waveform.to_c()
+        d.energy_decay_db = float(self.energy_decay_db)
+        d.max_timesteps = int(self.max_timesteps)
+        return d
+
+
+class Sweep:
+    """oems_sweep: frequencies shared by every instance; `concurrency`
+    engines run at a time on `device`."""
+
+    def __init__(self, freqs, concurrency: int = 4, device: int = -1, compressed: bool = False,
+                 autotune: bool = False, kernels: str = "register"):
+        self.freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+        flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
+            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS}[kernels]
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_sweep_create(device, concurrency, flags,
+                                          self.freqs.ctypes.data_as(ctypes.POINTER(N.c_f64)),
+                                          len(self.freqs), ctypes.byref(h)))
+        self._h = h
+        self.count = 0
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().oems_sweep_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def add(self, inst: SweepInstance) -> int:
+        d = inst.to_c()
+        iid = N.c_i32()
+        N.check(N.lib().oems_sweep_add(self._h, ctypes.byref(d), ctypes.byref(iid)))
+        self.count += 1
+        return iid.value
+
+    def run(self, batch_steps: int = 2000):
+        N.check(N.lib().oems_sweep_run(self._h, batch_steps))
+
+    def result(self, iid: int) -> dict:
+        info = N.SweepResultC()
+        nf = len(self.freqs)
+        bufs = [np.zeros(2 * nf) for _ in range(3)]
+        ptrs = [b.ctypes.data_as(ctypes.POINTER(N.c_f64)) for b in bufs]
+        N.check(N.lib().oems_sweep_get_result(self._h, iid, ctypes.byref(info), *ptrs))
+        uf, if_, s11 = (b[0::2] + 1j * b[1::2] for b in bufs)
+        return {"timesteps": int(info.timesteps), "termination_reason": int(info.termination_reason),
+                "final_decay_db": float(info.final_decay_db), "device_seconds": float(info.device_seconds),
+                "cells": float(info.cells), "uf": uf, "if": if_, "s11": s11}
+
+    def stats(self):
+        wall, cs = N.c_f64(), N.c_f64()
+        N.check(N.lib().oems_sweep_stats(self._h, ctypes.byref(wall), ctypes.byref(cs)))
+        return wall.value, cs.value
+
+
+def main(argv=None):
+    """Runs the seeded patch-antenna sweep and prints one JSON line:
+    python -m openems_b200.sweep [--count 64] [--seed 4] [--concurrency 6]"""
+    import argparse
+    import json
+    import time
+
+    from . import workloads as W
+
+    p = argparse.ArgumentParser(description="batched lumped-port sweep of seeded patch antennas")
+    p.add_argument("--count", type=int, default=64)
+    p.add_argument("--seed", type=int, default=4)
+    p.add_argument("--concurrency", type=int, default=6)
+    p.add_argument("--freqs", type=int, default=801, help="S11 points over 0-8 GHz")
+    p.add_argument("--decay-db", type=float, default=50.0)
+    p.add_argument("--max-steps", type=int, default=60000)
+    p.add_argument("--batch-steps", type=int, default=2000)
+    p.add_argument("--out", default=None, help="write S11 per instance to this .npz")
+    a = p.parse_args(argv)
+    freqs = np.linspace(0.0, 8e9, a.freqs)
+    specs = W.patch_specs(a.count, seed=a.seed)
+    t0 = time.perf_counter()
+    sw = Sweep(freqs, concurrency=a.concurrency)
+    ids = [sw.add(W.patch_sweep_instance(s, decay_db=a.decay_db, max_steps=a.max_steps)) for s in specs]
+    t1 = time.perf_counter()
+    sw.run(a.batch_steps)
+    wall, cell_steps = sw.stats()
+    res = [sw.result(i) for i in ids]
+    s11_db = [20 * np.log10(np.maximum(np.abs(r["s11"][1:]), 1e-30)) for r in res]
+    line = {
+        "workload": f"patch_sweep_{a.count}_seed{a.seed}",
+        "instances": a.count, "concurrency": a.concurrency, "freqs": a.freqs,
+        "cell_steps": cell_steps, "wall_s": wall, "setup_s": t1 - t0,
+        "mcells_per_s": cell_steps / wall / 1e6, "instances_per_hour": a.count / wall * 3600.0,
+        "device_seconds_sum": sum(r["device_seconds"] for r in res),
+        "decayed": sum(r["termination_reason"] == 1 for r in res),
+        "timesteps_mean": float(np.mean([r["timesteps"] for r in res])),
+        "timesteps_max": int(max(r["timesteps"] for r in res)),
+        "min_s11_db_median": float(np.median([d.min() for d in s11_db])),
+        "max_abs_s11": float(max(np.abs(r["s11"]).max() for r in res)),
+        "instances_abs_s11_above_1.01": int(sum(np.abs(r["s11"]).max() > 1.01 for r in res)),
+    }
+    print(json.dumps(line))
+    if a.out:
+        np.savez(a.out, freqs=freqs, s11=np.array([r["s11"] for r in res]),
+                 timesteps=np.array([r["timesteps"] for r in res]))
+
+
+if __name__ == "__main__":
+    main()

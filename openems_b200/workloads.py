@@ -77,3 +77,79 @@ def cpml_boxes(n: int = 256, steps: int = 10000) -> Workload:
     return Workload(f"cpml_boxes_{n}", (n, n, n), 1e-3, steps, 8, dielectric_boxes(n, 8),
                     1.0 / (np.pi * 10e9), (n // 2, n // 2, n // 2), 2,
                     [(2, (n // 2, n // 2, n // 2)), (2, (n // 4, n // 2, n // 2))])
+
+
+@dataclass
+class PatchSpec:
+    """One microstrip patch antenna of the sweep workload (cells of delta):
+    PEC ground layer at k_ground and substrate cells [k_ground + 1, k_patch),
+    both over the whole x-y extent (through the CPML),
+    PEC patch layer k_patch over [x0, x0 + W) x [y0, y0 + L), a PEC feed wire
+    from the port edge (Ez at (fx, fy, k_ground + 1)) up to the patch."""
+
+    dims: Tuple[int, int, int]
+    eps_r: float
+    h_cells: int
+    W: int
+    L: int
+    x0: int
+    y0: int
+    fx: int
+    fy: int
+    k_ground: int = 10
+    layers: int = 8
+
+    @property
+    def k_patch(self) -> int:
+        return self.k_ground + 1 + self.h_cells
+
+    @property
+    def cells(self) -> int:
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+
+def patch_specs(count: int = 64, seed: int = 4, layers: int = 8) -> List[PatchSpec]:
+    """Seeded patch geometries: n_{x,y,z} ~ U{48..160}; substrate eps_r ~
+    U[2.2, 10.2], thickness U[0.8, 3.2] mm = 2-6 cells of 0.5 mm; W, L ~
+    U[8, 40] mm = 16-80 cells clipped to the interior; feed on the L axis at
+    a seeded fraction U[0.2, 0.7] of L/2 from the centre."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        dims = tuple(int(v) for v in rng.integers(48, 161, size=3))
+        eps_r = float(rng.uniform(2.2, 10.2))
+        h = int(np.clip(round(rng.uniform(0.8, 3.2) / 0.5), 2, 6))
+        W = int(rng.integers(16, 81))
+        L = int(rng.integers(16, 81))
+        frac = float(rng.uniform(0.2, 0.7))
+        margin = layers + 4
+        W = max(4, min(W, dims[0] - 2 * margin))
+        L = max(4, min(L, dims[1] - 2 * margin))
+        x0 = (dims[0] - W) // 2
+        y0 = (dims[1] - L) // 2
+        fx = x0 + W // 2
+        fy = y0 + L // 2 - int(round(frac * (L // 2)))
+        out.append(PatchSpec(dims, eps_r, h, W, L, x0, y0, fx, fy, layers + 2, layers))
+    return out
+
+
+def patch_sweep_instance(spec: PatchSpec, delta: float = 0.5e-3, decay_db: float = 50.0,
+                         max_steps: int = 60000, fmax: float = 8e9):
+    """Operator, port and source of one patch (imported lazily: sweep.py
+    depends on fdtd only)."""
+    from .sweep import SweepInstance
+    nx, ny, nz = spec.dims
+    lo = spec.layers
+    op = fdtd.Operator(fdtd.Grid.uniform(nx, ny, nz, delta), fdtd.BoundaryConditions.all_pec())
+    kg, kp = spec.k_ground, spec.k_patch
+    # ground plane and substrate run through the CPML to the domain edge, so
+    # that substrate surface waves leave instead of ringing at a slab end
+    op.set_material(spec.eps_r, 1.0, 0.0, 0.0, (0, nx, 0, ny, kg + 1, kp))
+    op.set_pec((0, nx, 0, ny, kg, kg + 1))
+    op.set_pec((spec.x0, spec.x0 + spec.W, spec.y0, spec.y0 + spec.L, kp, kp + 1))
+    if kp > kg + 2:
+        op.set_pec((spec.fx, spec.fx + 1, spec.fy, spec.fy + 1, kg + 2, kp))
+    tau = 1.0 / (np.pi * fmax)
+    wave = fdtd.Excitation.gaussian_pulse(tau, 4.0 * tau, 2, (spec.fx, spec.fy, kg + 1))
+    return SweepInstance(op, (spec.fx, spec.fy, kg + 1), 2, wave, 50.0, spec.eps_r, 0.0,
+                         fdtd.CpmlBoundaries.uniform(lo), decay_db, max_steps)
