@@ -175,6 +175,15 @@ typedef struct oems_mur_desc {
   double phase_velocity; /* <= 0: c0 */
 } oems_mur_desc;
 
+/* PmlBoundaries (src/extensions/pml.rs:85-101): layers per face (-x +x -y
+ * +y -z +z; a face is active when 0 < layers < n), polynomial grading order
+ * and target reflection. */
+typedef struct oems_upml_desc {
+  uint32_t layers[6];
+  double grading_order;
+  double reflection_coeff;
+} oems_upml_desc;
+
 /* Dispersive material on a list of cells (src/extensions/dispersive.rs),
  * applied after the E update to all three components of every cell:
  *   kind 0 Drude    params (omega_p, gamma)            :476-535
@@ -283,6 +292,12 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);
 /* MurAbc::new (src/extensions/mur_abc.rs:175). */
 OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc);
+/* Upml::new (src/extensions/pml.rs:209-219) with the flux hooks of
+ * pml.rs:505-655 around the H and E updates.  Reproduces the reference's
+ * coefficients, under which the scheme grows without bound (the reference
+ * disables its PML tests, src/fdtd/engine_testing.rs:2322-2330); use
+ * oems_engine_add_cpml for absorption. */
+OEMS_API oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc);
 /* LorentzMaterial / DrudeMaterial / DebyeMaterial::new (src/extensions/
  * dispersive.rs:134, 476, 570); cells: ncells x (i, j, k). Materials apply in
  * the order they are added. */

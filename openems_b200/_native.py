@@ -133,6 +133,10 @@ class MurDescC(ctypes.Structure):
                 ("phase_velocity", c_f64)]
 
 
+class UpmlDescC(ctypes.Structure):
+    _fields_ = [("layers", c_u32 * 6), ("grading_order", c_f64), ("reflection_coeff", c_f64)]
+
+
 class DispersiveDescC(ctypes.Structure):
     _fields_ = [("kind", c_i32), ("reserved0", c_i32), ("params", c_f64 * 3), ("eps_inf", c_f64)]
 
@@ -199,6 +203,7 @@ SIGNATURES = {
     "oems_engine_reset": (c_i32, [P]),
     "oems_engine_add_cpml": (c_i32, [P, ctypes.POINTER(CpmlDescC)]),
     "oems_engine_add_mur": (c_i32, [P, ctypes.POINTER(MurDescC)]),
+    "oems_engine_add_upml": (c_i32, [P, ctypes.POINTER(UpmlDescC)]),
     "oems_engine_add_dispersive": (c_i32, [P, ctypes.POINTER(DispersiveDescC), P, c_u64]),
     "oems_engine_add_lumped_rlc": (c_i32, [P, ctypes.POINTER(LumpedRlcDescC), c_u64]),
     "oems_engine_add_field_dft": (c_i32, [P, ctypes.POINTER(FieldDftDescC), ctypes.POINTER(c_f64), c_u32,

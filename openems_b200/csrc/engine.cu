@@ -33,6 +33,7 @@
 #include "mur.cuh"
 #include "lumped_ade.cuh"
 #include "fd_nf2ff.cuh"
+#include "upml.cuh"
 
 namespace oems {
 
@@ -305,6 +306,12 @@ struct Nf2ffHost {
   std::unique_ptr<FdTable> tab{new FdTable};
 };
 
+struct UpmlHost {
+  bool on = false;
+  UpmlArgs e{}, h{};                 // E (voltage) and H (current) halves
+  DevBuf<float> coef, flux;          // [E coef | H coef], [E flux | H flux]
+};
+
 }  // namespace oems
 
 struct oems_engine {
@@ -330,6 +337,7 @@ struct oems_engine {
   oems::MurHost mur;
   std::vector<oems::DispHost> disp;
   oems::RlcHost rlc;
+  oems::UpmlHost upml;
   std::vector<oems::FieldDftHost> fdumps;
   std::vector<oems::Nf2ffHost> boxes;
 
@@ -659,16 +667,24 @@ static cudaError_t launch_post(oems_engine* en, int local) {
 // update (Mur post and apply), in the reference's hook order.
 static int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
 
+static cudaError_t launch_upml(oems_engine* en, bool h, bool pre);
+
 static cudaError_t launch_pre_e(oems_engine* en) {
   if (en->mur.on) {
     k_mur_pre<<<blocks_for(en->mur.args.total, 256), 256, 0, en->stream>>>(en->mur.args);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  // UPML innermost: its pre hook right before the E update
+  if (en->upml.on) return launch_upml(en, false, true);
   return cudaSuccess;
 }
 
 static cudaError_t launch_post_e(oems_engine* en) {
+  if (en->upml.on) {
+    cudaError_t e = launch_upml(en, false, false);
+    if (e != cudaSuccess) return e;
+  }
   if (en->mur.on) {
     const int b = blocks_for(en->mur.args.total, 256);
     k_mur_post<<<b, 256, 0, en->stream>>>(en->mur.args);
@@ -692,15 +708,34 @@ static cudaError_t launch_post_e(oems_engine* en) {
 }
 
 static int ext_kernels(const oems_engine* en) {
-  return (en->mur.on ? 3 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
+  return (en->mur.on ? 3 : 0) + (en->upml.on ? 4 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
 }
 
 static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + post_kernels(en); }
 
 // Launches `steps` timesteps directly (no graph).
+static cudaError_t launch_upml(oems_engine* en, bool h, bool pre) {
+  const UpmlArgs& a = h ? en->upml.h : en->upml.e;
+  const int b = blocks_for(a.total, 256);
+  if (pre)
+    k_upml_pre<<<b, 256, 0, en->stream>>>(a);
+  else
+    k_upml_post<<<b, 256, 0, en->stream>>>(a);
+  return cudaGetLastError();
+}
+
+// H update with the UPML current hooks around it (pml.rs:586-655).
+static cudaError_t launch_h_step(oems_engine* en) {
+  cudaError_t e;
+  if (en->upml.on && (e = launch_upml(en, true, true)) != cudaSuccess) return e;
+  if ((e = launch_h(en)) != cudaSuccess) return e;
+  if (en->upml.on) return launch_upml(en, true, false);
+  return cudaSuccess;
+}
+
 static oems_status launch_steps_direct(oems_engine* en, int steps) {
   for (int s = 0; s < steps; ++s) {
-    OEMS_CUDA(launch_h(en));
+    OEMS_CUDA(launch_h_step(en));
     OEMS_CUDA(launch_pre_e(en));
     OEMS_CUDA(launch_e(en));
     OEMS_CUDA(launch_post_e(en));
@@ -721,9 +756,11 @@ static oems_status launch_steps_profiled(oems_engine* en, int steps) {
     const int n = std::min(kChunk, steps - s0);
     for (int s = 0; s < n; ++s) {
       cudaEvent_t* ev = &en->prof_ev[4 * s];
+      if (en->upml.on) OEMS_CUDA(launch_upml(en, true, true));
       OEMS_CUDA(cudaEventRecord(ev[0], en->stream));
       OEMS_CUDA(launch_h(en));
       OEMS_CUDA(cudaEventRecord(ev[1], en->stream));
+      if (en->upml.on) OEMS_CUDA(launch_upml(en, true, false));
       OEMS_CUDA(launch_pre_e(en));
       OEMS_CUDA(cudaEventRecord(ev[2], en->stream));
       OEMS_CUDA(launch_e(en));
@@ -1571,6 +1608,8 @@ oems_status oems_engine_reset(oems_engine* engine) {
     OEMS_CUDA(cudaMemsetAsync(d.state->p, 0, d.state->n * sizeof(float), engine->stream));
   if (!engine->rlc.q.empty())
     OEMS_CUDA(cudaMemsetAsync(engine->rlc.d_int.p, 0, engine->rlc.q.size() * sizeof(float), engine->stream));
+  if (engine->upml.on)
+    OEMS_CUDA(cudaMemsetAsync(engine->upml.flux.p, 0, engine->upml.flux.n * sizeof(float), engine->stream));
   for (auto& d : engine->fdumps)
     OEMS_CUDA(cudaMemsetAsync(d.acc->p, 0, d.acc->n * sizeof(double), engine->stream));
   for (auto& x : engine->boxes)
@@ -2005,6 +2044,142 @@ oems_status oems_nf2ff_surface(int32_t device, const double* points, uint64_t np
   }
   cudaStreamDestroy(stream);
   return st;
+}
+
+// Upml::calculate_kappa (src/extensions/pml.rs:370-420): conductivity at a
+// node depth into the layer; the current grading is shifted by half a cell,
+// -1/2 for the component along the PML direction, +1/2 otherwise.
+static void upml_kappa(int comp, int dir, const long long pos[3], bool is_min, long long layers, double width,
+                       double smax, double m, const long long n[3], const double delta[3], double* kv, double* ki) {
+  const double d = delta[dir];
+  double depth = 0.0;
+  if (is_min) {
+    if (pos[dir] <= layers) depth = (double)(layers - pos[dir]) * d;
+  } else {
+    const long long bs = n[dir] - layers - 1;
+    if (pos[dir] >= bs) depth = (double)(pos[dir] - bs) * d;
+  }
+  if (depth <= 0.0) {
+    *kv = *ki = 0.0;
+    return;
+  }
+  *kv = smax * std::pow(depth / width, m);
+  const double di = depth + (comp == dir ? -0.5 : 0.5) * d;
+  const double ni = std::min(std::max(di / width, 0.0), 1.0);
+  *ki = smax * std::pow(ni, m);
+}
+
+oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc) {
+  if (!engine || !desc) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->upml.on) return fail(OEMS_ERR_CONFIG, "UPML already attached");
+  if (!(desc->reflection_coeff > 0.0 && desc->reflection_coeff < 1.0))
+    return fail(OEMS_ERR_CONFIG, "UPML reflection coefficient must be in (0, 1)");
+  DeviceGuard guard(engine->device);
+  const long long n[3] = {engine->nx, engine->ny, engine->nz};
+  const long long* L = nullptr;
+  long long lay[6];
+  for (int f = 0; f < 6; ++f) lay[f] = (long long)desc->layers[f];
+  L = lay;
+  // Upml::build_regions (pml.rs:222-296): x slabs over the full y-z plane,
+  // y slabs without the x corners, z slabs without x and y edges.
+  struct Reg {
+    long long start[3], size[3];
+    int dir;
+    bool is_min;
+  };
+  std::vector<Reg> regs;
+  if (L[0] > 0 && L[0] < n[0]) regs.push_back({{0, 0, 0}, {L[0] + 1, n[1], n[2]}, 0, true});
+  if (L[1] > 0 && L[1] < n[0]) regs.push_back({{n[0] - L[1] - 1, 0, 0}, {L[1] + 1, n[1], n[2]}, 0, false});
+  const long long xs = L[0] > 0 ? L[0] + 1 : 0, xe = L[1] > 0 ? n[0] - L[1] - 1 : n[0];
+  if (L[2] > 0 && L[2] < n[1] && xs < xe) regs.push_back({{xs, 0, 0}, {xe - xs, L[2] + 1, n[2]}, 1, true});
+  if (L[3] > 0 && L[3] < n[1] && xs < xe)
+    regs.push_back({{xs, n[1] - L[3] - 1, 0}, {xe - xs, L[3] + 1, n[2]}, 1, false});
+  const long long ys = L[2] > 0 ? L[2] + 1 : 0, ye = L[3] > 0 ? n[1] - L[3] - 1 : n[1];
+  if (L[4] > 0 && L[4] < n[2] && xs < xe && ys < ye)
+    regs.push_back({{xs, ys, 0}, {xe - xs, ye - ys, L[4] + 1}, 2, true});
+  if (L[5] > 0 && L[5] < n[2] && xs < xe && ys < ye)
+    regs.push_back({{xs, ys, n[2] - L[5] - 1}, {xe - xs, ye - ys, L[5] + 1}, 2, false});
+  if (regs.empty()) return fail(OEMS_ERR_CONFIG, "UPML has no active region");
+  long long total = 0;
+  for (const Reg& r : regs) total += r.size[0] * r.size[1] * r.size[2];
+  // Upml::init_region_coefficients (pml.rs:299-367)
+  std::vector<float> ce(9 * (size_t)total), ch(9 * (size_t)total);
+  const double dt = engine->dt, m = desc->grading_order, eps0 = 8.854187817e-12, z0 = 376.730313668;
+  long long base = 0;
+  for (const Reg& r : regs) {
+    const long long layers = L[2 * r.dir + (r.is_min ? 0 : 1)];
+    const double width = (double)layers * engine->delta[r.dir];
+    const double smax = -(m + 1.0) * std::log(desc->reflection_coeff) / (2.0 * z0 * width);
+    long long t = 0;
+    for (long long li = 0; li < r.size[0]; ++li)
+      for (long long lj = 0; lj < r.size[1]; ++lj)
+        for (long long lk = 0; lk < r.size[2]; ++lk, ++t) {
+          const long long pos[3] = {r.start[0] + li, r.start[1] + lj, r.start[2] + lk};
+          double kv[3], ki[3];
+          for (int c = 0; c < 3; ++c)
+            upml_kappa(c, r.dir, pos, r.is_min, layers, width, smax, m, n, engine->delta, &kv[c], &ki[c]);
+          for (int c = 0; c < 3; ++c) {
+            const int npp = (c + 2) % 3;
+            const size_t q = (size_t)(base + t);
+            float* v[3] = {&ce[(0 * 3 + c) * total + q], &ce[(1 * 3 + c) * total + q], &ce[(2 * 3 + c) * total + q]};
+            float* w[3] = {&ch[(0 * 3 + c) * total + q], &ch[(1 * 3 + c) * total + q], &ch[(2 * 3 + c) * total + q]};
+            if (kv[0] + kv[1] + kv[2] > 0.0) {
+              const double den = 2.0 * eps0 + kv[npp] * dt;
+              *v[0] = (float)((2.0 * eps0 - kv[npp] * dt) / den);
+              *v[1] = (float)((2.0 * eps0 - kv[c] * dt) / den);
+              *v[2] = (float)((2.0 * eps0 + kv[c] * dt) / den);
+            } else {
+              *v[0] = 1.0f;
+              *v[1] = 0.0f;
+              *v[2] = 1.0f;
+            }
+            if (ki[0] + ki[1] + ki[2] > 0.0) {
+              const double den = 2.0 * eps0 + ki[npp] * dt;
+              *w[0] = (float)((2.0 * eps0 - ki[npp] * dt) / den);
+              *w[1] = (float)((2.0 * eps0 - ki[c] * dt) / den);
+              *w[2] = (float)((2.0 * eps0 + ki[c] * dt) / den);
+            } else {
+              *w[0] = 1.0f;
+              *w[1] = 0.0f;
+              *w[2] = 1.0f;
+            }
+          }
+        }
+    base += t;
+  }
+  UpmlHost& U = engine->upml;
+  OEMS_CUDA(U.coef.ensure(18 * (size_t)total));
+  OEMS_CUDA(U.flux.ensure(6 * (size_t)total));
+  OEMS_CUDA(cudaMemcpy(U.coef.p, ce.data(), ce.size() * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpy(U.coef.p + 9 * total, ch.data(), ch.size() * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemset(U.flux.p, 0, 6 * (size_t)total * sizeof(float)));
+  for (UpmlArgs* a : {&U.e, &U.h}) {
+    *a = UpmlArgs{};
+    a->nreg = (int)regs.size();
+    a->off[0] = 0;
+    for (size_t i = 0; i < regs.size(); ++i) {
+      for (int k = 0; k < 3; ++k) {
+        a->start[i][k] = regs[i].start[k];
+        a->size[i][k] = regs[i].size[k];
+      }
+      a->off[i + 1] = a->off[i] + regs[i].size[0] * regs[i].size[1] * regs[i].size[2];
+    }
+    for (size_t i = regs.size(); i < 6; ++i) a->off[i + 1] = a->off[regs.size()];
+    a->total = total;
+    a->ny = engine->ny;
+    a->nzp = engine->g.nzp;
+  }
+  U.e.coef = U.coef.p;
+  U.h.coef = U.coef.p + 9 * total;
+  U.e.flux = U.flux.p;
+  U.h.flux = U.flux.p + 3 * total;
+  for (int c = 0; c < 3; ++c) {
+    U.e.f[c] = engine->E(c);
+    U.h.f[c] = engine->H(c);
+  }
+  U.on = true;
+  engine->graph_epoch++;
+  return OEMS_OK;
 }
 
 oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc) {

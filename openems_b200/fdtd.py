@@ -168,6 +168,38 @@ class MurAbcConfig:
 
 
 @dataclass
+class PmlBoundaries:
+    """PmlBoundaries (src/extensions/pml.rs:85-135) for the reference's UPML
+    (Engine.add_upml).  Its coefficients make the scheme grow without bound,
+    as in the reference; CpmlBoundaries is the working absorber."""
+
+    layers: Tuple[int, ...] = (8,) * 6
+    grading_order: float = 3.0
+    reflection_coeff: float = 1e-6
+
+    @classmethod
+    def uniform(cls, layers: int):
+        return cls(layers=(int(layers),) * 6)
+
+    def disable(self, face: int) -> "PmlBoundaries":
+        lay = list(self.layers)
+        lay[face] = 0
+        self.layers = tuple(lay)
+        return self
+
+    def any_enabled(self) -> bool:
+        return any(v > 0 for v in self.layers)
+
+    def to_c(self) -> N.UpmlDescC:
+        d = N.UpmlDescC()
+        for f in range(6):
+            d.layers[f] = int(self.layers[f])
+        d.grading_order = float(self.grading_order)
+        d.reflection_coeff = float(self.reflection_coeff)
+        return d
+
+
+@dataclass
 class DrudeMaterial:
     """DrudeMaterial (src/extensions/dispersive.rs:450-535): omega_p, gamma
     in rad/s; eps_inf divides the E correction (1 = the reference)."""
@@ -883,6 +915,10 @@ class Engine:
     def add_mur(self, mur: MurAbcConfig):
         d = mur.to_c()
         N.check(N.lib().oems_engine_add_mur(self._h, ctypes.byref(d)))
+
+    def add_upml(self, pml: PmlBoundaries):
+        d = pml.to_c()
+        N.check(N.lib().oems_engine_add_upml(self._h, ctypes.byref(d)))
 
     def add_dispersive(self, material, cells):
         """Dispersive material (Drude / Lorentz / Debye) on cells (n, 3)."""

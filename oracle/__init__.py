@@ -105,6 +105,10 @@ def lib() -> ctypes.CDLL:
         L.orc_add_nf2ff_box.argtypes = [P, P, P, P, P, I64, U64]
         L.orc_get_nf2ff_face.restype = I64
         L.orc_get_nf2ff_face.argtypes = [P, I32, I32, I64, P]
+        L.orc_enable_upml.restype = I32
+        L.orc_enable_upml.argtypes = [P, P, D, D]
+        L.orc_upml_kappa.argtypes = [P, I32, I32, P, I32, I64, D, D, D, ctypes.POINTER(D),
+                                     ctypes.POINTER(D)]
         L.orc_run_batch.restype = I32
         L.orc_run_batch.argtypes = [P, U64, U64, I32, U64, I32, D, D, ctypes.POINTER(BatchResult)]
         L.orc_get_energy_samples.argtypes = [P, ctypes.POINTER(EnergySample), U64]
@@ -319,6 +323,17 @@ class OracleSim:
             return None
         z = out[0::2] + 1j * out[1::2]
         return z.reshape(4, nb, nc)
+
+    def enable_upml(self, layers=(8,) * 6, grading_order=3.0, reflection_coeff=1e-6):
+        l6 = np.ascontiguousarray(layers, dtype=np.int64)
+        return lib().orc_enable_upml(self._h, _ptr(l6), grading_order, reflection_coeff)
+
+    def upml_kappa(self, comp, direction, pos, is_min, layers, width, sigma_max, m):
+        p = np.ascontiguousarray(pos, dtype=np.int64)
+        kv, ki = ctypes.c_double(), ctypes.c_double()
+        lib().orc_upml_kappa(self._h, comp, direction, _ptr(p), int(is_min), layers, width, sigma_max, m,
+                             ctypes.byref(kv), ctypes.byref(ki))
+        return kv.value, ki.value
 
     def cpml_profile(self, face):
         out = np.zeros((6, 256))

@@ -132,6 +132,137 @@ struct Sim {
   };
   std::vector<Nf2ffBox> boxes;
 
+  // Uniaxial PML as the reference (src/extensions/pml.rs:130-655): regions
+  // with per-cell coefficients (vv vvfo vvfn for E, ii iifo iifn for H) and
+  // flux arrays, applied before and after each field update.
+  struct UpmlRegion {
+    int64_t start[3], size[3];
+    std::vector<T> cv[3][3], ci[3][3];  // [vv|vvfo|vvfn][component]
+    std::vector<T> vflux[3], iflux[3];
+  };
+  std::vector<UpmlRegion> upml;
+
+  void upml_hook(bool h, bool pre) {
+    for (UpmlRegion& R : upml) {
+      int64_t m = 0;
+      for (int64_t li = 0; li < R.size[0]; ++li)
+        for (int64_t lj = 0; lj < R.size[1]; ++lj)
+          for (int64_t lk = 0; lk < R.size[2]; ++lk, ++m) {
+            const int64_t q = idx(R.start[0] + li, R.start[1] + lj, R.start[2] + lk);
+            for (int c = 0; c < 3; ++c) {
+              std::vector<T>& F = h ? H[c] : E[c];
+              std::vector<T>& fl = h ? R.iflux[c] : R.vflux[c];
+              auto& co = h ? R.ci : R.cv;
+              if (pre) {  // pml.rs:505-549 / 586-620
+                const T f_help = co[0][c][m] * F[q] - co[1][c][m] * fl[m];
+                F[q] = fl[m];
+                fl[m] = f_help;
+              } else {    // pml.rs:554-581 / 625-655
+                const T f_help = fl[m];
+                const T flux_new = F[q];
+                fl[m] = flux_new;
+                F[q] = f_help + co[2][c][m] * flux_new;
+              }
+            }
+          }
+    }
+  }
+
+  // Upml::calculate_kappa (pml.rs:370-420)
+  void upml_kappa(int comp, int dir, const int64_t pos[3], bool is_min, int64_t layers, double width,
+                  double smax, double m, double* kv, double* ki) const {
+    const int64_t ext[3] = {nx, ny, nz};
+    const double d = delta[dir];
+    double depth = 0.0;
+    if (is_min) {
+      if (pos[dir] <= layers) depth = (double)(layers - pos[dir]) * d;
+    } else {
+      const int64_t bs = ext[dir] - layers - 1;
+      if (pos[dir] >= bs) depth = (double)(pos[dir] - bs) * d;
+    }
+    if (depth <= 0.0) {
+      *kv = 0.0;
+      *ki = 0.0;
+      return;
+    }
+    *kv = smax * std::pow(depth / width, m);
+    const double di = depth + (comp == dir ? -0.5 : 0.5) * d;
+    *ki = smax * std::pow(std::clamp(di / width, 0.0, 1.0), m);
+  }
+
+  // Upml::build_regions + init_region_coefficients (pml.rs:222-367)
+  int enable_upml(const int64_t* L, double m, double R0) {
+    const int64_t ext[3] = {nx, ny, nz};
+    struct Box {
+      int64_t s[3], z[3];
+      int dir;
+      bool mn;
+    };
+    std::vector<Box> bx;
+    if (L[0] > 0 && L[0] < nx) bx.push_back({{0, 0, 0}, {L[0] + 1, ny, nz}, 0, true});
+    if (L[1] > 0 && L[1] < nx) bx.push_back({{nx - L[1] - 1, 0, 0}, {L[1] + 1, ny, nz}, 0, false});
+    const int64_t xs = L[0] > 0 ? L[0] + 1 : 0, xe = L[1] > 0 ? nx - L[1] - 1 : nx;
+    if (L[2] > 0 && L[2] < ny && xs < xe) bx.push_back({{xs, 0, 0}, {xe - xs, L[2] + 1, nz}, 1, true});
+    if (L[3] > 0 && L[3] < ny && xs < xe) bx.push_back({{xs, ny - L[3] - 1, 0}, {xe - xs, L[3] + 1, nz}, 1, false});
+    const int64_t ys = L[2] > 0 ? L[2] + 1 : 0, ye = L[3] > 0 ? ny - L[3] - 1 : ny;
+    if (L[4] > 0 && L[4] < nz && xs < xe && ys < ye)
+      bx.push_back({{xs, ys, 0}, {xe - xs, ye - ys, L[4] + 1}, 2, true});
+    if (L[5] > 0 && L[5] < nz && xs < xe && ys < ye)
+      bx.push_back({{xs, ys, nz - L[5] - 1}, {xe - xs, ye - ys, L[5] + 1}, 2, false});
+    (void)ext;
+    upml.clear();
+    for (const Box& b : bx) {
+      UpmlRegion Rg;
+      const int64_t layers = L[2 * b.dir + (b.mn ? 0 : 1)];
+      const double width = (double)layers * delta[b.dir];
+      const double smax = -(m + 1.0) * std::log(R0) / (2.0 * kZ0 * width);
+      const int64_t cnt = b.z[0] * b.z[1] * b.z[2];
+      for (int a = 0; a < 3; ++a) {
+        Rg.start[a] = b.s[a];
+        Rg.size[a] = b.z[a];
+        Rg.vflux[a].assign(cnt, T(0));
+        Rg.iflux[a].assign(cnt, T(0));
+        for (int k = 0; k < 3; ++k) {
+          Rg.cv[k][a].assign(cnt, T(0));
+          Rg.ci[k][a].assign(cnt, T(0));
+        }
+      }
+      int64_t t = 0;
+      for (int64_t li = 0; li < b.z[0]; ++li)
+        for (int64_t lj = 0; lj < b.z[1]; ++lj)
+          for (int64_t lk = 0; lk < b.z[2]; ++lk, ++t) {
+            const int64_t pos[3] = {b.s[0] + li, b.s[1] + lj, b.s[2] + lk};
+            double kv[3], ki[3];
+            for (int c = 0; c < 3; ++c) upml_kappa(c, b.dir, pos, b.mn, layers, width, smax, m, &kv[c], &ki[c]);
+            for (int c = 0; c < 3; ++c) {
+              const int npp = (c + 2) % 3;
+              if (kv[0] + kv[1] + kv[2] > 0.0) {
+                const double den = 2.0 * kEps0 + kv[npp] * dt;
+                Rg.cv[0][c][t] = T((2.0 * kEps0 - kv[npp] * dt) / den);
+                Rg.cv[1][c][t] = T((2.0 * kEps0 - kv[c] * dt) / den);
+                Rg.cv[2][c][t] = T((2.0 * kEps0 + kv[c] * dt) / den);
+              } else {
+                Rg.cv[0][c][t] = T(1);
+                Rg.cv[1][c][t] = T(0);
+                Rg.cv[2][c][t] = T(1);
+              }
+              if (ki[0] + ki[1] + ki[2] > 0.0) {
+                const double den = 2.0 * kEps0 + ki[npp] * dt;
+                Rg.ci[0][c][t] = T((2.0 * kEps0 - ki[npp] * dt) / den);
+                Rg.ci[1][c][t] = T((2.0 * kEps0 - ki[c] * dt) / den);
+                Rg.ci[2][c][t] = T((2.0 * kEps0 + ki[c] * dt) / den);
+              } else {
+                Rg.ci[0][c][t] = T(1);
+                Rg.ci[1][c][t] = T(0);
+                Rg.ci[2][c][t] = T(1);
+              }
+            }
+          }
+      upml.push_back(std::move(Rg));
+    }
+    return (int)upml.size();
+  }
+
   std::vector<orc_energy_sample> energy;
 
   // CPML state
@@ -735,9 +866,13 @@ struct Sim {
     traces.clear();
     for (uint64_t step = 0; step < num_steps; ++step) {
       uint64_t cur = timestep;
+      if (!upml.empty()) upml_hook(true, true);
       update_h();
+      if (!upml.empty()) upml_hook(true, false);
       if (!mur.empty()) mur_pre();
+      if (!upml.empty()) upml_hook(false, true);
       update_e();
+      if (!upml.empty()) upml_hook(false, false);
       if (!mur.empty()) mur_post_apply();
       if (!disp.empty()) apply_dispersive();
       if (!rlc.empty()) apply_rlc();
@@ -911,6 +1046,11 @@ void orc_reset(orc_sim* s) {
       }
     for (auto& r : S->rlc) r.i_int = T(0);
     for (auto& d : S->fdumps) std::fill(d.acc.begin(), d.acc.end(), 0.0);
+    for (auto& R : S->upml)
+      for (int c = 0; c < 3; ++c) {
+        std::fill(R.vflux[c].begin(), R.vflux[c].end(), T(0));
+        std::fill(R.iflux[c].begin(), R.iflux[c].end(), T(0));
+      }
     for (auto& B : S->boxes)
       for (auto& v : B.acc) std::fill(v.begin(), v.end(), 0.0);
     for (auto& F : S->mur)
@@ -1228,6 +1368,17 @@ double orc_set_lumped(orc_sim* s, const int64_t* pos, int32_t dir, double r, dou
     scale = r > 0 ? (dt / eps) / (1.0 + loss) / (r * area) : 0.0;
   });
   return scale;
+}
+
+int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff) {
+  int n = 0;
+  DISPATCH(s, n = S->enable_upml(layers6, grading_order, reflection_coeff));
+  return n;
+}
+
+void orc_upml_kappa(const orc_sim* s, int32_t comp, int32_t dir, const int64_t* pos3, int32_t is_min,
+                    int64_t layers, double width, double smax, double m, double* kv, double* ki) {
+  DISPATCH(s, S->upml_kappa(comp, dir, pos3, is_min != 0, layers, width, smax, m, kv, ki));
 }
 
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity) {

@@ -163,6 +163,12 @@ void orc_get_field_dft(const orc_sim* s, int32_t id, int64_t f, int64_t comp_slo
 int32_t orc_add_nf2ff_box(orc_sim* s, const int64_t* lo3, const int64_t* hi3, const int32_t* dirs6,
                           const double* freqs, int64_t nfreq, uint64_t interval);
 int64_t orc_get_nf2ff_face(const orc_sim* s, int32_t id, int32_t face, int64_t f, double* out);
+/* Uniaxial PML as the reference (src/extensions/pml.rs:194-655), hooks
+ * around the H and E updates (innermost); returns the number of regions. */
+int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff);
+/* Upml::calculate_kappa (pml.rs:370-420) for known-answer checks. */
+void orc_upml_kappa(const orc_sim* s, int32_t comp, int32_t dir, const int64_t* pos3, int32_t is_min,
+                    int64_t layers, double width, double smax, double m, double* kv, double* ki);
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity);
 
 /* Dispersive material on a list of cells (src/extensions/dispersive.rs),

@@ -33,6 +33,7 @@ class Scenario:
     dispersive: List[Tuple] = field(default_factory=list)  # (material, cells (n, 3))
     rlc: List[oe.RlcElement] = field(default_factory=list)
     lumped: List[Tuple] = field(default_factory=list)      # (pos, dir, R, C, eps_r, sigma)
+    upml: Optional[oe.PmlBoundaries] = None
 
     def batch_sizes(self):
         return list(self.batches) if self.batches else [self.num_steps]
@@ -58,6 +59,8 @@ def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kerne
         eng.add_cpml(sc.cpml)
     if sc.mur is not None:
         eng.add_mur(sc.mur)
+    if sc.upml is not None:
+        eng.add_upml(sc.upml)
     for mat, cells in sc.dispersive:
         eng.add_dispersive(mat, cells)
     if sc.rlc:
@@ -99,6 +102,8 @@ def run_oracle(sc: Scenario, precision=32, threads=1):
         s.enable_mur(sc.mur.enabled, sc.mur.order, sc.mur.phase_velocity or 0.0)
     for pos, d, r, c, eps_r, sig in sc.lumped:
         s.set_lumped(pos, d, r, c, eps_r, sig)
+    if sc.upml is not None:
+        s.enable_upml(sc.upml.layers, sc.upml.grading_order, sc.upml.reflection_coeff)
     for mat, cells in sc.dispersive:
         d = mat.to_c()
         s.add_dispersive(d.kind, list(d.params), cells, d.eps_inf)
@@ -307,4 +312,22 @@ def dispersive_scenarios() -> List[Scenario]:
                  num_steps=200, lumped=[((8, 8, 10), 2, 50.0, 0.0, 1.0, 0.0),
                                         ((4, 9, 6), 0, 0.0, 2e-13, 2.0, 0.01)],
                  cpml=oe.CpmlBoundaries.uniform(4), probes=[(2, (8, 8, 10)), (0, (4, 9, 6))]),
+    ]
+
+
+def upml_scenarios() -> List[Scenario]:
+    """The reference's UPML: short runs (it grows without bound), all faces
+    and partial faces, with a dielectric and Mur on other faces."""
+    E = oe.Excitation
+    return [
+        Scenario("upml_all_20", (20, 21, 22), 0.5e-3,
+                 excitations=[E.gaussian(3e9, 0.5, 2, (10, 10, 11))], num_steps=40, sample_interval=5,
+                 track_peak=True, upml=oe.PmlBoundaries.uniform(4),
+                 probes=[(2, (10, 10, 11)), (2, (2, 3, 4)), (4, (18, 18, 19))]),
+        Scenario("upml_partial", (17, 13, 23), 0.5e-3,
+                 materials=[(3.0, 1.0, 0.0, 0.0, (3, 14, 2, 11, 5, 18))],
+                 excitations=[E.gaussian(4e9, 0.5, 1, (8, 6, 11))], num_steps=35,
+                 upml=oe.PmlBoundaries(layers=(3, 0, 5, 4, 0, 6), grading_order=4.0, reflection_coeff=1e-5),
+                 mur=oe.MurAbcConfig(enabled=(0, 1, 0, 0, 1, 0)),
+                 probes=[(1, (8, 6, 11)), (3, (1, 1, 1))]),
     ]

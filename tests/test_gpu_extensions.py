@@ -5,7 +5,7 @@ import pytest
 
 import oracle
 import openems_b200 as oe
-from scenarios import dispersive_scenarios, run_engine, run_oracle
+from scenarios import dispersive_scenarios, run_engine, run_oracle, upml_scenarios
 from test_gpu_parity import KERNELS, assert_parity
 
 pytestmark = pytest.mark.gpu
@@ -15,6 +15,26 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("sc", dispersive_scenarios(), ids=lambda s: s.name)
 def test_extension_scenarios(sc, kernels):
     assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
+
+
+@pytest.mark.parametrize("kernels", KERNELS)
+@pytest.mark.parametrize("sc", upml_scenarios(), ids=lambda s: s.name)
+def test_upml_scenarios(sc, kernels):
+    """The reference's UPML, bit-exact over short runs (it diverges later)."""
+    assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
+
+
+def test_upml_reset_and_graphs():
+    sc = upml_scenarios()[0]
+    a, b = run_engine(sc, graphs=True), run_engine(sc, graphs=False)
+    assert np.array_equal(a["fields"], b["fields"])
+    eng = a["engine"]
+    eng.reset()
+    dt = a["operator"].timestep()
+    sched = [oe.ScheduledExcitation.from_excitation(x, 0, sc.num_steps, dt) for x in sc.excitations]
+    eng.run_batch(oe.EngineBatch(num_steps=sc.num_steps, excitations=sched))
+    e, h = eng.read_fields()
+    assert np.array_equal(np.concatenate([e, h]), a["fields"])
 
 
 def test_compressed_with_dispersive():
