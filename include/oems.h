@@ -78,6 +78,9 @@ typedef struct oems_engine oems_engine;
 #define OEMS_ENGINE_REGISTER_KERNELS 0x10u /* only the register-blocked update kernels */
 #define OEMS_ENGINE_STAGED_KERNELS 0x20u   /* only the bulk-async (TMA) staged update
                                               kernels, where their stages fit */
+#define OEMS_ENGINE_SPLIT_KERNELS 0x40u    /* with CPML: staged kernels on the box
+                                              between the x / y slabs, register
+                                              kernels on those slabs */
 
 /* What Operator hands to EngineImpl::new: dimensions, dt, cell sizes and the
  * 12 per-cell coefficient arrays (src/fdtd/operator.rs:21-38, :145-185). */
@@ -403,8 +406,10 @@ OEMS_API oems_status oems_field_energy_noalloc(const float* const fields[6], uin
  * totals. */
 OEMS_API oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable);
 /* Launch shape chosen for the update kernels (valid after the first batch):
- * staged = 1 for the bulk-async staged kernels, threads per CTA, x-planes per
- * work item, rows per tile (staged), pipeline stages (staged), CTAs. */
+ * staged = 1 for the bulk-async staged kernels (2: staged on the box between
+ * the x / y CPML slabs, register kernels on the slabs), threads per CTA, x-planes per
+ * work item, rows per tile (staged), pipeline stages (staged) or the L2
+ * prefetch distance in x-planes (register kernels, 0 = none), CTAs. */
 OEMS_API oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged,
                                              int32_t* threads, int32_t* ichunk,
                                              int32_t* rows_per_tile, int32_t* stages,

@@ -25,6 +25,7 @@ ENGINE_NO_AUTOTUNE = 0x2
 ENGINE_NO_GRAPHS = 0x4
 ENGINE_REGISTER_KERNELS = 0x10
 ENGINE_STAGED_KERNELS = 0x20
+ENGINE_SPLIT_KERNELS = 0x40
 
 
 class OpenEMSError(Exception):

@@ -222,6 +222,11 @@ __global__ void k_energy_final(const double* partials, double* out) {
 struct LaunchShape {
   int block = 256;
   int ichunk = 8;
+  int pf = 0;  // L2 prefetch distance (register kernels)
+  // split: staged kernels (tma) on the interior box, register CPML kernels
+  // with these settings on the x / y slabs
+  bool split = false;
+  int sh_block = 256, sh_ichunk = 8, grid_sh = 0, grid_se = 0;
   int grid_h = 0;
   int grid_e = 0;
   bool tma = false;
@@ -374,6 +379,7 @@ struct oems_engine {
   oems::DevBuf<int> d_err;  // device error word (bounded waits that gave up)
 
   oems::LaunchShape shape;
+  oems::Geom gs{};  // shell segments of a split shape
   bool tuned = false;
 
   // graphs keyed by span length; invalidated when any baked pointer changes
@@ -415,6 +421,49 @@ static Geom make_geom(const oems_engine* en, int block, int ichunk) {
   g.ichunk = ichunk;
   g.nchunks = (g.nx + ichunk - 1) / ichunk;
   g.work = g.tiles * g.nchunks;
+  g.nseg = 1;
+  g.seg[0] = Seg{0, g.nx, 0, g.plane4, g.tiles, 0};
+  return g;
+}
+
+// Interior box between the x and y CPML slabs: planes [i_lo, i_hi), rows
+// [j_lo, j_hi) (all of z).  Empty when the slabs leave nothing between them.
+static bool cpml_interior(const oems_engine* en, int* i_lo, int* i_hi, int* j_lo, int* j_hi) {
+  if (!en->cpml.on) return false;
+  const CpmlArgs& cp = en->cpml.args;
+  *i_lo = cp.L[0];
+  *i_hi = en->nx - cp.L[1];
+  *j_lo = cp.L[2];
+  *j_hi = en->ny - cp.L[3];
+  return *i_lo < *i_hi && *j_lo < *j_hi;
+}
+
+// The x / y slabs as register-kernel segments: whole planes of the x slabs,
+// slab rows of the planes between them.
+static Geom make_shell_geom(const oems_engine* en, int block, int ichunk) {
+  Geom g = make_geom(en, block, ichunk);
+  int ilo, ihi, jlo, jhi;
+  cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
+  const int nq = g.nzq;
+  const int segs[4][4] = {{0, ilo, 0, g.plane4},
+                          {ihi, g.nx, 0, g.plane4},
+                          {ilo, ihi, 0, jlo * nq},
+                          {ilo, ihi, jhi * nq, g.plane4}};
+  g.nseg = 0;
+  int work = 0;
+  for (const auto& sg : segs) {
+    if (sg[1] <= sg[0] || sg[3] <= sg[2]) continue;
+    Seg S;
+    S.i0 = sg[0];
+    S.i1 = sg[1];
+    S.c0 = sg[2];
+    S.c1 = sg[3];
+    S.tiles = (S.c1 - S.c0 + block - 1) / block;
+    S.work0 = work;
+    work += S.tiles * ((S.i1 - S.i0 + ichunk - 1) / ichunk);
+    g.seg[g.nseg++] = S;
+  }
+  g.work = work;
   return g;
 }
 
@@ -483,13 +532,19 @@ static size_t table_smem(const oems_engine* en) {
 // Stage layout of the bulk-staged kernels for tiles of TJ rows.  Returns the
 // dynamic shared memory in bytes, 0 if fewer than 2 stages fit in `limit`.
 static size_t make_tma_geom(const oems_engine* en, int TJ, int ichunk, int nconsumer, size_t limit, int ns_max,
-                            TmaGeom& t) {
+                            TmaGeom& t, bool interior = false) {
   const int nzp = en->g.nzp;
   t = TmaGeom{};
+  t.i_lo = 0;
+  t.i_hi = en->nx;
+  t.j_lo = 0;
+  t.j_hi = en->ny;
+  if (interior && !cpml_interior(en, &t.i_lo, &t.i_hi, &t.j_lo, &t.j_hi)) return 0;
+  t.xy_psi = en->cpml.on && !interior;
   t.TJ = TJ;
-  t.ntiles = (en->ny + TJ - 1) / TJ;
+  t.ntiles = (t.j_hi - t.j_lo + TJ - 1) / TJ;
   t.ichunk = ichunk;
-  t.nitems = t.ntiles * ((en->nx + ichunk - 1) / ichunk);
+  t.nitems = t.ntiles * ((t.i_hi - t.i_lo + ichunk - 1) / ichunk);
   t.nconsumer = nconsumer;
   int off = 0;
   t.off_f = off;
@@ -503,9 +558,9 @@ static size_t make_tma_geom(const oems_engine* en, int TJ, int ichunk, int ncons
     const CpmlArgs& cp = en->cpml.args;
     t.zwmax = std::max(cp.zw[0], cp.zw[1]);
     t.off_px = off;
-    off += 2 * TJ * nzp;
+    if (t.xy_psi) off += 2 * TJ * nzp;
     t.off_py = off;
-    off += 2 * TJ * nzp;
+    if (t.xy_psi) off += 2 * TJ * nzp;
     t.off_pz = off;
     off += 4 * TJ * t.zwmax;
     t.prof_floats = 0;
@@ -553,6 +608,14 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
     OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_update_tma<true>,
                                                             s.nconsumer + 32, s.smem));
     s.grid_h = s.grid_e = std::max(1, std::min(s.tg.nitems, std::max(1, occ) * sms));
+    if (s.split) {
+      int oh = 0, oe = 0;
+      OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oh, (const void*)pick_h(0, true), s.sh_block, 0));
+      OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oe, (const void*)pick_e(0, true), s.sh_block, 0));
+      const Geom gs = make_shell_geom(en, s.sh_block, s.sh_ichunk);
+      s.grid_sh = std::max(1, std::min(gs.work, std::max(1, oh) * sms));
+      s.grid_se = std::max(1, std::min(gs.work, std::max(1, oe) * sms));
+    }
     return OEMS_OK;
   }
   const size_t smem = table_smem(en);
@@ -570,6 +633,8 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
 static void apply_shape(oems_engine* en, const LaunchShape& s) {
   en->shape = s;
   en->g = make_geom(en, s.block, s.ichunk);
+  en->g.pf = s.tma ? 0 : s.pf;
+  if (s.split) en->gs = make_shell_geom(en, s.sh_block, s.sh_ichunk);
   en->graph_epoch++;
 }
 
@@ -593,6 +658,11 @@ static cudaError_t launch_h(oems_engine* en) {
   if (en->shape.tma) {
     TmaArgs a = tma_args(en, true);
     k_update_tma<true><<<en->shape.grid_h, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
+    if (en->shape.split) {
+      HArgs b = h_args(en);
+      b.g = en->gs;
+      pick_h(0, true)<<<en->shape.grid_sh, en->shape.sh_block, 0, en->stream>>>(b);
+    }
     return cudaGetLastError();
   }
   HArgs a = h_args(en);
@@ -603,6 +673,11 @@ static cudaError_t launch_e(oems_engine* en) {
   if (en->shape.tma) {
     TmaArgs a = tma_args(en, false);
     k_update_tma<false><<<en->shape.grid_e, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
+    if (en->shape.split) {
+      EArgs b = e_args(en);
+      b.g = en->gs;
+      pick_e(0, true)<<<en->shape.grid_se, en->shape.sh_block, 0, en->stream>>>(b);
+    }
     return cudaGetLastError();
   }
   EArgs a = e_args(en);
@@ -711,7 +786,9 @@ static int ext_kernels(const oems_engine* en) {
   return (en->mur.on ? 3 : 0) + (en->upml.on ? 4 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
 }
 
-static int kernels_per_step(const oems_engine* en) { return 2 + ext_kernels(en) + post_kernels(en); }
+static int kernels_per_step(const oems_engine* en) {
+  return (en->shape.split ? 4 : 2) + ext_kernels(en) + post_kernels(en);
+}
 
 // Launches `steps` timesteps directly (no graph).
 static cudaError_t launch_upml(oems_engine* en, bool h, bool pre) {
@@ -892,11 +969,28 @@ static std::mutex& tune_mutex() {
 // the state (fields and psi are saved and restored), keeps the fastest.
 static oems_status autotune(oems_engine* en) {
   en->tuned = true;
-  const bool want_reg = !(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0;
-  const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0;
+  int ilo, ihi, jlo, jhi;
+  const bool can_split = en->id_bytes == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
+  const bool only_split = (en->flags & OEMS_ENGINE_SPLIT_KERNELS) && can_split;
+  const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split;
+  const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0 && !only_split;
+  // split shapes are tried only on request: at 256^3 with 8-layer CPML the
+  // staged interior plus register slabs measured 36.8 GCells/s against 45.6
+  // for the register kernels on the whole grid (the z-slab lanes of every
+  // warp keep the CPML path in both families)
+  const bool want_split = only_split;
   if (en->flags & OEMS_ENGINE_NO_AUTOTUNE) {
     LaunchShape s;
-    if (!want_reg) {
+    if (only_split) {
+      size_t limit = 0;
+      OEMS_TRY(tma_smem_limit(en, &limit));
+      s.tma = true;
+      s.split = true;
+      s.nconsumer = 256;
+      s.ichunk = 16;
+      s.smem = make_tma_geom(en, std::max(1, std::min(jhi - jlo, 256 / en->g.nzq)), 16, 256, limit, 4, s.tg, true);
+      if (s.smem == 0) s = LaunchShape{};
+    } else if (!want_reg) {
       size_t limit = 0;
       OEMS_TRY(tma_smem_limit(en, &limit));
       s.tma = true;
@@ -910,7 +1004,7 @@ static oems_status autotune(oems_engine* en) {
     return OEMS_OK;
   }
   const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes,
-                    (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0)};
+                    (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0) | (want_split ? 8 : 0)};
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
     auto hit = tune_cache().find(key);
@@ -933,20 +1027,24 @@ static oems_status autotune(oems_engine* en) {
   float best_ms = 1e30f;
   std::vector<LaunchShape> cands;
   for (int b : {256, 512})
-    for (int c : {4, 8, 16, 32}) {
-      if (c > 2 * en->nx && c != 4) continue;
-      LaunchShape s;
-      s.block = b;
-      s.ichunk = c;
-      if (want_reg) cands.push_back(s);
-    }
+    for (int c : {4, 8, 16, 32})
+      for (int pf : {0, 2}) {
+        if (c > 2 * en->nx && c != 4) continue;
+        if (pf >= c) continue;
+        LaunchShape s;
+        s.block = b;
+        s.ichunk = c;
+        s.pf = pf;
+        if (want_reg) cands.push_back(s);
+      }
   if (want_tma) {
     size_t limit = 0;
     OEMS_TRY(tma_smem_limit(en, &limit));
     for (int nc : {128, 256})
       for (int per : {1, 2}) {
         const int tj = std::max(1, std::min(en->ny, per * nc / en->g.nzq));
-        for (int c : {8, 16, 32})
+        for (int c : {8, 16, 32}) {
+          int last_ns = 0;
           for (int ns : {4, 3}) {
             if (c > 2 * en->nx && c != 8) continue;
             LaunchShape s;
@@ -955,9 +1053,34 @@ static oems_status autotune(oems_engine* en) {
             s.ichunk = c;
             s.smem = make_tma_geom(en, tj, c, nc, limit, ns, s.tg);
             if (s.smem == 0) continue;
-            if (ns == 3 && s.tg.NS < 3) continue;  // same as the ns = 4 candidate
+            if (s.tg.NS == last_ns) continue;  // capped by shared memory: same shape
+            last_ns = s.tg.NS;
             cands.push_back(s);
           }
+        }
+      }
+  }
+  if (want_split) {
+    size_t limit = 0;
+    OEMS_TRY(tma_smem_limit(en, &limit));
+    for (int nc : {128, 192, 256})
+      for (int per : {1, 2}) {
+        const int tj = std::max(1, std::min(jhi - jlo, per * nc / en->g.nzq));
+        for (int c : {8, 16, 32}) {
+          int last_ns = 0;
+          for (int ns : {6, 5, 4, 3}) {
+            if (c > 2 * en->nx && c != 8) continue;
+            LaunchShape s;
+            s.tma = true;
+            s.split = true;
+            s.nconsumer = nc;
+            s.ichunk = c;
+            s.smem = make_tma_geom(en, tj, c, nc, limit, ns, s.tg, true);
+            if (s.smem == 0 || s.tg.NS == last_ns) continue;
+            last_ns = s.tg.NS;
+            cands.push_back(s);
+          }
+        }
       }
   }
   oems_status st = OEMS_OK;
@@ -2324,11 +2447,11 @@ oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged, 
                                     int32_t* rows_per_tile, int32_t* stages, int32_t* grid) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   const LaunchShape& s = engine->shape;
-  if (staged) *staged = s.tma ? 1 : 0;
+  if (staged) *staged = s.split ? 2 : s.tma ? 1 : 0;
   if (threads) *threads = s.tma ? s.nconsumer + 32 : s.block;
   if (ichunk) *ichunk = s.ichunk;
   if (rows_per_tile) *rows_per_tile = s.tma ? s.tg.TJ : 0;
-  if (stages) *stages = s.tma ? s.tg.NS : 0;
+  if (stages) *stages = s.tma ? s.tg.NS : s.pf;
   if (grid) *grid = s.grid_h;
   return OEMS_OK;
 }

@@ -36,6 +36,16 @@ namespace oems {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// A segment of the update: x-planes [i0, i1) x float4 chunks [c0, c1) of the
+// flattened (j, k) plane (c0, c1 on row boundaries), cut into tiles of one
+// CTA's chunks and runs of `ichunk` planes; work items of all segments are
+// numbered consecutively from work0.
+struct Seg {
+  int i0, i1, c0, c1;
+  int tiles, work0;
+};
+constexpr int kMaxSeg = 4;
+
 struct Geom {
   int nx, ny, nz, nzp, nzq;  // nzq = nzp / 4 float4 chunks per row
   long long plane;           // floats per x-plane = ny * nzp
@@ -43,8 +53,44 @@ struct Geom {
   int tiles;                 // CTA tiles per x-plane
   int ichunk;                // x-planes per work item
   int nchunks;               // ceil(nx / ichunk)
-  int work;                  // tiles * nchunks
+  int work;                  // work items over all segments
+  int pf;                    // L2 prefetch distance in x-planes (0 = off)
+  int nseg;                  // segments (1 = the whole grid)
+  Seg seg[kMaxSeg];
 };
+
+// Work item w -> segment, tile and plane run.
+struct Item {
+  int c0, c1, i0, i1, tile;
+};
+__device__ __forceinline__ Item work_item(const Geom& g, int w) {
+  int s = 0;
+  while (s + 1 < g.nseg && w >= g.seg[s + 1].work0) ++s;
+  const Seg& S = g.seg[s];
+  const int lw = w - S.work0;
+  Item it;
+  it.tile = lw % S.tiles;
+  it.c0 = S.c0 + it.tile * (int)blockDim.x;
+  it.c1 = min(it.c0 + (int)blockDim.x, S.c1);
+  it.i0 = S.i0 + (lw / S.tiles) * g.ichunk;
+  it.i1 = min(it.i0 + g.ichunk, S.i1);
+  return it;
+}
+
+// One thread per CTA asks L2 for the CTA's slice of plane p of an array ahead
+// of the loads (cp.async.bulk.prefetch: no registers, no completion to wait
+// for).  The slice is the tile's contiguous floats [o, o + n), widened by
+// `lo` floats before and `hi` after for the y-neighbour row, clamped to the
+// array; every bound is a multiple of 4 floats, so the 16-byte rule holds.
+__device__ __forceinline__ void l2_prefetch(const float* arr, long long o, long long n, long long limit) {
+  if (o < 0) {
+    n += o;
+    o = 0;
+  }
+  if (o + n > limit) n = limit - o;
+  if (n <= 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(arr + o), "r"((uint32_t)(n * 4)) : "memory");
+}
 
 // CPML state on the device.  Faces: 0 xmin 1 xmax 2 ymin 3 ymax 4 zmin 5 zmax.
 // psi layout per face:
@@ -241,6 +287,43 @@ __device__ __forceinline__ SlabInfo slab_info(const CpmlArgs& cp, const Geom& g,
   return s;
 }
 
+// L2 prefetch of one CTA's slice of an x-plane for the H / E update, issued
+// by thread 0 of the CTA, whose chunk is the first of the slice: o is that
+// thread's offset in the plane to prefetch, tn the slice length in floats.
+template <int kIdBytes>
+__device__ __forceinline__ void prefetch_h_plane(const HArgs& a, long long o, long long tn) {
+  const long long lim = (long long)a.g.nx * a.g.plane;
+  l2_prefetch(a.ex, o, tn + a.g.nzp, lim);
+  l2_prefetch(a.ey, o, tn, lim);
+  l2_prefetch(a.ez, o, tn + a.g.nzp, lim);
+  l2_prefetch(a.hx, o, tn, lim);
+  l2_prefetch(a.hy, o, tn, lim);
+  l2_prefetch(a.hz, o, tn, lim);
+  if constexpr (kIdBytes == 0)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l2_prefetch(a.da[c], o, tn, lim);
+      l2_prefetch(a.db[c], o, tn, lim);
+    }
+}
+
+template <int kIdBytes>
+__device__ __forceinline__ void prefetch_e_plane(const EArgs& a, long long o, long long tn) {
+  const long long lim = (long long)a.g.nx * a.g.plane;
+  l2_prefetch(a.hx, o - a.g.nzp, tn + a.g.nzp, lim);
+  l2_prefetch(a.hy, o, tn, lim);
+  l2_prefetch(a.hz, o - a.g.nzp, tn + a.g.nzp, lim);
+  l2_prefetch(a.ex, o, tn, lim);
+  l2_prefetch(a.ey, o, tn, lim);
+  l2_prefetch(a.ez, o, tn, lim);
+  if constexpr (kIdBytes == 0)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l2_prefetch(a.ca[c], o, tn, lim);
+      l2_prefetch(a.cb[c], o, tn, lim);
+    }
+}
+
 // H half-step: H = da*H + db*curl(E).
 template <int kIdBytes, bool kCpml>
 __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
@@ -249,25 +332,30 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
   const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
   const int lane = threadIdx.x & 31;
   for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
-    const int tile = w % g.tiles;
-    const int chunk = w / g.tiles;
-    int c = tile * blockDim.x + threadIdx.x;
-    const bool valid = c < g.plane4;
-    if (!valid) c = g.plane4 - 1;
+    const Item it = work_item(g, w);
+    int c = it.c0 + (int)threadIdx.x;
+    const bool valid = c < it.c1;
+    if (!valid) c = it.c1 - 1;
     const int j = c / g.nzq;
     const int k0 = (c - j * g.nzq) * 4;
-    const int i0 = chunk * g.ichunk;
-    const int i1 = min(i0 + g.ichunk, g.nx);
+    const int i0 = it.i0;
+    const int i1 = it.i1;
     const bool has_jp = j + 1 < g.ny;
     const bool need_kn = lane == 31 && k0 + 4 < g.nz;
     unsigned live = 0;
 #pragma unroll
     for (int e = 0; e < 4; ++e) live |= (k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
+    if (g.pf > 0 && threadIdx.x == 0) {
+      const long long tn = (long long)(it.c1 - it.c0) * 4;
+      for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_h_plane<kIdBytes>(a, q + p * g.plane, tn);
+    }
     float4 ey4 = ld_nc4(a.ey + q);
     float4 ez4 = ld_nc4(a.ez + q);
     for (int i = i0; i < i1; ++i, q += g.plane) {
       const bool has_ip = i + 1 < g.nx;
+      if (g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+        prefetch_h_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       // ---- every load of this plane first
       const float4 ex4 = ld_nc4(a.ex + q);
       const float4 ey1 = has_ip ? ld_nc4(a.ey + q + g.plane) : ey4;
@@ -396,15 +484,14 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
   const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
   const int lane = threadIdx.x & 31;
   for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
-    const int tile = w % g.tiles;
-    const int chunk = w / g.tiles;
-    int c = tile * blockDim.x + threadIdx.x;
-    const bool valid = c < g.plane4;
-    if (!valid) c = g.plane4 - 1;
+    const Item it = work_item(g, w);
+    int c = it.c0 + (int)threadIdx.x;
+    const bool valid = c < it.c1;
+    if (!valid) c = it.c1 - 1;
     const int j = c / g.nzq;
     const int k0 = (c - j * g.nzq) * 4;
-    const int i0 = chunk * g.ichunk;
-    const int i1 = min(i0 + g.ichunk, g.nx);
+    const int i0 = it.i0;
+    const int i1 = it.i1;
     const bool has_jm = j >= 1;
     const bool need_km = lane == 0 && k0 >= 4;
     // elements that are updated: 1 <= k < nz (i >= 1 and j >= 1 checked per plane)
@@ -412,12 +499,18 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
 #pragma unroll
     for (int e = 0; e < 4; ++e) live_k |= (k0 + e >= 1 && k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
+    if (g.pf > 0 && threadIdx.x == 0) {
+      const long long tn = (long long)(it.c1 - it.c0) * 4;
+      for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_e_plane<kIdBytes>(a, q + p * g.plane, tn);
+    }
     float4 hym4 = zero4(), hzm4 = zero4();  // H at i-1
     if (i0 > 0) {
       hym4 = ld_nc4(a.hy + q - g.plane);
       hzm4 = ld_nc4(a.hz + q - g.plane);
     }
     for (int i = i0; i < i1; ++i, q += g.plane) {
+      if (g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+        prefetch_e_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       const bool upd = i >= 1 && has_jm;
       const unsigned live = upd ? live_k : 0u;
       // ---- every load of this plane first

@@ -37,9 +37,12 @@ namespace oems {
 
 struct TmaGeom {
   int TJ;            // rows per tile
-  int ntiles;        // ceil(ny / TJ)
+  int ntiles;        // ceil((j_hi - j_lo) / TJ)
   int ichunk;        // x-planes per work item
-  int nitems;        // ntiles * ceil(nx / ichunk)
+  int nitems;        // ntiles * ceil((i_hi - i_lo) / ichunk)
+  int i_lo, i_hi;    // x-planes updated (the whole grid, or the interior
+  int j_lo, j_hi;    // box between the x and y CPML slabs)
+  int xy_psi;        // stages hold x / y slab psi rows
   int NS;            // pipeline stages
   int stage_floats;  // floats per stage (multiple of 4)
   int off_f, off_u, off_c, off_px, off_py, off_pz;  // float offsets inside a stage
@@ -127,8 +130,8 @@ __device__ __forceinline__ uint32_t bundle_bytes_or_issue(const TmaArgs& a, int 
                                                           uint64_t* bar, bool issue) {
   const Geom& g = a.g;
   const TmaGeom& t = a.t;
-  const int j0 = tile * t.TJ;
-  const int rows_u = min(t.TJ, g.ny - j0);
+  const int j0 = t.j_lo + tile * t.TJ;
+  const int rows_u = min(t.TJ, t.j_hi - j0);
   const size_t rowb = (size_t)g.nzp * sizeof(float);
   uint32_t bytes = 0;
   // F arrays: H kernel rows j0..j0+rows_u (+1 if it exists); E kernel rows j0-1..j0+rows_u-1.
@@ -165,7 +168,7 @@ __device__ __forceinline__ uint32_t bundle_bytes_or_issue(const TmaArgs& a, int 
     float* const* psi = kIsH ? &cp.psi_h[0][0] : &cp.psi_e[0][0];  // [face*2 + slot]
     // x slab: whole plane rows j0..j0+rows_u
     int lx;
-    const int fx = cpml_face(cp, 0, p, lx);
+    const int fx = t.xy_psi ? cpml_face(cp, 0, p, lx) : -1;
     if (fx >= 0) {
       const long long src = ((long long)lx * g.ny + j0) * g.nzp;
       for (int s = 0; s < 2; ++s) {
@@ -175,7 +178,7 @@ __device__ __forceinline__ uint32_t bundle_bytes_or_issue(const TmaArgs& a, int 
     }
     // y slabs: rows of the tile inside each y face
     for (int f = 2; f < 4; ++f) {
-      if (cp.L[f] == 0) continue;
+      if (cp.L[f] == 0 || !t.xy_psi) continue;
       const int lo = max(j0, cp.start[f]), hi = min(j0 + rows_u, cp.start[f] + cp.L[f]);
       if (hi <= lo) continue;
       const uint32_t nb = (uint32_t)((hi - lo) * rowb);
@@ -208,7 +211,7 @@ __device__ __forceinline__ void for_each_bundle(const TmaArgs& a, Fn&& fn) {
   const TmaGeom& t = a.t;
   for (int w = blockIdx.x; w < t.nitems; w += gridDim.x) {
     const int chunk = w / t.ntiles, tile = w % t.ntiles;
-    const int i0 = chunk * t.ichunk, i1 = min(i0 + t.ichunk, g.nx);
+    const int i0 = t.i_lo + chunk * t.ichunk, i1 = min(i0 + t.ichunk, t.i_hi);
     if (kIsH) {
       for (int p = i0; p < i1; ++p)
         if (!fn(tile, p, kFull)) return;
@@ -266,8 +269,8 @@ __device__ __forceinline__ void h_plane(const TmaArgs& a, const float* sprof_, c
                                         int tile, int i, int ctid) {
   const Geom& g = a.g;
   const TmaGeom& t = a.t;
-  const int j0 = tile * t.TJ;
-  const int rows_u = min(t.TJ, g.ny - j0);
+  const int j0 = t.j_lo + tile * t.TJ;
+  const int rows_u = min(t.TJ, t.j_hi - j0);
   const int nchunk = rows_u * g.nzq;
   const int FS = (t.TJ + 1) * g.nzp;  // F array stride
   const int US = t.TJ * g.nzp;        // U / C array stride
@@ -388,8 +391,8 @@ __device__ __forceinline__ void e_plane(const TmaArgs& a, const float* sprof_, c
   const Geom& g = a.g;
   const TmaGeom& t = a.t;
   if (i == 0) return;
-  const int j0 = tile * t.TJ;
-  const int rows_u = min(t.TJ, g.ny - j0);
+  const int j0 = t.j_lo + tile * t.TJ;
+  const int rows_u = min(t.TJ, t.j_hi - j0);
   const int nchunk = rows_u * g.nzq;
   const int FS = (t.TJ + 1) * g.nzp;
   const int US = t.TJ * g.nzp;

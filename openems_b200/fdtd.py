@@ -866,12 +866,14 @@ class Engine:
     def __init__(self, operator: Operator, engine_type: EngineType = EngineType.Cuda, *,
                  device: int = -1, compressed: bool = False, autotune: bool = True,
                  graphs: bool = True, kernels: str = "auto"):
-        """kernels: "auto" (tuner picks), "register" or "staged" (bulk-async)."""
+        """kernels: "auto" (tuner picks), "register", "staged" (bulk-async) or
+        "split" (staged between the x / y CPML slabs, register on them)."""
         if engine_type is not EngineType.Cuda:
             raise N.ConfigError("only the CUDA engine exists")
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
             | (0 if graphs else N.ENGINE_NO_GRAPHS) \
-            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS}[kernels]
+            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS,
+               "split": N.ENGINE_SPLIT_KERNELS}[kernels]
         desc = N.OperatorDesc()
         N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))
         h = ctypes.c_void_p()
