@@ -193,8 +193,11 @@ typedef struct oems_upml_desc {
  *   kind 1 Lorentz  params (omega_0, gamma, delta_eps) :134-196, as the
  *          reference (first order in J; unstable for usual parameters)
  *   kind 2 Debye    params (tau, delta_eps)             :570-630
- *   kind 3 Lorentz, second order: P' = a P + b P_prev + c E,
- *          E -= (P' - P) / (eps0 eps_inf)  (no counterpart in the reference)
+ *   kind 3 Lorentz, second order: P' = a P + b P_prev + c E_n,
+ *          E -= (P' - P) / (eps0 eps_inf), E_n the field before the E
+ *          update (no counterpart in the reference)
+ *   kind 4 Drude as the same recursion with omega_0 = 0, params (omega_p,
+ *          gamma): stable where kind 0 grows (gamma << omega_p)
  * Angular frequencies in rad/s.  eps_inf divides the E correction; 1 gives
  * the reference's coefficients. */
 typedef struct oems_dispersive_desc {

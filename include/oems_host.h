@@ -48,6 +48,11 @@ OEMS_API oems_status oems_operator_clone(const oems_operator* op, oems_operator*
 OEMS_API oems_status oems_operator_set_material(oems_operator* op, double eps_r, double mu_r,
                                        double sigma_e, double sigma_m, const uint64_t region[6]);
 OEMS_API oems_status oems_operator_set_pec(oems_operator* op, const uint64_t region[6]);
+/* set_material's coefficients on a list of cells (ncells x (i, j, k)), for
+ * shapes other than boxes (spheres, shells); later calls overwrite. */
+OEMS_API oems_status oems_operator_set_material_cells(oems_operator* op, double eps_r, double mu_r,
+                                                      double sigma_e, double sigma_m, const uint64_t* cells,
+                                                      uint64_t ncells);
 OEMS_API oems_status oems_operator_info(const oems_operator* op, uint64_t dims[3], double* dt,
                                double delta[3]);
 /* Borrowed pointers to the 12 coefficient arrays (ca0 ca1 ca2 cb0 cb1 cb2 da0

@@ -242,6 +242,7 @@ SIGNATURES = {
     "oems_operator_info": (c_i32, [P, c_u64 * 3, ctypes.POINTER(c_f64), c_f64 * 3]),
     "oems_operator_coefficients": (c_i32, [P, PF * 12]),
     "oems_operator_clone": (c_i32, [P, ctypes.POINTER(P)]),
+    "oems_operator_set_material_cells": (c_i32, [P, c_f64, c_f64, c_f64, c_f64, P, c_u64]),
     "oems_sweep_create": (c_i32, [c_i32, c_u32, c_u32, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(P)]),
     "oems_sweep_destroy": (None, [P]),
     "oems_sweep_add": (c_i32, [P, ctypes.POINTER(SweepInstanceC), ctypes.POINTER(c_i32)]),

@@ -744,12 +744,20 @@ static int blocks_for(long long n, int threads) { return (int)((n + threads - 1)
 
 static cudaError_t launch_upml(oems_engine* en, bool h, bool pre);
 
+static int second_order_disp(const oems_engine* en) {
+  int k = 0;
+  for (const DispHost& d : en->disp) k += d.args.kind >= 3 ? 1 : 0;
+  return k;
+}
+
 static cudaError_t launch_pre_e(oems_engine* en) {
   if (en->mur.on) {
     k_mur_pre<<<blocks_for(en->mur.args.total, 256), 256, 0, en->stream>>>(en->mur.args);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  for (const DispHost& d : en->disp)
+    if (d.args.kind >= 3) k_dispersive_pre<<<blocks_for(d.args.n, 256), 256, 0, en->stream>>>(d.args);
   // UPML innermost: its pre hook right before the E update
   if (en->upml.on) return launch_upml(en, false, true);
   return cudaSuccess;
@@ -783,7 +791,8 @@ static cudaError_t launch_post_e(oems_engine* en) {
 }
 
 static int ext_kernels(const oems_engine* en) {
-  return (en->mur.on ? 3 : 0) + (en->upml.on ? 4 : 0) + (int)en->disp.size() + (en->rlc.q.empty() ? 0 : 1);
+  return (en->mur.on ? 3 : 0) + (en->upml.on ? 4 : 0) + (int)en->disp.size() + second_order_disp(en) +
+         (en->rlc.q.empty() ? 0 : 1);
 }
 
 static int kernels_per_step(const oems_engine* en) {
@@ -1751,7 +1760,7 @@ oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc
 oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersive_desc* d, const uint64_t* cells,
                                        uint64_t ncells) {
   if (!engine || !d || (!cells && ncells)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (d->kind < 0 || d->kind > 3) return fail(OEMS_ERR_MATERIAL, "unknown dispersive material kind");
+  if (d->kind < 0 || d->kind > 4) return fail(OEMS_ERR_MATERIAL, "unknown dispersive material kind");
   if (!(d->eps_inf > 0.0)) return fail(OEMS_ERR_MATERIAL, "eps_inf must be positive");
   if (ncells == 0) return fail(OEMS_ERR_MATERIAL, "a dispersive material needs at least one cell");
   DeviceGuard guard(engine->device);
@@ -1771,6 +1780,12 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
     A.b = (float)((p[1] * dt / 2.0 - 1.0) / den);
     A.c = (float)(kEps0 * p[2] * p[0] * p[0] * dt * dt / den);
     A.c2 = (float)(1.0 / (kEps0 * d->eps_inf));
+  } else if (d->kind == 4) {  // Drude as a P recursion: P'' + g P' = eps0 wp^2 E
+    const double den = 1.0 + p[1] * dt / 2.0;
+    A.a = (float)(2.0 / den);
+    A.b = (float)((p[1] * dt / 2.0 - 1.0) / den);
+    A.c = (float)(kEps0 * p[0] * p[0] * dt * dt / den);
+    A.c2 = (float)(1.0 / (kEps0 * d->eps_inf));
   } else {  // DebyeMaterial::new (:570-592)
     const double den = 2.0 * p[0] + dt;
     A.a = (float)((2.0 * p[0] - dt) / den);
@@ -1786,13 +1801,14 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
     q[m] = ((long long)c[0] * engine->ny + (long long)c[1]) * engine->g.nzp + (long long)c[2];
   }
   OEMS_CUDA(h.q->ensure(ncells));
-  OEMS_CUDA(h.state->ensure(6 * ncells));
+  OEMS_CUDA(h.state->ensure(9 * ncells));
   OEMS_CUDA(cudaMemcpy(h.q->p, q.data(), ncells * sizeof(long long), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemset(h.state->p, 0, 6 * ncells * sizeof(float)));
+  OEMS_CUDA(cudaMemset(h.state->p, 0, 9 * ncells * sizeof(float)));
   A.n = (long long)ncells;
   A.q = h.q->p;
   A.st = h.state->p;
   A.pp = h.state->p + 3 * ncells;
+  A.ep = h.state->p + 6 * ncells;
   for (int c = 0; c < 3; ++c) A.e[c] = engine->E(c);
   engine->disp.push_back(std::move(h));
   engine->graph_epoch++;

@@ -8,6 +8,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/oems.h"
@@ -75,11 +76,23 @@ struct oems_operator {
     dt = 0.99 * (1.0 / (kC0 * std::sqrt(inv_sum)));
     const size_t cells = (size_t)(n[0] * n[1] * n[2]);
     // src/fdtd/operator.rs:92-141: vacuum Ca = Da = 1, Cb = dt/(eps0 d), Db = -dt/(mu0 d)
+    float v[12];
     for (int a = 0; a < 3; ++a) {
-      c[a].assign(cells, 1.0f);
-      c[3 + a].assign(cells, (float)(dt / (kEps0 * delta[a])));
-      c[6 + a].assign(cells, 1.0f);
-      c[9 + a].assign(cells, -(float)(dt / (kMu0 * delta[a])));
+      v[a] = 1.0f;
+      v[3 + a] = (float)(dt / (kEps0 * delta[a]));
+      v[6 + a] = 1.0f;
+      v[9 + a] = -(float)(dt / (kMu0 * delta[a]));
+    }
+    // the twelve arrays are independent: fill them on parallel threads when
+    // they are large (hundreds of MB at 256^3)
+    auto fill = [&](int a) { c[a].assign(cells, v[a]); };
+    if (cells < (size_t)1 << 20) {
+      for (int a = 0; a < 12; ++a) fill(a);
+    } else {
+      std::vector<std::thread> t;
+      for (int a = 1; a < 12; ++a) t.emplace_back(fill, a);
+      fill(0);
+      for (auto& x : t) x.join();
     }
   }
 };
@@ -221,6 +234,42 @@ oems_status oems_operator_set_material(oems_operator* op, double eps_r, double m
         std::fill(op->c[9 + a].begin() + q0 + r[4], op->c[9 + a].begin() + q0 + r[5], dbv[a]);
       }
     }
+  return OEMS_OK;
+}
+
+oems_status oems_operator_set_material_cells(oems_operator* op, double eps_r, double mu_r, double sigma_e,
+                                             double sigma_m, const uint64_t* cells, uint64_t ncells) {
+  if (!op || (!cells && ncells)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!(eps_r > 0.0) || !(mu_r > 0.0) || sigma_e < 0.0 || sigma_m < 0.0)
+    return hfail(OEMS_ERR_MATERIAL, "eps_r and mu_r must be positive, conductivities non-negative");
+  for (uint64_t m = 0; m < ncells; ++m)
+    if (cells[3 * m] >= op->n[0] || cells[3 * m + 1] >= op->n[1] || cells[3 * m + 2] >= op->n[2])
+      return hfail(OEMS_ERR_MATERIAL, "material cell outside the grid");
+  // the same coefficients as set_material (src/fdtd/operator.rs:195-220) on
+  // each listed cell
+  const double dt = op->dt;
+  const double eps = eps_r * kEps0;
+  const double loss_e = sigma_e * dt / (2.0 * eps);
+  const float ca_mat = (float)((1.0 - loss_e) / (1.0 + loss_e));
+  const double cb_factor = (dt / eps) / (1.0 + loss_e);
+  const double mu = mu_r * kMu0;
+  const double loss_m = sigma_m * dt / (2.0 * mu);
+  const float da_mat = (float)((1.0 - loss_m) / (1.0 + loss_m));
+  const double db_factor = -(dt / mu) / (1.0 + loss_m);
+  float cbv[3], dbv[3];
+  for (int a = 0; a < 3; ++a) {
+    cbv[a] = (float)(cb_factor / op->delta[a]);
+    dbv[a] = (float)(db_factor / op->delta[a]);
+  }
+  for (uint64_t m = 0; m < ncells; ++m) {
+    const size_t q = op->idx(cells[3 * m], cells[3 * m + 1], cells[3 * m + 2]);
+    for (int a = 0; a < 3; ++a) {
+      op->c[a][q] = ca_mat;
+      op->c[3 + a][q] = cbv[a];
+      op->c[6 + a][q] = da_mat;
+      op->c[9 + a][q] = dbv[a];
+    }
+  }
   return OEMS_OK;
 }
 

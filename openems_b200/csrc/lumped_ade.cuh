@@ -5,8 +5,10 @@
 //   Drude   (:510-535)  j = a j + b e;  e = e - c j
 //   Lorentz (:171-196)  j = a j + c e;  e = e - b j        (as the reference)
 //   Debye   (:604-630)  p' = a p + b e; e = e - c (p' - p) / dt
-//   Lorentz, second order (no counterpart: the reference drops P^{n-1} and
-//   diverges): p' = (a p + b p_prev) + c e; e = e - c2 (p' - p)
+//   second order (no counterpart: the reference's Lorentz drops P^{n-1} and
+//   diverges): p' = (a p + b p_prev) + c e_n; e = e - c2 (p' - p), with e_n
+//   the field before the E update (k_dispersive_pre), as the standard
+//   explicit Lorentz ADE; kind 3 Lorentz, kind 4 Drude (omega_0 = 0)
 // LumpedRlc (src/extensions/lumped_rlc.rs:263-286): e' = v_vv e + v_il int;
 //   int = int + e dt.
 // Arithmetic order and rounding match the f32 reference (no FMA).
@@ -22,9 +24,19 @@ struct DispArgs {
   long long n;
   const long long* q;  // cell (padded linear index)
   float* st;           // [3][n] J or P
-  float* pp;           // [3][n] P at n-1 (second-order Lorentz)
+  float* pp;           // [3][n] P at n-1 (second-order kinds)
+  float* ep;           // [3][n] E^n (second-order kinds)
   float* e[3];
 };
+
+// E^n of the second-order kinds, copied before the E update.
+__global__ void k_dispersive_pre(const DispArgs a) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n) return;
+  const long long q = a.q[m];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) a.ep[(long long)c * a.n + m] = a.e[c][q];
+}
 
 __global__ void k_dispersive(const DispArgs a) {
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -51,7 +63,8 @@ __global__ void k_dispersive(const DispArgs a) {
       *ef = __fsub_rn(e, __fmul_rn(a.c, dpdt));
     } else {
       float* ppp = a.pp + (long long)c * a.n + m;
-      const float pn = __fadd_rn(__fadd_rn(__fmul_rn(a.a, old), __fmul_rn(a.b, *ppp)), __fmul_rn(a.c, e));
+      const float en = a.ep[(long long)c * a.n + m];
+      const float pn = __fadd_rn(__fadd_rn(__fmul_rn(a.a, old), __fmul_rn(a.b, *ppp)), __fmul_rn(a.c, en));
       *ppp = old;
       *sp = pn;
       *ef = __fsub_rn(e, __fmul_rn(a.c2, __fsub_rn(pn, old)));

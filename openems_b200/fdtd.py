@@ -202,14 +202,20 @@ class PmlBoundaries:
 @dataclass
 class DrudeMaterial:
     """DrudeMaterial (src/extensions/dispersive.rs:450-535): omega_p, gamma
-    in rad/s; eps_inf divides the E correction (1 = the reference)."""
+    in rad/s; eps_inf divides the E correction (1 = the reference).
+    second_order False reproduces the reference's update, which grows when
+    gamma << omega_p in a 3D grid; True runs the polarisation recursion
+    P'' + gamma P' = eps0 omega_p^2 E driven by the field before the E
+    update, which stays bounded."""
 
     plasma_frequency: float
     collision_frequency: float
     eps_inf: float = 1.0
+    second_order: bool = False
 
     def to_c(self) -> N.DispersiveDescC:
-        return _disp_desc(0, (self.plasma_frequency, self.collision_frequency), self.eps_inf)
+        return _disp_desc(4 if self.second_order else 0, (self.plasma_frequency, self.collision_frequency),
+                          self.eps_inf)
 
 
 @dataclass
@@ -357,6 +363,12 @@ class Operator:
 
     def set_pec(self, region):
         N.check(N.lib().oems_operator_set_pec(self._h, self._region(region)))
+
+    def set_material_cells(self, eps_r, mu_r, sigma_e, sigma_m, cells):
+        """set_material on a list of cells (n, 3)."""
+        c = np.ascontiguousarray(cells, dtype=np.uint64).reshape(-1, 3)
+        N.check(N.lib().oems_operator_set_material_cells(self._h, eps_r, mu_r, sigma_e, sigma_m,
+                                                         c.ctypes.data, len(c)))
 
     def set_lumped(self, position, direction, resistance=0.0, capacitance=0.0, eps_r=1.0,
                    sigma=0.0) -> float:

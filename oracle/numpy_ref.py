@@ -91,6 +91,10 @@ def dispersive_coeffs(kind: int, params, dt: float, eps_inf: float = 1.0):
     if kind == 0:
         den = 1.0 + p[1] * dt / 2.0
         a, b, c = (1.0 - p[1] * dt / 2.0) / den, EPS0 * p[0] * p[0] * dt / den, dt / (EPS0 * eps_inf)
+    elif kind == 4:  # Drude as a polarisation recursion (omega_0 = 0)
+        den = 1.0 + p[1] * dt / 2.0
+        a, b, c = 2.0 / den, (p[1] * dt / 2.0 - 1.0) / den, EPS0 * p[0] * p[0] * dt * dt / den
+        c2 = 1.0 / (EPS0 * eps_inf)
     elif kind in (1, 3):
         den = 1.0 + p[1] * dt / 2.0
         a = (2.0 - p[0] * p[0] * dt * dt) / den
@@ -105,7 +109,9 @@ def dispersive_coeffs(kind: int, params, dt: float, eps_inf: float = 1.0):
 
 def dispersive_step(kind, coeffs, e, state, prev, dt):
     """One post_update_e of one field value (float32 scalars); returns
-    (e', state', prev').  Drude :510-535, Lorentz :171-196, Debye :604-630."""
+    (e', state', prev').  Drude :510-535, Lorentz :171-196, Debye :604-630;
+    kinds 3 / 4 are driven by the field before the E update, which on a grid
+    without curl (one cell) is the e passed here."""
     a, b, c, c2 = coeffs
     e, state, prev = f32(e), f32(state), f32(prev)
     if kind == 0:

@@ -297,7 +297,8 @@ struct Sim {
     int kind;
     float a, b, c, c2;          // as computed by the reference constructors, f32
     std::vector<int64_t> q;     // cells
-    std::vector<T> j[3], pp[3]; // state (J or P) and P at n-1 (second-order Lorentz)
+    std::vector<T> j[3], pp[3]; // state (J or P) and P at n-1 (second-order kinds)
+    std::vector<T> ep[3];       // E^n, taken before the E update (second-order kinds)
   };
   std::vector<Dispersive> disp;
 
@@ -311,6 +312,15 @@ struct Sim {
   std::vector<Rlc> rlc;
 
   // src/extensions/dispersive.rs:171-196, 510-535, 604-630 (+ second-order Lorentz)
+  // E^n of the second-order kinds, before the E update
+  void capture_dispersive() {
+    for (Dispersive& D : disp) {
+      if (D.kind < 3) continue;
+      for (size_t m = 0; m < D.q.size(); ++m)
+        for (int c = 0; c < 3; ++c) D.ep[c][m] = E[c][D.q[m]];
+    }
+  }
+
   void apply_dispersive() {
     const float dtf = (float)dt;
     for (Dispersive& D : disp) {
@@ -332,10 +342,10 @@ struct Sim {
             D.j[c][m] = pn;
             const T dpdt = (pn - old) / T(dtf);
             ef = e - T(D.c) * dpdt;
-          } else {  // second-order Lorentz
+          } else {  // second-order P recursion (Lorentz, kind 3; Drude, kind 4) driven by E^n
             const T t1 = T(D.a) * old;
             const T t2 = T(D.b) * D.pp[c][m];
-            const T t3 = T(D.c) * e;
+            const T t3 = T(D.c) * D.ep[c][m];
             const T pn = (t1 + t2) + t3;
             D.pp[c][m] = old;
             D.j[c][m] = pn;
@@ -870,6 +880,7 @@ struct Sim {
       update_h();
       if (!upml.empty()) upml_hook(true, false);
       if (!mur.empty()) mur_pre();
+      if (!disp.empty()) capture_dispersive();
       if (!upml.empty()) upml_hook(false, true);
       update_e();
       if (!upml.empty()) upml_hook(false, false);
@@ -1043,6 +1054,7 @@ void orc_reset(orc_sim* s) {
       for (int c = 0; c < 3; ++c) {
         std::fill(D.j[c].begin(), D.j[c].end(), T(0));
         std::fill(D.pp[c].begin(), D.pp[c].end(), T(0));
+        std::fill(D.ep[c].begin(), D.ep[c].end(), T(0));
       }
     for (auto& r : S->rlc) r.i_int = T(0);
     for (auto& d : S->fdumps) std::fill(d.acc.begin(), d.acc.end(), 0.0);
@@ -1287,7 +1299,7 @@ int32_t orc_cpml_profile(const orc_sim* s, int32_t f, double* out) {
 
 int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* p, double eps_inf, const int64_t* cells,
                            int64_t ncells) {
-  if (kind < 0 || kind > 3 || !(eps_inf > 0.0)) return -1;
+  if (kind < 0 || kind > 4 || !(eps_inf > 0.0)) return -1;
   int32_t rc = 0;
   DISPATCH(s, {
     typename std::remove_reference_t<decltype(*S)>::Dispersive D;
@@ -1304,6 +1316,12 @@ int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* p, double eps
       D.b = (float)((g * dt / 2.0 - 1.0) / den);
       D.c = (float)(kEps0 * de * w0 * w0 * dt * dt / den);
       D.c2 = (float)(1.0 / (kEps0 * eps_inf));
+    } else if (kind == 4) {  // Drude as a P recursion: P'' + g P' = eps0 wp^2 E
+      const double wp = p[0], g = p[1], den = 1.0 + g * dt / 2.0;
+      D.a = (float)(2.0 / den);
+      D.b = (float)((g * dt / 2.0 - 1.0) / den);
+      D.c = (float)(kEps0 * wp * wp * dt * dt / den);
+      D.c2 = (float)(1.0 / (kEps0 * eps_inf));
     } else {  // DebyeMaterial::new (dispersive.rs:570-592)
       const double tau = p[0], de = p[1], den = 2.0 * tau + dt;
       D.a = (float)((2.0 * tau - dt) / den);
@@ -1314,6 +1332,7 @@ int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* p, double eps
     for (int c = 0; c < 3; ++c) {
       D.j[c].assign(ncells, 0);
       D.pp[c].assign(ncells, 0);
+      D.ep[c].assign(ncells, 0);
     }
     S->disp.push_back(D);
   });

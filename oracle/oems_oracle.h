@@ -176,8 +176,9 @@ int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, doubl
  *   kind 0 Drude  (:476-535)  j = a j + b e;  e = e - c j
  *   kind 1 Lorentz as the reference (:134-196) j = a j + c e; e = e - b j
  *   kind 2 Debye  (:570-630)  p' = a p + b e; e = e - c (p' - p) / dt
- *   kind 3 Lorentz, second order: p' = a p + b p_prev + c e;
- *          e = e - (p' - p) / (eps0 eps_inf)
+ *   kind 3 Lorentz, second order: p' = a p + b p_prev + c e_n;
+ *          e = e - (p' - p) / (eps0 eps_inf), e_n = E before the E update
+ *   kind 4 Drude as the same recursion with omega_0 = 0 (params omega_p, gamma)
  * params: Drude (omega_p, gamma) rad/s; Lorentz (omega_0, gamma, delta_eps);
  * Debye (tau, delta_eps).  eps_inf divides the E correction (1 = reference). */
 int32_t orc_add_dispersive(orc_sim* s, int32_t kind, const double* params, double eps_inf,

@@ -298,8 +298,10 @@ def dispersive_scenarios() -> List[Scenario]:
                  probes=[(2, (11, 5, 14)), (0, (4, 13, 10))]),
         Scenario("lorentz2_overlap", (14, 13, 22), 1e-3, excitations=[x], num_steps=200,
                  dispersive=[(lorentz2, _box_cells(3, 12, 2, 11, 12, 20)),
-                             (drude, _box_cells(6, 9, 5, 8, 14, 17))],
-                 probes=[(2, (7, 6, 15))]),
+                             (drude, _box_cells(6, 9, 5, 8, 14, 17)),
+                             (oe.DrudeMaterial(2 * np.pi * 30e9, 0.0, eps_inf=1.5, second_order=True),
+                              _box_cells(2, 5, 2, 5, 3, 9))],
+                 probes=[(2, (7, 6, 15)), (1, (3, 3, 5))]),
         Scenario("lorentz_reference_short", (10, 11, 12), 1e-3,
                  excitations=[E.gaussian_modulated(12e9, 0.5, 1, (5, 5, 6))], num_steps=30,
                  dispersive=[(lorentz, _box_cells(2, 8, 2, 9, 3, 10))]),

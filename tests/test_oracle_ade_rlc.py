@@ -53,6 +53,8 @@ CASES = [
     (2, (1e-11, 3.0), 2.0),
     (2, (4e-12, 10.0), 1.0),  # explicit update unstable here (b / eps0 > 2): diverges alike
     (3, (2 * np.pi * 15e9, 2e9, 2.0), 1.5),
+    (4, (2 * np.pi * 20e9, 1e10), 1.0),
+    (4, (2 * np.pi * 35e9, 0.0), 2.5),
 ]
 
 
@@ -83,6 +85,42 @@ def test_drude_plasma_oscillation_frequency():
     s.run_batch(4000)
     f = dominant_frequency(s.probe_traces()[:, 2], DT)
     assert f == pytest.approx(wp / np.sqrt(eps_inf) / (2 * np.pi), rel=0.01)
+
+
+def test_second_order_drude_plasma_frequency():
+    wp, eps_inf = 2 * np.pi * 25e9, 2.0
+    s = one_cell()
+    s.add_dispersive(4, (wp, 0.0), [(0, 0, 0)], eps_inf)
+    s.run_batch(4000)
+    f = dominant_frequency(s.probe_traces()[:, 2], DT)
+    assert f == pytest.approx(wp / np.sqrt(eps_inf) / (2 * np.pi), rel=0.01)
+
+
+@pytest.mark.parametrize("kind,params,eps_inf,bounded", [
+    (0, (2 * np.pi * 5e9, 0.0), 1.0, False),          # the reference's Drude grows
+    (4, (2 * np.pi * 5e9, 0.0), 1.0, True),
+    (3, (2 * np.pi * 4e9, 0.0, 3.0), 2.0, True),
+])
+def test_lossless_dispersive_block_in_a_closed_box(kind, params, eps_inf, bounded):
+    """16^3 block of a lossless dispersive medium in a 32^3 PEC box, driven
+    by a zero-mean pulse: the total E + H energy must not keep growing (it
+    fluctuates: the polarisation holds part of the energy).  The reference's
+    Drude update, whose current is driven by the field after the curl
+    update, grows without bound here."""
+    n = 32
+    lines = [oracle.uniform_lines(n, 1e-3) for _ in range(3)]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(n, n, n, dt, delta, threads=8)
+    if eps_inf != 1.0:
+        s.set_material(eps_inf, 1.0, 0.0, 0.0, (8, 24, 8, 24, 8, 24))
+    s.add_dispersive(kind, params, np.mgrid[8:24, 8:24, 8:24].reshape(3, -1).T.astype(np.int64), eps_inf)
+    tau = 4e-11
+    t = np.arange(4000) * dt - 5 * tau
+    s.add_excitation_sampled((4, 16, 16), 2, True,
+                             (-(t / tau) * np.exp(-(t / tau) ** 2)).astype(np.float32))
+    e = [x[3] for x in s.run_batch(4000, sample_interval=400)["energy_samples"]]
+    growth = max(e[-3:]) / max(e[1:4])
+    assert (growth < 3.0) == bounded, e
 
 
 def test_lorentz_second_order_longitudinal_frequency():
