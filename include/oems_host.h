@@ -219,6 +219,12 @@ OEMS_API oems_status oems_sweep_run(oems_sweep* sweep, uint64_t batch_steps);
 /* uf, if_ and s11: 2 x nfreq doubles (re, im) each; any may be NULL. */
 OEMS_API oems_status oems_sweep_get_result(const oems_sweep* sweep, int32_t instance_id, oems_sweep_result* info,
                                            double* uf, double* if_, double* s11);
+/* Keep the port voltage / current time traces (f64, u then i per step) of
+ * the first `steps` timesteps of every instance run afterwards; 0 = none. */
+OEMS_API oems_status oems_sweep_set_trace_steps(oems_sweep* sweep, uint64_t steps);
+/* out: cap_steps x 2 doubles; *nsteps receives the recorded step count. */
+OEMS_API oems_status oems_sweep_get_trace(const oems_sweep* sweep, int32_t instance_id, double* out,
+                                          uint64_t cap_steps, uint64_t* nsteps);
 /* Wall time of the last run and the cell x timestep count it executed. */
 OEMS_API oems_status oems_sweep_stats(const oems_sweep* sweep, double* wall_seconds, double* cell_steps);
 

@@ -250,6 +250,20 @@ SIGNATURES = {
     "oems_sweep_get_result": (c_i32, [P, c_i32, ctypes.POINTER(SweepResultC), ctypes.POINTER(c_f64),
                                       ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_sweep_stats": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
+    "oems_sweep_set_trace_steps": (c_i32, [P, c_u64]),
+    "oems_tc_gemm_bf16": (c_i32, [P, c_i32, P, c_i32, P, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, P, P]),
+    "oems_tc_check": (c_i32, [P]),
+    "oems_pk_f32_to_bf16": (c_i32, [P, P, c_i64, P]),
+    "oems_pk_transpose_bf16": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, P]),
+    "oems_pk_im2col": (c_i32, [P, P, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
+    "oems_pk_col2im": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
+    "oems_pk_relu": (c_i32, [P, P, c_i64, c_i32, c_i32, P]),
+    "oems_pk_relu_bwd": (c_i32, [P, P, c_i64, P]),
+    "oems_pk_colsum": (c_i32, [P, c_i64, c_i32, P, P]),
+    "oems_pk_mse": (c_i32, [P, P, P, P, c_i64, c_i32, P, c_i32, P]),
+    "oems_pk_adam": (c_i32, [P, P, P, P, P, c_i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_float, c_i32, P]),
+    "oems_sweep_get_trace": (c_i32, [P, c_i32, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_u64)]),
     "oems_operator_set_lumped": (c_i32, [P, c_u64 * 3, c_i32, c_f64, c_f64, c_f64, c_f64,
                                          ctypes.POINTER(c_f64)]),
     "oems_operator_engine_desc": (c_i32, [P, c_i32, c_u32, ctypes.POINTER(OperatorDesc)]),

@@ -14,9 +14,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "liboems_b200.so")
-SOURCES = ["csrc/engine.cu", "csrc/host.cpp", "csrc/noalloc.cu", "csrc/sweep.cpp"]
+SOURCES = ["csrc/engine.cu", "csrc/host.cpp", "csrc/noalloc.cu", "csrc/sweep.cpp", "csrc/predictor_kernels.cu"]
 HEADERS = ["csrc/yee_kernels.cuh", "csrc/yee_tma.cuh", "csrc/mur.cuh", "csrc/lumped_ade.cuh",
-           "csrc/fd_nf2ff.cuh", "../include/oems.h", "../include/oems_host.h"]
+           "csrc/fd_nf2ff.cuh", "csrc/upml.cuh", "csrc/gemm_tc.cuh", "../include/oems.h",
+           "../include/oems_host.h", "../include/oems_predictor.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -36,6 +36,7 @@ struct Instance {
   oems_sweep_result res{};
   std::string error;
   std::vector<double> uf, if_;
+  std::vector<double> trace;  // [step][2]: u, i (first trace_steps steps)
 };
 
 oems_status sfail(oems_status st, const char* msg) {
@@ -52,6 +53,7 @@ struct oems_sweep {
   std::vector<double> freqs;
   std::vector<std::unique_ptr<Instance>> inst;
   double wall = 0.0, cell_steps = 0.0;
+  uint64_t trace_steps = 0;
 };
 
 namespace {
@@ -132,6 +134,14 @@ oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch) {
     r.energy_samples = es.data();
     r.energy_capacity = es.size();
     if ((st = oems_engine_run_batch(en, &b, &r)) != OEMS_OK) return st;
+    if (sw->trace_steps > run) {
+      // port u / i of this batch, kept up to trace_steps
+      const uint64_t keep = std::min<uint64_t>(r.timesteps_executed, sw->trace_steps - run);
+      std::vector<double> tr(2 * std::max<uint64_t>(r.timesteps_executed, 1));
+      uint64_t got = 0;
+      if ((st = oems_engine_read_probe_traces(en, tr.data(), r.timesteps_executed, &got)) != OEMS_OK) return st;
+      I.trace.insert(I.trace.end(), tr.begin(), tr.begin() + 2 * std::min(keep, got));
+    }
     uint64_t launches = 0;
     double dev_s = 0.0;
     oems_engine_last_batch_stats(en, &launches, &dev_s);
@@ -252,6 +262,22 @@ oems_status oems_sweep_get_result(const oems_sweep* s, int32_t id, oems_sweep_re
       s11[2 * f + 1] = den > 0.0 ? (bi * ar - br * ai) / den : 0.0;
     }
   }
+  return OEMS_OK;
+}
+
+oems_status oems_sweep_set_trace_steps(oems_sweep* s, uint64_t steps) {
+  if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
+  s->trace_steps = steps;
+  return OEMS_OK;
+}
+
+oems_status oems_sweep_get_trace(const oems_sweep* s, int32_t id, double* out, uint64_t cap_steps, uint64_t* nsteps) {
+  if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
+  if (id < 0 || id >= (int32_t)s->inst.size()) return sfail(OEMS_ERR_CONFIG, "unknown sweep instance");
+  const Instance& I = *s->inst[id];
+  const uint64_t n = I.trace.size() / 2;
+  if (nsteps) *nsteps = n;
+  if (out) std::copy(I.trace.begin(), I.trace.begin() + 2 * std::min(n, cap_steps), out);
   return OEMS_OK;
 }
 

@@ -97,6 +97,20 @@ class Sweep:
                 "final_decay_db": float(info.final_decay_db), "device_seconds": float(info.device_seconds),
                 "cells": float(info.cells), "uf": uf, "if": if_, "s11": s11}
 
+    def set_trace_steps(self, steps: int):
+        """Record the port u / i traces of the first `steps` timesteps."""
+        N.check(N.lib().oems_sweep_set_trace_steps(self._h, int(steps)))
+
+    def trace(self, iid: int) -> np.ndarray:
+        """(steps, 2) float64: u, i per recorded timestep."""
+        n = N.c_u64()
+        N.check(N.lib().oems_sweep_get_trace(self._h, iid, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 2))
+        if n.value:
+            N.check(N.lib().oems_sweep_get_trace(self._h, iid, out.ctypes.data_as(ctypes.POINTER(N.c_f64)),
+                                                 n.value, ctypes.byref(n)))
+        return out
+
     def stats(self):
         wall, cs = N.c_f64(), N.c_f64()
         N.check(N.lib().oems_sweep_stats(self._h, ctypes.byref(wall), ctypes.byref(cs)))

@@ -22,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("include/oems.h", "include/oems_host.h"):
+    for h in ("include/oems.h", "include/oems_host.h", "include/oems_predictor.h"):
         src = open(os.path.join(ROOT, h)).read()
         names |= set(re.findall(r"OEMS_API\s+[\w\s\*]+?\b(oems_\w+)\s*\(", src))
     return names

@@ -1,0 +1,103 @@
+"""Host side of early termination (no GPU): the closed-form tail DFT, the
+pole-grid fit, the matrix-pencil continuation on known damped sinusoids,
+and the seeded patch family."""
+import numpy as np
+import pytest
+
+from openems_b200 import predictor as P
+
+DT = P.grid_dt()
+FREQS = P.FREQS[::4]
+
+
+def damped(n, modes, dt=DT, start=0):
+    """sum_m a_m exp(-alpha_m t) cos(omega_m t + phi_m) at t = (start + k) dt."""
+    t = (start + np.arange(n)) * dt
+    return sum(a * np.exp(-al * t) * np.cos(w * t + ph) for a, al, w, ph in modes)
+
+
+MODES = [(1.0, 2.0e8, 2 * np.pi * 3.1e9, 0.3), (0.4, 6.0e8, 2 * np.pi * 7.7e9, -1.1),
+         (0.15, 1.0e8, 2 * np.pi * 1.3e9, 2.0)]
+
+
+def test_tail_dft_closed_form_matches_direct_sum():
+    poles = P.PoleGrid(nf=6, qs=(10.0,)).poles()
+    c = np.random.default_rng(0).normal(size=6) + 1j * np.random.default_rng(1).normal(size=6)
+    n, t0 = 3000, 123.5 * DT
+    x = (np.exp(np.outer(np.arange(n) * DT, poles)) @ c).real
+    want = 2 * DT * (np.exp(-2j * np.pi * np.outer(FREQS, t0 + np.arange(n) * DT)) @ x)
+    got = P.tail_dft(c, poles, t0, DT, FREQS, n)
+    assert np.abs(got - want).max() < 1e-10 * np.abs(want).max()
+
+
+def test_head_dft_is_the_engine_probe_dft():
+    x = np.random.default_rng(2).normal(size=50)
+    got = P.head_dft(x, 1, DT, FREQS, half=0.5)
+    want = [2 * DT * sum(x[k] * np.exp(-2j * np.pi * f * (k + 1 - 0.5) * DT) for k in range(50)) for f in FREQS]
+    assert np.allclose(got, want, rtol=1e-12, atol=0)
+
+
+def test_tail_matrix_matches_tail_dft():
+    poles = P.PoleGrid().poles()
+    T = P.tail_matrix(poles, 2048, DT, FREQS, 0.5, 6000)
+    c = np.random.default_rng(0).normal(size=64) + 1j * np.random.default_rng(1).normal(size=64)
+    x = P.tail_dft(c, poles, (2048 + 1 - 0.5) * DT, DT, FREQS, 6000 - 2048)
+    y = T @ np.concatenate([c.real, c.imag])
+    F = len(FREQS)
+    assert np.abs(y[:F] - x.real).max() < 1e-12 * np.abs(x).max()
+    assert np.abs(y[F:] - x.imag).max() < 1e-12 * np.abs(x).max()
+
+
+def test_fit_tail_recovers_grid_coefficients():
+    poles = P.PoleGrid(nf=8, qs=(8.0,)).poles()
+    c = np.random.default_rng(3).normal(size=8) + 1j * np.random.default_rng(4).normal(size=8)
+    tail = (np.exp(np.outer(np.arange(4000) * DT, poles)) @ c).real
+    got = P.fit_tail(tail, poles, DT, ridge=0.0)
+    assert np.abs(got - c).max() < 1e-6 * np.abs(c).max()
+    assert np.all(P.fit_tail(np.zeros(0), poles, DT) == 0)
+
+
+def test_matrix_pencil_finds_damped_modes():
+    y = damped(400, MODES)
+    z, r = P.matrix_pencil(y, 20)
+    assert len(z) == 6
+    k = np.arange(400)
+    assert np.abs((np.power.outer(z, k).T @ r).real - y).max() < 1e-9
+    got = np.sort(np.abs(np.angle(z)) / DT / (2 * np.pi))
+    want = np.sort(np.repeat([m[2] / (2 * np.pi) for m in MODES], 2))
+    assert np.allclose(got, want, rtol=1e-8)
+    # growing or silent input: nothing to continue
+    assert len(P.matrix_pencil(np.zeros(64), 8)[0]) == 0
+    assert len(P.matrix_pencil(1.01 ** np.arange(64), 8)[0]) == 0
+
+
+@pytest.mark.parametrize("half", [0.0, 0.5])
+def test_pencil_continuation_of_known_signal(half):
+    """The continuation of a sum of damped sinusoids from a 1536-sample
+    window is the exact DFT of its remaining samples."""
+    K, horizon = 2048, 12000
+    x = damped(horizon, MODES)
+    got = P.pencil_tail_dft(x[:K], K, DT, FREQS, half, horizon)
+    want = P.head_dft(x[K:], K + 1, DT, FREQS, half)
+    assert np.abs(got - want).max() < 1e-6 * np.abs(want).max()
+    # a signal that has already died away continues as nothing
+    assert np.all(P.pencil_tail_dft(np.zeros(K), K, DT, FREQS, half, horizon) == 0)
+
+
+def test_s11_of_matched_and_open_port():
+    uf = np.array([50.0 + 0j, 1.0 + 0j])
+    if_ = np.array([1.0 + 0j, 0.0 + 0j])
+    assert np.allclose(P.s11(uf, if_), [0.0, 1.0])
+
+
+def test_family_specs_seeded_and_in_range():
+    a, b = P.family_specs(32, seed=5), P.family_specs(32, seed=5)
+    assert a == b and a != P.family_specs(32, seed=50)
+    for s in a:
+        assert all(40 <= n <= 80 for n in s.dims)
+        assert 2.2 <= s.eps_r <= 10.2 and 2 <= s.h_cells <= 6
+        margin = s.layers + 4
+        assert s.x0 >= margin - 1 and s.x0 + s.W <= s.dims[0] - margin + 1
+        assert s.y0 >= margin - 1 and s.y0 + s.L <= s.dims[1] - margin + 1
+        assert s.x0 <= s.fx < s.x0 + s.W and s.y0 <= s.fy < s.y0 + s.L
+        assert s.k_patch + 1 < s.dims[2] - s.layers
