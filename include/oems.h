@@ -280,6 +280,12 @@ typedef struct oems_nf2ff_result {
 
 OEMS_API oems_status oems_engine_create(const oems_operator_desc* desc, oems_engine** out);
 OEMS_API void oems_engine_destroy(oems_engine* engine);
+/* Engine device memory comes from a stream-ordered pool per device that keeps
+ * freed blocks for the next engine (no device-wide synchronisation when an
+ * engine is destroyed); this returns the device's unused pooled memory and
+ * the cached pinned host buffers to the driver.  device < 0: the current
+ * device. */
+OEMS_API oems_status oems_release_cached_memory(int32_t device);
 
 /* ---- EngineImpl --------------------------------------------------------- */
 

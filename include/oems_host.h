@@ -205,6 +205,8 @@ typedef struct oems_sweep_result {
   double final_decay_db;
   double device_seconds;      /* sum over the instance's batches */
   double cells;
+  double setup_seconds;       /* host time from the start of the instance to its first batch */
+  double host_seconds;        /* host time of the whole instance, engine teardown included */
 } oems_sweep_result;
 
 /* freqs: the DFT frequencies of every instance (Hz).  engine_flags as for

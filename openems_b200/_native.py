@@ -189,7 +189,8 @@ class SweepInstanceC(ctypes.Structure):
 
 class SweepResultC(ctypes.Structure):
     _fields_ = [("timesteps", c_u64), ("termination_reason", c_i32), ("status", c_i32),
-                ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64)]
+                ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64),
+                ("setup_seconds", c_f64), ("host_seconds", c_f64)]
 
 
 # name -> (restype, argtypes); every symbol the headers declare
@@ -197,6 +198,7 @@ SIGNATURES = {
     # include/oems.h
     "oems_engine_create": (c_i32, [ctypes.POINTER(OperatorDesc), ctypes.POINTER(P)]),
     "oems_engine_destroy": (None, [P]),
+    "oems_release_cached_memory": (c_i32, [c_i32]),
     "oems_engine_run_batch": (c_i32, [P, ctypes.POINTER(BatchC), ctypes.POINTER(BatchResultC)]),
     "oems_engine_current_timestep": (c_i32, [P, ctypes.POINTER(c_u64)]),
     "oems_engine_read_fields": (c_i32, [P, PF * 3, PF * 3]),

@@ -235,21 +235,145 @@ struct LaunchShape {
   size_t smem = 0;
 };
 
+// ---------------------------------------------------------------------------
+// device and pinned host memory
+// ---------------------------------------------------------------------------
+// An engine's device buffers come from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the engine's stream).  cudaFree
+// waits for every stream of the device, so with several engines in flight
+// (a sweep) each engine teardown would stall all the others; a stream-ordered
+// free does not, and the freed blocks stay in the pool for the next engine
+// (oems_release_cached_memory hands them back to the driver).  A buffer is
+// allocated on the stream of the engine whose entry point is running
+// (EngineScope); outside an engine it falls back to cudaMalloc / cudaFree.
+
+thread_local cudaStream_t t_alloc_stream = nullptr;
+
+constexpr int kMaxDevices = 64;
+struct PoolTable {
+  std::mutex mu;
+  cudaMemPool_t pool[kMaxDevices] = {};
+};
+static PoolTable& pool_table() {
+  static PoolTable t;
+  return t;
+}
+
+static cudaError_t device_pool(int dev, bool create, cudaMemPool_t* out) {
+  *out = nullptr;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  PoolTable& t = pool_table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  if (!t.pool[dev] && create) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;  // freed blocks stay for reuse until trimmed
+    if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+      cudaMemPoolDestroy(p);
+      return e;
+    }
+    t.pool[dev] = p;
+  }
+  *out = t.pool[dev];
+  return cudaSuccess;
+}
+
+// `bytes` of device memory ordered on stream s (the current device's pool).
+static cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = nullptr;
+  if ((e = device_pool(dev, true, &pool)) != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), pool, s);
+}
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
+  cudaStream_t s = nullptr;  // stream of a pooled allocation (null: cudaMalloc)
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) {
+      if (s)
+        cudaFreeAsync(p, s);
+      else
+        cudaFree(p);
+    }
+    p = nullptr;
+    n = 0;
+    s = nullptr;
   }
   cudaError_t ensure(size_t count) {
     if (count <= n && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
-    if (e == cudaSuccess) n = std::max<size_t>(count, 1);
-    return e;
+    release();
+    const size_t c = std::max<size_t>(count, 1);
+    void* q = nullptr;
+    cudaError_t e = t_alloc_stream ? pool_alloc(&q, c * sizeof(T), t_alloc_stream) : cudaMalloc(&q, c * sizeof(T));
+    if (e != cudaSuccess) return e;
+    p = static_cast<T*>(q);
+    n = c;
+    s = t_alloc_stream;
+    return cudaSuccess;
+  }
+};
+
+// Pinned host buffers are cached by power-of-two size class: cudaFreeHost
+// synchronises the device like cudaFree.
+struct PinnedCache {
+  std::mutex mu;
+  std::multimap<size_t, void*> free;
+};
+static PinnedCache& pinned_cache() {
+  static PinnedCache c;
+  return c;
+}
+static size_t pinned_class(size_t bytes) {
+  size_t c = 4096;
+  while (c < bytes) c <<= 1;
+  return c;
+}
+static cudaError_t pinned_get(void** p, size_t bytes) {
+  const size_t c = pinned_class(bytes);
+  PinnedCache& pc = pinned_cache();
+  {
+    std::lock_guard<std::mutex> lk(pc.mu);
+    auto it = pc.free.find(c);
+    if (it != pc.free.end()) {
+      *p = it->second;
+      pc.free.erase(it);
+      return cudaSuccess;
+    }
+  }
+  return cudaMallocHost(p, c);
+}
+static void pinned_put(void* p, size_t bytes) {
+  if (!p) return;
+  PinnedCache& pc = pinned_cache();
+  std::lock_guard<std::mutex> lk(pc.mu);
+  pc.free.emplace(pinned_class(bytes), p);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
   }
 };
 
@@ -372,8 +496,8 @@ struct oems_engine {
   // energy
   oems::DevBuf<double> d_partials;
   oems::DevBuf<double> d_energy;  // [sample][2]
-  double* h_energy = nullptr;     // pinned mirror
-  size_t h_energy_cap = 0;
+  double* h_energy = nullptr;     // pinned mirror (cached pinned buffer)
+  size_t h_energy_cap = 0;        // samples
 
   oems::DevBuf<long long> d_base;
   oems::DevBuf<int> d_err;  // device error word (bounded waits that gave up)
@@ -402,6 +526,17 @@ struct oems_engine {
 };
 
 namespace oems {
+
+// Runs an entry point of an engine: its device is current and new buffers
+// are allocated on its stream.
+struct EngineScope {
+  DeviceGuard dev;
+  cudaStream_t prev;
+  explicit EngineScope(const oems_engine* en) : dev(en->device), prev(t_alloc_stream) {
+    t_alloc_stream = en->stream;
+  }
+  ~EngineScope() { t_alloc_stream = prev; }
+};
 
 static void drop_graphs(oems_engine* en) {
   for (auto& kv : en->graphs) cudaGraphExecDestroy(kv.second);
@@ -932,12 +1067,15 @@ static oems_status launch_energy(oems_engine* en, double* out2) {
 
 static oems_status ensure_host_energy(oems_engine* en, size_t samples) {
   if (samples <= en->h_energy_cap) return OEMS_OK;
-  if (en->h_energy) cudaFreeHost(en->h_energy);
-  for (cudaEvent_t e : en->prof_ev) cudaEventDestroy(e);
+  // the mirror is only read after a stream synchronisation: nothing in flight uses it
+  pinned_put(en->h_energy, en->h_energy_cap * 2 * sizeof(double));
   en->h_energy = nullptr;
   en->h_energy_cap = 0;
-  OEMS_CUDA(cudaMallocHost(&en->h_energy, std::max<size_t>(samples, 16) * 2 * sizeof(double)));
-  en->h_energy_cap = std::max<size_t>(samples, 16);
+  const size_t cap = std::max<size_t>(samples, 16);
+  void* p = nullptr;
+  OEMS_CUDA(pinned_get(&p, cap * 2 * sizeof(double)));
+  en->h_energy = static_cast<double*>(p);
+  en->h_energy_cap = cap;
   return OEMS_OK;
 }
 
@@ -1008,6 +1146,20 @@ static oems_status autotune(oems_engine* en) {
       s.smem = make_tma_geom(en, std::max(1, std::min(en->ny, 256 / en->g.nzq)), 16, 256, limit, 4, s.tg);
       if (s.smem == 0) s = LaunchShape{};
     }
+    if (!s.tma) {
+      // small grids: shorter x-runs, then narrower CTAs, until every SM has
+      // a work item (a 70^3 grid has 45 items at 256 x 8: most SMs would idle)
+      int sms = 0;
+      OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, en->device));
+      while (make_geom(en, s.block, s.ichunk).work < sms) {
+        if (s.ichunk > 1)
+          s.ichunk /= 2;
+        else if (s.block > 128)
+          s.block /= 2;
+        else
+          break;
+      }
+    }
     OEMS_TRY(size_grid(en, s));
     apply_shape(en, s);
     return OEMS_OK;
@@ -1024,8 +1176,8 @@ static oems_status autotune(oems_engine* en) {
   }
   const size_t fbytes = (size_t)6 * en->ncells_padded * sizeof(float);
   const size_t pbytes = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
-  float* save = nullptr;
-  OEMS_CUDA(cudaMalloc(&save, fbytes + pbytes));
+  void* save = nullptr;
+  OEMS_CUDA(pool_alloc(&save, fbytes + pbytes, en->stream));
   OEMS_CUDA(cudaMemcpyAsync(save, en->fields, fbytes, cudaMemcpyDeviceToDevice, en->stream));
   if (pbytes)
     OEMS_CUDA(cudaMemcpyAsync((char*)save + fbytes, en->cpml.psi.p, pbytes, cudaMemcpyDeviceToDevice,
@@ -1107,7 +1259,8 @@ static oems_status autotune(oems_engine* en) {
   }
   if (st == OEMS_OK) {
     int err = 0;
-    cudaMemcpy(&err, en->d_err.p, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpyAsync(&err, en->d_err.p, sizeof(int), cudaMemcpyDeviceToHost, en->stream);
+    cudaStreamSynchronize(en->stream);
     if (err) st = fail(OEMS_ERR_TIMEOUT, "a bounded device wait gave up while tuning");
   }
   apply_shape(en, best);
@@ -1117,8 +1270,8 @@ static oems_status autotune(oems_engine* en) {
   }
   cudaMemcpyAsync(en->fields, save, fbytes, cudaMemcpyDeviceToDevice, en->stream);
   if (pbytes) cudaMemcpyAsync(en->cpml.psi.p, (char*)save + fbytes, pbytes, cudaMemcpyDeviceToDevice, en->stream);
+  cudaFreeAsync(save, en->stream);
   cudaStreamSynchronize(en->stream);
-  cudaFree(save);
   return st;
 }
 
@@ -1143,7 +1296,8 @@ static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc
   for (int a = 0; a < 12; ++a)
     if (!src[a]) return fail(OEMS_ERR_INVALID_ARGUMENT, "coefficient array pointer is NULL");
   if (!(en->flags & OEMS_ENGINE_COMPRESSED)) {
-    OEMS_CUDA(cudaMalloc(&en->coeffs, (size_t)12 * en->ncells_padded * sizeof(float)));
+    OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->coeffs), (size_t)12 * en->ncells_padded * sizeof(float),
+                         en->stream));
     OEMS_CUDA(cudaMemsetAsync(en->coeffs, 0, (size_t)12 * en->ncells_padded * sizeof(float), en->stream));
     for (int a = 0; a < 12; ++a)
       OEMS_CUDA(cudaMemcpy2DAsync(en->C(a), nzp * sizeof(float), src[a], en->nz * sizeof(float),
@@ -1179,49 +1333,43 @@ static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc
   }
   (void)n;
   en->ntable = (int)map.size();
-  OEMS_CUDA(cudaMalloc(&en->table, table.size() * sizeof(float)));
-  OEMS_CUDA(cudaMemcpy(en->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->table), table.size() * sizeof(float), en->stream));
+  OEMS_CUDA(cudaMemcpyAsync(en->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            en->stream));
   if (en->ntable <= 256) {
     en->id_bytes = 1;
     std::vector<uint8_t> ids8(ids16.size());
     for (size_t q = 0; q < ids16.size(); ++q) ids8[q] = (uint8_t)ids16[q];
-    OEMS_CUDA(cudaMalloc(&en->ids, ids8.size()));
-    OEMS_CUDA(cudaMemcpy(en->ids, ids8.data(), ids8.size(), cudaMemcpyHostToDevice));
+    OEMS_CUDA(pool_alloc(&en->ids, ids8.size(), en->stream));
+    OEMS_CUDA(cudaMemcpyAsync(en->ids, ids8.data(), ids8.size(), cudaMemcpyHostToDevice, en->stream));
+    OEMS_CUDA(cudaStreamSynchronize(en->stream));
   } else {
     en->id_bytes = 2;
-    OEMS_CUDA(cudaMalloc(&en->ids, ids16.size() * sizeof(uint16_t)));
-    OEMS_CUDA(cudaMemcpy(en->ids, ids16.data(), ids16.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    OEMS_CUDA(pool_alloc(&en->ids, ids16.size() * sizeof(uint16_t), en->stream));
+    OEMS_CUDA(cudaMemcpyAsync(en->ids, ids16.data(), ids16.size() * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                              en->stream));
+    OEMS_CUDA(cudaStreamSynchronize(en->stream));
   }
   return OEMS_OK;
 }
 
+// Every buffer goes back to the pool on the engine's stream (the stream is
+// idle by then); the stream itself is destroyed last.
 static void destroy(oems_engine* en) {
   if (!en) return;
-  if (en->stream) cudaStreamSynchronize(en->stream);
+  cudaStream_t s = en->stream;
+  if (s) cudaStreamSynchronize(s);
   drop_graphs(en);
-  if (en->fields) cudaFree(en->fields);
-  if (en->coeffs) cudaFree(en->coeffs);
-  if (en->ids) cudaFree(en->ids);
-  if (en->table) cudaFree(en->table);
-  if (en->h_energy) cudaFreeHost(en->h_energy);
+  for (void* p : {(void*)en->fields, (void*)en->coeffs, en->ids, (void*)en->table})
+    if (p) cudaFreeAsync(p, s);
+  pinned_put(en->h_energy, en->h_energy_cap * 2 * sizeof(double));
   if (en->ev0) cudaEventDestroy(en->ev0);
   if (en->ev1) cudaEventDestroy(en->ev1);
-  if (en->stream) cudaStreamDestroy(en->stream);
-  delete en;
+  for (cudaEvent_t e : en->prof_ev)
+    if (e) cudaEventDestroy(e);
+  delete en;  // DevBuf members free on their stream
+  if (s) cudaStreamDestroy(s);
 }
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 static oems_status create(const oems_operator_desc* d, oems_engine** out) {
   if (!d || !out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL descriptor or output pointer");
@@ -1251,15 +1399,16 @@ static oems_status create(const oems_operator_desc* d, oems_engine** out) {
   en->dt = d->dt;
   for (int a = 0; a < 3; ++a) en->delta[a] = d->delta[a];
   OEMS_CUDA(cudaStreamCreateWithFlags(&en->stream, cudaStreamNonBlocking));
+  EngineScope scope(en.get());
   OEMS_CUDA(cudaEventCreate(&en->ev0));
   OEMS_CUDA(cudaEventCreate(&en->ev1));
   en->g = make_geom(en.get(), 256, 8);
   en->ncells_padded = (long long)en->nx * en->ny * en->g.nzp;
-  OEMS_CUDA(cudaMalloc(&en->fields, (size_t)6 * en->ncells_padded * sizeof(float)));
+  OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->fields), (size_t)6 * en->ncells_padded * sizeof(float),
+                       en->stream));
   OEMS_CUDA(cudaMemsetAsync(en->fields, 0, (size_t)6 * en->ncells_padded * sizeof(float), en->stream));
   OEMS_TRY(upload_coefficients(en.get(), d));
-  OEMS_CUDA(cudaMalloc(&en->d_partials.p, 6 * kEnergyBlocks * sizeof(double)));
-  en->d_partials.n = 6 * kEnergyBlocks;
+  OEMS_CUDA(en->d_partials.ensure(6 * kEnergyBlocks));
   OEMS_CUDA(en->d_base.ensure(1));
   OEMS_CUDA(en->d_err.ensure(1));
   OEMS_CUDA(cudaMemsetAsync(en->d_err.p, 0, sizeof(int), en->stream));
@@ -1353,7 +1502,7 @@ static oems_status fill_twiddles(oems_engine* en, FdTable* T, const std::vector<
 
 static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_result* r) {
   if (!b || !r) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL batch or result");
-  DeviceGuard guard(en->device);
+  EngineScope guard(en);
   const auto t_start = std::chrono::steady_clock::now();
   en->last_launches = 0;
   if (!en->tuned) OEMS_TRY(autotune(en));
@@ -1506,7 +1655,7 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
 }
 
 static oems_status copy_fields(oems_engine* en, float* const* host6, bool to_host) {
-  DeviceGuard guard(en->device);
+  EngineScope guard(en);
   const size_t rows = (size_t)en->nx * en->ny;
   for (int c = 0; c < 6; ++c) {
     if (!host6[c]) return fail(OEMS_ERR_INVALID_ARGUMENT, "field pointer is NULL");
@@ -1528,7 +1677,7 @@ static oems_status add_mur(oems_engine* en, const oems_mur_desc* d) {
   if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL Mur descriptor");
   if (en->mur.on) return fail(OEMS_ERR_CONFIG, "Mur boundary already attached");
   if (d->order != 1 && d->order != 2) return fail(OEMS_ERR_CONFIG, "Mur order must be 1 or 2");
-  DeviceGuard guard(en->device);
+  EngineScope guard(en);
   const int ext[3] = {en->nx, en->ny, en->nz};
   const double kC0 = 299792458.0;
   const double c = d->phase_velocity > 0.0 ? d->phase_velocity : kC0;
@@ -1580,7 +1729,7 @@ static oems_status add_mur(oems_engine* en, const oems_mur_desc* d) {
 static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
   if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL CPML descriptor");
   if (en->cpml.on) return fail(OEMS_ERR_CONFIG, "CPML already attached");
-  DeviceGuard guard(en->device);
+  EngineScope guard(en);
   const int ext[3] = {en->nx, en->ny, en->nz};
   int L[6];
   int lmax = 0;
@@ -1635,7 +1784,8 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
     prof.insert(prof.end(), rows.begin(), rows.end());
   }
   OEMS_CUDA(en->cpml.prof.ensure(prof.size()));
-  OEMS_CUDA(cudaMemcpy(en->cpml.prof.p, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpyAsync(en->cpml.prof.p, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            en->stream));
   A.prof = en->cpml.prof.p;
   // z faces: psi rows start at a multiple of 4 in k so chunks map to aligned float4s
   A.zbase[0] = 0;
@@ -1696,7 +1846,7 @@ oems_status oems_engine_create(const oems_operator_desc* desc, oems_engine** out
 
 void oems_engine_destroy(oems_engine* engine) {
   if (!engine) return;
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   destroy(engine);
 }
 
@@ -1727,7 +1877,7 @@ oems_status oems_engine_write_fields(oems_engine* engine, const float* const e[3
 
 oems_status oems_engine_reset(oems_engine* engine) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   OEMS_CUDA(cudaMemsetAsync(engine->fields, 0, (size_t)6 * engine->ncells_padded * sizeof(float), engine->stream));
   if (engine->cpml.on)
     OEMS_CUDA(cudaMemsetAsync(engine->cpml.psi.p, 0, engine->cpml.psi.n * sizeof(float), engine->stream));
@@ -1763,7 +1913,7 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
   if (d->kind < 0 || d->kind > 4) return fail(OEMS_ERR_MATERIAL, "unknown dispersive material kind");
   if (!(d->eps_inf > 0.0)) return fail(OEMS_ERR_MATERIAL, "eps_inf must be positive");
   if (ncells == 0) return fail(OEMS_ERR_MATERIAL, "a dispersive material needs at least one cell");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   DispHost h;
   DispArgs& A = h.args;
   A.kind = d->kind;
@@ -1802,8 +1952,8 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
   }
   OEMS_CUDA(h.q->ensure(ncells));
   OEMS_CUDA(h.state->ensure(9 * ncells));
-  OEMS_CUDA(cudaMemcpy(h.q->p, q.data(), ncells * sizeof(long long), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemset(h.state->p, 0, 9 * ncells * sizeof(float)));
+  OEMS_CUDA(cudaMemcpyAsync(h.q->p, q.data(), ncells * sizeof(long long), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemsetAsync(h.state->p, 0, 9 * ncells * sizeof(float), engine->stream));
   A.n = (long long)ncells;
   A.q = h.q->p;
   A.st = h.state->p;
@@ -1817,7 +1967,7 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
 
 oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rlc_desc* elems, uint64_t n) {
   if (!engine || (!elems && n)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   RlcHost& R = engine->rlc;
   const double dt = engine->dt, kEps0 = 8.854187817e-12;
   for (uint64_t m = 0; m < n; ++m) {  // validate the whole list before taking any of it
@@ -1859,11 +2009,11 @@ oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rl
   OEMS_CUDA(R.d_vv.ensure(k));
   OEMS_CUDA(R.d_vil.ensure(k));
   OEMS_CUDA(R.d_int.ensure(k));
-  OEMS_CUDA(cudaMemcpy(R.d_q.p, R.q.data(), k * sizeof(long long), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(R.d_dir.p, R.dir.data(), k * sizeof(int), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(R.d_vv.p, R.v_vv.data(), k * sizeof(float), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(R.d_vil.p, R.v_il.data(), k * sizeof(float), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemset(R.d_int.p, 0, k * sizeof(float)));
+  OEMS_CUDA(cudaMemcpyAsync(R.d_q.p, R.q.data(), k * sizeof(long long), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(R.d_dir.p, R.dir.data(), k * sizeof(int), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(R.d_vv.p, R.v_vv.data(), k * sizeof(float), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(R.d_vil.p, R.v_il.data(), k * sizeof(float), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemsetAsync(R.d_int.p, 0, k * sizeof(float), engine->stream));
   engine->graph_epoch++;
   return OEMS_OK;
 }
@@ -1874,7 +2024,7 @@ oems_status oems_engine_add_field_dft(oems_engine* engine, const oems_field_dft_
   if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "a field DFT needs at least one frequency");
   if ((d->components & 0x3Fu) == 0 || (d->components & ~0x3Fu))
     return fail(OEMS_ERR_CONFIG, "field DFT components must be a non-empty mask of bits 0..5");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   FieldDftHost h;
   FieldDftArgs& A = h.args;
   const long long ext[3] = {engine->nx, engine->ny, engine->nz};
@@ -1911,7 +2061,7 @@ oems_status oems_engine_add_field_dft(oems_engine* engine, const oems_field_dft_
   h.interval = std::max<uint32_t>(d->interval, 1u);
   const size_t nacc = 2 * (size_t)nfreq * A.ncomp * (size_t)A.npts;
   OEMS_CUDA(h.acc->ensure(nacc));
-  OEMS_CUDA(cudaMemset(h.acc->p, 0, nacc * sizeof(double)));
+  OEMS_CUDA(cudaMemsetAsync(h.acc->p, 0, nacc * sizeof(double), engine->stream));
   A.acc = reinterpret_cast<double2*>(h.acc->p);
   if (!engine->d_base.p) OEMS_CUDA(engine->d_base.ensure(1));
   engine->fdumps.push_back(std::move(h));
@@ -1929,11 +2079,13 @@ oems_status oems_engine_read_field_dft(oems_engine* engine, int32_t id, uint32_t
   const auto it = std::find(h.comps.begin(), h.comps.end(), (int)component);
   if (it == h.comps.end()) return fail(OEMS_ERR_CONFIG, "component not recorded by this field DFT");
   if (npoints < (uint64_t)h.args.npts) return fail(OEMS_ERR_INVALID_ARGUMENT, "output buffer too small");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   const size_t slot = it - h.comps.begin();
   const size_t off = 2 * ((size_t)f * h.comps.size() + slot) * (size_t)h.args.npts;
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
-  OEMS_CUDA(cudaMemcpy(out, h.acc->p + off, 2 * (size_t)h.args.npts * sizeof(double), cudaMemcpyDeviceToHost));
+  OEMS_CUDA(cudaMemcpyAsync(out, h.acc->p + off, 2 * (size_t)h.args.npts * sizeof(double), cudaMemcpyDeviceToHost,
+                            engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   return OEMS_OK;
 }
 
@@ -1945,7 +2097,7 @@ oems_status oems_engine_add_nf2ff_box(oems_engine* engine, const oems_nf2ff_box_
   for (int a = 0; a < 3; ++a)
     if (d->start[a] < 1 || d->stop[a] <= d->start[a] || d->stop[a] > (uint64_t)ext[a] - 1)
       return fail(OEMS_ERR_CONFIG, "NF2FF box must satisfy 1 <= start < stop <= n - 1 on every axis");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   Nf2ffHost h;
   Nf2ffAccArgs& A = h.args;
   for (int a = 0; a < 3; ++a) {
@@ -1974,7 +2126,7 @@ oems_status oems_engine_add_nf2ff_box(oems_engine* engine, const oems_nf2ff_box_
   if (A.nfaces == 0) return fail(OEMS_ERR_CONFIG, "NF2FF box has no face enabled");
   const size_t nacc = 8 * (size_t)nfreq * total;  // 4 complex values per point and frequency
   OEMS_CUDA(h.acc->ensure(nacc));
-  OEMS_CUDA(cudaMemset(h.acc->p, 0, nacc * sizeof(double)));
+  OEMS_CUDA(cudaMemsetAsync(h.acc->p, 0, nacc * sizeof(double), engine->stream));
   size_t off = 0;
   for (int i = 0; i < A.nfaces; ++i) {
     A.face[i].acc = reinterpret_cast<double2*>(h.acc->p + off);
@@ -2008,10 +2160,11 @@ oems_status oems_engine_read_nf2ff_face(oems_engine* engine, int32_t id, uint32_
     if (npoints) *npoints = (uint64_t)F.np;
     if (!out) return OEMS_OK;
     if (cap_doubles < 8 * (uint64_t)F.np) return fail(OEMS_ERR_INVALID_ARGUMENT, "output buffer too small");
-    DeviceGuard guard(engine->device);
+    EngineScope guard(engine);
     OEMS_CUDA(cudaStreamSynchronize(engine->stream));
-    OEMS_CUDA(cudaMemcpy(out, F.acc + (size_t)f * 4 * F.np, 8 * (size_t)F.np * sizeof(double),
-                         cudaMemcpyDeviceToHost));
+    OEMS_CUDA(cudaMemcpyAsync(out, F.acc + (size_t)f * 4 * F.np, 8 * (size_t)F.np * sizeof(double),
+                              cudaMemcpyDeviceToHost, engine->stream));
+    OEMS_CUDA(cudaStreamSynchronize(engine->stream));
     return OEMS_OK;
   }
   return fail(OEMS_ERR_CONFIG, "face not recorded by this NF2FF box");
@@ -2131,7 +2284,7 @@ oems_status oems_engine_nf2ff(oems_engine* engine, int32_t id, uint32_t f, const
   const Nf2ffHost& h = engine->boxes[id];
   if (f >= h.freqs.size()) return fail(OEMS_ERR_CONFIG, "frequency index out of range");
   OEMS_TRY(check_request(q, h.freqs[f]));
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   const long long ext[3] = {engine->nx, engine->ny, engine->nz};
   DevBuf<double> d_lines[3];
   Nf2ffPointsArgs P{};
@@ -2139,7 +2292,8 @@ oems_status oems_engine_nf2ff(oems_engine* engine, int32_t id, uint32_t f, const
     std::vector<double> l(ext[a] + 1);
     for (long long i = 0; i <= ext[a]; ++i) l[i] = q->lines[a] ? q->lines[a][i] : (double)i * engine->delta[a];
     OEMS_CUDA(d_lines[a].ensure(l.size()));
-    OEMS_CUDA(cudaMemcpy(d_lines[a].p, l.data(), l.size() * sizeof(double), cudaMemcpyHostToDevice));
+    OEMS_CUDA(cudaMemcpyAsync(d_lines[a].p, l.data(), l.size() * sizeof(double), cudaMemcpyHostToDevice,
+                              engine->stream));
     P.lines[a] = d_lines[a].p;
   }
   P.nfaces = h.args.nfaces;
@@ -2213,7 +2367,7 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
   if (engine->upml.on) return fail(OEMS_ERR_CONFIG, "UPML already attached");
   if (!(desc->reflection_coeff > 0.0 && desc->reflection_coeff < 1.0))
     return fail(OEMS_ERR_CONFIG, "UPML reflection coefficient must be in (0, 1)");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   const long long n[3] = {engine->nx, engine->ny, engine->nz};
   const long long* L = nullptr;
   long long lay[6];
@@ -2289,9 +2443,10 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
   UpmlHost& U = engine->upml;
   OEMS_CUDA(U.coef.ensure(18 * (size_t)total));
   OEMS_CUDA(U.flux.ensure(6 * (size_t)total));
-  OEMS_CUDA(cudaMemcpy(U.coef.p, ce.data(), ce.size() * sizeof(float), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(U.coef.p + 9 * total, ch.data(), ch.size() * sizeof(float), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemset(U.flux.p, 0, 6 * (size_t)total * sizeof(float)));
+  OEMS_CUDA(cudaMemcpyAsync(U.coef.p, ce.data(), ce.size() * sizeof(float), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(U.coef.p + 9 * total, ch.data(), ch.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            engine->stream));
+  OEMS_CUDA(cudaMemsetAsync(U.flux.p, 0, 6 * (size_t)total * sizeof(float), engine->stream));
   for (UpmlArgs* a : {&U.e, &U.h}) {
     *a = UpmlArgs{};
     a->nreg = (int)regs.size();
@@ -2343,7 +2498,7 @@ oems_status oems_engine_add_probe(oems_engine* engine, const oems_probe_term* te
     if (!std::isfinite(q.weight)) return fail(OEMS_ERR_CONFIG, "probe weight must be finite");
     all_h = all_h && q.component >= 3;
   }
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   for (uint64_t t = 0; t < nterms; ++t) {
     const oems_probe_term& q = terms[t];
     engine->term_idx.push_back(((long long)q.position[0] * engine->ny + (long long)q.position[1]) * engine->g.nzp +
@@ -2360,11 +2515,11 @@ oems_status oems_engine_add_probe(oems_engine* engine, const oems_probe_term* te
   OEMS_CUDA(engine->d_term_idx.ensure(nt));
   OEMS_CUDA(engine->d_term_comp.ensure(nt));
   OEMS_CUDA(engine->d_term_w.ensure(nt));
-  OEMS_CUDA(cudaMemcpy(engine->d_probe_off.p, engine->probe_off.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_probe_mode.p, engine->probe_mode.data(), np * sizeof(int), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_term_idx.p, engine->term_idx.data(), nt * sizeof(long long), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_term_comp.p, engine->term_comp.data(), nt * sizeof(int), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_term_w.p, engine->term_w.data(), nt * sizeof(double), cudaMemcpyHostToDevice));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_probe_off.p, engine->probe_off.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_probe_mode.p, engine->probe_mode.data(), np * sizeof(int), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_term_idx.p, engine->term_idx.data(), nt * sizeof(long long), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_term_comp.p, engine->term_comp.data(), nt * sizeof(int), cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_term_w.p, engine->term_w.data(), nt * sizeof(double), cudaMemcpyHostToDevice, engine->stream));
   engine->d_traces.ensure(0);
   engine->traces_steps = 0;
   engine->graph_epoch++;  // device table pointers and the probe count are baked into graphs
@@ -2389,8 +2544,10 @@ oems_status oems_engine_read_probe_traces(oems_engine* engine, double* out, uint
   const size_t np = engine->nprobe();
   if (steps == 0 || np == 0) return OEMS_OK;
   if (!out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL output buffer");
-  DeviceGuard guard(engine->device);
-  OEMS_CUDA(cudaMemcpy(out, engine->d_traces.p, steps * np * sizeof(double), cudaMemcpyDeviceToHost));
+  EngineScope guard(engine);
+  OEMS_CUDA(cudaMemcpyAsync(out, engine->d_traces.p, steps * np * sizeof(double), cudaMemcpyDeviceToHost,
+                            engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   return OEMS_OK;
 }
 
@@ -2399,7 +2556,7 @@ oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t probe_id, con
   if (!engine || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   if (probe_id < 0 || probe_id >= engine->nprobe()) return fail(OEMS_ERR_CONFIG, "unknown probe");
   if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "a DFT needs at least one frequency");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   engine->dft_first.push_back((int)engine->entry_probe.size());
   engine->dft_count.push_back((int)nfreq);
   for (uint64_t f = 0; f < nfreq; ++f) {
@@ -2411,19 +2568,23 @@ oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t probe_id, con
   // keep the accumulated values of existing DFTs
   std::vector<double> acc(2 * ne, 0.0);
   const size_t old = ne - nfreq;
-  if (old) OEMS_CUDA(cudaMemcpy(acc.data(), engine->d_dft_acc.p, 2 * old * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaStream_t s = engine->stream;
+  if (old) {
+    OEMS_CUDA(cudaMemcpyAsync(acc.data(), engine->d_dft_acc.p, 2 * old * sizeof(double), cudaMemcpyDeviceToHost, s));
+    OEMS_CUDA(cudaStreamSynchronize(s));
+  }
   OEMS_CUDA(engine->d_entry_probe.ensure(ne));
   OEMS_CUDA(engine->d_entry_freq.ensure(ne));
   OEMS_CUDA(engine->d_entry_half.ensure(ne));
-  if (engine->d_dft_acc.n < 2 * ne) {
-    engine->d_dft_acc.ensure(0);
-    OEMS_CUDA(cudaMalloc(&engine->d_dft_acc.p, 2 * ne * sizeof(double)));
-    engine->d_dft_acc.n = 2 * ne;
-  }
-  OEMS_CUDA(cudaMemcpy(engine->d_entry_probe.p, engine->entry_probe.data(), ne * sizeof(int), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_entry_freq.p, engine->entry_freq.data(), ne * sizeof(double), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_entry_half.p, engine->entry_half.data(), ne * sizeof(double), cudaMemcpyHostToDevice));
-  OEMS_CUDA(cudaMemcpy(engine->d_dft_acc.p, acc.data(), 2 * ne * sizeof(double), cudaMemcpyHostToDevice));
+  OEMS_CUDA(engine->d_dft_acc.ensure(2 * ne));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_entry_probe.p, engine->entry_probe.data(), ne * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_entry_freq.p, engine->entry_freq.data(), ne * sizeof(double),
+                            cudaMemcpyHostToDevice, s));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_entry_half.p, engine->entry_half.data(), ne * sizeof(double),
+                            cudaMemcpyHostToDevice, s));
+  OEMS_CUDA(cudaMemcpyAsync(engine->d_dft_acc.p, acc.data(), 2 * ne * sizeof(double), cudaMemcpyHostToDevice, s));
+  OEMS_CUDA(cudaStreamSynchronize(s));
   if (dft_id) *dft_id = (int32_t)engine->dft_first.size() - 1;
   return OEMS_OK;
 }
@@ -2431,16 +2592,17 @@ oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t probe_id, con
 oems_status oems_engine_read_probe_dft(oems_engine* engine, int32_t dft_id, double* out) {
   if (!engine || !out) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   if (dft_id < 0 || dft_id >= (int32_t)engine->dft_first.size()) return fail(OEMS_ERR_CONFIG, "unknown DFT");
-  DeviceGuard guard(engine->device);
-  OEMS_CUDA(cudaMemcpy(out, engine->d_dft_acc.p + 2 * engine->dft_first[dft_id],
-                       2 * engine->dft_count[dft_id] * sizeof(double), cudaMemcpyDeviceToHost));
+  EngineScope guard(engine);
+  OEMS_CUDA(cudaMemcpyAsync(out, engine->d_dft_acc.p + 2 * engine->dft_first[dft_id],
+                            2 * engine->dft_count[dft_id] * sizeof(double), cudaMemcpyDeviceToHost, engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   return OEMS_OK;
 }
 
 
 oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_energy) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
-  DeviceGuard guard(engine->device);
+  EngineScope guard(engine);
   OEMS_CUDA(engine->d_energy.ensure(2));
   OEMS_TRY(launch_energy(engine, engine->d_energy.p));
   double out[2];
@@ -2507,6 +2669,26 @@ oems_status oems_engine_last_batch_stats(const oems_engine* engine, uint64_t* ke
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   if (kernel_launches) *kernel_launches = engine->last_launches;
   if (device_seconds) *device_seconds = engine->last_device_seconds;
+  return OEMS_OK;
+}
+
+oems_status oems_release_cached_memory(int32_t device) {
+  int dev = device;
+  if (dev < 0) OEMS_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool = nullptr;
+  OEMS_CUDA(device_pool(dev, false, &pool));
+  if (pool) {
+    DeviceGuard guard(dev);
+    OEMS_CUDA(cudaDeviceSynchronize());  // frees still pending on engine streams complete first
+    OEMS_CUDA(cudaMemPoolTrimTo(pool, 0));
+  }
+  std::multimap<size_t, void*> bufs;
+  {
+    PinnedCache& pc = pinned_cache();
+    std::lock_guard<std::mutex> lk(pc.mu);
+    bufs.swap(pc.free);
+  }
+  for (auto& kv : bufs) OEMS_CUDA(cudaFreeHost(kv.second));
   return OEMS_OK;
 }
 

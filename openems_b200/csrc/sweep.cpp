@@ -73,7 +73,12 @@ oems_status port_probe(oems_engine* en, const oems_operator* op, const uint64_t 
   return oems_engine_add_probe(en, t.data(), n, OEMS_PROBE_SUM_F64, id);
 }
 
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch) {
+  const auto t_start = std::chrono::steady_clock::now();
   const oems_sweep_instance& d = I.desc;
   double scale = 0.0;
   oems_status st = oems_operator_set_lumped(I.op, d.port_position, d.port_direction, d.port_resistance, 0.0,
@@ -111,6 +116,7 @@ oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch) {
   const uint64_t cap = d.max_timesteps;
   double peak = 0.0;
   uint64_t run = 0;
+  I.res.setup_seconds = seconds_since(t_start);
   while (run < cap) {
     const uint64_t n = std::min(cap - run, batch);
     if ((st = oems_excitation_sample(&w, run, n, dt, samples.data())) != OEMS_OK) return st;
@@ -216,7 +222,9 @@ oems_status oems_sweep_run(oems_sweep* s, uint64_t batch_steps) {
   auto worker = [&]() {
     for (size_t k = next++; k < todo.size(); k = next++) {
       Instance& I = *todo[k];
+      const auto t_inst = std::chrono::steady_clock::now();
       const oems_status st = run_instance(s, I, batch);
+      I.res.host_seconds = seconds_since(t_inst);
       I.res.status = st;
       if (st != OEMS_OK) I.error = oems_last_error_message();
       I.done = true;

@@ -95,7 +95,8 @@ class Sweep:
         uf, if_, s11 = (b[0::2] + 1j * b[1::2] for b in bufs)
         return {"timesteps": int(info.timesteps), "termination_reason": int(info.termination_reason),
                 "final_decay_db": float(info.final_decay_db), "device_seconds": float(info.device_seconds),
-                "cells": float(info.cells), "uf": uf, "if": if_, "s11": s11}
+                "cells": float(info.cells), "setup_seconds": float(info.setup_seconds),
+                "host_seconds": float(info.host_seconds), "uf": uf, "if": if_, "s11": s11}
 
     def set_trace_steps(self, steps: int):
         """Record the port u / i traces of the first `steps` timesteps."""

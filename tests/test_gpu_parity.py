@@ -87,6 +87,16 @@ def test_mur(sc, kernels):
     assert_parity(run_engine(sc, kernels=kernels), run_oracle(sc))
 
 
+@pytest.mark.parametrize("sc", cpml_scenarios() + odd_scenarios()[3:5], ids=lambda s: s.name)
+def test_small_grid_default_shape(sc):
+    """Without the tuner a small grid gets shorter x-runs (and narrower CTAs)
+    so that every SM has a work item; the results stay bit-exact."""
+    got = run_engine(sc, autotune=False, kernels="register")
+    info = got["engine"].launch_info()
+    assert info["ichunk"] < 8 or info["threads"] < 256, info
+    assert_parity(got, run_oracle(sc))
+
+
 def test_staged_kernels_are_used_when_requested():
     sc = cpml_scenarios()[0]
     r = run_engine(sc, kernels="staged")
