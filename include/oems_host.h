@@ -202,11 +202,14 @@ typedef struct oems_sweep_result {
   uint64_t timesteps;
   int32_t termination_reason; /* OEMS_TERMINATION_* */
   int32_t status;             /* OEMS_OK or the instance's error */
-  double final_decay_db;
+  double final_decay_db;      /* energy of the last sample (every 100 steps) below the peak so far, dB
+                                 (<= 0); for a decayed instance the level that ended it */
   double device_seconds;      /* sum over the instance's batches */
   double cells;
   double setup_seconds;       /* host time from the start of the instance to its first batch */
-  double host_seconds;        /* host time of the whole instance, engine teardown included */
+  double host_seconds;        /* host time of the instance over every run call, teardown included */
+  int32_t paused;             /* 1: stopped at a run_until cap, engine kept for the next call */
+  int32_t reserved0;
 } oems_sweep_result;
 
 /* freqs: the DFT frequencies of every instance (Hz).  engine_flags as for
@@ -215,9 +218,18 @@ OEMS_API oems_status oems_sweep_create(int32_t device, uint32_t concurrency, uin
                                        const double* freqs, uint64_t nfreq, oems_sweep** out);
 OEMS_API void oems_sweep_destroy(oems_sweep* sweep);
 OEMS_API oems_status oems_sweep_add(oems_sweep* sweep, const oems_sweep_instance* inst, int32_t* instance_id);
-/* Runs every instance not run yet; batch_steps 0 = 2000.  Returns the first
- * instance error (the others still run; see oems_sweep_get_result). */
+/* Runs every instance that has not ended to its end (energy decay or
+ * max_timesteps); batch_steps 0 = 2000.  Returns the first instance error
+ * (the others still run; see oems_sweep_get_result). */
 OEMS_API oems_status oems_sweep_run(oems_sweep* sweep, uint64_t batch_steps);
+/* As oems_sweep_run, but an instance stops once it has run step_cap steps in
+ * total and keeps its engine (paused): a later run / run_until continues it
+ * bit-for-bit as if uninterrupted.  Results of a paused instance hold the
+ * DFTs and S11 of the steps run so far. */
+OEMS_API oems_status oems_sweep_run_until(oems_sweep* sweep, uint64_t batch_steps, uint64_t step_cap);
+/* Ends a paused instance (its engine is released); its result stays the
+ * partial one.  No-op for an instance that has ended. */
+OEMS_API oems_status oems_sweep_finish(oems_sweep* sweep, int32_t instance_id);
 /* uf, if_ and s11: 2 x nfreq doubles (re, im) each; any may be NULL. */
 OEMS_API oems_status oems_sweep_get_result(const oems_sweep* sweep, int32_t instance_id, oems_sweep_result* info,
                                            double* uf, double* if_, double* s11);
@@ -227,7 +239,8 @@ OEMS_API oems_status oems_sweep_set_trace_steps(oems_sweep* sweep, uint64_t step
 /* out: cap_steps x 2 doubles; *nsteps receives the recorded step count. */
 OEMS_API oems_status oems_sweep_get_trace(const oems_sweep* sweep, int32_t instance_id, double* out,
                                           uint64_t cap_steps, uint64_t* nsteps);
-/* Wall time of the last run and the cell x timestep count it executed. */
+/* Wall time of the last run / run_until call and the cell x timestep count
+ * it executed. */
 OEMS_API oems_status oems_sweep_stats(const oems_sweep* sweep, double* wall_seconds, double* cell_steps);
 
 #ifdef __cplusplus

@@ -190,7 +190,7 @@ class SweepInstanceC(ctypes.Structure):
 class SweepResultC(ctypes.Structure):
     _fields_ = [("timesteps", c_u64), ("termination_reason", c_i32), ("status", c_i32),
                 ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64),
-                ("setup_seconds", c_f64), ("host_seconds", c_f64)]
+                ("setup_seconds", c_f64), ("host_seconds", c_f64), ("paused", c_i32), ("reserved0", c_i32)]
 
 
 # name -> (restype, argtypes); every symbol the headers declare
@@ -253,6 +253,8 @@ SIGNATURES = {
                                       ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_sweep_stats": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_sweep_set_trace_steps": (c_i32, [P, c_u64]),
+    "oems_sweep_run_until": (c_i32, [P, c_u64, c_u64]),
+    "oems_sweep_finish": (c_i32, [P, c_i32]),
     "oems_tc_gemm_bf16": (c_i32, [P, c_i32, P, c_i32, P, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, P, P]),
     "oems_tc_check": (c_i32, [P]),
     "oems_pk_f32_to_bf16": (c_i32, [P, P, c_i64, P]),

@@ -9,6 +9,9 @@
 // f64 probes with running DFTs, and batches run until the energy has decayed
 // by the requested dB below its peak (the peak carried across batches) or the
 // step cap.  S11 follows Port.CalcPort (python/openEMS/ports.py:136-138).
+// oems_sweep_run_until stops every instance at a step count and keeps its
+// engine: a later call continues it where it stopped (the same bits as an
+// uninterrupted run), oems_sweep_finish ends it with its partial DFTs.
 // Only the public C ABI of the engine and the host operator is used.
 
 #include <algorithm>
@@ -32,11 +35,17 @@ namespace {
 struct Instance {
   oems_operator* op = nullptr;
   oems_sweep_instance desc{};
-  bool done = false;
+  bool done = false;  // ended: decayed, at max_timesteps, finished by the caller or failed
   oems_sweep_result res{};
   std::string error;
   std::vector<double> uf, if_;
   std::vector<double> trace;  // [step][2]: u, i (first trace_steps steps)
+  // state of a started instance, kept between calls while it is paused
+  oems_engine* en = nullptr;
+  oems_excitation wave{};
+  double dt = 0.0, peak = 0.0;
+  uint64_t run = 0;
+  int32_t du = -1, di = -1;
 };
 
 oems_status sfail(oems_status st, const char* msg) {
@@ -77,49 +86,60 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch) {
-  const auto t_start = std::chrono::steady_clock::now();
+// Engine, CPML, port probes and DFTs of an instance (its operator is
+// released once the engine holds the coefficients).
+oems_status start_instance(const oems_sweep* sw, Instance& I) {
   const oems_sweep_instance& d = I.desc;
   double scale = 0.0;
   oems_status st = oems_operator_set_lumped(I.op, d.port_position, d.port_direction, d.port_resistance, 0.0,
                                             d.port_eps_r, d.port_sigma, &scale);
   if (st != OEMS_OK) return st;
   uint64_t dims[3];
-  double dt = 0.0, delta[3];
-  oems_operator_info(I.op, dims, &dt, delta);
+  double delta[3];
+  oems_operator_info(I.op, dims, &I.dt, delta);
   I.res.cells = (double)dims[0] * (double)dims[1] * (double)dims[2];
   oems_operator_desc od;
   st = oems_operator_engine_desc(I.op, sw->device, sw->flags, &od);
   if (st != OEMS_OK) return st;
-  oems_engine* en = nullptr;
-  st = oems_engine_create(&od, &en);
-  if (st != OEMS_OK) return st;
-  std::unique_ptr<oems_engine, void (*)(oems_engine*)> guard(en, oems_engine_destroy);
+  if ((st = oems_engine_create(&od, &I.en)) != OEMS_OK) return st;
   bool cpml = false;
   for (int f = 0; f < 6; ++f) cpml = cpml || d.cpml.layers[f] > 0;
-  if (cpml && (st = oems_engine_add_cpml(en, &d.cpml)) != OEMS_OK) return st;
-  int32_t pu = -1, pi = -1, du = -1, di = -1;
-  if ((st = port_probe(en, I.op, d.port_position, d.port_direction, 0, &pu)) != OEMS_OK) return st;
-  if ((st = port_probe(en, I.op, d.port_position, d.port_direction, 1, &pi)) != OEMS_OK) return st;
+  if (cpml && (st = oems_engine_add_cpml(I.en, &d.cpml)) != OEMS_OK) return st;
+  int32_t pu = -1, pi = -1;
+  if ((st = port_probe(I.en, I.op, d.port_position, d.port_direction, 0, &pu)) != OEMS_OK) return st;
+  if ((st = port_probe(I.en, I.op, d.port_position, d.port_direction, 1, &pi)) != OEMS_OK) return st;
   const uint64_t nf = sw->freqs.size();
-  if ((st = oems_engine_add_probe_dft(en, pu, sw->freqs.data(), nf, &du)) != OEMS_OK) return st;
-  if ((st = oems_engine_add_probe_dft(en, pi, sw->freqs.data(), nf, &di)) != OEMS_OK) return st;
+  if ((st = oems_engine_add_probe_dft(I.en, pu, sw->freqs.data(), nf, &I.du)) != OEMS_OK) return st;
+  if ((st = oems_engine_add_probe_dft(I.en, pi, sw->freqs.data(), nf, &I.di)) != OEMS_OK) return st;
   // the engine holds its own copy of the coefficients from here on
   oems_operator_destroy(I.op);
   I.op = nullptr;
+  I.wave = d.waveform;
+  I.wave.amplitude *= scale;
+  return OEMS_OK;
+}
 
-  oems_excitation w = d.waveform;
-  w.amplitude *= scale;
+void end_instance(Instance& I) {
+  if (I.en) oems_engine_destroy(I.en);
+  I.en = nullptr;
+  I.done = true;
+  I.res.paused = 0;
+}
+
+// Runs batches until the instance ends or has run `cap` steps in total; the
+// port DFTs so far are read back either way.
+oems_status advance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t cap) {
+  const oems_sweep_instance& d = I.desc;
+  const uint64_t nf = sw->freqs.size();
+  const uint64_t limit = std::min<uint64_t>(cap, d.max_timesteps);
   std::vector<float> samples(batch);
   std::vector<oems_energy_sample> es(batch / 100 + 2);
   const bool has_decay = d.energy_decay_db != 0.0;
-  const uint64_t cap = d.max_timesteps;
-  double peak = 0.0;
-  uint64_t run = 0;
-  I.res.setup_seconds = seconds_since(t_start);
-  while (run < cap) {
-    const uint64_t n = std::min(cap - run, batch);
-    if ((st = oems_excitation_sample(&w, run, n, dt, samples.data())) != OEMS_OK) return st;
+  oems_status st = OEMS_OK;
+  bool ended = I.run >= d.max_timesteps;
+  while (!ended && I.run < limit) {
+    const uint64_t n = std::min(limit - I.run, batch);
+    if ((st = oems_excitation_sample(&I.wave, I.run, n, I.dt, samples.data())) != OEMS_OK) return st;
     oems_scheduled_excitation x{};
     for (int a = 0; a < 3; ++a) x.position[a] = d.port_position[a];
     x.direction = (uint32_t)d.port_direction;
@@ -135,35 +155,54 @@ oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch) {
     b.check_interval = 100;
     b.sample_interval = 100;
     b.track_peak = 1;
-    b.initial_peak_energy = peak;
+    b.initial_peak_energy = I.peak;
     oems_batch_result r{};
     r.energy_samples = es.data();
     r.energy_capacity = es.size();
-    if ((st = oems_engine_run_batch(en, &b, &r)) != OEMS_OK) return st;
-    if (sw->trace_steps > run) {
+    if ((st = oems_engine_run_batch(I.en, &b, &r)) != OEMS_OK) return st;
+    if (sw->trace_steps > I.run) {
       // port u / i of this batch, kept up to trace_steps
-      const uint64_t keep = std::min<uint64_t>(r.timesteps_executed, sw->trace_steps - run);
+      const uint64_t keep = std::min<uint64_t>(r.timesteps_executed, sw->trace_steps - I.run);
       std::vector<double> tr(2 * std::max<uint64_t>(r.timesteps_executed, 1));
       uint64_t got = 0;
-      if ((st = oems_engine_read_probe_traces(en, tr.data(), r.timesteps_executed, &got)) != OEMS_OK) return st;
+      if ((st = oems_engine_read_probe_traces(I.en, tr.data(), r.timesteps_executed, &got)) != OEMS_OK) return st;
       I.trace.insert(I.trace.end(), tr.begin(), tr.begin() + 2 * std::min(keep, got));
     }
     uint64_t launches = 0;
     double dev_s = 0.0;
-    oems_engine_last_batch_stats(en, &launches, &dev_s);
+    oems_engine_last_batch_stats(I.en, &launches, &dev_s);
     I.res.device_seconds += dev_s;
-    run += r.timesteps_executed;
-    peak = std::max(peak, r.peak_energy);
+    I.run += r.timesteps_executed;
+    I.peak = std::max(I.peak, r.peak_energy);
     I.res.termination_reason = r.termination_reason;
-    I.res.final_decay_db = r.final_decay_db;
-    if (r.termination_reason != OEMS_TERMINATION_STEPS_COMPLETED || r.timesteps_executed == 0) break;
+    const uint64_t ns = std::min<uint64_t>(r.num_energy_samples, es.size());
+    if (r.termination_reason == OEMS_TERMINATION_ENERGY_DECAY)
+      I.res.final_decay_db = r.final_decay_db;
+    else if (ns > 0 && I.peak > 0.0 && es[ns - 1].total_energy > 0.0)
+      I.res.final_decay_db = 10.0 * std::log10(es[ns - 1].total_energy / I.peak);
+    if (r.termination_reason != OEMS_TERMINATION_STEPS_COMPLETED || r.timesteps_executed == 0) ended = true;
   }
-  I.res.timesteps = run;
+  ended = ended || I.run >= d.max_timesteps;
+  I.res.timesteps = I.run;
   I.uf.assign(2 * nf, 0.0);
   I.if_.assign(2 * nf, 0.0);
-  if ((st = oems_engine_read_probe_dft(en, du, I.uf.data())) != OEMS_OK) return st;
-  if ((st = oems_engine_read_probe_dft(en, di, I.if_.data())) != OEMS_OK) return st;
+  if ((st = oems_engine_read_probe_dft(I.en, I.du, I.uf.data())) != OEMS_OK) return st;
+  if ((st = oems_engine_read_probe_dft(I.en, I.di, I.if_.data())) != OEMS_OK) return st;
+  if (ended)
+    end_instance(I);
+  else
+    I.res.paused = 1;
   return OEMS_OK;
+}
+
+oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t cap) {
+  if (!I.en) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const oems_status st = start_instance(sw, I);
+    I.res.setup_seconds = seconds_since(t_start);
+    if (st != OEMS_OK) return st;
+  }
+  return advance(sw, I, batch, cap);
 }
 
 }  // namespace
@@ -186,7 +225,10 @@ oems_status oems_sweep_create(int32_t device, uint32_t concurrency, uint32_t eng
 
 void oems_sweep_destroy(oems_sweep* s) {
   if (!s) return;
-  for (auto& I : s->inst) oems_operator_destroy(I->op);
+  for (auto& I : s->inst) {
+    if (I->en) oems_engine_destroy(I->en);
+    oems_operator_destroy(I->op);
+  }
   delete s;
 }
 
@@ -211,23 +253,27 @@ oems_status oems_sweep_add(oems_sweep* s, const oems_sweep_instance* d, int32_t*
   return OEMS_OK;
 }
 
-oems_status oems_sweep_run(oems_sweep* s, uint64_t batch_steps) {
+oems_status oems_sweep_run_until(oems_sweep* s, uint64_t batch_steps, uint64_t step_cap) {
   if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
   const uint64_t batch = batch_steps ? batch_steps : 2000;
   std::vector<Instance*> todo;
   for (auto& I : s->inst)
     if (!I->done) todo.push_back(I.get());
+  std::vector<uint64_t> before(todo.size());
+  for (size_t k = 0; k < todo.size(); ++k) before[k] = todo[k]->run;
   std::atomic<size_t> next{0};
   const auto t0 = std::chrono::steady_clock::now();
   auto worker = [&]() {
     for (size_t k = next++; k < todo.size(); k = next++) {
       Instance& I = *todo[k];
       const auto t_inst = std::chrono::steady_clock::now();
-      const oems_status st = run_instance(s, I, batch);
-      I.res.host_seconds = seconds_since(t_inst);
+      const oems_status st = run_instance(s, I, batch, step_cap);
       I.res.status = st;
-      if (st != OEMS_OK) I.error = oems_last_error_message();
-      I.done = true;
+      if (st != OEMS_OK) {
+        I.error = oems_last_error_message();
+        end_instance(I);
+      }
+      I.res.host_seconds += seconds_since(t_inst);
     }
   };
   const size_t nthreads = std::min<size_t>(s->concurrency, todo.size());
@@ -237,12 +283,25 @@ oems_status oems_sweep_run(oems_sweep* s, uint64_t batch_steps) {
   for (auto& t : pool) t.join();
   s->wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   s->cell_steps = 0.0;
-  for (Instance* I : todo) s->cell_steps += I->res.cells * (double)I->res.timesteps;
+  for (size_t k = 0; k < todo.size(); ++k) s->cell_steps += todo[k]->res.cells * (double)(todo[k]->run - before[k]);
   for (Instance* I : todo)
     if (I->res.status != OEMS_OK) {
       oems::g_last_error = "sweep instance failed: " + I->error;
       return (oems_status)I->res.status;
     }
+  return OEMS_OK;
+}
+
+oems_status oems_sweep_run(oems_sweep* s, uint64_t batch_steps) {
+  return oems_sweep_run_until(s, batch_steps, UINT64_MAX);
+}
+
+oems_status oems_sweep_finish(oems_sweep* s, int32_t id) {
+  if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
+  if (id < 0 || id >= (int32_t)s->inst.size()) return sfail(OEMS_ERR_CONFIG, "unknown sweep instance");
+  Instance& I = *s->inst[id];
+  if (!I.done && !I.en) return sfail(OEMS_ERR_CONFIG, "sweep instance has not run");
+  if (!I.done) end_instance(I);
   return OEMS_OK;
 }
 
@@ -252,7 +311,7 @@ oems_status oems_sweep_get_result(const oems_sweep* s, int32_t id, oems_sweep_re
   if (id < 0 || id >= (int32_t)s->inst.size()) return sfail(OEMS_ERR_CONFIG, "unknown sweep instance");
   const Instance& I = *s->inst[id];
   if (info) *info = I.res;
-  if (!I.done) return sfail(OEMS_ERR_CONFIG, "sweep instance has not run");
+  if (!I.done && !I.en) return sfail(OEMS_ERR_CONFIG, "sweep instance has not run");
   if (I.res.status != OEMS_OK) return sfail((oems_status)I.res.status, I.error.c_str());
   const size_t nf = s->freqs.size();
   if (uf) std::copy(I.uf.begin(), I.uf.end(), uf);

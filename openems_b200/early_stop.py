@@ -1,0 +1,330 @@
+"""Staged early termination of port sweeps.
+
+Every instance of a sweep runs to the first stage (K steps) and pauses
+(oems_sweep_run_until keeps its engine).  Its S11 is then predicted from the
+engine's port DFTs of the K simulated steps plus the matrix-pencil
+continuation of the last window of the port traces (predictor.py).  The
+residual check repeats the prediction from a window that ends `lag` steps
+earlier: when the two predicted S11 curves agree to within `tau` dB over the
+band (both clipped at -30 dB), the prediction is accepted and the instance
+ends there.  Otherwise the instance continues to the next stage, and after the
+last stage runs on to the plain end condition (-50 dB energy decay), whose
+S11 is exact: the full run is the fallback and the judge of the error.
+Instances that decay before a stage are exact as well.
+
+`calibrate` records the check and the prediction error of every instance at
+every stage against its full run, so that `tau` can be chosen on a training
+family; `main` times a staged sweep against the plain full-length sweep of the
+same instances.
+"""
+from __future__ import annotations
+
+import os
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import predictor as P
+from . import workloads as W
+from .sweep import Sweep
+
+FLOOR_DB = -30.0
+
+
+def s11_db(s: np.ndarray, floor: float = FLOOR_DB) -> np.ndarray:
+    return np.maximum(20.0 * np.log10(np.maximum(np.abs(s), 1e-30)), floor)
+
+
+def s11_db_error(a: np.ndarray, b: np.ndarray, band: np.ndarray, floor: float = FLOOR_DB) -> float:
+    """Largest |dB(a) - dB(b)| over the band, both clipped at `floor` dB."""
+    return float(np.abs(s11_db(a, floor) - s11_db(b, floor))[band].max())
+
+
+def s11_db_mean_error(a: np.ndarray, b: np.ndarray, band: np.ndarray, floor: float = FLOOR_DB) -> float:
+    """Mean |dB(a) - dB(b)| over the band, both clipped at `floor` dB."""
+    return float(np.abs(s11_db(a, floor) - s11_db(b, floor))[band].mean())
+
+
+def pencil_s11(trace: np.ndarray, uf: np.ndarray, if_: np.ndarray, K: int, dt: float, freqs: np.ndarray,
+               horizon: int, lag: int = 0, R: float = 50.0, **pencil) -> np.ndarray:
+    """S11 predicted at K: the engine's DFTs of steps [0, K - lag) (those of
+    [0, K) minus the last `lag` trace samples) plus the pencil continuation
+    of the window that ends at K - lag.  trace: (>= K, 2) port u, i."""
+    uh, ih = uf.copy(), if_.copy()
+    if lag:
+        uh -= P.head_dft(trace[K - lag:K, 0], K - lag + 1, dt, freqs, 0.0)
+        ih -= P.head_dft(trace[K - lag:K, 1], K - lag + 1, dt, freqs, 0.5)
+    ke = K - lag
+    ut = P.pencil_tail_dft(trace[:ke, 0], ke, dt, freqs, 0.0, horizon, **pencil)
+    it = P.pencil_tail_dft(trace[:ke, 1], ke, dt, freqs, 0.5, horizon, **pencil)
+    return P.s11(uh + ut, ih + it, R)
+
+
+def judge_end(u: np.ndarray, K: int, level_db: float, dt: float, decay_db: float, cap: int,
+              **pencil) -> int:
+    """Step at which the plain run would stop: its field energy, now
+    `level_db` below the peak, is continued with the pencil modes of the port
+    voltage (each mode's energy |c|^2 decaying at twice its rate) down to
+    -decay_db, rounded up to the run's 100-step energy checks, at most `cap`."""
+    p, c = P.pencil_modes(u, K, dt, **pencil)
+    target = 10.0 ** ((-abs(decay_db) - level_db) / 10.0)  # E(end) / E(now)
+    if len(p) == 0 or target >= 1.0:
+        return K
+    rate, w = -2.0 * p.real, np.abs(c) ** 2
+
+    def rest(t):
+        return (w * np.exp(-rate * t)).sum() / w.sum()
+
+    lo, hi = 0.0, (cap - K) * dt
+    if rest(hi) > target:
+        return cap
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if rest(mid) > target else (lo, mid)
+    return int(min(cap, np.ceil((K + hi / dt) / 100.0) * 100))
+
+
+@dataclass
+class StagePlan:
+    """Stages (step counts), the residual check's lag and threshold, the band
+    it is evaluated on and the pencil settings: at stage K the window is
+    `window_frac` K samples (at most `max_window`), decimated to about
+    `samples` points."""
+
+    stages: Sequence[int] = (2048, 4096, 8192, 16384)
+    lag: int = 256
+    tau: float = 0.1
+    fmin: float = 0.5e9
+    window_frac: float = 0.75
+    max_window: int = 12288
+    samples: int = 384
+    max_modes: int = 40
+    judge_horizon: bool = True
+
+    def band(self, freqs: np.ndarray) -> np.ndarray:
+        return np.asarray(freqs) >= self.fmin
+
+    def pencil(self, K: int) -> dict:
+        window = min(int(self.window_frac * K), self.max_window)
+        return dict(window=window, decimate=max(1, window // self.samples), max_modes=self.max_modes)
+
+
+def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan):
+    """(prediction at K, residual-check value in dB, continuation end step)."""
+    from threadpoolctl import threadpool_limits
+    pen = plan.pencil(K)
+    with threadpool_limits(1):
+        end = judge_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, **pen) \
+            if plan.judge_horizon else horizon
+        end = max(end, K)
+        a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, **pen)
+        b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
+    return a, s11_db_error(a, b, plan.band(freqs)), end
+
+
+def _pool():
+    return ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1))
+
+
+def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int = 16,
+                 batch_steps: int = 2000) -> dict:
+    """Runs the staged sweep; returns per instance S11, how it was obtained
+    ("decayed", "predicted" at a stage, or "full" fallback), the steps run,
+    and the wall time split into device runs and host checks."""
+    dt = instances[0].operator.timestep()
+    horizon = max(i.max_timesteps for i in instances)
+    decay_db = instances[0].energy_decay_db
+    sw = Sweep(freqs, concurrency=concurrency)
+    sw.set_trace_steps(max(plan.stages))
+    ids = [sw.add(i) for i in instances]
+    out: Dict[int, dict] = {}
+    t_run = t_check = 0.0
+    t0 = time.perf_counter()
+    with _pool() as pool:
+        for K in plan.stages:
+            sw.run_until(K, batch_steps)
+            t_run += sw.stats()[0]
+            tc = time.perf_counter()
+            live, jobs = [], []
+            for i in ids:
+                if i in out:
+                    continue
+                r = sw.result(i)
+                if not r["paused"]:
+                    out[i] = {"s11": r["s11"], "how": "decayed", "steps": r["timesteps"], "stage": K}
+                    continue
+                live.append((i, r))
+                jobs.append(pool.submit(check_instance, sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan))
+            for (i, r), j in zip(live, jobs):
+                pred, d, end = j.result()
+                if d < plan.tau:
+                    out[i] = {"s11": pred, "how": "predicted", "steps": K, "stage": K, "check_db": d,
+                              "end": end}
+                    sw.finish(i)
+            t_check += time.perf_counter() - tc
+    rest = [i for i in ids if i not in out]
+    if rest:
+        sw.run(batch_steps)
+        t_run += sw.stats()[0]
+        for i in rest:
+            r = sw.result(i)
+            out[i] = {"s11": r["s11"], "how": "full", "steps": r["timesteps"], "stage": None}
+    wall = time.perf_counter() - t0
+    res = [out[i] for i in ids]
+    sw.close()
+    return {"results": res, "wall_s": wall, "run_s": t_run, "check_s": t_check}
+
+
+def full_sweep(instances, freqs: np.ndarray, concurrency: int = 16, batch_steps: int = 2000) -> dict:
+    """The plain batched sweep: every instance to its end condition."""
+    t0 = time.perf_counter()
+    sw = Sweep(freqs, concurrency=concurrency)
+    ids = [sw.add(i) for i in instances]
+    sw.run(batch_steps)
+    res = [sw.result(i) for i in ids]
+    wall = time.perf_counter() - t0
+    sw.close()
+    return {"results": res, "wall_s": wall}
+
+
+def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.ndarray],
+              concurrency: int = 16, batch_steps: int = 2000) -> dict:
+    """Check values d[n, s] and prediction errors e[n, s] (dB, against the
+    full runs) of every instance at every stage, with no instance finished
+    early (NaN where the instance had already decayed)."""
+    dt = instances[0].operator.timestep()
+    horizon = max(i.max_timesteps for i in instances)
+    decay_db = instances[0].energy_decay_db
+    band = plan.band(freqs)
+    sw = Sweep(freqs, concurrency=concurrency)
+    sw.set_trace_steps(max(plan.stages))
+    ids = [sw.add(i) for i in instances]
+    n, ns = len(ids), len(plan.stages)
+    d = np.full((n, ns), np.nan)
+    e = np.full((n, ns), np.nan)
+    end = np.full((n, ns), np.nan)
+    em = np.full((n, ns), np.nan)
+    with _pool() as pool:
+        for s, K in enumerate(plan.stages):
+            sw.run_until(K, batch_steps)
+            jobs = {}
+            for k, i in enumerate(ids):
+                r = sw.result(i)
+                if r["paused"]:
+                    jobs[k] = pool.submit(check_instance, sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan)
+            for k, j in jobs.items():
+                pred, d[k, s], end[k, s] = j.result()
+                e[k, s] = s11_db_error(pred, full_s11[k], band)
+                em[k, s] = s11_db_mean_error(pred, full_s11[k], band)
+    sw.close()
+    return {"check_db": d, "error_db": e, "mean_error_db": em, "end": end}
+
+
+def simulate(cal: dict, tau: float) -> dict:
+    """Outcome of the staged rule with threshold tau on calibration records:
+    per instance the stage index it stops at (-1: decayed or full run) and
+    its S11 error (0 for exact)."""
+    d, e = cal["check_db"], cal["error_db"]
+    em = cal.get("mean_error_db", e)
+    stop = np.full(len(d), -1)
+    err = np.zeros(len(d))
+    merr = np.zeros(len(d))
+    for k in range(len(d)):
+        for s in range(d.shape[1]):
+            if np.isnan(d[k, s]):
+                break  # decayed before this stage: exact
+            if d[k, s] < tau:
+                stop[k], err[k], merr[k] = s, e[k, s], em[k, s]
+                break
+    return {"stop": stop, "error_db": err, "mean_error_db": merr}
+
+
+def family_instances(family: str, count: int, seed: int):
+    """(instances, freqs): "small" is the reduced patch family (n ~ U{40..80},
+    0-12 GHz, 241 points, cap 40000 steps); "patch" the 64-instance patch
+    sweep family (n ~ U{48..160}, 0-8 GHz, 801 points, cap 60000 steps)."""
+    if family == "small":
+        specs = P.family_specs(count, seed)
+        return ([W.patch_sweep_instance(s, delta=0.5e-3, decay_db=50.0, max_steps=P.HORIZON, fmax=12e9)
+                 for s in specs], P.FREQS)
+    specs = W.patch_specs(count, seed=seed)
+    return ([W.patch_sweep_instance(s, decay_db=50.0, max_steps=60000) for s in specs],
+            np.linspace(0.0, 8e9, 801))
+
+
+def main(argv=None):
+    """python -m openems_b200.early_stop {calibrate,run} --family small|patch
+    --count N --seed S [--tau T]: `calibrate` prints, per threshold, the
+    largest and 99th-percentile S11 error and the mean steps run; `run` times
+    the plain full sweep and the staged sweep of the same instances and prints
+    one JSON line (errors against the full runs, instances per hour)."""
+    import argparse
+    import json
+    p = argparse.ArgumentParser()
+    p.add_argument("cmd", choices=["calibrate", "run"])
+    p.add_argument("--family", choices=["small", "patch"], default="small")
+    p.add_argument("--count", type=int, default=500)
+    p.add_argument("--seed", type=int, default=50)
+    p.add_argument("--concurrency", type=int, default=16)
+    p.add_argument("--tau", type=float, default=0.1)
+    p.add_argument("--stages", default="2048,4096,8192,16384")
+    p.add_argument("--no-judge-horizon", action="store_true",
+                   help="continue every prediction to the step cap instead of the estimated end")
+    a = p.parse_args(argv)
+    plan = StagePlan(stages=tuple(int(x) for x in a.stages.split(",")), tau=a.tau,
+                     judge_horizon=not a.no_judge_horizon)
+    insts, freqs = family_instances(a.family, a.count, a.seed)
+    band = plan.band(freqs)
+    full = full_sweep(insts, freqs, a.concurrency)
+    fs11 = [r["s11"] for r in full["results"]]
+    steps_full = np.array([r["timesteps"] for r in full["results"]])
+    head = {"family": a.family, "count": a.count, "seed": a.seed, "stages": list(plan.stages),
+            "lag": plan.lag, "full_wall_s": full["wall_s"], "full_steps_mean": float(steps_full.mean()),
+            "instances_per_hour_full": a.count / full["wall_s"] * 3600.0}
+    if a.cmd == "calibrate":
+        insts, _ = family_instances(a.family, a.count, a.seed)
+        cal = calibrate(insts, freqs, plan, fs11, a.concurrency)
+        # how well the continuation end matches the plain run's own end
+        rel = np.abs(cal["end"] - steps_full[:, None]) / steps_full[:, None]
+        head["end_rel_error_median_per_stage"] = [float(np.nanmedian(rel[:, s])) if np.isfinite(rel[:, s]).any()
+                                                  else None for s in range(rel.shape[1])]
+        rows = []
+        for tau in (0.02, 0.05, 0.1, 0.2, 0.3, 0.5):
+            sim = simulate(cal, tau)
+            steps = np.where(sim["stop"] >= 0, np.array(plan.stages)[np.maximum(sim["stop"], 0)], steps_full)
+            rows.append({"tau": tau, "max_err_db": float(sim["error_db"].max()),
+                         "mean_err_db_max": float(sim["mean_error_db"].max()),
+                         "p99_err_db": float(np.percentile(sim["error_db"], 99)),
+                         "over_0.5db": int((sim["error_db"] > 0.5).sum()),
+                         "predicted": int((sim["stop"] >= 0).sum()),
+                         "steps_mean": float(steps.mean()),
+                         "step_ratio": float(steps_full.mean() / steps.mean())})
+        head["calibration"] = rows
+        print(json.dumps(head))
+        return
+    insts, _ = family_instances(a.family, a.count, a.seed)
+    st = staged_sweep(insts, freqs, plan, a.concurrency)
+    errs = np.array([0.0 if r["how"] != "predicted" else s11_db_error(r["s11"], f, band)
+                     for r, f in zip(st["results"], fs11)])
+    merrs = np.array([0.0 if r["how"] != "predicted" else s11_db_mean_error(r["s11"], f, band)
+                      for r, f in zip(st["results"], fs11)])
+    hows = [r["how"] for r in st["results"]]
+    head.update({"tau": plan.tau, "staged_wall_s": st["wall_s"], "staged_run_s": st["run_s"],
+                 "staged_check_s": st["check_s"],
+                 "instances_per_hour_staged": a.count / st["wall_s"] * 3600.0,
+                 "speedup": full["wall_s"] / st["wall_s"],
+                 "predicted": hows.count("predicted"), "decayed": hows.count("decayed"),
+                 "fallback_full": hows.count("full"),
+                 "staged_steps_mean": float(np.mean([r["steps"] for r in st["results"]])),
+                 "max_err_db": float(errs.max()), "p99_err_db": float(np.percentile(errs, 99)),
+                 "median_err_db_predicted": float(np.median(errs[errs > 0])) if (errs > 0).any() else 0.0,
+                 "over_0.5db": int((errs > 0.5).sum()), "mean_err_db_max": float(merrs.max()),
+                 "mean_over_0.5db": int((merrs > 0.5).sum())})
+    print(json.dumps(head))
+
+
+if __name__ == "__main__":
+    main()

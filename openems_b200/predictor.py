@@ -140,18 +140,30 @@ def matrix_pencil(y: np.ndarray, max_modes: int, rel_sv: float = 1e-7):
     return z, r
 
 
+def pencil_modes(x: np.ndarray, K: int, dt: float, window: int = 1536, decimate: int = 4, max_modes: int = 40):
+    """Continuous-time poles p and residues c (at sample K) of the modes the
+    matrix pencil finds in x[K - window : K] (clipped to the samples there
+    are) decimated by `decimate`: x[K + k] ~ sum c exp(p k dt)."""
+    start = max(0, K - window)
+    y = np.asarray(x[start:K:decimate], dtype=np.float64)
+    if len(y) < 8:
+        return np.zeros(0, complex), np.zeros(0, complex)
+    z, r = matrix_pencil(y, max_modes)
+    if len(z) == 0:
+        return z, r
+    p = np.log(z) / (decimate * dt)
+    return p, r * np.exp(p * (K - start) * dt)
+
+
 def pencil_tail_dft(x: np.ndarray, K: int, dt: float, freqs: np.ndarray, half: float, horizon: int = HORIZON,
                     window: int = 1536, decimate: int = 4, max_modes: int = 40) -> np.ndarray:
     """DFT of the continuation of x after sample K (to `horizon`), from the
     modes the matrix pencil finds in x[K - window : K] decimated by
     `decimate`; the engine's DFT scaling and sample times (x[k] taken after
     timestep k + 1, minus `half`)."""
-    y = np.asarray(x[K - window:K:decimate], dtype=np.float64)
-    z, r = matrix_pencil(y, max_modes)
-    if len(z) == 0:
+    p, c = pencil_modes(x, K, dt, window, decimate, max_modes)
+    if len(p) == 0:
         return np.zeros(len(freqs), complex)
-    p = np.log(z) / (decimate * dt)                      # continuous-time poles
-    c = r * np.exp(p * window * dt)                       # residues at sample K
     # the modes come in conjugate pairs: Re(sum) is the real continuation
     return tail_dft(c, p, (K + 1 - half) * dt, dt, freqs, horizon - K)
 

@@ -84,7 +84,17 @@ class Sweep:
         return iid.value
 
     def run(self, batch_steps: int = 2000):
+        """Runs every instance that has not ended to its end."""
         N.check(N.lib().oems_sweep_run(self._h, batch_steps))
+
+    def run_until(self, step_cap: int, batch_steps: int = 2000):
+        """Runs every instance that has not ended up to `step_cap` steps in
+        total; those that reach it pause and continue on the next call."""
+        N.check(N.lib().oems_sweep_run_until(self._h, batch_steps, int(step_cap)))
+
+    def finish(self, iid: int):
+        """Ends a paused instance with its partial result."""
+        N.check(N.lib().oems_sweep_finish(self._h, iid))
 
     def result(self, iid: int) -> dict:
         info = N.SweepResultC()
@@ -96,7 +106,8 @@ class Sweep:
         return {"timesteps": int(info.timesteps), "termination_reason": int(info.termination_reason),
                 "final_decay_db": float(info.final_decay_db), "device_seconds": float(info.device_seconds),
                 "cells": float(info.cells), "setup_seconds": float(info.setup_seconds),
-                "host_seconds": float(info.host_seconds), "uf": uf, "if": if_, "s11": s11}
+                "host_seconds": float(info.host_seconds), "paused": bool(info.paused),
+                "uf": uf, "if": if_, "s11": s11}
 
     def set_trace_steps(self, steps: int):
         """Record the port u / i traces of the first `steps` timesteps."""

@@ -99,3 +99,35 @@ def test_sweep_instance_matches_oracle():
     for d, key in zip(ids, ("uf", "if")):
         ref = s.probe_dft(d)
         assert np.abs(r[key] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_paused_instances_continue_bit_for_bit():
+    """run_until stops every instance at the cap and keeps its engine; the
+    continued runs equal uninterrupted ones, the paused results equal runs
+    capped at the same step count, and finish() ends an instance there."""
+    _, full = run_sweep(2)
+    sw = Sweep(FREQS, concurrency=2)
+    sw.set_trace_steps(1500)
+    ids = [sw.add(i) for i in instances()]
+    sw.run_until(1000, batch_steps=700)
+    part = [sw.result(i) for i in ids]
+    for r in part:
+        assert r["paused"] and r["timesteps"] == 1000
+    # the same instances run to 1000 steps only
+    capped = Sweep(FREQS, concurrency=2)
+    cids = [capped.add(W.patch_sweep_instance(s, delta=0.5e-3, decay_db=0.0, max_steps=1000, fmax=12e9))
+            for s in mini_specs()]
+    capped.run(batch_steps=700)
+    for p, c in zip(part, (capped.result(i) for i in cids)):
+        assert not c["paused"]
+        assert np.array_equal(p["uf"], c["uf"]) and np.array_equal(p["if"], c["if"])
+    sw.finish(ids[0])
+    sw.run_until(1600, batch_steps=700)
+    assert sw.result(ids[0])["timesteps"] == 1000 and not sw.result(ids[0])["paused"]
+    assert all(sw.result(i)["timesteps"] == 1600 for i in ids[1:])
+    sw.run(batch_steps=700)
+    for i, f in zip(ids[1:], full[1:]):
+        r = sw.result(i)
+        assert not r["paused"] and r["timesteps"] == f["timesteps"]
+        assert np.array_equal(r["uf"], f["uf"]) and np.array_equal(r["if"], f["if"])
+        assert sw.trace(i).shape == (1500, 2)

@@ -101,3 +101,56 @@ def test_family_specs_seeded_and_in_range():
         assert s.y0 >= margin - 1 and s.y0 + s.L <= s.dims[1] - margin + 1
         assert s.x0 <= s.fx < s.x0 + s.W and s.y0 <= s.fy < s.y0 + s.L
         assert s.k_patch + 1 < s.dims[2] - s.layers
+
+
+def test_s11_db_error_clips_at_floor():
+    from openems_b200 import early_stop as E
+    a = np.array([1e-3, 0.5, 0.9])
+    b = np.array([1e-4, 0.5 * 10 ** (0.2 / 20), 0.9])
+    band = np.array([True, True, True])
+    # -60 dB vs -80 dB both clip at -30 dB: no error there
+    assert E.s11_db_error(a, b, band) == pytest.approx(0.2, rel=1e-9)
+    assert E.s11_db_error(a, b, np.array([True, False, True])) == 0.0
+
+
+@pytest.mark.parametrize("lag", [0, 256])
+def test_pencil_s11_of_known_ringdown(lag):
+    """Port traces made of damped sinusoids: the prediction at K (from the
+    window ending at K - lag) equals the S11 of the whole traces."""
+    from openems_b200 import early_stop as E
+    K, H = 2048, 12000
+    u = damped(H, MODES)
+    i = 0.02 * damped(H, [(1.0, 2.0e8, 2 * np.pi * 3.1e9, 0.7), (0.3, 6.0e8, 2 * np.pi * 7.7e9, 0.1)])
+    tr = np.stack([u, i], 1)
+    uf, if_ = P.head_dft(u[:K], 1, DT, FREQS, 0.0), P.head_dft(i[:K], 1, DT, FREQS, 0.5)
+    full = P.s11(P.head_dft(u, 1, DT, FREQS, 0.0), P.head_dft(i, 1, DT, FREQS, 0.5))
+    got = E.pencil_s11(tr, uf, if_, K, DT, FREQS, H, lag)
+    assert E.s11_db_error(got, full, FREQS >= 0.5e9) < 1e-6
+
+
+def test_staged_rule_on_calibration_records():
+    from openems_b200 import early_stop as E
+    nan = np.nan
+    cal = {"check_db": np.array([[0.5, 0.05, 0.01], [0.01, 0.2, 0.3], [nan, nan, nan], [0.4, nan, nan],
+                                 [0.3, 0.3, 0.3]]),
+           "error_db": np.array([[2.0, 0.3, 0.1], [0.04, 0.5, 0.6], [nan, nan, nan], [1.0, nan, nan],
+                                 [1.0, 1.0, 1.0]])}
+    sim = E.simulate(cal, 0.1)
+    assert list(sim["stop"]) == [1, 0, -1, -1, -1]
+    assert np.allclose(sim["error_db"], [0.3, 0.04, 0.0, 0.0, 0.0])
+
+
+def test_judge_end_of_single_mode_decay():
+    """One mode decaying at alpha: the plain run's energy falls 50 dB below
+    its peak at ln(1e5) / (2 alpha); the estimate lands on the next 100-step
+    check after that."""
+    from openems_b200 import early_stop as E
+    K, H, alpha = 2048, 40000, 2e8
+    u = damped(K, [(1.0, alpha, 2 * np.pi * 3e9, 0.0)])
+    level = 10 * np.log10(np.exp(-2 * alpha * K * DT))
+    end = E.judge_end(u, K, level, DT, 50.0, H, **E.StagePlan().pencil(K))
+    want = np.log(1e5) / (2 * alpha) / DT
+    assert want <= end < want + 100
+    # already decayed: the end is now; a cap that comes first wins
+    assert E.judge_end(u, K, -60.0, DT, 50.0, H, **E.StagePlan().pencil(K)) == K
+    assert E.judge_end(u, K, level, DT, 50.0, 20000, **E.StagePlan().pencil(K)) == 20000

@@ -57,3 +57,7 @@ def test_sweep_argument_checks():
         sw.result(0)  # not run yet
     with pytest.raises(oe.ConfigError):
         sw.result(5)
+    with pytest.raises(oe.ConfigError):
+        sw.finish(0)  # not started
+    with pytest.raises(oe.ConfigError):
+        sw.finish(-1)
