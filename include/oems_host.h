@@ -227,6 +227,12 @@ OEMS_API oems_status oems_sweep_run(oems_sweep* sweep, uint64_t batch_steps);
  * bit-for-bit as if uninterrupted.  Results of a paused instance hold the
  * DFTs and S11 of the steps run so far. */
 OEMS_API oems_status oems_sweep_run_until(oems_sweep* sweep, uint64_t batch_steps, uint64_t step_cap);
+/* One instance only, on the calling thread: starts or continues it until it
+ * ends or has run step_cap steps in total.  Different instances may be
+ * advanced from different threads at the same time (one thread per instance
+ * at a time); no call may run concurrently with oems_sweep_run(_until). */
+OEMS_API oems_status oems_sweep_advance(oems_sweep* sweep, int32_t instance_id, uint64_t batch_steps,
+                                        uint64_t step_cap);
 /* Ends a paused instance (its engine is released); its result stays the
  * partial one.  No-op for an instance that has ended. */
 OEMS_API oems_status oems_sweep_finish(oems_sweep* sweep, int32_t instance_id);

@@ -255,6 +255,7 @@ SIGNATURES = {
     "oems_sweep_set_trace_steps": (c_i32, [P, c_u64]),
     "oems_sweep_run_until": (c_i32, [P, c_u64, c_u64]),
     "oems_sweep_finish": (c_i32, [P, c_i32]),
+    "oems_sweep_advance": (c_i32, [P, c_i32, c_u64, c_u64]),
     "oems_tc_gemm_bf16": (c_i32, [P, c_i32, P, c_i32, P, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, P, P]),
     "oems_tc_check": (c_i32, [P]),
     "oems_pk_f32_to_bf16": (c_i32, [P, P, c_i64, P]),

@@ -296,6 +296,22 @@ oems_status oems_sweep_run(oems_sweep* s, uint64_t batch_steps) {
   return oems_sweep_run_until(s, batch_steps, UINT64_MAX);
 }
 
+oems_status oems_sweep_advance(oems_sweep* s, int32_t id, uint64_t batch_steps, uint64_t step_cap) {
+  if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
+  if (id < 0 || id >= (int32_t)s->inst.size()) return sfail(OEMS_ERR_CONFIG, "unknown sweep instance");
+  Instance& I = *s->inst[id];
+  if (I.done) return OEMS_OK;
+  const auto t_inst = std::chrono::steady_clock::now();
+  const oems_status st = run_instance(s, I, batch_steps ? batch_steps : 2000, step_cap);
+  I.res.status = st;
+  if (st != OEMS_OK) {
+    I.error = oems_last_error_message();
+    end_instance(I);
+  }
+  I.res.host_seconds += seconds_since(t_inst);
+  return st;
+}
+
 oems_status oems_sweep_finish(oems_sweep* s, int32_t id) {
   if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
   if (id < 0 || id >= (int32_t)s->inst.size()) return sfail(OEMS_ERR_CONFIG, "unknown sweep instance");

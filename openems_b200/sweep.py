@@ -92,6 +92,11 @@ class Sweep:
         total; those that reach it pause and continue on the next call."""
         N.check(N.lib().oems_sweep_run_until(self._h, batch_steps, int(step_cap)))
 
+    def advance(self, iid: int, step_cap: int, batch_steps: int = 2000):
+        """One instance, on the calling thread, up to `step_cap` steps in
+        total (instances may be advanced from several threads at once)."""
+        N.check(N.lib().oems_sweep_advance(self._h, iid, batch_steps, int(step_cap)))
+
     def finish(self, iid: int):
         """Ends a paused instance with its partial result."""
         N.check(N.lib().oems_sweep_finish(self._h, iid))

@@ -1,5 +1,8 @@
 """Tensor-core BF16 GEMM (tcgen05) and the network kernels against plain
-PyTorch fp32/fp64 references of the same ops."""
+PyTorch fp32/fp64 references of the same ops and the CPU restatement of the
+network (oracle/tailnet_ref.py); training on the kernels against truncation
+on a synthetic ringdown family."""
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -178,3 +181,80 @@ def test_training_reduces_loss():
     losses = [net.train_step(x, y) for _ in range(120)]
     N.check(N.lib().oems_tc_check(None))
     assert losses[-1] < 0.5 * losses[0], (losses[0], losses[-1])
+
+
+@pytest.mark.parametrize("rounded,fwd_tol,grad_tol", [(True, 1e-5, 1e-2), (False, 3e-2, 0.15)])
+def test_network_matches_cpu_oracle(rounded, fwd_tol, grad_tol):
+    """Forward output and every weight and bias gradient of the tensor-core
+    network against the float64 CPU restatement (with bf16 rounding of the
+    GEMM operands: agreement to f32 accumulation; without: the bf16 error)."""
+    from oracle.tailnet_ref import TailNetRef
+    from openems_b200 import predictor as P
+    from openems_b200.predictor_net import NetConfig, TailNet
+    cfg = NetConfig(K=512, channels=(16, 32, 32), hidden=64, modes=64, batch=16)
+    net = TailNet(cfg, P.FREQS[:61], horizon=4000)
+    g = torch.Generator(device="cpu").manual_seed(4)
+    x = torch.randn(16, 512, 2, generator=g).cuda()
+    out = net.forward(x)
+    ref = TailNetRef.from_net(net)
+    ro = ref.forward(x.cpu().numpy(), bf16=rounded)
+    rel = np.abs(out.cpu().numpy() - ro).max() / np.abs(ro).max()
+    assert rel < fwd_tol, rel
+    dout = (2 * out.detach() / out.numel()).contiguous()
+    net.backward(dout)
+    N.check(N.lib().oems_tc_check(None))
+    grads = ref.backward(dout.cpu().numpy().astype(np.float64))
+    mine = [(c.fc.gw, c.fc.gb) for c in net.convs] + [(net.fc1.gw, net.fc1.gb), (net.fc2.gw, net.fc2.gb)]
+    for (mw, mb), (rw, rb) in zip(mine, grads):
+        for m, r in ((mw, rw), (mb, rb)):
+            rel = np.linalg.norm(m.cpu().numpy() - r) / max(np.linalg.norm(r), 1e-30)
+            assert rel < grad_tol, rel
+
+
+def _ringdowns(n, rng, net, K, dt, allowed):
+    """Port traces that are one damped sinusoid per channel on a pole of the
+    spectral layer's grid, and their exact scaled tail DFTs (the spectral
+    layer applied to the modal coefficients at K)."""
+    from openems_b200 import predictor as P
+    poles = P.PoleGrid().poles()[:net.cfg.modes]
+    m = len(poles)
+    E = np.exp(np.outer(np.arange(K) * dt, poles))
+    C = np.zeros((n, 2, m), complex)
+    for ch in range(2):
+        j = allowed[rng.integers(0, len(allowed), n)]
+        C[np.arange(n), ch, j] = rng.normal(size=n) + 1j * rng.normal(size=n)
+    x = np.einsum("km,ncm->nkc", E, C).real.astype(np.float32)
+    ck = C * np.exp(poles * K * dt)
+    coef = np.concatenate([ck[:, 0].real, ck[:, 0].imag, ck[:, 1].real, ck[:, 1].imag], 1)
+    y = coef @ net.spec.w.cpu().numpy().astype(np.float64).T
+    return torch.tensor(x).cuda(), torch.tensor(y, dtype=torch.float32).cuda()
+
+
+def test_trained_network_beats_truncation_on_synthetic_ringdowns():
+    """What training on the tensor-core kernels gains over stopping at K
+    without a prediction (a zero tail, relative error 1): on ringdowns whose
+    modes the first K steps resolve (>= 4 GHz, two periods or more in K), the
+    trained network predicts the tail DFT to well under half that error."""
+    from openems_b200 import predictor as P
+    from openems_b200.predictor_net import NetConfig, TailNet
+    K = 512
+    cfg = NetConfig(K=K, channels=(16, 32, 32), hidden=256, modes=64, batch=64, lr=1e-3)
+    net = TailNet(cfg, P.FREQS[::4], horizon=4000)
+    dt = P.grid_dt()
+    poles = P.PoleGrid().poles()
+    allowed = np.where(np.abs(poles.imag) / (2 * np.pi) >= 4e9)[0]
+    rng = np.random.default_rng(1)
+    xt, yt = _ringdowns(512, np.random.default_rng(2), net, K, dt, allowed)
+
+    def test_error():
+        out = torch.cat([net.forward(xt[i:i + 64].contiguous()) for i in range(0, 512, 64)])
+        return ((out - yt).norm() / yt.norm()).item()
+
+    before = test_error()
+    for _ in range(1500):
+        x, y = _ringdowns(64, rng, net, K, dt, allowed)
+        net.train_step(x, y)
+    N.check(N.lib().oems_tc_check(None))
+    after = test_error()
+    print(f"tail DFT relative error: untrained {before:.3f}, trained {after:.3f}, truncation 1.000")
+    assert after < 0.5, (before, after)

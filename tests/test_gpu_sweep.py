@@ -131,3 +131,29 @@ def test_paused_instances_continue_bit_for_bit():
         assert not r["paused"] and r["timesteps"] == f["timesteps"]
         assert np.array_equal(r["uf"], f["uf"]) and np.array_equal(r["if"], f["if"])
         assert sw.trace(i).shape == (1500, 2)
+
+
+def test_advance_from_threads_matches_sweep_run():
+    """Instances advanced one by one from several threads (through stages,
+    then to their end) give the bits of the batched run."""
+    import threading
+    _, full = run_sweep(2)
+    sw = Sweep(FREQS, concurrency=2)
+    ids = [sw.add(i) for i in instances()]
+
+    def drive(mine):
+        for i in mine:
+            for cap in (700, 1400):
+                sw.advance(i, cap, batch_steps=700)
+                assert sw.result(i)["timesteps"] == cap and sw.result(i)["paused"]
+            sw.advance(i, 10 ** 9, batch_steps=700)
+
+    ts = [threading.Thread(target=drive, args=(ids[k::2],)) for k in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    for i, f in zip(ids, full):
+        r = sw.result(i)
+        assert not r["paused"] and r["timesteps"] == f["timesteps"]
+        assert np.array_equal(r["uf"], f["uf"]) and np.array_equal(r["if"], f["if"])

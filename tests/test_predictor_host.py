@@ -154,3 +154,47 @@ def test_judge_end_of_single_mode_decay():
     # already decayed: the end is now; a cap that comes first wins
     assert E.judge_end(u, K, -60.0, DT, 50.0, H, **E.StagePlan().pencil(K)) == K
     assert E.judge_end(u, K, level, DT, 50.0, 20000, **E.StagePlan().pencil(K)) == 20000
+
+
+def _small_ref(seed=0):
+    from oracle.tailnet_ref import TailNetRef
+    rng = np.random.default_rng(seed)
+    convs = [(rng.normal(0, 0.4, (4, 8 * 2)), rng.normal(0, 0.1, 4)),
+             (rng.normal(0, 0.3, (6, 8 * 4)), rng.normal(0, 0.1, 6))]
+    # T 64 -> 15 -> 2
+    fc1 = (rng.normal(0, 0.3, (10, 2 * 6)), rng.normal(0, 0.1, 10))
+    fc2 = (rng.normal(0, 0.3, (8, 10)), rng.normal(0, 0.1, 8))
+    spec = rng.normal(0, 0.5, (12, 8))
+    return TailNetRef(convs, fc1, fc2, spec), rng.normal(size=(3, 64, 2))
+
+
+def test_tailnet_oracle_gradients_match_finite_differences():
+    """Pins the CPU restatement of the network: its hand-written backward
+    equals central differences of its forward (float64, no bf16)."""
+    net, x = _small_ref()
+    G = np.random.default_rng(9).normal(size=(3, 12))
+    net.forward(x)
+    grads = net.backward(G)
+    params = [p for c in net.convs for p in c] + list(net.fc1) + list(net.fc2)
+    flat = [g for pair in grads for g in pair]
+    rng = np.random.default_rng(10)
+    for p, g in zip(params, flat):
+        for _ in range(4):
+            idx = tuple(rng.integers(0, n) for n in p.shape)
+            old = p[idx]
+            p[idx] = old + 1e-6
+            up = (net.forward(x) * G).sum()
+            p[idx] = old - 1e-6
+            dn = (net.forward(x) * G).sum()
+            p[idx] = old
+            assert g[idx] == pytest.approx((up - dn) / 2e-6, rel=1e-5, abs=1e-8)
+
+
+def test_tailnet_oracle_im2col_adjoint_and_bf16_rounding():
+    from oracle.tailnet_ref import col2im, im2col, round_bf16
+    rng = np.random.default_rng(1)
+    x, d = rng.normal(size=(2, 37, 3)), rng.normal(size=(2 * 8, 8 * 3))
+    assert np.isclose((im2col(x, 8, 4) * d).sum(), (x * col2im(d, 2, 37, 3, 8, 4)).sum(), rtol=1e-12)
+    # round to nearest even on the 16 dropped bits
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, -2.5], dtype=np.float64)
+    assert list(round_bf16(v)) == [1.0, 1.0, 1.0 + 2 ** -6, 1.0, -2.5]
