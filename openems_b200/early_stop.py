@@ -1,9 +1,10 @@
 """Staged early termination of port sweeps.
 
 Every instance of a sweep runs to the first stage (K steps) and pauses
-(oems_sweep_run_until keeps its engine).  Its S11 is then predicted from the
+(oems_sweep_advance keeps its engine).  Its S11 is then predicted from the
 engine's port DFTs of the K simulated steps plus the matrix-pencil
-continuation of the last window of the port traces (predictor.py).  The
+continuation of the last window of the port traces (predictor.py), summed up
+to the step where the plain run is estimated to stop (judge_end).  The
 residual check repeats the prediction from a window that ends `lag` steps
 earlier: when the two predicted S11 curves agree to within `tau` dB over the
 band (both clipped at -30 dB), the prediction is accepted and the instance

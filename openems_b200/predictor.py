@@ -1,16 +1,17 @@
-"""Learned early termination of port sweeps.
+"""Early termination of port sweeps: the tail of a run stopped at K steps.
 
-A run is stopped after K timesteps; a network maps the normalised port
-voltage / current of those K steps to the remaining trace, written as 64
-damped sinusoids on a fixed pole grid, whose DFT is added in closed form to
-the DFT of the K simulated steps to give S11.
+A run is stopped after K timesteps and the rest of its port voltage /
+current is predicted as damped sinusoids, whose DFT is added in closed form
+to the DFT of the K simulated steps to give S11.  Two predictors use this
+module: the learned network (predictor_net.py; modal coefficients on a fixed
+pole grid, trained on the engine library's BF16 tensor-core kernels) and the
+matrix pencil (Hua & Sarkar), which finds the modes of the last window of
+the trace itself and drives the staged early stop (early_stop.py).
 
-This module holds the data side: the seeded patch family the network is
-trained on (the patch-antenna sweep family at a reduced size, n ~ U{40..80}
-cells of 0.5 mm), the runs that produce training traces, the pole grid and
-the least-squares fit of a trace tail onto it, and the closed-form DFT of a
-tail.  The network's forward and backward passes run in the engine library's
-BF16 tensor-core kernels (see predictor_net.py).
+Here: the seeded patch family the network is trained on (the patch-antenna
+sweep family at a reduced size, n ~ U{40..80} cells of 0.5 mm), the runs
+that produce training traces, the pole grid and the least-squares fit of a
+trace tail onto it, the closed-form DFT of a tail and the matrix pencil.
 """
 from __future__ import annotations
 
