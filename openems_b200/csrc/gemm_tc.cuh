@@ -4,15 +4,17 @@
 //
 // A and B are bf16, K-major (row-major with the reduction along the row),
 // row pitches multiples of 8 elements, K a multiple of 8; M and N are free.
-// One CTA computes a 128 x BN tile: four warps stage 128 x 64 (A) and
-// BN x 64 (B) blocks of K into shared memory in the 128-byte swizzled
-// K-major layout (8-row atoms of 1024 bytes, the 16-byte chunk j of row r
-// at chunk j ^ (r mod 8)), one thread issues four tcgen05.mma (K = 16 each)
-// per block with the accumulator in tensor memory, tcgen05.commit signals an
-// mbarrier, and after the last block each warp reads its 32 accumulator
-// lanes with tcgen05.ld.  Every mbarrier wait is bounded: on timeout the CTA
-// sets the error word, skips its remaining work, releases its tensor memory
-// and returns.
+// One CTA computes a 128 x BN tile.  Blocks of 64 along K go through a ring
+// of kStages shared-memory stages in the 128-byte swizzled K-major layout
+// (8-row atoms of 1024 bytes, the 16-byte chunk j of row r at chunk
+// j ^ (r mod 8)): all 128 threads fill a stage with 16-byte cp.async copies
+// (zero-filled past the matrix edge) kStages - 1 blocks ahead, one thread
+// issues the four tcgen05.mma (K = 16 each) of a block with the accumulator
+// in tensor memory and commits them to the stage's mbarrier, and a stage is
+// refilled only after that mbarrier says its MMAs are done.  After the last
+// block each warp reads its 32 accumulator lanes with tcgen05.ld.  Every
+// mbarrier wait is bounded: on timeout the CTA sets the error word, skips its
+// remaining work, releases its tensor memory and returns.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -90,19 +92,26 @@ struct GemmArgs {
   int* err;
 };
 
+constexpr int kGemmStages = 4;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool in_range) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in_range ? 16 : 0)
+               : "memory");
+}
+
 template <int BN>
 __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
   static_assert(BN == 64 || BN == 128, "BN");
-  constexpr int BM = 128, BK = 64;
+  constexpr int BM = 128, BK = 64, S = kGemmStages;
+  constexpr int kStageA = BM * 128, kStageB = BN * 128, kStage = kStageA + kStageB;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 1024-byte aligned operand tiles
+  // 1024-byte aligned operand stages, then the mbarriers and the TMEM slot
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* sa = base;                 // BM x 128 bytes
-  uint8_t* sb = base + BM * 128;      // BN x 128 bytes
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sb + BN * 128);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + S * kStage);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + S);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const uint32_t sbase = tc::smem_u32(base);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
@@ -111,7 +120,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    tc::mbar_init(bar, 1);
+    for (int st = 0; st < S; ++st) tc::mbar_init(bar + st, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -119,32 +128,44 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
-
   const int nkb = (p.K + BK - 1) / BK;
+
+  // copies of K-block kb into its stage: chunk j of row r at
+  // (r / 8) * 1024 + (r % 8) * 128 + ((j ^ (r % 8)) * 16); one commit group
+  // per block (empty past the last block, so group counting stays uniform)
+  auto load_block = [&](int kb) {
+    if (kb < nkb) {
+      const int k0 = kb * BK;
+      const uint32_t sa = sbase + (kb % S) * kStage, sb = sa + kStageA;
+      for (int q = tid; q < BM * 8; q += 128) {
+        const int r = q >> 3, j = q & 7;
+        const int gm = m0 + r, gk = k0 + j * 8;
+        const bool in = gm < p.M && gk < p.K;
+        cp_async16(sa + (r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4),
+                   in ? (const void*)(p.a + (size_t)gm * p.lda + gk) : (const void*)p.a, in);
+      }
+      for (int q = tid; q < BN * 8; q += 128) {
+        const int r = q >> 3, j = q & 7;
+        const int gn = n0 + r, gk = k0 + j * 8;
+        const bool in = gn < p.N && gk < p.K;
+        cp_async16(sb + (r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4),
+                   in ? (const void*)(p.b + (size_t)gn * p.ldb + gk) : (const void*)p.b, in);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  for (int kb = 0; kb < S - 1; ++kb) load_block(kb);
   bool ok = true;
   for (int kb = 0; kb < nkb && ok; ++kb) {
-    const int k0 = kb * BK;
-    // stage A and B: 16-byte chunks, chunk j of row r at (r / 8) * 1024 + (r % 8) * 128 + ((j ^ (r % 8)) * 16)
-    for (int q = tid; q < BM * 8; q += 128) {
-      const int r = q >> 3, j = q & 7;
-      const int gm = m0 + r, gk = k0 + j * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (gm < p.M && gk < p.K) v = *reinterpret_cast<const uint4*>(p.a + (size_t)gm * p.lda + gk);
-      *reinterpret_cast<uint4*>(sa + (r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4)) = v;
-    }
-    for (int q = tid; q < BN * 8; q += 128) {
-      const int r = q >> 3, j = q & 7;
-      const int gn = n0 + r, gk = k0 + j * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (gn < p.N && gk < p.K) v = *reinterpret_cast<const uint4*>(p.b + (size_t)gn * p.ldb + gk);
-      *reinterpret_cast<uint4*>(sb + (r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4)) = v;
-    }
-    // generic-proxy stores -> visible to the tensor cores (async proxy)
+    // block kb has landed (at most S - 2 younger groups in flight); its
+    // generic-proxy writes are made visible to the tensor cores
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a_addr = tc::smem_u32(sa), b_addr = tc::smem_u32(sb);
+      const uint32_t a_addr = sbase + (kb % S) * kStage, b_addr = a_addr + kStageA;
 #pragma unroll
       for (int k = 0; k < BK / 16; ++k) {
         // K = 16 bf16 = 32 bytes further along the swizzled row
@@ -159,15 +180,22 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       tc::smem_u32(bar))
+                       tc::smem_u32(bar + kb % S))
                    : "memory");
     }
-    // the MMAs of this block must finish before the next block overwrites the
-    // operand tiles; a block-wide vote keeps every thread on the same
-    // iteration count
-    ok = __syncthreads_and(tc::mbar_wait(bar, (uint32_t)(kb & 1), p.err)) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // the stage of block kb - 1 is refilled with block kb + S - 1 once that
+    // block's MMAs are done; a block-wide vote keeps every thread on the
+    // same iteration count
+    bool fine = true;
+    if (kb > 0) fine = tc::mbar_wait(bar + (kb - 1) % S, (uint32_t)(((kb - 1) / S) & 1), p.err);
+    ok = __syncthreads_and(fine) != 0;
+    if (ok) load_block(kb + S - 1);
   }
+  // the last block's MMAs (and with them every earlier one) are done
+  if (ok && nkb > 0) ok = __syncthreads_and(tc::mbar_wait(bar + (nkb - 1) % S, (uint32_t)(((nkb - 1) / S) & 1),
+                                                          p.err)) != 0;
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   if (ok) {
     // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w + 31
@@ -205,7 +233,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
 
 template <int BN>
 constexpr size_t gemm_tc_smem() {
-  return 1024 + 128 * 128 + (size_t)BN * 128 + 16;
+  return 1024 + (size_t)kGemmStages * (128 * 128 + (size_t)BN * 128) + kGemmStages * 8 + 16;
 }
 
 }  // namespace oems

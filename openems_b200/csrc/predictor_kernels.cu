@@ -206,10 +206,15 @@ oems_status oems_tc_gemm_bf16(const void* a, int lda, const void* b, int ldb, fl
   p.K = K;
   p.beta = beta;
   p.err = err;
+  // the stage ring needs more than the default 48 KB of dynamic shared memory
   if (N > 64) {
+    PK_CUDA(cudaFuncSetAttribute(oems::k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)oems::gemm_tc_smem<128>()));
     const dim3 grid((N + 127) / 128, (M + 127) / 128);
     oems::k_gemm_tc<128><<<grid, 128, oems::gemm_tc_smem<128>(), S(stream)>>>(p);
   } else {
+    PK_CUDA(cudaFuncSetAttribute(oems::k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)oems::gemm_tc_smem<64>()));
     const dim3 grid((N + 63) / 64, (M + 127) / 128);
     oems::k_gemm_tc<64><<<grid, 128, oems::gemm_tc_smem<64>(), S(stream)>>>(p);
   }
