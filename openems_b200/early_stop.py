@@ -104,6 +104,7 @@ class StagePlan:
     samples: int = 384
     max_modes: int = 40
     judge_horizon: bool = True
+    check: str = "max"  # residual statistic over the band: "max" or "mean" |dB difference|
 
     def band(self, freqs: np.ndarray) -> np.ndarray:
         return np.asarray(freqs) >= self.fmin
@@ -113,15 +114,20 @@ class StagePlan:
         return dict(window=window, decimate=max(1, window // self.samples), max_modes=self.max_modes)
 
 
-def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan):
-    """(prediction at K, residual-check value in dB, continuation end step)."""
+def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, both: bool = False):
+    """(prediction at K, residual-check value in dB, continuation end step);
+    with both=True the check value is the pair (max, mean) over the band."""
     pen = plan.pencil(K)
     end = judge_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, **pen) \
         if plan.judge_horizon else horizon
     end = max(end, K)
     a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, **pen)
     b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
-    return a, s11_db_error(a, b, plan.band(freqs)), end
+    band = plan.band(freqs)
+    if both:
+        return a, (s11_db_error(a, b, band), s11_db_mean_error(a, b, band)), end
+    stat = s11_db_mean_error if plan.check == "mean" else s11_db_error
+    return a, stat(a, b, band), end
 
 
 def _pool():
@@ -228,6 +234,7 @@ def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.n
     e = np.full((n, ns), np.nan)
     end = np.full((n, ns), np.nan)
     em = np.full((n, ns), np.nan)
+    dm = np.full((n, ns), np.nan)
     from threadpoolctl import threadpool_limits
     with _pool() as pool, threadpool_limits(1):
         for s, K in enumerate(plan.stages):
@@ -236,20 +243,22 @@ def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.n
             for k, i in enumerate(ids):
                 r = sw.result(i)
                 if r["paused"]:
-                    jobs[k] = pool.submit(check_instance, sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan)
+                    jobs[k] = pool.submit(check_instance, sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan,
+                                          True)
             for k, j in jobs.items():
-                pred, d[k, s], end[k, s] = j.result()
+                pred, (d[k, s], dm[k, s]), end[k, s] = j.result()
                 e[k, s] = s11_db_error(pred, full_s11[k], band)
                 em[k, s] = s11_db_mean_error(pred, full_s11[k], band)
     sw.close()
-    return {"check_db": d, "error_db": e, "mean_error_db": em, "end": end}
+    return {"check_db": d, "check_mean_db": dm, "error_db": e, "mean_error_db": em, "end": end}
 
 
-def simulate(cal: dict, tau: float) -> dict:
+def simulate(cal: dict, tau: float, check: str = "max") -> dict:
     """Outcome of the staged rule with threshold tau on calibration records:
     per instance the stage index it stops at (-1: decayed or full run) and
     its S11 error (0 for exact)."""
-    d, e = cal["check_db"], cal["error_db"]
+    d = cal["check_mean_db"] if check == "mean" else cal["check_db"]
+    e = cal["error_db"]
     em = cal.get("mean_error_db", e)
     stop = np.full(len(d), -1)
     err = np.zeros(len(d))
@@ -295,9 +304,12 @@ def main(argv=None):
     p.add_argument("--stages", default="2048,4096,8192,16384")
     p.add_argument("--no-judge-horizon", action="store_true",
                    help="continue every prediction to the step cap instead of the estimated end")
+    p.add_argument("--check", choices=["max", "mean"], default="max",
+                   help="residual statistic over the band (run)")
+    p.add_argument("--save", default=None, help="calibrate: write the per-instance records to this .npz")
     a = p.parse_args(argv)
     plan = StagePlan(stages=tuple(int(x) for x in a.stages.split(",")), tau=a.tau,
-                     judge_horizon=not a.no_judge_horizon)
+                     judge_horizon=not a.no_judge_horizon, check=a.check)
     insts, freqs = family_instances(a.family, a.count, a.seed)
     band = plan.band(freqs)
     full = full_sweep(insts, freqs, a.concurrency)
@@ -313,11 +325,14 @@ def main(argv=None):
         rel = np.abs(cal["end"] - steps_full[:, None]) / steps_full[:, None]
         head["end_rel_error_median_per_stage"] = [float(np.nanmedian(rel[:, s])) if np.isfinite(rel[:, s]).any()
                                                   else None for s in range(rel.shape[1])]
+        if a.save:
+            np.savez(a.save, steps_full=steps_full, stages=np.array(plan.stages), **cal)
         rows = []
-        for tau in (0.02, 0.05, 0.1, 0.2, 0.3, 0.5):
-            sim = simulate(cal, tau)
+        for check, tau in [("max", t) for t in (0.02, 0.05, 0.1, 0.2, 0.3, 0.5)] + \
+                          [("mean", t) for t in (0.01, 0.02, 0.05, 0.1, 0.2)]:
+            sim = simulate(cal, tau, check)
             steps = np.where(sim["stop"] >= 0, np.array(plan.stages)[np.maximum(sim["stop"], 0)], steps_full)
-            rows.append({"tau": tau, "max_err_db": float(sim["error_db"].max()),
+            rows.append({"check": check, "tau": tau, "max_err_db": float(sim["error_db"].max()),
                          "mean_err_db_max": float(sim["mean_error_db"].max()),
                          "p99_err_db": float(np.percentile(sim["error_db"], 99)),
                          "over_0.5db": int((sim["error_db"] > 0.5).sum()),
@@ -334,7 +349,7 @@ def main(argv=None):
     merrs = np.array([0.0 if r["how"] != "predicted" else s11_db_mean_error(r["s11"], f, band)
                       for r, f in zip(st["results"], fs11)])
     hows = [r["how"] for r in st["results"]]
-    head.update({"tau": plan.tau, "staged_wall_s": st["wall_s"], "staged_check_s_all_threads": st["check_s"],
+    head.update({"check": plan.check, "tau": plan.tau, "staged_wall_s": st["wall_s"], "staged_check_s_all_threads": st["check_s"],
                  "instances_per_hour_staged": a.count / st["wall_s"] * 3600.0,
                  "speedup": full["wall_s"] / st["wall_s"],
                  "predicted": hows.count("predicted"), "decayed": hows.count("decayed"),
