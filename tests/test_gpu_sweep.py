@@ -157,3 +157,23 @@ def test_advance_from_threads_matches_sweep_run():
         r = sw.result(i)
         assert not r["paused"] and r["timesteps"] == f["timesteps"]
         assert np.array_equal(r["uf"], f["uf"]) and np.array_equal(r["if"], f["if"])
+
+
+@pytest.mark.parametrize("check,tau", [("mean", 0.15), ("max", 0.05)])
+def test_staged_early_stop_against_full_runs(check, tau):
+    """The staged early stop on the small patches: a predicted instance stops
+    at a stage with its S11 within 0.5 dB of the full run's (mean over the
+    band, clipped at -30 dB); a decayed or fallback instance carries the full
+    run's bits."""
+    from openems_b200 import early_stop as E
+    full = E.full_sweep(instances(), FREQS, concurrency=2, batch_steps=700)
+    plan = E.StagePlan(stages=(1024, 2048, 4096), check=check, tau=tau)
+    st = E.staged_sweep(instances(), FREQS, plan, concurrency=2, batch_steps=700)
+    band = plan.band(FREQS)
+    for r, f in zip(st["results"], full["results"]):
+        if r["how"] == "predicted":
+            assert r["steps"] in plan.stages and r["steps"] < f["timesteps"]
+            assert E.s11_db_mean_error(r["s11"], f["s11"], band) < 0.5
+        else:
+            assert r["steps"] == f["timesteps"]
+            assert np.array_equal(r["s11"], f["s11"])
