@@ -4,13 +4,13 @@ Every instance of a sweep runs to the first stage (K steps) and pauses
 (oems_sweep_advance keeps its engine).  Its S11 is then predicted from the
 engine's port DFTs of the K simulated steps plus the matrix-pencil
 continuation of the last window of the port traces (predictor.py), summed up
-to the step where the plain run is estimated to stop (judge_end).  The
+to the step where the plain run is estimated to stop (plain_end).  The
 residual check repeats the prediction from a window that ends `lag` steps
 earlier: when the two predicted S11 curves agree to within `tau` dB over the
 band (both clipped at -30 dB), the prediction is accepted and the instance
 ends there.  Otherwise the instance continues to the next stage, and after the
 last stage runs on to the plain end condition (-50 dB energy decay), whose
-S11 is exact: the full run is the fallback and the judge of the error.
+S11 is exact: the full run is the fallback and the reference for the error.
 Instances that decay before a stage are exact as well.
 
 `calibrate` records the check and the prediction error of every instance at
@@ -64,7 +64,7 @@ def pencil_s11(trace: np.ndarray, uf: np.ndarray, if_: np.ndarray, K: int, dt: f
     return P.s11(uh + ut, ih + it, R)
 
 
-def judge_end(u: np.ndarray, K: int, level_db: float, dt: float, decay_db: float, cap: int,
+def plain_end(u: np.ndarray, K: int, level_db: float, dt: float, decay_db: float, cap: int,
               **pencil) -> int:
     """Step at which the plain run would stop: its field energy, now
     `level_db` below the peak, is continued with the pencil modes of the port
@@ -103,7 +103,7 @@ class StagePlan:
     max_window: int = 12288
     samples: int = 384
     max_modes: int = 40
-    judge_horizon: bool = True
+    end_estimate: bool = True
     check: str = "max"  # residual statistic over the band: "max" or "mean" |dB difference|
 
     def band(self, freqs: np.ndarray) -> np.ndarray:
@@ -118,8 +118,8 @@ def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, b
     """(prediction at K, residual-check value in dB, continuation end step);
     with both=True the check value is the pair (max, mean) over the band."""
     pen = plan.pencil(K)
-    end = judge_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, **pen) \
-        if plan.judge_horizon else horizon
+    end = plain_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, **pen) \
+        if plan.end_estimate else horizon
     end = max(end, K)
     a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, **pen)
     b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
@@ -302,14 +302,14 @@ def main(argv=None):
     p.add_argument("--concurrency", type=int, default=16)
     p.add_argument("--tau", type=float, default=0.1)
     p.add_argument("--stages", default="2048,4096,8192,16384")
-    p.add_argument("--no-judge-horizon", action="store_true",
+    p.add_argument("--no-end-estimate", action="store_true",
                    help="continue every prediction to the step cap instead of the estimated end")
     p.add_argument("--check", choices=["max", "mean"], default="max",
                    help="residual statistic over the band (run)")
     p.add_argument("--save", default=None, help="calibrate: write the per-instance records to this .npz")
     a = p.parse_args(argv)
     plan = StagePlan(stages=tuple(int(x) for x in a.stages.split(",")), tau=a.tau,
-                     judge_horizon=not a.no_judge_horizon, check=a.check)
+                     end_estimate=not a.no_end_estimate, check=a.check)
     insts, freqs = family_instances(a.family, a.count, a.seed)
     band = plan.band(freqs)
     full = full_sweep(insts, freqs, a.concurrency)

@@ -140,7 +140,7 @@ def test_staged_rule_on_calibration_records():
     assert np.allclose(sim["error_db"], [0.3, 0.04, 0.0, 0.0, 0.0])
 
 
-def test_judge_end_of_single_mode_decay():
+def test_plain_end_of_single_mode_decay():
     """One mode decaying at alpha: the plain run's energy falls 50 dB below
     its peak at ln(1e5) / (2 alpha); the estimate lands on the next 100-step
     check after that."""
@@ -148,12 +148,12 @@ def test_judge_end_of_single_mode_decay():
     K, H, alpha = 2048, 40000, 2e8
     u = damped(K, [(1.0, alpha, 2 * np.pi * 3e9, 0.0)])
     level = 10 * np.log10(np.exp(-2 * alpha * K * DT))
-    end = E.judge_end(u, K, level, DT, 50.0, H, **E.StagePlan().pencil(K))
+    end = E.plain_end(u, K, level, DT, 50.0, H, **E.StagePlan().pencil(K))
     want = np.log(1e5) / (2 * alpha) / DT
     assert want <= end < want + 100
     # already decayed: the end is now; a cap that comes first wins
-    assert E.judge_end(u, K, -60.0, DT, 50.0, H, **E.StagePlan().pencil(K)) == K
-    assert E.judge_end(u, K, level, DT, 50.0, 20000, **E.StagePlan().pencil(K)) == 20000
+    assert E.plain_end(u, K, -60.0, DT, 50.0, H, **E.StagePlan().pencil(K)) == K
+    assert E.plain_end(u, K, level, DT, 50.0, 20000, **E.StagePlan().pencil(K)) == 20000
 
 
 def _small_ref(seed=0):
