@@ -249,6 +249,21 @@ def cpu_sample(wl, target_s=12.0, threads=None, max_steps=400):
     return {"value": wl.cells * n / el / 1e6, "steps": n, "threads": threads, "seconds": el}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mcells(world: int, cells: int, timesteps: int, seconds: float) -> float:
+    """Whole-job throughput: every rank's cells x timesteps over the slowest rank's time."""
+    return world * cells * timesteps / seconds / 1e6
+
+
 def main():
     args = parse()
     from openems_b200 import workloads
@@ -310,18 +325,12 @@ def main():
 
     d = run_device(oe, wl, args, torch, dist)
     steps_total = args.steps * args.timesteps_per_step
-    t_dev = d["device_s"]
-    if dist is not None:
-        t = torch.tensor([t_dev], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t.item())
-    value = world * wl.cells * steps_total / t_dev / 1e6
+    t_dev = max_over_ranks(d["device_s"], dist, "cuda")
+    value = job_mcells(world, wl.cells, steps_total, t_dev)
     e2e = None if args.no_e2e else run_e2e(oe, wl, args, torch)
     if dist is not None:
         if e2e is not None:
-            t = torch.tensor([e2e["wall_s"]], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e["mcells"] = world * wl.cells * steps_total / float(t.item()) / 1e6
+            e2e["mcells"] = job_mcells(world, wl.cells, steps_total, max_over_ranks(e2e["wall_s"], dist, "cuda"))
         dist.barrier()
     if rank != 0:
         if dist is not None:
