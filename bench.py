@@ -16,7 +16,8 @@ run.  Working set 1.2 GB >> 126 MB L2, so no L2 flush is needed between steps.
          upload (H2D), K batches with their sampled waveforms (H2D) and energy
          samples / probe traces (D2H), and the final read_fields (D2H).
   roofline  the H and E update kernels (each ~half the step): 60 algorithmic
-         bytes per cell per launch (120 B per cell-step), timed with CUDA
+         bytes per cell per launch (120 B per cell-step; --compressed 37,
+         --storage f16/bf16 42, both 19: see kernel_bytes), timed with CUDA
          events around every launch on the engine's stream in a profiling
          batch of the same workload run after the timed region.
   cpu_baseline  the oracle's C++ restatement of the reference's Rayon engine
@@ -45,8 +46,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_CELL_STEP = 120.0       # uncompressed FP32 Yee step (H 60 B + E 60 B)
-BYTES_PER_CELL_KERNEL = 60.0      # one half-step kernel
+def kernel_bytes(storage: str, compressed: bool) -> float:
+    """Algorithmic bytes per cell of one half-step kernel: the other field
+    read, its own field read and written (9 values of the storage type), and
+    the coefficients (Ca/Cb or Da/Db, 6 floats; compressed: a one-byte
+    material id, the table being in shared memory)."""
+    elem = 4 if storage == "f32" else 2
+    return 9 * elem + (1 if compressed else 24)
 STEPS_PER_BENCH_STEP = 1000
 METRIC = "MCells/s (Yee FDTD throughput, % of HBM roofline)"
 
@@ -60,6 +66,8 @@ def parse():
     p.add_argument("--n", type=int, default=256, help="grid edge (default 256)")
     p.add_argument("--timesteps-per-step", type=int, default=STEPS_PER_BENCH_STEP)
     p.add_argument("--compressed", action="store_true", help="material-id coefficient storage")
+    p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32",
+                   help="field storage (arithmetic stays f32; f16 / bf16 run the register kernels)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernels", choices=("auto", "register", "staged"), default="auto")
@@ -128,9 +136,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_engine(oe, wl, compressed=False, kernels="auto"):
+def build_engine(oe, wl, compressed=False, kernels="auto", storage="f32"):
     op = wl.operator()
-    eng = oe.Engine(op, compressed=compressed, kernels=kernels)
+    eng = oe.Engine(op, compressed=compressed, kernels=kernels, storage=storage)
     if wl.cpml_layers:
         eng.add_cpml(wl.cpml())
     for comp, pos in wl.probes:
@@ -148,7 +156,7 @@ def batch_for(oe, wl, dt, start, n):
 
 def run_device(oe, wl, args, torch, dist):
     """value: device-resident batches timed with CUDA events (engine stream)."""
-    op, eng = build_engine(oe, wl, args.compressed, args.kernels)
+    op, eng = build_engine(oe, wl, args.compressed, args.kernels, args.storage)
     dt = op.timestep()
     T = args.timesteps_per_step
     t = 0
@@ -186,7 +194,7 @@ def run_e2e(oe, wl, args, torch):
     """e2e: public API from host buffers, copies inside the timed region."""
     T = args.timesteps_per_step
     # warm-up on a separate engine (context, kernels, autotune cache)
-    op, eng = build_engine(oe, wl, args.compressed, args.kernels)
+    op, eng = build_engine(oe, wl, args.compressed, args.kernels, args.storage)
     dt = op.timestep()
     for w in range(max(1, args.warmup)):
         eng.run_batch(batch_for(oe, wl, dt, w * T, T))
@@ -196,7 +204,8 @@ def run_e2e(oe, wl, args, torch):
     nprobe = len(wl.probes)
     t0 = time.perf_counter()
     op = wl.operator()                       # host-side operator (12 host arrays)
-    eng = oe.Engine(op, compressed=args.compressed, kernels=args.kernels)  # H2D of the coefficients
+    eng = oe.Engine(op, compressed=args.compressed, kernels=args.kernels,
+                    storage=args.storage)  # H2D of the coefficients
     if wl.cpml_layers:
         eng.add_cpml(wl.cpml())
     for comp, pos in wl.probes:
@@ -273,6 +282,7 @@ def main():
                           "(default_rng(2)), Gaussian Ez 0-10 GHz, FP32, 10000 timesteps",
               "timesteps_per_step": args.timesteps_per_step, "cells": wl.cells,
               "coefficients": "compressed (material id + table)" if args.compressed else "full arrays",
+              "field_storage": args.storage,
               "l2": "working set 1.2 GB > 126 MB L2; no flush", "parallelism": "replicas"}
 
     rank = int(os.environ.get("RANK", "0"))
@@ -338,10 +348,11 @@ def main():
         return
     kernel_avg = max(d["h_avg_s"], d["e_avg_s"])
     dominant = "k_update_h" if d["h_avg_s"] >= d["e_avg_s"] else "k_update_e"
-    achieved = BYTES_PER_CELL_KERNEL * wl.cells / kernel_avg / 1e9
+    per_kernel = kernel_bytes(args.storage, args.compressed)
+    achieved = per_kernel * wl.cells / kernel_avg / 1e9
     traffic = None
     prof_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof_path):
+    if os.path.exists(prof_path) and args.storage == "f32" and not args.compressed:  # captured for that variant
         try:
             with open(prof_path) as f:
                 tj = json.load(f)
@@ -350,7 +361,7 @@ def main():
         except Exception:
             traffic = None
     cpu = None if args.no_cpu_baseline else cpu_sample(wl)
-    step_gbs = BYTES_PER_CELL_STEP * wl.cells * steps_total / t_dev / 1e9 / world
+    step_gbs = 2 * per_kernel * wl.cells * steps_total / t_dev / 1e9 / world
     line = {
         "metric": METRIC, "value": value, "unit": "MCells/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -360,7 +371,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic,
-                     "algorithmic_bytes_per_launch": BYTES_PER_CELL_KERNEL * wl.cells,
+                     "algorithmic_bytes_per_launch": per_kernel * wl.cells,
                      "h_kernel_ms": d["h_avg_s"] * 1e3, "e_kernel_ms": d["e_avg_s"] * 1e3},
         "gpu_launches": d["launches"],
         "clocks": d["clocks"],

@@ -81,6 +81,18 @@ typedef struct oems_engine oems_engine;
 #define OEMS_ENGINE_SPLIT_KERNELS 0x40u    /* with CPML: staged kernels on the box
                                               between the x / y slabs, register
                                               kernels on those slabs */
+/* Field storage in 2 bytes per value, arithmetic still in float (no
+ * counterpart in the reference, whose fields are f32): IEEE half or
+ * bfloat16, rounded to nearest on every store.  H is kept multiplied by
+ * OEMS_H_STORAGE_SCALE (folded into the coefficients, a power of two, so the
+ * float arithmetic is exactly the scaled one) to keep it in half's range;
+ * probes, energies and read / write_fields see unscaled values.  Register
+ * kernels only; CPML, excitations, probes and their DFTs, energies and the
+ * energy-decay end condition are supported, the other extensions are
+ * refused with OEMS_ERR_CONFIG. */
+#define OEMS_ENGINE_FIELDS_F16 0x80u
+#define OEMS_ENGINE_FIELDS_BF16 0x100u
+#define OEMS_H_STORAGE_SCALE 512.0f
 
 /* What Operator hands to EngineImpl::new: dimensions, dt, cell sizes and the
  * 12 per-cell coefficient arrays (src/fdtd/operator.rs:21-38, :145-185). */

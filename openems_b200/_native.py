@@ -26,6 +26,10 @@ ENGINE_NO_GRAPHS = 0x4
 ENGINE_REGISTER_KERNELS = 0x10
 ENGINE_STAGED_KERNELS = 0x20
 ENGINE_SPLIT_KERNELS = 0x40
+ENGINE_FIELDS_F16 = 0x80
+ENGINE_FIELDS_BF16 = 0x100
+H_STORAGE_SCALE = 512.0
+STORAGE_FLAGS = {"f32": 0, "f16": ENGINE_FIELDS_F16, "bf16": ENGINE_FIELDS_BF16}
 
 
 class OpenEMSError(Exception):

@@ -24,6 +24,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -91,8 +92,22 @@ struct PostArgs {
   double* traces;              // [batch step][probe]
   const long long* d_base;     // batch step of local step 0
   int local;
+  float h_inv;                 // 2-byte storage: 1 / the H scale
 };
 
+// One field value of component c at linear index q (H stored scaled in the
+// 2-byte storage modes: multiplied back by h_inv, a power of two).
+template <typename T>
+__device__ __forceinline__ float field_value(const PostArgs& a, int c, long long q) {
+  if constexpr (std::is_same<T, float>::value) {
+    return (c < 3 ? a.e[c] : a.h[c - 3])[q];
+  } else {
+    const float v = FieldIO<T>::ld1(c < 3 ? a.e[c] : a.h[c - 3], q);
+    return c < 3 ? v : v * a.h_inv;
+  }
+}
+
+template <typename T = float>
 __global__ void k_post_step(const PostArgs a) {
   const long long s = *a.d_base + a.local;
   if (threadIdx.x == 0) {
@@ -100,8 +115,14 @@ __global__ void k_post_step(const PostArgs a) {
       if (s >= a.exc_count[x]) continue;
       const float v = a.exc_samples[a.exc_off[x] + s];
       const int meta = a.exc_meta[x];
-      float* p = a.e[meta & 3] + a.exc_idx[x];
-      *p = (meta >> 2) ? __fadd_rn(*p, v) : v;
+      if constexpr (std::is_same<T, float>::value) {
+        float* p = a.e[meta & 3] + a.exc_idx[x];
+        *p = (meta >> 2) ? __fadd_rn(*p, v) : v;
+      } else {
+        float* b = a.e[meta & 3];
+        const float cur = FieldIO<T>::ld1(b, a.exc_idx[x]);
+        FieldIO<T>::st1(b, a.exc_idx[x], (meta >> 2) ? __fadd_rn(cur, v) : v);
+      }
     }
   }
   __syncthreads();
@@ -110,16 +131,14 @@ __global__ void k_post_step(const PostArgs a) {
     if (a.probe_mode[p] == 0) {
       float acc = 0.0f;
       for (int t = a.probe_off[p]; t < a.probe_off[p + 1]; ++t) {
-        const int c = a.term_comp[t];
-        const float v = (c < 3 ? a.e[c] : a.h[c - 3])[a.term_idx[t]];
+        const float v = field_value<T>(a, a.term_comp[t], a.term_idx[t]);
         acc = a.term_w[t] >= 0.0 ? __fadd_rn(acc, v) : __fsub_rn(acc, v);
       }
       val = (double)acc;
     } else {
       double acc = 0.0;
       for (int t = a.probe_off[p]; t < a.probe_off[p + 1]; ++t) {
-        const int c = a.term_comp[t];
-        const float v = (c < 3 ? a.e[c] : a.h[c - 3])[a.term_idx[t]];
+        const float v = field_value<T>(a, a.term_comp[t], a.term_idx[t]);
         acc = __dadd_rn(acc, __dmul_rn(a.term_w[t], (double)v));
       }
       val = acc;
@@ -176,12 +195,17 @@ struct EnergyArgs {
   double* partials;      // [6][kEnergyBlocks]
 };
 
+template <typename T = float>
 __global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyArgs a) {
   const float4* p = reinterpret_cast<const float4*>(a.arr[blockIdx.y]);
   double s = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.n4;
        t += (long long)gridDim.x * blockDim.x) {
-    const float4 v = __ldcs(p + t);
+    float4 v;
+    if constexpr (std::is_same<T, float>::value)
+      v = __ldcs(p + t);
+    else
+      v = FieldIO<T>::ldg4(a.arr[blockIdx.y], 4 * t);
     s += (double)v.x * (double)v.x + (double)v.y * (double)v.y + (double)v.z * (double)v.z +
          (double)v.w * (double)v.w;
   }
@@ -197,13 +221,15 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyA
 
 // out[0] = E energy, out[1] = H energy (each the sum over its 3 components in
 // component order, like VectorField3D::energy, src/arrays/field.rs:314-316).
-__global__ void k_energy_final(const double* partials, double* out) {
+// h_inv2: 1 / the square of the H storage scale (1 for float storage; a
+// power of two, so exact).
+__global__ void k_energy_final(const double* partials, double* out, double h_inv2) {
   __shared__ double comp[6];
   const int c = threadIdx.x;
   if (c < 6) {
     double s = 0.0;
     for (int b = 0; b < kEnergyBlocks; ++b) s += partials[c * kEnergyBlocks + b];
-    comp[c] = s;
+    comp[c] = c < 3 ? s : s * h_inv2;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -520,8 +546,15 @@ struct oems_engine {
   double last_device_seconds = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-  float* E(int c) { return fields + (size_t)c * ncells_padded; }
-  float* H(int c) { return fields + (size_t)(3 + c) * ncells_padded; }
+  // field storage: 0 float, 1 half, 2 bfloat16 (arithmetic in float); with
+  // 2-byte storage H is kept multiplied by h_scale (a power of two)
+  int storage = 0;
+  size_t elem = sizeof(float);
+  float h_scale = 1.0f;
+  float* at(size_t c) { return reinterpret_cast<float*>(reinterpret_cast<char*>(fields) + c * ncells_padded * elem); }
+  float* E(int c) { return at((size_t)c); }
+  float* H(int c) { return at((size_t)(3 + c)); }
+  size_t field_bytes() const { return 6 * (size_t)ncells_padded * elem; }
   float* C(int a) { return coeffs + (size_t)a * ncells_padded; }
 };
 
@@ -649,15 +682,27 @@ static EArgs e_args(oems_engine* en) {
 using HKernel = void (*)(HArgs);
 using EKernel = void (*)(EArgs);
 
-static HKernel pick_h(int id_bytes, bool cpml) {
-  if (id_bytes == 0) return cpml ? k_update_h<0, true> : k_update_h<0, false>;
-  if (id_bytes == 1) return cpml ? k_update_h<1, true> : k_update_h<1, false>;
-  return cpml ? k_update_h<2, true> : k_update_h<2, false>;
+template <typename T>
+static HKernel pick_h_t(int id_bytes, bool cpml) {
+  if (id_bytes == 0) return cpml ? k_update_h<0, true, T> : k_update_h<0, false, T>;
+  if (id_bytes == 1) return cpml ? k_update_h<1, true, T> : k_update_h<1, false, T>;
+  return cpml ? k_update_h<2, true, T> : k_update_h<2, false, T>;
 }
-static EKernel pick_e(int id_bytes, bool cpml) {
-  if (id_bytes == 0) return cpml ? k_update_e<0, true> : k_update_e<0, false>;
-  if (id_bytes == 1) return cpml ? k_update_e<1, true> : k_update_e<1, false>;
-  return cpml ? k_update_e<2, true> : k_update_e<2, false>;
+template <typename T>
+static EKernel pick_e_t(int id_bytes, bool cpml) {
+  if (id_bytes == 0) return cpml ? k_update_e<0, true, T> : k_update_e<0, false, T>;
+  if (id_bytes == 1) return cpml ? k_update_e<1, true, T> : k_update_e<1, false, T>;
+  return cpml ? k_update_e<2, true, T> : k_update_e<2, false, T>;
+}
+static HKernel pick_h(int id_bytes, bool cpml, int storage = 0) {
+  if (storage == 1) return pick_h_t<__half>(id_bytes, cpml);
+  if (storage == 2) return pick_h_t<__nv_bfloat16>(id_bytes, cpml);
+  return pick_h_t<float>(id_bytes, cpml);
+}
+static EKernel pick_e(int id_bytes, bool cpml, int storage = 0) {
+  if (storage == 1) return pick_e_t<__half>(id_bytes, cpml);
+  if (storage == 2) return pick_e_t<__nv_bfloat16>(id_bytes, cpml);
+  return pick_e_t<float>(id_bytes, cpml);
 }
 
 static size_t table_smem(const oems_engine* en) {
@@ -756,9 +801,9 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   const size_t smem = table_smem(en);
   int occ_h = 0, occ_e = 0;
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_h, (const void*)pick_h(en->id_bytes, en->cpml.on), s.block, smem));
+      &occ_h, (const void*)pick_h(en->id_bytes, en->cpml.on, en->storage), s.block, smem));
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_e, (const void*)pick_e(en->id_bytes, en->cpml.on), s.block, smem));
+      &occ_e, (const void*)pick_e(en->id_bytes, en->cpml.on, en->storage), s.block, smem));
   const Geom g = make_geom(en, s.block, s.ichunk);
   s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h) * sms));
   s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e) * sms));
@@ -801,7 +846,7 @@ static cudaError_t launch_h(oems_engine* en) {
     return cudaGetLastError();
   }
   HArgs a = h_args(en);
-  pick_h(en->id_bytes, en->cpml.on)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
+  pick_h(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
 }
 static cudaError_t launch_e(oems_engine* en) {
@@ -816,7 +861,7 @@ static cudaError_t launch_e(oems_engine* en) {
     return cudaGetLastError();
   }
   EArgs a = e_args(en);
-  pick_e(en->id_bytes, en->cpml.on)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
+  pick_e(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -867,7 +912,13 @@ static cudaError_t launch_post(oems_engine* en, int local) {
   a.traces = en->d_traces.p;
   a.d_base = en->d_base.p;
   a.local = local;
-  k_post_step<<<1, 128, 0, en->stream>>>(a);
+  a.h_inv = 1.0f / en->h_scale;
+  if (en->storage == 1)
+    k_post_step<__half><<<1, 128, 0, en->stream>>>(a);
+  else if (en->storage == 2)
+    k_post_step<__nv_bfloat16><<<1, 128, 0, en->stream>>>(a);
+  else
+    k_post_step<float><<<1, 128, 0, en->stream>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_fd(en, local);
@@ -1054,12 +1105,17 @@ static oems_status run_span(oems_engine* en, long long base, int steps) {
 
 static oems_status launch_energy(oems_engine* en, double* out2) {
   EnergyArgs a{};
-  for (int c = 0; c < 6; ++c) a.arr[c] = en->fields + (size_t)c * en->ncells_padded;
+  for (int c = 0; c < 6; ++c) a.arr[c] = en->at((size_t)c);
   a.n4 = en->ncells_padded / 4;
   a.partials = en->d_partials.p;
-  k_energy_partial<<<dim3(kEnergyBlocks, 6), kEnergyThreads, 0, en->stream>>>(a);
+  if (en->storage == 1)
+    k_energy_partial<__half><<<dim3(kEnergyBlocks, 6), kEnergyThreads, 0, en->stream>>>(a);
+  else if (en->storage == 2)
+    k_energy_partial<__nv_bfloat16><<<dim3(kEnergyBlocks, 6), kEnergyThreads, 0, en->stream>>>(a);
+  else
+    k_energy_partial<float><<<dim3(kEnergyBlocks, 6), kEnergyThreads, 0, en->stream>>>(a);
   OEMS_CUDA(cudaGetLastError());
-  k_energy_final<<<1, 32, 0, en->stream>>>(en->d_partials.p, out2);
+  k_energy_final<<<1, 32, 0, en->stream>>>(en->d_partials.p, out2, 1.0 / ((double)en->h_scale * en->h_scale));
   OEMS_CUDA(cudaGetLastError());
   en->last_launches += 2;
   return OEMS_OK;
@@ -1117,10 +1173,11 @@ static std::mutex& tune_mutex() {
 static oems_status autotune(oems_engine* en) {
   en->tuned = true;
   int ilo, ihi, jlo, jhi;
-  const bool can_split = en->id_bytes == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
+  const bool can_split = en->id_bytes == 0 && en->storage == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const bool only_split = (en->flags & OEMS_ENGINE_SPLIT_KERNELS) && can_split;
   const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split;
-  const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0 && !only_split;
+  const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0 && !only_split &&
+                        en->storage == 0;
   // split shapes are tried only on request: at 256^3 with 8-layer CPML the
   // staged interior plus register slabs measured 36.8 GCells/s against 45.6
   // for the register kernels on the whole grid (the z-slab lanes of every
@@ -1174,7 +1231,7 @@ static oems_status autotune(oems_engine* en) {
       return OEMS_OK;
     }
   }
-  const size_t fbytes = (size_t)6 * en->ncells_padded * sizeof(float);
+  const size_t fbytes = en->field_bytes();
   const size_t pbytes = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
   void* save = nullptr;
   OEMS_CUDA(pool_alloc(&save, fbytes + pbytes, en->stream));
@@ -1288,6 +1345,15 @@ struct CoefKeyHash {
   }
 };
 
+// Factor applied to coefficient array a (ca0..2 cb0..2 da0..2 db0..2) when H
+// is stored multiplied by h_scale: Cb / s (E sees H / s) and Db * s.
+static float coef_storage_factor(const oems_engine* en, int a) {
+  if (en->h_scale == 1.0f) return 1.0f;
+  if (a >= 3 && a < 6) return 1.0f / en->h_scale;
+  if (a >= 9) return en->h_scale;
+  return 1.0f;
+}
+
 static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc* d) {
   const size_t nzp = en->g.nzp;
   const size_t rows = (size_t)en->nx * en->ny;
@@ -1299,9 +1365,20 @@ static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc
     OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->coeffs), (size_t)12 * en->ncells_padded * sizeof(float),
                          en->stream));
     OEMS_CUDA(cudaMemsetAsync(en->coeffs, 0, (size_t)12 * en->ncells_padded * sizeof(float), en->stream));
-    for (int a = 0; a < 12; ++a)
-      OEMS_CUDA(cudaMemcpy2DAsync(en->C(a), nzp * sizeof(float), src[a], en->nz * sizeof(float),
+    std::vector<float> scaled;
+    for (int a = 0; a < 12; ++a) {
+      const float* from = src[a];
+      const float f = coef_storage_factor(en, a);
+      if (f != 1.0f) {
+        // Cb / s and Db * s for H kept scaled by s (a power of two: exact)
+        scaled.resize(rows * en->nz);
+        for (size_t q = 0; q < scaled.size(); ++q) scaled[q] = src[a][q] * f;
+        from = scaled.data();
+      }
+      OEMS_CUDA(cudaMemcpy2DAsync(en->C(a), nzp * sizeof(float), from, en->nz * sizeof(float),
                                   en->nz * sizeof(float), rows, cudaMemcpyHostToDevice, en->stream));
+      if (f != 1.0f) OEMS_CUDA(cudaStreamSynchronize(en->stream));
+    }
     OEMS_CUDA(cudaStreamSynchronize(en->stream));
     return OEMS_OK;
   }
@@ -1333,6 +1410,7 @@ static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc
   }
   (void)n;
   en->ntable = (int)map.size();
+  for (size_t t = 0; t < table.size(); ++t) table[t] *= coef_storage_factor(en, (int)(t % 12));
   OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->table), table.size() * sizeof(float), en->stream));
   OEMS_CUDA(cudaMemcpyAsync(en->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
                             en->stream));
@@ -1393,6 +1471,14 @@ static oems_status create(const oems_operator_desc* d, oems_engine** out) {
   std::unique_ptr<oems_engine, void (*)(oems_engine*)> en(new oems_engine, destroy);
   en->device = dev;
   en->flags = d->flags;
+  const uint32_t half_flags = d->flags & (OEMS_ENGINE_FIELDS_F16 | OEMS_ENGINE_FIELDS_BF16);
+  if (half_flags == (OEMS_ENGINE_FIELDS_F16 | OEMS_ENGINE_FIELDS_BF16))
+    return fail(OEMS_ERR_CONFIG, "choose one field storage: half or bfloat16");
+  if (half_flags && (d->flags & (OEMS_ENGINE_STAGED_KERNELS | OEMS_ENGINE_SPLIT_KERNELS)))
+    return fail(OEMS_ERR_CONFIG, "2-byte field storage runs the register kernels only");
+  en->storage = (d->flags & OEMS_ENGINE_FIELDS_F16) ? 1 : (d->flags & OEMS_ENGINE_FIELDS_BF16) ? 2 : 0;
+  en->elem = en->storage ? 2 : sizeof(float);
+  en->h_scale = en->storage ? OEMS_H_STORAGE_SCALE : 1.0f;
   en->nx = (int)d->nx;
   en->ny = (int)d->ny;
   en->nz = (int)d->nz;
@@ -1404,9 +1490,8 @@ static oems_status create(const oems_operator_desc* d, oems_engine** out) {
   OEMS_CUDA(cudaEventCreate(&en->ev1));
   en->g = make_geom(en.get(), 256, 8);
   en->ncells_padded = (long long)en->nx * en->ny * en->g.nzp;
-  OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->fields), (size_t)6 * en->ncells_padded * sizeof(float),
-                       en->stream));
-  OEMS_CUDA(cudaMemsetAsync(en->fields, 0, (size_t)6 * en->ncells_padded * sizeof(float), en->stream));
+  OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->fields), en->field_bytes(), en->stream));
+  OEMS_CUDA(cudaMemsetAsync(en->fields, 0, en->field_bytes(), en->stream));
   OEMS_TRY(upload_coefficients(en.get(), d));
   OEMS_CUDA(en->d_partials.ensure(6 * kEnergyBlocks));
   OEMS_CUDA(en->d_base.ensure(1));
@@ -1654,8 +1739,41 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
   return OEMS_OK;
 }
 
+// 2-byte storage: values converted on the host (rounded to nearest on the
+// way in), H scaled by h_scale on the device.
+static oems_status copy_fields_2byte(oems_engine* en, float* const* host6, bool to_host) {
+  const size_t rows = (size_t)en->nx * en->ny, n = rows * en->nz;
+  std::vector<uint16_t> buf(n);
+  for (int c = 0; c < 6; ++c) {
+    if (!host6[c]) return fail(OEMS_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+    const float scale = c < 3 ? 1.0f : en->h_scale;
+    float* dev = en->at((size_t)c);
+    if (to_host) {
+      OEMS_CUDA(cudaMemcpy2DAsync(buf.data(), en->nz * 2, dev, en->g.nzp * 2, en->nz * 2, rows,
+                                  cudaMemcpyDeviceToHost, en->stream));
+      OEMS_CUDA(cudaStreamSynchronize(en->stream));
+      for (size_t q = 0; q < n; ++q) {
+        const float v = en->storage == 1 ? __half2float(__ushort_as_half(buf[q]))
+                                         : __bfloat162float(__ushort_as_bfloat16(buf[q]));
+        host6[c][q] = v / scale;
+      }
+    } else {
+      for (size_t q = 0; q < n; ++q) {
+        const float v = host6[c][q] * scale;
+        buf[q] = en->storage == 1 ? __half_as_ushort(__float2half_rn(v))
+                                  : __bfloat16_as_ushort(__float2bfloat16_rn(v));
+      }
+      OEMS_CUDA(cudaMemcpy2DAsync(dev, en->g.nzp * 2, buf.data(), en->nz * 2, en->nz * 2, rows,
+                                  cudaMemcpyHostToDevice, en->stream));
+      OEMS_CUDA(cudaStreamSynchronize(en->stream));
+    }
+  }
+  return OEMS_OK;
+}
+
 static oems_status copy_fields(oems_engine* en, float* const* host6, bool to_host) {
   EngineScope guard(en);
+  if (en->storage) return copy_fields_2byte(en, host6, to_host);
   const size_t rows = (size_t)en->nx * en->ny;
   for (int c = 0; c < 6; ++c) {
     if (!host6[c]) return fail(OEMS_ERR_INVALID_ARGUMENT, "field pointer is NULL");
@@ -1675,6 +1793,7 @@ static oems_status copy_fields(oems_engine* en, float* const* host6, bool to_hos
 // (:88-151); second order as described in mur.cuh.
 static oems_status add_mur(oems_engine* en, const oems_mur_desc* d) {
   if (!d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL Mur descriptor");
+  if (en->storage) return fail(OEMS_ERR_CONFIG, "Mur boundaries need float field storage");
   if (en->mur.on) return fail(OEMS_ERR_CONFIG, "Mur boundary already attached");
   if (d->order != 1 && d->order != 2) return fail(OEMS_ERR_CONFIG, "Mur order must be 1 or 2");
   EngineScope guard(en);
@@ -1878,7 +1997,7 @@ oems_status oems_engine_write_fields(oems_engine* engine, const float* const e[3
 oems_status oems_engine_reset(oems_engine* engine) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   EngineScope guard(engine);
-  OEMS_CUDA(cudaMemsetAsync(engine->fields, 0, (size_t)6 * engine->ncells_padded * sizeof(float), engine->stream));
+  OEMS_CUDA(cudaMemsetAsync(engine->fields, 0, engine->field_bytes(), engine->stream));
   if (engine->cpml.on)
     OEMS_CUDA(cudaMemsetAsync(engine->cpml.psi.p, 0, engine->cpml.psi.n * sizeof(float), engine->stream));
   if (engine->mur.on)
@@ -1910,6 +2029,7 @@ oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc
 oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersive_desc* d, const uint64_t* cells,
                                        uint64_t ncells) {
   if (!engine || !d || (!cells && ncells)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "dispersive materials need float field storage");
   if (d->kind < 0 || d->kind > 4) return fail(OEMS_ERR_MATERIAL, "unknown dispersive material kind");
   if (!(d->eps_inf > 0.0)) return fail(OEMS_ERR_MATERIAL, "eps_inf must be positive");
   if (ncells == 0) return fail(OEMS_ERR_MATERIAL, "a dispersive material needs at least one cell");
@@ -1967,6 +2087,7 @@ oems_status oems_engine_add_dispersive(oems_engine* engine, const oems_dispersiv
 
 oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rlc_desc* elems, uint64_t n) {
   if (!engine || (!elems && n)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "lumped RLC elements need float field storage");
   EngineScope guard(engine);
   RlcHost& R = engine->rlc;
   const double dt = engine->dt, kEps0 = 8.854187817e-12;
@@ -2021,6 +2142,7 @@ oems_status oems_engine_add_lumped_rlc(oems_engine* engine, const oems_lumped_rl
 oems_status oems_engine_add_field_dft(oems_engine* engine, const oems_field_dft_desc* d, const double* freqs,
                                       uint32_t nfreq, int32_t* dump_id) {
   if (!engine || !d || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "field DFT dumps need float field storage");
   if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "a field DFT needs at least one frequency");
   if ((d->components & 0x3Fu) == 0 || (d->components & ~0x3Fu))
     return fail(OEMS_ERR_CONFIG, "field DFT components must be a non-empty mask of bits 0..5");
@@ -2092,6 +2214,7 @@ oems_status oems_engine_read_field_dft(oems_engine* engine, int32_t id, uint32_t
 oems_status oems_engine_add_nf2ff_box(oems_engine* engine, const oems_nf2ff_box_desc* d, const double* freqs,
                                       uint32_t nfreq, int32_t* box_id) {
   if (!engine || !d || (!freqs && nfreq)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "NF2FF boxes need float field storage");
   if (nfreq == 0) return fail(OEMS_ERR_CONFIG, "an NF2FF box needs at least one frequency");
   const long long ext[3] = {engine->nx, engine->ny, engine->nz};
   for (int a = 0; a < 3; ++a)
@@ -2364,6 +2487,7 @@ static void upml_kappa(int comp, int dir, const long long pos[3], bool is_min, l
 
 oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc) {
   if (!engine || !desc) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "UPML needs float field storage");
   if (engine->upml.on) return fail(OEMS_ERR_CONFIG, "UPML already attached");
   if (!(desc->reflection_coeff > 0.0 && desc->reflection_coeff < 1.0))
     return fail(OEMS_ERR_CONFIG, "UPML reflection coefficient must be in (0, 1)");

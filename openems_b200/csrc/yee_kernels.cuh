@@ -29,6 +29,9 @@
 // along the slab normal becomes d*inv_kappa + psi with psi = b*psi + c*d.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -147,6 +150,99 @@ __device__ __forceinline__ float4 ld_nc4(const float* p) { return __ldg(reinterp
 __device__ __forceinline__ float4 ld_cs4(const float* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+// Field storage: float (the reference's layout), or IEEE half / bfloat16
+// with the arithmetic still in float (values converted on load, rounded to
+// nearest on store).  Offsets are in elements; a chunk of 4 elements starts
+// at a multiple of 4, so it is one 16-byte (float) or 8-byte (2-byte types)
+// access.  Field pointers travel as float* and are reinterpreted here.
+template <typename T>
+struct FieldIO;
+
+template <>
+struct FieldIO<float> {
+  static constexpr bool kFloat = true;
+  __device__ __forceinline__ static float4 ldg4(const float* b, long long q) {
+    return __ldg(reinterpret_cast<const float4*>(b + q));
+  }
+  __device__ __forceinline__ static float4 ld4(const float* b, long long q) {
+    return *reinterpret_cast<const float4*>(b + q);
+  }
+  __device__ __forceinline__ static void st4(float* b, long long q, float4 v) {
+    *reinterpret_cast<float4*>(b + q) = v;
+  }
+  __device__ __forceinline__ static float ldg1(const float* b, long long q) { return __ldg(b + q); }
+  __device__ __forceinline__ static float ld1(const float* b, long long q) { return b[q]; }
+  __device__ __forceinline__ static void st1(float* b, long long q, float v) { b[q] = v; }
+};
+
+template <typename H2, typename H1>
+struct FieldIO2 {
+  static constexpr bool kFloat = false;
+  __device__ __forceinline__ static float4 unpack(uint2 r) {
+    const float2 lo = cvt(*reinterpret_cast<const H2*>(&r.x));
+    const float2 hi = cvt(*reinterpret_cast<const H2*>(&r.y));
+    return make_float4(lo.x, lo.y, hi.x, hi.y);
+  }
+  __device__ __forceinline__ static float4 ldg4(const float* b, long long q) {
+    return unpack(__ldg(reinterpret_cast<const uint2*>(reinterpret_cast<const H1*>(b) + q)));
+  }
+  __device__ __forceinline__ static float4 ld4(const float* b, long long q) {
+    return unpack(*reinterpret_cast<const uint2*>(reinterpret_cast<const H1*>(b) + q));
+  }
+  __device__ __forceinline__ static void st4(float* b, long long q, float4 v) {
+    const H2 lo = pack(v.x, v.y), hi = pack(v.z, v.w);
+    uint2 r;
+    r.x = *reinterpret_cast<const unsigned int*>(&lo);
+    r.y = *reinterpret_cast<const unsigned int*>(&hi);
+    *reinterpret_cast<uint2*>(reinterpret_cast<H1*>(b) + q) = r;
+  }
+  __device__ __forceinline__ static float ldg1(const float* b, long long q) {
+    return cvt1(__ldg(reinterpret_cast<const H1*>(b) + q));
+  }
+  __device__ __forceinline__ static float ld1(const float* b, long long q) {
+    return cvt1(reinterpret_cast<const H1*>(b)[q]);
+  }
+  __device__ __forceinline__ static void st1(float* b, long long q, float v) {
+    reinterpret_cast<H1*>(b)[q] = round1(v);
+  }
+  __device__ __forceinline__ static float2 cvt(H2 h);
+  __device__ __forceinline__ static H2 pack(float x, float y);
+  __device__ __forceinline__ static float cvt1(H1 h);
+  __device__ __forceinline__ static H1 round1(float v);
+};
+
+template <>
+__device__ __forceinline__ float2 FieldIO2<__half2, __half>::cvt(__half2 h) { return __half22float2(h); }
+template <>
+__device__ __forceinline__ __half2 FieldIO2<__half2, __half>::pack(float x, float y) {
+  return __floats2half2_rn(x, y);
+}
+template <>
+__device__ __forceinline__ float FieldIO2<__half2, __half>::cvt1(__half h) { return __half2float(h); }
+template <>
+__device__ __forceinline__ __half FieldIO2<__half2, __half>::round1(float v) { return __float2half_rn(v); }
+template <>
+__device__ __forceinline__ float2 FieldIO2<__nv_bfloat162, __nv_bfloat16>::cvt(__nv_bfloat162 h) {
+  return __bfloat1622float2(h);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat162 FieldIO2<__nv_bfloat162, __nv_bfloat16>::pack(float x, float y) {
+  return __floats2bfloat162_rn(x, y);
+}
+template <>
+__device__ __forceinline__ float FieldIO2<__nv_bfloat162, __nv_bfloat16>::cvt1(__nv_bfloat16 h) {
+  return __bfloat162float(h);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 FieldIO2<__nv_bfloat162, __nv_bfloat16>::round1(float v) {
+  return __float2bfloat16_rn(v);
+}
+
+template <>
+struct FieldIO<__half> : FieldIO2<__half2, __half> {};
+template <>
+struct FieldIO<__nv_bfloat16> : FieldIO2<__nv_bfloat162, __nv_bfloat16> {};
 
 __device__ __forceinline__ void to_arr(float4 v, float (&a)[4]) {
   a[0] = v.x;
@@ -324,9 +420,10 @@ __device__ __forceinline__ void prefetch_e_plane(const EArgs& a, long long o, lo
     }
 }
 
-// H half-step: H = da*H + db*curl(E).
-template <int kIdBytes, bool kCpml>
+// H half-step: H = da*H + db*curl(E).  T: field storage type.
+template <int kIdBytes, bool kCpml, typename T = float>
 __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
+  using IO = FieldIO<T>;
   extern __shared__ float s_table[];
   const Geom& g = a.g;
   const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
@@ -346,30 +443,30 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
 #pragma unroll
     for (int e = 0; e < 4; ++e) live |= (k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
-    if (g.pf > 0 && threadIdx.x == 0) {
+    if (IO::kFloat && g.pf > 0 && threadIdx.x == 0) {
       const long long tn = (long long)(it.c1 - it.c0) * 4;
       for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_h_plane<kIdBytes>(a, q + p * g.plane, tn);
     }
-    float4 ey4 = ld_nc4(a.ey + q);
-    float4 ez4 = ld_nc4(a.ez + q);
+    float4 ey4 = IO::ldg4(a.ey, q);
+    float4 ez4 = IO::ldg4(a.ez, q);
     for (int i = i0; i < i1; ++i, q += g.plane) {
       const bool has_ip = i + 1 < g.nx;
-      if (g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+      if (IO::kFloat && g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
         prefetch_h_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       // ---- every load of this plane first
-      const float4 ex4 = ld_nc4(a.ex + q);
-      const float4 ey1 = has_ip ? ld_nc4(a.ey + q + g.plane) : ey4;
-      const float4 ez1 = has_ip ? ld_nc4(a.ez + q + g.plane) : ez4;
-      const float4 exj = has_jp ? ld_nc4(a.ex + q + g.nzp) : ex4;
-      const float4 ezj = has_jp ? ld_nc4(a.ez + q + g.nzp) : ez4;
-      const float exn_m = need_kn ? __ldg(a.ex + q + 4) : 0.f;
-      const float eyn_m = need_kn ? __ldg(a.ey + q + 4) : 0.f;
+      const float4 ex4 = IO::ldg4(a.ex, q);
+      const float4 ey1 = has_ip ? IO::ldg4(a.ey, q + g.plane) : ey4;
+      const float4 ez1 = has_ip ? IO::ldg4(a.ez, q + g.plane) : ez4;
+      const float4 exj = has_jp ? IO::ldg4(a.ex, q + g.nzp) : ex4;
+      const float4 ezj = has_jp ? IO::ldg4(a.ez, q + g.nzp) : ez4;
+      const float exn_m = need_kn ? IO::ldg1(a.ex, q + 4) : 0.f;
+      const float eyn_m = need_kn ? IO::ldg1(a.ey, q + 4) : 0.f;
       float co_a[3][4], co_b[3][4], h[3][4];
       Coef<kIdBytes>::load(a.da, a.ids, tab, 6, q, co_a);
       Coef<kIdBytes>::load(a.db, a.ids, tab, 9, q, co_b);
-      to_arr(ld4(a.hx + q), h[0]);
-      to_arr(ld4(a.hy + q), h[1]);
-      to_arr(ld4(a.hz + q), h[2]);
+      to_arr(IO::ld4(a.hx, q), h[0]);
+      to_arr(IO::ld4(a.hy, q), h[1]);
+      to_arr(IO::ld4(a.hz, q), h[2]);
       SlabInfo sl;
       float4 px0, px1, py0, py1, pzn0, pzn1, pzx0, pzx1;
       if constexpr (kCpml) {
@@ -448,9 +545,9 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
         }
       }
       if (valid) {
-        st4(a.hx + q, to_f4(out[0]));
-        st4(a.hy + q, to_f4(out[1]));
-        st4(a.hz + q, to_f4(out[2]));
+        IO::st4(a.hx, q, to_f4(out[0]));
+        IO::st4(a.hy, q, to_f4(out[1]));
+        IO::st4(a.hz, q, to_f4(out[2]));
         if constexpr (kCpml) {
           if (sl.fy >= 0) {
             st4(a.cp.psi_h[sl.fy][0] + sl.py, py0);
@@ -476,9 +573,11 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
   }
 }
 
-// E half-step: E = ca*E + cb*curl(H), cells with i, j, k >= 1 only.
-template <int kIdBytes, bool kCpml>
+// E half-step: E = ca*E + cb*curl(H), cells with i, j, k >= 1 only.  T: field
+// storage type.
+template <int kIdBytes, bool kCpml, typename T = float>
 __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
+  using IO = FieldIO<T>;
   extern __shared__ float s_table[];
   const Geom& g = a.g;
   const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
@@ -499,35 +598,35 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
 #pragma unroll
     for (int e = 0; e < 4; ++e) live_k |= (k0 + e >= 1 && k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
-    if (g.pf > 0 && threadIdx.x == 0) {
+    if (IO::kFloat && g.pf > 0 && threadIdx.x == 0) {
       const long long tn = (long long)(it.c1 - it.c0) * 4;
       for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_e_plane<kIdBytes>(a, q + p * g.plane, tn);
     }
     float4 hym4 = zero4(), hzm4 = zero4();  // H at i-1
     if (i0 > 0) {
-      hym4 = ld_nc4(a.hy + q - g.plane);
-      hzm4 = ld_nc4(a.hz + q - g.plane);
+      hym4 = IO::ldg4(a.hy, q - g.plane);
+      hzm4 = IO::ldg4(a.hz, q - g.plane);
     }
     for (int i = i0; i < i1; ++i, q += g.plane) {
-      if (g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+      if (IO::kFloat && g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
         prefetch_e_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       const bool upd = i >= 1 && has_jm;
       const unsigned live = upd ? live_k : 0u;
       // ---- every load of this plane first
-      const float4 hx4 = ld_nc4(a.hx + q);
-      const float4 hy4 = ld_nc4(a.hy + q);
-      const float4 hz4 = ld_nc4(a.hz + q);
-      const float4 hxj4 = upd ? ld_nc4(a.hx + q - g.nzp) : zero4();
-      const float4 hzj4 = upd ? ld_nc4(a.hz + q - g.nzp) : zero4();
-      const float hxm_m = need_km ? __ldg(a.hx + q - 1) : 0.f;
-      const float hym_m = need_km ? __ldg(a.hy + q - 1) : 0.f;
+      const float4 hx4 = IO::ldg4(a.hx, q);
+      const float4 hy4 = IO::ldg4(a.hy, q);
+      const float4 hz4 = IO::ldg4(a.hz, q);
+      const float4 hxj4 = upd ? IO::ldg4(a.hx, q - g.nzp) : zero4();
+      const float4 hzj4 = upd ? IO::ldg4(a.hz, q - g.nzp) : zero4();
+      const float hxm_m = need_km ? IO::ldg1(a.hx, q - 1) : 0.f;
+      const float hym_m = need_km ? IO::ldg1(a.hy, q - 1) : 0.f;
       float co_a[3][4], co_b[3][4], ev[3][4];
       if (upd) {
         Coef<kIdBytes>::load(a.ca, a.ids, tab, 0, q, co_a);
         Coef<kIdBytes>::load(a.cb, a.ids, tab, 3, q, co_b);
-        to_arr(ld4(a.ex + q), ev[0]);
-        to_arr(ld4(a.ey + q), ev[1]);
-        to_arr(ld4(a.ez + q), ev[2]);
+        to_arr(IO::ld4(a.ex, q), ev[0]);
+        to_arr(IO::ld4(a.ey, q), ev[1]);
+        to_arr(IO::ld4(a.ez, q), ev[2]);
       }
       SlabInfo sl;
       float4 px0, px1, py0, py1, pzn0, pzn1, pzx0, pzx1;
@@ -611,9 +710,9 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
           }
         }
         if (valid) {
-          st4(a.ex + q, to_f4(out[0]));
-          st4(a.ey + q, to_f4(out[1]));
-          st4(a.ez + q, to_f4(out[2]));
+          IO::st4(a.ex, q, to_f4(out[0]));
+          IO::st4(a.ey, q, to_f4(out[1]));
+          IO::st4(a.ez, q, to_f4(out[2]));
           if constexpr (kCpml) {
             if (sl.fy >= 0) {
               st4(a.cp.psi_e[sl.fy][0] + sl.py, py0);

@@ -877,15 +877,19 @@ class Engine:
 
     def __init__(self, operator: Operator, engine_type: EngineType = EngineType.Cuda, *,
                  device: int = -1, compressed: bool = False, autotune: bool = True,
-                 graphs: bool = True, kernels: str = "auto"):
+                 graphs: bool = True, kernels: str = "auto", storage: str = "f32"):
         """kernels: "auto" (tuner picks), "register", "staged" (bulk-async) or
-        "split" (staged between the x / y CPML slabs, register on them)."""
+        "split" (staged between the x / y CPML slabs, register on them).
+        storage: field storage "f32", or "f16" / "bf16" (2 bytes per value,
+        float arithmetic; register kernels, CPML, sources, probes, energies)."""
         if engine_type is not EngineType.Cuda:
             raise N.ConfigError("only the CUDA engine exists")
+        if storage not in N.STORAGE_FLAGS:
+            raise N.ConfigError(f"unknown field storage {storage!r}")
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
             | (0 if graphs else N.ENGINE_NO_GRAPHS) \
             | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS,
-               "split": N.ENGINE_SPLIT_KERNELS}[kernels]
+               "split": N.ENGINE_SPLIT_KERNELS}[kernels] | N.STORAGE_FLAGS[storage]
         desc = N.OperatorDesc()
         N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))
         h = ctypes.c_void_p()

@@ -56,10 +56,13 @@ class Sweep:
     engines run at a time on `device`."""
 
     def __init__(self, freqs, concurrency: int = 4, device: int = -1, compressed: bool = False,
-                 autotune: bool = False, kernels: str = "register"):
+                 autotune: bool = False, kernels: str = "register", storage: str = "f32"):
         self.freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+        if storage not in N.STORAGE_FLAGS:
+            raise N.ConfigError(f"unknown field storage {storage!r}")
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
-            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS}[kernels]
+            | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS}[kernels] \
+            | N.STORAGE_FLAGS[storage]
         h = ctypes.c_void_p()
         N.check(N.lib().oems_sweep_create(device, concurrency, flags,
                                           self.freqs.ctypes.data_as(ctypes.POINTER(N.c_f64)),
@@ -152,11 +155,12 @@ def main(argv=None):
     p.add_argument("--max-steps", type=int, default=60000)
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--out", default=None, help="write S11 per instance to this .npz")
+    p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32", help="field storage")
     a = p.parse_args(argv)
     freqs = np.linspace(0.0, 8e9, a.freqs)
     specs = W.patch_specs(a.count, seed=a.seed)
     t0 = time.perf_counter()
-    sw = Sweep(freqs, concurrency=a.concurrency)
+    sw = Sweep(freqs, concurrency=a.concurrency, storage=a.storage)
     ids = [sw.add(W.patch_sweep_instance(s, decay_db=a.decay_db, max_steps=a.max_steps)) for s in specs]
     t1 = time.perf_counter()
     sw.run(a.batch_steps)
@@ -164,7 +168,7 @@ def main(argv=None):
     res = [sw.result(i) for i in ids]
     s11_db = [20 * np.log10(np.maximum(np.abs(r["s11"][1:]), 1e-30)) for r in res]
     line = {
-        "workload": f"patch_sweep_{a.count}_seed{a.seed}",
+        "workload": f"patch_sweep_{a.count}_seed{a.seed}", "field_storage": a.storage,
         "instances": a.count, "concurrency": a.concurrency, "freqs": a.freqs,
         "cell_steps": cell_steps, "wall_s": wall, "setup_s": t1 - t0,
         "mcells_per_s": cell_steps / wall / 1e6, "instances_per_hour": a.count / wall * 3600.0,

@@ -72,6 +72,58 @@ def run(coeffs12: np.ndarray, fields6: np.ndarray, num_steps: int, excitations=(
     return np.stack([ex, ey, ez, hx, hy, hz])
 
 
+def round_to_storage(a: np.ndarray, store: str) -> np.ndarray:
+    """float32 values rounded to nearest (even) in the 2-byte storage type
+    and back: "f16" IEEE half, "bf16" bfloat16 (the top 16 bits of a float32),
+    "f32" unchanged."""
+    a = np.asarray(a, dtype=np.float32)
+    if store == "f32":
+        return a
+    if store == "f16":
+        return a.astype(np.float16).astype(np.float32)
+    b = a.view(np.uint32).astype(np.uint64)
+    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return (b & 0xFFFFFFFF).astype(np.uint32).view(np.float32).reshape(a.shape)
+
+
+def run_stored(coeffs12: np.ndarray, fields6: np.ndarray, num_steps: int, excitations=(), store: str = "f16",
+               h_scale: float = 512.0) -> np.ndarray:
+    """The update of ``run`` with 2-byte field storage: arithmetic in float32,
+    every stored field value rounded to ``store``, H kept multiplied by
+    ``h_scale`` (a power of two, folded into Cb / s and Db * s, so the
+    float32 arithmetic is exactly the scaled one).  Returns unscaled fields.
+    This restates the engine's OEMS_ENGINE_FIELDS_F16 / _BF16 modes (no
+    counterpart in the reference)."""
+    s = np.float32(h_scale)
+    c = [np.asarray(x, dtype=np.float32) for x in coeffs12]
+    ca, cb, da, db = c[0:3], [x / s for x in c[3:6]], c[6:9], [x * s for x in c[9:12]]
+    R = lambda a: round_to_storage(a, store)  # noqa: E731
+    f = [R(np.asarray(x, dtype=np.float32) * (s if k >= 3 else np.float32(1.0))) for k, x in enumerate(fields6)]
+    ex, ey, ez, hx, hy, hz = f
+    for step in range(num_steps):
+        dez_dy, dey_dz = _fwd(ez, 1), _fwd(ey, 2)
+        dex_dz, dez_dx = _fwd(ex, 2), _fwd(ez, 0)
+        dey_dx, dex_dy = _fwd(ey, 0), _fwd(ex, 1)
+        hx = R(da[0] * hx + db[0] * (dez_dy - dey_dz))
+        hy = R(da[1] * hy + db[1] * (dex_dz - dez_dx))
+        hz = R(da[2] * hz + db[2] * (dey_dx - dex_dy))
+        inner = (slice(1, None),) * 3
+        cx = _bwd(hz, 1) - _bwd(hy, 2)
+        cy = _bwd(hx, 2) - _bwd(hz, 0)
+        cz = _bwd(hy, 0) - _bwd(hx, 1)
+        ex[inner] = R(ca[0] * ex + cb[0] * cx)[inner]
+        ey[inner] = R(ca[1] * ey + cb[1] * cy)[inner]
+        ez[inner] = R(ca[2] * ez + cb[2] * cz)[inner]
+        comps = (ex, ey, ez)
+        for pos, d, soft, samples in excitations:
+            if step >= len(samples):
+                continue
+            v = np.float32(samples[step])
+            p = tuple(pos)
+            comps[d][p] = R(np.array(comps[d][p] + v if soft else v, dtype=np.float32))
+    return np.stack([ex, ey, ez, hx / s, hy / s, hz / s])
+
+
 # ---------------------------------------------------------------------------
 # per-cell extensions, written separately from oems_oracle.cpp
 # ---------------------------------------------------------------------------

@@ -51,10 +51,11 @@ def make_operator(sc: Scenario) -> oe.Operator:
     return op
 
 
-def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kernels="auto"):
+def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kernels="auto", storage="f32"):
     """Runs the scenario on the CUDA engine; returns dict of results."""
     op = make_operator(sc)
-    eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune, kernels=kernels)
+    eng = oe.Engine(op, compressed=compressed, graphs=graphs, autotune=autotune, kernels=kernels,
+                    storage=storage)
     if sc.cpml is not None:
         eng.add_cpml(sc.cpml)
     if sc.mur is not None:

@@ -225,3 +225,21 @@ def test_voltage_integral_weights_and_sign():
     t = oe.voltage_integral(op, (2, 3, 4), (2, 3, 9))
     assert len(t.terms) == 5 and all(c == 2 and abs(w + 1e-3) < 1e-15 for c, _, w in t.terms)
     assert abs(_probe_value(t, lambda f: f[2].fill(4.0)) - (-5 * 4.0 * 1e-3)) < 1e-15
+
+
+def test_storage_rounding_restatement():
+    """2-byte storage in the numpy restatement: bfloat16 rounds to nearest
+    even on the 16 dropped bits, half as numpy's float16; the f32 "storage"
+    run is the plain update."""
+    from oracle.numpy_ref import round_to_storage, run, run_stored
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 3.0e38], dtype=np.float32)
+    assert list(round_to_storage(v, "bf16")[:4]) == [1.0, 1.0, 1.0 + 2 ** -6, -2.5]
+    assert round_to_storage(np.float32(1 + 2 ** -11), "f16") == 1.0
+    rng = np.random.default_rng(0)
+    co = [np.full((6, 5, 7), x, np.float32) for x in (1.0, 1.0, 1.0, 0.4, 0.4, 0.4, 1.0, 1.0, 1.0,
+                                                         -0.3, -0.3, -0.3)]
+    f = rng.standard_normal((6, 6, 5, 7)).astype(np.float32)
+    assert np.array_equal(run_stored(co, f, 5, store="f32", h_scale=1.0), run(co, f, 5))
+    # half storage of the same update stays within a few half ulps per step
+    a = run_stored(co, f, 5, store="f16")
+    assert np.abs(a - run(co, f, 5)).max() < 5 * 2 ** -11 * np.abs(f).max() * 8
