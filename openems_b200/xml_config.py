@@ -275,23 +275,24 @@ def waveform(cfg: SimulationConfig, position, component, weight) -> fdtd.Excitat
     return e.with_amplitude(e.amplitude * weight)
 
 
-def run(cfg: SimulationConfig, device: int = -1, batch: int = 1000, storage: str = "f32") -> dict:
-    """Runs a parsed configuration on the GPU; returns the run's figures."""
+def run_operator(operator: fdtd.Operator, excitations: Sequence[fdtd.Excitation], cap: int,
+                 end_db: Optional[float] = None, mur_faces: Sequence[bool] = (False,) * 6, device: int = -1,
+                 batch: int = 1000, storage: str = "f32") -> dict:
+    """Runs an operator (CPML from its PML faces, Mur on `mur_faces`) with
+    soft / hard point sources for `cap` steps or until the energy has
+    decayed by end_db below its peak (the peak carried across batches, as
+    Simulation::run does); returns the run's figures and the engine."""
     import time
-    b = build(cfg)
-    eng = fdtd.Engine(b.operator, device=device, storage=storage)
-    if any(b.mur_faces):
-        eng.add_mur(fdtd.MurAbcConfig(enabled=b.mur_faces))
-    dt = b.operator.timestep()
-    excs = [waveform(cfg, pos, comp, w) for pos, comp, w in b.sources]
-    end_db = cfg.end_criteria_db
-    cap = cfg.num_timesteps if cfg.num_timesteps > 0 else (10000 if end_db is None else 10 ** 7)
+    eng = fdtd.Engine(operator, device=device, storage=storage)
+    if any(mur_faces):
+        eng.add_mur(fdtd.MurAbcConfig(enabled=tuple(bool(v) for v in mur_faces)))
+    dt = operator.timestep()
     start, peak, reason, final_db = 0, 0.0, 0, 0.0
     t0 = time.perf_counter()
     while start < cap:
         n = min(batch, cap - start)
         res = eng.run_batch(fdtd.EngineBatch(
-            num_steps=n, excitations=[fdtd.ScheduledExcitation.from_excitation(x, start, n, dt) for x in excs],
+            num_steps=n, excitations=[fdtd.ScheduledExcitation.from_excitation(x, start, n, dt) for x in excitations],
             termination=fdtd.TerminationConfig(max_timesteps=n, energy_decay_db=end_db, check_interval=100),
             energy_monitoring=fdtd.EnergyMonitorConfig(sample_interval=100, track_peak=True),
             initial_peak_energy=peak))
@@ -301,12 +302,21 @@ def run(cfg: SimulationConfig, device: int = -1, batch: int = 1000, storage: str
         if res.termination_reason != fdtd.TerminationReason.StepsCompleted or res.timesteps_executed == 0:
             break
     wall = time.perf_counter() - t0
-    dims = b.operator.dimensions()
+    dims = operator.dimensions()
     cells = dims[0] * dims[1] * dims[2]
     e, h = eng.energy()
     return {"dims": list(dims), "timesteps": start, "termination_reason": reason, "final_decay_db": final_db,
-            "sources": len(excs), "wall_s": wall, "mcells_per_s": cells * start / wall / 1e6,
-            "energy": e + h, "engine": eng}
+            "sources": len(excitations), "wall_s": wall, "mcells_per_s": cells * start / max(wall, 1e-12) / 1e6,
+            "peak_energy": peak, "energy": e + h, "engine": eng}
+
+
+def run(cfg: SimulationConfig, device: int = -1, batch: int = 1000, storage: str = "f32") -> dict:
+    """Runs a parsed configuration on the GPU; returns the run's figures."""
+    b = build(cfg)
+    excs = [waveform(cfg, pos, comp, w) for pos, comp, w in b.sources]
+    end_db = cfg.end_criteria_db
+    cap = cfg.num_timesteps if cfg.num_timesteps > 0 else (10000 if end_db is None else 10 ** 7)
+    return run_operator(b.operator, excs, cap, end_db, b.mur_faces, device, batch, storage)
 
 
 def main(argv: Optional[Sequence[str]] = None):
