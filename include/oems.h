@@ -299,6 +299,28 @@ OEMS_API void oems_engine_destroy(oems_engine* engine);
  * device. */
 OEMS_API oems_status oems_release_cached_memory(int32_t device);
 
+/* ---- TF/SF plane source (src/extensions/tfsf.rs:54-355) ---------------- */
+
+/* TfsfConfig: direction 0 XPlus 1 XMinus 2 YPlus 3 YMinus 4 ZPlus 5 ZMinus
+ * (as in the reference only the axis is used), polarization 0 Transverse1
+ * (E along axis+1, H along axis+2) or 1 Transverse2, frequency (Hz) and
+ * amplitude (V/m) of the sinusoid driving the 1D auxiliary grid,
+ * boundary_layer the plane index along the axis, phase_velocity <= 0: c0. */
+typedef struct oems_tfsf_desc {
+  int32_t direction;
+  int32_t polarization;
+  double frequency;
+  double amplitude;
+  uint64_t boundary_layer;
+  double phase_velocity;
+  int32_t kind;      /* 0: the reference's update, whose 1D grid has the wrong
+                        sign in its E update and grows exponentially; 1: the
+                        corrected source (positive directions, boundary_layer
+                        >= 1): stable 1D grid, scattered-side H plane at
+                        boundary_layer - 1, total-side E plane at boundary_layer */
+  int32_t reserved0;
+} oems_tfsf_desc;
+
 /* ---- EngineImpl --------------------------------------------------------- */
 
 OEMS_API oems_status oems_engine_run_batch(oems_engine* engine, const oems_batch* batch,
@@ -316,6 +338,11 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);
 /* MurAbc::new (src/extensions/mur_abc.rs:175). */
 OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_desc* desc);
+/* TfsfBoundary::new (src/extensions/tfsf.rs:142-190): before every H update
+ * plane boundary_layer of the H component gets h - db e_inc, before every E
+ * update that of the E component gets e + cb h_inc, the 1D grid's values
+ * there.  Float field storage only. */
+OEMS_API oems_status oems_engine_add_tfsf(oems_engine* engine, const oems_tfsf_desc* desc);
 /* Upml::new (src/extensions/pml.rs:209-219) with the flux hooks of
  * pml.rs:505-655 around the H and E updates.  Reproduces the reference's
  * coefficients, under which the scheme grows without bound (the reference

@@ -15,6 +15,7 @@ from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, 
                    EngineType, Engine, EndCondition, SimulationStats, Simulation,
                    ProbeTerms, voltage_probe, current_probe, voltage_integral, current_integral,
                    port_probe, LumpedPort, DrudeMaterial, LorentzMaterial, DebyeMaterial,
-                   RlcType, RlcElement, Nf2ffBox, Nf2ffResults, nf2ff_surface, PmlBoundaries)
+                   RlcType, RlcElement, Nf2ffBox, Nf2ffResults, nf2ff_surface, PmlBoundaries,
+                   PropagationDirection, Polarization, TfsfConfig)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -191,6 +191,11 @@ class SweepInstanceC(ctypes.Structure):
                 ("energy_decay_db", c_f64), ("max_timesteps", c_u64)]
 
 
+class TfsfDescC(ctypes.Structure):
+    _fields_ = [("direction", c_i32), ("polarization", c_i32), ("frequency", c_f64), ("amplitude", c_f64),
+                ("boundary_layer", c_u64), ("phase_velocity", c_f64), ("kind", c_i32), ("reserved0", c_i32)]
+
+
 class SweepResultC(ctypes.Structure):
     _fields_ = [("timesteps", c_u64), ("termination_reason", c_i32), ("status", c_i32),
                 ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64),
@@ -203,6 +208,7 @@ SIGNATURES = {
     "oems_engine_create": (c_i32, [ctypes.POINTER(OperatorDesc), ctypes.POINTER(P)]),
     "oems_engine_destroy": (None, [P]),
     "oems_release_cached_memory": (c_i32, [c_i32]),
+    "oems_engine_add_tfsf": (c_i32, [P, ctypes.POINTER(TfsfDescC)]),
     "oems_engine_run_batch": (c_i32, [P, ctypes.POINTER(BatchC), ctypes.POINTER(BatchResultC)]),
     "oems_engine_current_timestep": (c_i32, [P, ctypes.POINTER(c_u64)]),
     "oems_engine_read_fields": (c_i32, [P, PF * 3, PF * 3]),

@@ -184,6 +184,31 @@ __global__ void k_probe_dft(const DftArgs a) {
 
 __global__ void k_set_i64(long long* p, long long v) { *p = v; }
 
+// TF/SF plane injection (src/extensions/tfsf.rs:241-355): every cell of one
+// plane of one field component gets f + coef * v (add) or f - coef * v, v the
+// 1D grid's value of batch step *d_base + local (computed on the host).
+struct TfsfArgs {
+  float* f;
+  long long plane_off, s1, s2;  // first cell, strides of the two in-plane axes
+  int n1, n2;
+  float coef;
+  int add;
+  const float* samples;
+  const long long* d_base;
+  int local;
+};
+
+__global__ void k_tfsf_plane(const TfsfArgs a) {
+  const float v = a.samples[*a.d_base + a.local];
+  const float d = __fmul_rn(a.coef, v);
+  const long long n = (long long)a.n1 * a.n2;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long u = t / a.n2, w = t - u * a.n2;
+    float* p = a.f + a.plane_off + u * a.s1 + w * a.s2;
+    *p = a.add ? __fadd_rn(*p, d) : __fsub_rn(*p, d);
+  }
+}
+
 // Energy: per-block partial sums of x^2 in f64 over one array (blockIdx.y),
 // then a fixed-order final sum (deterministic run to run).
 constexpr int kEnergyBlocks = 296;
@@ -461,6 +486,21 @@ struct Nf2ffHost {
   std::unique_ptr<FdTable> tab{new FdTable};
 };
 
+// TF/SF plane source: the 1D auxiliary grid lives on the host (it does not
+// depend on the 3D fields); each batch uploads its per-step values at the
+// boundary plane: [e_inc of every step | h_inc of every step].
+struct TfsfHost {
+  bool on = false;
+  int kind = 0;  // 0 the reference's update, 1 corrected
+  int prop = 0, e_axis = 1, h_axis = 2;
+  long long pos = 10;
+  double freq = 0.0, amp = 0.0, v = 0.0;
+  std::vector<float> e1d, h1d;
+  uint64_t t = 0;
+  uint64_t cap = 0;  // steps per half of `samples`
+  DevBuf<float> samples;
+};
+
 struct UpmlHost {
   bool on = false;
   UpmlArgs e{}, h{};                 // E (voltage) and H (current) halves
@@ -493,6 +533,7 @@ struct oems_engine {
   std::vector<oems::DispHost> disp;
   oems::RlcHost rlc;
   oems::UpmlHost upml;
+  oems::TfsfHost tfsf;
   std::vector<oems::FieldDftHost> fdumps;
   std::vector<oems::Nf2ffHost> boxes;
 
@@ -978,7 +1019,7 @@ static cudaError_t launch_post_e(oems_engine* en) {
 
 static int ext_kernels(const oems_engine* en) {
   return (en->mur.on ? 3 : 0) + (en->upml.on ? 4 : 0) + (int)en->disp.size() + second_order_disp(en) +
-         (en->rlc.q.empty() ? 0 : 1);
+         (en->rlc.q.empty() ? 0 : 1) + (en->tfsf.on ? 2 : 0);
 }
 
 static int kernels_per_step(const oems_engine* en) {
@@ -1005,9 +1046,101 @@ static cudaError_t launch_h_step(oems_engine* en) {
   return cudaSuccess;
 }
 
+// One step of the TF/SF 1D grid (src/extensions/tfsf.rs:204-238), f32 as
+// the reference: H update, sin source at the first H node, E update, Mur end.
+static void tfsf_step_1d(TfsfHost& T, double dt, double dx) {
+  constexpr double kMu0 = 1.256637062e-6, kEps0 = 8.854187817e-12, kPi = 3.14159265358979323846;
+  const size_t len = T.h1d.size();
+  for (size_t i = 0; i + 1 < len; ++i) {
+    const float db = (float)(-(dt / (kMu0 * dx)));
+    T.h1d[i] += db * (T.e1d[i + 1] - T.e1d[i]);
+  }
+  const double t = (double)T.t * dt;
+  const double eta = std::sqrt(kMu0 / kEps0);
+  T.h1d[0] = (float)((T.amp / eta) * std::sin(2.0 * kPi * T.freq * t));
+  for (size_t i = 1; i < len; ++i) {
+    const float cb = (float)(dt / (kEps0 * dx));
+    T.e1d[i] += cb * (T.h1d[i] - T.h1d[i - 1]);
+  }
+  const float coeff = (float)((T.v * dt - dx) / (T.v * dt + dx));
+  T.e1d[len - 1] = coeff * T.e1d[len - 2];
+  T.t += 1;
+}
+
+// Corrected 1D step (kind 1): hard E source at node 0 at time n, H to
+// n + 1/2, E to n + 1 with the wave equation's sign (the reference's E
+// update has the opposite sign and grows exponentially), first-order Mur at
+// the last node.  e_inc: E at node pos, time n; h_inc: H at pos - 1/2.
+static void tfsf_step_1d_fixed(TfsfHost& T, double dt, double dx, float* e_inc, float* h_inc) {
+  constexpr double kMu0 = 1.256637062e-6, kEps0 = 8.854187817e-12, kPi = 3.14159265358979323846;
+  const size_t len = T.e1d.size();
+  const float db = (float)(-(dt / (kMu0 * dx))), cb = (float)(dt / (kEps0 * dx));
+  T.e1d[0] = (float)(T.amp * std::sin(2.0 * kPi * T.freq * ((double)T.t * dt)));
+  *e_inc = T.e1d[T.pos];
+  for (size_t i = 0; i + 1 < len; ++i) T.h1d[i] += db * (T.e1d[i + 1] - T.e1d[i]);
+  *h_inc = T.h1d[T.pos - 1];
+  const float en1 = T.e1d[len - 2], en = T.e1d[len - 1];
+  for (size_t i = 1; i < len; ++i) T.e1d[i] -= cb * (T.h1d[i] - T.h1d[i - 1]);
+  const float coeff = (float)((T.v * dt - dx) / (T.v * dt + dx));
+  T.e1d[len - 1] = en1 + coeff * (T.e1d[len - 2] - en);
+  T.t += 1;
+}
+
+// One step of the 1D grid of either kind; the values the two planes get.
+static void tfsf_advance(TfsfHost& T, double dt, double dx, float* e_inc, float* h_inc) {
+  if (T.kind == 1) {
+    tfsf_step_1d_fixed(T, dt, dx, e_inc, h_inc);
+    return;
+  }
+  tfsf_step_1d(T, dt, dx);
+  *e_inc = (size_t)T.pos < T.e1d.size() ? T.e1d[T.pos] : 0.0f;
+  *h_inc = (size_t)T.pos < T.h1d.size() ? T.h1d[T.pos] : 0.0f;
+}
+
+// TF/SF hook of batch step `local`: before H (h_pre) or before E.  Kind 0:
+// both planes at pos, h - db e_inc and e + cb h_inc (the reference).  Kind
+// 1: the scattered-side H plane pos - 1 gets -Db E_inc (+dt/(mu0 dx) E_inc
+// for Transverse1, whose 1D H is the 3D H component, minus that for
+// Transverse2), the total-side E plane pos gets +Cb H_inc on the cells the
+// E update writes (transverse indices >= 1).
+static cudaError_t launch_tfsf(oems_engine* en, bool h_pre, int local) {
+  if (!en->tfsf.on) return cudaSuccess;
+  const TfsfHost& T = en->tfsf;
+  constexpr double kMu0 = 1.256637062e-6, kEps0 = 8.854187817e-12;
+  const double dx = en->delta[T.prop];
+  TfsfArgs a{};
+  a.f = h_pre ? en->H(T.h_axis) : en->E(T.e_axis);
+  const long long nzp = en->g.nzp, ny = en->ny;
+  const long long stride[3] = {ny * nzp, nzp, 1};
+  const int n[3] = {en->nx, en->ny, en->nz};
+  const int a1 = T.prop == 0 ? 1 : 0, a2 = T.prop == 2 ? 1 : 2;
+  const long long plane = (T.kind == 1 && h_pre) ? T.pos - 1 : T.pos;
+  const int first = (T.kind == 1 && !h_pre) ? 1 : 0;
+  a.plane_off = plane * stride[T.prop] + first * (stride[a1] + stride[a2]);
+  a.s1 = stride[a1];
+  a.s2 = stride[a2];
+  a.n1 = n[a1] - first;
+  a.n2 = n[a2] - first;
+  if (T.kind == 1) {
+    a.coef = h_pre ? (float)(en->dt / (kMu0 * dx)) : (float)(en->dt / (kEps0 * dx));
+    a.add = h_pre ? (T.e_axis == (T.prop + 1) % 3 ? 1 : 0) : 1;
+  } else {
+    a.coef = h_pre ? (float)(-(en->dt / (kMu0 * dx))) : (float)(en->dt / (kEps0 * dx));
+    a.add = h_pre ? 0 : 1;
+  }
+  a.samples = T.samples.p + (h_pre ? 0 : T.cap);
+  a.d_base = en->d_base.p;
+  a.local = local;
+  const long long cells = (long long)a.n1 * a.n2;
+  k_tfsf_plane<<<(int)std::min<long long>((cells + 255) / 256, 1184), 256, 0, en->stream>>>(a);
+  return cudaGetLastError();
+}
+
 static oems_status launch_steps_direct(oems_engine* en, int steps) {
   for (int s = 0; s < steps; ++s) {
+    OEMS_CUDA(launch_tfsf(en, true, s));
     OEMS_CUDA(launch_h_step(en));
+    OEMS_CUDA(launch_tfsf(en, false, s));
     OEMS_CUDA(launch_pre_e(en));
     OEMS_CUDA(launch_e(en));
     OEMS_CUDA(launch_post_e(en));
@@ -1028,11 +1161,13 @@ static oems_status launch_steps_profiled(oems_engine* en, int steps) {
     const int n = std::min(kChunk, steps - s0);
     for (int s = 0; s < n; ++s) {
       cudaEvent_t* ev = &en->prof_ev[4 * s];
+      OEMS_CUDA(launch_tfsf(en, true, s0 + s));
       if (en->upml.on) OEMS_CUDA(launch_upml(en, true, true));
       OEMS_CUDA(cudaEventRecord(ev[0], en->stream));
       OEMS_CUDA(launch_h(en));
       OEMS_CUDA(cudaEventRecord(ev[1], en->stream));
       if (en->upml.on) OEMS_CUDA(launch_upml(en, true, false));
+      OEMS_CUDA(launch_tfsf(en, false, s0 + s));
       OEMS_CUDA(launch_pre_e(en));
       OEMS_CUDA(cudaEventRecord(ev[2], en->stream));
       OEMS_CUDA(launch_e(en));
@@ -1085,7 +1220,7 @@ static oems_status get_graph(oems_engine* en, int steps, cudaGraphExec_t* out) {
 
 // Runs batch steps [base, base + steps).
 static oems_status run_span(oems_engine* en, long long base, int steps) {
-  if (need_post(en)) {
+  if (need_post(en) || en->tfsf.on) {
     k_set_i64<<<1, 1, 0, en->stream>>>(en->d_base.p, base);
     OEMS_CUDA(cudaGetLastError());
     en->last_launches += 1;
@@ -1605,6 +1740,27 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
   }
   for (FieldDftHost& d : en->fdumps) OEMS_TRY(fill_twiddles(en, d.tab.get(), d.freqs, d.interval, steps));
   for (Nf2ffHost& x : en->boxes) OEMS_TRY(fill_twiddles(en, x.tab.get(), x.freqs, x.interval, steps));
+  // TF/SF: this batch's 1D-grid values; the state is kept to replay a batch
+  // that ends early
+  std::vector<float> tf_e0, tf_h0;
+  uint64_t tf_t0 = 0;
+  if (en->tfsf.on && steps > 0) {
+    TfsfHost& T = en->tfsf;
+    tf_e0 = T.e1d;
+    tf_h0 = T.h1d;
+    tf_t0 = T.t;
+    if (steps > T.cap) {
+      T.cap = steps;
+      OEMS_CUDA(T.samples.ensure(2 * T.cap));
+      en->graph_epoch++;  // the h_inc half moved
+    }
+    std::vector<float> smp(2 * T.cap, 0.0f);
+    const double dx = en->delta[T.prop];
+    for (uint64_t q = 0; q < steps; ++q) tfsf_advance(T, en->dt, dx, &smp[q], &smp[T.cap + q]);
+    OEMS_CUDA(cudaMemcpyAsync(T.samples.p, smp.data(), smp.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              en->stream));
+    OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  }
   const uint64_t si = b->sample_interval, ci = b->check_interval;
   const bool has_decay = b->has_energy_decay_db != 0;
   // worst-case number of energy samples this batch can take
@@ -1721,6 +1877,14 @@ static oems_status run_batch(oems_engine* en, const oems_batch* b, oems_batch_re
   cudaEventElapsedTime(&ms, en->ev0, en->ev1);
   en->last_device_seconds = ms * 1e-3;
   en->timestep = t0 + executed;
+  if (en->tfsf.on && executed < steps) {
+    TfsfHost& T = en->tfsf;
+    T.e1d = tf_e0;
+    T.h1d = tf_h0;
+    T.t = tf_t0;
+    float e_inc, h_inc;
+    for (uint64_t q = 0; q < executed; ++q) tfsf_advance(T, en->dt, en->delta[T.prop], &e_inc, &h_inc);
+  }
   en->traces_steps = executed;
   r->timesteps_executed = executed;
   r->termination_reason = reason;
@@ -2016,6 +2180,9 @@ oems_status oems_engine_reset(oems_engine* engine) {
   for (auto& x : engine->boxes)
     OEMS_CUDA(cudaMemsetAsync(x.acc->p, 0, x.acc->n * sizeof(double), engine->stream));
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  std::fill(engine->tfsf.e1d.begin(), engine->tfsf.e1d.end(), 0.0f);
+  std::fill(engine->tfsf.h1d.begin(), engine->tfsf.h1d.end(), 0.0f);
+  engine->tfsf.t = 0;
   engine->timestep = 0;
   engine->traces_steps = 0;
   return OEMS_OK;
@@ -2596,6 +2763,37 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
     U.h.f[c] = engine->H(c);
   }
   U.on = true;
+  engine->graph_epoch++;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_add_tfsf(oems_engine* engine, const oems_tfsf_desc* d) {
+  if (!engine || !d) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (engine->storage) return fail(OEMS_ERR_CONFIG, "TF/SF needs float field storage");
+  if (engine->tfsf.on) return fail(OEMS_ERR_CONFIG, "TF/SF already attached");
+  if (d->direction < 0 || d->direction > 5) return fail(OEMS_ERR_CONFIG, "TF/SF direction must be 0..5");
+  if (d->polarization < 0 || d->polarization > 1) return fail(OEMS_ERR_CONFIG, "TF/SF polarization must be 0 or 1");
+  if (!std::isfinite(d->frequency) || !std::isfinite(d->amplitude))
+    return fail(OEMS_ERR_CONFIG, "TF/SF frequency and amplitude must be finite");
+  TfsfHost& T = engine->tfsf;
+  const int prop = d->direction / 2;
+  const int n[3] = {engine->nx, engine->ny, engine->nz};
+  if (d->boundary_layer >= (uint64_t)n[prop]) return fail(OEMS_ERR_CONFIG, "TF/SF boundary layer outside the grid");
+  if (d->kind < 0 || d->kind > 1) return fail(OEMS_ERR_CONFIG, "TF/SF kind must be 0 or 1");
+  if (d->kind == 1 && (d->boundary_layer < 1 || d->direction % 2 != 0))
+    return fail(OEMS_ERR_CONFIG, "the corrected TF/SF needs a positive direction and boundary_layer >= 1");
+  T.kind = d->kind;
+  T.prop = prop;
+  T.e_axis = d->polarization == 0 ? (prop + 1) % 3 : (prop + 2) % 3;
+  T.h_axis = d->polarization == 0 ? (prop + 2) % 3 : (prop + 1) % 3;
+  T.pos = (long long)d->boundary_layer;
+  T.freq = d->frequency;
+  T.amp = d->amplitude;
+  T.v = d->phase_velocity > 0.0 ? d->phase_velocity : 299792458.0;
+  T.e1d.assign(n[prop] + 1, 0.0f);
+  T.h1d.assign(n[prop] + 1, 0.0f);
+  T.t = 0;
+  T.on = true;
   engine->graph_epoch++;
   return OEMS_OK;
 }

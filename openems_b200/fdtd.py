@@ -145,6 +145,55 @@ class CpmlBoundaries:
         return d
 
 
+class PropagationDirection(enum.IntEnum):
+    """PropagationDirection (src/extensions/tfsf.rs:11-41)."""
+    XPlus = 0
+    XMinus = 1
+    YPlus = 2
+    YMinus = 3
+    ZPlus = 4
+    ZMinus = 5
+
+    def axis(self) -> int:
+        return int(self) // 2
+
+    def is_positive(self) -> bool:
+        return int(self) % 2 == 0
+
+
+class Polarization(enum.IntEnum):
+    """Polarization (src/extensions/tfsf.rs:44-50)."""
+    Transverse1 = 0
+    Transverse2 = 1
+
+
+@dataclass
+class TfsfConfig:
+    """TfsfConfig (src/extensions/tfsf.rs:54-103): defaults Transverse1,
+    boundary layer 10, phase velocity c0.  corrected=False reproduces the
+    reference's update (its 1D grid grows exponentially); True is the stable
+    plane-wave source (positive directions, boundary_layer >= 1)."""
+
+    direction: PropagationDirection
+    frequency: float
+    amplitude: float
+    polarization: Polarization = Polarization.Transverse1
+    boundary_layer: int = 10
+    phase_velocity: Optional[float] = None
+    corrected: bool = False
+
+    def to_c(self) -> N.TfsfDescC:
+        d = N.TfsfDescC()
+        d.direction = int(self.direction)
+        d.polarization = int(self.polarization)
+        d.frequency = float(self.frequency)
+        d.amplitude = float(self.amplitude)
+        d.boundary_layer = int(self.boundary_layer)
+        d.phase_velocity = float(self.phase_velocity or 0.0)
+        d.kind = 1 if self.corrected else 0
+        return d
+
+
 @dataclass
 class MurAbcConfig:
     """MurAbcConfig (src/extensions/mur_abc.rs:13-58); order 2 selects the
@@ -929,6 +978,11 @@ class Engine:
     def add_cpml(self, cpml: CpmlBoundaries):
         d = cpml.to_c()
         N.check(N.lib().oems_engine_add_cpml(self._h, ctypes.byref(d)))
+
+    def add_tfsf(self, cfg: TfsfConfig):
+        """TF/SF plane source (TfsfBoundary)."""
+        d = cfg.to_c()
+        N.check(N.lib().oems_engine_add_tfsf(self._h, ctypes.byref(d)))
 
     def add_mur(self, mur: MurAbcConfig):
         d = mur.to_c()

@@ -90,6 +90,8 @@ def lib() -> ctypes.CDLL:
         L.orc_cpml_profile.argtypes = [P, I32, P]
         L.orc_enable_mur.restype = I32
         L.orc_enable_mur.argtypes = [P, P, I32, D]
+        L.orc_enable_tfsf.restype = I32
+        L.orc_enable_tfsf.argtypes = [P, I32, I32, D, D, I64, D, I32]
         L.orc_add_dispersive.restype = I32
         L.orc_add_dispersive.argtypes = [P, I32, P, D, P, I64]
         L.orc_add_lumped_rlc.restype = I32
@@ -261,6 +263,13 @@ class OracleSim:
                                    kappa_max)
         if rc != 0:
             raise ValueError(f"invalid CPML configuration ({rc})")
+
+    def enable_tfsf(self, direction, polarization, frequency, amplitude, boundary_layer=10, phase_velocity=0.0,
+                    kind=0):
+        rc = lib().orc_enable_tfsf(self._h, int(direction), int(polarization), float(frequency),
+                                   float(amplitude), int(boundary_layer), float(phase_velocity), int(kind))
+        if rc != 0:
+            raise ValueError(f"TF/SF configuration rejected ({rc})")
 
     def enable_mur(self, enabled=(1,) * 6, order=1, phase_velocity=0.0):
         e = np.ascontiguousarray([int(bool(v)) for v in enabled], dtype=np.int32)

@@ -864,6 +864,126 @@ struct Sim {
     *h = sumsq(H[0]) + sumsq(H[1]) + sumsq(H[2]);
   }
 
+  // TF/SF plane source as the reference (src/extensions/tfsf.rs:115-355):
+  // a 1D auxiliary grid in f32 driven by sin at its first H node and closed
+  // by a first-order Mur end; before every H update the whole plane `pos`
+  // of the H component gets h - db e_inc, before every E update the plane
+  // of the E component gets e + cb h_inc (the 1D values at pos).
+  struct Tfsf {
+    bool on = false;
+    int kind = 0;  // 0 the reference's update, 1 corrected (see tfsf_pre_h)
+    int prop = 0, e_axis = 1, h_axis = 2;
+    int64_t pos = 10;
+    double freq = 0.0, amp = 0.0, v = kC0;
+    std::vector<float> e1d, h1d;
+    uint64_t t = 0;
+  } tf;
+
+  void tfsf_step_1d() {
+    const double dx = delta[tf.prop];
+    const size_t len = tf.h1d.size();
+    for (size_t i = 0; i + 1 < len; ++i) {
+      const float db = (float)(-(dt / (kMu0 * dx)));
+      tf.h1d[i] += db * (tf.e1d[i + 1] - tf.e1d[i]);
+    }
+    const double t = (double)tf.t * dt;
+    const double eta = std::sqrt(kMu0 / kEps0);
+    tf.h1d[0] = (float)((tf.amp / eta) * std::sin(2.0 * kPi * tf.freq * t));
+    for (size_t i = 1; i < len; ++i) {
+      const float cb = (float)(dt / (kEps0 * dx));
+      tf.e1d[i] += cb * (tf.h1d[i] - tf.h1d[i - 1]);
+    }
+    const float coeff = (float)((tf.v * dt - dx) / (tf.v * dt + dx));
+    tf.e1d[len - 1] = coeff * tf.e1d[len - 2];
+  }
+
+  // Corrected 1D step: hard E source at node 0 at time n, H to n + 1/2,
+  // E to n + 1 with the sign of the wave equation (the reference's E update
+  // has the opposite sign and grows exponentially), first-order Mur at the
+  // last node.  e_inc: E at node pos, time n; h_inc: H at pos - 1/2, n + 1/2.
+  void tfsf_step_1d_fixed(float& e_inc, float& h_inc) {
+    const double dx = delta[tf.prop];
+    const size_t len = tf.e1d.size();
+    const float db = (float)(-(dt / (kMu0 * dx))), cb = (float)(dt / (kEps0 * dx));
+    tf.e1d[0] = (float)(tf.amp * std::sin(2.0 * kPi * tf.freq * ((double)tf.t * dt)));
+    e_inc = tf.e1d[tf.pos];
+    for (size_t i = 0; i + 1 < len; ++i) tf.h1d[i] += db * (tf.e1d[i + 1] - tf.e1d[i]);
+    h_inc = tf.h1d[tf.pos - 1];
+    const float en1 = tf.e1d[len - 2], en = tf.e1d[len - 1];
+    for (size_t i = 1; i < len; ++i) tf.e1d[i] -= cb * (tf.h1d[i] - tf.h1d[i - 1]);
+    const float coeff = (float)((tf.v * dt - dx) / (tf.v * dt + dx));
+    tf.e1d[len - 1] = en1 + coeff * (tf.e1d[len - 2] - en);
+    tf.t += 1;
+  }
+  float tf_h_inc = 0.0f;  // kind 1: H sample of the current step for the E correction
+
+  // every cell of plane `plane` along the propagation axis of component
+  // array f: f = f + coef * v (add) or f - coef * v
+  // (first = 1 skips the index-0 lines the E update never writes)
+  void tfsf_plane(std::vector<T>& f, T coef, T val, bool add, int64_t plane, int64_t first = 0) {
+    const int64_t nn[3] = {nx, ny, nz};
+    int64_t lo[3] = {first, first, first}, hi[3] = {nn[0], nn[1], nn[2]};
+    lo[tf.prop] = plane;
+    hi[tf.prop] = plane + 1;
+    for (int64_t i = lo[0]; i < hi[0]; ++i)
+      for (int64_t j = lo[1]; j < hi[1]; ++j)
+        for (int64_t k = lo[2]; k < hi[2]; ++k) {
+          T& x = f[(i * ny + j) * nz + k];
+          x = add ? x + coef * val : x - coef * val;
+        }
+  }
+
+  // Kind 1 corrections: the scattered-side H plane pos - 1 sees total E at
+  // pos, so it gets -Db E_inc (= +dt/(mu0 dx) E_inc for Transverse1, where
+  // the 1D H is the 3D H component; -dt/(mu0 dx) E_inc for Transverse2,
+  // where it is minus it); the total-side E plane pos sees scattered H at
+  // pos - 1, so it gets +Cb H_inc.
+  void tfsf_pre_h() {
+    if (tf.kind == 1) {
+      float e_inc = 0.0f;
+      tfsf_step_1d_fixed(e_inc, tf_h_inc);
+      const float c = (float)(dt / (kMu0 * delta[tf.prop]));
+      tfsf_plane(H[tf.h_axis], (T)c, (T)e_inc, tf.e_axis == (tf.prop + 1) % 3, tf.pos - 1);
+      return;
+    }
+    tfsf_step_1d();
+    const float e_inc = (size_t)tf.pos < tf.e1d.size() ? tf.e1d[tf.pos] : 0.0f;
+    const float db = (float)(-(dt / (kMu0 * delta[tf.prop])));
+    tfsf_plane(H[tf.h_axis], (T)db, (T)e_inc, false, tf.pos);
+  }
+
+  void tfsf_pre_e() {
+    const float cb = (float)(dt / (kEps0 * delta[tf.prop]));
+    if (tf.kind == 1) {
+      tfsf_plane(E[tf.e_axis], (T)cb, (T)tf_h_inc, true, tf.pos, 1);
+      return;
+    }
+    const float h_inc = (size_t)tf.pos < tf.h1d.size() ? tf.h1d[tf.pos] : 0.0f;
+    tfsf_plane(E[tf.e_axis], (T)cb, (T)h_inc, true, tf.pos);
+    tf.t += 1;
+  }
+
+  int enable_tfsf(int direction, int polarization, double freq, double amp, int64_t layer, double vphase,
+                  int kind) {
+    if (direction < 0 || direction > 5 || polarization < 0 || polarization > 1 || kind < 0 || kind > 1) return -1;
+    tf.prop = direction / 2;
+    const int64_t nn[3] = {nx, ny, nz};
+    if (layer < 0 || layer >= nn[tf.prop]) return -2;
+    if (kind == 1 && (layer < 1 || direction % 2 != 0)) return -3;
+    tf.kind = kind;
+    tf.on = true;
+    tf.e_axis = polarization == 0 ? (tf.prop + 1) % 3 : (tf.prop + 2) % 3;
+    tf.h_axis = polarization == 0 ? (tf.prop + 2) % 3 : (tf.prop + 1) % 3;
+    tf.pos = layer;
+    tf.freq = freq;
+    tf.amp = amp;
+    tf.v = vphase > 0.0 ? vphase : kC0;
+    tf.e1d.assign(nn[tf.prop] + 1, 0.0f);
+    tf.h1d.assign(nn[tf.prop] + 1, 0.0f);
+    tf.t = 0;
+    return 0;
+  }
+
   // src/fdtd/basic_engine.rs:56-163
   int run_batch(uint64_t num_steps, uint64_t sample_interval, bool track_peak,
                 uint64_t check_interval, bool has_decay, double decay_db, double peak0,
@@ -876,9 +996,11 @@ struct Sim {
     traces.clear();
     for (uint64_t step = 0; step < num_steps; ++step) {
       uint64_t cur = timestep;
+      if (tf.on) tfsf_pre_h();
       if (!upml.empty()) upml_hook(true, true);
       update_h();
       if (!upml.empty()) upml_hook(true, false);
+      if (tf.on) tfsf_pre_e();
       if (!mur.empty()) mur_pre();
       if (!disp.empty()) capture_dispersive();
       if (!upml.empty()) upml_hook(false, true);
@@ -1071,6 +1193,9 @@ void orc_reset(orc_sim* s) {
         std::fill(F.ob[t].begin(), F.ob[t].end(), T(0));
         std::fill(F.os[t].begin(), F.os[t].end(), T(0));
       }
+    std::fill(S->tf.e1d.begin(), S->tf.e1d.end(), 0.0f);
+    std::fill(S->tf.h1d.begin(), S->tf.h1d.end(), 0.0f);
+    S->tf.t = 0;
     S->timestep = 0;
   });
 }
@@ -1404,6 +1529,14 @@ int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, doubl
   if (order != 1 && order != 2) return -2;
   int rc = 0;
   DISPATCH(s, rc = S->enable_mur(enabled6, order, phase_velocity));
+  return rc;
+}
+
+int32_t orc_enable_tfsf(orc_sim* s, int32_t direction, int32_t polarization, double frequency, double amplitude,
+                        int64_t boundary_layer, double phase_velocity, int32_t kind) {
+  int rc = 0;
+  DISPATCH(s, rc = S->enable_tfsf(direction, polarization, frequency, amplitude, boundary_layer, phase_velocity,
+                                  kind));
   return rc;
 }
 

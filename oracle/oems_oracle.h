@@ -170,6 +170,14 @@ int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order
 void orc_upml_kappa(const orc_sim* s, int32_t comp, int32_t dir, const int64_t* pos3, int32_t is_min,
                     int64_t layers, double width, double smax, double m, double* kv, double* ki);
 int32_t orc_enable_mur(orc_sim* s, const int32_t* enabled6, int32_t order, double phase_velocity);
+/* TF/SF plane source (src/extensions/tfsf.rs:115-355): direction 0 +x 1 -x
+ * 2 +y 3 -y 4 +z 5 -z (kind 0: only the axis matters, as in the
+ * reference), polarization 0 / 1 (Transverse1 / 2), phase_velocity <= 0:
+ * c0; kind 0 the reference's update (its 1D grid grows exponentially), 1 the
+ * corrected one (positive directions, boundary_layer >= 1).  -1 bad enum,
+ * -2 boundary_layer outside the grid, -3 kind 1 limits. */
+int32_t orc_enable_tfsf(orc_sim* s, int32_t direction, int32_t polarization, double frequency, double amplitude,
+                        int64_t boundary_layer, double phase_velocity, int32_t kind);
 
 /* Dispersive material on a list of cells (src/extensions/dispersive.rs),
  * applied after the E update, all three components per cell:

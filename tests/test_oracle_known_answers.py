@@ -243,3 +243,80 @@ def test_storage_rounding_restatement():
     # half storage of the same update stays within a few half ulps per step
     a = run_stored(co, f, 5, store="f16")
     assert np.abs(a - run(co, f, 5)).max() < 5 * 2 ** -11 * np.abs(f).max() * 8
+
+
+def _tfsf_samples(n_steps, length, pos, dt, dx, freq, amp, v=299792458.0):
+    """The reference's TF/SF 1D auxiliary grid (src/extensions/tfsf.rs:204-238)
+    restated in numpy float32: (e_inc, h_inc) at `pos` after each step."""
+    EPS0, MU0 = 8.854187817e-12, 1.256637062e-6
+    e, h = np.zeros(length, np.float32), np.zeros(length, np.float32)
+    db, cb = np.float32(-(dt / (MU0 * dx))), np.float32(dt / (EPS0 * dx))
+    coeff = np.float32((v * dt - dx) / (v * dt + dx))
+    eta = np.sqrt(MU0 / EPS0)
+    out = []
+    for t in range(n_steps):
+        for i in range(length - 1):
+            h[i] = h[i] + db * (e[i + 1] - e[i])
+        h[0] = np.float32((amp / eta) * np.sin(2.0 * np.pi * freq * (t * dt)))
+        for i in range(1, length):
+            e[i] = e[i] + cb * (h[i] - h[i - 1])
+        e[length - 1] = coeff * e[length - 2]
+        out.append((e[pos], h[pos]))
+    return out
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_tfsf_plane_injection_known_answer(precision):
+    """With Ca = Da = 1 and Cb = Db = 0 the Yee update leaves the fields as
+    they are, so after n steps plane `pos` of the H component holds
+    -sum db e_inc and that of the E component sum cb h_inc (f32 steps of the
+    numpy restatement of the 1D grid); nothing else changes."""
+    n = (9, 7, 12)
+    dt, dx = 1e-12, 1e-3
+    s = oracle.OracleSim(*n, dt, (dx,) * 3, precision=precision)
+    co = np.zeros((12,) + n)
+    co[0:3] = 1.0
+    co[6:9] = 1.0
+    s.set_coefficients(co.astype(np.float32 if precision == 32 else np.float64))
+    s.enable_tfsf(4, 0, 20e9, 2.0, boundary_layer=5)  # +z, E along x, H along y
+    s.run_batch(40)
+    f = s.fields()
+    samples = _tfsf_samples(40, n[2] + 1, 5, dt, dx, 20e9, 2.0)
+    T = np.float32 if precision == 32 else np.float64
+    db, cb = T(np.float32(-(dt / (1.256637062e-6 * dx)))), T(np.float32(dt / (8.854187817e-12 * dx)))
+    hy, ex = T(0), T(0)
+    for e_inc, h_inc in samples:
+        hy = hy - db * T(e_inc)
+        ex = ex + cb * T(h_inc)
+    assert np.all(f[4][:, :, 5] == hy) and np.all(f[0][:, :, 5] == ex) and hy != 0 and ex != 0
+    rest = f.copy()
+    rest[4][:, :, 5] = 0
+    rest[0][:, :, 5] = 0
+    assert np.all(rest == 0)
+    with pytest.raises(ValueError):
+        oracle.OracleSim(*n, dt, (dx,) * 3).enable_tfsf(0, 0, 1e9, 1.0, boundary_layer=9)
+
+
+@pytest.mark.parametrize("polarization,e_axis", [(0, 1), (1, 2)])
+def test_corrected_tfsf_separates_total_and_scattered_fields(polarization, e_axis):
+    """The corrected TF/SF source (kind 1) on a grid with CPML on every face,
+    so that a plane wave uniform across y and z is an exact solution: before
+    any wave comes back from the domain's ends, the scattered region (x <
+    boundary) stays below 1e-3 of the amplitude and the total region carries
+    the wave at the amplitude (numerical dispersion and switch-on within 20%)."""
+    nx, ny, nz = 120, 24, 24
+    lines = [oracle.uniform_lines(n, 1e-3) for n in (nx, ny, nz)]
+    dt, d3 = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(nx, ny, nz, dt, d3, threads=8)
+    s.enable_cpml((6,) * 6)
+    s.enable_tfsf(0, polarization, 15e9, 1.0, boundary_layer=20, kind=1)
+    worst_scattered, total = 0.0, []
+    for _ in range(5):
+        s.run_batch(60)
+        e = s.fields()[e_axis][:, ny // 2, nz // 2]
+        worst_scattered = max(worst_scattered, float(np.abs(e[8:19]).max()))
+        total.append(float(np.abs(e[25:100]).max()))
+    assert worst_scattered < 1e-3
+    assert 0.9 < max(total[1:]) < 1.2
+    with pytest.raises(ValueError):  # the corrected source needs a positive direction
+        oracle.OracleSim(nx, ny, nz, dt, d3).enable_tfsf(1, 0, 15e9, 1.0, boundary_layer=20, kind=1)
