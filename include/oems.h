@@ -466,6 +466,37 @@ OEMS_API oems_status oems_engine_kernel_profile(const oems_engine* engine, doubl
                                                 uint64_t* h_launches, double* e_seconds,
                                                 uint64_t* e_launches);
 
+/* ---- cylindrical engine (src/fdtd/cylindrical.rs:394-638) ------------- */
+
+/* CylindricalOperator's per-cell coefficients (rho-major, z fastest, n_rho x
+ * n_alpha x n_z floats each): vi[c] = dt / (eps0 area), iv[c] = dt / (mu0
+ * length) of component c (rho, alpha, z); vv = ii = 1. */
+typedef struct oems_cyl_engine oems_cyl_engine;
+typedef struct oems_cyl_desc {
+  uint64_t n_rho, n_alpha, n_z;
+  int32_t closed_alpha; /* alpha spans 2 pi: neighbours wrap around */
+  int32_t r0_included;  /* the first rho line is R = 0 (needs n_rho >= 2) */
+  double dt;
+  const float* vi[3];
+  const float* iv[3];
+  int32_t device;       /* < 0: current */
+  int32_t reserved0;
+} oems_cyl_desc;
+/* CylindricalEngine::new; fields start at zero. */
+OEMS_API oems_status oems_cyl_create(const oems_cyl_desc* desc, oems_cyl_engine** out);
+OEMS_API void oems_cyl_destroy(oems_cyl_engine* engine);
+/* `steps` x step(): voltage pass, the R = 0 fix-up, current pass. */
+OEMS_API oems_status oems_cyl_step(oems_cyl_engine* engine, uint64_t steps);
+/* e[c], h[c]: host buffers of n_rho * n_alpha * n_z floats. */
+OEMS_API oems_status oems_cyl_read_fields(oems_cyl_engine* engine, float* const e[3], float* const h[3]);
+OEMS_API oems_status oems_cyl_write_fields(oems_cyl_engine* engine, const float* const e[3],
+                                           const float* const h[3]);
+OEMS_API oems_status oems_cyl_reset(oems_cyl_engine* engine);
+/* Device time (CUDA events on the engine's stream) of the last oems_cyl_step. */
+OEMS_API oems_status oems_cyl_last_step_ms(const oems_cyl_engine* engine, float* ms);
+/* timestep() and time() (the sum of dt over the steps, as the reference). */
+OEMS_API oems_status oems_cyl_time(const oems_cyl_engine* engine, uint64_t* timestep, double* time);
+
 OEMS_API const char* oems_status_string(oems_status status);
 /* Detail of the last failure on the calling thread ("" if none). */
 OEMS_API const char* oems_last_error_message(void);

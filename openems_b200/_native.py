@@ -196,6 +196,12 @@ class TfsfDescC(ctypes.Structure):
                 ("boundary_layer", c_u64), ("phase_velocity", c_f64), ("kind", c_i32), ("reserved0", c_i32)]
 
 
+class CylDescC(ctypes.Structure):
+    _fields_ = [("n_rho", c_u64), ("n_alpha", c_u64), ("n_z", c_u64), ("closed_alpha", c_i32),
+                ("r0_included", c_i32), ("dt", c_f64), ("vi", PF * 3), ("iv", PF * 3), ("device", c_i32),
+                ("reserved0", c_i32)]
+
+
 class SweepResultC(ctypes.Structure):
     _fields_ = [("timesteps", c_u64), ("termination_reason", c_i32), ("status", c_i32),
                 ("final_decay_db", c_f64), ("device_seconds", c_f64), ("cells", c_f64),
@@ -209,6 +215,14 @@ SIGNATURES = {
     "oems_engine_destroy": (None, [P]),
     "oems_release_cached_memory": (c_i32, [c_i32]),
     "oems_engine_add_tfsf": (c_i32, [P, ctypes.POINTER(TfsfDescC)]),
+    "oems_cyl_create": (c_i32, [ctypes.POINTER(CylDescC), ctypes.POINTER(P)]),
+    "oems_cyl_destroy": (None, [P]),
+    "oems_cyl_step": (c_i32, [P, c_u64]),
+    "oems_cyl_read_fields": (c_i32, [P, PF * 3, PF * 3]),
+    "oems_cyl_write_fields": (c_i32, [P, PF * 3, PF * 3]),
+    "oems_cyl_reset": (c_i32, [P]),
+    "oems_cyl_time": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_f64)]),
+    "oems_cyl_last_step_ms": (c_i32, [P, ctypes.POINTER(c_f32)]),
     "oems_engine_run_batch": (c_i32, [P, ctypes.POINTER(BatchC), ctypes.POINTER(BatchResultC)]),
     "oems_engine_current_timestep": (c_i32, [P, ctypes.POINTER(c_u64)]),
     "oems_engine_read_fields": (c_i32, [P, PF * 3, PF * 3]),
