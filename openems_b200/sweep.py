@@ -137,11 +137,72 @@ class Sweep:
         return wall.value, cs.value
 
 
+# ---------------------------------------------------------------------------
+# several GPUs: instances split across ranks, results gathered once
+# ---------------------------------------------------------------------------
+
+
+def instance_cost(dims) -> float:
+    """Relative cost of one instance: cells x (nx + ny + nz), since the
+    steps to energy decay grow with the time light needs to cross the grid."""
+    nx, ny, nz = dims
+    return float(nx) * ny * nz * (nx + ny + nz)
+
+
+def shard_instances(costs, world: int):
+    """Instance indices per rank, longest first onto the least-loaded rank
+    (ties to the lower index): deterministic, so every rank computes the
+    same split without communicating.  Each list is in ascending order."""
+    if world < 1:
+        raise N.ConfigError("world size must be at least 1")
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [sorted(sh) for sh in shards]
+
+
+def run_sharded(costs, run_local, dist=None):
+    """Runs this rank's share of the instances and gathers every rank's
+    results on rank 0, the only collective of the path.
+
+    run_local(indices) -> (results {index: result}, wall_s, cell_steps).
+    Rank 0 gets {"results": [result per instance, in index order], "wall_s":
+    the slowest rank's wall time, "cell_steps": the sum, "shards": the
+    split}; the other ranks get None."""
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    shards = shard_instances(costs, world)
+    results, wall, cell_steps = run_local(shards[rank])
+    if set(results) != set(shards[rank]):
+        raise N.OpenEMSError(f"rank {rank} returned results for {sorted(results)}, expected {shards[rank]}")
+    mine = {"results": results, "wall_s": float(wall), "cell_steps": int(cell_steps)}
+    if dist is None:
+        parts = [mine]
+    else:
+        parts = [None] * world if rank == 0 else None
+        dist.gather_object(mine, parts, dst=0)
+        if rank != 0:
+            return None
+    merged = {}
+    for part in parts:
+        merged.update(part["results"])
+    return {"results": [merged[i] for i in range(len(costs))],
+            "wall_s": max(part["wall_s"] for part in parts),
+            "cell_steps": sum(part["cell_steps"] for part in parts), "shards": shards}
+
+
 def main(argv=None):
     """Runs the seeded patch-antenna sweep and prints one JSON line:
-    python -m openems_b200.sweep [--count 64] [--seed 4] [--concurrency 6]"""
+    python -m openems_b200.sweep [--count 64] [--seed 4] [--concurrency 6]
+    Under torchrun (WORLD_SIZE > 1) each rank runs its share of the
+    instances on GPU LOCAL_RANK and rank 0 prints the whole job's line."""
     import argparse
+    import datetime
     import json
+    import os
     import time
 
     from . import workloads as W
@@ -156,21 +217,47 @@ def main(argv=None):
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--out", default=None, help="write S11 per instance to this .npz")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32", help="field storage")
+    p.add_argument("--dist-timeout", type=float, default=3600.0,
+                   help="seconds a rank waits at the final gather (several GPUs)")
     a = p.parse_args(argv)
     freqs = np.linspace(0.0, 8e9, a.freqs)
     specs = W.patch_specs(a.count, seed=a.seed)
-    t0 = time.perf_counter()
-    sw = Sweep(freqs, concurrency=a.concurrency, storage=a.storage)
-    ids = [sw.add(W.patch_sweep_instance(s, decay_db=a.decay_db, max_steps=a.max_steps)) for s in specs]
-    t1 = time.perf_counter()
-    sw.run(a.batch_steps)
-    wall, cell_steps = sw.stats()
-    res = [sw.result(i) for i in ids]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dist, device = None, -1
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        device = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(device)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=a.dist_timeout),
+                                device_id=torch.device("cuda", device))
+    setup = [0.0]
+
+    def run_local(indices):
+        t0 = time.perf_counter()
+        sw = Sweep(freqs, concurrency=a.concurrency, device=device, storage=a.storage)
+        ids = {i: sw.add(W.patch_sweep_instance(specs[i], decay_db=a.decay_db, max_steps=a.max_steps))
+               for i in indices}
+        setup[0] = time.perf_counter() - t0
+        sw.run(a.batch_steps)
+        wall, cell_steps = sw.stats()
+        out = {i: sw.result(iid) for i, iid in ids.items()}
+        sw.close()
+        return out, wall, cell_steps
+
+    try:
+        job = run_sharded([instance_cost(sp.dims) for sp in specs], run_local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if job is None:
+        return
+    res, wall, cell_steps = job["results"], job["wall_s"], job["cell_steps"]
     s11_db = [20 * np.log10(np.maximum(np.abs(r["s11"][1:]), 1e-30)) for r in res]
     line = {
         "workload": f"patch_sweep_{a.count}_seed{a.seed}", "field_storage": a.storage,
-        "instances": a.count, "concurrency": a.concurrency, "freqs": a.freqs,
-        "cell_steps": cell_steps, "wall_s": wall, "setup_s": t1 - t0,
+        "instances": a.count, "concurrency": a.concurrency, "freqs": a.freqs, "ranks": world,
+        "cell_steps": cell_steps, "wall_s": wall, "setup_s": setup[0],
         "mcells_per_s": cell_steps / wall / 1e6, "instances_per_hour": a.count / wall * 3600.0,
         "device_seconds_sum": sum(r["device_seconds"] for r in res),
         "decayed": sum(r["termination_reason"] == 1 for r in res),

@@ -177,3 +177,22 @@ def test_staged_early_stop_against_full_runs(check, tau):
         else:
             assert r["steps"] == f["timesteps"]
             assert np.array_equal(r["s11"], f["s11"])
+
+
+def test_command_line_matches_direct_sweep(tmp_path, capsys):
+    """`python -m openems_b200.sweep` on one rank: the whole share, in instance
+    order, equal to a direct Sweep of the same seeded instances."""
+    import json
+
+    from openems_b200 import sweep as S
+    out = tmp_path / "s11.npz"
+    S.main(["--count", "3", "--freqs", "41", "--max-steps", "3000", "--batch-steps", "1000", "--out", str(out)])
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["ranks"] == 1 and line["instances"] == 3 and line["cell_steps"] > 0
+    got = np.load(out)
+    sw = Sweep(np.linspace(0.0, 8e9, 41), concurrency=2)
+    ids = [sw.add(W.patch_sweep_instance(s, decay_db=50.0, max_steps=3000)) for s in W.patch_specs(3, seed=4)]
+    sw.run(1000)
+    want = [sw.result(i) for i in ids]
+    assert np.array_equal(got["timesteps"], [r["timesteps"] for r in want])
+    assert np.array_equal(got["s11"], np.array([r["s11"] for r in want]))
