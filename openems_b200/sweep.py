@@ -171,21 +171,37 @@ def run_sharded(costs, run_local, dist=None):
     run_local(indices) -> (results {index: result}, wall_s, cell_steps).
     Rank 0 gets {"results": [result per instance, in index order], "wall_s":
     the slowest rank's wall time, "cell_steps": the sum, "shards": the
-    split}; the other ranks get None."""
+    split}; the other ranks get None.
+
+    A rank whose share fails still joins the gather with its error, so no
+    rank waits on it: rank 0 then raises OpenEMSError naming every failed
+    rank, and the failed rank re-raises its own exception after the gather."""
     world = dist.get_world_size() if dist is not None else 1
     rank = dist.get_rank() if dist is not None else 0
     shards = shard_instances(costs, world)
-    results, wall, cell_steps = run_local(shards[rank])
-    if set(results) != set(shards[rank]):
-        raise N.OpenEMSError(f"rank {rank} returned results for {sorted(results)}, expected {shards[rank]}")
-    mine = {"results": results, "wall_s": float(wall), "cell_steps": int(cell_steps)}
+    failure = None
+    try:
+        results, wall, cell_steps = run_local(shards[rank])
+        if set(results) != set(shards[rank]):
+            raise N.OpenEMSError(f"rank {rank} returned results for {sorted(results)}, expected {shards[rank]}")
+        mine = {"results": results, "wall_s": float(wall), "cell_steps": int(cell_steps)}
+    except Exception as e:  # reported through the gather, re-raised below
+        failure = e
+        mine = {"error": f"{type(e).__name__}: {e}"}
     if dist is None:
+        if failure is not None:
+            raise failure
         parts = [mine]
     else:
         parts = [None] * world if rank == 0 else None
         dist.gather_object(mine, parts, dst=0)
         if rank != 0:
+            if failure is not None:
+                raise failure
             return None
+        failed = [(r, part["error"]) for r, part in enumerate(parts) if "error" in part]
+        if failed:
+            raise N.OpenEMSError("sweep failed on " + "; ".join(f"rank {r}: {msg}" for r, msg in failed))
     merged = {}
     for part in parts:
         merged.update(part["results"])

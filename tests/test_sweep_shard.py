@@ -53,6 +53,8 @@ def test_single_rank_runs_everything():
 def test_runner_must_return_its_share():
     with pytest.raises(N.OpenEMSError):
         run_sharded([1.0, 2.0], lambda idx: ({0: {}}, 1.0, 1))
+    with pytest.raises(RuntimeError):
+        run_sharded([1.0], _failing_runner)
 
 
 def _free_port():
@@ -61,7 +63,11 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, costs, out):
+def _failing_runner(indices):
+    raise RuntimeError("device lost on this rank")
+
+
+def _rank(rank, world, port, costs, out, fail_rank=-1):
     import datetime
     import sys
     import torch.distributed as dist
@@ -70,25 +76,41 @@ def _rank(rank, world, port, costs, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        job = run_sharded(costs, _fake_runner(rank), dist)
-        out.put((rank, job))
+        try:
+            job = run_sharded(costs, _failing_runner if rank == fail_rank else _fake_runner(rank), dist)
+            out.put((rank, job))
+        except Exception as e:
+            out.put((rank, f"{type(e).__name__}: {e}"))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_ranks_gather_on_rank0():
+def _spawn(costs, world, fail_rank=-1):
     import torch.multiprocessing as mp
-    costs = [instance_cost(s.dims) for s in W.patch_specs(10, seed=4)]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, costs, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, costs, q, fail_rank)) for r in range(world)]
     for p in procs:
         p.start()
     got = dict(q.get(timeout=120) for _ in procs)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    return got
+
+
+def test_failed_rank_is_reported_not_waited_for():
+    """Rank 1's share raises: both ranks return promptly, rank 0 with an
+    error naming rank 1, rank 1 with its own exception."""
+    got = _spawn([1.0, 2.0, 3.0, 4.0], 2, fail_rank=1)
+    assert got[0].startswith("OpenEMSError") and "rank 1: RuntimeError: device lost" in got[0]
+    assert got[1] == "RuntimeError: device lost on this rank"
+
+
+def test_two_ranks_gather_on_rank0():
+    costs = [instance_cost(s.dims) for s in W.patch_specs(10, seed=4)]
+    got = _spawn(costs, 2)
     assert got[1] is None
     job = got[0]
     shards = shard_instances(costs, 2)
