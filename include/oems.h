@@ -333,6 +333,45 @@ OEMS_API oems_status oems_engine_write_fields(oems_engine* engine, const float* 
 /* Clears fields, extension state and the timestep counter. */
 OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 
+/* ---- checkpoint / resume --------------------------------------------------
+ * The engine's evolving state as sections: the buffers oems_engine_reset
+ * clears (fields in their storage type, CPML psi, Mur, probe DFTs, each
+ * dispersive material, lumped RLC, UPML flux, each field DFT dump, each NF2FF
+ * box, the TF/SF 1D grid), in a fixed order that depends only on the
+ * extensions attached.  A snapshot is every section plus the two counters;
+ * loading it into an engine built the same way continues the run bit for bit.
+ * The reference has only read_fields / write_fields (src/fdtd/engine_impl.rs:59-70). */
+enum {
+  OEMS_STATE_FIELDS = 1,
+  OEMS_STATE_CPML = 2,
+  OEMS_STATE_MUR = 3,
+  OEMS_STATE_PROBE_DFT = 4,
+  OEMS_STATE_DISPERSIVE = 5,
+  OEMS_STATE_LUMPED_RLC = 6,
+  OEMS_STATE_UPML = 7,
+  OEMS_STATE_FIELD_DFT = 8,
+  OEMS_STATE_NF2FF = 9,
+  OEMS_STATE_TFSF_E = 10,
+  OEMS_STATE_TFSF_H = 11
+};
+typedef struct oems_state_section {
+  uint32_t kind; /* OEMS_STATE_* */
+  uint32_t reserved0;
+  uint64_t bytes;
+} oems_state_section;
+/* Writes up to `capacity` section descriptors; *count = the number of sections. */
+OEMS_API oems_status oems_engine_state_sections(oems_engine* engine, oems_state_section* out,
+                                                uint64_t capacity, uint64_t* count);
+/* Copies section `index` to / from host memory; `bytes` must equal its size. */
+OEMS_API oems_status oems_engine_read_state(oems_engine* engine, uint64_t index, void* host, uint64_t bytes);
+OEMS_API oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, const void* host,
+                                             uint64_t bytes);
+/* The step counter and the TF/SF 1D grid's step; setting them also empties
+ * the probe-trace buffer, as oems_engine_reset does. */
+OEMS_API oems_status oems_engine_get_state_counters(const oems_engine* engine, uint64_t* timestep,
+                                                    uint64_t* tfsf_step);
+OEMS_API oems_status oems_engine_set_state_counters(oems_engine* engine, uint64_t timestep, uint64_t tfsf_step);
+
 /* ---- extensions ---------------------------------------------------------- */
 
 OEMS_API oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc);

@@ -196,6 +196,10 @@ class TfsfDescC(ctypes.Structure):
                 ("boundary_layer", c_u64), ("phase_velocity", c_f64), ("kind", c_i32), ("reserved0", c_i32)]
 
 
+class StateSectionC(ctypes.Structure):
+    _fields_ = [("kind", c_u32), ("reserved0", c_u32), ("bytes", c_u64)]
+
+
 class CylDescC(ctypes.Structure):
     _fields_ = [("n_rho", c_u64), ("n_alpha", c_u64), ("n_z", c_u64), ("closed_alpha", c_i32),
                 ("r0_included", c_i32), ("dt", c_f64), ("vi", PF * 3), ("iv", PF * 3), ("device", c_i32),
@@ -215,6 +219,11 @@ SIGNATURES = {
     "oems_engine_destroy": (None, [P]),
     "oems_release_cached_memory": (c_i32, [c_i32]),
     "oems_engine_add_tfsf": (c_i32, [P, ctypes.POINTER(TfsfDescC)]),
+    "oems_engine_state_sections": (c_i32, [P, ctypes.POINTER(StateSectionC), c_u64, ctypes.POINTER(c_u64)]),
+    "oems_engine_read_state": (c_i32, [P, c_u64, ctypes.c_void_p, c_u64]),
+    "oems_engine_write_state": (c_i32, [P, c_u64, ctypes.c_char_p, c_u64]),
+    "oems_engine_get_state_counters": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_u64)]),
+    "oems_engine_set_state_counters": (c_i32, [P, c_u64, c_u64]),
     "oems_cyl_create": (c_i32, [ctypes.POINTER(CylDescC), ctypes.POINTER(P)]),
     "oems_cyl_destroy": (None, [P]),
     "oems_cyl_step": (c_i32, [P, c_u64]),

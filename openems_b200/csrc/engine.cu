@@ -2188,6 +2188,102 @@ oems_status oems_engine_reset(oems_engine* engine) {
   return OEMS_OK;
 }
 
+// ---- state sections (checkpoint / resume) ---------------------------------
+// Exactly the buffers oems_engine_reset clears, with the same pointers and
+// byte counts, in a fixed order; the TF/SF 1D grid lives on the host.
+}  // extern "C"
+
+namespace {
+struct StateSection {
+  uint32_t kind;
+  void* dev;   // device buffer, or null for a host one
+  void* host;  // host buffer, or null for a device one
+  size_t bytes;
+};
+
+std::vector<StateSection> state_sections(oems_engine* en) {
+  std::vector<StateSection> s;
+  s.push_back({OEMS_STATE_FIELDS, en->fields, nullptr, en->field_bytes()});
+  if (en->cpml.on) s.push_back({OEMS_STATE_CPML, en->cpml.psi.p, nullptr, en->cpml.psi.n * sizeof(float)});
+  if (en->mur.on) s.push_back({OEMS_STATE_MUR, en->mur.state.p, nullptr, en->mur.state.n * sizeof(float)});
+  if (!en->entry_probe.empty())
+    s.push_back({OEMS_STATE_PROBE_DFT, en->d_dft_acc.p, nullptr, 2 * en->entry_probe.size() * sizeof(double)});
+  for (auto& d : en->disp) s.push_back({OEMS_STATE_DISPERSIVE, d.state->p, nullptr, d.state->n * sizeof(float)});
+  if (!en->rlc.q.empty())
+    s.push_back({OEMS_STATE_LUMPED_RLC, en->rlc.d_int.p, nullptr, en->rlc.q.size() * sizeof(float)});
+  if (en->upml.on) s.push_back({OEMS_STATE_UPML, en->upml.flux.p, nullptr, en->upml.flux.n * sizeof(float)});
+  for (auto& d : en->fdumps) s.push_back({OEMS_STATE_FIELD_DFT, d.acc->p, nullptr, d.acc->n * sizeof(double)});
+  for (auto& x : en->boxes) s.push_back({OEMS_STATE_NF2FF, x.acc->p, nullptr, x.acc->n * sizeof(double)});
+  if (en->tfsf.on) {
+    s.push_back({OEMS_STATE_TFSF_E, nullptr, en->tfsf.e1d.data(), en->tfsf.e1d.size() * sizeof(float)});
+    s.push_back({OEMS_STATE_TFSF_H, nullptr, en->tfsf.h1d.data(), en->tfsf.h1d.size() * sizeof(float)});
+  }
+  return s;
+}
+
+oems_status state_copy(oems_engine* en, uint64_t index, void* out, const void* in, uint64_t bytes) {
+  const std::vector<StateSection> s = state_sections(en);
+  if (index >= s.size()) return fail(OEMS_ERR_INVALID_ARGUMENT, "state section index out of range");
+  const StateSection& q = s[index];
+  if (bytes != q.bytes) return fail(OEMS_ERR_INVALID_ARGUMENT, "state section size differs from the engine's");
+  if (bytes == 0) return OEMS_OK;
+  if (q.host) {
+    if (out) std::memcpy(out, q.host, bytes);
+    else std::memcpy(q.host, in, bytes);
+    return OEMS_OK;
+  }
+  if (!q.dev) return fail(OEMS_ERR_CONFIG, "state section has no buffer");
+  if (out)
+    OEMS_CUDA(cudaMemcpyAsync(out, q.dev, bytes, cudaMemcpyDeviceToHost, en->stream));
+  else
+    OEMS_CUDA(cudaMemcpyAsync(q.dev, in, bytes, cudaMemcpyHostToDevice, en->stream));
+  OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  return OEMS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+oems_status oems_engine_state_sections(oems_engine* engine, oems_state_section* out, uint64_t capacity,
+                                       uint64_t* count) {
+  if (!engine || (!out && capacity)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  const std::vector<StateSection> s = state_sections(engine);
+  if (count) *count = s.size();
+  for (size_t k = 0; k < s.size() && k < capacity; ++k) {
+    out[k].kind = s[k].kind;
+    out[k].reserved0 = 0;
+    out[k].bytes = s[k].bytes;
+  }
+  return OEMS_OK;
+}
+
+oems_status oems_engine_read_state(oems_engine* engine, uint64_t index, void* host, uint64_t bytes) {
+  if (!engine || (!host && bytes)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  EngineScope guard(engine);
+  return state_copy(engine, index, host, nullptr, bytes);
+}
+
+oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, const void* host, uint64_t bytes) {
+  if (!engine || (!host && bytes)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  EngineScope guard(engine);
+  return state_copy(engine, index, nullptr, host, bytes);
+}
+
+oems_status oems_engine_get_state_counters(const oems_engine* engine, uint64_t* timestep, uint64_t* tfsf_step) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  if (timestep) *timestep = engine->timestep;
+  if (tfsf_step) *tfsf_step = engine->tfsf.t;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_set_state_counters(oems_engine* engine, uint64_t timestep, uint64_t tfsf_step) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  engine->timestep = timestep;
+  engine->tfsf.t = tfsf_step;
+  engine->traces_steps = 0;
+  return OEMS_OK;
+}
+
 oems_status oems_engine_add_cpml(oems_engine* engine, const oems_cpml_desc* desc) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   return add_cpml(engine, desc);

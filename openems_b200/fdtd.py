@@ -1157,6 +1157,44 @@ class Engine:
     def reset(self) -> None:
         N.check(N.lib().oems_engine_reset(self._h))
 
+    # -- checkpoint / resume (openems_b200.checkpoint) ----------------------
+
+    def state_sections(self) -> List[Tuple[int, int]]:
+        """(kind, bytes) of every state section, in the engine's order."""
+        n = N.c_u64()
+        N.check(N.lib().oems_engine_state_sections(self._h, None, 0, ctypes.byref(n)))
+        arr = (N.StateSectionC * max(n.value, 1))()
+        N.check(N.lib().oems_engine_state_sections(self._h, arr, n.value, ctypes.byref(n)))
+        return [(int(arr[i].kind), int(arr[i].bytes)) for i in range(n.value)]
+
+    def read_state(self, index: int, nbytes: int) -> bytes:
+        buf = ctypes.create_string_buffer(max(int(nbytes), 1))
+        N.check(N.lib().oems_engine_read_state(self._h, int(index), buf, int(nbytes)))
+        return buf.raw[:int(nbytes)]
+
+    def write_state(self, index: int, data: bytes) -> None:
+        data = bytes(data)
+        N.check(N.lib().oems_engine_write_state(self._h, int(index), data, len(data)))
+
+    def state_counters(self) -> Tuple[int, int]:
+        """(timestep, TF/SF step)."""
+        t, f = N.c_u64(), N.c_u64()
+        N.check(N.lib().oems_engine_get_state_counters(self._h, ctypes.byref(t), ctypes.byref(f)))
+        return int(t.value), int(f.value)
+
+    def set_state_counters(self, timestep: int, tfsf_step: int) -> None:
+        N.check(N.lib().oems_engine_set_state_counters(self._h, int(timestep), int(tfsf_step)))
+
+    def save_state(self) -> bytes:
+        """The whole evolving state as a checkpoint blob."""
+        from . import checkpoint
+        return checkpoint.pack(self)
+
+    def load_state(self, blob) -> None:
+        """Continues from a checkpoint of an engine built the same way."""
+        from . import checkpoint
+        checkpoint.unpack(self, blob)
+
     def energy(self) -> Tuple[float, float]:
         e, h = N.c_f64(), N.c_f64()
         N.check(N.lib().oems_engine_energy(self._h, ctypes.byref(e), ctypes.byref(h)))
