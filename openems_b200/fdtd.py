@@ -1167,10 +1167,11 @@ class Engine:
         N.check(N.lib().oems_engine_state_sections(self._h, arr, n.value, ctypes.byref(n)))
         return [(int(arr[i].kind), int(arr[i].bytes)) for i in range(n.value)]
 
-    def read_state(self, index: int, nbytes: int) -> bytes:
-        buf = ctypes.create_string_buffer(max(int(nbytes), 1))
-        N.check(N.lib().oems_engine_read_state(self._h, int(index), buf, int(nbytes)))
-        return buf.raw[:int(nbytes)]
+    def read_state(self, index: int, nbytes: int) -> bytearray:
+        buf = bytearray(int(nbytes))
+        ptr = (ctypes.c_char * len(buf)).from_buffer(buf) if buf else None  # no extra copy
+        N.check(N.lib().oems_engine_read_state(self._h, int(index), ptr, int(nbytes)))
+        return buf
 
     def write_state(self, index: int, data: bytes) -> None:
         data = bytes(data)
