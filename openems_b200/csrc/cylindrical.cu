@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <string>
 
@@ -218,8 +220,7 @@ void oems_cyl_destroy(oems_cyl_engine* en) {
   delete en;
 }
 
-oems_status oems_cyl_step(oems_cyl_engine* en, uint64_t steps) {
-  if (!en) return cfail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+static oems_status cyl_launch(oems_cyl_engine* en, uint64_t steps) {
   Dev g(en->device);
   const CylArgs v = args(en, true), c = args(en, false);
   const int gn = grid_of(en->n), gr = grid_of(en->na * en->nz);
@@ -245,6 +246,14 @@ oems_status oems_cyl_step(oems_cyl_engine* en, uint64_t steps) {
   CYL_CUDA(cudaStreamSynchronize(en->stream));
   CYL_CUDA(cudaEventElapsedTime(&en->last_ms, en->ev[0], en->ev[1]));
   return OEMS_OK;
+}
+
+oems_status oems_cyl_step(oems_cyl_engine* en, uint64_t steps) {
+  if (!en) return cfail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  nvtxRangePushA("oems_cyl_step");
+  const oems_status st = cyl_launch(en, steps);
+  nvtxRangePop();
+  return st;
 }
 
 static oems_status cyl_copy(oems_cyl_engine* en, float* const* host6, bool to_host) {

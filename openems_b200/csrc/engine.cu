@@ -19,6 +19,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+
+#include <nvtx3/nvToolsExt.h>  // header-only; the ranges cost nothing without a profiler attached
 #include <map>
 #include <memory>
 #include <mutex>
@@ -2136,7 +2138,10 @@ void oems_engine_destroy(oems_engine* engine) {
 oems_status oems_engine_run_batch(oems_engine* engine, const oems_batch* batch, oems_batch_result* result) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   g_last_error.clear();
-  return run_batch(engine, batch, result);
+  nvtxRangePushA("oems_engine_run_batch");
+  const oems_status st = run_batch(engine, batch, result);
+  nvtxRangePop();
+  return st;
 }
 
 oems_status oems_engine_current_timestep(const oems_engine* engine, uint64_t* timestep) {
