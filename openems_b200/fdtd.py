@@ -27,7 +27,6 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _native as N
-from .constants import PI
 
 # ---------------------------------------------------------------------------
 # geometry
