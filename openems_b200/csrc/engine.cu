@@ -653,7 +653,7 @@ static bool cpml_interior(const oems_engine* en, int* i_lo, int* i_hi, int* j_lo
 // slab rows of the planes between them.
 static Geom make_shell_geom(const oems_engine* en, int block, int ichunk) {
   Geom g = make_geom(en, block, ichunk);
-  int ilo, ihi, jlo, jhi;
+  int ilo = 0, ihi = 0, jlo = 0, jhi = 0;
   cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const int nq = g.nzq;
   const int segs[4][4] = {{0, ilo, 0, g.plane4},
@@ -1309,7 +1309,7 @@ static std::mutex& tune_mutex() {
 // the state (fields and psi are saved and restored), keeps the fastest.
 static oems_status autotune(oems_engine* en) {
   en->tuned = true;
-  int ilo, ihi, jlo, jhi;
+  int ilo = 0, ihi = 0, jlo = 0, jhi = 0;
   const bool can_split = en->id_bytes == 0 && en->storage == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const bool only_split = (en->flags & OEMS_ENGINE_SPLIT_KERNELS) && can_split;
   const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split;
