@@ -11,7 +11,10 @@ vectorised, for larger grids.  Only tests import this module.
 Parity is unpinned beyond the reference's own tests for this module
 (src/fdtd/cylindrical.rs:640-760): they check grid flags, alpha wrapping,
 array sizes, step/time counters and reset, and hold no numeric fixtures;
-the reference is Rust and cannot be built here to make some.
+the reference is Rust and cannot be built here to make some.  The tests also
+hold impulse responses worked out by hand from the reference's update lines
+(one H or E value of 1, every neighbour, alpha wrap, clamped edges, R = 0),
+which this restatement reproduces exactly.
 """
 from __future__ import annotations
 

@@ -125,3 +125,81 @@ def test_engine_refuses_bad_grids():
         CylindricalEngine(CylindricalOperator(CylindricalGrid([0.01, 0.02], [0.0, 1.0], [0.0]), 1e-12))
     with pytest.raises(N.GridError):  # through R = 0 with a single rho cell
         CylindricalEngine(CylindricalOperator(CylindricalGrid([0.0, 0.01], [0.0, 1.0], [0.0, 0.01]), 1e-12))
+
+
+# -- impulse responses derived by hand from the reference's update lines -----
+# update_voltage (src/fdtd/cylindrical.rs:441-486): with E = 0 and one H value
+# of 1, E_rho gains +vi where the impulse is the cell's own hz / -vi where it is
+# hz(j - 1) ... ; update_current (:540-583) likewise from one E value.
+
+def _impulse_step(g, comp, pos, field):
+    op = CylindricalOperator(g, 1e-13)
+    shape = g.dimensions()
+    e = [np.zeros(shape, np.float32) for _ in range(3)]
+    h = [np.zeros(shape, np.float32) for _ in range(3)]
+    (h if field == "h" else e)[comp][pos] = 1.0
+    ref.step(e, h, op.vi(), op.iv(), g.closed_alpha, g.r0_included)
+    return op, e, h
+
+
+def _expect_only(arrs, expected):
+    """Every array zero except the listed (component, index) -> value."""
+    for c, a in enumerate(arrs):
+        want = np.zeros_like(a)
+        for (cc, idx), v in expected.items():
+            if cc == c:
+                want[idx] += v
+        assert np.array_equal(a, want), (c, np.argwhere(a != want)[:4])
+
+
+CLOSED = CylindricalGrid.uniform(0.005, 0.015, 5, 6, 0.0, 0.01, 5)
+
+
+def test_voltage_impulse_from_hz_wraps_alpha():
+    i, j, k = 2, 5, 2  # j = n_alpha - 1: its j + 1 neighbour is j = 0 on a closed mesh
+    op, e, _ = _impulse_step(CLOSED, 2, (i, j, k), "h")
+    vi = op.vi()
+    _expect_only(e, {(0, (i, j, k)): vi[0][i, j, k], (0, (i, 0, k)): -vi[0][i, 0, k],
+                     (1, (i, j, k)): -vi[1][i, j, k], (1, (i + 1, j, k)): vi[1][i + 1, j, k]})
+
+
+def test_voltage_impulse_from_halpha_and_hrho():
+    i, j, k = 2, 3, 2
+    op, e, _ = _impulse_step(CLOSED, 1, (i, j, k), "h")
+    vi = op.vi()
+    _expect_only(e, {(0, (i, j, k)): -vi[0][i, j, k], (0, (i, j, k + 1)): vi[0][i, j, k + 1],
+                     (2, (i, j, k)): vi[2][i, j, k], (2, (i + 1, j, k)): -vi[2][i + 1, j, k]})
+    op, e, _ = _impulse_step(CLOSED, 0, (i, j, k), "h")
+    _expect_only(e, {(1, (i, j, k)): vi[1][i, j, k], (1, (i, j, k + 1)): -vi[1][i, j, k + 1],
+                     (2, (i, j, k)): -vi[2][i, j, k], (2, (i, j + 1, k)): vi[2][i, j + 1, k]})
+
+
+def test_current_impulse_from_ez_and_clamped_edges():
+    i, j, k = 2, 0, 2  # j = 0: its j - 1 neighbour is the last alpha cell
+    op, e, h = _impulse_step(CLOSED, 2, (i, j, k), "e")
+    iv = op.iv()
+    _expect_only(e, {(2, (i, j, k)): np.float32(1.0)})  # H was zero: the voltage pass leaves E alone
+    _expect_only(h, {(0, (i, j, k)): iv[0][i, j, k], (0, (i, 5, k)): -iv[0][i, 5, k],
+                     (1, (i, j, k)): -iv[1][i, j, k], (1, (i - 1, j, k)): iv[1][i - 1, j, k]})
+    # at the last rho line the forward neighbour is the cell itself: no H_alpha there from ez
+    i = 4
+    op, _, h = _impulse_step(CLOSED, 2, (i, 3, k), "e")
+    _expect_only(h, {(0, (i, 3, k)): iv[0][i, 3, k], (0, (i, 2, k)): -iv[0][i, 2, k],
+                     (1, (i - 1, 3, k)): iv[1][i - 1, 3, k]})
+
+
+def test_axis_rules():
+    g = CylindricalGrid([i * 0.001 for i in range(5)], [j * 2 * math.pi / 6 for j in range(7)],
+                        [k * 0.002 for k in range(5)])
+    assert g.r0_included
+    # hz at the axis: E_rho and E_z curls are zero for i = 0, E_alpha(0) is forced to 0
+    op, e, _ = _impulse_step(g, 2, (0, 3, 2), "h")
+    vi = op.vi()
+    _expect_only(e, {(1, (1, 3, 2)): vi[1][1, 3, 2]})
+    # ha at i = 1: E_z(1) gains +vi and E_z(2) -vi (ha(i) - ha(i - 1)), and
+    # E_z(0) is then set to E_z(1) / 2
+    op, e, _ = _impulse_step(g, 1, (1, 3, 2), "h")
+    ez1 = vi[2][1, 3, 2]
+    _expect_only(e, {(0, (1, 3, 2)): -vi[0][1, 3, 2], (0, (1, 3, 3)): vi[0][1, 3, 3],
+                     (2, (1, 3, 2)): ez1, (2, (2, 3, 2)): -vi[2][2, 3, 2],
+                     (2, (0, 3, 2)): np.float32(ez1 * np.float32(0.5))})
