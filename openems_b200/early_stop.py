@@ -50,27 +50,30 @@ def s11_db_mean_error(a: np.ndarray, b: np.ndarray, band: np.ndarray, floor: flo
 
 
 def pencil_s11(trace: np.ndarray, uf: np.ndarray, if_: np.ndarray, K: int, dt: float, freqs: np.ndarray,
-               horizon: int, lag: int = 0, R: float = 50.0, **pencil) -> np.ndarray:
+               horizon: int, lag: int = 0, R: float = 50.0, u_modes=None, **pencil) -> np.ndarray:
     """S11 predicted at K: the engine's DFTs of steps [0, K - lag) (those of
     [0, K) minus the last `lag` trace samples) plus the pencil continuation
-    of the window that ends at K - lag.  trace: (>= K, 2) port u, i."""
+    of the window that ends at K - lag.  trace: (>= K, 2) port u, i.
+    u_modes: the port voltage's pencil modes of that window, if already
+    computed."""
     uh, ih = uf.copy(), if_.copy()
     if lag:
         uh -= P.head_dft(trace[K - lag:K, 0], K - lag + 1, dt, freqs, 0.0)
         ih -= P.head_dft(trace[K - lag:K, 1], K - lag + 1, dt, freqs, 0.5)
     ke = K - lag
-    ut = P.pencil_tail_dft(trace[:ke, 0], ke, dt, freqs, 0.0, horizon, **pencil)
+    ut = P.pencil_tail_dft(trace[:ke, 0], ke, dt, freqs, 0.0, horizon, modes=u_modes, **pencil)
     it = P.pencil_tail_dft(trace[:ke, 1], ke, dt, freqs, 0.5, horizon, **pencil)
     return P.s11(uh + ut, ih + it, R)
 
 
 def plain_end(u: np.ndarray, K: int, level_db: float, dt: float, decay_db: float, cap: int,
-              **pencil) -> int:
+              modes=None, **pencil) -> int:
     """Step at which the plain run would stop: its field energy, now
     `level_db` below the peak, is continued with the pencil modes of the port
     voltage (each mode's energy |c|^2 decaying at twice its rate) down to
-    -decay_db, rounded up to the run's 100-step energy checks, at most `cap`."""
-    p, c = P.pencil_modes(u, K, dt, **pencil)
+    -decay_db, rounded up to the run's 100-step energy checks, at most `cap`.
+    modes: pencil_modes(u, K, dt, **pencil) if already computed."""
+    p, c = modes if modes is not None else P.pencil_modes(u, K, dt, **pencil)
     target = 10.0 ** ((-abs(decay_db) - level_db) / 10.0)  # E(end) / E(now)
     if len(p) == 0 or target >= 1.0:
         return K
@@ -106,6 +109,17 @@ class StagePlan:
     end_estimate: bool = True
     check: str = "max"  # residual statistic over the band: "max" or "mean" |dB difference|
 
+    @classmethod
+    def dense(cls, **kw) -> "StagePlan":
+        """The strict-check operating point with a denser pencil: ten stages
+        from 1,024 to 24,576 steps, 512 samples per window, up to 150 modes,
+        largest-error check at 0.1 dB (chosen on the seed-5 training patches
+        as the largest threshold with no instance above 0.5 dB)."""
+        base = dict(stages=(1024, 1536, 2048, 3072, 4096, 6144, 8192, 12288, 16384, 24576), samples=512,
+                    max_modes=150, tau=0.1, check="max")
+        base.update(kw)
+        return cls(**base)
+
     def band(self, freqs: np.ndarray) -> np.ndarray:
         return np.asarray(freqs) >= self.fmin
 
@@ -118,10 +132,11 @@ def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, b
     """(prediction at K, residual-check value in dB, continuation end step);
     with both=True the check value is the pair (max, mean) over the band."""
     pen = plan.pencil(K)
-    end = plain_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, **pen) \
+    um = P.pencil_modes(trace[:K, 0], K, dt, **pen)  # serves both the end estimate and the prediction
+    end = plain_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, modes=um, **pen) \
         if plan.end_estimate else horizon
     end = max(end, K)
-    a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, **pen)
+    a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, u_modes=um, **pen)
     b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
     band = plan.band(freqs)
     if both:
@@ -300,16 +315,25 @@ def main(argv=None):
     p.add_argument("--count", type=int, default=500)
     p.add_argument("--seed", type=int, default=50)
     p.add_argument("--concurrency", type=int, default=16)
-    p.add_argument("--tau", type=float, default=0.1)
-    p.add_argument("--stages", default="2048,4096,8192,16384")
+    p.add_argument("--plan", choices=["standard", "dense"], default="standard",
+                   help="dense: StagePlan.dense() (ten stages, 512 samples, 150 modes, max check at 0.1 dB)")
+    p.add_argument("--tau", type=float, default=None, help="default 0.1")
+    p.add_argument("--stages", default=None, help="default 2048,4096,8192,16384 (standard plan)")
     p.add_argument("--no-end-estimate", action="store_true",
                    help="continue every prediction to the step cap instead of the estimated end")
     p.add_argument("--check", choices=["max", "mean"], default="max",
                    help="residual statistic over the band (run)")
     p.add_argument("--save", default=None, help="calibrate: write the per-instance records to this .npz")
     a = p.parse_args(argv)
-    plan = StagePlan(stages=tuple(int(x) for x in a.stages.split(",")), tau=a.tau,
-                     end_estimate=not a.no_end_estimate, check=a.check)
+    kw = dict(end_estimate=not a.no_end_estimate)
+    if a.tau is not None:
+        kw["tau"] = a.tau
+    if a.stages is not None:
+        kw["stages"] = tuple(int(x) for x in a.stages.split(","))
+    if a.plan == "dense":
+        plan = StagePlan.dense(check=a.check, **kw)
+    else:
+        plan = StagePlan(check=a.check, **{"tau": 0.1, "stages": (2048, 4096, 8192, 16384), **kw})
     insts, freqs = family_instances(a.family, a.count, a.seed)
     band = plan.band(freqs)
     full = full_sweep(insts, freqs, a.concurrency)

@@ -157,12 +157,13 @@ def pencil_modes(x: np.ndarray, K: int, dt: float, window: int = 1536, decimate:
 
 
 def pencil_tail_dft(x: np.ndarray, K: int, dt: float, freqs: np.ndarray, half: float, horizon: int = HORIZON,
-                    window: int = 1536, decimate: int = 4, max_modes: int = 40) -> np.ndarray:
+                    window: int = 1536, decimate: int = 4, max_modes: int = 40, modes=None) -> np.ndarray:
     """DFT of the continuation of x after sample K (to `horizon`), from the
     modes the matrix pencil finds in x[K - window : K] decimated by
-    `decimate`; the engine's DFT scaling and sample times (x[k] taken after
-    timestep k + 1, minus `half`)."""
-    p, c = pencil_modes(x, K, dt, window, decimate, max_modes)
+    `decimate` (or `modes` = (p, c) of pencil_modes, already computed); the
+    engine's DFT scaling and sample times (x[k] taken after timestep k + 1,
+    minus `half`)."""
+    p, c = modes if modes is not None else pencil_modes(x, K, dt, window, decimate, max_modes)
     if len(p) == 0:
         return np.zeros(len(freqs), complex)
     # the modes come in conjugate pairs: Re(sum) is the real continuation
