@@ -81,6 +81,11 @@ typedef struct oems_engine oems_engine;
 #define OEMS_ENGINE_SPLIT_KERNELS 0x40u    /* with CPML: staged kernels on the box
                                               between the x / y slabs, register
                                               kernels on those slabs */
+#define OEMS_ENGINE_ZSPLIT_KERNELS 0x200u  /* with CPML: plain register kernels on
+                                              the CPML-free box (between the x / y
+                                              slabs, float4 chunks clear of the z
+                                              slabs), CPML register kernels on
+                                              every slab cell */
 /* Field storage in 2 bytes per value, arithmetic still in float (no
  * counterpart in the reference, whose fields are f32): IEEE half or
  * bfloat16, rounded to nearest on every store.  H is kept multiplied by
@@ -355,17 +360,22 @@ enum {
   OEMS_STATE_TFSF_H = 11
 };
 typedef struct oems_state_section {
-  uint32_t kind; /* OEMS_STATE_* */
-  uint32_t reserved0;
+  uint32_t kind;    /* OEMS_STATE_* */
+  uint32_t variant; /* how the bytes are encoded beyond their kind: for
+                       OEMS_STATE_FIELDS the field storage (0 float, 1 IEEE
+                       half, 2 bfloat16 -- half and bfloat16 sections have the
+                       same size, so only this tells them apart); 0 otherwise */
   uint64_t bytes;
 } oems_state_section;
 /* Writes up to `capacity` section descriptors; *count = the number of sections. */
 OEMS_API oems_status oems_engine_state_sections(oems_engine* engine, oems_state_section* out,
                                                 uint64_t capacity, uint64_t* count);
-/* Copies section `index` to / from host memory; `bytes` must equal its size. */
+/* Copies section `index` to / from host memory; `bytes` must equal its size,
+ * and for a write `variant` must equal the section's (a snapshot of half
+ * fields is refused by a bfloat16 engine and the reverse). */
 OEMS_API oems_status oems_engine_read_state(oems_engine* engine, uint64_t index, void* host, uint64_t bytes);
-OEMS_API oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, const void* host,
-                                             uint64_t bytes);
+OEMS_API oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, uint32_t variant,
+                                             const void* host, uint64_t bytes);
 /* The step counter and the TF/SF 1D grid's step; setting them also empties
  * the probe-trace buffer, as oems_engine_reset does. */
 OEMS_API oems_status oems_engine_get_state_counters(const oems_engine* engine, uint64_t* timestep,
@@ -479,9 +489,10 @@ OEMS_API oems_status oems_engine_energy(oems_engine* engine, double* e_energy, d
  * (energies[0] = sum E^2, energies[1] = sum H^2), on `stream` (a
  * cudaStream_t; NULL = the legacy default stream), asynchronously.  Partial
  * sums live in a fixed 192 KB device array inside the library that every call
- * on a device shares (calls that overlap on the GPU race on it).  The first
- * call on each device looks up that array's address; make it before any
- * stream capture. */
+ * on a device shares (calls that overlap on the GPU race on it).  Each call
+ * looks up that array's address in the current context (so a device reset
+ * leaves no stale address behind); the first call on a device also loads the
+ * library's device code there, so make it before any stream capture. */
 OEMS_API oems_status oems_field_energy_noalloc(const float* const fields[6], uint64_t count,
                                                double* energies, void* stream);
 
@@ -494,13 +505,34 @@ OEMS_API oems_status oems_field_energy_noalloc(const float* const fields[6], uin
 OEMS_API oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable);
 /* Launch shape chosen for the update kernels (valid after the first batch):
  * staged = 1 for the bulk-async staged kernels (2: staged on the box between
- * the x / y CPML slabs, register kernels on the slabs), threads per CTA, x-planes per
+ * the x / y CPML slabs, register kernels on the slabs; 3: register kernels
+ * with the z-only CPML path on that box and the full CPML path on the x / y
+ * slabs), threads per CTA, x-planes per
  * work item, rows per tile (staged), pipeline stages (staged) or the L2
  * prefetch distance in x-planes (register kernels, 0 = none), CTAs. */
 OEMS_API oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged,
                                              int32_t* threads, int32_t* ichunk,
                                              int32_t* rows_per_tile, int32_t* stages,
                                              int32_t* grid);
+/* One launch shape the autotuner timed: kind as `staged` above, threads per
+ * CTA, x-planes per work item, pipeline stages (staged) or L2 prefetch
+ * distance (register), the number of H + E pairs timed and their device time
+ * in milliseconds. */
+typedef struct oems_tune_entry {
+  int32_t kind;
+  int32_t threads;
+  int32_t ichunk;
+  int32_t extra;
+  int32_t reps;
+  float ms;
+} oems_tune_entry;
+/* The candidates of the tuning that chose this engine's shape (the process
+ * caches tunings per grid and variant, so a later engine of the same grid
+ * reports the same list).  Writes min(capacity, count) entries; out may be
+ * NULL to ask for the count.  No reference counterpart: a diagnostic of the
+ * project's autotuner. */
+OEMS_API oems_status oems_engine_tune_report(const oems_engine* engine, oems_tune_entry* out,
+                                             uint64_t capacity, uint64_t* count);
 OEMS_API oems_status oems_engine_kernel_profile(const oems_engine* engine, double* h_seconds,
                                                 uint64_t* h_launches, double* e_seconds,
                                                 uint64_t* e_launches);

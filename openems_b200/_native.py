@@ -28,6 +28,7 @@ ENGINE_STAGED_KERNELS = 0x20
 ENGINE_SPLIT_KERNELS = 0x40
 ENGINE_FIELDS_F16 = 0x80
 ENGINE_FIELDS_BF16 = 0x100
+ENGINE_ZSPLIT_KERNELS = 0x200
 H_STORAGE_SCALE = 512.0
 STORAGE_FLAGS = {"f32": 0, "f16": ENGINE_FIELDS_F16, "bf16": ENGINE_FIELDS_BF16}
 
@@ -197,7 +198,7 @@ class TfsfDescC(ctypes.Structure):
 
 
 class StateSectionC(ctypes.Structure):
-    _fields_ = [("kind", c_u32), ("reserved0", c_u32), ("bytes", c_u64)]
+    _fields_ = [("kind", c_u32), ("variant", c_u32), ("bytes", c_u64)]
 
 
 class CylDescC(ctypes.Structure):
@@ -221,7 +222,7 @@ SIGNATURES = {
     "oems_engine_add_tfsf": (c_i32, [P, ctypes.POINTER(TfsfDescC)]),
     "oems_engine_state_sections": (c_i32, [P, ctypes.POINTER(StateSectionC), c_u64, ctypes.POINTER(c_u64)]),
     "oems_engine_read_state": (c_i32, [P, c_u64, ctypes.c_void_p, c_u64]),
-    "oems_engine_write_state": (c_i32, [P, c_u64, ctypes.c_char_p, c_u64]),
+    "oems_engine_write_state": (c_i32, [P, c_u64, c_u32, ctypes.c_char_p, c_u64]),
     "oems_engine_get_state_counters": (c_i32, [P, ctypes.POINTER(c_u64), ctypes.POINTER(c_u64)]),
     "oems_engine_set_state_counters": (c_i32, [P, c_u64, c_u64]),
     "oems_cyl_create": (c_i32, [ctypes.POINTER(CylDescC), ctypes.POINTER(P)]),
@@ -266,6 +267,7 @@ SIGNATURES = {
     "oems_field_energy_noalloc": (c_i32, [ctypes.c_void_p * 6, c_u64, P, P]),
     "oems_engine_set_kernel_profiling": (c_i32, [P, c_i32]),
     "oems_engine_launch_info": (c_i32, [P] + [ctypes.POINTER(c_i32)] * 6),
+    "oems_engine_tune_report": (c_i32, [P, P, c_u64, ctypes.POINTER(c_u64)]),
     "oems_engine_kernel_profile": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_u64),
                                            ctypes.POINTER(c_f64), ctypes.POINTER(c_u64)]),
     # include/oems_host.h

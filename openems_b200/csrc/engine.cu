@@ -279,6 +279,9 @@ struct LaunchShape {
   // split: staged kernels (tma) on the interior box, register CPML kernels
   // with these settings on the x / y slabs
   bool split = false;
+  // zsplit: plain register kernels (no CPML) on the CPML-free box and the
+  // CPML kernels (sh_block, sh_ichunk) on every slab cell (x, y and z)
+  bool zsplit = false;
   int sh_block = 256, sh_ichunk = 8, grid_sh = 0, grid_se = 0;
   int grid_h = 0;
   int grid_e = 0;
@@ -574,6 +577,7 @@ struct oems_engine {
   oems::LaunchShape shape;
   oems::Geom gs{};  // shell segments of a split shape
   bool tuned = false;
+  std::vector<oems_tune_entry> tune_report;  // candidates timed by the last tuning
 
   // graphs keyed by span length; invalidated when any baked pointer changes
   std::map<int, cudaGraphExec_t> graphs;
@@ -633,8 +637,36 @@ static Geom make_geom(const oems_engine* en, int block, int ichunk) {
   g.nchunks = (g.nx + ichunk - 1) / ichunk;
   g.work = g.tiles * g.nchunks;
   g.nseg = 1;
-  g.seg[0] = Seg{0, g.nx, 0, g.plane4, g.tiles, 0};
+  g.seg[0] = Seg{0, g.nx, 0, 0, g.nzq, g.plane4, g.tiles, 0};
   return g;
+}
+
+// Appends segment planes [i0, i1) x rows [j0, j1) x chunks [q0, q1) of each
+// row (skipped when empty).
+static void add_seg(Geom& g, int block, int ichunk, int i0, int i1, int j0, int j1, int q0, int q1) {
+  if (i1 <= i0 || j1 <= j0 || q1 <= q0) return;
+  Seg S;
+  S.i0 = i0;
+  S.i1 = i1;
+  S.j0 = j0;
+  S.q0 = q0;
+  S.w = q1 - q0;
+  S.n = (j1 - j0) * S.w;
+  S.tiles = (S.n + block - 1) / block;
+  S.work0 = g.work;
+  g.work += S.tiles * ((i1 - i0 + ichunk - 1) / ichunk);
+  g.seg[g.nseg++] = S;
+}
+
+// Chunks [qa, qb) of a row touch neither z slab: chunk q (cells 4q..4q+3)
+// meets the z-min slab when 4q < L and the z-max slab when 4q + 3 >= its
+// first cell.
+static void zfree_chunks(const oems_engine* en, int* qa, int* qb) {
+  const int nzq = (en->nz + 3) / 4;
+  const CpmlArgs& cp = en->cpml.args;
+  *qa = (cp.L[4] + 3) / 4;
+  *qb = cp.L[5] > 0 ? (std::max(cp.start[5] - 3, 0) + 3) / 4 : nzq;
+  *qb = std::min(*qb, nzq);
 }
 
 // Interior box between the x and y CPML slabs: planes [i_lo, i_hi), rows
@@ -650,32 +682,46 @@ static bool cpml_interior(const oems_engine* en, int* i_lo, int* i_hi, int* j_lo
 }
 
 // The x / y slabs as register-kernel segments: whole planes of the x slabs,
-// slab rows of the planes between them.
-static Geom make_shell_geom(const oems_engine* en, int block, int ichunk) {
+// slab rows of the planes between them; with_z adds the z-slab chunks of the
+// interior rows (the chunks the plain interior launch of a z-split leaves).
+static Geom make_shell_geom(const oems_engine* en, int block, int ichunk, bool with_z = false) {
   Geom g = make_geom(en, block, ichunk);
   int ilo = 0, ihi = 0, jlo = 0, jhi = 0;
   cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const int nq = g.nzq;
-  const int segs[4][4] = {{0, ilo, 0, g.plane4},
-                          {ihi, g.nx, 0, g.plane4},
-                          {ilo, ihi, 0, jlo * nq},
-                          {ilo, ihi, jhi * nq, g.plane4}};
   g.nseg = 0;
-  int work = 0;
-  for (const auto& sg : segs) {
-    if (sg[1] <= sg[0] || sg[3] <= sg[2]) continue;
-    Seg S;
-    S.i0 = sg[0];
-    S.i1 = sg[1];
-    S.c0 = sg[2];
-    S.c1 = sg[3];
-    S.tiles = (S.c1 - S.c0 + block - 1) / block;
-    S.work0 = work;
-    work += S.tiles * ((S.i1 - S.i0 + ichunk - 1) / ichunk);
-    g.seg[g.nseg++] = S;
+  g.work = 0;
+  add_seg(g, block, ichunk, 0, ilo, 0, g.ny, 0, nq);
+  add_seg(g, block, ichunk, ihi, g.nx, 0, g.ny, 0, nq);
+  add_seg(g, block, ichunk, ilo, ihi, 0, jlo, 0, nq);
+  add_seg(g, block, ichunk, ilo, ihi, jhi, g.ny, 0, nq);
+  if (with_z) {
+    int qa = 0, qb = 0;
+    zfree_chunks(en, &qa, &qb);
+    qb = std::max(qa, qb);  // never twice over a chunk
+    add_seg(g, block, ichunk, ilo, ihi, jlo, jhi, 0, qa);
+    add_seg(g, block, ichunk, ilo, ihi, jlo, jhi, qb, nq);
   }
-  g.work = work;
   return g;
+}
+
+// The CPML-free box: planes and rows between the x / y slabs, chunks clear
+// of both z slabs, as one segment for the plain (no CPML) kernels.
+static Geom make_interior_geom(const oems_engine* en, int block, int ichunk) {
+  Geom g = make_geom(en, block, ichunk);
+  g.nseg = 0;
+  g.work = 0;
+  int ilo = 0, ihi = 0, jlo = 0, jhi = 0;
+  if (!cpml_interior(en, &ilo, &ihi, &jlo, &jhi)) return g;
+  int qa = 0, qb = 0;
+  zfree_chunks(en, &qa, &qb);
+  add_seg(g, block, ichunk, ilo, ihi, jlo, jhi, qa, qb);
+  return g;
+}
+
+// A z-split needs a non-empty CPML-free box.
+static bool can_zsplit(const oems_engine* en) {
+  return en->cpml.on && make_interior_geom(en, 256, 8).work > 0;
 }
 
 static HArgs h_args(oems_engine* en) {
@@ -843,21 +889,32 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   }
   const size_t smem = table_smem(en);
   int occ_h = 0, occ_e = 0;
+  const bool mode = en->cpml.on && !s.zsplit;
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_h, (const void*)pick_h(en->id_bytes, en->cpml.on, en->storage), s.block, smem));
+      &occ_h, (const void*)pick_h(en->id_bytes, mode, en->storage), s.block, smem));
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_e, (const void*)pick_e(en->id_bytes, en->cpml.on, en->storage), s.block, smem));
-  const Geom g = make_geom(en, s.block, s.ichunk);
+      &occ_e, (const void*)pick_e(en->id_bytes, mode, en->storage), s.block, smem));
+  const Geom g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
   s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h) * sms));
   s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e) * sms));
+  if (s.zsplit) {
+    int oh = 0, oe = 0;
+    OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &oh, (const void*)pick_h(en->id_bytes, true, en->storage), s.sh_block, smem));
+    OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &oe, (const void*)pick_e(en->id_bytes, true, en->storage), s.sh_block, smem));
+    const Geom gs = make_shell_geom(en, s.sh_block, s.sh_ichunk, true);
+    s.grid_sh = std::max(1, std::min(gs.work, std::max(1, oh) * sms));
+    s.grid_se = std::max(1, std::min(gs.work, std::max(1, oe) * sms));
+  }
   return OEMS_OK;
 }
 
 static void apply_shape(oems_engine* en, const LaunchShape& s) {
   en->shape = s;
-  en->g = make_geom(en, s.block, s.ichunk);
+  en->g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
   en->g.pf = s.tma ? 0 : s.pf;
-  if (s.split) en->gs = make_shell_geom(en, s.sh_block, s.sh_ichunk);
+  if (s.split || s.zsplit) en->gs = make_shell_geom(en, s.sh_block, s.sh_ichunk, s.zsplit);
   en->graph_epoch++;
 }
 
@@ -889,6 +946,16 @@ static cudaError_t launch_h(oems_engine* en) {
     return cudaGetLastError();
   }
   HArgs a = h_args(en);
+  if (en->shape.zsplit) {
+    pick_h(en->id_bytes, false, en->storage)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
+    if (en->gs.work > 0) {
+      HArgs b = a;
+      b.g = en->gs;
+      pick_h(en->id_bytes, true, en->storage)<<<en->shape.grid_sh, en->shape.sh_block, table_smem(en),
+                                                     en->stream>>>(b);
+    }
+    return cudaGetLastError();
+  }
   pick_h(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
 }
@@ -904,6 +971,16 @@ static cudaError_t launch_e(oems_engine* en) {
     return cudaGetLastError();
   }
   EArgs a = e_args(en);
+  if (en->shape.zsplit) {
+    pick_e(en->id_bytes, false, en->storage)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
+    if (en->gs.work > 0) {
+      EArgs b = a;
+      b.g = en->gs;
+      pick_e(en->id_bytes, true, en->storage)<<<en->shape.grid_se, en->shape.sh_block, table_smem(en),
+                                                     en->stream>>>(b);
+    }
+    return cudaGetLastError();
+  }
   pick_e(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
   return cudaGetLastError();
 }
@@ -1025,7 +1102,8 @@ static int ext_kernels(const oems_engine* en) {
 }
 
 static int kernels_per_step(const oems_engine* en) {
-  return (en->shape.split ? 4 : 2) + ext_kernels(en) + post_kernels(en);
+  const int upd = en->shape.split ? 4 : en->shape.zsplit ? (en->gs.work > 0 ? 4 : 2) : 2;
+  return upd + ext_kernels(en) + post_kernels(en);
 }
 
 // Launches `steps` timesteps directly (no graph).
@@ -1295,10 +1373,16 @@ struct TuneKey {
     return std::tie(dev, nx, ny, nz, id_bytes, cpml) < std::tie(o.dev, o.nx, o.ny, o.nz, o.id_bytes, o.cpml);
   }
 };
-static std::map<TuneKey, LaunchShape>& tune_cache() {
-  static std::map<TuneKey, LaunchShape> m;
+struct TuneResult {
+  LaunchShape best;
+  std::vector<oems_tune_entry> report;
+};
+static std::map<TuneKey, TuneResult>& tune_cache() {
+  static std::map<TuneKey, TuneResult> m;
   return m;
 }
+
+static int shape_kind(const LaunchShape& s) { return s.split ? 2 : s.tma ? 1 : s.zsplit ? 3 : 0; }
 // engines may be driven from several host threads (one engine per thread)
 static std::mutex& tune_mutex() {
   static std::mutex m;
@@ -1312,9 +1396,11 @@ static oems_status autotune(oems_engine* en) {
   int ilo = 0, ihi = 0, jlo = 0, jhi = 0;
   const bool can_split = en->id_bytes == 0 && en->storage == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const bool only_split = (en->flags & OEMS_ENGINE_SPLIT_KERNELS) && can_split;
-  const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split;
+  const bool only_z = (en->flags & OEMS_ENGINE_ZSPLIT_KERNELS) && !only_split && can_zsplit(en);
+  const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split &&
+                        !only_z;
   const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0 && !only_split &&
-                        en->storage == 0;
+                        !only_z && en->storage == 0;
   // split shapes are tried only on request: at 256^3 with 8-layer CPML the
   // staged interior plus register slabs measured 36.8 GCells/s against 45.6
   // for the register kernels on the whole grid (the z-slab lanes of every
@@ -1340,6 +1426,10 @@ static oems_status autotune(oems_engine* en) {
       s.smem = make_tma_geom(en, std::max(1, std::min(en->ny, 256 / en->g.nzq)), 16, 256, limit, 4, s.tg);
       if (s.smem == 0) s = LaunchShape{};
     }
+    if (only_z) {
+      s.zsplit = true;
+      s.sh_ichunk = 4;
+    }
     if (!s.tma) {
       // small grids: shorter x-runs, then narrower CTAs, until every SM has
       // a work item (a 70^3 grid has 45 items at 256 x 8: most SMs would idle)
@@ -1358,13 +1448,16 @@ static oems_status autotune(oems_engine* en) {
     apply_shape(en, s);
     return OEMS_OK;
   }
+  const bool want_z = (want_reg || only_z) && can_zsplit(en);
   const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes,
-                    (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0) | (want_split ? 8 : 0)};
+                    (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0) | (want_split ? 8 : 0) |
+                        (want_z ? 16 : 0) | (en->storage << 5)};
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
     auto hit = tune_cache().find(key);
     if (hit != tune_cache().end()) {
-      apply_shape(en, hit->second);
+      en->tune_report = hit->second.report;
+      apply_shape(en, hit->second.best);
       return OEMS_OK;
     }
   }
@@ -1381,6 +1474,9 @@ static oems_status autotune(oems_engine* en) {
   LaunchShape best = en->shape;
   float best_ms = 1e30f;
   std::vector<LaunchShape> cands;
+  // plain kernels on the CPML-free box plus one CPML launch over the slabs
+  // (want_z): most cells run with the plain kernels' register budget (64 /
+  // 92 registers against 128 with spills for the CPML forms)
   for (int b : {256, 512})
     for (int c : {4, 8, 16, 32})
       for (int pf : {0, 2}) {
@@ -1391,6 +1487,12 @@ static oems_status autotune(oems_engine* en) {
         s.ichunk = c;
         s.pf = pf;
         if (want_reg) cands.push_back(s);
+        if (want_z) {
+          s.zsplit = true;
+          s.sh_block = 256;
+          s.sh_ichunk = std::min(c, 8);
+          cands.push_back(s);
+        }
       }
   if (want_tma) {
     size_t limit = 0;
@@ -1439,6 +1541,7 @@ static oems_status autotune(oems_engine* en) {
       }
   }
   oems_status st = OEMS_OK;
+  en->tune_report.clear();
   for (LaunchShape s : cands) {
     st = size_grid(en, s);
     if (st != OEMS_OK) break;
@@ -1446,6 +1549,14 @@ static oems_status autotune(oems_engine* en) {
     float ms = 0.f;
     st = time_shape(en, reps, &ms);
     if (st != OEMS_OK) break;
+    oems_tune_entry te{};
+    te.kind = shape_kind(s);
+    te.threads = s.tma ? s.nconsumer + 32 : s.block;
+    te.ichunk = s.ichunk;
+    te.extra = s.tma ? s.tg.NS : s.pf;
+    te.reps = reps;
+    te.ms = ms;
+    en->tune_report.push_back(te);
     if (ms < best_ms) {
       best_ms = ms;
       best = s;
@@ -1460,7 +1571,7 @@ static oems_status autotune(oems_engine* en) {
   apply_shape(en, best);
   if (st == OEMS_OK) {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    tune_cache()[key] = best;
+    tune_cache()[key] = TuneResult{best, en->tune_report};
   }
   cudaMemcpyAsync(en->fields, save, fbytes, cudaMemcpyDeviceToDevice, en->stream);
   if (pbytes) cudaMemcpyAsync(en->cpml.psi.p, (char*)save + fbytes, pbytes, cudaMemcpyDeviceToDevice, en->stream);
@@ -2048,9 +2159,17 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
     const double width = (double)L[f] * en->delta[a];
     std::vector<float> rows(6 * L[f]);
     for (int l = 0; l < L[f]; ++l) {
-      // src/extensions/cpml.rs:114-124
-      const double depth_e = is_min ? (double)(L[f] - l) * en->delta[a] : (double)(l + 1) * en->delta[a];
-      const double depth_h = depth_e - 0.5 * en->delta[a];
+      // Depth of the E and H difference positions of layer l below the
+      // slab's inner interface.  The grading formulas are those of
+      // src/extensions/cpml.rs:114-155; its max-face depths ((l + 1) d for
+      // E, (l + 1/2) d for H) put E one cell deeper than the H between the
+      // same E nodes, a mismatch that reflects about -14 dB of a normally
+      // incident wave (the reference never applies psi, so it does not show
+      // there).  Here both faces use the positions of the differences: the
+      // backward E difference of cell g sits at g d, the forward H
+      // difference at (g + 1/2) d.
+      const double depth_e = is_min ? (double)(L[f] - l) * en->delta[a] : (double)l * en->delta[a];
+      const double depth_h = is_min ? depth_e - 0.5 * en->delta[a] : depth_e + 0.5 * en->delta[a];
       for (int w = 0; w < 2; ++w) {
         const double depth = w == 0 ? depth_e : depth_h;
         const double rho = std::min(1.0, std::max(0.0, depth / width));
@@ -2201,6 +2320,7 @@ oems_status oems_engine_reset(oems_engine* engine) {
 namespace {
 struct StateSection {
   uint32_t kind;
+  uint32_t variant;  // OEMS_STATE_FIELDS: the storage type; 0 otherwise
   void* dev;   // device buffer, or null for a host one
   void* host;  // host buffer, or null for a device one
   size_t bytes;
@@ -2208,29 +2328,34 @@ struct StateSection {
 
 std::vector<StateSection> state_sections(oems_engine* en) {
   std::vector<StateSection> s;
-  s.push_back({OEMS_STATE_FIELDS, en->fields, nullptr, en->field_bytes()});
-  if (en->cpml.on) s.push_back({OEMS_STATE_CPML, en->cpml.psi.p, nullptr, en->cpml.psi.n * sizeof(float)});
-  if (en->mur.on) s.push_back({OEMS_STATE_MUR, en->mur.state.p, nullptr, en->mur.state.n * sizeof(float)});
+  s.push_back({OEMS_STATE_FIELDS, (uint32_t)en->storage, en->fields, nullptr, en->field_bytes()});
+  if (en->cpml.on) s.push_back({OEMS_STATE_CPML, 0, en->cpml.psi.p, nullptr, en->cpml.psi.n * sizeof(float)});
+  if (en->mur.on) s.push_back({OEMS_STATE_MUR, 0, en->mur.state.p, nullptr, en->mur.state.n * sizeof(float)});
   if (!en->entry_probe.empty())
-    s.push_back({OEMS_STATE_PROBE_DFT, en->d_dft_acc.p, nullptr, 2 * en->entry_probe.size() * sizeof(double)});
-  for (auto& d : en->disp) s.push_back({OEMS_STATE_DISPERSIVE, d.state->p, nullptr, d.state->n * sizeof(float)});
+    s.push_back({OEMS_STATE_PROBE_DFT, 0, en->d_dft_acc.p, nullptr, 2 * en->entry_probe.size() * sizeof(double)});
+  for (auto& d : en->disp)
+    s.push_back({OEMS_STATE_DISPERSIVE, 0, d.state->p, nullptr, d.state->n * sizeof(float)});
   if (!en->rlc.q.empty())
-    s.push_back({OEMS_STATE_LUMPED_RLC, en->rlc.d_int.p, nullptr, en->rlc.q.size() * sizeof(float)});
-  if (en->upml.on) s.push_back({OEMS_STATE_UPML, en->upml.flux.p, nullptr, en->upml.flux.n * sizeof(float)});
-  for (auto& d : en->fdumps) s.push_back({OEMS_STATE_FIELD_DFT, d.acc->p, nullptr, d.acc->n * sizeof(double)});
-  for (auto& x : en->boxes) s.push_back({OEMS_STATE_NF2FF, x.acc->p, nullptr, x.acc->n * sizeof(double)});
+    s.push_back({OEMS_STATE_LUMPED_RLC, 0, en->rlc.d_int.p, nullptr, en->rlc.q.size() * sizeof(float)});
+  if (en->upml.on) s.push_back({OEMS_STATE_UPML, 0, en->upml.flux.p, nullptr, en->upml.flux.n * sizeof(float)});
+  for (auto& d : en->fdumps)
+    s.push_back({OEMS_STATE_FIELD_DFT, 0, d.acc->p, nullptr, d.acc->n * sizeof(double)});
+  for (auto& x : en->boxes) s.push_back({OEMS_STATE_NF2FF, 0, x.acc->p, nullptr, x.acc->n * sizeof(double)});
   if (en->tfsf.on) {
-    s.push_back({OEMS_STATE_TFSF_E, nullptr, en->tfsf.e1d.data(), en->tfsf.e1d.size() * sizeof(float)});
-    s.push_back({OEMS_STATE_TFSF_H, nullptr, en->tfsf.h1d.data(), en->tfsf.h1d.size() * sizeof(float)});
+    s.push_back({OEMS_STATE_TFSF_E, 0, nullptr, en->tfsf.e1d.data(), en->tfsf.e1d.size() * sizeof(float)});
+    s.push_back({OEMS_STATE_TFSF_H, 0, nullptr, en->tfsf.h1d.data(), en->tfsf.h1d.size() * sizeof(float)});
   }
   return s;
 }
 
-oems_status state_copy(oems_engine* en, uint64_t index, void* out, const void* in, uint64_t bytes) {
+oems_status state_copy(oems_engine* en, uint64_t index, void* out, const void* in, uint64_t bytes,
+                       uint32_t variant) {
   const std::vector<StateSection> s = state_sections(en);
   if (index >= s.size()) return fail(OEMS_ERR_INVALID_ARGUMENT, "state section index out of range");
   const StateSection& q = s[index];
   if (bytes != q.bytes) return fail(OEMS_ERR_INVALID_ARGUMENT, "state section size differs from the engine's");
+  if (!out && variant != q.variant)
+    return fail(OEMS_ERR_CONFIG, "state section encoding differs from the engine's (field storage type)");
   if (bytes == 0) return OEMS_OK;
   if (q.host) {
     if (out) std::memcpy(out, q.host, bytes);
@@ -2256,7 +2381,7 @@ oems_status oems_engine_state_sections(oems_engine* engine, oems_state_section* 
   if (count) *count = s.size();
   for (size_t k = 0; k < s.size() && k < capacity; ++k) {
     out[k].kind = s[k].kind;
-    out[k].reserved0 = 0;
+    out[k].variant = s[k].variant;
     out[k].bytes = s[k].bytes;
   }
   return OEMS_OK;
@@ -2265,13 +2390,14 @@ oems_status oems_engine_state_sections(oems_engine* engine, oems_state_section* 
 oems_status oems_engine_read_state(oems_engine* engine, uint64_t index, void* host, uint64_t bytes) {
   if (!engine || (!host && bytes)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   EngineScope guard(engine);
-  return state_copy(engine, index, host, nullptr, bytes);
+  return state_copy(engine, index, host, nullptr, bytes, 0);
 }
 
-oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, const void* host, uint64_t bytes) {
+oems_status oems_engine_write_state(oems_engine* engine, uint64_t index, uint32_t variant, const void* host,
+                                    uint64_t bytes) {
   if (!engine || (!host && bytes)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   EngineScope guard(engine);
-  return state_copy(engine, index, nullptr, host, bytes);
+  return state_copy(engine, index, nullptr, host, bytes, variant);
 }
 
 oems_status oems_engine_get_state_counters(const oems_engine* engine, uint64_t* timestep, uint64_t* tfsf_step) {
@@ -3048,12 +3174,22 @@ oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged, 
                                     int32_t* rows_per_tile, int32_t* stages, int32_t* grid) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   const LaunchShape& s = engine->shape;
-  if (staged) *staged = s.split ? 2 : s.tma ? 1 : 0;
+  if (staged) *staged = s.split ? 2 : s.tma ? 1 : s.zsplit ? 3 : 0;
   if (threads) *threads = s.tma ? s.nconsumer + 32 : s.block;
   if (ichunk) *ichunk = s.ichunk;
   if (rows_per_tile) *rows_per_tile = s.tma ? s.tg.TJ : 0;
   if (stages) *stages = s.tma ? s.tg.NS : s.pf;
   if (grid) *grid = s.grid_h;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_tune_report(const oems_engine* engine, oems_tune_entry* out, uint64_t capacity,
+                                    uint64_t* count) {
+  if (!engine || !count) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine or count");
+  *count = engine->tune_report.size();
+  if (out)
+    for (uint64_t i = 0; i < std::min<uint64_t>(capacity, engine->tune_report.size()); ++i)
+      out[i] = engine->tune_report[i];
   return OEMS_OK;
 }
 

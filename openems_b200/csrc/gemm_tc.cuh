@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
 
   for (int kb = 0; kb < S - 1; ++kb) load_block(kb);
   bool ok = true;
+  int issued = 0;  // K-blocks whose MMAs thread 0 has committed
   for (int kb = 0; kb < nkb && ok; ++kb) {
     // block kb has landed (at most S - 2 younger groups in flight); its
     // generic-proxy writes are made visible to the tensor cores
@@ -183,6 +184,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
                        tc::smem_u32(bar + kb % S))
                    : "memory");
     }
+    issued = kb + 1;
     // the stage of block kb - 1 is refilled with block kb + S - 1 once that
     // block's MMAs are done; a block-wide vote keeps every thread on the
     // same iteration count
@@ -194,6 +196,13 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const GemmArgs p) {
   // the last block's MMAs (and with them every earlier one) are done
   if (ok && nkb > 0) ok = __syncthreads_and(tc::mbar_wait(bar + (nkb - 1) % S, (uint32_t)(((nkb - 1) / S) & 1),
                                                           p.err)) != 0;
+  else if (!ok && issued > 0)
+    // a wait gave up: before tensor memory and shared memory are released,
+    // wait (bounded again) for the last committed block, whose commit
+    // tracks every earlier MMA; if that wait gives up too the CTA's tile is
+    // left undefined (the error word is already set)
+    (void)__syncthreads_and(
+        tc::mbar_wait(bar + (issued - 1) % S, (uint32_t)(((issued - 1) / S) & 1), p.err));
   asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 

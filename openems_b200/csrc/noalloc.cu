@@ -11,9 +11,12 @@
 //
 // The scratch array is shared by every call on a device and keeps the last
 // call's contents; its completion counter is cleared before every launch.
-// Calls that overlap on the GPU (concurrent streams) race on it.  The first
-// call on each device looks up the array's device address (once per device,
-// with that device current); make that first call before any stream capture.
+// Calls that overlap on the GPU (concurrent streams) race on it.  Every call
+// looks up the array's device address with the device current (a host-side
+// lookup, no allocation): an address kept from an earlier call would dangle
+// after cudaDeviceReset or a re-created context, which reload the module.
+// The first call on each device loads the module; make it before any stream
+// capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -108,26 +111,23 @@ __global__ void __launch_bounds__(kNaThreads) k_energy_noalloc(const NaArgs a, d
 }
 
 std::mutex g_na_mutex;
-double* g_na_ptr[kNaMaxDevices] = {};
 
 oems_status na_fail(oems_status st, const char* msg) {
   oems::g_last_error = msg;
   return st;
 }
 
-// Device address of the scratch array on the current device (looked up once).
-oems_status na_scratch(int dev, double** out) {
+// Device address of the scratch array in the current device's context,
+// looked up on every call (see the file comment: a cached one can go stale).
+oems_status na_scratch(double** out) {
   std::lock_guard<std::mutex> lock(g_na_mutex);
-  if (!g_na_ptr[dev]) {
-    double* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_energy_scratch);
-    if (e != cudaSuccess || !ptr) {
-      oems::g_last_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-      return OEMS_ERR_CUDA;
-    }
-    g_na_ptr[dev] = ptr;
+  double* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_energy_scratch);
+  if (e != cudaSuccess || !ptr) {
+    oems::g_last_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+    return OEMS_ERR_CUDA;
   }
-  *out = g_na_ptr[dev];
+  *out = ptr;
   return OEMS_OK;
 }
 
@@ -154,7 +154,7 @@ extern "C" oems_status oems_field_energy_noalloc(const float* const fields[6], u
   }
   if (dev < 0 || dev >= kNaMaxDevices) return na_fail(OEMS_ERR_NO_DEVICE, "device ordinal out of range");
   double* scratch = nullptr;
-  const oems_status st = na_scratch(dev, &scratch);
+  const oems_status st = na_scratch(&scratch);
   if (st != OEMS_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the completion counter must start at zero; the partials are overwritten

@@ -39,15 +39,20 @@ namespace oems {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
-// A segment of the update: x-planes [i0, i1) x float4 chunks [c0, c1) of the
-// flattened (j, k) plane (c0, c1 on row boundaries), cut into tiles of one
-// CTA's chunks and runs of `ichunk` planes; work items of all segments are
-// numbered consecutively from work0.
+// A segment of the update: x-planes [i0, i1) x rows [j0, j0 + n / w) x
+// float4 chunks [q0, q0 + w) of each row.  Its n chunks are numbered row by
+// row (local index c -> row j0 + c / w, chunk q0 + c % w) and cut into tiles
+// of one CTA's chunks and runs of `ichunk` planes; work items of all
+// segments are numbered consecutively from work0.  A segment of whole rows
+// (q0 = 0, w = chunks per row) is a contiguous range of the plane; a partial
+// one (the chunks between or inside the z slabs) is not, and its row ends
+// fall inside warps.
 struct Seg {
-  int i0, i1, c0, c1;
+  int i0, i1;
+  int j0, q0, w, n;
   int tiles, work0;
 };
-constexpr int kMaxSeg = 4;
+constexpr int kMaxSeg = 6;
 
 struct Geom {
   int nx, ny, nz, nzp, nzq;  // nzq = nzp / 4 float4 chunks per row
@@ -62,9 +67,11 @@ struct Geom {
   Seg seg[kMaxSeg];
 };
 
-// Work item w -> segment, tile and plane run.
+// Work item w -> segment, tile (local chunks [c0, c1)) and plane run.
 struct Item {
   int c0, c1, i0, i1, tile;
+  int j0, q0, w;
+  bool whole;  // whole rows: c0..c1 is contiguous in the plane
 };
 __device__ __forceinline__ Item work_item(const Geom& g, int w) {
   int s = 0;
@@ -73,10 +80,14 @@ __device__ __forceinline__ Item work_item(const Geom& g, int w) {
   const int lw = w - S.work0;
   Item it;
   it.tile = lw % S.tiles;
-  it.c0 = S.c0 + it.tile * (int)blockDim.x;
-  it.c1 = min(it.c0 + (int)blockDim.x, S.c1);
+  it.c0 = it.tile * (int)blockDim.x;
+  it.c1 = min(it.c0 + (int)blockDim.x, S.n);
   it.i0 = S.i0 + (lw / S.tiles) * g.ichunk;
   it.i1 = min(it.i0 + g.ichunk, S.i1);
+  it.j0 = S.j0;
+  it.q0 = S.q0;
+  it.w = S.w;
+  it.whole = S.w == g.nzq;
   return it;
 }
 
@@ -433,17 +444,21 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
     int c = it.c0 + (int)threadIdx.x;
     const bool valid = c < it.c1;
     if (!valid) c = it.c1 - 1;
-    const int j = c / g.nzq;
-    const int k0 = (c - j * g.nzq) * 4;
+    const int jr = c / it.w;
+    const int qr = c - jr * it.w;
+    const int j = it.j0 + jr;
+    const int k0 = (it.q0 + qr) * 4;
     const int i0 = it.i0;
     const int i1 = it.i1;
     const bool has_jp = j + 1 < g.ny;
-    const bool need_kn = lane == 31 && k0 + 4 < g.nz;
+    // the next chunk comes from lane + 1 unless this lane ends the warp or
+    // its segment's part of the row
+    const bool need_kn = (lane == 31 || qr == it.w - 1) && k0 + 4 < g.nz;
     unsigned live = 0;
 #pragma unroll
     for (int e = 0; e < 4; ++e) live |= (k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
-    if (IO::kFloat && g.pf > 0 && threadIdx.x == 0) {
+    if (IO::kFloat && g.pf > 0 && it.whole && threadIdx.x == 0) {
       const long long tn = (long long)(it.c1 - it.c0) * 4;
       for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_h_plane<kIdBytes>(a, q + p * g.plane, tn);
     }
@@ -451,7 +466,7 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
     float4 ez4 = IO::ldg4(a.ez, q);
     for (int i = i0; i < i1; ++i, q += g.plane) {
       const bool has_ip = i + 1 < g.nx;
-      if (IO::kFloat && g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+      if (IO::kFloat && g.pf > 0 && it.whole && threadIdx.x == 0 && i + g.pf < i1)
         prefetch_h_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       // ---- every load of this plane first
       const float4 ex4 = IO::ldg4(a.ex, q);
@@ -587,18 +602,22 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
     int c = it.c0 + (int)threadIdx.x;
     const bool valid = c < it.c1;
     if (!valid) c = it.c1 - 1;
-    const int j = c / g.nzq;
-    const int k0 = (c - j * g.nzq) * 4;
+    const int jr = c / it.w;
+    const int qr = c - jr * it.w;
+    const int j = it.j0 + jr;
+    const int k0 = (it.q0 + qr) * 4;
     const int i0 = it.i0;
     const int i1 = it.i1;
     const bool has_jm = j >= 1;
-    const bool need_km = lane == 0 && k0 >= 4;
+    // the previous chunk comes from lane - 1 unless this lane starts the
+    // warp or its segment's part of the row
+    const bool need_km = (lane == 0 || qr == 0) && k0 >= 4;
     // elements that are updated: 1 <= k < nz (i >= 1 and j >= 1 checked per plane)
     unsigned live_k = 0;
 #pragma unroll
     for (int e = 0; e < 4; ++e) live_k |= (k0 + e >= 1 && k0 + e < g.nz ? 1u : 0u) << e;
     long long q = (long long)i0 * g.plane + (long long)j * g.nzp + k0;
-    if (IO::kFloat && g.pf > 0 && threadIdx.x == 0) {
+    if (IO::kFloat && g.pf > 0 && it.whole && threadIdx.x == 0) {
       const long long tn = (long long)(it.c1 - it.c0) * 4;
       for (int p = 0; p < min(g.pf, i1 - i0); ++p) prefetch_e_plane<kIdBytes>(a, q + p * g.plane, tn);
     }
@@ -608,7 +627,7 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
       hzm4 = IO::ldg4(a.hz, q - g.plane);
     }
     for (int i = i0; i < i1; ++i, q += g.plane) {
-      if (IO::kFloat && g.pf > 0 && threadIdx.x == 0 && i + g.pf < i1)
+      if (IO::kFloat && g.pf > 0 && it.whole && threadIdx.x == 0 && i + g.pf < i1)
         prefetch_e_plane<kIdBytes>(a, q + g.pf * g.plane, (long long)(it.c1 - it.c0) * 4);
       const bool upd = i >= 1 && has_jm;
       const unsigned live = upd ? live_k : 0u;

@@ -926,8 +926,10 @@ class Engine:
     def __init__(self, operator: Operator, engine_type: EngineType = EngineType.Cuda, *,
                  device: int = -1, compressed: bool = False, autotune: bool = True,
                  graphs: bool = True, kernels: str = "auto", storage: str = "f32"):
-        """kernels: "auto" (tuner picks), "register", "staged" (bulk-async) or
-        "split" (staged between the x / y CPML slabs, register on them).
+        """kernels: "auto" (tuner picks), "register", "staged" (bulk-async),
+        "split" (staged between the x / y CPML slabs, register on them) or
+        "zsplit" (plain register kernels on the CPML-free box, CPML register
+        kernels on every slab cell).
         storage: field storage "f32", or "f16" / "bf16" (2 bytes per value,
         float arithmetic; register kernels, CPML, sources, probes, energies)."""
         if engine_type is not EngineType.Cuda:
@@ -937,7 +939,8 @@ class Engine:
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
             | (0 if graphs else N.ENGINE_NO_GRAPHS) \
             | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS,
-               "split": N.ENGINE_SPLIT_KERNELS}[kernels] | N.STORAGE_FLAGS[storage]
+               "split": N.ENGINE_SPLIT_KERNELS, "zsplit": N.ENGINE_ZSPLIT_KERNELS}[kernels] \
+            | N.STORAGE_FLAGS[storage]
         desc = N.OperatorDesc()
         N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))
         h = ctypes.c_void_p()
@@ -1158,13 +1161,15 @@ class Engine:
 
     # -- checkpoint / resume (openems_b200.checkpoint) ----------------------
 
-    def state_sections(self) -> List[Tuple[int, int]]:
-        """(kind, bytes) of every state section, in the engine's order."""
+    def state_sections(self) -> List[Tuple[int, int, int]]:
+        """(kind, bytes, variant) of every state section, in the engine's
+        order; variant is the field storage type of the fields section (0
+        float, 1 half, 2 bfloat16) and 0 for the others."""
         n = N.c_u64()
         N.check(N.lib().oems_engine_state_sections(self._h, None, 0, ctypes.byref(n)))
         arr = (N.StateSectionC * max(n.value, 1))()
         N.check(N.lib().oems_engine_state_sections(self._h, arr, n.value, ctypes.byref(n)))
-        return [(int(arr[i].kind), int(arr[i].bytes)) for i in range(n.value)]
+        return [(int(arr[i].kind), int(arr[i].bytes), int(arr[i].variant)) for i in range(n.value)]
 
     def read_state(self, index: int, nbytes: int) -> bytearray:
         buf = bytearray(int(nbytes))
@@ -1172,9 +1177,11 @@ class Engine:
         N.check(N.lib().oems_engine_read_state(self._h, int(index), ptr, int(nbytes)))
         return buf
 
-    def write_state(self, index: int, data: bytes) -> None:
+    def write_state(self, index: int, data: bytes, variant: int = 0) -> None:
+        """Writes section `index`; `variant` must be the section's (the field
+        storage type for the fields section)."""
         data = bytes(data)
-        N.check(N.lib().oems_engine_write_state(self._h, int(index), data, len(data)))
+        N.check(N.lib().oems_engine_write_state(self._h, int(index), int(variant), data, len(data)))
 
     def state_counters(self) -> Tuple[int, int]:
         """(timestep, TF/SF step)."""
@@ -1215,6 +1222,19 @@ class Engine:
         N.check(N.lib().oems_engine_launch_info(self._h, *[ctypes.byref(x) for x in v]))
         keys = ("staged", "threads", "ichunk", "rows_per_tile", "stages", "grid")
         return {k: int(x.value) for k, x in zip(keys, v)}
+
+    def tune_report(self) -> list:
+        """Launch shapes the autotuner timed for this grid: dicts with kind (0
+        register, 1 staged, 2 staged interior + register slabs, 3 register
+        z-only interior + full-CPML slabs), threads, ichunk, extra (stages or
+        prefetch distance), reps and ms (device time of the timed H + E pairs)."""
+        n = N.c_u64()
+        N.check(N.lib().oems_engine_tune_report(self._h, None, 0, ctypes.byref(n)))
+        rec = np.zeros(int(n.value), dtype=[("kind", "<i4"), ("threads", "<i4"), ("ichunk", "<i4"),
+                                            ("extra", "<i4"), ("reps", "<i4"), ("ms", "<f4")])
+        if len(rec):
+            N.check(N.lib().oems_engine_tune_report(self._h, rec.ctypes.data, len(rec), ctypes.byref(n)))
+        return [{k: (float(r[k]) if k == "ms" else int(r[k])) for k in rec.dtype.names} for r in rec]
 
     def last_batch_stats(self) -> Tuple[int, float]:
         n, s = N.c_u64(), N.c_f64()

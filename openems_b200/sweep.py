@@ -164,9 +164,12 @@ def shard_instances(costs, world: int):
     return [sorted(sh) for sh in shards]
 
 
-def run_sharded(costs, run_local, dist=None):
+def run_sharded(costs, run_local, dist=None, group=None):
     """Runs this rank's share of the instances and gathers every rank's
-    results on rank 0, the only collective of the path.
+    results on rank 0, the only collective of the path.  `group` is the
+    process group of the gather: give it a gloo group, so that a rank whose
+    failure was a sticky CUDA error (its context unusable) can still report
+    it; with NCCL the gather would move the objects through CUDA tensors.
 
     run_local(indices) -> (results {index: result}, wall_s, cell_steps).
     Rank 0 gets {"results": [result per instance, in index order], "wall_s":
@@ -194,7 +197,7 @@ def run_sharded(costs, run_local, dist=None):
         parts = [mine]
     else:
         parts = [None] * world if rank == 0 else None
-        dist.gather_object(mine, parts, dst=0)
+        dist.gather_object(mine, parts, dst=0, group=group)
         if rank != 0:
             if failure is not None:
                 raise failure
@@ -233,7 +236,7 @@ def main(argv=None):
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--out", default=None, help="write S11 per instance to this .npz")
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32", help="field storage")
-    p.add_argument("--dist-timeout", type=float, default=3600.0,
+    p.add_argument("--dist-timeout", type=float, default=900.0,
                    help="seconds a rank waits at the final gather (several GPUs)")
     a = p.parse_args(argv)
     freqs = np.linspace(0.0, 8e9, a.freqs)
@@ -247,6 +250,11 @@ def main(argv=None):
         torch.cuda.set_device(device)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=a.dist_timeout),
                                 device_id=torch.device("cuda", device))
+        # the results travel over gloo: host memory only, so a rank with a
+        # broken CUDA context still delivers its error report
+        gather_group = dist.new_group(backend="gloo", timeout=datetime.timedelta(seconds=a.dist_timeout))
+    else:
+        gather_group = None
     setup = [0.0]
 
     def run_local(indices):
@@ -262,7 +270,7 @@ def main(argv=None):
         return out, wall, cell_steps
 
     try:
-        job = run_sharded([instance_cost(sp.dims) for sp in specs], run_local, dist)
+        job = run_sharded([instance_cost(sp.dims) for sp in specs], run_local, dist, gather_group)
     finally:
         if dist is not None:
             dist.destroy_process_group()

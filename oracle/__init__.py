@@ -64,6 +64,7 @@ def lib() -> ctypes.CDLL:
         L.orc_new.argtypes = [I32, I64, I64, I64, D, D, D, D]
         L.orc_free.argtypes = [P]
         L.orc_set_threads.argtypes = [P, I32]
+        L.orc_set_zline.argtypes = [P, I32]
         L.orc_set_material.argtypes = [P, D, D, D, D, P]
         L.orc_set_pec.argtypes = [P, P]
         L.orc_get_coefficients.argtypes = [P, P]
@@ -150,7 +151,7 @@ def excitation_eval(kind, params, amplitude, t):
 class OracleSim:
     """One oracle simulation (BasicEngine semantics) in FP32 or FP64."""
 
-    def __init__(self, nx, ny, nz, dt, delta, precision=32, threads=1):
+    def __init__(self, nx, ny, nz, dt, delta, precision=32, threads=1, zline=False):
         self.shape = (nx, ny, nz)
         self.n = nx * ny * nz
         self.dt = dt
@@ -162,6 +163,11 @@ class OracleSim:
         self.num_probes = 0
         self._last_steps = 0
         lib().orc_set_threads(self._h, threads)
+        lib().orc_set_zline(self._h, int(bool(zline)))
+
+    def set_zline(self, on: bool):
+        """Switch the H / E loops to the SIMD engine's z-line form (same bits)."""
+        lib().orc_set_zline(self._h, int(bool(on)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -78,6 +78,7 @@ struct Sim {
   double dt;
   double delta[3];
   int threads = 1;
+  bool zline = false;  // z-line (SimdEngine) loop form of the H / E updates
   uint64_t timestep = 0;
   std::vector<T> E[3], H[3], ca[3], cb[3], da[3], db[3];
 
@@ -465,8 +466,12 @@ struct Sim {
         F.c_h.resize(L);
         F.ik_h.resize(L);
         for (int l = 0; l < L; ++l) {
-          double depth_e = s == 0 ? (double)(L - l) * delta[a] : (double)(l + 1) * delta[a];
-          double depth_h = depth_e - 0.5 * delta[a];
+          // grading of src/extensions/cpml.rs:114-155 at the positions of
+          // the differences (min face: E (L - l) d, H half a cell shallower;
+          // max face: E l d, H half a cell deeper); the reference's max-face
+          // depths ((l + 1) d and (l + 1/2) d) mismatch E and H by a cell
+          double depth_e = s == 0 ? (double)(L - l) * delta[a] : (double)l * delta[a];
+          double depth_h = s == 0 ? depth_e - 0.5 * delta[a] : depth_e + 0.5 * delta[a];
           for (int w = 0; w < 2; ++w) {
             double depth = w == 0 ? depth_e : depth_h;
             double rho = std::min(1.0, std::max(0.0, depth / width));
@@ -533,8 +538,181 @@ struct Sim {
     d = stretch(d, psi_e[which][q], T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
   }
 
+  // CPML stretch of one z-line of differences d[k0, k1) with the profile of
+  // one layer (x / y slabs: the whole line shares the layer).
+  static void stretch_line(T* d, T* psi, int64_t k0, int64_t k1, T b, T c, T ik) {
+    for (int64_t k = k0; k < k1; ++k) d[k] = stretch(d[k], psi[k], b, c, ik);
+  }
+  // z slabs of one line: each k has its own layer.
+  void stretch_zslabs(T* d, T* psi, bool is_h) const {
+    for (int s = 0; s < 2; ++s) {
+      const CpmlFace& F = face[4 + s];
+      if (F.layers <= 0) continue;
+      const int64_t k0 = s == 0 ? 0 : nz - F.layers, k1 = s == 0 ? F.layers : nz;
+      for (int64_t k = k0; k < k1; ++k) {
+        const int l = layer[2][k];
+        d[k] = is_h ? stretch(d[k], psi[k], T(F.b_h[l]), T(F.c_h[l]), T(F.ik_h[l]))
+                    : stretch(d[k], psi[k], T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
+      }
+    }
+  }
+  void stretch_row(int axis, int64_t g, T* d, T* psi, bool is_h) const {
+    const int s = side[axis][g];
+    if (s < 0) return;
+    const CpmlFace& F = face[2 * axis + s];
+    const int l = layer[axis][g];
+    if (is_h)
+      stretch_line(d, psi, 0, nz, T(F.b_h[l]), T(F.c_h[l]), T(F.ik_h[l]));
+    else
+      stretch_line(d, psi, 0, nz, T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
+  }
+
+  // The same H update in the loop form of the reference's SimdEngine
+  // (src/fdtd/simd_engine.rs:252-331): per (i, j) z-line, the differences are
+  // formed in contiguous row buffers (a missing neighbour line gives 0, the
+  // last k of a z difference is 0), CPML stretches the slab parts of those
+  // rows, then one loop per component updates the line.  Every value goes
+  // through the same rounded operations as update_h, so the results are
+  // bit-identical; only the loop order differs, which lets the compiler
+  // vectorise the k loops.  OpenMP over x-planes as the parallel engine.
+  void update_h_zline() {
+    const T* ex = E[0].data();
+    const T* ey = E[1].data();
+    const T* ez = E[2].data();
+#pragma omp parallel num_threads(threads) if (threads > 1)
+    {
+      std::vector<T> buf(6 * nz);
+      T* dzy = buf.data();
+      T* dyz = dzy + nz;
+      T* dxz = dyz + nz;
+      T* dzx = dxz + nz;
+      T* dyx = dzx + nz;
+      T* dxy = dyx + nz;
+#pragma omp for schedule(static)
+      for (int64_t i = 0; i < nx; ++i)
+        for (int64_t j = 0; j < ny; ++j) {
+          const int64_t q = idx(i, j, 0);
+          const T* exl = ex + q;
+          const T* eyl = ey + q;
+          const T* ezl = ez + q;
+          if (j + 1 < ny) {
+            for (int64_t k = 0; k < nz; ++k) dzy[k] = ezl[k + nz] - ezl[k];
+            for (int64_t k = 0; k < nz; ++k) dxy[k] = exl[k + nz] - exl[k];
+          } else {
+            for (int64_t k = 0; k < nz; ++k) dzy[k] = dxy[k] = T(0);
+          }
+          for (int64_t k = 0; k + 1 < nz; ++k) dyz[k] = eyl[k + 1] - eyl[k];
+          for (int64_t k = 0; k + 1 < nz; ++k) dxz[k] = exl[k + 1] - exl[k];
+          dyz[nz - 1] = dxz[nz - 1] = T(0);
+          if (i + 1 < nx) {
+            const int64_t P = ny * nz;
+            for (int64_t k = 0; k < nz; ++k) dzx[k] = ezl[k + P] - ezl[k];
+            for (int64_t k = 0; k < nz; ++k) dyx[k] = eyl[k + P] - eyl[k];
+          } else {
+            for (int64_t k = 0; k < nz; ++k) dzx[k] = dyx[k] = T(0);
+          }
+          if (cpml) {
+            stretch_row(1, j, dzy, psi_h[0].data() + q, true);
+            stretch_zslabs(dyz, psi_h[1].data() + q, true);
+            stretch_zslabs(dxz, psi_h[2].data() + q, true);
+            stretch_row(0, i, dzx, psi_h[3].data() + q, true);
+            stretch_row(0, i, dyx, psi_h[4].data() + q, true);
+            stretch_row(1, j, dxy, psi_h[5].data() + q, true);
+          }
+          line_update(H[0].data() + q, da[0].data() + q, db[0].data() + q, dzy, dyz, 0);
+          line_update(H[1].data() + q, da[1].data() + q, db[1].data() + q, dxz, dzx, 0);
+          line_update(H[2].data() + q, da[2].data() + q, db[2].data() + q, dyx, dxy, 0);
+        }
+    }
+  }
+
+  // f[k] = a[k] * f[k] + b[k] * (d1[k] - d2[k]) for k in [k0, nz), each
+  // product and sum rounded.
+  void line_update(T* __restrict f, const T* __restrict a, const T* __restrict b, const T* __restrict d1,
+                   const T* __restrict d2, int64_t k0) const {
+    for (int64_t k = k0; k < nz; ++k) {
+      const T curl = d1[k] - d2[k];
+      const T t0 = a[k] * f[k];
+      const T t1 = b[k] * curl;
+      f[k] = t0 + t1;
+    }
+  }
+
+  // E update in the SimdEngine loop form (src/fdtd/simd_engine.rs:339-391):
+  // lines with i, j >= 1, elements k >= 1; bit-identical to update_e.
+  void update_e_zline() {
+    const T* hx = H[0].data();
+    const T* hy = H[1].data();
+    const T* hz = H[2].data();
+#pragma omp parallel num_threads(threads) if (threads > 1)
+    {
+      std::vector<T> buf(6 * nz);
+      T* dzy = buf.data();
+      T* dyz = dzy + nz;
+      T* dxz = dyz + nz;
+      T* dzx = dxz + nz;
+      T* dyx = dzx + nz;
+      T* dxy = dyx + nz;
+      const int64_t P = ny * nz;
+#pragma omp for schedule(static)
+      for (int64_t i = 1; i < nx; ++i)
+        for (int64_t j = 1; j < ny; ++j) {
+          const int64_t q = idx(i, j, 0);
+          const T* hxl = hx + q;
+          const T* hyl = hy + q;
+          const T* hzl = hz + q;
+          for (int64_t k = 1; k < nz; ++k) dzy[k] = hzl[k] - hzl[k - nz];
+          for (int64_t k = 1; k < nz; ++k) dyz[k] = hyl[k] - hyl[k - 1];
+          for (int64_t k = 1; k < nz; ++k) dxz[k] = hxl[k] - hxl[k - 1];
+          for (int64_t k = 1; k < nz; ++k) dzx[k] = hzl[k] - hzl[k - P];
+          for (int64_t k = 1; k < nz; ++k) dyx[k] = hyl[k] - hyl[k - P];
+          for (int64_t k = 1; k < nz; ++k) dxy[k] = hxl[k] - hxl[k - nz];
+          dzy[0] = dyz[0] = dxz[0] = dzx[0] = dyx[0] = dxy[0] = T(0);
+          if (cpml) {
+            // element k = 0 is never written, so stretching it (with its
+            // psi, which stays untouched at 0 -> b*0 + c*0) is harmless only
+            // if it does not change psi: skip it by starting at k = 1.
+            stretch_row_from1(1, j, dzy, psi_e[0].data() + q, false);
+            stretch_zslabs_from1(dyz, psi_e[1].data() + q);
+            stretch_zslabs_from1(dxz, psi_e[2].data() + q);
+            stretch_row_from1(0, i, dzx, psi_e[3].data() + q, false);
+            stretch_row_from1(0, i, dyx, psi_e[4].data() + q, false);
+            stretch_row_from1(1, j, dxy, psi_e[5].data() + q, false);
+          }
+          line_update(E[0].data() + q, ca[0].data() + q, cb[0].data() + q, dzy, dyz, 1);
+          line_update(E[1].data() + q, ca[1].data() + q, cb[1].data() + q, dxz, dzx, 1);
+          line_update(E[2].data() + q, ca[2].data() + q, cb[2].data() + q, dyx, dxy, 1);
+        }
+    }
+  }
+  void stretch_row_from1(int axis, int64_t g, T* d, T* psi, bool is_h) const {
+    const int s = side[axis][g];
+    if (s < 0) return;
+    const CpmlFace& F = face[2 * axis + s];
+    const int l = layer[axis][g];
+    if (is_h)
+      stretch_line(d, psi, 1, nz, T(F.b_h[l]), T(F.c_h[l]), T(F.ik_h[l]));
+    else
+      stretch_line(d, psi, 1, nz, T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
+  }
+  void stretch_zslabs_from1(T* d, T* psi) const {
+    for (int s = 0; s < 2; ++s) {
+      const CpmlFace& F = face[4 + s];
+      if (F.layers <= 0) continue;
+      const int64_t k0 = s == 0 ? 1 : nz - F.layers, k1 = s == 0 ? F.layers : nz;
+      for (int64_t k = std::max<int64_t>(k0, 1); k < k1; ++k) {
+        const int l = layer[2][k];
+        d[k] = stretch(d[k], psi[k], T(F.b_e[l]), T(F.c_e[l]), T(F.ik_e[l]));
+      }
+    }
+  }
+
   // src/fdtd/basic_engine.rs:191-254
   void update_h() {
+    if (zline) {
+      update_h_zline();
+      return;
+    }
     const T* ex = E[0].data();
     const T* ey = E[1].data();
     const T* ez = E[2].data();
@@ -574,6 +752,10 @@ struct Sim {
 
   // src/fdtd/basic_engine.rs:262-306 (only i, j, k >= 1 are updated)
   void update_e() {
+    if (zline) {
+      update_e_zline();
+      return;
+    }
     const T* hx = H[0].data();
     const T* hy = H[1].data();
     const T* hz = H[2].data();
@@ -1111,6 +1293,7 @@ void orc_free(orc_sim* s) {
 }
 
 void orc_set_threads(orc_sim* s, int32_t threads) { DISPATCH(s, S->threads = threads < 1 ? 1 : threads); }
+void orc_set_zline(orc_sim* s, int32_t on) { DISPATCH(s, S->zline = on != 0); }
 
 void orc_set_material(orc_sim* s, double eps_r, double mu_r, double sigma_e, double sigma_m,
                       const int64_t* r) {

@@ -83,6 +83,11 @@ orc_sim* orc_new(int32_t precision, int64_t nx, int64_t ny, int64_t nz, double d
                  double dx, double dy, double dz);
 void orc_free(orc_sim* s);
 void orc_set_threads(orc_sim* s, int32_t threads);
+/* Loop form of the H / E updates: 0 the parallel engine's cell loop
+ * (src/fdtd/parallel_engine.rs:108-172), 1 the SIMD engine's z-lines
+ * (src/fdtd/simd_engine.rs:252-391) with OpenMP over x-planes.  Both give
+ * identical bits. */
+void orc_set_zline(orc_sim* s, int32_t on);
 
 /* Operator::set_material / set_pec (src/fdtd/operator.rs:187-263). region =
  * i0,i1,j0,j1,k0,k1 (half-open). */

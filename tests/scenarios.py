@@ -87,11 +87,12 @@ def run_engine(sc: Scenario, compressed=False, graphs=True, autotune=True, kerne
             "timestep": eng.current_timestep(), "engine": eng, "operator": op}
 
 
-def run_oracle(sc: Scenario, precision=32, threads=1):
-    """Runs the scenario on the oracle (BasicEngine semantics)."""
+def run_oracle(sc: Scenario, precision=32, threads=1, zline=False):
+    """Runs the scenario on the oracle (BasicEngine semantics); zline picks
+    the SIMD engine's loop form (same bits, faster on large grids)."""
     lines = [oracle.uniform_lines(n, sc.delta) for n in sc.dims]
     dt, delta = oracle.grid_timestep(*lines)
-    s = oracle.OracleSim(*sc.dims, dt, delta, precision=precision, threads=threads)
+    s = oracle.OracleSim(*sc.dims, dt, delta, precision=precision, threads=threads, zline=zline)
     for eps_r, mu_r, se, sm, reg in sc.materials:
         s.set_material(eps_r, mu_r, se, sm, reg)
     for reg in sc.pec:
@@ -239,6 +240,15 @@ def cpml_scenarios() -> List[Scenario]:
                  cpml=oe.CpmlBoundaries(layers=(4, 5, 0, 6, 7, 3), grading_order=4.0,
                                         reflection_coeff=1e-5, alpha_max=0.05, kappa_max=3.0),
                  probes=[(1, (9, 11, 14)), (5, (1, 1, 1))]),
+        # z slabs only, nz not a multiple of 4, a row of 12 chunks: the
+        # CPML-free box of a z-split has partial rows that end inside warps
+        Scenario("cpml_z_only_45", (14, 26, 45), 1e-3,
+                 materials=[(2.0, 1.0, 0.01, 0.0, (3, 11, 4, 20, 2, 43))],
+                 excitations=[E.gaussian_pulse(tau, 4 * tau, 2, (7, 13, 22)),
+                              E.gaussian_pulse(tau, 4 * tau, 0, (5, 9, 5))],
+                 num_steps=160, sample_interval=20, track_peak=True,
+                 cpml=oe.CpmlBoundaries(layers=(0, 0, 0, 0, 5, 6)),
+                 probes=[(2, (7, 13, 22)), (0, (5, 9, 2)), (4, (7, 13, 41))]),
     ]
 
 

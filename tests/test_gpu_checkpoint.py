@@ -49,7 +49,7 @@ def test_resume_in_fresh_engine_and_after_reset(name):
     a, dt = _engine(sc)
     _batch(a, sc, dt, 0, 60)
     blob = a.save_state()
-    kinds = [k for k, _ in a.state_sections()]
+    kinds = [k for k, _, _ in a.state_sections()]
     assert kinds[0] == 1  # the fields come first
     assert (2 in kinds) == (sc.cpml is not None) and (3 in kinds) == (sc.mur is not None)
     assert kinds.count(5) == len(sc.dispersive) and (6 in kinds) == bool(sc.rlc)
@@ -83,7 +83,7 @@ def test_resume_tfsf_with_cpml():
     a = build()
     a.run_batch(oe.EngineBatch(num_steps=50))
     blob = a.save_state()
-    assert [k for k, _ in a.state_sections()][-2:] == [10, 11]
+    assert [k for k, _, _ in a.state_sections()][-2:] == [10, 11]
     a.run_batch(oe.EngineBatch(num_steps=40))
     want = fields(a)
     assert np.abs(want).max() > 0
@@ -109,3 +109,17 @@ def test_resume_half_storage():
         c.load_state(blob)
     e, h = c.read_fields()
     assert np.array_equal(np.concatenate([e, h]), before) and c.current_timestep() == 5
+    # bfloat16 fields have the half section's size: the storage variant
+    # refuses the snapshot, in the blob check and in the C entry point
+    d, _ = _engine(sc, storage="bf16")
+    before = _batch(d, sc, dt, 0, 5)[0]
+    assert d.state_sections()[0][:2] == b.state_sections()[0][:2]
+    assert (d.state_sections()[0][2], b.state_sections()[0][2]) == (2, 1)
+    with pytest.raises(oe.ConfigError, match="variant"):
+        d.load_state(blob)
+    from openems_b200 import checkpoint
+    fields_bytes = checkpoint.parse(blob).sections[0][1]
+    with pytest.raises(oe.ConfigError):
+        d.write_state(0, fields_bytes, variant=1)
+    e, h = d.read_fields()
+    assert np.array_equal(np.concatenate([e, h]), before) and d.current_timestep() == 5

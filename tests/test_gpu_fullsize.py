@@ -1,0 +1,142 @@
+"""The benchmark configurations at their own size and step count, engine vs oracle.
+
+Config 2 (the timed workload): 256^3, 1 mm, 8-cell CPML (m = 3, R0 = 1e-6) on
+every face, 40 seeded dielectric boxes, soft Gaussian Ez 0-10 GHz at the
+centre, 10,000 timesteps in batches of 1000 with energy samples every 100
+steps, as `bench.py` runs it, with the launch shape the autotuner picks and
+with each kernel family forced.  Its variants: compressed coefficients
+(material id + table) and second-order Mur in place of CPML.  Config 3: the
+384^3 dispersive scene (Drude sphere, second-order Lorentz shell, 50 ohm
+lumped port in a wire dipole, CPML, NF2FF box with f64 DFTs) for 500 steps.
+
+The oracle restates the reference's update (src/fdtd/basic_engine.rs:191-306)
+in the loop form of its SIMD engine (src/fdtd/simd_engine.rs:252-391), on
+every host core.  Fields, probe traces and DFT accumulators must be
+bit-identical, so the stated gate (relative L2 <= 1e-5 per field array and
+probe trace after the stated step count) holds with margin; the test asserts
+both and prints the relative L2 of each array.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import openems_b200 as oe
+from openems_b200 import workloads
+from conftest import rel_l2
+from scenarios import Scenario, run_engine, run_oracle
+from test_gpu_parity import assert_parity
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+
+
+def config2_scenario(mur_order=0, steps=10000) -> Scenario:
+    wl = workloads.cpml_boxes(256, steps)
+    return Scenario(f"cpml_boxes_256{'_mur%d' % mur_order if mur_order else ''}", wl.dims, wl.delta,
+                    materials=list(wl.boxes), excitations=[wl.excitation()], num_steps=steps,
+                    sample_interval=100, track_peak=True,
+                    cpml=None if mur_order else wl.cpml(),
+                    mur=oe.MurAbcConfig.all(mur_order) if mur_order else None,
+                    probes=list(wl.probes), batches=(1000,) * (steps // 1000))
+
+
+def report(tag, got, ref):
+    errs = [rel_l2(got["fields"][c], ref["fields"][c]) for c in range(6)]
+    terr = [rel_l2(got["traces"][:, p], ref["traces"][:, p]) for p in range(ref["traces"].shape[1])]
+    print(f"{tag}: field rel-L2 {['%.1e' % e for e in errs]}, probe traces {['%.1e' % e for e in terr]}")
+
+
+@pytest.fixture(scope="module")
+def config2_oracle():
+    return run_oracle(config2_scenario(), precision=32, threads=THREADS, zline=True)
+
+
+@pytest.mark.parametrize("kernels", ("auto", "register", "zsplit", "staged"))
+def test_config2_cpml_boxes_256_10000_steps(config2_oracle, kernels):
+    got = run_engine(config2_scenario(), kernels=kernels)
+    report(f"config 2 ({kernels}, shape {got['engine'].launch_info()})", got, config2_oracle)
+    assert np.abs(config2_oracle["fields"]).max() > 0
+    assert_parity(got, config2_oracle)
+
+
+def test_config2_compressed_256_10000_steps(config2_oracle):
+    got = run_engine(config2_scenario(), compressed=True)
+    assert_parity(got, config2_oracle)
+
+
+def test_config2_mur2_256_10000_steps():
+    sc = config2_scenario(mur_order=2)
+    got = run_engine(sc)
+    ref = run_oracle(sc, precision=32, threads=THREADS, zline=True)
+    report("config 2, second-order Mur", got, ref)
+    assert_parity(got, ref)
+
+
+def test_config3_dispersive_scene_384_500_steps():
+    from openems_b200.scene import ScatterScene
+    sc = ScatterScene(n=384, steps=500)
+    op, port, sphere, shell = sc.operator()
+    eng = oe.Engine(op)
+    box = sc.attach(eng, port, sphere, shell)
+    exc = port.excitation(sc.waveform())
+    dt = op.timestep()
+    batches = (200, 300)
+    start = 0
+    for n in batches:
+        eng.run_batch(oe.EngineBatch(num_steps=n, excitations=[
+            oe.ScheduledExcitation.from_excitation(exc, start, n, dt)]))
+        start += n
+
+    # the same scene on the oracle, built from its own operator calls
+    lines = [oracle.uniform_lines(sc.n, sc.delta)] * 3
+    dt_o, d3 = oracle.grid_timestep(*lines)
+    assert dt_o == dt
+    s = oracle.OracleSim(sc.n, sc.n, sc.n, dt_o, d3, threads=THREADS, zline=True)
+    eps_inf = sc.lorentz[3]
+    for c in shell.astype(np.int64):
+        s.set_material(eps_inf, 1.0, 0.0, 0.0, (c[0], c[0] + 1, c[1], c[1] + 1, c[2], c[2] + 1))
+    px, py, pz = sc.port
+    s.set_pec((px, px + 1, py, py + 1, pz - sc.arm, pz))
+    s.set_pec((px, px + 1, py, py + 1, pz + 1, pz + 1 + sc.arm))
+    scale = s.set_lumped(sc.port, 2, 50.0, 0.0, 1.0, 0.0)
+    assert scale == pytest.approx(port.source_scale, rel=0, abs=0)
+    assert np.array_equal(s.coefficients(), op.coefficients())
+    s.enable_cpml((sc.layers,) * 6)
+    wp, g = sc.drude
+    d = oe.DrudeMaterial(wp, g, second_order=True).to_c()
+    s.add_dispersive(d.kind, list(d.params), sphere.astype(np.int64), d.eps_inf)
+    w0, gl, de, ei = sc.lorentz
+    d = oe.LorentzMaterial(w0, gl, de, eps_inf=ei, second_order=True).to_c()
+    s.add_dispersive(d.kind, list(d.params), shell.astype(np.int64), d.eps_inf)
+    freqs = np.asarray(sc.freqs)
+    dft = []
+    for kind in (0, 1):
+        t = oe.port_probe(op, sc.port, 2, kind)
+        dft.append(s.add_probe_dft(s.add_probe([(c, q, -w) for c, q, w in t.terms], t.mode), freqs))
+    lo, hi = sc.box
+    obox = s.add_nf2ff_box(lo, hi, list(sc.freqs), interval=sc.nf2ff_interval)
+    start = 0
+    for n in batches:
+        s.clear_excitations()
+        s.add_excitation_analytic(exc.position, exc.direction, True, int(exc.excitation_type),
+                                  list(exc.params), exc.amplitude, start, n)
+        s.run_batch(n)
+        start += n
+
+    e, h = eng.read_fields()
+    got = np.concatenate([e, h])
+    ref = s.fields()
+    errs = [rel_l2(got[c], ref[c]) for c in range(6)]
+    print("config 3 (500 steps): field rel-L2", ["%.1e" % v for v in errs])
+    assert np.abs(ref[2]).max() > 0
+    assert max(errs) <= 1e-5
+    assert np.array_equal(got, ref)
+    port.calc_port(eng)
+    assert np.array_equal(port.uf_tot, s.probe_dft(dft[0]))
+    assert np.array_equal(port.if_tot, s.probe_dft(dft[1]))
+    for face in range(6):
+        for fi in range(len(sc.freqs)):
+            assert np.array_equal(box.face(face, fi), s.nf2ff_face(obox, face, fi, lo, hi)), (face, fi)

@@ -67,7 +67,7 @@ def _failing_runner(indices):
     raise RuntimeError("device lost on this rank")
 
 
-def _rank(rank, world, port, costs, out, fail_rank=-1):
+def _rank(rank, world, port, costs, out, fail_rank=-1, own_group=False):
     import datetime
     import sys
     import torch.distributed as dist
@@ -75,9 +75,12 @@ def _rank(rank, world, port, costs, out, fail_rank=-1):
     from openems_b200.sweep import run_sharded
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    # the sweep's command line gathers over a gloo group of its own (beside
+    # the NCCL default group); own_group does the same here
+    group = dist.new_group(backend="gloo") if own_group else None
     try:
         try:
-            job = run_sharded(costs, _failing_runner if rank == fail_rank else _fake_runner(rank), dist)
+            job = run_sharded(costs, _failing_runner if rank == fail_rank else _fake_runner(rank), dist, group)
             out.put((rank, job))
         except Exception as e:
             out.put((rank, f"{type(e).__name__}: {e}"))
@@ -85,12 +88,12 @@ def _rank(rank, world, port, costs, out, fail_rank=-1):
         dist.destroy_process_group()
 
 
-def _spawn(costs, world, fail_rank=-1):
+def _spawn(costs, world, fail_rank=-1, own_group=False):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, costs, q, fail_rank)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, costs, q, fail_rank, own_group)) for r in range(world)]
     for p in procs:
         p.start()
     got = dict(q.get(timeout=120) for _ in procs)
@@ -100,10 +103,12 @@ def _spawn(costs, world, fail_rank=-1):
     return got
 
 
-def test_failed_rank_is_reported_not_waited_for():
+@pytest.mark.parametrize("own_group", (False, True))
+def test_failed_rank_is_reported_not_waited_for(own_group):
     """Rank 1's share raises: both ranks return promptly, rank 0 with an
-    error naming rank 1, rank 1 with its own exception."""
-    got = _spawn([1.0, 2.0, 3.0, 4.0], 2, fail_rank=1)
+    error naming rank 1, rank 1 with its own exception (over the default
+    group, and over a separate gloo group as the command line uses)."""
+    got = _spawn([1.0, 2.0, 3.0, 4.0], 2, fail_rank=1, own_group=own_group)
     assert got[0].startswith("OpenEMSError") and "rank 1: RuntimeError: device lost" in got[0]
     assert got[1] == "RuntimeError: device lost on this rank"
 
