@@ -197,11 +197,19 @@ typedef struct oems_mur_desc {
 
 /* PmlBoundaries (src/extensions/pml.rs:85-101): layers per face (-x +x -y
  * +y -z +z; a face is active when 0 < layers < n), polynomial grading order
- * and target reflection. */
+ * and target reflection.  kind 0: the reference's coefficients (they grow
+ * without bound); kind 1: the uniaxial PML of Taflove & Hagness 7.8 in the
+ * reference's flux form -- per-axis conductivities at each component's Yee
+ * position (edges and corners graded along every axis whose slab holds
+ * them), consistent flux coefficients, and the next axis' conductivity
+ * folded into the region cells' main update coefficients (Ca, Cb, Da, Db;
+ * PEC cells stay as they are).  Kind 1 needs full coefficient arrays. */
 typedef struct oems_upml_desc {
   uint32_t layers[6];
   double grading_order;
   double reflection_coeff;
+  int32_t kind;
+  int32_t reserved0;
 } oems_upml_desc;
 
 /* Dispersive material on a list of cells (src/extensions/dispersive.rs),
@@ -338,6 +346,29 @@ OEMS_API oems_status oems_engine_write_fields(oems_engine* engine, const float* 
 /* Clears fields, extension state and the timestep counter. */
 OEMS_API oems_status oems_engine_reset(oems_engine* engine);
 
+/* ---- packs: several engines stepped together ------------------------------
+ * No counterpart in the reference (its EngineBatch batches timesteps of one
+ * grid, src/fdtd/batch.rs:12-32).  A pack holds engines of one device and
+ * one field storage, with full coefficient arrays and only CPML, sources,
+ * probes and probe DFTs attached.  oems_pack_run_batch runs batches[i] on
+ * engine i for every i with batches[i] != NULL, with the results and state
+ * oems_engine_run_batch would give each engine on its own (bit for bit),
+ * but every half-step of all of them is one launch of the plain update
+ * kernels over their CPML-free boxes and one of the CPML kernels over their
+ * slab cells, replayed from CUDA graphs, with one post-step launch and one
+ * energy launch pair for all.  The batches must share num_steps,
+ * sample_interval, check_interval and whether they carry an energy-decay end
+ * condition, and their engines must be at the same timestep; each engine
+ * keeps its own decay threshold, peak and termination step.  statuses[i] is
+ * OEMS_ERR_NUMERICAL for an engine whose energy stopped being finite (it
+ * stops at that check), OEMS_OK otherwise.  The engines must not be used
+ * elsewhere while a pack call runs; destroy the pack before its engines. */
+typedef struct oems_pack oems_pack;
+OEMS_API oems_status oems_pack_create(oems_engine* const* engines, uint64_t count, oems_pack** out);
+OEMS_API void oems_pack_destroy(oems_pack* pack);
+OEMS_API oems_status oems_pack_run_batch(oems_pack* pack, const oems_batch* const* batches,
+                                         oems_batch_result* results, oems_status* statuses);
+
 /* ---- checkpoint / resume --------------------------------------------------
  * The engine's evolving state as sections: the buffers oems_engine_reset
  * clears (fields in their storage type, CPML psi, Mur, probe DFTs, each
@@ -393,10 +424,10 @@ OEMS_API oems_status oems_engine_add_mur(oems_engine* engine, const oems_mur_des
  * there.  Float field storage only. */
 OEMS_API oems_status oems_engine_add_tfsf(oems_engine* engine, const oems_tfsf_desc* desc);
 /* Upml::new (src/extensions/pml.rs:209-219) with the flux hooks of
- * pml.rs:505-655 around the H and E updates.  Reproduces the reference's
- * coefficients, under which the scheme grows without bound (the reference
- * disables its PML tests, src/fdtd/engine_testing.rs:2322-2330); use
- * oems_engine_add_cpml for absorption. */
+ * pml.rs:505-655 around the H and E updates.  Kind 0 reproduces the
+ * reference's coefficients, under which the scheme grows without bound (the
+ * reference disables its PML tests, src/fdtd/engine_testing.rs:2322-2330);
+ * kind 1 is the corrected uniaxial PML (see oems_upml_desc). */
 OEMS_API oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc);
 /* LorentzMaterial / DrudeMaterial / DebyeMaterial::new (src/extensions/
  * dispersive.rs:134, 476, 570); cells: ncells x (i, j, k). Materials apply in

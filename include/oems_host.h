@@ -245,6 +245,14 @@ OEMS_API oems_status oems_sweep_set_trace_steps(oems_sweep* sweep, uint64_t step
 /* out: cap_steps x 2 doubles; *nsteps receives the recorded step count. */
 OEMS_API oems_status oems_sweep_get_trace(const oems_sweep* sweep, int32_t instance_id, double* out,
                                           uint64_t cap_steps, uint64_t* nsteps);
+/* on != 0: oems_sweep_run / run_until step the instances that have run the
+ * same number of steps together through one pack (oems_pack_run_batch in
+ * oems.h): shared launches over all their grids instead of one engine and
+ * stream per instance, each instance ending with the same bits.  Needs full
+ * coefficient arrays (no OEMS_ENGINE_COMPRESSED).  host_seconds of a packed
+ * instance is the wall time of the packed runs it took part in.
+ * oems_sweep_advance always runs one instance on its own. */
+OEMS_API oems_status oems_sweep_set_packed(oems_sweep* sweep, int32_t on);
 /* Wall time of the last run / run_until call and the cell x timestep count
  * it executed. */
 OEMS_API oems_status oems_sweep_stats(const oems_sweep* sweep, double* wall_seconds, double* cell_steps);

@@ -140,7 +140,8 @@ class MurDescC(ctypes.Structure):
 
 
 class UpmlDescC(ctypes.Structure):
-    _fields_ = [("layers", c_u32 * 6), ("grading_order", c_f64), ("reflection_coeff", c_f64)]
+    _fields_ = [("layers", c_u32 * 6), ("grading_order", c_f64), ("reflection_coeff", c_f64), ("kind", c_i32),
+                ("reserved0", c_i32)]
 
 
 class DispersiveDescC(ctypes.Structure):
@@ -288,6 +289,10 @@ SIGNATURES = {
                                       ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_sweep_stats": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
     "oems_sweep_set_trace_steps": (c_i32, [P, c_u64]),
+    "oems_sweep_set_packed": (c_i32, [P, c_i32]),
+    "oems_pack_create": (c_i32, [ctypes.POINTER(P), c_u64, ctypes.POINTER(P)]),
+    "oems_pack_destroy": (None, [P]),
+    "oems_pack_run_batch": (c_i32, [P, ctypes.POINTER(ctypes.c_void_p), P, ctypes.POINTER(c_i32)]),
     "oems_sweep_run_until": (c_i32, [P, c_u64, c_u64]),
     "oems_sweep_finish": (c_i32, [P, c_i32]),
     "oems_sweep_advance": (c_i32, [P, c_i32, c_u64, c_u64]),

@@ -109,9 +109,9 @@ __device__ __forceinline__ float field_value(const PostArgs& a, int c, long long
   }
 }
 
-template <typename T = float>
-__global__ void k_post_step(const PostArgs a) {
-  const long long s = *a.d_base + a.local;
+// Post-step work of batch step s (one CTA).
+template <typename T>
+__device__ __forceinline__ void post_step_body(const PostArgs& a, long long s) {
   if (threadIdx.x == 0) {
     for (int x = 0; x < a.nexc; ++x) {
       if (s >= a.exc_count[x]) continue;
@@ -147,6 +147,17 @@ __global__ void k_post_step(const PostArgs a) {
     }
     a.traces[s * a.nprobe + p] = val;
   }
+}
+
+template <typename T = float>
+__global__ void k_post_step(const PostArgs a) {
+  post_step_body<T>(a, *a.d_base + a.local);
+}
+
+// The post-step work of several grids (a pack): CTA b does grid b's.
+template <typename T = float>
+__global__ void k_post_step_pack(const PostArgs* args, const long long* d_base, int local) {
+  post_step_body<T>(args[blockIdx.x], *d_base + local);
 }
 
 // Running DFT of probe traces over the steps of a batch
@@ -222,8 +233,8 @@ struct EnergyArgs {
   double* partials;      // [6][kEnergyBlocks]
 };
 
-template <typename T = float>
-__global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyArgs a) {
+template <typename T>
+__device__ __forceinline__ void energy_partial_body(const EnergyArgs& a) {
   const float4* p = reinterpret_cast<const float4*>(a.arr[blockIdx.y]);
   double s = 0.0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.n4;
@@ -246,11 +257,23 @@ __global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyA
   if (threadIdx.x == 0) a.partials[blockIdx.y * kEnergyBlocks + blockIdx.x] = red[0];
 }
 
+template <typename T = float>
+__global__ void __launch_bounds__(kEnergyThreads) k_energy_partial(const EnergyArgs a) {
+  energy_partial_body<T>(a);
+}
+
+// Several grids: blockIdx.z picks the grid; each grid's partition and sum
+// order are those of k_energy_partial, so its energies are the same bits.
+template <typename T = float>
+__global__ void __launch_bounds__(kEnergyThreads) k_energy_partial_pack(const EnergyArgs* args) {
+  energy_partial_body<T>(args[blockIdx.z]);
+}
+
 // out[0] = E energy, out[1] = H energy (each the sum over its 3 components in
 // component order, like VectorField3D::energy, src/arrays/field.rs:314-316).
 // h_inv2: 1 / the square of the H storage scale (1 for float storage; a
 // power of two, so exact).
-__global__ void k_energy_final(const double* partials, double* out, double h_inv2) {
+__device__ __forceinline__ void energy_final_body(const double* partials, double* out, double h_inv2) {
   __shared__ double comp[6];
   const int c = threadIdx.x;
   if (c < 6) {
@@ -263,6 +286,15 @@ __global__ void k_energy_final(const double* partials, double* out, double h_inv
     out[0] = comp[0] + comp[1] + comp[2];
     out[1] = comp[3] + comp[4] + comp[5];
   }
+}
+
+__global__ void k_energy_final(const double* partials, double* out, double h_inv2) {
+  energy_final_body(partials, out, h_inv2);
+}
+
+// Several grids: CTA b sums grid b's partials into out[2 b], out[2 b + 1].
+__global__ void k_energy_final_pack(const EnergyArgs* args, double* out, double h_inv2) {
+  energy_final_body(args[blockIdx.x].partials, out + 2 * blockIdx.x, h_inv2);
 }
 
 // ---------------------------------------------------------------------------
@@ -2879,9 +2911,34 @@ static void upml_kappa(int comp, int dir, const long long pos[3], bool is_min, l
   *ki = smax * std::pow(ni, m);
 }
 
+// Conductivity of the corrected UPML along axis `dir` at index i, at the node
+// (half = false) or half a cell above it, over both faces of that axis (a
+// position lies in at most one slab): sigma_max (depth / width)^m with the
+// depth from the region's inner node, L at a min face and n - L - 1 at a max
+// face (the nodes the reference grades from, pml.rs:370-420), taken at the
+// Yee position of the component.
+static double upml_sigma_axis(const long long L[6], int dir, long long i, bool half, double m, double R0,
+                              const long long n[3], const double delta[3]) {
+  const double z0 = 376.730313668;
+  double sg = 0.0;
+  for (int side = 0; side < 2; ++side) {
+    const long long l = L[2 * dir + side];
+    if (l <= 0 || l >= n[dir]) continue;
+    const double smax = -(m + 1.0) * std::log(R0) / (2.0 * z0 * (double)l * delta[dir]);
+    const double x = (double)i + (half ? 0.5 : 0.0);
+    double depth = side == 0 ? (double)l - x : x - (double)(n[dir] - l - 1);
+    depth = std::min(std::max(depth, 0.0), (double)l);
+    sg = std::max(sg, smax * std::pow(depth / (double)l, m));
+  }
+  return sg;
+}
+
 oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc) {
   if (!engine || !desc) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
   if (engine->storage) return fail(OEMS_ERR_CONFIG, "UPML needs float field storage");
+  if (desc->kind != 0 && desc->kind != 1) return fail(OEMS_ERR_CONFIG, "UPML kind must be 0 or 1");
+  if (desc->kind == 1 && engine->id_bytes != 0)
+    return fail(OEMS_ERR_CONFIG, "the corrected UPML rewrites coefficients: needs full coefficient arrays");
   if (engine->upml.on) return fail(OEMS_ERR_CONFIG, "UPML already attached");
   if (!(desc->reflection_coeff > 0.0 && desc->reflection_coeff < 1.0))
     return fail(OEMS_ERR_CONFIG, "UPML reflection coefficient must be in (0, 1)");
@@ -2916,6 +2973,17 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
   // Upml::init_region_coefficients (pml.rs:299-367)
   std::vector<float> ce(9 * (size_t)total), ch(9 * (size_t)total);
   const double dt = engine->dt, m = desc->grading_order, eps0 = 8.854187817e-12, z0 = 376.730313668;
+  // kind 1 rewrites the region cells' main coefficients: work on a host copy
+  // of the 12 arrays (padded layout), uploaded again below
+  const size_t ncoef = (size_t)engine->ncells_padded;
+  std::vector<float> coef;
+  if (desc->kind == 1) {
+    coef.resize(12 * ncoef);
+    for (int a = 0; a < 12; ++a)
+      OEMS_CUDA(cudaMemcpyAsync(coef.data() + a * ncoef, engine->C(a), ncoef * sizeof(float),
+                                cudaMemcpyDeviceToHost, engine->stream));
+    OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  }
   long long base = 0;
   for (const Reg& r : regs) {
     const long long layers = L[2 * r.dir + (r.is_min ? 0 : 1)];
@@ -2926,6 +2994,41 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
       for (long long lj = 0; lj < r.size[1]; ++lj)
         for (long long lk = 0; lk < r.size[2]; ++lk, ++t) {
           const long long pos[3] = {r.start[0] + li, r.start[1] + lj, r.start[2] + lk};
+          if (desc->kind == 1) {
+            // Taflove & Hagness 7.8 for component c (cp, cpp the next axes):
+            // D_c advances with sigma_cp in the main update, E_c follows
+            // from D_c through the hooks with sigma_cpp and sigma_c; H likewise
+            const size_t qc = (size_t)((pos[0] * engine->ny + pos[1]) * engine->g.nzp + pos[2]);
+            const size_t q = (size_t)(base + t);
+            for (int c = 0; c < 3; ++c) {
+              double sv[3], si[3];
+              for (int dd = 0; dd < 3; ++dd) {
+                sv[dd] = upml_sigma_axis(L, dd, pos[dd], c == dd, m, desc->reflection_coeff, n, engine->delta);
+                si[dd] = upml_sigma_axis(L, dd, pos[dd], c != dd, m, desc->reflection_coeff, n, engine->delta);
+              }
+              const int np = (c + 1) % 3, npp = (c + 2) % 3;
+              const double dv = 2.0 * eps0 + sv[npp] * dt, di = 2.0 * eps0 + si[npp] * dt;
+              ce[(0 * 3 + c) * total + q] = (float)((2.0 * eps0 - sv[npp] * dt) / dv);
+              ce[(1 * 3 + c) * total + q] = (float)((2.0 * eps0 - sv[c] * dt) / dv);
+              ce[(2 * 3 + c) * total + q] = (float)((2.0 * eps0 + sv[c] * dt) / dv);
+              ch[(0 * 3 + c) * total + q] = (float)((2.0 * eps0 - si[npp] * dt) / di);
+              ch[(1 * 3 + c) * total + q] = (float)((2.0 * eps0 - si[c] * dt) / di);
+              ch[(2 * 3 + c) * total + q] = (float)((2.0 * eps0 + si[c] * dt) / di);
+              float* ca = coef.data() + (size_t)c * ncoef;
+              float* cb = coef.data() + (size_t)(3 + c) * ncoef;
+              float* da = coef.data() + (size_t)(6 + c) * ncoef;
+              float* db = coef.data() + (size_t)(9 + c) * ncoef;
+              if (ca[qc] != 0.0f || cb[qc] != 0.0f) {
+                ca[qc] = (float)((2.0 * eps0 - sv[np] * dt) / (2.0 * eps0 + sv[np] * dt));
+                cb[qc] = (float)((double)cb[qc] * (2.0 * eps0 / (2.0 * eps0 + sv[np] * dt)));
+              }
+              if (da[qc] != 0.0f || db[qc] != 0.0f) {
+                da[qc] = (float)((2.0 * eps0 - si[np] * dt) / (2.0 * eps0 + si[np] * dt));
+                db[qc] = (float)((double)db[qc] * (2.0 * eps0 / (2.0 * eps0 + si[np] * dt)));
+              }
+            }
+            continue;
+          }
           double kv[3], ki[3];
           for (int c = 0; c < 3; ++c)
             upml_kappa(c, r.dir, pos, r.is_min, layers, width, smax, m, n, engine->delta, &kv[c], &ki[c]);
@@ -2958,6 +3061,10 @@ oems_status oems_engine_add_upml(oems_engine* engine, const oems_upml_desc* desc
         }
     base += t;
   }
+  if (desc->kind == 1)
+    for (int a = 0; a < 12; ++a)
+      OEMS_CUDA(cudaMemcpyAsync(engine->C(a), coef.data() + a * ncoef, ncoef * sizeof(float),
+                                cudaMemcpyHostToDevice, engine->stream));
   UpmlHost& U = engine->upml;
   OEMS_CUDA(U.coef.ensure(18 * (size_t)total));
   OEMS_CUDA(U.flux.ensure(6 * (size_t)total));
@@ -3249,6 +3356,473 @@ oems_status oems_release_cached_memory(int32_t device) {
   }
   for (auto& kv : bufs) OEMS_CUDA(cudaFreeHost(kv.second));
   return OEMS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// packs: several engines stepped by shared launches
+// ---------------------------------------------------------------------------
+// A sweep's instances are small independent grids.  Run one by one, each
+// half-step of each grid is a launch too small to fill the GPU, and every
+// grid keeps its own graphs and host round trips.  A pack steps a set of
+// engines together: per half-step one launch of the plain update kernels over
+// the CPML-free boxes of every grid and one of the CPML kernels over all
+// their slab cells (work items of all grids in one list, each grid's
+// arguments in a device table), then one post-step launch with a CTA per
+// grid; energies of all grids in two launches; CUDA graphs per span length.
+// Every grid's cells, sources, probes, energies, DFTs and termination are
+// computed by the same code in the same order as oems_engine_run_batch, so
+// each engine ends with the bits it would have on its own.
+struct oems_pack {
+  int device = 0;
+  int storage = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<oems_engine*> en;
+  // layout of the active engines: plain parts first, then CPML parts
+  std::vector<int> active;
+  int n_plain = 0, n_cpml = 0;
+  int grid_hp = 1, grid_hc = 1, grid_ep = 1, grid_ec = 1;
+  oems::DevBuf<oems::HArgs> h_args;
+  oems::DevBuf<oems::EArgs> e_args;
+  oems::DevBuf<int> off;  // [n_plain + 1] then [n_cpml + 1]
+  oems::DevBuf<oems::PostArgs> post;
+  oems::DevBuf<oems::EnergyArgs> energy;
+  oems::DevBuf<long long> d_base;
+  oems::DevBuf<double> d_energy;  // [active][2]
+  double* h_energy = nullptr;     // pinned mirror
+  size_t h_energy_cap = 0;
+  std::map<int, cudaGraphExec_t> graphs;
+};
+
+namespace oems {
+
+static void pack_drop_graphs(oems_pack* p) {
+  for (auto& kv : p->graphs) cudaGraphExecDestroy(kv.second);
+  p->graphs.clear();
+}
+
+constexpr int kPackThreads = 256;
+constexpr int kPackIchunk = 8;
+
+template <typename T>
+static oems_status pack_grids(oems_pack* p) {
+  int sms = 0, o = 0;
+  OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<false, T>, kPackThreads, 0));
+  p->grid_hp = std::max(1, o) * sms;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<true, T>, kPackThreads, 0));
+  p->grid_hc = std::max(1, o) * sms;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<false, T>, kPackThreads, 0));
+  p->grid_ep = std::max(1, o) * sms;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<true, T>, kPackThreads, 0));
+  p->grid_ec = std::max(1, o) * sms;
+  return OEMS_OK;
+}
+
+// Device tables of the active engines (uploaded on the pack's stream); the
+// graphs bake the part counts and the post / energy grid sizes, so they are
+// dropped whenever the active set changes.
+static oems_status pack_layout(oems_pack* p, const std::vector<int>& active) {
+  std::vector<HArgs> hp, hc;
+  std::vector<EArgs> ep, ec;
+  std::vector<int> op{0}, oc{0};
+  std::vector<PostArgs> post;
+  std::vector<EnergyArgs> energy;
+  for (int i : active) {
+    oems_engine* en = p->en[i];
+    HArgs a = h_args(en);
+    EArgs b = e_args(en);
+    auto add = [&](const Geom& g, bool cpml) {
+      if (g.work <= 0) return;
+      a.g = g;
+      b.g = g;
+      a.g.pf = b.g.pf = 0;
+      if (cpml) {
+        hc.push_back(a);
+        ec.push_back(b);
+        oc.push_back(oc.back() + g.work);
+      } else {
+        hp.push_back(a);
+        ep.push_back(b);
+        op.push_back(op.back() + g.work);
+      }
+    };
+    if (en->cpml.on && can_zsplit(en)) {
+      add(make_interior_geom(en, kPackThreads, kPackIchunk), false);
+      add(make_shell_geom(en, kPackThreads, kPackIchunk, true), true);
+    } else {
+      add(make_geom(en, kPackThreads, kPackIchunk), en->cpml.on);
+    }
+    PostArgs q{};
+    for (int c = 0; c < 3; ++c) {
+      q.e[c] = en->E(c);
+      q.h[c] = en->H(c);
+    }
+    q.nexc = en->nexc;
+    q.exc_idx = en->d_exc_idx.p;
+    q.exc_meta = en->d_exc_meta.p;
+    q.exc_off = en->d_exc_off.p;
+    q.exc_count = en->d_exc_count.p;
+    q.exc_samples = en->d_exc_samples.p;
+    q.nprobe = en->nprobe();
+    q.probe_off = en->d_probe_off.p;
+    q.probe_mode = en->d_probe_mode.p;
+    q.term_idx = en->d_term_idx.p;
+    q.term_comp = en->d_term_comp.p;
+    q.term_w = en->d_term_w.p;
+    q.traces = en->d_traces.p;
+    q.d_base = p->d_base.p;
+    q.h_inv = 1.0f / en->h_scale;
+    post.push_back(q);
+    EnergyArgs ea{};
+    for (int c = 0; c < 6; ++c) ea.arr[c] = en->at((size_t)c);
+    ea.n4 = en->ncells_padded / 4;
+    ea.partials = en->d_partials.p;
+    energy.push_back(ea);
+  }
+  const size_t na = std::max<size_t>(active.size(), 1);
+  OEMS_CUDA(p->h_args.ensure(std::max<size_t>(hp.size() + hc.size(), 1)));
+  OEMS_CUDA(p->e_args.ensure(std::max<size_t>(ep.size() + ec.size(), 1)));
+  OEMS_CUDA(p->off.ensure(op.size() + oc.size()));
+  OEMS_CUDA(p->post.ensure(na));
+  OEMS_CUDA(p->energy.ensure(na));
+  OEMS_CUDA(p->d_energy.ensure(2 * na));
+  std::vector<HArgs> hall(hp);
+  hall.insert(hall.end(), hc.begin(), hc.end());
+  std::vector<EArgs> eall(ep);
+  eall.insert(eall.end(), ec.begin(), ec.end());
+  std::vector<int> oall(op);
+  oall.insert(oall.end(), oc.begin(), oc.end());
+  if (!hall.empty()) {
+    OEMS_CUDA(cudaMemcpyAsync(p->h_args.p, hall.data(), hall.size() * sizeof(HArgs), cudaMemcpyHostToDevice, p->stream));
+    OEMS_CUDA(cudaMemcpyAsync(p->e_args.p, eall.data(), eall.size() * sizeof(EArgs), cudaMemcpyHostToDevice, p->stream));
+  }
+  OEMS_CUDA(cudaMemcpyAsync(p->off.p, oall.data(), oall.size() * sizeof(int), cudaMemcpyHostToDevice, p->stream));
+  if (!post.empty()) {
+    OEMS_CUDA(cudaMemcpyAsync(p->post.p, post.data(), post.size() * sizeof(PostArgs), cudaMemcpyHostToDevice, p->stream));
+    OEMS_CUDA(cudaMemcpyAsync(p->energy.p, energy.data(), energy.size() * sizeof(EnergyArgs), cudaMemcpyHostToDevice,
+                              p->stream));
+  }
+  // the host vectors are released on return
+  OEMS_CUDA(cudaStreamSynchronize(p->stream));
+  p->n_plain = (int)hp.size();
+  p->n_cpml = (int)hc.size();
+  p->active = active;
+  pack_drop_graphs(p);
+  return OEMS_OK;
+}
+
+template <typename T>
+static cudaError_t pack_launch_steps(oems_pack* p, int steps) {
+  const int na = (int)p->active.size();
+  const PackH hp{p->n_plain, p->off.p, p->h_args.p};
+  const PackH hc{p->n_cpml, p->off.p + p->n_plain + 1, p->h_args.p + p->n_plain};
+  const PackE ep{p->n_plain, p->off.p, p->e_args.p};
+  const PackE ec{p->n_cpml, p->off.p + p->n_plain + 1, p->e_args.p + p->n_plain};
+  for (int s = 0; s < steps; ++s) {
+    if (p->n_plain) k_update_h_pack<false, T><<<p->grid_hp, kPackThreads, 0, p->stream>>>(hp);
+    if (p->n_cpml) k_update_h_pack<true, T><<<p->grid_hc, kPackThreads, 0, p->stream>>>(hc);
+    if (p->n_plain) k_update_e_pack<false, T><<<p->grid_ep, kPackThreads, 0, p->stream>>>(ep);
+    if (p->n_cpml) k_update_e_pack<true, T><<<p->grid_ec, kPackThreads, 0, p->stream>>>(ec);
+    k_post_step_pack<T><<<na, 128, 0, p->stream>>>(p->post.p, p->d_base.p, s);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t pack_launch_steps_any(oems_pack* p, int steps) {
+  if (p->storage == 1) return pack_launch_steps<__half>(p, steps);
+  if (p->storage == 2) return pack_launch_steps<__nv_bfloat16>(p, steps);
+  return pack_launch_steps<float>(p, steps);
+}
+
+static oems_status pack_run_span(oems_pack* p, long long base, int steps) {
+  k_set_i64<<<1, 1, 0, p->stream>>>(p->d_base.p, base);
+  OEMS_CUDA(cudaGetLastError());
+  auto it = p->graphs.find(steps);
+  if (it == p->graphs.end()) {
+    if (p->graphs.size() >= 8) pack_drop_graphs(p);
+    cudaGraph_t graph = nullptr;
+    OEMS_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t le = pack_launch_steps_any(p, steps);
+    const cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return fail(OEMS_ERR_CUDA, std::string("pack graph capture: ") +
+                                     cudaGetErrorString(le != cudaSuccess ? le : ce));
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(OEMS_ERR_CUDA, std::string("pack graph instantiate: ") + cudaGetErrorString(ie));
+    it = p->graphs.emplace(steps, exec).first;
+  }
+  OEMS_CUDA(cudaGraphLaunch(it->second, p->stream));
+  return OEMS_OK;
+}
+
+// Energies of the active engines into p->h_energy[2 k], [2 k + 1].
+static oems_status pack_energy(oems_pack* p) {
+  const int na = (int)p->active.size();
+  const dim3 grid(kEnergyBlocks, 6, na);
+  if (p->storage == 1)
+    k_energy_partial_pack<__half><<<grid, kEnergyThreads, 0, p->stream>>>(p->energy.p);
+  else if (p->storage == 2)
+    k_energy_partial_pack<__nv_bfloat16><<<grid, kEnergyThreads, 0, p->stream>>>(p->energy.p);
+  else
+    k_energy_partial_pack<float><<<grid, kEnergyThreads, 0, p->stream>>>(p->energy.p);
+  OEMS_CUDA(cudaGetLastError());
+  const float hs = p->en[p->active[0]]->h_scale;
+  k_energy_final_pack<<<na, 32, 0, p->stream>>>(p->energy.p, p->d_energy.p, 1.0 / ((double)hs * hs));
+  OEMS_CUDA(cudaGetLastError());
+  if (p->h_energy_cap < (size_t)na) {
+    pinned_put(p->h_energy, p->h_energy_cap * 2 * sizeof(double));
+    p->h_energy = nullptr;
+    p->h_energy_cap = 0;
+    void* q = nullptr;
+    OEMS_CUDA(pinned_get(&q, (size_t)na * 2 * sizeof(double)));
+    p->h_energy = static_cast<double*>(q);
+    p->h_energy_cap = na;
+  }
+  OEMS_CUDA(cudaMemcpyAsync(p->h_energy, p->d_energy.p, (size_t)na * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                            p->stream));
+  OEMS_CUDA(cudaStreamSynchronize(p->stream));
+  return OEMS_OK;
+}
+
+// Per-engine state of one pack batch (the locals of run_batch).
+struct PackRun {
+  const oems_batch* b = nullptr;
+  uint64_t t0 = 0, executed = 0;
+  int reason = OEMS_TERMINATION_STEPS_COMPLETED;
+  double final_db = 0.0, peak = 0.0;
+  bool numerical = false, running = false;
+  std::vector<oems_energy_sample> samples;
+  size_t peaked = 0;
+};
+
+static oems_status pack_run_batch(oems_pack* p, const oems_batch* const* batches, oems_batch_result* results,
+                                  oems_status* statuses) {
+  const auto t_start = std::chrono::steady_clock::now();
+  const size_t n = p->en.size();
+  std::vector<PackRun> R(n);
+  std::vector<int> part;
+  const oems_batch* b0 = nullptr;
+  for (size_t i = 0; i < n; ++i) {
+    statuses[i] = OEMS_OK;
+    if (!batches[i]) continue;
+    const oems_batch* b = batches[i];
+    if (!b0) b0 = b;
+    if (b->num_steps != b0->num_steps || b->sample_interval != b0->sample_interval ||
+        b->check_interval != b0->check_interval || b->has_energy_decay_db != b0->has_energy_decay_db ||
+        p->en[i]->timestep != p->en[part.empty() ? i : part[0]]->timestep)
+      return fail(OEMS_ERR_CONFIG, "the batches of a pack must share step count, intervals and start step");
+    part.push_back((int)i);
+  }
+  if (part.empty()) return OEMS_OK;
+  const uint64_t steps = b0->num_steps;
+  for (int i : part) {
+    oems_engine* en = p->en[i];
+    EngineScope guard(en);
+    PackRun& r = R[i];
+    r.b = batches[i];
+    r.t0 = en->timestep;
+    r.peak = r.b->initial_peak_energy;
+    r.running = true;
+    OEMS_TRY(upload_excitations(en, r.b));
+    const int np = en->nprobe();
+    if (np > 0) OEMS_CUDA(en->d_traces.ensure((size_t)std::max<uint64_t>(steps, 1) * np));
+    OEMS_CUDA(cudaStreamSynchronize(en->stream));
+  }
+  DeviceGuard dg(p->device);
+  OEMS_TRY(pack_layout(p, part));
+  const uint64_t si = b0->sample_interval, ci = b0->check_interval;
+  const bool has_decay = b0->has_energy_decay_db != 0;
+  const uint64_t t0 = R[part[0]].t0;
+  OEMS_CUDA(cudaEventRecord(p->ev0, p->stream));
+  uint64_t s = 0;
+  while (s < steps && !p->active.empty()) {
+    const uint64_t cur = t0 + s;
+    uint64_t ev = UINT64_MAX;
+    if (si > 0) ev = std::min(ev, (cur + si - 1) / si * si);
+    if (has_decay && ci > 0) {
+      uint64_t c = (cur + ci - 1) / ci * ci;
+      if (c == 0) c = ci;
+      ev = std::min(ev, c);
+    }
+    uint64_t span = steps - s;
+    if (ev != UINT64_MAX && ev - cur + 1 < span) span = ev - cur + 1;
+    span = std::min<uint64_t>(span, 1u << 20);
+    OEMS_TRY(pack_run_span(p, (long long)s, (int)span));
+    s += span;
+    const uint64_t last = t0 + s - 1;
+    const bool do_sample = si > 0 && last % si == 0;
+    const bool do_check = has_decay && ci > 0 && last > 0 && last % ci == 0;
+    if (!do_sample && !do_check) continue;
+    OEMS_TRY(pack_energy(p));
+    std::vector<int> still;
+    for (size_t k = 0; k < p->active.size(); ++k) {
+      const int i = p->active[k];
+      PackRun& r = R[i];
+      const double e = p->h_energy[2 * k], h = p->h_energy[2 * k + 1];
+      if (do_sample) r.samples.push_back({last, e, h, e + h});
+      bool stop = false;
+      if (do_check) {
+        // run_batch's check: fold the samples since the last check into
+        // the peak, then compare this energy with it
+        for (; r.peaked < r.samples.size(); ++r.peaked) {
+          const double tot = r.samples[r.peaked].total_energy;
+          if (!std::isfinite(tot)) r.numerical = true;
+          if (r.b->track_peak) r.peak = std::max(r.peak, tot);
+        }
+        const double tot = e + h;
+        if (!std::isfinite(tot)) r.numerical = true;
+        if (r.numerical) {
+          stop = true;
+        } else if (r.peak > 0.0 && tot > 0.0) {
+          const double d = 10.0 * std::log10(tot / r.peak);
+          if (d < -std::fabs(r.b->energy_decay_db)) {
+            r.reason = OEMS_TERMINATION_ENERGY_DECAY;
+            r.final_db = d;
+            stop = true;
+          }
+        }
+      }
+      if (stop) {
+        r.executed = s;
+        r.running = false;
+      } else {
+        still.push_back(i);
+      }
+    }
+    if (still.size() != p->active.size()) {
+      if (still.empty())
+        p->active.clear();
+      else
+        OEMS_TRY(pack_layout(p, still));
+    }
+  }
+  for (int i : p->active) R[i].executed = s;
+  // probe DFTs of each engine's executed steps
+  for (int i : part) {
+    oems_engine* en = p->en[i];
+    if (en->entry_probe.empty() || R[i].executed == 0) continue;
+    DftArgs da{};
+    da.nentries = (int)en->entry_probe.size();
+    da.entry_probe = en->d_entry_probe.p;
+    da.entry_freq = en->d_entry_freq.p;
+    da.entry_half = en->d_entry_half.p;
+    da.acc = en->d_dft_acc.p;
+    da.traces = en->d_traces.p;
+    da.nprobe = en->nprobe();
+    da.steps = (long long)R[i].executed;
+    da.t0 = (long long)R[i].t0;
+    da.dt = en->dt;
+    k_probe_dft<<<(da.nentries + 127) / 128, 128, 0, p->stream>>>(da);
+    OEMS_CUDA(cudaGetLastError());
+  }
+  OEMS_CUDA(cudaEventRecord(p->ev1, p->stream));
+  OEMS_CUDA(cudaStreamSynchronize(p->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+  double cell_steps = 0.0;
+  for (int i : part) cell_steps += (double)p->en[i]->nx * p->en[i]->ny * p->en[i]->nz * (double)R[i].executed;
+  const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  for (int i : part) {
+    oems_engine* en = p->en[i];
+    PackRun& r = R[i];
+    for (; r.peaked < r.samples.size(); ++r.peaked) {
+      const double tot = r.samples[r.peaked].total_energy;
+      if (!std::isfinite(tot)) r.numerical = true;
+      if (r.b->track_peak) r.peak = std::max(r.peak, tot);
+    }
+    en->timestep = r.t0 + r.executed;
+    en->traces_steps = r.executed;
+    const double share = cell_steps > 0.0 ? (double)en->nx * en->ny * en->nz * (double)r.executed / cell_steps : 0.0;
+    en->last_device_seconds = ms * 1e-3 * share;
+    en->last_launches = 0;
+    oems_batch_result& out = results[i];
+    out.timesteps_executed = r.executed;
+    out.termination_reason = r.reason;
+    out.reserved0 = 0;
+    out.final_decay_db = r.final_db;
+    out.num_energy_samples = r.samples.size();
+    out.peak_energy = r.peak;
+    for (size_t q = 0; q < r.samples.size() && out.energy_samples && q < out.energy_capacity; ++q)
+      out.energy_samples[q] = r.samples[q];
+    out.elapsed_seconds = elapsed;
+    if (r.numerical) statuses[i] = OEMS_ERR_NUMERICAL;
+  }
+  return OEMS_OK;
+}
+
+}  // namespace oems
+
+extern "C" {
+
+oems_status oems_pack_create(oems_engine* const* engines, uint64_t count, oems_pack** out) {
+  if (!out || (!engines && count)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (count == 0) return fail(OEMS_ERR_CONFIG, "a pack needs at least one engine");
+  for (uint64_t i = 0; i < count; ++i) {
+    const oems_engine* en = engines[i];
+    if (!en) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine in the pack");
+    if (en->device != engines[0]->device) return fail(OEMS_ERR_CONFIG, "the engines of a pack share one device");
+    if (en->storage != engines[0]->storage) return fail(OEMS_ERR_CONFIG, "the engines of a pack share one field storage");
+    if (en->id_bytes != 0) return fail(OEMS_ERR_CONFIG, "a pack needs full coefficient arrays");
+    if (en->mur.on || en->upml.on || en->tfsf.on || !en->disp.empty() || !en->rlc.q.empty() || !en->fdumps.empty() ||
+        !en->boxes.empty())
+      return fail(OEMS_ERR_CONFIG, "a pack runs CPML, sources, probes and probe DFTs only");
+    for (uint64_t j = 0; j < i; ++j)
+      if (engines[j] == en) return fail(OEMS_ERR_CONFIG, "an engine appears twice in the pack");
+  }
+  auto p = std::make_unique<oems_pack>();
+  p->device = engines[0]->device;
+  p->storage = engines[0]->storage;
+  p->en.assign(engines, engines + count);
+  DeviceGuard dg(p->device);
+  OEMS_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  OEMS_CUDA(cudaEventCreate(&p->ev0));
+  OEMS_CUDA(cudaEventCreate(&p->ev1));
+  OEMS_CUDA(p->d_base.ensure(1));
+  oems_status st = OEMS_OK;
+  if (p->storage == 1)
+    st = pack_grids<__half>(p.get());
+  else if (p->storage == 2)
+    st = pack_grids<__nv_bfloat16>(p.get());
+  else
+    st = pack_grids<float>(p.get());
+  if (st != OEMS_OK) {
+    oems_pack_destroy(p.release());
+    return st;
+  }
+  *out = p.release();
+  return OEMS_OK;
+}
+
+void oems_pack_destroy(oems_pack* pack) {
+  if (!pack) return;
+  DeviceGuard dg(pack->device);
+  if (pack->stream) cudaStreamSynchronize(pack->stream);
+  oems::pack_drop_graphs(pack);
+  pack->h_args.release();
+  pack->e_args.release();
+  pack->off.release();
+  pack->post.release();
+  pack->energy.release();
+  pack->d_base.release();
+  pack->d_energy.release();
+  oems::pinned_put(pack->h_energy, pack->h_energy_cap * 2 * sizeof(double));
+  if (pack->ev0) cudaEventDestroy(pack->ev0);
+  if (pack->ev1) cudaEventDestroy(pack->ev1);
+  if (pack->stream) cudaStreamDestroy(pack->stream);
+  delete pack;
+}
+
+oems_status oems_pack_run_batch(oems_pack* pack, const oems_batch* const* batches, oems_batch_result* results,
+                                oems_status* statuses) {
+  if (!pack || !batches || !results || !statuses) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  return oems::pack_run_batch(pack, batches, results, statuses);
 }
 
 }  // extern "C"

@@ -12,6 +12,10 @@
 // oems_sweep_run_until stops every instance at a step count and keeps its
 // engine: a later call continues it where it stopped (the same bits as an
 // uninterrupted run), oems_sweep_finish ends it with its partial DFTs.
+// With packing on (oems_sweep_set_packed), run / run_until step the
+// instances that are at the same step count together through one pack
+// (oems_pack_run_batch): shared launches over all their grids instead of one
+// stream per instance, with the same bits per instance.
 // Only the public C ABI of the engine and the host operator is used.
 
 #include <algorithm>
@@ -63,6 +67,7 @@ struct oems_sweep {
   std::vector<std::unique_ptr<Instance>> inst;
   double wall = 0.0, cell_steps = 0.0;
   uint64_t trace_steps = 0;
+  bool packed = false;
 };
 
 namespace {
@@ -126,40 +131,52 @@ void end_instance(Instance& I) {
   I.res.paused = 0;
 }
 
-// Runs batches until the instance ends or has run `cap` steps in total; the
-// port DFTs so far are read back either way.
-oems_status advance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t cap) {
+// One batch of an instance: n steps from its current step, with the port
+// source's samples, energy samples and decay checks every 100 steps and the
+// peak carried in.
+struct BatchBuf {
+  std::vector<float> samples;
+  std::vector<oems_energy_sample> es;
+  oems_scheduled_excitation x{};
+  oems_batch b{};
+  oems_batch_result r{};
+};
+
+oems_status prepare_batch(const Instance& I, uint64_t n, BatchBuf& B) {
   const oems_sweep_instance& d = I.desc;
-  const uint64_t nf = sw->freqs.size();
-  const uint64_t limit = std::min<uint64_t>(cap, d.max_timesteps);
-  std::vector<float> samples(batch);
-  std::vector<oems_energy_sample> es(batch / 100 + 2);
-  const bool has_decay = d.energy_decay_db != 0.0;
+  B.samples.resize(std::max<uint64_t>(n, 1));
+  B.es.resize(n / 100 + 2);
+  const oems_status st = oems_excitation_sample(&I.wave, I.run, n, I.dt, B.samples.data());
+  if (st != OEMS_OK) return st;
+  B.x = oems_scheduled_excitation{};
+  for (int a = 0; a < 3; ++a) B.x.position[a] = d.port_position[a];
+  B.x.direction = (uint32_t)d.port_direction;
+  B.x.soft_source = 1;
+  B.x.samples = B.samples.data();
+  B.x.num_samples = n;
+  B.b = oems_batch{};
+  B.b.num_steps = n;
+  B.b.excitations = &B.x;
+  B.b.num_excitations = 1;
+  B.b.has_energy_decay_db = d.energy_decay_db != 0.0 ? 1 : 0;
+  B.b.energy_decay_db = std::fabs(d.energy_decay_db);
+  B.b.check_interval = 100;
+  B.b.sample_interval = 100;
+  B.b.track_peak = 1;
+  B.b.initial_peak_energy = I.peak;
+  B.r = oems_batch_result{};
+  B.r.energy_samples = B.es.data();
+  B.r.energy_capacity = B.es.size();
+  return OEMS_OK;
+}
+
+// Folds a finished batch into the instance: traces, counters, peak and
+// termination; `ended` is set when the batch ended the instance.
+oems_status apply_batch(const oems_sweep* sw, Instance& I, BatchBuf& B, bool& ended) {
+  const oems_batch_result& r = B.r;
+  const std::vector<oems_energy_sample>& es = B.es;
   oems_status st = OEMS_OK;
-  bool ended = I.run >= d.max_timesteps;
-  while (!ended && I.run < limit) {
-    const uint64_t n = std::min(limit - I.run, batch);
-    if ((st = oems_excitation_sample(&I.wave, I.run, n, I.dt, samples.data())) != OEMS_OK) return st;
-    oems_scheduled_excitation x{};
-    for (int a = 0; a < 3; ++a) x.position[a] = d.port_position[a];
-    x.direction = (uint32_t)d.port_direction;
-    x.soft_source = 1;
-    x.samples = samples.data();
-    x.num_samples = n;
-    oems_batch b{};
-    b.num_steps = n;
-    b.excitations = &x;
-    b.num_excitations = 1;
-    b.has_energy_decay_db = has_decay ? 1 : 0;
-    b.energy_decay_db = std::fabs(d.energy_decay_db);
-    b.check_interval = 100;
-    b.sample_interval = 100;
-    b.track_peak = 1;
-    b.initial_peak_energy = I.peak;
-    oems_batch_result r{};
-    r.energy_samples = es.data();
-    r.energy_capacity = es.size();
-    if ((st = oems_engine_run_batch(I.en, &b, &r)) != OEMS_OK) return st;
+  {
     if (sw->trace_steps > I.run) {
       // port u / i of this batch, kept up to trace_steps
       const uint64_t keep = std::min<uint64_t>(r.timesteps_executed, sw->trace_steps - I.run);
@@ -182,7 +199,15 @@ oems_status advance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t 
       I.res.final_decay_db = 10.0 * std::log10(es[ns - 1].total_energy / I.peak);
     if (r.termination_reason != OEMS_TERMINATION_STEPS_COMPLETED || r.timesteps_executed == 0) ended = true;
   }
-  ended = ended || I.run >= d.max_timesteps;
+  return OEMS_OK;
+}
+
+// After the last batch of a call: reads the port DFTs back, then ends the
+// instance or leaves it paused.
+oems_status close_advance(const oems_sweep* sw, Instance& I, bool ended) {
+  const uint64_t nf = sw->freqs.size();
+  oems_status st = OEMS_OK;
+  ended = ended || I.run >= I.desc.max_timesteps;
   I.res.timesteps = I.run;
   I.uf.assign(2 * nf, 0.0);
   I.if_.assign(2 * nf, 0.0);
@@ -195,6 +220,21 @@ oems_status advance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t 
   return OEMS_OK;
 }
 
+// Runs batches until the instance ends or has run `cap` steps in total; the
+// port DFTs so far are read back either way.
+oems_status advance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t cap) {
+  const uint64_t limit = std::min<uint64_t>(cap, I.desc.max_timesteps);
+  BatchBuf B;
+  oems_status st = OEMS_OK;
+  bool ended = I.run >= I.desc.max_timesteps;
+  while (!ended && I.run < limit) {
+    if ((st = prepare_batch(I, std::min(limit - I.run, batch), B)) != OEMS_OK) return st;
+    if ((st = oems_engine_run_batch(I.en, &B.b, &B.r)) != OEMS_OK) return st;
+    if ((st = apply_batch(sw, I, B, ended)) != OEMS_OK) return st;
+  }
+  return close_advance(sw, I, ended);
+}
+
 oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch, uint64_t cap) {
   if (!I.en) {
     const auto t_start = std::chrono::steady_clock::now();
@@ -205,9 +245,129 @@ oems_status run_instance(const oems_sweep* sw, Instance& I, uint64_t batch, uint
   return advance(sw, I, batch, cap);
 }
 
+// Packed run: starts every instance (set-up on `concurrency` threads), then
+// steps the instances that are at the same step count together through one
+// pack, batch by batch, each batch as long as the shortest remaining run of
+// the group allows (the results do not depend on batch boundaries).  An
+// instance leaves the group when it ends or reaches its cap; groups are
+// formed until every instance has ended or stopped at its cap.
+oems_status run_packed(oems_sweep* s, std::vector<Instance*>& todo, uint64_t batch, uint64_t cap) {
+  std::atomic<size_t> next{0};
+  auto starter = [&]() {
+    for (size_t k = next++; k < todo.size(); k = next++) {
+      Instance& I = *todo[k];
+      if (I.en) continue;
+      const auto t_start = std::chrono::steady_clock::now();
+      const oems_status st = start_instance(s, I);
+      I.res.setup_seconds = seconds_since(t_start);
+      I.res.status = st;
+      if (st != OEMS_OK) {
+        I.error = oems_last_error_message();
+        end_instance(I);
+      }
+    }
+  };
+  {
+    const size_t nthreads = std::min<size_t>(s->concurrency, todo.size());
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(starter);
+    if (nthreads > 0) starter();
+    for (auto& t : pool) t.join();
+  }
+  auto limit_of = [&](const Instance& I) { return std::min<uint64_t>(cap, I.desc.max_timesteps); };
+  auto fail_instance = [&](Instance& I, oems_status st) {
+    I.res.status = st;
+    I.error = oems_last_error_message();
+    end_instance(I);
+  };
+  while (true) {
+    // the next group: live instances below their cap at the smallest step count
+    std::vector<Instance*> live;
+    for (Instance* I : todo)
+      if (!I->done && I->en && I->res.status == OEMS_OK) live.push_back(I);
+    std::vector<Instance*> group;
+    uint64_t r0 = UINT64_MAX;
+    for (Instance* I : live)
+      if (I->run < limit_of(*I) && I->run < I->desc.max_timesteps) r0 = std::min(r0, I->run);
+    for (Instance* I : live)
+      if (I->run == r0 && I->run < limit_of(*I) && I->run < I->desc.max_timesteps) group.push_back(I);
+    if (group.empty()) break;
+    std::vector<oems_engine*> engines;
+    for (Instance* I : group) engines.push_back(I->en);
+    oems_pack* pack = nullptr;
+    oems_status st = oems_pack_create(engines.data(), engines.size(), &pack);
+    if (st != OEMS_OK) return st;
+    const auto t_group = std::chrono::steady_clock::now();
+    std::vector<BatchBuf> bufs(group.size());
+    std::vector<char> in(group.size(), 1), ended(group.size(), 0);
+    std::vector<const oems_batch*> bp(group.size(), nullptr);
+    std::vector<oems_batch_result> res(group.size());
+    std::vector<oems_status> sts(group.size(), OEMS_OK);
+    size_t left = group.size();
+    while (left > 0) {
+      uint64_t n = batch;
+      for (size_t k = 0; k < group.size(); ++k)
+        if (in[k]) n = std::min(n, limit_of(*group[k]) - group[k]->run);
+      for (size_t k = 0; k < group.size(); ++k) {
+        bp[k] = nullptr;
+        if (!in[k]) continue;
+        if ((st = prepare_batch(*group[k], n, bufs[k])) != OEMS_OK) {
+          oems_pack_destroy(pack);
+          return st;
+        }
+        bp[k] = &bufs[k].b;
+        res[k] = bufs[k].r;  // energy sample buffer and capacity
+      }
+      if ((st = oems_pack_run_batch(pack, bp.data(), res.data(), sts.data())) != OEMS_OK) {
+        oems_pack_destroy(pack);
+        return st;
+      }
+      for (size_t k = 0; k < group.size(); ++k) {
+        if (!in[k]) continue;
+        Instance& I = *group[k];
+        bufs[k].r = res[k];
+        bool e = false;
+        if (sts[k] != OEMS_OK) {
+          oems::g_last_error = "field energy became NaN or infinite";
+          fail_instance(I, sts[k]);
+          in[k] = 0;
+          --left;
+          continue;
+        }
+        if ((st = apply_batch(s, I, bufs[k], e)) != OEMS_OK) {
+          fail_instance(I, st);
+          in[k] = 0;
+          --left;
+          continue;
+        }
+        if (e || I.run >= limit_of(I) || I.run >= I.desc.max_timesteps) {
+          ended[k] = e ? 1 : 0;
+          in[k] = 0;
+          --left;
+        }
+      }
+    }
+    oems_pack_destroy(pack);
+    const double group_s = seconds_since(t_group);
+    for (size_t k = 0; k < group.size(); ++k) {
+      Instance& I = *group[k];
+      I.res.host_seconds += group_s;
+      if (I.done) continue;  // failed above
+      if ((st = close_advance(s, I, ended[k] != 0)) != OEMS_OK) fail_instance(I, st);
+    }
+  }
+  return OEMS_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+oems_status oems_sweep_set_packed(oems_sweep* s, int32_t on) {
+  if (!s) return sfail(OEMS_ERR_INVALID_ARGUMENT, "NULL sweep");
+  s->packed = on != 0;
+  return OEMS_OK;
+}
 
 oems_status oems_sweep_create(int32_t device, uint32_t concurrency, uint32_t engine_flags, const double* freqs,
                               uint64_t nfreq, oems_sweep** out) {
@@ -261,6 +421,21 @@ oems_status oems_sweep_run_until(oems_sweep* s, uint64_t batch_steps, uint64_t s
     if (!I->done) todo.push_back(I.get());
   std::vector<uint64_t> before(todo.size());
   for (size_t k = 0; k < todo.size(); ++k) before[k] = todo[k]->run;
+  if (s->packed) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const oems_status st = run_packed(s, todo, batch, step_cap);
+    s->wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    s->cell_steps = 0.0;
+    for (size_t k = 0; k < todo.size(); ++k)
+      s->cell_steps += todo[k]->res.cells * (double)(todo[k]->run - before[k]);
+    if (st != OEMS_OK) return st;
+    for (Instance* I : todo)
+      if (I->res.status != OEMS_OK) {
+        oems::g_last_error = "sweep instance failed: " + I->error;
+        return (oems_status)I->res.status;
+      }
+    return OEMS_OK;
+  }
   std::atomic<size_t> next{0};
   const auto t0 = std::chrono::steady_clock::now();
   auto worker = [&]() {

@@ -431,15 +431,14 @@ __device__ __forceinline__ void prefetch_e_plane(const EArgs& a, long long o, lo
     }
 }
 
-// H half-step: H = da*H + db*curl(E).  T: field storage type.
-template <int kIdBytes, bool kCpml, typename T = float>
-__global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
+// H half-step of one work item w of a.g: H = da*H + db*curl(E).  T: field
+// storage type.  Every thread of the CTA calls it with the same w.
+template <int kIdBytes, bool kCpml, typename T>
+__device__ __forceinline__ void h_item(const HArgs& a, const float* tab, int w) {
   using IO = FieldIO<T>;
-  extern __shared__ float s_table[];
   const Geom& g = a.g;
-  const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
   const int lane = threadIdx.x & 31;
-  for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
+  {
     const Item it = work_item(g, w);
     int c = it.c0 + (int)threadIdx.x;
     const bool valid = c < it.c1;
@@ -588,16 +587,22 @@ __global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
   }
 }
 
-// E half-step: E = ca*E + cb*curl(H), cells with i, j, k >= 1 only.  T: field
-// storage type.
+// H half-step over the grid: CTAs loop over the work items.
 template <int kIdBytes, bool kCpml, typename T = float>
-__global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
-  using IO = FieldIO<T>;
+__global__ void __launch_bounds__(512) k_update_h(const HArgs a) {
   extern __shared__ float s_table[];
-  const Geom& g = a.g;
   const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
+  for (int w = blockIdx.x; w < a.g.work; w += gridDim.x) h_item<kIdBytes, kCpml, T>(a, tab, w);
+}
+
+// E half-step of one work item w of a.g: E = ca*E + cb*curl(H), cells with
+// i, j, k >= 1 only.  T: field storage type.
+template <int kIdBytes, bool kCpml, typename T>
+__device__ __forceinline__ void e_item(const EArgs& a, const float* tab, int w) {
+  using IO = FieldIO<T>;
+  const Geom& g = a.g;
   const int lane = threadIdx.x & 31;
-  for (int w = blockIdx.x; w < g.work; w += gridDim.x) {
+  {
     const Item it = work_item(g, w);
     int c = it.c0 + (int)threadIdx.x;
     const bool valid = c < it.c1;
@@ -755,6 +760,61 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
       hym4 = hy4;
       hzm4 = hz4;
     }
+  }
+}
+
+// E half-step over the grid: CTAs loop over the work items.
+template <int kIdBytes, bool kCpml, typename T = float>
+__global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
+  extern __shared__ float s_table[];
+  const float* tab = stage_table<kIdBytes>(a.table, a.ntable, s_table);
+  for (int w = blockIdx.x; w < a.g.work; w += gridDim.x) e_item<kIdBytes, kCpml, T>(a, tab, w);
+}
+
+// Several grids in one launch (independent instances of a sweep): part p of
+// the launch is one grid's update over one geometry (its interior or its
+// CPML shell), args[p] its arguments in device memory, its work items
+// numbered from off[p]; off[nparts] is the total.  Every part uses the
+// launch's block size and full coefficient arrays.
+struct PackH {
+  int nparts;
+  const int* off;
+  const HArgs* args;
+};
+struct PackE {
+  int nparts;
+  const int* off;
+  const EArgs* args;
+};
+
+// Part holding global work item w: the last p with off[p] <= w.
+__device__ __forceinline__ int pack_part(const int* off, int nparts, int w) {
+  int lo = 0, hi = nparts - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= w)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <bool kCpml, typename T = float>
+__global__ void __launch_bounds__(512) k_update_h_pack(const PackH p) {
+  const int total = __ldg(p.off + p.nparts);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int q = pack_part(p.off, p.nparts, w);
+    h_item<0, kCpml, T>(p.args[q], nullptr, w - __ldg(p.off + q));
+  }
+}
+
+template <bool kCpml, typename T = float>
+__global__ void __launch_bounds__(512) k_update_e_pack(const PackE p) {
+  const int total = __ldg(p.off + p.nparts);
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    const int q = pack_part(p.off, p.nparts, w);
+    e_item<0, kCpml, T>(p.args[q], nullptr, w - __ldg(p.off + q));
   }
 }
 

@@ -217,17 +217,20 @@ class MurAbcConfig:
 
 @dataclass
 class PmlBoundaries:
-    """PmlBoundaries (src/extensions/pml.rs:85-135) for the reference's UPML
-    (Engine.add_upml).  Its coefficients make the scheme grow without bound,
-    as in the reference; CpmlBoundaries is the working absorber."""
+    """PmlBoundaries (src/extensions/pml.rs:85-135) for the UPML
+    (Engine.add_upml).  kind 0 is the reference's: its coefficients make the
+    scheme grow without bound.  kind 1 is the corrected uniaxial PML
+    (Taflove & Hagness 7.8 in the same flux form), which absorbs as well as
+    CpmlBoundaries."""
 
     layers: Tuple[int, ...] = (8,) * 6
     grading_order: float = 3.0
     reflection_coeff: float = 1e-6
+    kind: int = 0
 
     @classmethod
-    def uniform(cls, layers: int):
-        return cls(layers=(int(layers),) * 6)
+    def uniform(cls, layers: int, kind: int = 0):
+        return cls(layers=(int(layers),) * 6, kind=int(kind))
 
     def disable(self, face: int) -> "PmlBoundaries":
         lay = list(self.layers)
@@ -244,6 +247,7 @@ class PmlBoundaries:
             d.layers[f] = int(self.layers[f])
         d.grading_order = float(self.grading_order)
         d.reflection_coeff = float(self.reflection_coeff)
+        d.kind = int(self.kind)
         return d
 
 
@@ -1093,44 +1097,9 @@ class Engine:
         return (out[0::2] + 1j * out[1::2]).reshape(shape)
 
     def run_batch(self, batch: EngineBatch) -> BatchResult:
-        num_steps = batch.num_steps
-        if num_steps is None:
-            num_steps = batch.termination.max_timesteps
-        if num_steps is None:
-            raise N.ConfigError("EngineBatch needs num_steps or termination.max_timesteps")
-        keep = []
-        arr = (N.ScheduledExcitationC * max(1, len(batch.excitations)))()
-        for x, e in enumerate(batch.excitations):
-            s = np.ascontiguousarray(e.samples, dtype=np.float32)
-            keep.append(s)
-            for a in range(3):
-                arr[x].position[a] = int(e.position[a])
-            arr[x].direction = int(e.direction)
-            arr[x].soft_source = int(bool(e.soft_source))
-            arr[x].samples = N.fptr(s)
-            arr[x].num_samples = len(s)
-        b = N.BatchC()
-        b.num_steps = int(num_steps)
-        b.excitations = arr
-        b.num_excitations = len(batch.excitations)
-        b.has_energy_decay_db = int(batch.termination.energy_decay_db is not None)
-        b.energy_decay_db = float(batch.termination.energy_decay_db or 0.0)
-        b.check_interval = int(batch.termination.check_interval)
-        b.sample_interval = int(batch.energy_monitoring.sample_interval)
-        b.track_peak = int(bool(batch.energy_monitoring.track_peak))
-        b.initial_peak_energy = float(batch.initial_peak_energy)
-        si = batch.energy_monitoring.sample_interval
-        cap = (int(num_steps) // si + 2) if si > 0 else 1
-        samples = (N.EnergySampleC * cap)()
-        r = N.BatchResultC()
-        r.energy_samples = samples
-        r.energy_capacity = cap
+        b, r, samples, cap, keep = _batch_c(batch)
         N.check(N.lib().oems_engine_run_batch(self._h, ctypes.byref(b), ctypes.byref(r)))
-        es = [EnergySample(int(s.timestep), s.e_energy, s.h_energy, s.total_energy)
-              for s in samples[:min(cap, r.num_energy_samples)]]
-        return BatchResult(int(r.timesteps_executed), TerminationReason(r.termination_reason),
-                           float(r.final_decay_db), es, float(r.peak_energy),
-                           float(r.elapsed_seconds))
+        return _batch_result(r, samples, cap)
 
     def current_timestep(self) -> int:
         t = N.c_u64()
@@ -1240,6 +1209,101 @@ class Engine:
         n, s = N.c_u64(), N.c_f64()
         N.check(N.lib().oems_engine_last_batch_stats(self._h, ctypes.byref(n), ctypes.byref(s)))
         return int(n.value), float(s.value)
+
+
+def _batch_c(batch: "EngineBatch"):
+    """The C form of an EngineBatch: (batch, result with its energy sample
+    buffer, that buffer, its capacity, the arrays the batch borrows)."""
+    num_steps = batch.num_steps
+    if num_steps is None:
+        num_steps = batch.termination.max_timesteps
+    if num_steps is None:
+        raise N.ConfigError("EngineBatch needs num_steps or termination.max_timesteps")
+    keep = []
+    arr = (N.ScheduledExcitationC * max(1, len(batch.excitations)))()
+    for x, e in enumerate(batch.excitations):
+        s = np.ascontiguousarray(e.samples, dtype=np.float32)
+        keep.append(s)
+        for a in range(3):
+            arr[x].position[a] = int(e.position[a])
+        arr[x].direction = int(e.direction)
+        arr[x].soft_source = int(bool(e.soft_source))
+        arr[x].samples = N.fptr(s)
+        arr[x].num_samples = len(s)
+    keep.append(arr)
+    b = N.BatchC()
+    b.num_steps = int(num_steps)
+    b.excitations = arr
+    b.num_excitations = len(batch.excitations)
+    b.has_energy_decay_db = int(batch.termination.energy_decay_db is not None)
+    b.energy_decay_db = float(batch.termination.energy_decay_db or 0.0)
+    b.check_interval = int(batch.termination.check_interval)
+    b.sample_interval = int(batch.energy_monitoring.sample_interval)
+    b.track_peak = int(bool(batch.energy_monitoring.track_peak))
+    b.initial_peak_energy = float(batch.initial_peak_energy)
+    si = batch.energy_monitoring.sample_interval
+    cap = (int(num_steps) // si + 2) if si > 0 else 1
+    samples = (N.EnergySampleC * cap)()
+    r = N.BatchResultC()
+    r.energy_samples = samples
+    r.energy_capacity = cap
+    return b, r, samples, cap, keep
+
+
+def _batch_result(r, samples, cap) -> "BatchResult":
+    es = [EnergySample(int(s.timestep), s.e_energy, s.h_energy, s.total_energy)
+          for s in samples[:min(cap, r.num_energy_samples)]]
+    return BatchResult(int(r.timesteps_executed), TerminationReason(r.termination_reason),
+                       float(r.final_decay_db), es, float(r.peak_energy), float(r.elapsed_seconds))
+
+
+class Pack:
+    """Several engines stepped by shared launches (oems_pack_*): one launch
+    per half-step of the plain update kernels over all their CPML-free boxes
+    and one of the CPML kernels over all their slab cells, a post-step
+    launch with a CTA per engine and two energy launches for all.  Each
+    engine ends a batch with the bits oems_engine_run_batch would give it.
+    The engines need full coefficients and only CPML, sources, probes and
+    probe DFTs; keep them alive while the pack exists."""
+
+    def __init__(self, engines: Sequence["Engine"]):
+        self.engines = list(engines)
+        arr = (ctypes.c_void_p * len(self.engines))(*[e._h for e in self.engines])
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_pack_create(arr, len(self.engines), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib().oems_pack_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def run_batch(self, batches: Sequence[Optional["EngineBatch"]]):
+        """batches[i] for engine i (None: engine i sits this batch out); the
+        batches share num_steps, the energy intervals and whether they carry
+        a decay end condition, and the engines their timestep.  Returns a
+        BatchResult per engine (None where skipped); raises NumericalError
+        if an engine's energy stopped being finite (the others still ran)."""
+        n = len(self.engines)
+        if len(batches) != n:
+            raise N.ConfigError("one batch (or None) per engine of the pack")
+        conv = [(_batch_c(b) if b is not None else None) for b in batches]
+        bp = (ctypes.c_void_p * n)(*[ctypes.addressof(c[0]) if c else None for c in conv])
+        res = (N.BatchResultC * n)()
+        for i, c in enumerate(conv):
+            if c:
+                res[i] = c[1]
+        st = (N.c_i32 * n)()
+        N.check(N.lib().oems_pack_run_batch(self._h, bp, res, st))
+        out = [(_batch_result(res[i], c[2], c[3]) if c else None) for i, c in enumerate(conv)]
+        bad = [i for i in range(n) if st[i] != N.OK]
+        if bad:
+            N.check(st[bad[0]])
+        return out
 
 
 # ---------------------------------------------------------------------------

@@ -53,10 +53,13 @@ class SweepInstance:
 
 class Sweep:
     """oems_sweep: frequencies shared by every instance; `concurrency`
-    engines run at a time on `device`."""
+    engines run at a time on `device`.  packed=True: run / run_until step
+    the instances that share a step count together (one launch per
+    half-step over all their grids, oems_sweep_set_packed), with the same
+    bits per instance; `concurrency` then only parallelises their set-up."""
 
     def __init__(self, freqs, concurrency: int = 4, device: int = -1, compressed: bool = False,
-                 autotune: bool = False, kernels: str = "register", storage: str = "f32"):
+                 autotune: bool = False, kernels: str = "register", storage: str = "f32", packed: bool = False):
         self.freqs = np.ascontiguousarray(freqs, dtype=np.float64)
         if storage not in N.STORAGE_FLAGS:
             raise N.ConfigError(f"unknown field storage {storage!r}")
@@ -69,6 +72,8 @@ class Sweep:
                                           len(self.freqs), ctypes.byref(h)))
         self._h = h
         self.count = 0
+        if packed:
+            N.check(N.lib().oems_sweep_set_packed(h, 1))
 
     def close(self):
         h = getattr(self, "_h", None)

@@ -109,7 +109,7 @@ def lib() -> ctypes.CDLL:
         L.orc_get_nf2ff_face.restype = I64
         L.orc_get_nf2ff_face.argtypes = [P, I32, I32, I64, P]
         L.orc_enable_upml.restype = I32
-        L.orc_enable_upml.argtypes = [P, P, D, D]
+        L.orc_enable_upml.argtypes = [P, P, D, D, I32]
         L.orc_upml_kappa.argtypes = [P, I32, I32, P, I32, I64, D, D, D, ctypes.POINTER(D),
                                      ctypes.POINTER(D)]
         L.orc_run_batch.restype = I32
@@ -339,9 +339,13 @@ class OracleSim:
         z = out[0::2] + 1j * out[1::2]
         return z.reshape(4, nb, nc)
 
-    def enable_upml(self, layers=(8,) * 6, grading_order=3.0, reflection_coeff=1e-6):
+    def enable_upml(self, layers=(8,) * 6, grading_order=3.0, reflection_coeff=1e-6, kind=0):
+        """kind 0: the reference's UPML; kind 1: the corrected uniaxial PML."""
         l6 = np.ascontiguousarray(layers, dtype=np.int64)
-        return lib().orc_enable_upml(self._h, _ptr(l6), grading_order, reflection_coeff)
+        n = lib().orc_enable_upml(self._h, _ptr(l6), grading_order, reflection_coeff, int(kind))
+        if n < 0:
+            raise ValueError(f"invalid UPML kind {kind}")
+        return n
 
     def upml_kappa(self, comp, direction, pos, is_min, layers, width, sigma_max, m):
         p = np.ascontiguousarray(pos, dtype=np.int64)

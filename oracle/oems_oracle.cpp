@@ -191,8 +191,48 @@ struct Sim {
     *ki = smax * std::pow(std::clamp(di / width, 0.0, 1.0), m);
   }
 
-  // Upml::build_regions + init_region_coefficients (pml.rs:222-367)
-  int enable_upml(const int64_t* L, double m, double R0) {
+  // Conductivity of the corrected UPML (kind 1) along `dir` at cell index
+  // i, at the node (half = false) or half a cell above it: the graded
+  // sigma_max (depth / width)^m with the depth measured from the region's
+  // inner node (L at a min face, n - L - 1 at a max face), as the reference
+  // grades, but at the Yee position of the component.
+  double upml_sigma(int dir, bool is_min, int64_t L, int64_t i, bool half, double smax, double m) const {
+    const int64_t ext[3] = {nx, ny, nz};
+    const double x = (double)i + (half ? 0.5 : 0.0);
+    double depth = is_min ? (double)L - x : x - (double)(ext[dir] - L - 1);
+    depth = std::clamp(depth, 0.0, (double)L);
+    return smax * std::pow(depth / (double)L, m);
+  }
+  // Conductivity along `dir` at index i of every active face of that axis
+  // (a cell lies in at most one of them): corners and edges of the PML are
+  // graded along each axis whose slab they are in.
+  double upml_sigma_axis(const int64_t* L, int dir, int64_t i, bool half, double m, double R0) const {
+    const int64_t ext[3] = {nx, ny, nz};
+    double sg = 0.0;
+    for (int side = 0; side < 2; ++side) {
+      const int64_t l = L[2 * dir + side];
+      if (l <= 0 || l >= ext[dir]) continue;
+      const double smax = -(m + 1.0) * std::log(R0) / (2.0 * kZ0 * (double)l * delta[dir]);
+      sg = std::max(sg, upml_sigma(dir, side == 0, l, i, half, smax, m));
+    }
+    return sg;
+  }
+
+  // Upml::build_regions + init_region_coefficients (pml.rs:222-367).
+  // kind 0: the reference's coefficients.  kind 1: the uniaxial PML of
+  // Taflove & Hagness 7.8 in the same flux form: for component n (nP, nPP
+  // the next two axes) the main update advances D with sigma_nP
+  // (Ca = (2 eps0 - s_nP dt) / (2 eps0 + s_nP dt), Cb scaled by
+  // 2 eps0 / (2 eps0 + s_nP dt)), and the hooks take E from D with
+  // vv = (2 eps0 - s_nPP dt) / den, vvfo / vvfn = (2 eps0 -/+ s_n dt) / den,
+  // den = 2 eps0 + s_nPP dt.  Every cell of the regions is graded along
+  // each axis whose slab holds it (so edges and corners absorb along all
+  // of them), at the Yee position of each component; a zero conductivity
+  // gives vv = vvfo = vvfn = 1 (E follows D).  The reference instead grades
+  // only the region's own axis and puts that value in every axis slot,
+  // writes vvfo = 0 where nothing is graded and leaves the main update
+  // unchanged, which grows without bound.
+  int enable_upml(const int64_t* L, double m, double R0, int kind = 0) {
     const int64_t ext[3] = {nx, ny, nz};
     struct Box {
       int64_t s[3], z[3];
@@ -233,6 +273,34 @@ struct Sim {
         for (int64_t lj = 0; lj < b.z[1]; ++lj)
           for (int64_t lk = 0; lk < b.z[2]; ++lk, ++t) {
             const int64_t pos[3] = {b.s[0] + li, b.s[1] + lj, b.s[2] + lk};
+            if (kind == 1) {
+              const int64_t q = idx(pos[0], pos[1], pos[2]);
+              for (int c = 0; c < 3; ++c) {
+                // E_c sits half a cell up its own axis, H_c along the others
+                double sv[3], si[3];
+                for (int d = 0; d < 3; ++d) {
+                  sv[d] = upml_sigma_axis(L, d, pos[d], c == d, m, R0);
+                  si[d] = upml_sigma_axis(L, d, pos[d], c != d, m, R0);
+                }
+                const int np = (c + 1) % 3, npp = (c + 2) % 3;
+                const double dv = 2.0 * kEps0 + sv[npp] * dt, di = 2.0 * kEps0 + si[npp] * dt;
+                Rg.cv[0][c][t] = T((2.0 * kEps0 - sv[npp] * dt) / dv);
+                Rg.cv[1][c][t] = T((2.0 * kEps0 - sv[c] * dt) / dv);
+                Rg.cv[2][c][t] = T((2.0 * kEps0 + sv[c] * dt) / dv);
+                Rg.ci[0][c][t] = T((2.0 * kEps0 - si[npp] * dt) / di);
+                Rg.ci[1][c][t] = T((2.0 * kEps0 - si[c] * dt) / di);
+                Rg.ci[2][c][t] = T((2.0 * kEps0 + si[c] * dt) / di);
+                if (ca[c][q] != T(0) || cb[c][q] != T(0)) {
+                  ca[c][q] = T((2.0 * kEps0 - sv[np] * dt) / (2.0 * kEps0 + sv[np] * dt));
+                  cb[c][q] = T((double)cb[c][q] * (2.0 * kEps0 / (2.0 * kEps0 + sv[np] * dt)));
+                }
+                if (da[c][q] != T(0) || db[c][q] != T(0)) {
+                  da[c][q] = T((2.0 * kEps0 - si[np] * dt) / (2.0 * kEps0 + si[np] * dt));
+                  db[c][q] = T((double)db[c][q] * (2.0 * kEps0 / (2.0 * kEps0 + si[np] * dt)));
+                }
+              }
+              continue;
+            }
             double kv[3], ki[3];
             for (int c = 0; c < 3; ++c) upml_kappa(c, b.dir, pos, b.mn, layers, width, smax, m, &kv[c], &ki[c]);
             for (int c = 0; c < 3; ++c) {
@@ -1697,9 +1765,11 @@ double orc_set_lumped(orc_sim* s, const int64_t* pos, int32_t dir, double r, dou
   return scale;
 }
 
-int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff) {
+int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff,
+                        int32_t kind) {
+  if (kind != 0 && kind != 1) return -1;
   int n = 0;
-  DISPATCH(s, n = S->enable_upml(layers6, grading_order, reflection_coeff));
+  DISPATCH(s, n = S->enable_upml(layers6, grading_order, reflection_coeff, kind));
   return n;
 }
 

@@ -170,7 +170,10 @@ int32_t orc_add_nf2ff_box(orc_sim* s, const int64_t* lo3, const int64_t* hi3, co
 int64_t orc_get_nf2ff_face(const orc_sim* s, int32_t id, int32_t face, int64_t f, double* out);
 /* Uniaxial PML as the reference (src/extensions/pml.rs:194-655), hooks
  * around the H and E updates (innermost); returns the number of regions. */
-int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff);
+/* kind 0: the reference's UPML coefficients; kind 1: the corrected uniaxial
+ * PML (main update coefficients of the region cells changed as well). */
+int32_t orc_enable_upml(orc_sim* s, const int64_t* layers6, double grading_order, double reflection_coeff,
+                        int32_t kind);
 /* Upml::calculate_kappa (pml.rs:370-420) for known-answer checks. */
 void orc_upml_kappa(const orc_sim* s, int32_t comp, int32_t dir, const int64_t* pos3, int32_t is_min,
                     int64_t layers, double width, double smax, double m, double* kv, double* ki);

@@ -105,7 +105,7 @@ def run_oracle(sc: Scenario, precision=32, threads=1, zline=False):
     for pos, d, r, c, eps_r, sig in sc.lumped:
         s.set_lumped(pos, d, r, c, eps_r, sig)
     if sc.upml is not None:
-        s.enable_upml(sc.upml.layers, sc.upml.grading_order, sc.upml.reflection_coeff)
+        s.enable_upml(sc.upml.layers, sc.upml.grading_order, sc.upml.reflection_coeff, sc.upml.kind)
     for mat, cells in sc.dispersive:
         d = mat.to_c()
         s.add_dispersive(d.kind, list(d.params), cells, d.eps_inf)
@@ -330,9 +330,25 @@ def dispersive_scenarios() -> List[Scenario]:
 
 def upml_scenarios() -> List[Scenario]:
     """The reference's UPML: short runs (it grows without bound), all faces
-    and partial faces, with a dielectric and Mur on other faces."""
+    and partial faces, with a dielectric and Mur on other faces; the
+    corrected UPML (kind 1): the reference's PML scenario for its full 300
+    steps, and partial faces with a lossy dielectric and a PEC block that
+    reach into the PML."""
     E = oe.Excitation
     return [
+        Scenario("upml_fixed_reference_scenario", (60, 60, 60), 0.5e-3,
+                 excitations=[E.gaussian(3e9, 0.5, 2, (30, 30, 30))], num_steps=300, sample_interval=30,
+                 track_peak=True, upml=oe.PmlBoundaries.uniform(8, kind=1),
+                 probes=[(2, (30, 30, 30)), (2, (3, 30, 30)), (4, (55, 5, 57))]),
+        Scenario("upml_fixed_partial", (19, 15, 26), 0.5e-3,
+                 materials=[(3.0, 1.0, 0.02, 0.0, (2, 17, 3, 12, 4, 24))],
+                 pec=[(8, 10, 0, 4, 10, 14)],
+                 excitations=[E.gaussian(4e9, 0.5, 1, (9, 7, 13)), E.gaussian(5e9, 0.5, 0, (12, 9, 15))],
+                 num_steps=160, sample_interval=20, track_peak=True,
+                 upml=oe.PmlBoundaries(layers=(4, 0, 3, 5, 0, 6), grading_order=4.0, reflection_coeff=1e-5,
+                                       kind=1),
+                 mur=oe.MurAbcConfig(enabled=(0, 1, 0, 0, 1, 0)),
+                 probes=[(1, (9, 7, 13)), (3, (1, 1, 1)), (0, (17, 13, 24))]),
         Scenario("upml_all_20", (20, 21, 22), 0.5e-3,
                  excitations=[E.gaussian(3e9, 0.5, 2, (10, 10, 11))], num_steps=40, sample_interval=5,
                  track_peak=True, upml=oe.PmlBoundaries.uniform(4),

@@ -1,5 +1,6 @@
-"""CPML absorption: how much of a pulse the 8-cell CPML of the benchmark
-configuration (m = 3, R0 = 1e-6, kappa 1, alpha 0) reflects.
+"""CPML and UPML absorption: how much of a pulse the 8-cell CPML of the
+benchmark configuration (m = 3, R0 = 1e-6, kappa 1, alpha 0), and the
+corrected UPML with the same grading, reflect.
 
 The reference only checks that its CPML scenario stays finite
 (src/fdtd/engine_testing.rs:1780-1864), and its psi is never applied to the
@@ -21,11 +22,13 @@ N_SMALL, MARGIN, LAYERS, STEPS = 72, 52, 8, 260
 F0, BW = 12e9, 8e9
 
 
-def _traces(n, layers, probes, sources, precision=32):
+def _traces(n, layers, probes, sources, precision=32, upml=False):
     lines = [oracle.uniform_lines(n, 1e-3)] * 3
     dt, d3 = oracle.grid_timestep(*lines)
     s = oracle.OracleSim(n, n, n, dt, d3, precision=precision, threads=8, zline=True)
-    if layers:
+    if layers and upml:
+        s.enable_upml((layers,) * 6, 3.0, 1e-6, kind=1)
+    elif layers:
         s.enable_cpml((layers,) * 6, 3.0, 1e-6, 0.0, 1.0)
     c = n // 2
     tau = 1.0 / (np.pi * BW)
@@ -61,6 +64,15 @@ def test_cpml_reflection_below_minus_60_db(reference_traces):
     small = _traces(N_SMALL, LAYERS, PROBES, (2, 0))
     refl = _reflection_db(small, reference_traces)
     print("CPML 8 reflection (dB) towards +x -x +y -y +z -z:", np.round(refl, 1))
+    assert np.all(refl < -60.0), refl
+
+
+def test_corrected_upml_reflection_below_minus_60_db(reference_traces):
+    """The corrected UPML (kind 1) with the same grading absorbs like the
+    CPML; the reference's coefficients (kind 0) grow instead."""
+    small = _traces(N_SMALL, LAYERS, PROBES, (2, 0), upml=True)
+    refl = _reflection_db(small, reference_traces)
+    print("UPML 8 reflection (dB) towards +x -x +y -y +z -z:", np.round(refl, 1))
     assert np.all(refl < -60.0), refl
 
 

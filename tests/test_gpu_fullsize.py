@@ -11,10 +11,13 @@ lumped port in a wire dipole, CPML, NF2FF box with f64 DFTs) for 500 steps.
 
 The oracle restates the reference's update (src/fdtd/basic_engine.rs:191-306)
 in the loop form of its SIMD engine (src/fdtd/simd_engine.rs:252-391), on
-every host core.  Fields, probe traces and DFT accumulators must be
-bit-identical, so the stated gate (relative L2 <= 1e-5 per field array and
-probe trace after the stated step count) holds with margin; the test asserts
-both and prints the relative L2 of each array.
+every host core.  Fields, probe traces and NF2FF accumulators must be
+bit-identical (port DFTs within 1e-12: their twiddles come from the device's
+sincos), so the stated gate (relative L2 <= 1e-5 per field array and probe
+trace after the stated step count) holds with margin; the test asserts both
+and prints the relative L2 of each array.  The kernel families: the shape
+the autotuner picks, the z-split (plain kernels on the CPML-free box) and
+the bulk-async staged kernels.
 """
 import os
 
@@ -54,7 +57,7 @@ def config2_oracle():
     return run_oracle(config2_scenario(), precision=32, threads=THREADS, zline=True)
 
 
-@pytest.mark.parametrize("kernels", ("auto", "register", "zsplit", "staged"))
+@pytest.mark.parametrize("kernels", ("auto", "zsplit", "staged"))
 def test_config2_cpml_boxes_256_10000_steps(config2_oracle, kernels):
     got = run_engine(config2_scenario(), kernels=kernels)
     report(f"config 2 ({kernels}, shape {got['engine'].launch_info()})", got, config2_oracle)
@@ -134,9 +137,13 @@ def test_config3_dispersive_scene_384_500_steps():
     assert np.abs(ref[2]).max() > 0
     assert max(errs) <= 1e-5
     assert np.array_equal(got, ref)
+    # the port DFTs take their twiddles from the device's sincos and the
+    # host's libm (the same 1e-12 bar as the sweep's oracle test); the NF2FF
+    # accumulators use one host twiddle table and match bit for bit
     port.calc_port(eng)
-    assert np.array_equal(port.uf_tot, s.probe_dft(dft[0]))
-    assert np.array_equal(port.if_tot, s.probe_dft(dft[1]))
+    for got_f, d in ((port.uf_tot, dft[0]), (port.if_tot, dft[1])):
+        want = s.probe_dft(d)
+        assert np.abs(got_f - want).max() <= 1e-12 * np.abs(want).max()
     for face in range(6):
         for fi in range(len(sc.freqs)):
             assert np.array_equal(box.face(face, fi), s.nf2ff_face(obox, face, fi, lo, hi)), (face, fi)
