@@ -241,42 +241,66 @@ def sweep_metric(count=64, seed=4, concurrency=16):
     stop against the plain full-length batched sweep, on the patch-antenna
     sweep family (n_{x,y,z} ~ U{48..160}, 0.5 mm, CPML 8, 50 ohm lumped feed,
     Gaussian 0-8 GHz, -50 dB energy decay or 60,000 steps, S11 at 801
-    points).  Both sweeps run the same instances on this GPU, each timed on
+    points).  Every sweep runs the same instances on this GPU, each timed on
     the host clock around the whole sweep (every instance's engine set-up,
-    device runs, DFTs, checks and read-backs).  The staged sweep uses the
-    dense pencil plan with the strict residual check; its S11 error per
-    instance is the largest |dB difference| to the plain run over f >= 0.5
-    GHz with both clipped at -30 dB (instances that decay or fall back to a
-    full run are exact)."""
+    device runs, DFTs, checks and read-backs).  The plain sweep runs twice,
+    with an engine and stream per instance and packed (all instances stepped
+    together), and the faster one is the baseline.  The staged sweeps use
+    the dense pencil plan, accepting a stage by the residual check alone
+    (tau 0.1 dB) or by the trained acceptance network
+    (openems_b200/data/stage_net.npz).  The S11 error of an instance is the
+    largest |dB difference| to the plain run over f >= 0.5 GHz with both
+    clipped at -30 dB (instances that decay or fall back to a full run are
+    exact)."""
     from openems_b200 import early_stop as ES
-    insts, freqs = ES.family_instances("patch", count, seed)
+    from openems_b200 import stage_net as SN
     plan = ES.StagePlan.dense()
+
+    def fresh():
+        return ES.family_instances("patch", count, seed)
+
+    insts, freqs = fresh()
     band = plan.band(freqs)
     full = ES.full_sweep(insts, freqs, concurrency)
     fs11 = [r["s11"] for r in full["results"]]
-    insts, _ = ES.family_instances("patch", count, seed)
-    st = ES.staged_sweep(insts, freqs, plan, concurrency)
-    errs = np.array([0.0 if r["how"] != "predicted" else ES.s11_db_error(r["s11"], f, band)
-                     for r, f in zip(st["results"], fs11)])
-    hows = [r["how"] for r in st["results"]]
+    packed = ES.full_sweep(fresh()[0], freqs, concurrency, packed=True)
+    same = all(np.array_equal(a["s11"], b["s11"]) and a["timesteps"] == b["timesteps"]
+               for a, b in zip(full["results"], packed["results"]))
+    plain_s = min(full["wall_s"], packed["wall_s"])
     steps_full = np.array([r["timesteps"] for r in full["results"]], dtype=np.float64)
-    steps_st = np.array([r["steps"] for r in st["results"]], dtype=np.float64)
-    plain_h = count / full["wall_s"] * 3600.0
-    staged_h = count / st["wall_s"] * 3600.0
+    cells = np.array([r["cells"] for r in full["results"]], dtype=np.float64)
+
+    def staged(net=None):
+        st = ES.staged_sweep(fresh()[0], freqs, plan, concurrency, net=net)
+        errs = np.array([0.0 if r["how"] != "predicted" else ES.s11_db_error(r["s11"], f, band)
+                         for r, f in zip(st["results"], fs11)])
+        hows = [r["how"] for r in st["results"]]
+        steps = np.array([r["steps"] for r in st["results"]], dtype=np.float64)
+        return {"instances_per_hour": count / st["wall_s"] * 3600.0, "wall_s": st["wall_s"],
+                "speedup": plain_s / st["wall_s"], "step_ratio": float(steps_full.sum() / steps.sum()),
+                "predicted": hows.count("predicted"), "decayed": hows.count("decayed"),
+                "fallback_full": hows.count("full"), "max_err_db": float(errs.max()),
+                "median_err_db_predicted": float(np.median(errs[errs > 0])) if (errs > 0).any() else 0.0,
+                "instances_over_0.5db": int((errs > 0.5).sum())}
+
+    check = staged()
+    net = SN.load_default()
+    learned = staged(net) if net is not None else None
+    head = learned if learned is not None else check
     return {
         "metric": "S11 sweeps/hr learned vs plain at <= 0.5 dB",
         "workload": f"patch_sweep_{count}_seed{seed}: n ~ U{{48..160}}^3, 0.5 mm, CPML 8, 50 ohm feed, "
                     "Gaussian 0-8 GHz, -50 dB or 60000 steps, 801 S11 points",
-        "plain_instances_per_hour": plain_h, "staged_instances_per_hour": staged_h,
-        "speedup": staged_h / plain_h, "plain_wall_s": full["wall_s"], "staged_wall_s": st["wall_s"],
-        "step_ratio": float(steps_full.sum() / steps_st.sum()),
+        "plain_instances_per_hour": count / plain_s * 3600.0,
+        "plain_streams_wall_s": full["wall_s"], "plain_packed_wall_s": packed["wall_s"],
+        "plain_streams_mcells": float((cells * steps_full).sum() / full["wall_s"] / 1e6),
+        "plain_packed_mcells": float((cells * steps_full).sum() / packed["wall_s"] / 1e6),
+        "packed_equals_streams": bool(same),
+        "staged_instances_per_hour": head["instances_per_hour"], "speedup": head["speedup"],
+        "rule": "learned" if learned is not None else "residual check",
+        "staged_learned": learned, "staged_residual_check": check,
         "plan": {"stages": list(plan.stages), "tau_db": plan.tau, "check": plan.check,
                  "samples": plan.samples, "max_modes": plan.max_modes},
-        "predicted": hows.count("predicted"), "decayed": hows.count("decayed"),
-        "fallback_full": hows.count("full"),
-        "max_err_db": float(errs.max()), "median_err_db_predicted":
-            float(np.median(errs[errs > 0])) if (errs > 0).any() else 0.0,
-        "instances_over_0.5db": int((errs > 0.5).sum()),
         "error": "per instance: max over f >= 0.5 GHz of |dB(staged) - dB(plain)|, both clipped at -30 dB",
     }
 

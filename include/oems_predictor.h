@@ -35,6 +35,14 @@ OEMS_API oems_status oems_pk_im2col(const float* x, void* cols, int B, int T, in
 /* Adjoint of im2col: dx[b, tau, c] = sum of the dcols entries that read x[b, tau, c]. */
 OEMS_API oems_status oems_pk_col2im(const float* dcols, int ldc, float* dx, int B, int T, int C, int ks, int s,
                                     void* stream);
+/* Causal dilated conv1d as im2col over (B, T, C) f32: cols (B T rows, pitch
+ * ldc >= ks C, bf16) row (b, t) holds x[b, t - (ks - 1 - k) dil, c] at
+ * column k C + c, 0 before the start; the output keeps the length T. */
+OEMS_API oems_status oems_pk_im2col_causal(const float* x, void* cols, int B, int T, int C, int ks, int dil,
+                                           int ldc, void* stream);
+/* Adjoint of the causal im2col: dx[b, tau, c] sums the dcols entries that read x[b, tau, c]. */
+OEMS_API oems_status oems_pk_col2im_causal(const float* dcols, int ldc, float* dx, int B, int T, int C, int ks,
+                                           int dil, void* stream);
 /* x = max(x, 0) for rows x w values; xb (may be NULL) receives a bf16 copy with row pitch ldb. */
 OEMS_API oems_status oems_pk_relu(float* x, void* xb, int64_t rows, int w, int ldb, void* stream);
 OEMS_API oems_status oems_pk_relu_bwd(float* dy, const float* y, int64_t n, void* stream);

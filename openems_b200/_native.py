@@ -302,6 +302,8 @@ SIGNATURES = {
     "oems_pk_transpose_bf16": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, P]),
     "oems_pk_im2col": (c_i32, [P, P, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
     "oems_pk_col2im": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
+    "oems_pk_im2col_causal": (c_i32, [P, P, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
+    "oems_pk_col2im_causal": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, c_i32, c_i32, P]),
     "oems_pk_relu": (c_i32, [P, P, c_i64, c_i32, c_i32, P]),
     "oems_pk_relu_bwd": (c_i32, [P, P, c_i64, P]),
     "oems_pk_colsum": (c_i32, [P, c_i64, c_i32, P, P]),

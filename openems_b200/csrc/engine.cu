@@ -1449,7 +1449,7 @@ static oems_status autotune(oems_engine* en) {
       s.ichunk = 16;
       s.smem = make_tma_geom(en, std::max(1, std::min(jhi - jlo, 256 / en->g.nzq)), 16, 256, limit, 4, s.tg, true);
       if (s.smem == 0) s = LaunchShape{};
-    } else if (!want_reg) {
+    } else if (!want_reg && !only_z) {
       size_t limit = 0;
       OEMS_TRY(tma_smem_limit(en, &limit));
       s.tma = true;

@@ -111,6 +111,43 @@ __global__ void k_col2im(const float* dcols, int ldc, float* dx, int B, int T, i
   }
 }
 
+// Causal dilated im2col: output length T; row (b, t) holds, at k C + c,
+// x[b, t - (ks - 1 - k) dil, c] (0 before the start), so tap ks - 1 is the
+// current step and the others reach back by multiples of the dilation.
+__global__ void k_im2col_causal(const float* x, __nv_bfloat16* cols, int B, int T, int C, int ks, int dil, int ldc) {
+  const long long n = (long long)B * T * ks * C;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    long long r = i / C;
+    const int k = (int)(r % ks);
+    r /= ks;
+    const int t = (int)(r % T);
+    const int b = (int)(r / T);
+    const int u = t - (ks - 1 - k) * dil;
+    const float v = u >= 0 ? x[((long long)b * T + u) * C + c] : 0.0f;
+    cols[((long long)b * T + t) * ldc + (long long)k * C + c] = __float2bfloat16_rn(v);
+  }
+}
+
+// Adjoint: dx[b, tau, c] = sum over k of dcols[(b, tau + (ks - 1 - k) dil), k C + c]
+// (terms past the end dropped), summed in k order.
+__global__ void k_col2im_causal(const float* dcols, int ldc, float* dx, int B, int T, int C, int ks, int dil) {
+  const long long n = (long long)B * T * C;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long long r = i / C;
+    const int tau = (int)(r % T);
+    const int b = (int)(r / T);
+    float acc = 0.f;
+    for (int k = 0; k < ks; ++k) {
+      const int t = tau + (ks - 1 - k) * dil;
+      if (t >= T) continue;
+      acc += dcols[((long long)b * T + t) * ldc + (long long)k * C + c];
+    }
+    dx[i] = acc;
+  }
+}
+
 // y = max(x, 0) in place, with a bf16 copy of y (pitch ldb, rows of width w)
 __global__ void k_relu(float* x, __nv_bfloat16* xb, long long rows, int w, int ldb) {
   const long long n = rows * w;
@@ -264,6 +301,25 @@ oems_status oems_pk_col2im(const float* dcols, int ldc, float* dx, int B, int T,
   const int Tout = (T - ks) / s + 1;
   const long long n = (long long)B * T * C;
   k_col2im<<<grid_for(n, 8192), 256, 0, S(stream)>>>(dcols, ldc, dx, B, T, C, ks, s, Tout);
+  PK_CUDA(cudaGetLastError());
+  return OEMS_OK;
+}
+
+oems_status oems_pk_im2col_causal(const float* x, void* cols, int B, int T, int C, int ks, int dil, int ldc,
+                                  void* stream) {
+  if (ks < 1 || dil < 1 || ldc < ks * C) return pfail(OEMS_ERR_CONFIG, "im2col_causal: bad kernel, dilation or pitch");
+  const long long n = (long long)B * T * ks * C;
+  k_im2col_causal<<<grid_for(n, 8192), 256, 0, S(stream)>>>(x, static_cast<__nv_bfloat16*>(cols), B, T, C, ks, dil,
+                                                            ldc);
+  PK_CUDA(cudaGetLastError());
+  return OEMS_OK;
+}
+
+oems_status oems_pk_col2im_causal(const float* dcols, int ldc, float* dx, int B, int T, int C, int ks, int dil,
+                                  void* stream) {
+  if (ks < 1 || dil < 1 || ldc < ks * C) return pfail(OEMS_ERR_CONFIG, "col2im_causal: bad kernel, dilation or pitch");
+  const long long n = (long long)B * T * C;
+  k_col2im_causal<<<grid_for(n, 8192), 256, 0, S(stream)>>>(dcols, ldc, dx, B, T, C, ks, dil);
   PK_CUDA(cudaGetLastError());
   return OEMS_OK;
 }

@@ -128,9 +128,13 @@ class StagePlan:
         return dict(window=window, decimate=max(1, window // self.samples), max_modes=self.max_modes)
 
 
-def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, both: bool = False):
-    """(prediction at K, residual-check value in dB, continuation end step);
-    with both=True the check value is the pair (max, mean) over the band."""
+def stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan) -> dict:
+    """Everything known about an instance paused at stage K: the pencil
+    prediction of S11 ("pred"), the residual check's largest and mean |dB|
+    difference over the band ("check_max", "check_mean"), the estimated
+    end step of the plain run ("end"), the port voltage's pencil mode count
+    ("modes"), the pencil window ("window") and the energy level below the
+    peak ("level", dB)."""
     pen = plan.pencil(K)
     um = P.pencil_modes(trace[:K, 0], K, dt, **pen)  # serves both the end estimate and the prediction
     end = plain_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, modes=um, **pen) \
@@ -139,10 +143,27 @@ def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, b
     a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, u_modes=um, **pen)
     b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
     band = plan.band(freqs)
+    return {"pred": a, "check_max": s11_db_error(a, b, band), "check_mean": s11_db_mean_error(a, b, band),
+            "end": end, "modes": len(um[0]), "window": pen["window"], "level": float(r["final_decay_db"])}
+
+
+def stage_features(trace, c: dict, K: int, horizon: int, plan: StagePlan):
+    """The learned rule's inputs (stage_net.window_input, scalar_input) from
+    a stage_check record."""
+    from . import stage_net as SN
+    x = SN.window_input(trace, K, c["window"])
+    sc = SN.scalar_input(c["check_max"], c["check_mean"], c["level"], K, c["end"], horizon, c["modes"],
+                         plan.max_modes)
+    return x, sc
+
+
+def check_instance(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan, both: bool = False):
+    """(prediction at K, residual-check value in dB, continuation end step);
+    with both=True the check value is the pair (max, mean) over the band."""
+    c = stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan)
     if both:
-        return a, (s11_db_error(a, b, band), s11_db_mean_error(a, b, band)), end
-    stat = s11_db_mean_error if plan.check == "mean" else s11_db_error
-    return a, stat(a, b, band), end
+        return c["pred"], (c["check_max"], c["check_mean"]), c["end"]
+    return c["pred"], c["check_mean"] if plan.check == "mean" else c["check_max"], c["end"]
 
 
 def _pool():
@@ -150,12 +171,15 @@ def _pool():
 
 
 def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int = 16,
-                 batch_steps: int = 2000) -> dict:
+                 batch_steps: int = 2000, net=None) -> dict:
     """Runs the staged sweep; returns per instance S11, how it was obtained
     ("decayed", "predicted" at a stage, or "full" fallback) and the steps
     run.  `concurrency` worker threads each take one instance at a time
     through its stages (oems_sweep_advance) and checks, so the host checks of
-    one instance overlap the device runs of the others."""
+    one instance overlap the device runs of the others.  With a trained
+    stage_net.StageNet `net`, a stage is accepted when the network's
+    predicted error is below its threshold instead of by the residual check
+    alone (the check values are among the network's inputs)."""
     import queue
     import threading
 
@@ -173,6 +197,7 @@ def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int
     errors: List[BaseException] = []
     check_s = [0.0]
     lock = threading.Lock()
+    net_lock = threading.Lock()
 
     def one(i):
         for K in plan.stages:
@@ -181,12 +206,22 @@ def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int
             if not r["paused"]:
                 return {"s11": r["s11"], "how": "decayed", "steps": r["timesteps"], "stage": K}
             tc = time.perf_counter()
-            pred, d, end = check_instance(sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan)
+            trace = sw.trace(i)
+            c = stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan)
+            d = c["check_mean"] if plan.check == "mean" else c["check_max"]
+            if net is not None:
+                x, sc = stage_features(trace, c, K, horizon, plan)
+                with net_lock:  # one forward at a time (the network keeps its activations)
+                    score = float(net.predict(x[None], sc[None])[0])
+                ok = score < net.threshold
+            else:
+                score, ok = d, d < plan.tau
             with lock:
                 check_s[0] += time.perf_counter() - tc
-            if d < plan.tau:
+            if ok:
                 sw.finish(i)
-                return {"s11": pred, "how": "predicted", "steps": K, "stage": K, "check_db": d, "end": end}
+                return {"s11": c["pred"], "how": "predicted", "steps": K, "stage": K, "check_db": d,
+                        "score": score, "end": c["end"]}
         sw.advance(i, horizon, batch_steps)
         r = sw.result(i)
         return {"s11": r["s11"], "how": "full", "steps": r["timesteps"], "stage": None}
@@ -220,10 +255,12 @@ def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int
     return {"results": [out[i] for i in ids], "wall_s": wall, "check_s": check_s[0]}
 
 
-def full_sweep(instances, freqs: np.ndarray, concurrency: int = 16, batch_steps: int = 2000) -> dict:
-    """The plain batched sweep: every instance to its end condition."""
+def full_sweep(instances, freqs: np.ndarray, concurrency: int = 16, batch_steps: int = 2000,
+               packed: bool = False) -> dict:
+    """The plain batched sweep: every instance to its end condition (packed:
+    all instances stepped together through one pack)."""
     t0 = time.perf_counter()
-    sw = Sweep(freqs, concurrency=concurrency)
+    sw = Sweep(freqs, concurrency=concurrency, packed=packed)
     ids = [sw.add(i) for i in instances]
     sw.run(batch_steps)
     res = [sw.result(i) for i in ids]
@@ -233,10 +270,12 @@ def full_sweep(instances, freqs: np.ndarray, concurrency: int = 16, batch_steps:
 
 
 def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.ndarray],
-              concurrency: int = 16, batch_steps: int = 2000) -> dict:
+              concurrency: int = 16, batch_steps: int = 2000, features: bool = False) -> dict:
     """Check values d[n, s] and prediction errors e[n, s] (dB, against the
     full runs) of every instance at every stage, with no instance finished
-    early (NaN where the instance had already decayed)."""
+    early (NaN where the instance had already decayed).  features=True also
+    keeps the learned rule's inputs: "x" (n, s, T_WIN, 2) float16 windows and
+    "s" (n, s, N_SCALAR) float32 (zeros where the instance had decayed)."""
     dt = instances[0].operator.timestep()
     horizon = max(i.max_timesteps for i in instances)
     decay_db = instances[0].energy_decay_db
@@ -250,6 +289,16 @@ def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.n
     end = np.full((n, ns), np.nan)
     em = np.full((n, ns), np.nan)
     dm = np.full((n, ns), np.nan)
+    if features:
+        from . import stage_net as SN
+        X = np.zeros((n, ns, SN.T_WIN, 2), dtype=np.float16)
+        S = np.zeros((n, ns, SN.N_SCALAR), dtype=np.float32)
+
+    def job(trace, r, K):
+        c = stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan)
+        f = stage_features(trace, c, K, horizon, plan) if features else None
+        return c, f
+
     from threadpoolctl import threadpool_limits
     with _pool() as pool, threadpool_limits(1):
         for s, K in enumerate(plan.stages):
@@ -258,14 +307,20 @@ def calibrate(instances, freqs: np.ndarray, plan: StagePlan, full_s11: List[np.n
             for k, i in enumerate(ids):
                 r = sw.result(i)
                 if r["paused"]:
-                    jobs[k] = pool.submit(check_instance, sw.trace(i), r, K, dt, freqs, horizon, decay_db, plan,
-                                          True)
+                    jobs[k] = pool.submit(job, sw.trace(i), r, K)
             for k, j in jobs.items():
-                pred, (d[k, s], dm[k, s]), end[k, s] = j.result()
-                e[k, s] = s11_db_error(pred, full_s11[k], band)
-                em[k, s] = s11_db_mean_error(pred, full_s11[k], band)
+                c, f = j.result()
+                d[k, s], dm[k, s], end[k, s] = c["check_max"], c["check_mean"], c["end"]
+                e[k, s] = s11_db_error(c["pred"], full_s11[k], band)
+                em[k, s] = s11_db_mean_error(c["pred"], full_s11[k], band)
+                if features:
+                    X[k, s] = f[0][:, :2].astype(np.float16)
+                    S[k, s] = f[1]
     sw.close()
-    return {"check_db": d, "check_mean_db": dm, "error_db": e, "mean_error_db": em, "end": end}
+    out = {"check_db": d, "check_mean_db": dm, "error_db": e, "mean_error_db": em, "end": end}
+    if features:
+        out["x"], out["s"] = X, S
+    return out
 
 
 def simulate(cal: dict, tau: float, check: str = "max") -> dict:

@@ -64,15 +64,24 @@ def test_pack_equals_separate_engines(storage):
     pack.close()
 
 
+def _decaying():
+    """CPML on all faces, on some faces, only on z, and none: with a
+    modulated Gaussian each falls 20 dB below its peak at another step."""
+    scs = cpml_scenarios() + [reference_scenarios()[2]]
+    for sc in scs:
+        sc.excitations = [oe.Excitation.gaussian_modulated(15e9, 0.5, 2, tuple(n // 2 for n in sc.dims))]
+    return scs
+
+
 def test_pack_skips_engines_and_stops_each_at_its_decay():
     """An engine given no batch stays untouched; engines end at their own
     decay checks within one pack batch, as they do alone."""
-    scs = _mixed()[:3]
+    scs = _decaying()
     alone = [_engine(sc) for sc in scs]
     packed = [_engine(sc) for sc in scs]
     pack = oe.Pack([e for _, e in packed])
-    want = [eng.run_batch(_batch(sc, op, 0, 600, decay=8.0)) for sc, (op, eng) in zip(scs, alone)]
-    got = pack.run_batch([_batch(sc, op, 0, 600, decay=8.0) for sc, (op, _) in zip(scs, packed)])
+    want = [eng.run_batch(_batch(sc, op, 0, 1500, decay=20.0)) for sc, (op, eng) in zip(scs, alone)]
+    got = pack.run_batch([_batch(sc, op, 0, 1500, decay=20.0) for sc, (op, _) in zip(scs, packed)])
     assert len({w.timesteps_executed for w in want}) > 1  # they end at different steps
     for w, g in zip(want, got):
         assert (g.timesteps_executed, g.termination_reason, g.final_decay_db) == \

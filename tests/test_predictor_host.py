@@ -198,3 +198,66 @@ def test_tailnet_oracle_im2col_adjoint_and_bf16_rounding():
     # round to nearest even on the 16 dropped bits
     v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, 1.0 + 2 ** -9, -2.5], dtype=np.float64)
     assert list(round_bf16(v)) == [1.0, 1.0, 1.0 + 2 ** -6, 1.0, -2.5]
+
+
+def _small_stage_ref():
+    from oracle.tailnet_ref import StageNetRef
+    rng = np.random.default_rng(21)
+    ch, ks = 6, 3
+    convs = [(rng.normal(0, 0.4, (ch, ks * 4)), rng.normal(0, 0.1, ch))] + \
+            [(rng.normal(0, 0.3, (ch, ks * ch)), rng.normal(0, 0.1, ch)) for _ in range(2)]
+    fc1 = (rng.normal(0, 0.3, (9, ch + 3)), rng.normal(0, 0.1, 9))
+    fc2 = (rng.normal(0, 0.3, (4, 9)), rng.normal(0, 0.1, 4))
+    return StageNetRef(convs, fc1, fc2, ks), rng.normal(size=(3, 40, 4)), rng.normal(size=(3, 3))
+
+
+def test_stagenet_oracle_gradients_match_finite_differences():
+    """Pins the CPU restatement of the acceptance network (causal dilated
+    TCN read at the last step, scalars, MLP): its hand-written backward
+    equals central differences of its forward (float64)."""
+    net, x, s = _small_stage_ref()
+    G = np.random.default_rng(22).normal(size=(3, 4))
+    net.forward(x, s)
+    grads = net.backward(G)
+    params = [p for c in net.convs for p in c] + list(net.fc1) + list(net.fc2)
+    flat = [g for pair in grads for g in pair]
+    rng = np.random.default_rng(23)
+    for p, g in zip(params, flat):
+        for _ in range(4):
+            idx = tuple(rng.integers(0, n) for n in p.shape)
+            old = p[idx]
+            p[idx] = old + 1e-6
+            up = (net.forward(x, s) * G).sum()
+            p[idx] = old - 1e-6
+            dn = (net.forward(x, s) * G).sum()
+            p[idx] = old
+            assert g[idx] == pytest.approx((up - dn) / 2e-6, rel=1e-5, abs=1e-8)
+
+
+def test_causal_im2col_adjoint_and_causality():
+    from oracle.tailnet_ref import col2im_causal, im2col_causal
+    rng = np.random.default_rng(3)
+    x, d = rng.normal(size=(2, 29, 3)), rng.normal(size=(2 * 29, 5 * 3))
+    assert np.isclose((im2col_causal(x, 5, 4) * d).sum(), (x * col2im_causal(d, 2, 29, 3, 5, 4)).sum(),
+                      rtol=1e-12)
+    cols = im2col_causal(x, 5, 4).reshape(2, 29, 5, 3)
+    assert np.array_equal(cols[:, 20, 4], x[:, 20]) and np.array_equal(cols[:, 20, 0], x[:, 4])
+    assert not cols[:, 3, :4].any()  # before the start
+
+
+def test_stage_rule_threshold_and_evaluation():
+    """first_accept / choose_threshold / evaluate on hand-made records: two
+    instances, three stages."""
+    from openems_b200 import stage_net as SN
+    score = np.array([0.5, -0.2, -0.9, 0.1, -0.5])
+    err = np.array([2.0, 0.3, 0.1, 0.9, 0.2])
+    stage = np.array([0, 1, 2, 0, 1])
+    inst = np.array([0, 0, 0, 1, 1])
+    acc, worst = SN.first_accept(score, err, stage, inst, 0.0)
+    assert acc == {0: 1, 1: 1} and worst == 0.3
+    acc, worst = SN.first_accept(score, err, stage, inst, 0.2)
+    assert acc == {0: 1, 1: 0} and worst == 0.9
+    thr = SN.choose_threshold(score, err, stage, inst, limit_db=0.5)
+    assert SN.first_accept(score, err, stage, inst, thr)[1] <= 0.5 and thr >= -0.2
+    r = SN.evaluate(score, 0.0, err, stage, inst, [100, 200, 400], np.array([1000.0, 1000.0]))
+    assert r["accepted"] == 2 and r["over_limit"] == 0 and r["step_ratio"] == pytest.approx(2000 / 400)
