@@ -546,9 +546,11 @@ OEMS_API oems_status oems_engine_launch_info(const oems_engine* engine, int32_t*
                                              int32_t* rows_per_tile, int32_t* stages,
                                              int32_t* grid);
 /* One launch shape the autotuner timed: kind as `staged` above, threads per
- * CTA, x-planes per work item, pipeline stages (staged) or L2 prefetch
- * distance (register), the number of H + E pairs timed and their device time
- * in milliseconds. */
+ * CTA, x-planes per work item, pipeline stages (staged) or, for the register
+ * kernels, the L2 prefetch distance + 10 x the register budget variant + 100
+ * x that of the CPML slab kernels of a z-split (0: up to 128 registers with
+ * 512-thread CTAs, 1 / 2: 256-thread CTAs capped at 85 / 64 registers), the
+ * number of H + E pairs timed and their device time in milliseconds. */
 typedef struct oems_tune_entry {
   int32_t kind;
   int32_t threads;

@@ -314,6 +314,8 @@ struct LaunchShape {
   // zsplit: plain register kernels (no CPML) on the CPML-free box and the
   // CPML kernels (sh_block, sh_ichunk) on every slab cell (x, y and z)
   bool zsplit = false;
+  int occ = 0;      // register budget of the (interior) register kernels
+  int sh_occ = 0;   // ... of the CPML slab kernels of a z-split
   int sh_block = 256, sh_ichunk = 8, grid_sh = 0, grid_se = 0;
   int grid_h = 0;
   int grid_e = 0;
@@ -815,14 +817,22 @@ static EKernel pick_e_t(int id_bytes, bool cpml) {
   if (id_bytes == 1) return cpml ? k_update_e<1, true, T> : k_update_e<1, false, T>;
   return cpml ? k_update_e<2, true, T> : k_update_e<2, false, T>;
 }
-static HKernel pick_h(int id_bytes, bool cpml, int storage = 0) {
+// occ: register budget variant, 0 the uncapped kernels, 1 / 2 the capped
+// ones (k_update_*_cap with 3 / 4 CTAs of 256 per SM), built for float
+// storage and full coefficients, the benchmark's kernels; other variants
+// ignore it.
+static HKernel pick_h(int id_bytes, bool cpml, int storage = 0, int occ = 0) {
   if (storage == 1) return pick_h_t<__half>(id_bytes, cpml);
   if (storage == 2) return pick_h_t<__nv_bfloat16>(id_bytes, cpml);
+  if (id_bytes == 0 && occ == 1) return cpml ? k_update_h_cap<true, 3> : k_update_h_cap<false, 3>;
+  if (id_bytes == 0 && occ == 2) return cpml ? k_update_h_cap<true, 4> : k_update_h_cap<false, 4>;
   return pick_h_t<float>(id_bytes, cpml);
 }
-static EKernel pick_e(int id_bytes, bool cpml, int storage = 0) {
+static EKernel pick_e(int id_bytes, bool cpml, int storage = 0, int occ = 0) {
   if (storage == 1) return pick_e_t<__half>(id_bytes, cpml);
   if (storage == 2) return pick_e_t<__nv_bfloat16>(id_bytes, cpml);
+  if (id_bytes == 0 && occ == 1) return cpml ? k_update_e_cap<true, 3> : k_update_e_cap<false, 3>;
+  if (id_bytes == 0 && occ == 2) return cpml ? k_update_e_cap<true, 4> : k_update_e_cap<false, 4>;
   return pick_e_t<float>(id_bytes, cpml);
 }
 
@@ -923,18 +933,18 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   int occ_h = 0, occ_e = 0;
   const bool mode = en->cpml.on && !s.zsplit;
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_h, (const void*)pick_h(en->id_bytes, mode, en->storage), s.block, smem));
+      &occ_h, (const void*)pick_h(en->id_bytes, mode, en->storage, s.occ), s.block, smem));
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ_e, (const void*)pick_e(en->id_bytes, mode, en->storage), s.block, smem));
+      &occ_e, (const void*)pick_e(en->id_bytes, mode, en->storage, s.occ), s.block, smem));
   const Geom g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
   s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h) * sms));
   s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e) * sms));
   if (s.zsplit) {
     int oh = 0, oe = 0;
     OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &oh, (const void*)pick_h(en->id_bytes, true, en->storage), s.sh_block, smem));
+        &oh, (const void*)pick_h(en->id_bytes, true, en->storage, s.sh_occ), s.sh_block, smem));
     OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &oe, (const void*)pick_e(en->id_bytes, true, en->storage), s.sh_block, smem));
+        &oe, (const void*)pick_e(en->id_bytes, true, en->storage, s.sh_occ), s.sh_block, smem));
     const Geom gs = make_shell_geom(en, s.sh_block, s.sh_ichunk, true);
     s.grid_sh = std::max(1, std::min(gs.work, std::max(1, oh) * sms));
     s.grid_se = std::max(1, std::min(gs.work, std::max(1, oe) * sms));
@@ -979,16 +989,18 @@ static cudaError_t launch_h(oems_engine* en) {
   }
   HArgs a = h_args(en);
   if (en->shape.zsplit) {
-    pick_h(en->id_bytes, false, en->storage)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
+    pick_h(en->id_bytes, false, en->storage, en->shape.occ)<<<en->shape.grid_h, en->shape.block, table_smem(en),
+                                                              en->stream>>>(a);
     if (en->gs.work > 0) {
       HArgs b = a;
       b.g = en->gs;
-      pick_h(en->id_bytes, true, en->storage)<<<en->shape.grid_sh, en->shape.sh_block, table_smem(en),
-                                                     en->stream>>>(b);
+      pick_h(en->id_bytes, true, en->storage, en->shape.sh_occ)<<<en->shape.grid_sh, en->shape.sh_block,
+                                                                 table_smem(en), en->stream>>>(b);
     }
     return cudaGetLastError();
   }
-  pick_h(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_h, en->shape.block, table_smem(en), en->stream>>>(a);
+  pick_h(en->id_bytes, en->cpml.on, en->storage, en->shape.occ)<<<en->shape.grid_h, en->shape.block, table_smem(en),
+                                                                  en->stream>>>(a);
   return cudaGetLastError();
 }
 static cudaError_t launch_e(oems_engine* en) {
@@ -1004,16 +1016,18 @@ static cudaError_t launch_e(oems_engine* en) {
   }
   EArgs a = e_args(en);
   if (en->shape.zsplit) {
-    pick_e(en->id_bytes, false, en->storage)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
+    pick_e(en->id_bytes, false, en->storage, en->shape.occ)<<<en->shape.grid_e, en->shape.block, table_smem(en),
+                                                              en->stream>>>(a);
     if (en->gs.work > 0) {
       EArgs b = a;
       b.g = en->gs;
-      pick_e(en->id_bytes, true, en->storage)<<<en->shape.grid_se, en->shape.sh_block, table_smem(en),
-                                                     en->stream>>>(b);
+      pick_e(en->id_bytes, true, en->storage, en->shape.sh_occ)<<<en->shape.grid_se, en->shape.sh_block,
+                                                                 table_smem(en), en->stream>>>(b);
     }
     return cudaGetLastError();
   }
-  pick_e(en->id_bytes, en->cpml.on, en->storage)<<<en->shape.grid_e, en->shape.block, table_smem(en), en->stream>>>(a);
+  pick_e(en->id_bytes, en->cpml.on, en->storage, en->shape.occ)<<<en->shape.grid_e, en->shape.block, table_smem(en),
+                                                                  en->stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -1509,23 +1523,31 @@ static oems_status autotune(oems_engine* en) {
   // plain kernels on the CPML-free box plus one CPML launch over the slabs
   // (want_z): most cells run with the plain kernels' register budget (64 /
   // 92 registers against 128 with spills for the CPML forms)
+  // register budgets (occ) only exist for float storage and full arrays
+  const int nocc = (en->storage == 0 && en->id_bytes == 0) ? 3 : 1;
   for (int b : {256, 512})
     for (int c : {4, 8, 16, 32})
-      for (int pf : {0, 2}) {
-        if (c > 2 * en->nx && c != 4) continue;
-        if (pf >= c) continue;
-        LaunchShape s;
-        s.block = b;
-        s.ichunk = c;
-        s.pf = pf;
-        if (want_reg) cands.push_back(s);
-        if (want_z) {
-          s.zsplit = true;
-          s.sh_block = 256;
-          s.sh_ichunk = std::min(c, 8);
-          cands.push_back(s);
+      for (int pf : {0, 2})
+        for (int occ = 0; occ < nocc; ++occ) {
+          if (c > 2 * en->nx && c != 4) continue;
+          if (pf >= c) continue;
+          if (occ > 0 && b != 256) continue;
+          LaunchShape s;
+          s.block = b;
+          s.ichunk = c;
+          s.pf = pf;
+          s.occ = occ;
+          if (want_reg) cands.push_back(s);
+          if (want_z) {
+            s.zsplit = true;
+            s.sh_block = 256;
+            s.sh_ichunk = std::min(c, 8);
+            for (int so = 0; so < nocc; ++so) {
+              s.sh_occ = so;
+              cands.push_back(s);
+            }
+          }
         }
-      }
   if (want_tma) {
     size_t limit = 0;
     OEMS_TRY(tma_smem_limit(en, &limit));
@@ -1585,7 +1607,7 @@ static oems_status autotune(oems_engine* en) {
     te.kind = shape_kind(s);
     te.threads = s.tma ? s.nconsumer + 32 : s.block;
     te.ichunk = s.ichunk;
-    te.extra = s.tma ? s.tg.NS : s.pf;
+    te.extra = s.tma ? s.tg.NS : s.pf + 10 * s.occ + 100 * s.sh_occ;
     te.reps = reps;
     te.ms = ms;
     en->tune_report.push_back(te);

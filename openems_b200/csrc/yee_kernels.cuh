@@ -771,6 +771,20 @@ __global__ void __launch_bounds__(512) k_update_e(const EArgs a) {
   for (int w = blockIdx.x; w < a.g.work; w += gridDim.x) e_item<kIdBytes, kCpml, T>(a, tab, w);
 }
 
+// The same kernels (float fields, full coefficient arrays) with a capped
+// register budget: 256-thread CTAs, kMinBlocks of them resident per SM
+// (3: <= 85 registers, 4: <= 64), spilling what does not fit, which trades
+// spills for more warps to hide the loads' latency.  The autotuner times
+// them against the uncapped kernels.
+template <bool kCpml, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_update_h_cap(const HArgs a) {
+  for (int w = blockIdx.x; w < a.g.work; w += gridDim.x) h_item<0, kCpml, float>(a, nullptr, w);
+}
+template <bool kCpml, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_update_e_cap(const EArgs a) {
+  for (int w = blockIdx.x; w < a.g.work; w += gridDim.x) e_item<0, kCpml, float>(a, nullptr, w);
+}
+
 // Several grids in one launch (independent instances of a sweep): part p of
 // the launch is one grid's update over one geometry (its interior or its
 // CPML shell), args[p] its arguments in device memory, its work items

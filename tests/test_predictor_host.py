@@ -261,3 +261,23 @@ def test_stage_rule_threshold_and_evaluation():
     assert SN.first_accept(score, err, stage, inst, thr)[1] <= 0.5 and thr >= -0.2
     r = SN.evaluate(score, 0.0, err, stage, inst, [100, 200, 400], np.array([1000.0, 1000.0]))
     assert r["accepted"] == 2 and r["over_limit"] == 0 and r["step_ratio"] == pytest.approx(2000 / 400)
+
+
+def test_stage_inputs_window_and_scalars():
+    """The acceptance network's inputs: the window ends at K - 1, keeps the
+    newest samples, is scaled per channel, and pads short windows at the
+    front with zeros."""
+    from openems_b200 import stage_net as SN
+    t = np.arange(5000, dtype=np.float64)
+    trace = np.stack([np.sin(t / 7.0) * (1 + t), np.cos(t / 5.0)], axis=1)
+    x = SN.window_input(trace, 4096, 3072)
+    assert x.shape == (SN.T_WIN, SN.C_IN) and x.dtype == np.float32
+    dec = 3072 // SN.T_WIN
+    w = trace[4096 - 3072:4096][::-1][::dec][::-1][-SN.T_WIN:]
+    assert np.allclose(x[:, :2], w / np.abs(w).max(axis=0), rtol=1e-6)
+    assert not x[:, 2:].any()
+    short = SN.window_input(trace, 300, 3072)
+    assert not short[:SN.T_WIN - (300 + dec - 1) // dec, :2].any() and np.abs(short[-1, :2]).max() > 0
+    s = SN.scalar_input(0.2, 0.05, -23.0, 4096, 20000, 40000, 30, 150)
+    assert s.shape == (SN.N_SCALAR,) and s[-1] == 1.0
+    assert s[0] == pytest.approx(np.log10(0.21)) and s[3] == pytest.approx(2.0 / 5.0)
