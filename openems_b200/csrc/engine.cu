@@ -1539,13 +1539,16 @@ static oems_status autotune(oems_engine* en) {
           s.occ = occ;
           if (want_reg) cands.push_back(s);
           if (want_z) {
+            // the slab launch: its work items are short (8 layers) and its
+            // z-slab parts uncoalesced, so it is latency-bound: short x-runs
+            // and narrow CTAs give it more items in flight
             s.zsplit = true;
-            s.sh_block = 256;
-            s.sh_ichunk = std::min(c, 8);
-            for (int so = 0; so < nocc; ++so) {
-              s.sh_occ = so;
-              cands.push_back(s);
-            }
+            for (int sb : {128, 256})
+              for (int sc : {1, 2, 4}) {
+                s.sh_block = sb;
+                s.sh_ichunk = sc;
+                cands.push_back(s);
+              }
           }
         }
   if (want_tma) {
@@ -3393,6 +3396,7 @@ oems_status oems_release_cached_memory(int32_t device) {
 // their slab cells (work items of all grids in one list, each grid's
 // arguments in a device table), then one post-step launch with a CTA per
 // grid; energies of all grids in two launches; CUDA graphs per span length.
+// Each grid is one part of the launch of its kind (plain or CPML).
 // Every grid's cells, sources, probes, energies, DFTs and termination are
 // computed by the same code in the same order as oems_engine_run_batch, so
 // each engine ends with the bits it would have on its own.
@@ -3471,12 +3475,10 @@ static oems_status pack_layout(oems_pack* p, const std::vector<int>& active) {
         op.push_back(op.back() + g.work);
       }
     };
-    if (en->cpml.on && can_zsplit(en)) {
-      add(make_interior_geom(en, kPackThreads, kPackIchunk), false);
-      add(make_shell_geom(en, kPackThreads, kPackIchunk, true), true);
-    } else {
-      add(make_geom(en, kPackThreads, kPackIchunk), en->cpml.on);
-    }
+    // the whole grid as one part: a sweep's grids are small, so most of
+    // their cells lie in the CPML slabs, where a z-split's slab launch is
+    // the slow one (measured: 23 GCells/s split against 34 with whole grids)
+    add(make_geom(en, kPackThreads, kPackIchunk), en->cpml.on);
     PostArgs q{};
     for (int c = 0; c < 3; ++c) {
       q.e[c] = en->E(c);

@@ -193,9 +193,11 @@ class StageNet:
         return self
 
 
-def train(x, s, y, cfg: StageNetConfig = StageNetConfig(), log=print) -> StageNet:
+def train(x, s, y, cfg: StageNetConfig = StageNetConfig(), log=print, val=None) -> StageNet:
     """Fits the network to log10(error + 0.01) targets y (n,) on the GPU:
-    Adam on the squared error of output 0 (outputs 1..7 carry no loss)."""
+    Adam on the squared error of output 0 (outputs 1..7 carry no loss).
+    With val = (x, s, y) of held-out instances, keeps the weights of the
+    epoch with the lowest validation loss (early stopping)."""
     torch = _torch()
     net = StageNet(cfg)
     n = len(x)
@@ -204,14 +206,23 @@ def train(x, s, y, cfg: StageNetConfig = StageNetConfig(), log=print) -> StageNe
     yt = torch.tensor(y, dtype=torch.float32, device="cuda")
     rng = np.random.default_rng(cfg.seed + 1)
     B = min(cfg.batch, n)
+    best, best_loss = None, np.inf
     for ep in range(cfg.epochs):
         perm = rng.permutation(n)
         losses = []
         for a in range(0, n - B + 1, B):
             idx = torch.tensor(perm[a:a + B], device="cuda")
             losses.append(train_step(net, xt[idx].contiguous(), st[idx].contiguous(), yt[idx].contiguous()))
+        vloss = None
+        if val is not None:
+            vloss = float(np.mean((net.predict(val[0], val[1]) - val[2]) ** 2))
+            if vloss < best_loss:
+                best_loss, best = vloss, net.state()
         if log and (ep % 10 == 0 or ep == cfg.epochs - 1):
-            log(f"epoch {ep}: loss {np.mean(losses):.4f}")
+            log(f"epoch {ep}: loss {np.mean(losses):.4f}" + ("" if vloss is None else f", validation {vloss:.4f}"))
+    if best is not None:
+        net.load(best)
+        net.best_validation_loss = best_loss
     return net
 
 
@@ -289,55 +300,115 @@ def evaluate(score, thr, err, stage_of, inst_of, stages, steps_full, limit_db: f
             "over_limit": int((errs > limit_db).sum()), "steps_mean": float(steps.mean())}
 
 
+def tradeoff(score, err, stage_of, inst_of, stages, steps_full, budgets=(0, 0.01, 0.02, 0.05)) -> list:
+    """For each violation budget (fraction of instances allowed above 0.5
+    dB), the largest threshold that meets it on these records and the step
+    ratio it gives: a rule's operating curve, for comparing rules at equal
+    error."""
+    n = len(steps_full)
+    out = []
+    cands = np.unique(np.quantile(score, np.linspace(0.0, 1.0, 400)))
+    for b in budgets:
+        allowed = int(np.floor(b * n + 1e-9))
+        best = None
+        for thr in cands:
+            r = evaluate(score, thr, err, stage_of, inst_of, stages, steps_full)
+            if r["over_limit"] <= allowed and (best is None or r["step_ratio"] > best["step_ratio"]):
+                best = r
+        out.append({"budget": b, "allowed": allowed, **(best or {"step_ratio": 1.0})})
+    return out
+
+
+def _records(family, count, seed, plan, concurrency, log, t0):
+    import time
+    from . import early_stop as ES
+    insts, freqs = ES.family_instances(family, count, seed)
+    full = ES.full_sweep(insts, freqs, concurrency)
+    fs11 = [r["s11"] for r in full["results"]]
+    insts, _ = ES.family_instances(family, count, seed)
+    cal = ES.calibrate(insts, freqs, plan, fs11, concurrency, features=True)
+    cal["steps_full"] = np.array([r["timesteps"] for r in full["results"]], dtype=np.float64)
+    if log:
+        log(f"{family} seed {seed}: {count} instances recorded ({time.perf_counter() - t0:.0f} s)")
+    return cal
+
+
+def _concat(a: dict, b: dict) -> dict:
+    """Records of two families as one (instances of b after those of a;
+    they share the stage list)."""
+    return {k: np.concatenate([a[k], b[k]]) for k in a}
+
+
 def learn(train_count: int = 1500, test_count: int = 400, family: str = "small", train_seed: int = 5,
-          test_seed: int = 50, cfg: StageNetConfig = StageNetConfig(), concurrency: int = 16, log=print):
-    """Generates the training and held-out records with the batched engine
-    (full runs for the reference S11, then every instance through every
-    stage of the dense plan), trains the network on the training family,
-    picks both rules' thresholds there (the largest keeping every training
-    instance within 0.5 dB) and compares them on the held-out family.
-    Returns (net, report, train records, test records)."""
+          test_seed: int = 50, extra_patch: int = 0, val_frac: float = 0.2,
+          cfg: StageNetConfig = StageNetConfig(), concurrency: int = 16, log=print):
+    """Generates the records with the batched engine (full runs for the
+    reference S11, then every instance through every stage of the dense
+    plan): train_count instances of `family` (plus extra_patch of the
+    64-patch sweep family, seed train_seed + 1) for training and test_count
+    held out.  A val_frac share of the training instances is held back for
+    validation: early stopping, and both rules' thresholds are chosen on the
+    validation instances' out-of-sample scores (the largest threshold
+    keeping every validation instance within 0.5 dB, and within a 1%
+    budget).  Returns (net, report, train records, test records)."""
     import time
     from . import early_stop as ES
     plan = ES.StagePlan.dense()
-    recs = {}
     t0 = time.perf_counter()
-    for name, count, seed in (("train", train_count, train_seed), ("test", test_count, test_seed)):
-        insts, freqs = ES.family_instances(family, count, seed)
-        full = ES.full_sweep(insts, freqs, concurrency)
-        fs11 = [r["s11"] for r in full["results"]]
-        insts, _ = ES.family_instances(family, count, seed)
-        cal = ES.calibrate(insts, freqs, plan, fs11, concurrency, features=True)
-        cal["steps_full"] = np.array([r["timesteps"] for r in full["results"]], dtype=np.float64)
-        recs[name] = cal
-        if log:
-            log(f"{name}: {count} instances recorded ({time.perf_counter() - t0:.0f} s)")
-    xtr, str_, etr, sgtr, ittr = rows(recs["train"])
+    rtr = _records(family, train_count, train_seed, plan, concurrency, log, t0)
+    if extra_patch:
+        rtr = _concat(rtr, _records("patch", extra_patch, train_seed + 1, plan, concurrency, log, t0))
+    rte = _records(family, test_count, test_seed, plan, concurrency, log, t0)
+    x, sc, e, sg, it = rows(rtr)
+    n_inst = len(rtr["steps_full"])
+    rng = np.random.default_rng(cfg.seed + 7)
+    val_inst = rng.permutation(n_inst)[:int(round(val_frac * n_inst))]
+    is_val = np.isin(it, val_inst)
+    y = np.log10(e + LOG_FLOOR)
     t1 = time.perf_counter()
-    net = train(xtr, str_, np.log10(etr + LOG_FLOOR), cfg, log=log)
+    net = train(x[~is_val], sc[~is_val], y[~is_val], cfg, log=log, val=(x[is_val], sc[is_val], y[is_val]))
     train_s = time.perf_counter() - t1
-    ptr = net.predict(xtr, str_)
-    net.threshold = choose_threshold(ptr, etr, sgtr, ittr)
-    ctr = np.log10(recs["train"]["check_db"][ittr, sgtr] + LOG_FLOOR)
-    check_thr = choose_threshold(ctr, etr, sgtr, ittr)
-    xte, ste, ete, sgte, itte = rows(recs["test"])
-    pte = net.predict(xte, ste)
-    cte = np.log10(recs["test"]["check_db"][itte, sgte] + LOG_FLOOR)
     stages = list(plan.stages)
-    sf_tr, sf_te = recs["train"]["steps_full"], recs["test"]["steps_full"]
+    # validation records, instances renumbered 0..v-1
+    vmap = {int(k): j for j, k in enumerate(sorted(val_inst))}
+    vi = np.array([vmap[int(k)] for k in it[is_val]])
+    vsteps = rtr["steps_full"][sorted(val_inst)]
+    pv = net.predict(x[is_val], sc[is_val])
+    cv = np.log10(rtr["check_db"][it[is_val], sg[is_val]] + LOG_FLOOR)
+    ev, sv = e[is_val], sg[is_val]
+
+    def thr_for(score, budget):
+        allowed = int(np.floor(budget * len(vsteps) + 1e-9))
+        best = -np.inf
+        for thr in np.unique(np.quantile(score, np.linspace(0.0, 1.0, 400))):
+            if evaluate(score, thr, ev, sv, vi, stages, vsteps)["over_limit"] <= allowed:
+                best = max(best, float(thr))
+        return best
+
+    xte, ste, ete, sgte, itte = rows(rte)
+    pte = net.predict(xte, ste)
+    cte = np.log10(rte["check_db"][itte, sgte] + LOG_FLOOR)
+    sf = rte["steps_full"]
+    deployed = {}
+    for budget in (0.0, 0.01):
+        tn, tc = thr_for(pv, budget), thr_for(cv, budget)
+        deployed[str(budget)] = {"network": evaluate(pte, tn, ete, sgte, itte, stages, sf),
+                                 "residual_check": evaluate(cte, tc, ete, sgte, itte, stages, sf)}
+    net.threshold = thr_for(pv, 0.0)
     report = {
-        "family": family, "train": train_count, "test": test_count, "train_seed": train_seed,
-        "test_seed": test_seed, "stages": stages, "records_train": int(len(etr)), "records_test": int(len(ete)),
-        "train_seconds": train_s, "epochs": cfg.epochs,
-        "network": {"train": evaluate(ptr, net.threshold, etr, sgtr, ittr, stages, sf_tr),
-                    "test": evaluate(pte, net.threshold, ete, sgte, itte, stages, sf_te)},
-        "residual_check": {"train": evaluate(ctr, check_thr, etr, sgtr, ittr, stages, sf_tr),
-                           "test": evaluate(cte, check_thr, ete, sgte, itte, stages, sf_te)},
+        "family": family, "train": train_count, "extra_patch": extra_patch, "test": test_count,
+        "train_seed": train_seed, "test_seed": test_seed, "validation_instances": int(len(val_inst)),
+        "stages": stages, "records_train": int((~is_val).sum()), "records_validation": int(is_val.sum()),
+        "records_test": int(len(ete)), "train_seconds": train_s, "epochs": cfg.epochs,
+        "best_validation_loss": float(getattr(net, "best_validation_loss", np.nan)),
+        "deployed_thresholds_from_validation": deployed,
+        "tradeoff_test": {"network": tradeoff(pte, ete, sgte, itte, stages, sf),
+                          "residual_check": tradeoff(cte, ete, sgte, itte, stages, sf)},
         # the best any rule can do: accept each instance at its first stage within 0.5 dB
-        "perfect_rule_test": evaluate(np.where(ete <= 0.5, -1.0, 1.0), 0.0, ete, sgte, itte, stages, sf_te),
+        "perfect_rule_test": evaluate(np.where(ete <= 0.5, -1.0, 1.0), 0.0, ete, sgte, itte, stages, sf),
         "pred_corr_test": float(np.corrcoef(pte, np.log10(ete + LOG_FLOOR))[0, 1]),
     }
-    return net, report, recs["train"], recs["test"]
+    return net, report, rtr, rte
 
 
 def default_weights_path() -> str:
@@ -367,14 +438,16 @@ def main(argv=None):
     p.add_argument("--train", type=int, default=1500)
     p.add_argument("--test", type=int, default=400)
     p.add_argument("--family", choices=["small", "patch"], default="small")
+    p.add_argument("--extra-patch", type=int, default=0,
+                   help="also train on this many instances of the 64-patch sweep family")
     p.add_argument("--epochs", type=int, default=StageNetConfig.epochs)
     p.add_argument("--concurrency", type=int, default=16)
     p.add_argument("--out", default=".")
     p.add_argument("--save-records", action="store_true", help="also write the records (.npz, float16 windows)")
     a = p.parse_args(argv)
     cfg = StageNetConfig(epochs=a.epochs)
-    net, report, rtr, rte = learn(a.train, a.test, a.family, cfg=cfg, concurrency=a.concurrency,
-                                  log=lambda m: print(m, flush=True))
+    net, report, rtr, rte = learn(a.train, a.test, a.family, extra_patch=a.extra_patch, cfg=cfg,
+                                  concurrency=a.concurrency, log=lambda m: print(m, flush=True))
     os.makedirs(a.out, exist_ok=True)
     np.savez(os.path.join(a.out, "stage_net.npz"), **net.state())
     if a.save_records:

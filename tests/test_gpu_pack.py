@@ -92,7 +92,8 @@ def test_pack_skips_engines_and_stops_each_at_its_decay():
     # an engine given no batch sits it out untouched
     fresh = [_engine(sc) for sc in scs]
     pack = oe.Pack([e for _, e in fresh])
-    res = pack.run_batch([_batch(scs[0], fresh[0][0], 0, 50), None, _batch(scs[2], fresh[2][0], 0, 50)])
+    res = pack.run_batch([_batch(scs[0], fresh[0][0], 0, 50), None, _batch(scs[2], fresh[2][0], 0, 50),
+                          _batch(scs[3], fresh[3][0], 0, 50)])
     assert res[1] is None and res[0].timesteps_executed == res[2].timesteps_executed == 50
     assert fresh[1][1].current_timestep() == 0
     assert not np.any(np.concatenate(fresh[1][1].read_fields()))
