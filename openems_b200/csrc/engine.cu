@@ -316,6 +316,11 @@ struct LaunchShape {
   bool zsplit = false;
   int occ = 0;      // register budget of the (interior) register kernels
   int sh_occ = 0;   // ... of the CPML slab kernels of a z-split
+  // z-split only: the slab launch runs on a second stream beside the
+  // interior launch (fork / join by events, captured into the graphs), the
+  // interior grid cut by `cut` CTAs per SM to leave room for it
+  bool fork = false;
+  int cut = 0;
   int sh_block = 256, sh_ichunk = 8, grid_sh = 0, grid_se = 0;
   int grid_h = 0;
   int grid_e = 0;
@@ -626,6 +631,9 @@ struct oems_engine {
   uint64_t last_launches = 0;
   double last_device_seconds = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // second stream of a forked z-split and its fork / join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
   // field storage: 0 float, 1 half, 2 bfloat16 (arithmetic in float); with
   // 2-byte storage H is kept multiplied by h_scale (a power of two)
@@ -937,8 +945,9 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &occ_e, (const void*)pick_e(en->id_bytes, mode, en->storage, s.occ), s.block, smem));
   const Geom g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
-  s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h) * sms));
-  s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e) * sms));
+  const int cut = s.zsplit && s.fork ? s.cut : 0;
+  s.grid_h = std::max(1, std::min(g.work, std::max(1, occ_h - cut) * sms));
+  s.grid_e = std::max(1, std::min(g.work, std::max(1, occ_e - cut) * sms));
   if (s.zsplit) {
     int oh = 0, oe = 0;
     OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -953,7 +962,15 @@ static oems_status size_grid(oems_engine* en, LaunchShape& s) {
 }
 
 static void apply_shape(oems_engine* en, const LaunchShape& s) {
+  if (s.fork && !en->side) {
+    // created on first use; failures leave the shape unforked
+    if (cudaStreamCreateWithFlags(&en->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&en->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&en->join_ev, cudaEventDisableTiming) != cudaSuccess)
+      cudaGetLastError();
+  }
   en->shape = s;
+  if (s.fork && !(en->side && en->fork_ev && en->join_ev)) en->shape.fork = false;
   en->g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
   en->g.pf = s.tma ? 0 : s.pf;
   if (s.split || s.zsplit) en->gs = make_shell_geom(en, s.sh_block, s.sh_ichunk, s.zsplit);
@@ -989,13 +1006,23 @@ static cudaError_t launch_h(oems_engine* en) {
   }
   HArgs a = h_args(en);
   if (en->shape.zsplit) {
+    const bool fork = en->shape.fork && en->gs.work > 0;
+    cudaStream_t ss = fork ? en->side : en->stream;
+    if (fork) {
+      cudaEventRecord(en->fork_ev, en->stream);
+      cudaStreamWaitEvent(ss, en->fork_ev, 0);
+    }
     pick_h(en->id_bytes, false, en->storage, en->shape.occ)<<<en->shape.grid_h, en->shape.block, table_smem(en),
                                                               en->stream>>>(a);
     if (en->gs.work > 0) {
       HArgs b = a;
       b.g = en->gs;
       pick_h(en->id_bytes, true, en->storage, en->shape.sh_occ)<<<en->shape.grid_sh, en->shape.sh_block,
-                                                                 table_smem(en), en->stream>>>(b);
+                                                                 table_smem(en), ss>>>(b);
+    }
+    if (fork) {
+      cudaEventRecord(en->join_ev, ss);
+      cudaStreamWaitEvent(en->stream, en->join_ev, 0);
     }
     return cudaGetLastError();
   }
@@ -1016,13 +1043,23 @@ static cudaError_t launch_e(oems_engine* en) {
   }
   EArgs a = e_args(en);
   if (en->shape.zsplit) {
+    const bool fork = en->shape.fork && en->gs.work > 0;
+    cudaStream_t ss = fork ? en->side : en->stream;
+    if (fork) {
+      cudaEventRecord(en->fork_ev, en->stream);
+      cudaStreamWaitEvent(ss, en->fork_ev, 0);
+    }
     pick_e(en->id_bytes, false, en->storage, en->shape.occ)<<<en->shape.grid_e, en->shape.block, table_smem(en),
                                                               en->stream>>>(a);
     if (en->gs.work > 0) {
       EArgs b = a;
       b.g = en->gs;
       pick_e(en->id_bytes, true, en->storage, en->shape.sh_occ)<<<en->shape.grid_se, en->shape.sh_block,
-                                                                 table_smem(en), en->stream>>>(b);
+                                                                 table_smem(en), ss>>>(b);
+    }
+    if (fork) {
+      cudaEventRecord(en->join_ev, ss);
+      cudaStreamWaitEvent(en->stream, en->join_ev, 0);
     }
     return cudaGetLastError();
   }
@@ -1473,8 +1510,11 @@ static oems_status autotune(oems_engine* en) {
       if (s.smem == 0) s = LaunchShape{};
     }
     if (only_z) {
+      // the untuned z-split: the slab launch forked beside the interior one
       s.zsplit = true;
-      s.sh_ichunk = 4;
+      s.fork = true;
+      s.sh_block = 128;
+      s.sh_ichunk = 2;
     }
     if (!s.tma) {
       // small grids: shorter x-runs, then narrower CTAs, until every SM has
@@ -1538,17 +1578,22 @@ static oems_status autotune(oems_engine* en) {
           s.pf = pf;
           s.occ = occ;
           if (want_reg) cands.push_back(s);
-          if (want_z) {
+          if (want_z && b == 256 && pf == 0 && (c == 4 || c == 8)) {
             // the slab launch: its work items are short (8 layers) and its
             // z-slab parts uncoalesced, so it is latency-bound: short x-runs
-            // and narrow CTAs give it more items in flight
+            // and narrow CTAs give it more items in flight; forked, it runs
+            // beside the interior launch in the room a cut interior grid
+            // leaves
             s.zsplit = true;
-            for (int sb : {128, 256})
-              for (int sc : {1, 2, 4}) {
-                s.sh_block = sb;
-                s.sh_ichunk = sc;
-                cands.push_back(s);
-              }
+            for (int fk = 0; fk < 3; ++fk)
+              for (int sb : {128, 256})
+                for (int sc : {1, 2, 4}) {
+                  s.fork = fk > 0;
+                  s.cut = fk == 2 ? 1 : 0;
+                  s.sh_block = sb;
+                  s.sh_ichunk = sc;
+                  cands.push_back(s);
+                }
           }
         }
   if (want_tma) {
@@ -1610,7 +1655,7 @@ static oems_status autotune(oems_engine* en) {
     te.kind = shape_kind(s);
     te.threads = s.tma ? s.nconsumer + 32 : s.block;
     te.ichunk = s.ichunk;
-    te.extra = s.tma ? s.tg.NS : s.pf + 10 * s.occ + 100 * s.sh_occ;
+    te.extra = s.tma ? s.tg.NS : s.pf + 10 * s.occ + 100 * s.sh_occ + 1000 * (s.fork ? 1 + s.cut : 0);
     te.reps = reps;
     te.ms = ms;
     en->tune_report.push_back(te);
@@ -1748,6 +1793,12 @@ static void destroy(oems_engine* en) {
   pinned_put(en->h_energy, en->h_energy_cap * 2 * sizeof(double));
   if (en->ev0) cudaEventDestroy(en->ev0);
   if (en->ev1) cudaEventDestroy(en->ev1);
+  if (en->fork_ev) cudaEventDestroy(en->fork_ev);
+  if (en->join_ev) cudaEventDestroy(en->join_ev);
+  if (en->side) {
+    cudaStreamSynchronize(en->side);
+    cudaStreamDestroy(en->side);
+  }
   for (cudaEvent_t e : en->prof_ev)
     if (e) cudaEventDestroy(e);
   delete en;  // DevBuf members free on their stream

@@ -11,7 +11,7 @@ import pytest
 
 import openems_b200 as oe
 from conftest import rel_l2
-from scenarios import (config1_scenario, cpml_scenarios, mur_scenarios, odd_scenarios,
+from scenarios import (config1_scenario, cpml_scenarios, mur_scenarios, odd_scenarios, probe_scenario,
                        reference_scenarios, run_engine, run_oracle)
 
 pytestmark = pytest.mark.gpu
@@ -95,6 +95,19 @@ def test_small_grid_default_shape(sc):
     info = got["engine"].launch_info()
     assert info["ichunk"] < 8 or info["threads"] < 256, info
     assert_parity(got, run_oracle(sc))
+
+
+@pytest.mark.parametrize("sc", cpml_scenarios() + [probe_scenario()], ids=lambda s: s.name)
+def test_zsplit_forked_default_shape(sc):
+    """The untuned z-split forks its CPML slab launch onto a second stream
+    beside the plain interior launch (joined by events, inside the graphs
+    and in direct launches alike); the results stay bit-exact."""
+    got = run_engine(sc, autotune=False, kernels="zsplit")
+    assert got["engine"].launch_info()["staged"] == 3
+    ref = run_oracle(sc)
+    assert_parity(got, ref)
+    direct = run_engine(sc, autotune=False, kernels="zsplit", graphs=False)
+    assert np.array_equal(direct["fields"], got["fields"])
 
 
 def test_staged_kernels_are_used_when_requested():
