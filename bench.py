@@ -176,6 +176,9 @@ def run_device(oe, wl, args, torch, dist):
     dev_s, launches = 0.0, 0
     with ClockSampler(torch.cuda.current_device()) as clk:
         w0 = time.perf_counter()
+        # an NVTX range around the timed batches: `ncu --nvtx --nvtx-include
+        # bench_timed/` profiles exactly these launches (not the tuner's)
+        torch.cuda.nvtx.range_push("bench_timed")
         for _ in range(args.steps):
             eng.run_batch(batch_for(oe, wl, dt, t, T))
             n, s = eng.last_batch_stats()
@@ -183,6 +186,7 @@ def run_device(oe, wl, args, torch, dist):
             launches += n
             t += T
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         wall = time.perf_counter() - w0
     if dist is not None:
         dist.barrier()

@@ -814,21 +814,47 @@ __device__ __forceinline__ int pack_part(const int* off, int nparts, int w) {
   return lo;
 }
 
+// The arguments of the CTA's current part are staged in shared memory:
+// read through a reference into global memory, every field would be
+// re-read after each of the kernel's global stores (the compiler cannot
+// rule out aliasing), in the innermost loops.
+template <typename A>
+__device__ __forceinline__ void stage_args(A& dst, const A* src) {
+  static_assert(sizeof(A) % 4 == 0, "argument block of whole words");
+  __syncthreads();  // every thread is done with the previous part's arguments
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (int t = threadIdx.x; t < (int)(sizeof(A) / 4); t += blockDim.x) d[t] = __ldg(s + t);
+  __syncthreads();
+}
+
 template <bool kCpml, typename T = float>
 __global__ void __launch_bounds__(512) k_update_h_pack(const PackH p) {
+  __shared__ __align__(16) HArgs sa;
+  int cur = -1;
   const int total = __ldg(p.off + p.nparts);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
     const int q = pack_part(p.off, p.nparts, w);
-    h_item<0, kCpml, T>(p.args[q], nullptr, w - __ldg(p.off + q));
+    if (q != cur) {
+      stage_args(sa, p.args + q);
+      cur = q;
+    }
+    h_item<0, kCpml, T>(sa, nullptr, w - __ldg(p.off + q));
   }
 }
 
 template <bool kCpml, typename T = float>
 __global__ void __launch_bounds__(512) k_update_e_pack(const PackE p) {
+  __shared__ __align__(16) EArgs sa;
+  int cur = -1;
   const int total = __ldg(p.off + p.nparts);
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
     const int q = pack_part(p.off, p.nparts, w);
-    e_item<0, kCpml, T>(p.args[q], nullptr, w - __ldg(p.off + q));
+    if (q != cur) {
+      stage_args(sa, p.args + q);
+      cur = q;
+    }
+    e_item<0, kCpml, T>(sa, nullptr, w - __ldg(p.off + q));
   }
 }
 

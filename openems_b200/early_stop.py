@@ -50,12 +50,13 @@ def s11_db_mean_error(a: np.ndarray, b: np.ndarray, band: np.ndarray, floor: flo
 
 
 def pencil_s11(trace: np.ndarray, uf: np.ndarray, if_: np.ndarray, K: int, dt: float, freqs: np.ndarray,
-               horizon: int, lag: int = 0, R: float = 50.0, u_modes=None, **pencil) -> np.ndarray:
+               horizon: int, lag: int = 0, R: float = 50.0, u_modes=None, parts: bool = False,
+               **pencil) -> np.ndarray:
     """S11 predicted at K: the engine's DFTs of steps [0, K - lag) (those of
     [0, K) minus the last `lag` trace samples) plus the pencil continuation
     of the window that ends at K - lag.  trace: (>= K, 2) port u, i.
     u_modes: the port voltage's pencil modes of that window, if already
-    computed."""
+    computed.  parts=True returns (S11, head u, tail u, head i, tail i)."""
     uh, ih = uf.copy(), if_.copy()
     if lag:
         uh -= P.head_dft(trace[K - lag:K, 0], K - lag + 1, dt, freqs, 0.0)
@@ -63,6 +64,8 @@ def pencil_s11(trace: np.ndarray, uf: np.ndarray, if_: np.ndarray, K: int, dt: f
     ke = K - lag
     ut = P.pencil_tail_dft(trace[:ke, 0], ke, dt, freqs, 0.0, horizon, modes=u_modes, **pencil)
     it = P.pencil_tail_dft(trace[:ke, 1], ke, dt, freqs, 0.5, horizon, **pencil)
+    if parts:
+        return P.s11(uh + ut, ih + it, R), uh, ut, ih, it
     return P.s11(uh + ut, ih + it, R)
 
 
@@ -131,19 +134,26 @@ class StagePlan:
 def stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan: StagePlan) -> dict:
     """Everything known about an instance paused at stage K: the pencil
     prediction of S11 ("pred"), the residual check's largest and mean |dB|
-    difference over the band ("check_max", "check_mean"), the estimated
-    end step of the plain run ("end"), the port voltage's pencil mode count
-    ("modes"), the pencil window ("window") and the energy level below the
-    peak ("level", dB)."""
+    difference over the band ("check_max", "check_mean"), the same largest
+    difference against the prediction from a window 1024 steps earlier
+    ("check_far"), how far the prediction moves when its continuation is
+    scaled by 1.1 ("tail_sens", largest |dB| change over the band), the
+    estimated end step of the plain run ("end"), the port voltage's pencil
+    mode count ("modes"), the pencil window ("window") and the energy level
+    below the peak ("level", dB)."""
     pen = plan.pencil(K)
     um = P.pencil_modes(trace[:K, 0], K, dt, **pen)  # serves both the end estimate and the prediction
     end = plain_end(trace[:, 0], K, r["final_decay_db"], dt, decay_db, horizon, modes=um, **pen) \
         if plan.end_estimate else horizon
     end = max(end, K)
-    a = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, u_modes=um, **pen)
+    a, uh, ut, ih, it = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, 0, u_modes=um, parts=True, **pen)
     b = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, plan.lag, **pen)
+    far = min(4 * plan.lag, K // 2)
+    c = pencil_s11(trace, r["uf"], r["if"], K, dt, freqs, end, far, **pen)
     band = plan.band(freqs)
+    sens = s11_db_error(P.s11(uh + 1.1 * ut, ih + 1.1 * it), a, band)
     return {"pred": a, "check_max": s11_db_error(a, b, band), "check_mean": s11_db_mean_error(a, b, band),
+            "check_far": s11_db_error(a, c, band), "tail_sens": sens,
             "end": end, "modes": len(um[0]), "window": pen["window"], "level": float(r["final_decay_db"])}
 
 
@@ -152,8 +162,7 @@ def stage_features(trace, c: dict, K: int, horizon: int, plan: StagePlan):
     a stage_check record."""
     from . import stage_net as SN
     x = SN.window_input(trace, K, c["window"])
-    sc = SN.scalar_input(c["check_max"], c["check_mean"], c["level"], K, c["end"], horizon, c["modes"],
-                         plan.max_modes)
+    sc = SN.scalar_input(c["check_max"], c["check_mean"], c["check_far"], c["tail_sens"], c["level"], K, c["end"])
     return x, sc
 
 

@@ -14,8 +14,11 @@ makes the decision from more of what is known at K:
             channels, ReLU (receptive field 341 samples: the whole window),
             read at the last sample
     scalars the residual check (largest and mean |dB| difference over the
-            band), the energy level below the peak, log K, the continuation's
-            end step over K and over the step cap, the pencil's mode count
+            band, and the largest against the prediction from a window 1024
+            steps earlier), the prediction's sensitivity to its tail (its
+            largest |dB| change when the continuation is scaled by 1.1), the
+            energy level below the peak, log K, the continuation's end step
+            over K
     mlp     (128 + 8) -> 256 (ReLU) -> 8; output 0 is log10(error + 0.01),
             error = the largest |dB(S11_pred) - dB(S11_full)| over the band
 
@@ -62,12 +65,16 @@ def window_input(trace: np.ndarray, K: int, window: int) -> np.ndarray:
     return out
 
 
-def scalar_input(check_max: float, check_mean: float, level_db: float, K: int, end: int, horizon: int,
-                 modes: int, max_modes: int) -> np.ndarray:
-    """(N_SCALAR,) float32 of the pencil diagnostics at stage K."""
-    return np.array([np.log10(check_max + LOG_FLOOR), np.log10(check_mean + LOG_FLOOR), level_db / 50.0,
-                     np.log2(K / 1024.0) / 5.0, min(end / K, 32.0) / 8.0, end / max(horizon, 1), modes / max_modes,
-                     1.0], dtype=np.float32)
+def scalar_input(check_max: float, check_mean: float, check_far: float, tail_sens: float, level_db: float,
+                 K: int, end: int) -> np.ndarray:
+    """(N_SCALAR,) float32 of the pencil diagnostics at stage K: the
+    residual check (largest and mean |dB| over the band, and the largest
+    against a window 1024 steps earlier), the prediction's sensitivity to
+    its continuation (largest |dB| change when the tail is scaled by 1.1),
+    the energy level below the peak, log K and the estimated remaining run."""
+    lg = lambda v: np.log10(v + LOG_FLOOR)  # noqa: E731
+    return np.array([lg(check_max), lg(check_mean), lg(check_far), lg(tail_sens), level_db / 50.0,
+                     np.log2(K / 1024.0) / 5.0, min(end / K, 32.0) / 8.0, 1.0], dtype=np.float32)
 
 
 class CausalConv:
@@ -319,7 +326,11 @@ def tradeoff(score, err, stage_of, inst_of, stages, steps_full, budgets=(0, 0.01
     return out
 
 
-def _records(family, count, seed, plan, concurrency, log, t0):
+def records(family, count, seed, plan, concurrency, log, t0):
+    """Records of `count` instances of `family` (seed `seed`): the full runs
+    give each instance's reference S11 and step count ("steps_full"), then
+    early_stop.calibrate with features runs them through every stage of
+    `plan`.  log(msg) reports the elapsed time since perf_counter() t0."""
     import time
     from . import early_stop as ES
     insts, freqs = ES.family_instances(family, count, seed)
@@ -355,10 +366,10 @@ def learn(train_count: int = 1500, test_count: int = 400, family: str = "small",
     from . import early_stop as ES
     plan = ES.StagePlan.dense()
     t0 = time.perf_counter()
-    rtr = _records(family, train_count, train_seed, plan, concurrency, log, t0)
+    rtr = records(family, train_count, train_seed, plan, concurrency, log, t0)
     if extra_patch:
-        rtr = _concat(rtr, _records("patch", extra_patch, train_seed + 1, plan, concurrency, log, t0))
-    rte = _records(family, test_count, test_seed, plan, concurrency, log, t0)
+        rtr = _concat(rtr, records("patch", extra_patch, train_seed + 1, plan, concurrency, log, t0))
+    rte = records(family, test_count, test_seed, plan, concurrency, log, t0)
     x, sc, e, sg, it = rows(rtr)
     n_inst = len(rtr["steps_full"])
     rng = np.random.default_rng(cfg.seed + 7)

@@ -72,3 +72,32 @@ def test_stage_net_training_reduces_loss():
     losses = [SN.train_step(net, xs, ss, y.contiguous()) for _ in range(150)]
     N.check(N.lib().oems_tc_check(None))
     assert losses[-1] < 0.2 * losses[0], (losses[0], losses[-1])
+
+
+def test_committed_network_beats_residual_check_on_held_out_patches():
+    """Held-out small patch antennas (a seed no training run used), recorded
+    with the batched engine through every stage of the dense plan: at equal
+    violation budgets (no instance, and 1% and 2% of them, above 0.5 dB) the
+    committed network's first-accept rule stops the sweep earlier than the
+    residual check alone, and its deployed threshold keeps the worst
+    accepted error near the limit."""
+    import time
+    from openems_b200 import early_stop as ES
+    net = SN.load_default()
+    assert net is not None, "no committed network"
+    plan = ES.StagePlan.dense()
+    rec = SN.records("small", 240, 77, plan, 16, None, time.perf_counter())
+    x, s, e, sg, it = SN.rows(rec)
+    stages, sf = list(plan.stages), rec["steps_full"]
+    score_net = net.predict(x, s)
+    score_chk = np.log10(rec["check_db"][it, sg] + SN.LOG_FLOOR)
+    budgets = (0, 0.01, 0.02)
+    tn = SN.tradeoff(score_net, e, sg, it, stages, sf, budgets)
+    tc = SN.tradeoff(score_chk, e, sg, it, stages, sf, budgets)
+    print("network", [round(r["step_ratio"], 3) for r in tn], "residual check",
+          [round(r["step_ratio"], 3) for r in tc])
+    assert tn[0]["step_ratio"] > tc[0]["step_ratio"]
+    assert sum(r["step_ratio"] for r in tn) > sum(r["step_ratio"] for r in tc)
+    dep = SN.evaluate(score_net, net.threshold, e, sg, it, stages, sf)
+    print("deployed", dep)
+    assert dep["step_ratio"] > 1.0 and dep["over_limit"] <= 0.02 * len(sf)

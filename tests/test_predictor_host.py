@@ -278,6 +278,7 @@ def test_stage_inputs_window_and_scalars():
     assert not x[:, 2:].any()
     short = SN.window_input(trace, 300, 3072)
     assert not short[:SN.T_WIN - (300 + dec - 1) // dec, :2].any() and np.abs(short[-1, :2]).max() > 0
-    s = SN.scalar_input(0.2, 0.05, -23.0, 4096, 20000, 40000, 30, 150)
+    s = SN.scalar_input(0.2, 0.05, 0.4, 1.5, -23.0, 4096, 20000)
     assert s.shape == (SN.N_SCALAR,) and s[-1] == 1.0
-    assert s[0] == pytest.approx(np.log10(0.21)) and s[3] == pytest.approx(2.0 / 5.0)
+    assert s[0] == pytest.approx(np.log10(0.21)) and s[3] == pytest.approx(np.log10(1.51))
+    assert s[5] == pytest.approx(2.0 / 5.0)
