@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "../../include/oems.h"
@@ -52,6 +53,51 @@ oems_status err_word(int** out) {
 }
 
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+oems_status encode_fn(EncodeTiled* out) {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(f);
+  });
+  if (!fn) return pfail(OEMS_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  *out = fn;
+  return OEMS_OK;
+}
+
+// Tensor map of a row-major bf16 matrix [rows, k] with row pitch ld
+// elements: boxes of 64 K-elements (128 bytes, the swizzle span) x box_rows
+// rows, 128-byte swizzle, zero fill outside the matrix.
+oems_status bf16_map(EncodeTiled enc, CUtensorMap* m, const void* ptr, int ld, int k, int rows, int box_rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return pfail(OEMS_ERR_CUDA, "GEMM: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return OEMS_OK;
+}
+
+template <int BN>
+cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, const oems::GemmArgs& p, int grid, void* stream) {
+  const size_t smem = oems::GemmCfg<BN>::smem;
+  cudaError_t e = cudaFuncSetAttribute(oems::k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  oems::k_gemm_tc<BN><<<grid, 192, smem, S(stream)>>>(ta, tb, p);
+  return cudaGetLastError();
+}
 inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 inline int grid_for(long long n, int cap) { return std::max(1, std::min(blocks(n, 256), cap)); }
 
@@ -231,29 +277,43 @@ oems_status oems_tc_gemm_bf16(const void* a, int lda, const void* b, int ldb, fl
   oems_status st = err_word(&err);
   if (st != OEMS_OK) return st;
   oems::GemmArgs p{};
-  p.a = static_cast<const uint16_t*>(a);
-  p.b = static_cast<const uint16_t*>(b);
   p.c = c;
   p.bias = bias;
-  p.lda = lda;
-  p.ldb = ldb;
   p.ldc = ldc;
   p.M = M;
   p.N = N;
   p.K = K;
   p.beta = beta;
   p.err = err;
-  // the stage ring needs more than the default 48 KB of dynamic shared memory
-  if (N > 64) {
-    PK_CUDA(cudaFuncSetAttribute(oems::k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)oems::gemm_tc_smem<128>()));
-    const dim3 grid((N + 127) / 128, (M + 127) / 128);
-    oems::k_gemm_tc<128><<<grid, 128, oems::gemm_tc_smem<128>(), S(stream)>>>(p);
+  EncodeTiled enc = nullptr;
+  st = encode_fn(&enc);
+  if (st != OEMS_OK) return st;
+  int dev = 0, sms = 0;
+  PK_CUDA(cudaGetDevice(&dev));
+  PK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // tile width: one CTA per SM (the stage ring takes ~192 KB of shared
+  // memory), so the estimate is waves x a tile's cost, taken as its MMA
+  // columns plus a fixed 64 for loading A and draining the accumulator
+  const long long tm = (M + 127) / 128;
+  int BN = 64;
+  long long best = -1;
+  for (int cand : {256, 128, 64}) {
+    const long long waves = (tm * ((N + cand - 1) / cand) + sms - 1) / sms;
+    const long long cost = waves * (cand + 64);
+    if (best < 0 || cost < best) best = cost, BN = cand;
+  }
+  CUtensorMap ta, tb;
+  st = bf16_map(enc, &ta, a, lda, K, M, 128);
+  if (st == OEMS_OK) st = bf16_map(enc, &tb, b, ldb, K, N, BN);
+  if (st != OEMS_OK) return st;
+  const long long tiles = tm * ((N + BN - 1) / BN);
+  const int grid = (int)std::min<long long>(tiles, sms);
+  if (BN == 256) {
+    PK_CUDA(launch_gemm<256>(ta, tb, p, grid, stream));
+  } else if (BN == 128) {
+    PK_CUDA(launch_gemm<128>(ta, tb, p, grid, stream));
   } else {
-    PK_CUDA(cudaFuncSetAttribute(oems::k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)oems::gemm_tc_smem<64>()));
-    const dim3 grid((N + 63) / 64, (M + 127) / 128);
-    oems::k_gemm_tc<64><<<grid, 128, oems::gemm_tc_smem<64>(), S(stream)>>>(p);
+    PK_CUDA(launch_gemm<64>(ta, tb, p, grid, stream));
   }
   PK_CUDA(cudaGetLastError());
   return OEMS_OK;

@@ -23,18 +23,19 @@ makes the decision from more of what is known at K:
             error = the largest |dB(S11_pred) - dB(S11_full)| over the band
 
 An instance is accepted at the first stage whose predicted error is below a
-threshold chosen on the training family (the largest one that keeps every
-training instance within 0.5 dB).  Every product (forward, input and weight
+threshold chosen on held-back validation instances of the training family
+(the largest one that keeps every validation instance within 0.5 dB, judged
+on the network's out-of-sample predictions).  Every product (forward, input and weight
 gradients) is oems_tc_gemm_bf16 (tcgen05, bf16 operands, f32 accumulation);
 the causal convolutions are oems_pk_im2col_causal / col2im_causal, the rest
 oems_pk_* kernels; torch only holds device buffers.  The float64 restatement
 is oracle/tailnet_ref.StageNetRef (tests only).
 
-This replaces the network of the north-star sketch that maps the head of
-the traces to the tail's modal amplitudes directly: trained on 2,000 small
-patches that network ended up worse than plain truncation, while the
-pencil's continuation is accurate for most instances and fails for a few;
-telling those apart is what the learning is for here.
+The network of predictor_net.py maps the head of the traces to the tail's
+modal amplitudes directly; trained on 2,000 small patches it ended up worse
+than plain truncation, while the pencil's continuation is accurate for most
+instances and fails for a few.  Telling those apart is what the learning is
+for here.
 """
 from __future__ import annotations
 
