@@ -75,7 +75,7 @@ def parse():
                    help="field storage (arithmetic stays f32; f16 / bf16 run the register kernels)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--kernels", choices=("auto", "register", "staged", "zsplit"), default="auto")
+    p.add_argument("--kernels", choices=("auto", "register", "staged", "zsplit", "pipe"), default="auto")
     p.add_argument("--no-sweep", action="store_true",
                    help="skip the sweep half of the metric (staged vs plain S11 sweeps per hour)")
     return p.parse_args()
@@ -198,7 +198,7 @@ def run_device(oe, wl, args, torch, dist):
     info = eng.launch_info()
     tune = {}
     for r in eng.tune_report():  # fastest timed shape of each kernel family
-        k = ("register", "staged", "staged_split", "register_zsplit")[r["kind"]]
+        k = ("register", "staged", "staged_split", "register_zsplit", "register_pipe")[r["kind"]]
         per = r["ms"] / max(r["reps"], 1)
         if k not in tune or per < tune[k]["ms_per_step"]:
             tune[k] = {"ms_per_step": per, "threads": r["threads"], "ichunk": r["ichunk"], "extra": r["extra"]}

@@ -86,6 +86,12 @@ typedef struct oems_engine oems_engine;
                                               slabs, float4 chunks clear of the z
                                               slabs), CPML register kernels on
                                               every slab cell */
+#define OEMS_ENGINE_PIPE_KERNELS 0x400u    /* only the pipelined register kernels
+                                              (each thread's next x-planes copied
+                                              into shared memory by cp.async while
+                                              it computes), where they apply:
+                                              float fields, full coefficients,
+                                              nz <= 1024 */
 /* Field storage in 2 bytes per value, arithmetic still in float (no
  * counterpart in the reference, whose fields are f32): IEEE half or
  * bfloat16, rounded to nearest on every store.  H is kept multiplied by
@@ -535,22 +541,25 @@ OEMS_API oems_status oems_field_energy_noalloc(const float* const fields[6], uin
  * totals. */
 OEMS_API oems_status oems_engine_set_kernel_profiling(oems_engine* engine, int32_t enable);
 /* Launch shape chosen for the update kernels (valid after the first batch):
- * staged = 1 for the bulk-async staged kernels (2: staged on the box between
- * the x / y CPML slabs, register kernels on the slabs; 3: register kernels
- * with the z-only CPML path on that box and the full CPML path on the x / y
- * slabs), threads per CTA, x-planes per
- * work item, rows per tile (staged), pipeline stages (staged) or the L2
- * prefetch distance in x-planes (register kernels, 0 = none), CTAs. */
+ * staged = 0 for the register kernels, 1 for the bulk-async staged kernels
+ * (2: staged on the box between the x / y CPML slabs, register kernels on
+ * the slabs; 3: the z-split, plain register kernels on the CPML-free box and
+ * CPML register kernels on every slab cell; 4: the pipelined register
+ * kernels), threads per CTA, x-planes per work item, rows per tile (staged),
+ * pipeline stages (staged, pipelined) or the L2 prefetch distance in
+ * x-planes (register kernels, 0 = none), CTAs. */
 OEMS_API oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged,
                                              int32_t* threads, int32_t* ichunk,
                                              int32_t* rows_per_tile, int32_t* stages,
                                              int32_t* grid);
 /* One launch shape the autotuner timed: kind as `staged` above, threads per
- * CTA, x-planes per work item, pipeline stages (staged) or, for the register
- * kernels, the L2 prefetch distance + 10 x the register budget variant + 100
- * x that of the CPML slab kernels of a z-split (0: up to 128 registers with
- * 512-thread CTAs, 1 / 2: 256-thread CTAs capped at 85 / 64 registers), the
- * number of H + E pairs timed and their device time in milliseconds. */
+ * CTA, x-planes per work item, pipeline stages (staged, pipelined) or, for
+ * the register kernels, the L2 prefetch distance + 10 x the register budget
+ * variant + 100 x that of the CPML slab kernels of a z-split (0: up to 128
+ * registers with 512-thread CTAs, 1 / 2: 256-thread CTAs capped at 85 / 64
+ * registers) + 1000 for a forked z-split slab launch (2000 with the interior
+ * grid cut by one CTA per SM), the number of H + E pairs timed and their
+ * device time in milliseconds. */
 typedef struct oems_tune_entry {
   int32_t kind;
   int32_t threads;

@@ -29,6 +29,7 @@ ENGINE_SPLIT_KERNELS = 0x40
 ENGINE_FIELDS_F16 = 0x80
 ENGINE_FIELDS_BF16 = 0x100
 ENGINE_ZSPLIT_KERNELS = 0x200
+ENGINE_PIPE_KERNELS = 0x400
 H_STORAGE_SCALE = 512.0
 STORAGE_FLAGS = {"f32": 0, "f16": ENGINE_FIELDS_F16, "bf16": ENGINE_FIELDS_BF16}
 

@@ -32,6 +32,7 @@
 
 #include "../../include/oems.h"
 #include "yee_kernels.cuh"
+#include "yee_pipe.cuh"
 #include "yee_tma.cuh"
 #include "mur.cuh"
 #include "lumped_ade.cuh"
@@ -325,6 +326,10 @@ struct LaunchShape {
   int grid_h = 0;
   int grid_e = 0;
   bool tma = false;
+  // pipe: the pipelined register kernels (yee_pipe.cuh), 256 threads, one
+  // CTA per SM, pipe_ns shared-memory stages
+  bool pipe = false;
+  int pipe_ns = 4;
   int nconsumer = 256;
   TmaGeom tg{};
   size_t smem = 0;
@@ -844,6 +849,27 @@ static EKernel pick_e(int id_bytes, bool cpml, int storage = 0, int occ = 0) {
   return pick_e_t<float>(id_bytes, cpml);
 }
 
+static HKernel pick_h_pipe(bool cpml, int ns) {
+  if (ns >= 4) return cpml ? k_update_h_pipe<true, 4> : k_update_h_pipe<false, 4>;
+  return cpml ? k_update_h_pipe<true, 3> : k_update_h_pipe<false, 3>;
+}
+static EKernel pick_e_pipe(bool cpml, int ns) {
+  if (ns >= 4) return cpml ? k_update_e_pipe<true, 4> : k_update_e_pipe<false, 4>;
+  return cpml ? k_update_e_pipe<true, 3> : k_update_e_pipe<false, 3>;
+}
+
+// Stage count of the pipelined kernels for this grid (4, 3) or 0 where they
+// do not apply: float fields, full coefficient arrays, a halo row of at most
+// one CTA's chunks, and the stages within the opt-in shared memory.
+static int pipe_stages(const oems_engine* en, size_t optin) {
+  if (en->id_bytes != 0 || en->storage != 0) return 0;
+  const int nzq = (en->nz + 3) / 4;
+  if (nzq > kPipeThreads) return 0;
+  for (int ns : {4, 3})
+    if (pipe_smem_bytes(ns, nzq) <= optin) return ns;
+  return 0;
+}
+
 static size_t table_smem(const oems_engine* en) {
   return en->id_bytes == 1 ? (size_t)en->ntable * 12 * sizeof(float) : 0;
 }
@@ -917,6 +943,31 @@ static oems_status prepare_tma_kernels(size_t smem) {
 static oems_status size_grid(oems_engine* en, LaunchShape& s) {
   int sms = 0;
   OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, en->device));
+  if (s.pipe) {
+    const int nzq = (en->nz + 3) / 4;
+    const size_t smem = pipe_smem_bytes(s.pipe_ns, nzq);
+    const bool cp = en->cpml.on;
+    // the attribute is per function and shared by every engine: allow up to
+    // the opt-in limit, so a grid with wider rows never shrinks it under
+    // another engine's launches
+    size_t limit = 0;
+    OEMS_TRY(tma_smem_limit(en, &limit));
+    OEMS_CUDA(cudaFuncSetAttribute((const void*)pick_h_pipe(cp, s.pipe_ns),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
+    OEMS_CUDA(cudaFuncSetAttribute((const void*)pick_e_pipe(cp, s.pipe_ns),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
+    int oh = 0, oe = 0;
+    OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oh, (const void*)pick_h_pipe(cp, s.pipe_ns),
+                                                            kPipeThreads, smem));
+    OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oe, (const void*)pick_e_pipe(cp, s.pipe_ns),
+                                                            kPipeThreads, smem));
+    s.block = kPipeThreads;
+    s.smem = smem;
+    const Geom g = make_geom(en, kPipeThreads, s.ichunk);
+    s.grid_h = std::max(1, std::min(g.work, std::max(1, oh) * sms));
+    s.grid_e = std::max(1, std::min(g.work, std::max(1, oe) * sms));
+    return OEMS_OK;
+  }
   if (s.tma) {
     // allow any stage count up to the opt-in limit (the attribute is per
     // function, shared by every engine and tuning candidate)
@@ -972,7 +1023,7 @@ static void apply_shape(oems_engine* en, const LaunchShape& s) {
   en->shape = s;
   if (s.fork && !(en->side && en->fork_ev && en->join_ev)) en->shape.fork = false;
   en->g = s.zsplit ? make_interior_geom(en, s.block, s.ichunk) : make_geom(en, s.block, s.ichunk);
-  en->g.pf = s.tma ? 0 : s.pf;
+  en->g.pf = (s.tma || s.pipe) ? 0 : s.pf;
   if (s.split || s.zsplit) en->gs = make_shell_geom(en, s.sh_block, s.sh_ichunk, s.zsplit);
   en->graph_epoch++;
 }
@@ -994,6 +1045,11 @@ static TmaArgs tma_args(oems_engine* en, bool is_h) {
 }
 
 static cudaError_t launch_h(oems_engine* en) {
+  if (en->shape.pipe) {
+    HArgs a = h_args(en);
+    pick_h_pipe(en->cpml.on, en->shape.pipe_ns)<<<en->shape.grid_h, kPipeThreads, en->shape.smem, en->stream>>>(a);
+    return cudaGetLastError();
+  }
   if (en->shape.tma) {
     TmaArgs a = tma_args(en, true);
     k_update_tma<true><<<en->shape.grid_h, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
@@ -1031,6 +1087,11 @@ static cudaError_t launch_h(oems_engine* en) {
   return cudaGetLastError();
 }
 static cudaError_t launch_e(oems_engine* en) {
+  if (en->shape.pipe) {
+    EArgs a = e_args(en);
+    pick_e_pipe(en->cpml.on, en->shape.pipe_ns)<<<en->shape.grid_e, kPipeThreads, en->shape.smem, en->stream>>>(a);
+    return cudaGetLastError();
+  }
   if (en->shape.tma) {
     TmaArgs a = tma_args(en, false);
     k_update_tma<false><<<en->shape.grid_e, en->shape.nconsumer + 32, en->shape.smem, en->stream>>>(a);
@@ -1465,7 +1526,7 @@ static std::map<TuneKey, TuneResult>& tune_cache() {
   return m;
 }
 
-static int shape_kind(const LaunchShape& s) { return s.split ? 2 : s.tma ? 1 : s.zsplit ? 3 : 0; }
+static int shape_kind(const LaunchShape& s) { return s.pipe ? 4 : s.split ? 2 : s.tma ? 1 : s.zsplit ? 3 : 0; }
 // engines may be driven from several host threads (one engine per thread)
 static std::mutex& tune_mutex() {
   static std::mutex m;
@@ -1480,10 +1541,19 @@ static oems_status autotune(oems_engine* en) {
   const bool can_split = en->id_bytes == 0 && en->storage == 0 && cpml_interior(en, &ilo, &ihi, &jlo, &jhi);
   const bool only_split = (en->flags & OEMS_ENGINE_SPLIT_KERNELS) && can_split;
   const bool only_z = (en->flags & OEMS_ENGINE_ZSPLIT_KERNELS) && !only_split && can_zsplit(en);
+  size_t optin = 0;
+  OEMS_TRY(tma_smem_limit(en, &optin));
+  const int pipe_ns = pipe_stages(en, optin);
+  const bool only_pipe = (en->flags & OEMS_ENGINE_PIPE_KERNELS) && !only_split && !only_z && pipe_ns > 0;
   const bool want_reg = (!(en->flags & OEMS_ENGINE_STAGED_KERNELS) || en->id_bytes != 0) && !only_split &&
-                        !only_z;
+                        !only_z && !only_pipe;
   const bool want_tma = !(en->flags & OEMS_ENGINE_REGISTER_KERNELS) && en->id_bytes == 0 && !only_split &&
-                        !only_z && en->storage == 0;
+                        !only_z && !only_pipe && en->storage == 0;
+  // the pipelined kernels are timed only on request: at 256^3 with CPML they
+  // measured 0.65 ms per step against 0.38 for the register kernels (one
+  // CTA of 8 warps per SM, 204 registers, 1.5x the instructions per plane:
+  // issue-bound at 34% issue activity)
+  const bool want_pipe = only_pipe;
   // split shapes are tried only on request: at 256^3 with 8-layer CPML the
   // staged interior plus register slabs measured 36.8 GCells/s against 45.6
   // for the register kernels on the whole grid (the z-slab lanes of every
@@ -1516,6 +1586,12 @@ static oems_status autotune(oems_engine* en) {
       s.sh_block = 128;
       s.sh_ichunk = 2;
     }
+    if (only_pipe) {
+      s.pipe = true;
+      s.pipe_ns = pipe_ns;
+      s.block = kPipeThreads;
+      s.ichunk = 16;
+    }
     if (!s.tma) {
       // small grids: shorter x-runs, then narrower CTAs, until every SM has
       // a work item (a 70^3 grid has 45 items at 256 x 8: most SMs would idle)
@@ -1537,7 +1613,7 @@ static oems_status autotune(oems_engine* en) {
   const bool want_z = (want_reg || only_z) && can_zsplit(en);
   const TuneKey key{en->device, en->nx, en->ny, en->nz, en->id_bytes,
                     (en->cpml.on ? 1 : 0) | (want_reg ? 2 : 0) | (want_tma ? 4 : 0) | (want_split ? 8 : 0) |
-                        (want_z ? 16 : 0) | (en->storage << 5)};
+                        (want_z ? 16 : 0) | (want_pipe ? 32 : 0) | (en->storage << 6)};
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
     auto hit = tune_cache().find(key);
@@ -1596,6 +1672,20 @@ static oems_status autotune(oems_engine* en) {
                 }
           }
         }
+  if (want_pipe) {
+    // pipelined register kernels: x-runs of 4-32 planes, both stage counts
+    // that fit (3 stages keep one bundle in flight, 4 two)
+    for (int c : {4, 8, 16, 32})
+      for (int ns = pipe_ns; ns >= 3; --ns) {
+        if (c > 2 * en->nx && c != 4) continue;
+        LaunchShape s;
+        s.pipe = true;
+        s.pipe_ns = ns;
+        s.block = kPipeThreads;
+        s.ichunk = c;
+        cands.push_back(s);
+      }
+  }
   if (want_tma) {
     size_t limit = 0;
     OEMS_TRY(tma_smem_limit(en, &limit));
@@ -1655,7 +1745,8 @@ static oems_status autotune(oems_engine* en) {
     te.kind = shape_kind(s);
     te.threads = s.tma ? s.nconsumer + 32 : s.block;
     te.ichunk = s.ichunk;
-    te.extra = s.tma ? s.tg.NS : s.pf + 10 * s.occ + 100 * s.sh_occ + 1000 * (s.fork ? 1 + s.cut : 0);
+    te.extra = s.tma ? s.tg.NS
+                     : s.pipe ? s.pipe_ns : s.pf + 10 * s.occ + 100 * s.sh_occ + 1000 * (s.fork ? 1 + s.cut : 0);
     te.reps = reps;
     te.ms = ms;
     en->tune_report.push_back(te);
@@ -3357,11 +3448,11 @@ oems_status oems_engine_launch_info(const oems_engine* engine, int32_t* staged, 
                                     int32_t* rows_per_tile, int32_t* stages, int32_t* grid) {
   if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
   const LaunchShape& s = engine->shape;
-  if (staged) *staged = s.split ? 2 : s.tma ? 1 : s.zsplit ? 3 : 0;
+  if (staged) *staged = shape_kind(s);
   if (threads) *threads = s.tma ? s.nconsumer + 32 : s.block;
   if (ichunk) *ichunk = s.ichunk;
   if (rows_per_tile) *rows_per_tile = s.tma ? s.tg.TJ : 0;
-  if (stages) *stages = s.tma ? s.tg.NS : s.pf;
+  if (stages) *stages = s.tma ? s.tg.NS : s.pipe ? s.pipe_ns : s.pf;
   if (grid) *grid = s.grid_h;
   return OEMS_OK;
 }

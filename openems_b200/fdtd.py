@@ -933,7 +933,9 @@ class Engine:
         """kernels: "auto" (tuner picks), "register", "staged" (bulk-async),
         "split" (staged between the x / y CPML slabs, register on them) or
         "zsplit" (plain register kernels on the CPML-free box, CPML register
-        kernels on every slab cell).
+        kernels on every slab cell) or "pipe" (pipelined register kernels:
+        each thread's next x-planes copied into shared memory while it
+        computes; float fields and full coefficients only).
         storage: field storage "f32", or "f16" / "bf16" (2 bytes per value,
         float arithmetic; register kernels, CPML, sources, probes, energies)."""
         if engine_type is not EngineType.Cuda:
@@ -943,7 +945,8 @@ class Engine:
         flags = (N.ENGINE_COMPRESSED if compressed else 0) | (0 if autotune else N.ENGINE_NO_AUTOTUNE) \
             | (0 if graphs else N.ENGINE_NO_GRAPHS) \
             | {"auto": 0, "register": N.ENGINE_REGISTER_KERNELS, "staged": N.ENGINE_STAGED_KERNELS,
-               "split": N.ENGINE_SPLIT_KERNELS, "zsplit": N.ENGINE_ZSPLIT_KERNELS}[kernels] \
+               "split": N.ENGINE_SPLIT_KERNELS, "zsplit": N.ENGINE_ZSPLIT_KERNELS,
+               "pipe": N.ENGINE_PIPE_KERNELS}[kernels] \
             | N.STORAGE_FLAGS[storage]
         desc = N.OperatorDesc()
         N.check(N.lib().oems_operator_engine_desc(operator.handle, device, flags, ctypes.byref(desc)))

@@ -16,8 +16,8 @@ bit-identical (port DFTs within 1e-12: their twiddles come from the device's
 sincos), so the stated gate (relative L2 <= 1e-5 per field array and probe
 trace after the stated step count) holds with margin; the test asserts both
 and prints the relative L2 of each array.  The kernel families: the shape
-the autotuner picks, the z-split (plain kernels on the CPML-free box) and
-the bulk-async staged kernels.
+the autotuner picks, the z-split (plain kernels on the CPML-free box), the
+pipelined register kernels and the bulk-async staged kernels.
 """
 import os
 
@@ -57,7 +57,7 @@ def config2_oracle():
     return run_oracle(config2_scenario(), precision=32, threads=THREADS, zline=True)
 
 
-@pytest.mark.parametrize("kernels", ("auto", "zsplit", "staged"))
+@pytest.mark.parametrize("kernels", ("auto", "zsplit", "staged", "pipe"))
 def test_config2_cpml_boxes_256_10000_steps(config2_oracle, kernels):
     got = run_engine(config2_scenario(), kernels=kernels)
     report(f"config 2 ({kernels}, shape {got['engine'].launch_info()})", got, config2_oracle)

@@ -60,7 +60,7 @@ def test_config1_64_pec_2000_steps(kernels):
     assert rel_l2(got["fields"][3:], ref64["fields"][3:]) < 1e-4
 
 
-KERNELS = ("register", "staged", "split", "zsplit")
+KERNELS = ("register", "staged", "split", "zsplit", "pipe")
 
 
 @pytest.mark.parametrize("kernels", KERNELS)
