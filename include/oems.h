@@ -360,9 +360,12 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
  * engine i for every i with batches[i] != NULL, with the results and state
  * oems_engine_run_batch would give each engine on its own (bit for bit),
  * but every half-step of all of them is one launch of the plain update
- * kernels over their CPML-free boxes and one of the CPML kernels over their
- * slab cells, replayed from CUDA graphs, with one post-step launch and one
- * energy launch pair for all.  The batches must share num_steps,
+ * kernels over the grids without CPML and one of the CPML kernels over the
+ * grids with it, replayed from CUDA graphs, with one post-step launch and
+ * one energy launch pair for all.  The first batch times the update
+ * kernels' CTA size, x-planes per work item and whether CPML grids enter
+ * whole or split (below) on saved copies of the engines' state (restored
+ * afterwards) and keeps the fastest, unless oems_pack_set_shape chose one.  The batches must share num_steps,
  * sample_interval, check_interval and whether they carry an energy-decay end
  * condition, and their engines must be at the same timestep; each engine
  * keeps its own decay threshold, peak and termination step.  statuses[i] is
@@ -374,6 +377,17 @@ OEMS_API oems_status oems_pack_create(oems_engine* const* engines, uint64_t coun
 OEMS_API void oems_pack_destroy(oems_pack* pack);
 OEMS_API oems_status oems_pack_run_batch(oems_pack* pack, const oems_batch* const* batches,
                                          oems_batch_result* results, oems_status* statuses);
+/* The update kernels' launch shape: CTAs of `threads` (a multiple of 32, at
+ * most 512) over work items of `ichunk` x-planes, and `split`: 0 gives each
+ * CPML grid to the CPML launch whole; 1 as two parts, its CPML-free box
+ * (plain kernels) and its slab cells (CPML kernels); 2 and 3 as 1 with the
+ * CPML launch on a second stream beside the plain one (3: the plain
+ * launch's grid cut by one CTA per SM to leave room for it).  Setting it
+ * skips the tuning of the first batch. */
+OEMS_API oems_status oems_pack_set_shape(oems_pack* pack, int32_t threads, int32_t ichunk,
+                                         int32_t split);
+OEMS_API oems_status oems_pack_shape(const oems_pack* pack, int32_t* threads, int32_t* ichunk,
+                                     int32_t* split);
 
 /* ---- checkpoint / resume --------------------------------------------------
  * The engine's evolving state as sections: the buffers oems_engine_reset

@@ -25,6 +25,10 @@ OEMS_API oems_status oems_tc_gemm_bf16(const void* a, int lda, const void* b, in
 /* Synchronises the stream and reports (then clears) a GEMM whose bounded
  * wait for its MMAs gave up: OEMS_ERR_TIMEOUT. */
 OEMS_API oems_status oems_tc_check(void* stream);
+/* Launches one CTA whose bounded mbarrier wait (the GEMM's own, about one
+ * second) runs out on a barrier nothing arrives at; the next oems_tc_check
+ * on the stream reports OEMS_ERR_TIMEOUT.  For tests of the timeout path. */
+OEMS_API oems_status oems_tc_wait_probe(void* stream);
 OEMS_API oems_status oems_pk_f32_to_bf16(const float* x, void* y, int64_t n, void* stream);
 /* y[c * ldy + r] = x[r * ldx + c], r < R, c < C (bf16). */
 OEMS_API oems_status oems_pk_transpose_bf16(const void* x, int ldx, void* y, int ldy, int R, int C, void* stream);

@@ -294,11 +294,14 @@ SIGNATURES = {
     "oems_pack_create": (c_i32, [ctypes.POINTER(P), c_u64, ctypes.POINTER(P)]),
     "oems_pack_destroy": (None, [P]),
     "oems_pack_run_batch": (c_i32, [P, ctypes.POINTER(ctypes.c_void_p), P, ctypes.POINTER(c_i32)]),
+    "oems_pack_set_shape": (c_i32, [P, c_i32, c_i32, c_i32]),
+    "oems_pack_shape": (c_i32, [P, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)]),
     "oems_sweep_run_until": (c_i32, [P, c_u64, c_u64]),
     "oems_sweep_finish": (c_i32, [P, c_i32]),
     "oems_sweep_advance": (c_i32, [P, c_i32, c_u64, c_u64]),
     "oems_tc_gemm_bf16": (c_i32, [P, c_i32, P, c_i32, P, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, P, P]),
     "oems_tc_check": (c_i32, [P]),
+    "oems_tc_wait_probe": (c_i32, [P]),
     "oems_pk_f32_to_bf16": (c_i32, [P, P, c_i64, P]),
     "oems_pk_transpose_bf16": (c_i32, [P, c_i32, P, c_i32, c_i32, c_i32, P]),
     "oems_pk_im2col": (c_i32, [P, P, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, P]),

@@ -3562,6 +3562,21 @@ struct oems_pack {
   double* h_energy = nullptr;     // pinned mirror
   size_t h_energy_cap = 0;
   std::map<int, cudaGraphExec_t> graphs;
+  // launch shape of the update kernels: CTA size and x-planes per work item,
+  // chosen by pack_tune on the first batch unless set explicitly
+  int threads = 256, ichunk = 8;
+  // split: a CPML grid enters as two parts, its CPML-free box (plain
+  // kernels) and its slab cells (CPML kernels), as the engine's z-split
+  bool split = false;
+  // fork (split only): each half-step's CPML launch runs on a second stream
+  // beside the plain one, whose grid is cut by `cut` CTAs per SM to leave
+  // room for it (the bandwidth-bound interiors overlap the latency-bound
+  // slabs)
+  bool fork = false;
+  int cut = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  bool tuned = false;
 };
 
 namespace oems {
@@ -3571,20 +3586,19 @@ static void pack_drop_graphs(oems_pack* p) {
   p->graphs.clear();
 }
 
-constexpr int kPackThreads = 256;
-constexpr int kPackIchunk = 8;
 
 template <typename T>
 static oems_status pack_grids(oems_pack* p) {
   int sms = 0, o = 0;
   OEMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
-  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<false, T>, kPackThreads, 0));
-  p->grid_hp = std::max(1, o) * sms;
-  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<true, T>, kPackThreads, 0));
+  const int cut = p->fork ? p->cut : 0;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<false, T>, p->threads, 0));
+  p->grid_hp = std::max(1, o - cut) * sms;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_h_pack<true, T>, p->threads, 0));
   p->grid_hc = std::max(1, o) * sms;
-  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<false, T>, kPackThreads, 0));
-  p->grid_ep = std::max(1, o) * sms;
-  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<true, T>, kPackThreads, 0));
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<false, T>, p->threads, 0));
+  p->grid_ep = std::max(1, o - cut) * sms;
+  OEMS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, (const void*)k_update_e_pack<true, T>, p->threads, 0));
   p->grid_ec = std::max(1, o) * sms;
   return OEMS_OK;
 }
@@ -3617,10 +3631,15 @@ static oems_status pack_layout(oems_pack* p, const std::vector<int>& active) {
         op.push_back(op.back() + g.work);
       }
     };
-    // the whole grid as one part: a sweep's grids are small, so most of
-    // their cells lie in the CPML slabs, where a z-split's slab launch is
-    // the slow one (measured: 23 GCells/s split against 34 with whole grids)
-    add(make_geom(en, kPackThreads, kPackIchunk), en->cpml.on);
+    // a CPML grid as one part, or (split) as its CPML-free box for the
+    // plain kernels plus its slab cells for the CPML kernels; the tuner
+    // times both
+    if (p->split && can_zsplit(en)) {
+      add(make_interior_geom(en, p->threads, p->ichunk), false);
+      add(make_shell_geom(en, p->threads, p->ichunk, true), true);
+    } else {
+      add(make_geom(en, p->threads, p->ichunk), en->cpml.on);
+    }
     PostArgs q{};
     for (int c = 0; c < 3; ++c) {
       q.e[c] = en->E(c);
@@ -3681,26 +3700,127 @@ static oems_status pack_layout(oems_pack* p, const std::vector<int>& active) {
 }
 
 template <typename T>
-static cudaError_t pack_launch_steps(oems_pack* p, int steps) {
+static cudaError_t pack_launch_steps(oems_pack* p, int steps, bool post = true) {
   const int na = (int)p->active.size();
   const PackH hp{p->n_plain, p->off.p, p->h_args.p};
   const PackH hc{p->n_cpml, p->off.p + p->n_plain + 1, p->h_args.p + p->n_plain};
   const PackE ep{p->n_plain, p->off.p, p->e_args.p};
   const PackE ec{p->n_cpml, p->off.p + p->n_plain + 1, p->e_args.p + p->n_plain};
+  const bool fork = p->fork && p->side && p->n_plain && p->n_cpml;
+  cudaStream_t cs = fork ? p->side : p->stream;
   for (int s = 0; s < steps; ++s) {
-    if (p->n_plain) k_update_h_pack<false, T><<<p->grid_hp, kPackThreads, 0, p->stream>>>(hp);
-    if (p->n_cpml) k_update_h_pack<true, T><<<p->grid_hc, kPackThreads, 0, p->stream>>>(hc);
-    if (p->n_plain) k_update_e_pack<false, T><<<p->grid_ep, kPackThreads, 0, p->stream>>>(ep);
-    if (p->n_cpml) k_update_e_pack<true, T><<<p->grid_ec, kPackThreads, 0, p->stream>>>(ec);
-    k_post_step_pack<T><<<na, 128, 0, p->stream>>>(p->post.p, p->d_base.p, s);
+    if (fork) {
+      cudaEventRecord(p->fork_ev, p->stream);
+      cudaStreamWaitEvent(cs, p->fork_ev, 0);
+    }
+    if (p->n_plain) k_update_h_pack<false, T><<<p->grid_hp, p->threads, 0, p->stream>>>(hp);
+    if (p->n_cpml) k_update_h_pack<true, T><<<p->grid_hc, p->threads, 0, cs>>>(hc);
+    if (fork) {
+      cudaEventRecord(p->join_ev, cs);
+      cudaStreamWaitEvent(p->stream, p->join_ev, 0);
+      cudaEventRecord(p->fork_ev, p->stream);
+      cudaStreamWaitEvent(cs, p->fork_ev, 0);
+    }
+    if (p->n_plain) k_update_e_pack<false, T><<<p->grid_ep, p->threads, 0, p->stream>>>(ep);
+    if (p->n_cpml) k_update_e_pack<true, T><<<p->grid_ec, p->threads, 0, cs>>>(ec);
+    if (fork) {
+      cudaEventRecord(p->join_ev, cs);
+      cudaStreamWaitEvent(p->stream, p->join_ev, 0);
+    }
+    if (post) k_post_step_pack<T><<<na, 128, 0, p->stream>>>(p->post.p, p->d_base.p, s);
   }
   return cudaGetLastError();
 }
 
-static cudaError_t pack_launch_steps_any(oems_pack* p, int steps) {
-  if (p->storage == 1) return pack_launch_steps<__half>(p, steps);
-  if (p->storage == 2) return pack_launch_steps<__nv_bfloat16>(p, steps);
-  return pack_launch_steps<float>(p, steps);
+static cudaError_t pack_launch_steps_any(oems_pack* p, int steps, bool post = true) {
+  if (p->storage == 1) return pack_launch_steps<__half>(p, steps, post);
+  if (p->storage == 2) return pack_launch_steps<__nv_bfloat16>(p, steps, post);
+  return pack_launch_steps<float>(p, steps, post);
+}
+
+static oems_status pack_grids_any(oems_pack* p) {
+  if (p->storage == 1) return pack_grids<__half>(p);
+  if (p->storage == 2) return pack_grids<__nv_bfloat16>(p);
+  return pack_grids<float>(p);
+}
+
+// Times the update kernels of the active engines at each candidate shape
+// (CTA size x x-planes per work item) on saved copies of their fields and
+// CPML psi, restores the state and keeps the fastest.  Sweeps pack small
+// grids, most of whose cells lie in the CPML slabs, so the single-grid
+// tuner's choice does not carry over.
+static oems_status pack_tune(oems_pack* p) {
+  p->tuned = true;
+  const std::vector<int> act = p->active;
+  if (act.empty()) return OEMS_OK;
+  std::vector<void*> saved(act.size(), nullptr);
+  long long cells = 0;
+  oems_status st = OEMS_OK;
+  for (size_t k = 0; k < act.size() && st == OEMS_OK; ++k) {
+    oems_engine* en = p->en[act[k]];
+    const size_t fb = en->field_bytes(), pb = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
+    cells += (long long)en->nx * en->ny * en->nz;
+    if (pool_alloc(&saved[k], fb + pb, p->stream) != cudaSuccess ||
+        cudaMemcpyAsync(saved[k], en->fields, fb, cudaMemcpyDeviceToDevice, p->stream) != cudaSuccess ||
+        (pb && cudaMemcpyAsync((char*)saved[k] + fb, en->cpml.psi.p, pb, cudaMemcpyDeviceToDevice, p->stream) !=
+                   cudaSuccess))
+      st = fail(OEMS_ERR_CUDA, "pack tuning: saving the state failed");
+  }
+  const int reps = (int)std::max<long long>(4, std::min<long long>(20, 400000000LL / std::max(1LL, cells)));
+  int best_t = p->threads, best_c = p->ichunk, best_cut = p->cut;
+  bool best_split = p->split, best_fork = p->fork;
+  float best_ms = 1e30f;
+  // modes: 0 whole grids, 1 split, 2 / 3 split with the CPML launch forked
+  // beside the plain one (interior grid cut by 0 / 1 CTA per SM)
+  for (int mode = 0; mode < (p->side ? 4 : 2); ++mode)
+  for (int t : {128, 256, 512})
+    for (int c : {2, 4, 8, 16}) {
+      if (st != OEMS_OK) break;
+      if (mode >= 2 && (t == 512 || c == 16)) continue;
+      p->split = mode >= 1;
+      p->fork = mode >= 2;
+      p->cut = mode == 3 ? 1 : 0;
+      p->threads = t;
+      p->ichunk = c;
+      if ((st = pack_grids_any(p)) != OEMS_OK || (st = pack_layout(p, act)) != OEMS_OK) break;
+      cudaError_t e = pack_launch_steps_any(p, 1, false);
+      if (e == cudaSuccess) e = cudaEventRecord(p->ev0, p->stream);
+      if (e == cudaSuccess) e = pack_launch_steps_any(p, reps, false);
+      if (e == cudaSuccess) e = cudaEventRecord(p->ev1, p->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(p->ev1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+      if (e != cudaSuccess) {
+        st = fail(OEMS_ERR_CUDA, std::string("pack tuning: ") + cudaGetErrorString(e));
+        break;
+      }
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_t = t;
+        best_c = c;
+        best_split = p->split;
+        best_fork = p->fork;
+        best_cut = p->cut;
+      }
+    }
+  for (size_t k = 0; k < act.size(); ++k) {
+    if (!saved[k]) continue;
+    oems_engine* en = p->en[act[k]];
+    const size_t fb = en->field_bytes(), pb = en->cpml.on ? en->cpml.psi.n * sizeof(float) : 0;
+    cudaMemcpyAsync(en->fields, saved[k], fb, cudaMemcpyDeviceToDevice, p->stream);
+    if (pb) cudaMemcpyAsync(en->cpml.psi.p, (char*)saved[k] + fb, pb, cudaMemcpyDeviceToDevice, p->stream);
+    cudaFreeAsync(saved[k], p->stream);
+  }
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess && st == OEMS_OK)
+    st = fail(OEMS_ERR_CUDA, "pack tuning: restoring the state failed");
+  if (st != OEMS_OK) return st;
+  p->threads = best_t;
+  p->ichunk = best_c;
+  p->split = best_split;
+  p->fork = best_fork;
+  p->cut = best_cut;
+  OEMS_TRY(pack_grids_any(p));
+  return pack_layout(p, act);
 }
 
 static oems_status pack_run_span(oems_pack* p, long long base, int steps) {
@@ -3803,6 +3923,7 @@ static oems_status pack_run_batch(oems_pack* p, const oems_batch* const* batches
   }
   DeviceGuard dg(p->device);
   OEMS_TRY(pack_layout(p, part));
+  if (!p->tuned) OEMS_TRY(pack_tune(p));
   const uint64_t si = b0->sample_interval, ci = b0->check_interval;
   const bool has_decay = b0->has_energy_decay_db != 0;
   const uint64_t t0 = R[part[0]].t0;
@@ -3950,14 +4071,19 @@ oems_status oems_pack_create(oems_engine* const* engines, uint64_t count, oems_p
   OEMS_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   OEMS_CUDA(cudaEventCreate(&p->ev0));
   OEMS_CUDA(cudaEventCreate(&p->ev1));
+  // the fork's stream and events: a failure leaves the pack unforked
+  if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (p->side) cudaStreamDestroy(p->side);
+    if (p->fork_ev) cudaEventDestroy(p->fork_ev);
+    if (p->join_ev) cudaEventDestroy(p->join_ev);
+    p->side = nullptr;
+    p->fork_ev = p->join_ev = nullptr;
+  }
   OEMS_CUDA(p->d_base.ensure(1));
-  oems_status st = OEMS_OK;
-  if (p->storage == 1)
-    st = pack_grids<__half>(p.get());
-  else if (p->storage == 2)
-    st = pack_grids<__nv_bfloat16>(p.get());
-  else
-    st = pack_grids<float>(p.get());
+  const oems_status st = pack_grids_any(p.get());
   if (st != OEMS_OK) {
     oems_pack_destroy(p.release());
     return st;
@@ -3981,8 +4107,40 @@ void oems_pack_destroy(oems_pack* pack) {
   oems::pinned_put(pack->h_energy, pack->h_energy_cap * 2 * sizeof(double));
   if (pack->ev0) cudaEventDestroy(pack->ev0);
   if (pack->ev1) cudaEventDestroy(pack->ev1);
+  if (pack->side) {
+    cudaStreamSynchronize(pack->side);
+    cudaStreamDestroy(pack->side);
+  }
+  if (pack->fork_ev) cudaEventDestroy(pack->fork_ev);
+  if (pack->join_ev) cudaEventDestroy(pack->join_ev);
   if (pack->stream) cudaStreamDestroy(pack->stream);
   delete pack;
+}
+
+oems_status oems_pack_set_shape(oems_pack* pack, int32_t threads, int32_t ichunk, int32_t split) {
+  if (!pack) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL pack");
+  if (threads < 32 || threads > 512 || threads % 32 || ichunk < 1)
+    return fail(OEMS_ERR_CONFIG, "pack shape: threads a multiple of 32 in [32, 512], ichunk >= 1");
+  DeviceGuard dg(pack->device);
+  if (split < 0 || split > 3 || (split >= 2 && !pack->side))
+    return fail(OEMS_ERR_CONFIG, "pack shape: split 0 (whole), 1 (split), 2 / 3 (split, forked, cut 0 / 1)");
+  pack->threads = threads;
+  pack->ichunk = ichunk;
+  pack->split = split != 0;
+  pack->fork = split >= 2;
+  pack->cut = split == 3 ? 1 : 0;
+  pack->tuned = true;
+  OEMS_TRY(oems::pack_grids_any(pack));
+  if (!pack->active.empty()) OEMS_TRY(oems::pack_layout(pack, pack->active));
+  return OEMS_OK;
+}
+
+oems_status oems_pack_shape(const oems_pack* pack, int32_t* threads, int32_t* ichunk, int32_t* split) {
+  if (!pack) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL pack");
+  if (threads) *threads = pack->threads;
+  if (ichunk) *ichunk = pack->ichunk;
+  if (split) *split = !pack->split ? 0 : !pack->fork ? 1 : 2 + pack->cut;
+  return OEMS_OK;
 }
 
 oems_status oems_pack_run_batch(oems_pack* pack, const oems_batch* const* batches, oems_batch_result* results,

@@ -321,4 +321,20 @@ __global__ void __launch_bounds__(192, 1)
   }
 }
 
+// One CTA waits, through the GEMM's own bounded wait, on an mbarrier that no
+// thread or copy ever arrives at: the wait gives up after its limit and sets
+// the error word.  Nothing is in flight on the barrier, so the CTA exits
+// cleanly.  For tests of the timeout path: the host reads the error word
+// (oems_tc_check) and the context stays usable.
+__global__ void k_tc_wait_probe(int* err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) (void)tc::mbar_wait(&bar, 0, err);
+  __syncthreads();
+}
+
 }  // namespace oems

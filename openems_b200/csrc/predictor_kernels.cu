@@ -319,6 +319,15 @@ oems_status oems_tc_gemm_bf16(const void* a, int lda, const void* b, int ldb, fl
   return OEMS_OK;
 }
 
+oems_status oems_tc_wait_probe(void* stream) {
+  int* err = nullptr;
+  oems_status st = err_word(&err);
+  if (st != OEMS_OK) return st;
+  oems::k_tc_wait_probe<<<1, 32, 0, S(stream)>>>(err);
+  PK_CUDA(cudaGetLastError());
+  return OEMS_OK;
+}
+
 oems_status oems_tc_check(void* stream) {
   int* err = nullptr;
   oems_status st = err_word(&err);

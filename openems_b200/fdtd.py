@@ -376,10 +376,15 @@ class Operator:
         self._h = h
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h:
-            N.lib().oems_operator_destroy(h)
-            self._h = None
+        # at interpreter exit the module globals (the library handle) may be
+        # gone already; the process is ending and the driver frees the device
+        try:
+            h = getattr(self, "_h", None)
+            if h:
+                N.lib().oems_operator_destroy(h)
+                self._h = None
+        except (TypeError, AttributeError):
+            pass
 
     @property
     def handle(self):
@@ -978,7 +983,12 @@ class Engine:
             self._h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module globals (the library handle) may be
+        # gone already; the process is ending and the driver frees the device
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     @property
     def handle(self):
@@ -1262,12 +1272,13 @@ def _batch_result(r, samples, cap) -> "BatchResult":
 
 class Pack:
     """Several engines stepped by shared launches (oems_pack_*): one launch
-    per half-step of the plain update kernels over all their CPML-free boxes
-    and one of the CPML kernels over all their slab cells, a post-step
-    launch with a CTA per engine and two energy launches for all.  Each
-    engine ends a batch with the bits oems_engine_run_batch would give it.
-    The engines need full coefficients and only CPML, sources, probes and
-    probe DFTs; keep them alive while the pack exists."""
+    per half-step of the plain update kernels over the grids without CPML
+    and one of the CPML kernels over the grids with it, a post-step launch
+    with a CTA per engine and two energy launches for all.  Each engine ends
+    a batch with the bits oems_engine_run_batch would give it.  The first
+    batch tunes the launch shape (CTA size, x-planes per work item, CPML
+    grids whole or split into box and slabs) unless set_shape chose one.  The engines need full coefficients and only CPML,
+    sources, probes and probe DFTs; keep them alive while the pack exists."""
 
     def __init__(self, engines: Sequence["Engine"]):
         self.engines = list(engines)
@@ -1283,7 +1294,25 @@ class Pack:
             self._h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module globals (the library handle) may be
+        # gone already; the process is ending and the driver frees the device
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
+
+    def set_shape(self, threads: int, ichunk: int, split: int = 0):
+        """CTAs of `threads` over work items of `ichunk` x-planes; split: 0
+        CPML grids whole, 1 as their CPML-free box plus their slab cells, 2 / 3
+        as 1 with the slab launch on a second stream beside the box launch
+        (3: the box launch's grid cut by one CTA per SM).  No tuning."""
+        N.check(N.lib().oems_pack_set_shape(self._h, threads, ichunk, int(split)))
+
+    def shape(self) -> tuple:
+        """(threads, ichunk, split) of the update launches."""
+        t, c, sp = N.c_i32(), N.c_i32(), N.c_i32()
+        N.check(N.lib().oems_pack_shape(self._h, ctypes.byref(t), ctypes.byref(c), ctypes.byref(sp)))
+        return t.value, c.value, sp.value
 
     def run_batch(self, batches: Sequence[Optional["EngineBatch"]]):
         """batches[i] for engine i (None: engine i sits this batch out); the
@@ -1366,10 +1395,15 @@ class Simulation:
         self._sim = None
 
     def __del__(self):
-        s = getattr(self, "_sim", None)
-        if s:
-            N.lib().oems_simulation_destroy(s)
-            self._sim = None
+        # at interpreter exit the module globals (the library handle) may be
+        # gone already; the process is ending and the driver frees the device
+        try:
+            s = getattr(self, "_sim", None)
+            if s:
+                N.lib().oems_simulation_destroy(s)
+                self._sim = None
+        except (TypeError, AttributeError):
+            pass
 
     def set_boundaries(self, boundaries: BoundaryConditions):
         self.boundaries = boundaries

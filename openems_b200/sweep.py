@@ -82,7 +82,12 @@ class Sweep:
             self._h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module globals (the library handle) may be
+        # gone already; the process is ending and the driver frees the device
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     def add(self, inst: SweepInstance) -> int:
         d = inst.to_c()

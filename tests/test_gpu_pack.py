@@ -100,6 +100,35 @@ def test_pack_skips_engines_and_stops_each_at_its_decay():
     pack.close()
 
 
+@pytest.mark.parametrize("shape", [(128, 2, 0), (512, 16, 0), (256, 4, 1), (128, 8, 1), (128, 4, 2), (256, 2, 3),
+                                   None])
+def test_pack_shapes_give_the_same_bits(shape):
+    """Every launch shape (set, or tuned on the first batch over saved
+    state) gives each engine the bits of its own run."""
+    scs = _mixed()
+    alone = [_engine(sc) for sc in scs]
+    packed = [_engine(sc) for sc in scs]
+    pack = oe.Pack([e for _, e in packed])
+    if shape:
+        pack.set_shape(*shape)
+    want = [eng.run_batch(_batch(sc, op, 0, 150)) for sc, (op, eng) in zip(scs, alone)]
+    got = pack.run_batch([_batch(sc, op, 0, 150) for sc, (op, _) in zip(scs, packed)])
+    if shape:
+        assert pack.shape() == shape
+    else:
+        assert pack.shape()[:2] in [(t, c) for t in (128, 256, 512) for c in (2, 4, 8, 16)]
+    for w, g in zip(want, got):
+        assert [(s.timestep, s.e_energy, s.h_energy) for s in g.energy_samples] == \
+               [(s.timestep, s.e_energy, s.h_energy) for s in w.energy_samples]
+    for (_, a), (_, b) in zip(alone, packed):
+        assert np.array_equal(np.concatenate(a.read_fields()), np.concatenate(b.read_fields()))
+        if a.probe_traces().size:
+            assert np.array_equal(a.probe_traces(), b.probe_traces())
+    with pytest.raises(oe.ConfigError):
+        pack.set_shape(100, 4)
+    pack.close()
+
+
 def test_pack_refuses_unsupported_engines():
     sc = cpml_scenarios()[0]
     op = make_operator(sc)

@@ -51,6 +51,25 @@ def test_gemm_bias_beta_and_pitch():
     assert torch.equal(c[:, 130:], c0[:, 130:])  # columns beyond N untouched
 
 
+def test_bounded_wait_runs_out_and_the_context_stays_usable():
+    """A wait on an mbarrier nothing arrives at gives up after its limit
+    (about a second), the host reads OEMS_ERR_TIMEOUT, and a GEMM on the same
+    stream afterwards is correct."""
+    import time
+    t0 = time.perf_counter()
+    N.check(N.lib().oems_tc_wait_probe(None))
+    with pytest.raises(N.DeviceTimeoutError):
+        N.check(N.lib().oems_tc_check(None))
+    assert time.perf_counter() - t0 < 30.0
+    N.check(N.lib().oems_tc_check(None))  # the error word was cleared
+    g = torch.Generator(device="cpu").manual_seed(9)
+    a = torch.randn(256, 64, generator=g).to(torch.bfloat16).cuda()
+    b = torch.randn(128, 64, generator=g).to(torch.bfloat16).cuda()
+    c = gemm(a, b)
+    ref = (a.double() @ b.double().T).float()
+    assert (c - ref).abs().max().item() < 1e-5 * ref.abs().max().item()
+
+
 def test_gemm_rejects_bad_shapes():
     a = torch.zeros(16, 12, dtype=torch.bfloat16, device="cuda")
     b = torch.zeros(16, 12, dtype=torch.bfloat16, device="cuda")
