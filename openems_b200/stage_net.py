@@ -353,7 +353,8 @@ def _concat(a: dict, b: dict) -> dict:
 
 def learn(train_count: int = 1500, test_count: int = 400, family: str = "small", train_seed: int = 5,
           test_seed: int = 50, extra_patch: int = 0, val_frac: float = 0.2,
-          cfg: StageNetConfig = StageNetConfig(), concurrency: int = 16, log=print):
+          cfg: StageNetConfig = StageNetConfig(), concurrency: int = 16, log=print, reuse: Optional[str] = None,
+          patch_seed: Optional[int] = None):
     """Generates the records with the batched engine (full runs for the
     reference S11, then every instance through every stage of the dense
     plan): train_count instances of `family` (plus extra_patch of the
@@ -362,15 +363,28 @@ def learn(train_count: int = 1500, test_count: int = 400, family: str = "small",
     validation: early stopping, and both rules' thresholds are chosen on the
     validation instances' out-of-sample scores (the largest threshold
     keeping every validation instance within 0.5 dB, and within a 1%
-    budget).  Returns (net, report, train records, test records)."""
+    budget).  reuse: a directory with the records an earlier run saved
+    (stage_records_train.npz / _test.npz), used instead of recording them
+    again; extra_patch instances (seed patch_seed, default train_seed + 1)
+    are then recorded and added to its training records.  Returns (net,
+    report, train records, test records)."""
     import time
     from . import early_stop as ES
     plan = ES.StagePlan.dense()
     t0 = time.perf_counter()
-    rtr = records(family, train_count, train_seed, plan, concurrency, log, t0)
+    if reuse:
+        import os
+        with np.load(os.path.join(reuse, "stage_records_train.npz")) as d:
+            rtr = {k: d[k] for k in d.files}
+        with np.load(os.path.join(reuse, "stage_records_test.npz")) as d:
+            rte = {k: d[k] for k in d.files}
+    else:
+        rtr = records(family, train_count, train_seed, plan, concurrency, log, t0)
     if extra_patch:
-        rtr = _concat(rtr, records("patch", extra_patch, train_seed + 1, plan, concurrency, log, t0))
-    rte = records(family, test_count, test_seed, plan, concurrency, log, t0)
+        ps = train_seed + 1 if patch_seed is None else patch_seed
+        rtr = _concat(rtr, records("patch", extra_patch, ps, plan, concurrency, log, t0))
+    if not reuse:
+        rte = records(family, test_count, test_seed, plan, concurrency, log, t0)
     x, sc, e, sg, it = rows(rtr)
     n_inst = len(rtr["steps_full"])
     rng = np.random.default_rng(cfg.seed + 7)
@@ -409,6 +423,7 @@ def learn(train_count: int = 1500, test_count: int = 400, family: str = "small",
     net.threshold = thr_for(pv, 0.0)
     report = {
         "family": family, "train": train_count, "extra_patch": extra_patch, "test": test_count,
+        "reused_records": reuse is not None, "patch_seed": train_seed + 1 if patch_seed is None else patch_seed,
         "train_seed": train_seed, "test_seed": test_seed, "validation_instances": int(len(val_inst)),
         "stages": stages, "records_train": int((~is_val).sum()), "records_validation": int(is_val.sum()),
         "records_test": int(len(ete)), "train_seconds": train_s, "epochs": cfg.epochs,
@@ -456,10 +471,13 @@ def main(argv=None):
     p.add_argument("--concurrency", type=int, default=16)
     p.add_argument("--out", default=".")
     p.add_argument("--save-records", action="store_true", help="also write the records (.npz, float16 windows)")
+    p.add_argument("--reuse", default=None, help="directory of an earlier run's saved records, used instead")
+    p.add_argument("--patch-seed", type=int, default=None, help="seed of the --extra-patch instances")
     a = p.parse_args(argv)
     cfg = StageNetConfig(epochs=a.epochs)
     net, report, rtr, rte = learn(a.train, a.test, a.family, extra_patch=a.extra_patch, cfg=cfg,
-                                  concurrency=a.concurrency, log=lambda m: print(m, flush=True))
+                                  concurrency=a.concurrency, log=lambda m: print(m, flush=True), reuse=a.reuse,
+                                  patch_seed=a.patch_seed)
     os.makedirs(a.out, exist_ok=True)
     np.savez(os.path.join(a.out, "stage_net.npz"), **net.state())
     if a.save_records:
