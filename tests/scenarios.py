@@ -249,6 +249,14 @@ def cpml_scenarios() -> List[Scenario]:
                  num_steps=160, sample_interval=20, track_peak=True,
                  cpml=oe.CpmlBoundaries(layers=(0, 0, 0, 0, 5, 6)),
                  probes=[(2, (7, 13, 22)), (0, (5, 9, 2)), (4, (7, 13, 41))]),
+        # z slabs that meet (5 + 5 layers on nz = 10): the float4 chunk of
+        # k = 4..7 lies in both, so its update stretches with both z faces
+        Scenario("cpml_z_thin_10", (16, 18, 10), 1e-3,
+                 excitations=[E.gaussian_pulse(tau, 4 * tau, 2, (8, 9, 5)),
+                              E.gaussian_pulse(tau, 4 * tau, 1, (6, 10, 4))],
+                 num_steps=120, sample_interval=20, track_peak=True,
+                 cpml=oe.CpmlBoundaries(layers=(3, 3, 0, 2, 5, 5)),
+                 probes=[(2, (8, 9, 5)), (1, (6, 10, 7))]),
     ]
 
 

@@ -67,7 +67,7 @@ def test_pack_equals_separate_engines(storage):
 def _decaying():
     """CPML on all faces, on some faces, only on z, and none: with a
     modulated Gaussian each falls 20 dB below its peak at another step."""
-    scs = cpml_scenarios() + [reference_scenarios()[2]]
+    scs = cpml_scenarios()[:3] + [reference_scenarios()[2]]
     for sc in scs:
         sc.excitations = [oe.Excitation.gaussian_modulated(15e9, 0.5, 2, tuple(n // 2 for n in sc.dims))]
     return scs

@@ -97,7 +97,8 @@ def test_small_grid_default_shape(sc):
     assert_parity(got, run_oracle(sc))
 
 
-@pytest.mark.parametrize("sc", cpml_scenarios() + [probe_scenario()], ids=lambda s: s.name)
+# the grids whose CPML leaves a CPML-free box (the thin-z one has none)
+@pytest.mark.parametrize("sc", cpml_scenarios()[:3] + [probe_scenario()], ids=lambda s: s.name)
 def test_zsplit_forked_default_shape(sc):
     """The untuned z-split forks its CPML slab launch onto a second stream
     beside the plain interior launch (joined by events, inside the graphs
