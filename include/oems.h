@@ -365,7 +365,9 @@ OEMS_API oems_status oems_engine_reset(oems_engine* engine);
  * one energy launch pair for all.  The first batch times the update
  * kernels' CTA size, x-planes per work item and whether CPML grids enter
  * whole or split (below) on saved copies of the engines' state (restored
- * afterwards) and keeps the fastest, unless oems_pack_set_shape chose one.  The batches must share num_steps,
+ * afterwards) and keeps the fastest; a batch whose engines hold under half
+ * the cells of the tuned set tunes again.  oems_pack_set_shape fixes the
+ * shape instead.  The batches must share num_steps,
  * sample_interval, check_interval and whether they carry an energy-decay end
  * condition, and their engines must be at the same timestep; each engine
  * keeps its own decay threshold, peak and termination step.  statuses[i] is

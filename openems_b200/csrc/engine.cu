@@ -3577,6 +3577,8 @@ struct oems_pack {
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   bool tuned = false;
+  bool shape_set = false;  // chosen by oems_pack_set_shape: never re-tuned
+  double tuned_cells = 0;  // cells of the engines the shape was tuned on
 };
 
 namespace oems {
@@ -3753,6 +3755,8 @@ static oems_status pack_tune(oems_pack* p) {
   p->tuned = true;
   const std::vector<int> act = p->active;
   if (act.empty()) return OEMS_OK;
+  p->tuned_cells = 0;
+  for (int i : act) p->tuned_cells += (double)p->en[i]->nx * p->en[i]->ny * p->en[i]->nz;
   std::vector<void*> saved(act.size(), nullptr);
   long long cells = 0;
   oems_status st = OEMS_OK;
@@ -3923,7 +3927,12 @@ static oems_status pack_run_batch(oems_pack* p, const oems_batch* const* batches
   }
   DeviceGuard dg(p->device);
   OEMS_TRY(pack_layout(p, part));
-  if (!p->tuned) OEMS_TRY(pack_tune(p));
+  // tuned on the first batch, and again when the engines in the batch hold
+  // under half the cells the shape was tuned on (a sweep's pack shrinks as
+  // its instances end)
+  double cells = 0;
+  for (int i : part) cells += (double)p->en[i]->nx * p->en[i]->ny * p->en[i]->nz;
+  if (!p->shape_set && (!p->tuned || cells < 0.5 * p->tuned_cells)) OEMS_TRY(pack_tune(p));
   const uint64_t si = b0->sample_interval, ci = b0->check_interval;
   const bool has_decay = b0->has_energy_decay_db != 0;
   const uint64_t t0 = R[part[0]].t0;
@@ -4130,6 +4139,7 @@ oems_status oems_pack_set_shape(oems_pack* pack, int32_t threads, int32_t ichunk
   pack->fork = split >= 2;
   pack->cut = split == 3 ? 1 : 0;
   pack->tuned = true;
+  pack->shape_set = true;
   OEMS_TRY(oems::pack_grids_any(pack));
   if (!pack->active.empty()) OEMS_TRY(oems::pack_layout(pack, pack->active));
   return OEMS_OK;
