@@ -489,11 +489,10 @@ __device__ __forceinline__ void h_item(const HArgs& a, const float* tab, int w) 
         px1 = sl.fx >= 0 ? ld4(a.cp.psi_h[sl.fx][1] + sl.px) : zero4();
         py0 = sl.fy >= 0 ? ld4(a.cp.psi_h[sl.fy][0] + sl.py) : zero4();
         py1 = sl.fy >= 0 ? ld4(a.cp.psi_h[sl.fy][1] + sl.py) : zero4();
-        // the z face of this chunk (z-min first where a chunk of a thin
-        // grid touches both; the other face then follows after the update)
-        const bool zin = sl.zmin || sl.zmax;
-        pzn0 = zin ? ld4(a.cp.psi_h[sl.zmin ? 4 : 5][0] + (sl.zmin ? sl.pz0 : sl.pz1)) : zero4();
-        pzn1 = zin ? ld4(a.cp.psi_h[sl.zmin ? 4 : 5][1] + (sl.zmin ? sl.pz0 : sl.pz1)) : zero4();
+        pzn0 = sl.zmin ? ld4(a.cp.psi_h[4][0] + sl.pz0) : zero4();
+        pzn1 = sl.zmin ? ld4(a.cp.psi_h[4][1] + sl.pz0) : zero4();
+        pzx0 = sl.zmax ? ld4(a.cp.psi_h[5][0] + sl.pz1) : zero4();
+        pzx1 = sl.zmax ? ld4(a.cp.psi_h[5][1] + sl.pz1) : zero4();
       }
       // ---- neighbours along z: first element of the next chunk (k0 + 4)
       float exn = __shfl_down_sync(kFullMask, ex4.x, 1);
@@ -532,24 +531,13 @@ __device__ __forceinline__ void h_item(const HArgs& a, const float* tab, int w) 
           stretch_vec(dex_dy, py1, b, cc, ik, live);
         }
         // z-slab: Hx (dEy/dz, slot 0), Hy (dEx/dz, slot 1)
-        if (sl.zmin || sl.zmax) {
-          const int fz = sl.zmin ? 4 : 5;
-          stretch_z(a.cp, fz, k0, true, dey_dz, pzn0, live);
-          stretch_z(a.cp, fz, k0, true, dex_dz, pzn1, live);
-          if (valid) {
-            st4(a.cp.psi_h[fz][0] + (sl.zmin ? sl.pz0 : sl.pz1), pzn0);
-            st4(a.cp.psi_h[fz][1] + (sl.zmin ? sl.pz0 : sl.pz1), pzn1);
-          }
+        if (sl.zmin) {
+          stretch_z(a.cp, 4, k0, true, dey_dz, pzn0, live);
+          stretch_z(a.cp, 4, k0, true, dex_dz, pzn1, live);
         }
-        if (sl.zmin && sl.zmax) {
-          pzx0 = ld4(a.cp.psi_h[5][0] + sl.pz1);
-          pzx1 = ld4(a.cp.psi_h[5][1] + sl.pz1);
+        if (sl.zmax) {
           stretch_z(a.cp, 5, k0, true, dey_dz, pzx0, live);
           stretch_z(a.cp, 5, k0, true, dex_dz, pzx1, live);
-          if (valid) {
-            st4(a.cp.psi_h[5][0] + sl.pz1, pzx0);
-            st4(a.cp.psi_h[5][1] + sl.pz1, pzx1);
-          }
         }
         // x-slab: Hy (dEz/dx, slot 0), Hz (dEy/dx, slot 1)
         if (sl.fx >= 0) {
@@ -578,6 +566,14 @@ __device__ __forceinline__ void h_item(const HArgs& a, const float* tab, int w) 
           if (sl.fy >= 0) {
             st4(a.cp.psi_h[sl.fy][0] + sl.py, py0);
             st4(a.cp.psi_h[sl.fy][1] + sl.py, py1);
+          }
+          if (sl.zmin) {
+            st4(a.cp.psi_h[4][0] + sl.pz0, pzn0);
+            st4(a.cp.psi_h[4][1] + sl.pz0, pzn1);
+          }
+          if (sl.zmax) {
+            st4(a.cp.psi_h[5][0] + sl.pz1, pzx0);
+            st4(a.cp.psi_h[5][1] + sl.pz1, pzx1);
           }
           if (sl.fx >= 0) {
             st4(a.cp.psi_h[sl.fx][0] + sl.px, px0);
@@ -668,11 +664,10 @@ __device__ __forceinline__ void e_item(const EArgs& a, const float* tab, int w) 
         px1 = sl.fx >= 0 ? ld4(a.cp.psi_e[sl.fx][1] + sl.px) : zero4();
         py0 = sl.fy >= 0 ? ld4(a.cp.psi_e[sl.fy][0] + sl.py) : zero4();
         py1 = sl.fy >= 0 ? ld4(a.cp.psi_e[sl.fy][1] + sl.py) : zero4();
-        // the z face of this chunk (z-min first where a chunk of a thin
-        // grid touches both; the other face then follows after the update)
-        const bool zin = sl.zmin || sl.zmax;
-        pzn0 = zin ? ld4(a.cp.psi_e[sl.zmin ? 4 : 5][0] + (sl.zmin ? sl.pz0 : sl.pz1)) : zero4();
-        pzn1 = zin ? ld4(a.cp.psi_e[sl.zmin ? 4 : 5][1] + (sl.zmin ? sl.pz0 : sl.pz1)) : zero4();
+        pzn0 = sl.zmin ? ld4(a.cp.psi_e[4][0] + sl.pz0) : zero4();
+        pzn1 = sl.zmin ? ld4(a.cp.psi_e[4][1] + sl.pz0) : zero4();
+        pzx0 = sl.zmax ? ld4(a.cp.psi_e[5][0] + sl.pz1) : zero4();
+        pzx1 = sl.zmax ? ld4(a.cp.psi_e[5][1] + sl.pz1) : zero4();
       }
       // ---- neighbours along z: last element of the previous chunk (k0 - 1)
       float hxm = __shfl_up_sync(kFullMask, hx4.w, 1);
@@ -711,24 +706,13 @@ __device__ __forceinline__ void e_item(const EArgs& a, const float* tab, int w) 
             stretch_vec(dhx_dy, py1, b, cc, ik, live);
           }
           // z-slab: Ex (dHy/dz, slot 0), Ey (dHx/dz, slot 1)
-          if (sl.zmin || sl.zmax) {
-            const int fz = sl.zmin ? 4 : 5;
-            stretch_z(a.cp, fz, k0, false, dhy_dz, pzn0, live);
-            stretch_z(a.cp, fz, k0, false, dhx_dz, pzn1, live);
-            if (valid) {
-              st4(a.cp.psi_e[fz][0] + (sl.zmin ? sl.pz0 : sl.pz1), pzn0);
-              st4(a.cp.psi_e[fz][1] + (sl.zmin ? sl.pz0 : sl.pz1), pzn1);
-            }
+          if (sl.zmin) {
+            stretch_z(a.cp, 4, k0, false, dhy_dz, pzn0, live);
+            stretch_z(a.cp, 4, k0, false, dhx_dz, pzn1, live);
           }
-          if (sl.zmin && sl.zmax) {
-            pzx0 = ld4(a.cp.psi_e[5][0] + sl.pz1);
-            pzx1 = ld4(a.cp.psi_e[5][1] + sl.pz1);
+          if (sl.zmax) {
             stretch_z(a.cp, 5, k0, false, dhy_dz, pzx0, live);
             stretch_z(a.cp, 5, k0, false, dhx_dz, pzx1, live);
-            if (valid) {
-              st4(a.cp.psi_e[5][0] + sl.pz1, pzx0);
-              st4(a.cp.psi_e[5][1] + sl.pz1, pzx1);
-            }
           }
           // x-slab: Ey (dHz/dx, slot 0), Ez (dHy/dx, slot 1)
           if (sl.fx >= 0) {
@@ -757,6 +741,14 @@ __device__ __forceinline__ void e_item(const EArgs& a, const float* tab, int w) 
             if (sl.fy >= 0) {
               st4(a.cp.psi_e[sl.fy][0] + sl.py, py0);
               st4(a.cp.psi_e[sl.fy][1] + sl.py, py1);
+            }
+            if (sl.zmin) {
+              st4(a.cp.psi_e[4][0] + sl.pz0, pzn0);
+              st4(a.cp.psi_e[4][1] + sl.pz0, pzn1);
+            }
+            if (sl.zmax) {
+              st4(a.cp.psi_e[5][0] + sl.pz1, pzx0);
+              st4(a.cp.psi_e[5][1] + sl.pz1, pzx1);
             }
             if (sl.fx >= 0) {
               st4(a.cp.psi_e[sl.fx][0] + sl.px, px0);
