@@ -34,6 +34,17 @@ typedef struct oems_simulation oems_simulation;
 
 /* ---- Operator ----------------------------------------------------------- */
 
+/* Compressed coefficients (replaces CompressedCoefficients::from_fields,
+ * src/fdtd/compressed.rs:125-192): deduplicates the 12 coefficients of each
+ * of ncells cells (coef = ca0..2, cb0..2, da0..2, db0..2, one float per cell
+ * each) into a table of unique sets, compared bit for bit, with ids in cell
+ * order -- the engine's OEMS_ENGINE_COMPRESSED storage.  ids (ncells,
+ * may be NULL) receives each cell's set; table (may be NULL) the first
+ * table_cap sets, 12 floats each; *nunique the number of sets.
+ * OEMS_ERR_MATERIAL above 65536 sets. */
+OEMS_API oems_status oems_compress_coefficients(const float* const coef[12], uint64_t ncells, uint16_t* ids,
+                                                float* table, uint32_t table_cap, uint32_t* nunique);
+
 /* Cartesian grid from mesh lines (cells = lines - 1 per axis), scaled by unit. */
 OEMS_API oems_status oems_operator_create(const double* x_lines, uint64_t nxl, const double* y_lines,
                                  uint64_t nyl, const double* z_lines, uint64_t nzl, double unit,

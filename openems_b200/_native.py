@@ -274,6 +274,7 @@ SIGNATURES = {
                                            ctypes.POINTER(c_f64), ctypes.POINTER(c_u64)]),
     # include/oems_host.h
     "oems_operator_create": (c_i32, [P, c_u64, P, c_u64, P, c_u64, c_f64, ctypes.POINTER(P)]),
+    "oems_compress_coefficients": (c_i32, [ctypes.POINTER(ctypes.c_void_p), c_u64, P, P, c_u32, ctypes.POINTER(c_u32)]),
     "oems_operator_create_uniform": (c_i32, [c_u64, c_u64, c_u64, c_f64, ctypes.POINTER(P)]),
     "oems_operator_destroy": (None, [P]),
     "oems_operator_set_material": (c_i32, [P, c_f64, c_f64, c_f64, c_f64, c_u64 * 6]),

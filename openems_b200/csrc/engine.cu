@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/oems.h"
+#include "../../include/oems_host.h"
 #include "yee_kernels.cuh"
 #include "yee_pipe.cuh"
 #include "yee_tma.cuh"
@@ -1773,19 +1774,6 @@ static oems_status autotune(oems_engine* en) {
   return st;
 }
 
-struct CoefKey {
-  float v[12];
-  bool operator==(const CoefKey& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
-};
-struct CoefKeyHash {
-  size_t operator()(const CoefKey& k) const {
-    uint64_t h = 1469598103934665603ull;
-    const unsigned char* p = reinterpret_cast<const unsigned char*>(k.v);
-    for (size_t i = 0; i < sizeof(k.v); ++i) h = (h ^ p[i]) * 1099511628211ull;
-    return (size_t)h;
-  }
-};
-
 // Factor applied to coefficient array a (ca0..2 cb0..2 da0..2 db0..2) when H
 // is stored multiplied by h_scale: Cb / s (E sees H / s) and Db * s.
 static float coef_storage_factor(const oems_engine* en, int a) {
@@ -1823,34 +1811,20 @@ static oems_status upload_coefficients(oems_engine* en, const oems_operator_desc
     OEMS_CUDA(cudaStreamSynchronize(en->stream));
     return OEMS_OK;
   }
-  // Compressed: exact (bitwise) deduplication of the 12 coefficients of each
-  // cell into a table; the reference quantises at 1e-10
-  // (src/fdtd/compressed.rs:11-31), which is below one f32 ulp for every
-  // coefficient magnitude the operator produces, so the two agree.
-  std::unordered_map<CoefKey, uint32_t, CoefKeyHash> map;
-  std::vector<float> table;
-  std::vector<uint16_t> ids16((size_t)en->ncells_padded, 0);
+  // Compressed: the 12 coefficients of each cell deduplicated bit for bit
+  // into a table (oems_compress_coefficients, the host routine of
+  // CompressedCoefficients::from_fields), ids padded to the row pitch
   const size_t n = (size_t)en->nx * en->ny * en->nz;
-  for (size_t r = 0; r < rows; ++r) {
-    for (int k = 0; k < en->nz; ++k) {
-      const size_t q = r * en->nz + k;
-      CoefKey key;
-      for (int a = 0; a < 12; ++a) key.v[a] = src[a][q];
-      auto it = map.find(key);
-      uint32_t id;
-      if (it == map.end()) {
-        id = (uint32_t)map.size();
-        if (id >= 65536) return fail(OEMS_ERR_MATERIAL, "more than 65536 unique coefficient sets; compressed storage refused");
-        map.emplace(key, id);
-        table.insert(table.end(), key.v, key.v + 12);
-      } else {
-        id = it->second;
-      }
-      ids16[r * nzp + k] = (uint16_t)id;
-    }
-  }
-  (void)n;
-  en->ntable = (int)map.size();
+  std::vector<uint16_t> dense(n);
+  std::vector<float> table((size_t)65536 * 12);
+  uint32_t nunique = 0;
+  const oems_status cst = oems_compress_coefficients(src, n, dense.data(), table.data(), 65536, &nunique);
+  if (cst != OEMS_OK) return cst;
+  table.resize((size_t)nunique * 12);
+  std::vector<uint16_t> ids16((size_t)en->ncells_padded, 0);
+  for (size_t r = 0; r < rows; ++r)
+    std::memcpy(ids16.data() + r * nzp, dense.data() + r * en->nz, (size_t)en->nz * sizeof(uint16_t));
+  en->ntable = (int)nunique;
   for (size_t t = 0; t < table.size(); ++t) table[t] *= coef_storage_factor(en, (int)(t % 12));
   OEMS_CUDA(pool_alloc(reinterpret_cast<void**>(&en->table), table.size() * sizeof(float), en->stream));
   OEMS_CUDA(cudaMemcpyAsync(en->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,

@@ -5,10 +5,12 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <limits>
 #include <memory>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/oems.h"
@@ -164,6 +166,52 @@ void fill_exc(int32_t kind, uint32_t dir, const uint64_t* pos, oems_excitation* 
 }  // namespace
 
 extern "C" {
+
+// ---- compressed coefficients (src/fdtd/compressed.rs:125-192) -------------
+// Exact (bitwise) deduplication of each cell's 12 coefficients into a table:
+// the reference quantises at 1e-10 (compressed.rs:11-31), below one f32 ulp
+// of every coefficient magnitude the operator produces, so both find the
+// same sets.  Ids are assigned in cell order.
+namespace {
+struct CoefSet {
+  float v[12];
+  bool operator==(const CoefSet& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
+};
+struct CoefSetHash {
+  size_t operator()(const CoefSet& k) const {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a over the 48 bytes
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(k.v);
+    for (size_t i = 0; i < sizeof(k.v); ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return (size_t)h;
+  }
+};
+}  // namespace
+
+oems_status oems_compress_coefficients(const float* const coef[12], uint64_t ncells, uint16_t* ids, float* table,
+                                       uint32_t table_cap, uint32_t* nunique) {
+  if (!coef || !nunique) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int a = 0; a < 12; ++a)
+    if (!coef[a] && ncells) return hfail(OEMS_ERR_INVALID_ARGUMENT, "coefficient array pointer is NULL");
+  std::unordered_map<CoefSet, uint32_t, CoefSetHash> map;
+  for (uint64_t q = 0; q < ncells; ++q) {
+    CoefSet key;
+    for (int a = 0; a < 12; ++a) key.v[a] = coef[a][q];
+    auto it = map.find(key);
+    uint32_t id;
+    if (it == map.end()) {
+      id = (uint32_t)map.size();
+      if (id >= 65536)
+        return hfail(OEMS_ERR_MATERIAL, "more than 65536 unique coefficient sets; compressed storage refused");
+      map.emplace(key, id);
+      if (table && id < table_cap) std::memcpy(table + (size_t)id * 12, key.v, sizeof(key.v));
+    } else {
+      id = it->second;
+    }
+    if (ids) ids[q] = (uint16_t)id;
+  }
+  *nunique = (uint32_t)map.size();
+  return OEMS_OK;
+}
 
 oems_status oems_operator_create(const double* xl, uint64_t nxl, const double* yl, uint64_t nyl, const double* zl,
                                  uint64_t nzl, double unit, oems_operator** out) {

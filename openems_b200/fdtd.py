@@ -206,6 +206,19 @@ class MurAbcConfig:
     def all(cls, order: int = 1):
         return cls(order=order)
 
+    @classmethod
+    def none(cls):
+        return cls(enabled=(False,) * 6)
+
+    def set_enabled(self, face: int, on: bool):
+        """Face 0..5 = x-min, x-max, y-min, y-max, z-min, z-max."""
+        e = list(self.enabled)
+        e[face] = bool(on)
+        self.enabled = tuple(e)
+
+    def num_faces(self) -> int:
+        return sum(bool(e) for e in self.enabled)
+
     def to_c(self) -> N.MurDescC:
         d = N.MurDescC()
         for f in range(6):
@@ -927,6 +940,26 @@ class EngineType(enum.Enum):
     """The engine is CUDA-only; `Cuda` is the single implementation."""
 
     Cuda = "cuda"
+
+
+def compress_coefficients(coef) -> Tuple[np.ndarray, np.ndarray]:
+    """CompressedCoefficients::from_fields (src/fdtd/compressed.rs:125-192)
+    as the engine's compressed storage does it (oems_compress_coefficients):
+    coef holds the 12 per-cell arrays ca0..2, cb0..2, da0..2, db0..2 (first
+    axis; e.g. Operator.coefficients()); returns (ids, table): a uint16 set
+    per cell (C order of the other axes) and the unique sets (n, 12) float32,
+    compared bit for bit."""
+    c = np.ascontiguousarray(coef, dtype=np.float32)
+    if c.shape[0] != 12:
+        raise N.ConfigError("12 coefficient arrays expected")
+    flat = c.reshape(12, -1)
+    n = flat.shape[1]
+    ptrs = (ctypes.c_void_p * 12)(*[flat[a].ctypes.data for a in range(12)])
+    ids = np.empty(n, dtype=np.uint16)
+    table = np.empty((65536, 12), dtype=np.float32)
+    nu = N.c_u32()
+    N.check(N.lib().oems_compress_coefficients(ptrs, n, ids.ctypes.data, table.ctypes.data, 65536, ctypes.byref(nu)))
+    return ids.reshape(c.shape[1:]), table[:nu.value].copy()
 
 
 class Engine:
