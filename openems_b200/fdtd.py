@@ -68,6 +68,10 @@ class Grid:
         return tuple(self._min_delta(v) * self.unit
                      for v in (self.x_lines, self.y_lines, self.z_lines))
 
+    def set_unit(self, unit: float):
+        """Grid::set_unit: the lines are in units of `unit` metres."""
+        self.unit = float(unit)
+
 
 # ---------------------------------------------------------------------------
 # boundaries

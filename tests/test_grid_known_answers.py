@@ -1,0 +1,52 @@
+"""The reference's grid unit tests for the hot path's inputs (Grid::uniform,
+Grid::cartesian, set_unit, cell_size: src/geometry/mod.rs, tests module),
+replayed on the Python Grid and on the C++ host operator that builds the
+engine's coefficients (oems_operator_create / _create_uniform, whose
+dimensions and cell sizes the timestep and coefficients use).  CPU only."""
+import numpy as np
+import pytest
+
+import openems_b200 as oe
+
+
+def test_uniform_grid():
+    """test_uniform_grid: 10 x 20 x 30 cells of 1 mm."""
+    g = oe.Grid.uniform(10, 20, 30, 0.001)
+    assert g.dimensions() == (10, 20, 30)
+    assert g.cell_size() == pytest.approx((0.001, 0.001, 0.001), abs=1e-10)
+    op = oe.Operator(g, oe.BoundaryConditions.all_pec())
+    assert op.dimensions() == (10, 20, 30)
+
+
+def test_cartesian_constructor():
+    """test_cartesian_constructor: 4 / 3 / 5 lines give 3 / 2 / 4 cells."""
+    g = oe.Grid.cartesian([0.0, 0.001, 0.003, 0.006], [0.0, 0.002, 0.004],
+                          [0.0, 0.001, 0.002, 0.003, 0.004])
+    assert g.dimensions() == (3, 2, 4)
+    op = oe.Operator(g, oe.BoundaryConditions.all_pec())
+    assert op.dimensions() == (3, 2, 4)
+    # the smallest spacing per axis sets the cell size the timestep uses
+    assert g.cell_size() == pytest.approx((0.001, 0.002, 0.001), abs=1e-10)
+
+
+def test_set_unit_scaling():
+    """test_set_unit_scaling: 1-unit cells at unit 1 mm are 1 mm cells."""
+    g = oe.Grid.uniform(10, 10, 10, 1.0)
+    g.set_unit(0.001)
+    assert g.cell_size() == pytest.approx((0.001, 0.001, 0.001), abs=1e-10)
+    # the operator scales the lines by the unit: same timestep as 1 mm lines
+    dt_unit = oe.Operator(g, oe.BoundaryConditions.all_pec()).timestep()
+    dt_mm = oe.Operator(oe.Grid.uniform(10, 10, 10, 0.001), oe.BoundaryConditions.all_pec()).timestep()
+    assert dt_unit == pytest.approx(dt_mm, rel=1e-12)
+
+
+def test_grid_bounds_and_volume():
+    """test_grid_bounds (10 x 20 x 30 mm spans) and test_grid_volume (a
+    10^3 grid of 1 mm cells holds 1e-6 m^3)."""
+    g = oe.Grid.uniform(10, 20, 30, 0.001)
+    assert (g.x_lines[0], g.x_lines[-1]) == pytest.approx((0.0, 0.01), abs=1e-10)
+    assert (g.y_lines[0], g.y_lines[-1]) == pytest.approx((0.0, 0.02), abs=1e-10)
+    assert (g.z_lines[0], g.z_lines[-1]) == pytest.approx((0.0, 0.03), abs=1e-10)
+    c = oe.Grid.uniform(10, 10, 10, 0.001)
+    volume = float(np.prod([(v[-1] - v[0]) * c.unit for v in (c.x_lines, c.y_lines, c.z_lines)]))
+    assert abs(volume - 1e-6) < 1e-15
