@@ -16,6 +16,7 @@ from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, 
                    ProbeTerms, voltage_probe, current_probe, voltage_integral, current_integral,
                    port_probe, LumpedPort, DrudeMaterial, LorentzMaterial, DebyeMaterial,
                    RlcType, RlcElement, Nf2ffBox, Nf2ffResults, nf2ff_surface, PmlBoundaries,
-                   PropagationDirection, Polarization, TfsfConfig, Pack, compress_coefficients)
+                   PropagationDirection, Polarization, TfsfConfig, Pack, compress_coefficients,
+                   waveguide_te10)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

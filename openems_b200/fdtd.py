@@ -623,6 +623,7 @@ class ExcitationType(enum.IntEnum):
     GaussianModulated = 2
     Dirac = 3
     Step = 4
+    Custom = 5  # sampled (times, values), linearly interpolated
 
 
 @dataclass
@@ -630,7 +631,10 @@ class Excitation:
     """Excitation (src/fdtd/excitation.rs:46-226).
 
     params: Gaussian (t0, tau); Sinusoidal (frequency,); GaussianModulated
-    (frequency, t0, tau); Dirac / Step ().
+    (frequency, t0, tau); Dirac / Step (); Custom (): its waveform is
+    `times` / `values` (seconds, amplitudes), evaluated here on the host
+    and passed to the engine as a sampled ScheduledExcitation like every
+    other kind.
     """
 
     excitation_type: ExcitationType
@@ -639,6 +643,8 @@ class Excitation:
     position: Tuple[int, int, int]
     amplitude: float = 1.0
     soft_source: bool = True
+    times: Tuple[float, ...] = ()
+    values: Tuple[float, ...] = ()
 
     @classmethod
     def _from_c(cls, c: N.ExcitationC):
@@ -687,6 +693,14 @@ class Excitation:
                                               ctypes.byref(c)))
         return cls._from_c(c)
 
+    @classmethod
+    def custom(cls, times, values, direction, position, amplitude=1.0):
+        """ExcitationType::Custom { times, values } (src/fdtd/excitation.rs:35-41)."""
+        if len(times) != len(values):
+            raise N.ConfigError("custom waveform: times and values differ in length")
+        return cls(ExcitationType.Custom, (), direction, tuple(position), float(amplitude), True,
+                   tuple(float(t) for t in times), tuple(float(v) for v in values))
+
     def with_amplitude(self, amplitude):
         self.amplitude = float(amplitude)
         return self
@@ -696,6 +710,9 @@ class Excitation:
         return self
 
     def to_c(self) -> N.ExcitationC:
+        if self.excitation_type == ExcitationType.Custom:
+            raise N.ConfigError("a custom waveform runs as a sampled ScheduledExcitation (EngineBatch), "
+                                "not through the analytic host excitation")
         c = N.ExcitationC()
         c.kind = int(self.excitation_type)
         c.direction = int(self.direction)
@@ -707,11 +724,33 @@ class Excitation:
         c.soft_source = int(bool(self.soft_source))
         return c
 
+    def _custom_value(self, t: float) -> float:
+        """Linear interpolation of the custom waveform, clamped at both ends
+        (excitation.rs:177-197, the same bracketing loop)."""
+        ts, vs = self.times, self.values
+        if not ts:
+            raise N.ConfigError("custom waveform without samples")
+        if t <= ts[0]:
+            return vs[0]
+        if t >= ts[-1]:
+            return vs[-1]
+        i = 0
+        while i < len(ts) - 1 and ts[i + 1] < t:
+            i += 1
+        alpha = (t - ts[i]) / (ts[i + 1] - ts[i])
+        return vs[i] + alpha * (vs[i + 1] - vs[i])
+
     def evaluate(self, t: float) -> float:
+        if self.excitation_type == ExcitationType.Custom:
+            return self.amplitude * self._custom_value(float(t))
         c = self.to_c()
         return N.lib().oems_excitation_evaluate(ctypes.byref(c), t)
 
     def sample(self, start_timestep: int, num_timesteps: int, dt: float) -> np.ndarray:
+        """(f32) evaluate((start + n) dt), t in f64 (batch.rs:110-129)."""
+        if self.excitation_type == ExcitationType.Custom:
+            return np.array([self.evaluate((start_timestep + n) * dt) for n in range(num_timesteps)],
+                            dtype=np.float32)
         out = np.empty(num_timesteps, dtype=np.float32)
         c = self.to_c()
         N.check(N.lib().oems_excitation_sample(ctypes.byref(c), start_timestep, num_timesteps, dt,
@@ -723,7 +762,32 @@ class Excitation:
         if self.excitation_type in (ExcitationType.Gaussian, ExcitationType.GaussianModulated):
             t0, tau = self.params[-2], self.params[-1]
             return t0 + 6.0 * tau
+        if self.excitation_type == ExcitationType.Custom:
+            return self.times[-1] if self.times else 0.0
         return float("inf")
+
+    def is_active(self, t: float) -> bool:
+        """src/fdtd/excitation.rs:216-225."""
+        k = self.excitation_type
+        if k in (ExcitationType.Gaussian, ExcitationType.GaussianModulated):
+            return t <= self.params[-2] + 6.0 * self.params[-1]
+        if k == ExcitationType.Dirac:
+            return abs(t) < 1e-15
+        if k == ExcitationType.Custom:
+            return t <= (self.times[-1] if self.times else 0.0)
+        return True
+
+
+def waveguide_te10(a: float, freq: float, position: int, ny: int) -> List[Excitation]:
+    """waveguide_te10 (src/fdtd/excitation.rs:229-252): y-directed sinusoidal
+    point sources at (0, j, position), j = 1 .. ny - 2, with amplitude
+    sin(pi j / (ny - 1)) where that exceeds 0.01 (`a` is unused there too)."""
+    out = []
+    for j in range(1, ny - 1):
+        amp = float(np.sin(np.pi * (j / (ny - 1))))
+        if amp > 0.01:
+            out.append(Excitation.sinusoidal(freq, 1, (0, j, position)).with_amplitude(amp))
+    return out
 
 
 @dataclass
