@@ -20,6 +20,7 @@ numpy float32 arrays of shape (3, nx, ny, nz), z fastest.
 from __future__ import annotations
 
 import ctypes
+import math
 import enum
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
@@ -407,6 +408,15 @@ class Operator:
     def handle(self):
         return self._h
 
+    def clone(self) -> "Operator":
+        """An independent copy: grid, dt and every coefficient (the
+        reference's coefficient structs are Clone, operator.rs:21-38)."""
+        h = ctypes.c_void_p()
+        N.check(N.lib().oems_operator_clone(self._h, ctypes.byref(h)))
+        out = Operator.__new__(Operator)
+        out.grid, out.boundaries, out._h = self.grid, self.boundaries, h
+        return out
+
     def _info(self):
         dims = (N.c_u64 * 3)()
         dt = N.c_f64()
@@ -416,6 +426,11 @@ class Operator:
 
     def timestep(self) -> float:
         return self._info()[1]
+
+    def nyquist_timesteps(self, freq: float) -> int:
+        """Operator::nyquist_timesteps (src/fdtd/operator.rs:266-270): steps
+        in one period of freq, rounded up."""
+        return int(math.ceil((1.0 / freq) / self.timestep()))
 
     def dimensions(self) -> Tuple[int, int, int]:
         return tuple(int(v) for v in self._info()[0])

@@ -50,3 +50,47 @@ def test_grid_bounds_and_volume():
     c = oe.Grid.uniform(10, 10, 10, 0.001)
     volume = float(np.prod([(v[-1] - v[0]) * c.unit for v in (c.x_lines, c.y_lines, c.z_lines)]))
     assert abs(volume - 1e-6) < 1e-15
+
+
+# ---- src/fdtd/operator.rs tests module: creation, vacuum coefficients, the
+# ---- Nyquist step count, the CFL bound and coefficient copies -------------
+
+def _op5():
+    """create_test_grid (operator.rs tests): 5 cells of 1 mm per axis."""
+    lines = [0.0, 0.001, 0.002, 0.003, 0.004, 0.005]
+    return oe.Operator(oe.Grid.cartesian(lines, lines, lines), oe.BoundaryConditions.all_pec())
+
+
+def test_operator_creation_and_vacuum_coefficients():
+    op = _op5()
+    assert op.timestep() > 0.0 and op.dimensions() == (5, 5, 5)
+    c = op.coefficients()
+    for d in range(3):
+        assert abs(c[d, 2, 2, 2] - 1.0) < 1e-6          # Ca = 1
+        assert c[3 + d, 2, 2, 2] > 0.0                  # Cb = dt / (eps0 delta) > 0
+        assert abs(c[6 + d, 2, 2, 2] - 1.0) < 1e-6      # Da = 1
+        assert c[9 + d, 2, 2, 2] < 0.0                  # Db carries the minus sign
+
+
+def test_nyquist_timesteps():
+    op = _op5()
+    steps = op.nyquist_timesteps(1e9)
+    assert steps > 100 and op.nyquist_timesteps(10e9) < steps
+
+
+def test_timestep_cfl_condition():
+    """1 / 2 / 0.5 mm cells: dt below the CFL bound of the three spacings,
+    within 10% of it (the 0.99 factor)."""
+    g = oe.Grid.cartesian([0.0, 0.001, 0.002, 0.003], [0.0, 0.002, 0.004, 0.006], [0.0, 0.0005, 0.001])
+    dt = oe.Operator(g, oe.BoundaryConditions.all_pec()).timestep()
+    bound = 1.0 / (oe.C0 * np.sqrt(1.0 / 0.001 ** 2 + 1.0 / 0.002 ** 2 + 1.0 / 0.0005 ** 2))
+    assert 0.9 * bound < dt < bound
+
+
+def test_coefficient_copies():
+    """test_e_coefficient_clone / test_h_coefficient_clone: a copied operator
+    keeps the coefficients."""
+    op = _op5()
+    op.set_material(3.0, 2.0, 0.1, 0.0, (1, 4, 1, 4, 1, 4))
+    cp = op.clone()
+    assert np.array_equal(op.coefficients(), cp.coefficients())
