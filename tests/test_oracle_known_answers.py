@@ -118,6 +118,18 @@ def test_dirac_and_step():
 
 # ---- src/fdtd/batch.rs:235-294 ----------------------------------------------
 
+def test_batch_config_defaults():
+    """test_termination_config_default / test_energy_monitor_config_default:
+    no step cap, no decay threshold, checks every 100 steps; no sampling,
+    no peak tracking, no threshold (the Python mirror's defaults, which the
+    C structs take over)."""
+    import openems_b200 as oe
+    t = oe.TerminationConfig()
+    assert t.max_timesteps is None and t.energy_decay_db is None and t.check_interval == 100
+    m = oe.EnergyMonitorConfig()
+    assert m.sample_interval == 0 and not m.track_peak and m.decay_threshold is None
+
+
 def test_scheduled_samples_match_evaluate():
     """ScheduledExcitation::from_excitation: samples[i] == (f32) evaluate(i*dt)."""
     p = gaussian_params(1e9, 0.5)
