@@ -230,6 +230,36 @@ def test_current_probe_sums():
     assert t.terms == [] and abs(_probe_value(t, lambda f: f[4].fill(1.0))) < 1e-10
 
 
+def test_engine_interface_integrals():
+    """test_voltage_integral / test_current_integral_{y,z}_normal
+    (src/fdtd/engine_interface.rs tests module): E_x = 100 V/m over 5 cells
+    of 1 mm integrates to -0.5 V (V = -sum E dl); uniform H through a y- or
+    z-normal surface gives a non-zero current."""
+    import openems_b200 as oe
+    op = oe.Operator(oe.Grid.uniform(10, 10, 10, 1e-3), oe.BoundaryConditions.all_pec())
+    v = _probe_value(oe.voltage_integral(op, (0, 5, 5), (5, 5, 5)), lambda f: f[0].fill(100.0))
+    assert v < 0.0 and abs(v - (-0.5)) < 1e-12
+
+    def yfill(f):
+        f[3].fill(1.0)
+        f[5].fill(0.5)
+
+    def zfill(f):
+        f[3].fill(1.0)
+        f[4].fill(0.5)
+    assert abs(_probe_value(oe.current_integral(op, (0, 5, 0), (5, 5, 5), 1), yfill)) > 0.0
+    assert abs(_probe_value(oe.current_integral(op, (0, 0, 5), (5, 5, 5), 2), zfill)) > 0.0
+
+
+def test_constants():
+    """src/constants.rs tests: Z0 = MU0 C0, C0 = 1 / sqrt(EPS0 MU0), and a
+    1 GHz wavelength of 0.299792458 m."""
+    from openems_b200.constants import C0, EPS0, MU0, Z0
+    assert abs(Z0 - MU0 * C0) < 1e-6
+    assert abs(C0 - 1.0 / np.sqrt(EPS0 * MU0)) < 1.0
+    assert abs(C0 / 1e9 - 0.299792458) < 1e-6
+
+
 def test_voltage_integral_weights_and_sign():
     """V = -sum E . dl (src/fdtd/engine_interface.rs:206-247)."""
     import openems_b200 as oe
