@@ -251,11 +251,19 @@ oems_status oems_operator_create_uniform(uint64_t nx, uint64_t ny, uint64_t nz, 
 
 void oems_operator_destroy(oems_operator* op) { delete op; }
 
+// Finite, positive permittivity and permeability, finite non-negative
+// conductivities: anything else (NaN or infinite parameters included)
+// would put non-finite numbers into the coefficients.
+static bool material_ok(double eps_r, double mu_r, double sigma_e, double sigma_m) {
+  return std::isfinite(eps_r) && eps_r > 0.0 && std::isfinite(mu_r) && mu_r > 0.0 && std::isfinite(sigma_e) &&
+         sigma_e >= 0.0 && std::isfinite(sigma_m) && sigma_m >= 0.0;
+}
+
 oems_status oems_operator_set_material(oems_operator* op, double eps_r, double mu_r, double sigma_e, double sigma_m,
                                        const uint64_t region[6]) {
   if (!op || !region) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (!(eps_r > 0.0) || !(mu_r > 0.0) || sigma_e < 0.0 || sigma_m < 0.0)
-    return hfail(OEMS_ERR_MATERIAL, "eps_r and mu_r must be positive, conductivities non-negative");
+  if (!material_ok(eps_r, mu_r, sigma_e, sigma_m))
+    return hfail(OEMS_ERR_MATERIAL, "eps_r and mu_r must be positive, conductivities non-negative, all finite");
   uint64_t r[6];
   clip_region(op, region, r);
   // src/fdtd/operator.rs:195-220
@@ -288,8 +296,8 @@ oems_status oems_operator_set_material(oems_operator* op, double eps_r, double m
 oems_status oems_operator_set_material_cells(oems_operator* op, double eps_r, double mu_r, double sigma_e,
                                              double sigma_m, const uint64_t* cells, uint64_t ncells) {
   if (!op || (!cells && ncells)) return hfail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (!(eps_r > 0.0) || !(mu_r > 0.0) || sigma_e < 0.0 || sigma_m < 0.0)
-    return hfail(OEMS_ERR_MATERIAL, "eps_r and mu_r must be positive, conductivities non-negative");
+  if (!material_ok(eps_r, mu_r, sigma_e, sigma_m))
+    return hfail(OEMS_ERR_MATERIAL, "eps_r and mu_r must be positive, conductivities non-negative, all finite");
   for (uint64_t m = 0; m < ncells; ++m)
     if (cells[3 * m] >= op->n[0] || cells[3 * m + 1] >= op->n[1] || cells[3 * m + 2] >= op->n[2])
       return hfail(OEMS_ERR_MATERIAL, "material cell outside the grid");

@@ -319,3 +319,28 @@ def test_probes_and_dft_match_oracle(kernels):
     for d, od in zip(dfts, odfts):
         g, r = eng.probe_dft(d), s.probe_dft(od)
         assert np.abs(g - r).max() <= 1e-12 * np.abs(r).max() + 1e-300
+
+
+def test_corrupted_coefficient_is_reported_as_numerical_error():
+    """Fault injection on the host: one coefficient of the operator set to
+    NaN before the engine copies it.  The run's energy check sees the
+    non-finite energy and the batch ends with NumericalError (no clamping,
+    no device fault); the same engine resets and runs on cleanly after the
+    field is written again."""
+    import ctypes
+    from openems_b200 import _native as N
+    op = oe.Operator(oe.Grid.uniform(16, 16, 16, 1e-3), oe.BoundaryConditions.all_pec())
+    ptrs = (N.PF * 12)()
+    N.check(N.lib().oems_operator_coefficients(op.handle, ptrs))
+    ca0 = ctypes.cast(ptrs[0], ctypes.POINTER(ctypes.c_float))
+    ca0[(8 * 16 + 8) * 16 + 8] = float("nan")  # Ca_x of cell (8, 8, 8)
+    eng = oe.Engine(op)
+    e = np.zeros((3, 16, 16, 16), np.float32)
+    e[0, 8, 8, 8] = 1.0
+    eng.write_fields(e, np.zeros_like(e))
+    with pytest.raises(oe.NumericalError):
+        eng.run_batch(oe.EngineBatch(num_steps=200, excitations=[],
+                                     energy_monitoring=oe.EnergyMonitorConfig(sample_interval=10)))
+    eng.reset()
+    assert eng.current_timestep() == 0 and not np.any(np.concatenate(eng.read_fields()))
+    eng.close()

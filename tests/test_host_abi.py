@@ -95,6 +95,15 @@ def test_region_clipping_and_validation():
     op.set_material(2.0, 1.0, 0.0, 0.0, (2, 100, 0, 100, 0, 100))  # clipped, no error
     with pytest.raises(oe.MaterialError):
         op.set_material(-1.0, 1.0, 0.0, 0.0, (0, 1, 0, 1, 0, 1))
+    # non-finite parameters would put NaN / inf into the coefficients: refused
+    before = op.coefficients().copy()
+    for bad in ((np.nan, 1.0, 0.0, 0.0), (np.inf, 1.0, 0.0, 0.0), (2.0, np.inf, 0.0, 0.0),
+                (2.0, 1.0, np.nan, 0.0), (2.0, 1.0, np.inf, 0.0), (2.0, 1.0, 0.0, np.nan)):
+        with pytest.raises(oe.MaterialError):
+            op.set_material(*bad, (0, 2, 0, 2, 0, 2))
+        with pytest.raises(oe.MaterialError):
+            op.set_material_cells(*bad, [(1, 1, 1)])
+    assert np.array_equal(op.coefficients(), before)
     with pytest.raises(oe.GridError):
         oe.Operator(oe.Grid([0.0, 1.0, 0.5], [0.0, 1.0], [0.0, 1.0]))
 
