@@ -320,16 +320,35 @@ def run(cfg: SimulationConfig, device: int = -1, batch: int = 1000, storage: str
 
 
 def main(argv: Optional[Sequence[str]] = None):
-    """python -m openems_b200.xml_config FILE.xml [--no-simulation] [--storage f16]
-    (the reference's command line, src/main.rs:100-160); prints one JSON line."""
+    """python -m openems_b200.xml_config FILE.xml [--no-simulation]
+    [--dump-statistics] [--storage f16] with the reference's flags
+    (src/main.rs:15-53, 100-185); prints one JSON line.  --engine names
+    the reference's CPU engines and is kept for its command lines: every run
+    uses the CUDA engine.  --num-threads, --disable-dumps, --debug-material
+    and --debug-operator are accepted and, as in the reference, change
+    nothing.  --dump-statistics writes FILE.stats.json with the reference's
+    keys."""
     import argparse
     import json
+    import os
+    import sys
     p = argparse.ArgumentParser(description="run an openEMS XML configuration on the B200 engine")
     p.add_argument("input")
     p.add_argument("--no-simulation", action="store_true", help="parse and set up only")
+    p.add_argument("--dump-statistics", action="store_true", help="write FILE.stats.json")
+    p.add_argument("--engine", default="cuda", help="basic | simd | parallel | cuda (all run on the GPU)")
+    p.add_argument("--num-threads", type=int, default=0)
+    p.add_argument("--disable-dumps", action="store_true")
+    p.add_argument("--debug-material", action="store_true")
+    p.add_argument("--debug-operator", action="store_true")
+    p.add_argument("-v", "--verbose", type=int, default=1)
     p.add_argument("--storage", choices=("f32", "f16", "bf16"), default="f32")
     p.add_argument("--batch", type=int, default=1000)
     a = p.parse_args(argv)
+    if a.engine not in ("basic", "simd", "parallel", "cuda") and a.verbose > 0:
+        print(f"unknown engine type '{a.engine}', using the CUDA engine", file=sys.stderr)
+    if not os.path.exists(a.input):
+        raise SystemExit(f"input file not found: {a.input}")
     cfg = parse_config(a.input)
     if a.no_simulation:
         b = build(cfg)
@@ -337,7 +356,14 @@ def main(argv: Optional[Sequence[str]] = None):
                           "timestep": b.operator.timestep(), "boundaries": cfg.boundaries}))
         return
     r = run(cfg, batch=a.batch, storage=a.storage)
-    r.pop("engine")
+    eng = r.pop("engine")
+    if a.dump_statistics:
+        # the reference's keys (main.rs:163-172): simulated time is steps x dt
+        stats = {"timesteps": r["timesteps"], "sim_time": r["timesteps"] * eng.dt, "wall_time": r["wall_s"],
+                 "peak_energy": r["peak_energy"], "final_energy": r["energy"],
+                 "speed_mcells_per_sec": r["mcells_per_s"]}
+        with open(os.path.splitext(a.input)[0] + ".stats.json", "w") as f:
+            json.dump(stats, f, indent=2)
     print(json.dumps(r))
 
 

@@ -62,3 +62,19 @@ def test_reference_python_surface_cavity_matches_oracle():
     # peak over the energy samples (every 100 steps): the source is still
     # feeding the cavity at step 120, so the final energy can exceed it
     assert st.peak_energy > 0
+
+
+def test_command_line_dumps_statistics(tmp_path, capsys):
+    """--dump-statistics writes FILE.stats.json with the reference's keys
+    (src/main.rs:163-172) after the run."""
+    import json
+    from openems_b200 import xml_config as X
+    from test_xml_config import PATCH
+    f = tmp_path / "patch.xml"
+    f.write_text(PATCH)
+    X.main([str(f), "--dump-statistics", "--batch", "200"])
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    st = json.loads((tmp_path / "patch.stats.json").read_text())
+    assert set(st) == {"timesteps", "sim_time", "wall_time", "peak_energy", "final_energy", "speed_mcells_per_sec"}
+    assert st["timesteps"] == out["timesteps"] > 0 and st["speed_mcells_per_sec"] > 0
+    assert st["sim_time"] > 0 and st["peak_energy"] >= st["final_energy"] >= 0

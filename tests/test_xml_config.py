@@ -93,6 +93,21 @@ def test_command_line_without_simulation(tmp_path, capsys):
     assert out["dims"] == [16, 12, 8] and out["sources"] == 2 and out["boundaries"] == [3, 3, 3, 2, 0, 0]
 
 
+def test_command_line_accepts_the_reference_flags(tmp_path, capsys):
+    """The reference's flags (src/main.rs:15-53) parse; the engine names of
+    its CPU engines run on the GPU engine, and the debug / thread flags
+    change nothing (as in the reference)."""
+    f = tmp_path / "patch.xml"
+    f.write_text(PATCH)
+    X.main([str(f), "--no-simulation", "--engine", "parallel", "--num-threads", "4", "--disable-dumps",
+            "--debug-material", "--debug-operator", "-v", "0", "--dump-statistics"])
+    out = json.loads(capsys.readouterr().out)
+    assert out["dims"] == [16, 12, 8]
+    assert not (tmp_path / "patch.stats.json").exists()  # no run, no statistics
+    with pytest.raises(SystemExit):
+        X.main([str(tmp_path / "missing.xml"), "--no-simulation"])
+
+
 def test_waveform_of_the_fdtd_excitation():
     """Type 0 with centre f0 and cutoff fc: a pulse without carrier (tau =
     1 / (pi fc), t0 = 4 tau) for f0 = 0, else modulated at f0 with the same
