@@ -24,7 +24,7 @@ makes the decision from more of what is known at K:
 
 An instance is accepted at the first stage whose predicted error is below a
 threshold chosen on held-back validation instances of the training family
-(the largest one that keeps every validation instance within 0.5 dB, judged
+(the largest one that keeps every validation instance within 0.5 dB, assessed
 on the network's out-of-sample predictions).  Every product (forward, input and weight
 gradients) is oems_tc_gemm_bf16 (tcgen05, bf16 operands, f32 accumulation);
 the causal convolutions are oems_pk_im2col_causal / col2im_causal, the rest

@@ -75,7 +75,7 @@ def test_cpml_against_fp64_oracle(storage):
     """With CPML the pulse has left the box after 300 steps: the final fields
     are the small static remainder of the source's DC part (H almost zero),
     whose relative error in 2-byte storage is larger than that of the pulse.
-    The run is judged by the Ez / Hy probe traces over all its steps, the
+    The run is assessed by the Ez / Hy probe traces over all its steps, the
     final E by twice the bound."""
     sc = modulated_cube(32, 300, oe.CpmlBoundaries.uniform(6))
     sc.probes = [(c, p) for p in [(10, 16, 16), (16, 22, 12), (20, 12, 18)] for c in (2, 4)]
