@@ -319,15 +319,40 @@ def run(cfg: SimulationConfig, device: int = -1, batch: int = 1000, storage: str
     return run_operator(b.operator, excs, cap, end_db, b.mur_faces, device, batch, storage)
 
 
+def debug_dumps(op: "fdtd.Operator", stem: str, material: bool, operator: bool) -> List[str]:
+    """The --debug-material / --debug-operator files of an operator (cell
+    data on its mesh lines); returns the paths written."""
+    from . import field_io
+    g = op.grid
+    lines = [np.asarray(v, dtype=np.float64) * g.unit for v in (g.x_lines, g.y_lines, g.z_lines)]
+    c = op.coefficients()
+    out = []
+    if material:
+        ids, _ = fdtd.compress_coefficients(c)
+        path = stem + ".material.vtk"
+        field_io.write_field_vtk(path, ids.astype(np.float32), lines, "material")
+        out.append(path)
+    if operator:
+        for k, name in enumerate(("ca", "cb", "da", "db")):
+            path = stem + "." + name + ".vtk"
+            field_io.write_vector_field_vtk(path, c[3 * k:3 * k + 3], lines, name.capitalize())
+            out.append(path)
+    return out
+
+
 def main(argv: Optional[Sequence[str]] = None):
     """python -m openems_b200.xml_config FILE.xml [--no-simulation]
     [--dump-statistics] [--storage f16] with the reference's flags
     (src/main.rs:15-53, 100-185); prints one JSON line.  --engine names
     the reference's CPU engines and is kept for its command lines: every run
-    uses the CUDA engine.  --num-threads, --disable-dumps, --debug-material
-    and --debug-operator are accepted and, as in the reference, change
-    nothing.  --dump-statistics writes FILE.stats.json with the reference's
-    keys."""
+    uses the CUDA engine.  --num-threads and --disable-dumps are accepted
+    and, as in the reference, change nothing.  --debug-material writes
+    FILE.material.vtk (each cell's material: its index among the distinct
+    coefficient sets, oems_compress_coefficients) and --debug-operator
+    FILE.ca.vtk / .cb.vtk / .da.vtk / .db.vtk (the coefficients as vector
+    fields), legacy VTK as the reference's writer; the reference parses the
+    two flags but writes nothing.  --dump-statistics writes FILE.stats.json
+    with the reference's keys."""
     import argparse
     import json
     import os
@@ -350,6 +375,8 @@ def main(argv: Optional[Sequence[str]] = None):
     if not os.path.exists(a.input):
         raise SystemExit(f"input file not found: {a.input}")
     cfg = parse_config(a.input)
+    if a.debug_material or a.debug_operator:
+        debug_dumps(build(cfg).operator, os.path.splitext(a.input)[0], a.debug_material, a.debug_operator)
     if a.no_simulation:
         b = build(cfg)
         print(json.dumps({"dims": list(b.operator.dimensions()), "sources": len(b.sources),

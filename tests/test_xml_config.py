@@ -108,6 +108,30 @@ def test_command_line_accepts_the_reference_flags(tmp_path, capsys):
         X.main([str(tmp_path / "missing.xml"), "--no-simulation"])
 
 
+def test_debug_dumps(tmp_path):
+    """--debug-material: one cell value per material (vacuum, substrate,
+    PEC sheet); --debug-operator: the coefficients as VTK vector fields."""
+    from openems_b200.field_io import write_field_vtk
+    f = tmp_path / "patch.xml"
+    f.write_text(PATCH)
+    X.main([str(f), "--no-simulation", "--debug-material", "--debug-operator"])
+    mat = (tmp_path / "patch.material.vtk").read_text().splitlines()
+    n = mat.index("LOOKUP_TABLE default")
+    vals = np.array([float(v) for v in mat[n + 1:]])
+    assert len(vals) == 16 * 12 * 8 and set(np.unique(vals)) >= {0.0, 1.0, 2.0}
+    op = X.build(X.parse_config(str(f))).operator
+    ids, table = oe.compress_coefficients(op.coefficients())
+    assert np.array_equal(vals.reshape(16, 12, 8), ids.astype(np.float64))
+    # the same writer gives the same bytes
+    g = op.grid
+    lines = [np.asarray(v) * g.unit for v in (g.x_lines, g.y_lines, g.z_lines)]
+    write_field_vtk(tmp_path / "again.vtk", ids.astype(np.float32), lines, "material")
+    assert (tmp_path / "again.vtk").read_text() == (tmp_path / "patch.material.vtk").read_text()
+    for name in ("ca", "cb", "da", "db"):
+        txt = (tmp_path / f"patch.{name}.vtk").read_text()
+        assert f"VECTORS {name.capitalize()} float" in txt and txt.count("\n") > 16 * 12 * 8
+
+
 def test_waveform_of_the_fdtd_excitation():
     """Type 0 with centre f0 and cutoff fc: a pulse without carrier (tau =
     1 / (pi fc), t0 = 4 tau) for f0 = 0, else modulated at f0 with the same
