@@ -12,7 +12,7 @@ from .constants import C0, EPS0, MU0, Z0  # noqa: F401
 from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, MurAbcConfig, Operator,  # noqa: F401
                    Excitation, ExcitationType, ScheduledExcitation, TerminationConfig,
                    EnergyMonitorConfig, EngineBatch, TerminationReason, EnergySample, BatchResult,
-                   EngineType, Engine, EndCondition, SimulationStats, Simulation,
+                   EngineType, Engine, EndCondition, SimulationStats, Simulation, SimulationState, TimestepInfo,
                    ProbeTerms, voltage_probe, current_probe, voltage_integral, current_integral,
                    port_probe, LumpedPort, DrudeMaterial, LorentzMaterial, DebyeMaterial,
                    RlcType, RlcElement, Nf2ffBox, Nf2ffResults, nf2ff_surface, PmlBoundaries,

@@ -1481,6 +1481,55 @@ class EndCondition:
 
 
 @dataclass
+class TimestepInfo:
+    """TimestepInfo (src/fdtd/timestep.rs:7-75): dt = 0.99 of the 3D CFL
+    limit of the grid's smallest spacings, the Nyquist frequency, the cell
+    count and the reference's memory estimate (18 f32 arrays per cell)."""
+
+    dt: float
+    dt_max: float
+    nyquist_freq: float
+    num_cells: int
+    memory_bytes: int
+
+    @classmethod
+    def calculate(cls, grid: Grid) -> "TimestepInfo":
+        from .constants import C0
+        dx, dy, dz = grid.cell_size()
+        nx, ny, nz = grid.dimensions()
+        dt_max = 1.0 / (C0 * math.sqrt(1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz)))
+        dt = 0.99 * dt_max
+        n = nx * ny * nz
+        return cls(dt, dt_max, 1.0 / (2.0 * dt), n, n * 18 * 4)
+
+    def timesteps_for_duration(self, duration: float) -> int:
+        return int(math.ceil(duration / self.dt))
+
+    def timesteps_per_period(self, frequency: float) -> float:
+        return 1.0 / (frequency * self.dt)
+
+    def memory_display(self) -> str:
+        b = float(self.memory_bytes)
+        if b < 1024.0:
+            return f"{b:.0f} B"
+        if b < 1024.0 ** 2:
+            return f"{b / 1024.0:.2f} KB"
+        if b < 1024.0 ** 3:
+            return f"{b / 1024.0 ** 2:.2f} MB"
+        return f"{b / 1024.0 ** 3:.2f} GB"
+
+
+class SimulationState(enum.Enum):
+    """SimulationState (src/fdtd/simulation.rs:21-32)."""
+
+    Created = 0
+    Ready = 1
+    Running = 2
+    Finished = 3
+    Stopped = 4
+
+
+@dataclass
 class SimulationStats:
     timesteps: int
     sim_time: float
@@ -1508,6 +1557,9 @@ class Simulation:
         self.batch_size: Optional[int] = None
         self.device = device
         self.flags = N.ENGINE_COMPRESSED if compressed else 0
+        self.verbose = 1
+        self.show_progress = True
+        self._state = SimulationState.Created
         self._sim = None
 
     def __del__(self):
@@ -1538,6 +1590,31 @@ class Simulation:
         self.batch_size = n
         return self
 
+    def set_engine_type(self, engine_type: "EngineType"):
+        """Only EngineType.Cuda exists; the reference's CPU engine types are
+        refused like in Engine()."""
+        if engine_type is not EngineType.Cuda:
+            raise N.ConfigError("only the CUDA engine exists")
+        return self
+
+    def set_verbose(self, level: int):
+        """Kept for the reference's builder chain (its log level); this
+        mirror logs nothing."""
+        self.verbose = int(level)
+        return self
+
+    def set_show_progress(self, show: bool):
+        """Kept for the reference's builder chain (its progress bar); this
+        mirror draws none."""
+        self.show_progress = bool(show)
+        return self
+
+    def timestep_info(self) -> TimestepInfo:
+        return TimestepInfo.calculate(self.grid)
+
+    def state(self) -> SimulationState:
+        return self._state
+
     def timestep(self) -> float:
         return self.operator.timestep()
 
@@ -1559,12 +1636,20 @@ class Simulation:
             d = CpmlBoundaries(layers=layers).to_c()
             N.check(N.lib().oems_simulation_set_cpml(h, ctypes.byref(d)))
         N.check(N.lib().oems_simulation_setup(h))
+        self._state = SimulationState.Ready
 
     def run(self) -> SimulationStats:
-        if self._sim is None:
+        """Sets up if needed, then runs (Simulation::run, simulation.rs:200-360):
+        the state goes Ready -> Running -> Finished; a second run is refused
+        as in the reference."""
+        if self._state == SimulationState.Created:
             self.setup()
+        if self._state != SimulationState.Ready:
+            raise N.ConfigError("Simulation not ready to run")
+        self._state = SimulationState.Running
         st = N.SimulationStatsC()
         N.check(N.lib().oems_simulation_run(self._sim, ctypes.byref(st)))
+        self._state = SimulationState.Finished
         return SimulationStats(int(st.timesteps), st.sim_time, st.wall_time, st.peak_energy,
                                st.final_energy, st.speed_mcells_per_sec)
 

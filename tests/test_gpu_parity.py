@@ -239,8 +239,12 @@ def test_simulation_run_api():
     g = oe.Grid.uniform(32, 32, 32, 1e-3)
     sim = oe.Simulation(g, oe.BoundaryConditions.all_pec())
     sim.add_excitation(oe.Excitation.gaussian(5e9, 0.5, 2, (16, 16, 16)))
-    sim.set_end_condition(oe.EndCondition.timesteps(2500))
+    sim.set_end_condition(oe.EndCondition.timesteps(2500)).set_verbose(0).set_show_progress(False)
+    assert sim.state() is oe.SimulationState.Created
     st = sim.run()
+    assert sim.state() is oe.SimulationState.Finished
+    with pytest.raises(oe.ConfigError):  # a second run, as in the reference
+        sim.run()
     assert st.timesteps == 2500
     assert st.speed_mcells_per_sec > 0
     assert np.isfinite(st.final_energy) and st.final_energy > 0
@@ -257,6 +261,18 @@ def test_simulation_run_api():
         s.run_batch(n, sample_interval=100, track_peak=True)
     e, h = s.energy()
     assert st.final_energy == pytest.approx(e + h, rel=1e-10)
+
+
+def test_simulation_basic():
+    """test_simulation_basic (src/fdtd/simulation.rs tests): 20^3, 100 steps
+    of a 1 GHz Gaussian."""
+    sim = oe.Simulation(oe.Grid.uniform(20, 20, 20, 1e-3))
+    sim.set_end_condition(oe.EndCondition.timesteps(100)).set_verbose(0).set_show_progress(False)
+    sim.add_excitation(oe.Excitation.gaussian(1e9, 0.5, 2, (10, 10, 10)))
+    sim.setup()
+    assert sim.state() is oe.SimulationState.Ready
+    st = sim.run()
+    assert st.timesteps == 100 and st.speed_mcells_per_sec > 0.0
 
 
 def test_energy_decay_end_condition_stops_simulation():

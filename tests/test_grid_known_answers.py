@@ -94,3 +94,33 @@ def test_coefficient_copies():
     op.set_material(3.0, 2.0, 0.1, 0.0, (1, 4, 1, 4, 1, 4))
     cp = op.clone()
     assert np.array_equal(op.coefficients(), cp.coefficients())
+
+
+
+# ---- src/fdtd/timestep.rs and the Simulation's host-side surface -------------
+
+def test_timestep_info():
+    """TimestepInfo::calculate: dt = 0.99 of the CFL limit (the operator's
+    dt), Nyquist 1 / (2 dt), 18 f32 arrays per cell."""
+    g = oe.Grid.cartesian([0.0, 0.001, 0.002, 0.003], [0.0, 0.002, 0.004, 0.006], [0.0, 0.0005, 0.001])
+    ti = oe.TimestepInfo.calculate(g)
+    assert ti.dt == pytest.approx(0.99 * ti.dt_max, rel=1e-15)
+    assert ti.dt == pytest.approx(oe.Operator(g, oe.BoundaryConditions.all_pec()).timestep(), rel=1e-12)
+    assert ti.nyquist_freq == pytest.approx(1.0 / (2.0 * ti.dt))
+    assert ti.num_cells == 3 * 3 * 2 and ti.memory_bytes == 18 * 18 * 4
+    assert ti.timesteps_for_duration(10 * ti.dt) == 10
+    assert ti.timesteps_per_period(1.0 / (7 * ti.dt)) == pytest.approx(7.0)
+    assert ti.memory_display() == "1.27 KB"
+    assert oe.TimestepInfo.calculate(oe.Grid.uniform(2, 2, 2, 1e-3)).memory_display() == "576 B"
+    assert oe.TimestepInfo.calculate(oe.Grid.uniform(100, 100, 100, 1e-3)).memory_display() == "68.66 MB"
+
+
+def test_simulation_builder_on_the_host():
+    """The reference's builder chain before setup (no GPU needed): state
+    Created, the setters return the simulation, a CPU engine type is
+    refused (only the CUDA engine exists)."""
+    sim = oe.Simulation(oe.Grid.uniform(8, 8, 8, 1e-3))
+    assert sim.state() is oe.SimulationState.Created
+    assert sim.set_verbose(0).set_show_progress(False).set_batch_size(None) is sim
+    assert sim.set_engine_type(oe.EngineType.Cuda) is sim
+    assert sim.timestep_info().dt == pytest.approx(sim.timestep(), rel=1e-12)
