@@ -502,9 +502,12 @@ typedef struct oems_probe_term {
 
 /* Probe modes.  F32: the term values summed in order in f32, weight +1 adds
  * and weight -1 subtracts (VoltageProbe::sample / CurrentProbe::sample,
- * src/processing/probes.rs:98-239).  F64: sum of weight * value in f64
- * (EngineInterface::calc_voltage_integral / calc_current_integral,
- * src/fdtd/engine_interface.rs:208-305; port loop integrals). */
+ * src/processing/probes.rs:98-239).  F64: sum of weight * value in f64, one
+ * rounding per term (the integrals of EngineInterface::calc_voltage_integral /
+ * calc_current_integral, src/fdtd/engine_interface.rs:208-305, recorded per
+ * step, and the port loop integrals; for a current integral the reference
+ * subtracts each cell's two products before adding them, which
+ * oems_engine_integral follows). */
 #define OEMS_PROBE_SUM_F32 0
 #define OEMS_PROBE_SUM_F64 1
 
@@ -528,6 +531,61 @@ OEMS_API oems_status oems_engine_add_probe_dft(oems_engine* engine, int32_t prob
                                                const double* freqs, uint64_t nfreq, int32_t* dft_id);
 /* out: 2 * nfreq doubles (re, im per frequency). */
 OEMS_API oems_status oems_engine_read_probe_dft(oems_engine* engine, int32_t dft_id, double* out);
+
+/* ---- engine interface (EngineInterface / EngineInterfaceMut,
+ * src/fdtd/engine_interface.rs:27-595): field reads at positions, on the
+ * resident fields ---- */
+
+/* Sampled quantity: E, H (get_e_field / get_h_field, :131-154) or curl H at
+ * the snapped cell (get_rot_h_field and get_j_field, :157-206, :336-377;
+ * interpolation is ignored for it). */
+#define OEMS_SAMPLE_E 0
+#define OEMS_SAMPLE_H 1
+#define OEMS_SAMPLE_CURL_H 2
+/* InterpolationType (:12-20). */
+#define OEMS_INTERP_NONE 0
+#define OEMS_INTERP_NODE 1
+#define OEMS_INTERP_CELL 2
+
+typedef struct oems_sample_desc {
+  int32_t quantity;        /* OEMS_SAMPLE_* */
+  int32_t interpolation;   /* OEMS_INTERP_*; used with positions only */
+  const double* lines[3];  /* the grid's mesh lines per axis, in grid units */
+  uint64_t nlines[3];      /* lines per axis: the engine's cells + 1 */
+  double unit;             /* metres per grid unit (Grid::unit) */
+} oems_sample_desc;
+
+/* count queries, each either a position in metres (positions: [count][3];
+ * snapped like EngineInterface::snap_to_grid, :327-333, then read as the
+ * interpolation says) or a cell (cells: [count][3]; get_e_field_raw /
+ * get_h_field_raw, :113-128, or curl H there).  Give exactly one of the two.
+ * values: [count][3] f64, the bits of the reference's f64 arithmetic;
+ * snapped (optional): [count][3], the cell each query read at (for
+ * get_d_field / get_b_field, :165-199, which scale by the material there).
+ * Synchronous: returns after the values are in host memory. */
+OEMS_API oems_status oems_engine_sample(oems_engine* engine, const oems_sample_desc* desc, const double* positions,
+                                        const uint64_t* cells, uint64_t count, double* values, uint64_t* snapped);
+/* calc_voltage_integral (kind 0, :208-247) or calc_current_integral (kind 1,
+ * :251-305; normal_dir 0 = x, 1 = y, anything larger = z) between two
+ * positions in metres, snapped like the samples, on the current fields: the
+ * reference's loop order and f64 arithmetic (a current term's two products
+ * are subtracted before the sum takes them).  desc gives the grid; its
+ * quantity and interpolation are ignored.  Synchronous. */
+OEMS_API oems_status oems_engine_integral(oems_engine* engine, const oems_sample_desc* desc, int32_t kind,
+                                          const double start[3], const double stop[3], int32_t normal_dir,
+                                          double* value);
+/* A probe term list evaluated once on the current fields, in list order with
+ * the probes' arithmetic: with OEMS_PROBE_SUM_F32 the VoltageProbe /
+ * CurrentProbe::sample of the present step (src/processing/probes.rs:98-239).
+ * Synchronous. */
+OEMS_API oems_status oems_engine_eval_terms(oems_engine* engine, const oems_probe_term* terms, uint64_t nterms,
+                                            int32_t mode, double* value);
+/* EngineInterfaceMut::set_e_field / set_h_field / add_e_field (:542-561):
+ * field 0 = E, 1 = H; values [count][3] f32 replace (add = 0) or are added
+ * to (add != 0) the cell's three components, applied in list order.
+ * Synchronous. */
+OEMS_API oems_status oems_engine_set_cells(oems_engine* engine, int32_t field, const uint64_t* cells,
+                                           const float* values, uint64_t count, int32_t add);
 
 /* Unweighted field energies sum(E^2), sum(H^2) in f64 over the whole grid
  * (VectorField3D::energy, src/arrays/field.rs:314-316), computed on the GPU. */

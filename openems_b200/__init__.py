@@ -18,5 +18,6 @@ from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, 
                    RlcType, RlcElement, Nf2ffBox, Nf2ffResults, nf2ff_surface, PmlBoundaries,
                    PropagationDirection, Polarization, TfsfConfig, Pack, compress_coefficients,
                    waveguide_te10)
+from .engine_interface import EngineInterface, EngineInterfaceMut, InterpolationType  # noqa: F401
 
 __all__ = [n for n in dir() if not n.startswith("_")]

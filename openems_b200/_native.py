@@ -134,6 +134,14 @@ class ProbeTermC(ctypes.Structure):
 PROBE_SUM_F32 = 0
 PROBE_SUM_F64 = 1
 
+SAMPLE_E, SAMPLE_H, SAMPLE_CURL_H = 0, 1, 2
+INTERP_NONE, INTERP_NODE, INTERP_CELL = 0, 1, 2
+
+
+class SampleDescC(ctypes.Structure):
+    _fields_ = [("quantity", c_i32), ("interpolation", c_i32), ("lines", ctypes.POINTER(c_f64) * 3),
+                ("nlines", c_u64 * 3), ("unit", c_f64)]
+
 
 class MurDescC(ctypes.Structure):
     _fields_ = [("enabled", c_i32 * 6), ("order", c_i32), ("reserved0", c_i32),
@@ -262,6 +270,11 @@ SIGNATURES = {
     "oems_engine_add_probe_dft": (c_i32, [P, c_i32, ctypes.POINTER(c_f64), c_u64, ctypes.POINTER(c_i32)]),
     "oems_engine_read_probe_dft": (c_i32, [P, c_i32, ctypes.POINTER(c_f64)]),
     "oems_engine_energy": (c_i32, [P, ctypes.POINTER(c_f64), ctypes.POINTER(c_f64)]),
+    "oems_engine_sample": (c_i32, [P, ctypes.POINTER(SampleDescC), P, P, c_u64, P, P]),
+    "oems_engine_integral": (c_i32, [P, ctypes.POINTER(SampleDescC), c_i32, c_f64 * 3, c_f64 * 3, c_i32,
+                                     ctypes.POINTER(c_f64)]),
+    "oems_engine_eval_terms": (c_i32, [P, ctypes.POINTER(ProbeTermC), c_u64, c_i32, ctypes.POINTER(c_f64)]),
+    "oems_engine_set_cells": (c_i32, [P, c_i32, P, P, c_u64, c_i32]),
     "oems_status_string": (ctypes.c_char_p, [c_i32]),
     "oems_last_error_message": (ctypes.c_char_p, []),
     "oems_abi_version": (c_i32, []),

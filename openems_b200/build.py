@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "liboems_b200.so")
 SOURCES = ["csrc/engine.cu", "csrc/host.cpp", "csrc/noalloc.cu", "csrc/sweep.cpp", "csrc/predictor_kernels.cu",
            "csrc/cylindrical.cu"]
 HEADERS = ["csrc/yee_kernels.cuh", "csrc/yee_pipe.cuh", "csrc/yee_tma.cuh", "csrc/mur.cuh", "csrc/lumped_ade.cuh",
-           "csrc/fd_nf2ff.cuh", "csrc/upml.cuh", "csrc/gemm_tc.cuh", "../include/oems.h",
+           "csrc/fd_nf2ff.cuh", "csrc/upml.cuh", "csrc/interface.cuh", "csrc/gemm_tc.cuh", "../include/oems.h",
            "../include/oems_host.h", "../include/oems_predictor.h"]
 
 NVCC_FLAGS = [

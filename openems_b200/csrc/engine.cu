@@ -39,6 +39,7 @@
 #include "lumped_ade.cuh"
 #include "fd_nf2ff.cuh"
 #include "upml.cuh"
+#include "interface.cuh"
 
 namespace oems {
 
@@ -618,6 +619,7 @@ struct oems_engine {
 
   oems::DevBuf<long long> d_base;
   oems::DevBuf<int> d_err;  // device error word (bounded waits that gave up)
+  oems::DevBuf<unsigned long long> d_iface;  // queries and results of the interface reads, 8-byte words
 
   oems::LaunchShape shape;
   oems::Geom gs{};  // shell segments of a split shape
@@ -2414,6 +2416,36 @@ static oems_status add_cpml(oems_engine* en, const oems_cpml_desc* d) {
 
 using namespace oems;
 
+// Launch helpers of the engine-interface entry points.
+namespace {
+struct KSample {
+  template <typename T>
+  static void go(const SampleArgs& a, int b, int t, cudaStream_t s) { k_iface_sample<T><<<b, t, 0, s>>>(a); }
+};
+struct KTerms {
+  template <typename T>
+  static void go(const TermArgs& a, int b, int t, cudaStream_t s) { k_iface_terms<T><<<b, t, 0, s>>>(a); }
+};
+struct KIntegral {
+  template <typename T>
+  static void go(const IntegralArgs& a, int b, int t, cudaStream_t s) { k_iface_integral<T><<<b, t, 0, s>>>(a); }
+};
+struct KSet {
+  template <typename T>
+  static void go(const SetArgs& a, int b, int t, cudaStream_t s) { k_iface_set<T><<<b, t, 0, s>>>(a); }
+};
+// Launches kernel K for the engine's field storage type.
+template <typename K, typename A>
+void launch_storage(const oems_engine* en, const A& a, int blocks, int threads) {
+  if (en->storage == 1)
+    K::template go<__half>(a, blocks, threads, en->stream);
+  else if (en->storage == 2)
+    K::template go<__nv_bfloat16>(a, blocks, threads, en->stream);
+  else
+    K::template go<float>(a, blocks, threads, en->stream);
+}
+}  // namespace
+
 extern "C" {
 
 oems_status oems_engine_create(const oems_operator_desc* desc, oems_engine** out) {
@@ -3407,6 +3439,200 @@ oems_status oems_engine_energy(oems_engine* engine, double* e_energy, double* h_
   OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   if (e_energy) *e_energy = out[0];
   if (h_energy) *h_energy = out[1];
+  return OEMS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// engine interface (src/fdtd/engine_interface.rs:27-595)
+// ---------------------------------------------------------------------------
+
+
+// Checks a sample descriptor's grid against the engine; *words = the lines' count.
+static oems_status check_sample_grid(const oems_engine* en, const oems_sample_desc* d, uint64_t* words) {
+  if (!std::isfinite(d->unit) || d->unit == 0.0) return fail(OEMS_ERR_CONFIG, "grid unit must be finite and non-zero");
+  const int ext[3] = {en->nx, en->ny, en->nz};
+  *words = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const uint64_t nl = d->nlines[ax];
+    if (!d->lines[ax] || nl == 0) return fail(OEMS_ERR_INVALID_ARGUMENT, "mesh lines missing");
+    if (std::max<uint64_t>(nl, 2) - 1 != (uint64_t)ext[ax])
+      return fail(OEMS_ERR_CONFIG, "mesh lines do not match the engine's grid");
+    *words += nl;
+  }
+  return OEMS_OK;
+}
+
+// The grid part of SampleArgs, with the lines copied to words base[0..).
+static oems_status upload_sample_grid(oems_engine* en, const oems_sample_desc* d, unsigned long long* base,
+                                      SampleArgs* a) {
+  for (int c = 0; c < 6; ++c) a->f[c] = c < 3 ? en->E(c) : en->H(c - 3);
+  a->nx = en->nx;
+  a->ny = en->ny;
+  a->nz = en->nz;
+  a->nzp = en->g.nzp;
+  uint64_t off = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    a->lines[ax] = reinterpret_cast<const double*>(base + off);
+    a->nl[ax] = (int)d->nlines[ax];
+    a->sorted[ax] = std::is_sorted(d->lines[ax], d->lines[ax] + d->nlines[ax]) ? 1 : 0;
+    OEMS_CUDA(cudaMemcpyAsync(base + off, d->lines[ax], d->nlines[ax] * 8, cudaMemcpyHostToDevice, en->stream));
+    off += d->nlines[ax];
+  }
+  a->unit = d->unit;
+  a->h_inv = 1.0f / en->h_scale;
+  return OEMS_OK;
+}
+
+oems_status oems_engine_sample(oems_engine* engine, const oems_sample_desc* desc, const double* positions,
+                               const uint64_t* cells, uint64_t count, double* values, uint64_t* snapped) {
+  if (!engine || !desc) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine or descriptor");
+  if (count == 0) return OEMS_OK;
+  if (!values) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL values");
+  if ((positions != nullptr) == (cells != nullptr))
+    return fail(OEMS_ERR_INVALID_ARGUMENT, "give either positions or cells");
+  if (desc->quantity < OEMS_SAMPLE_E || desc->quantity > OEMS_SAMPLE_CURL_H)
+    return fail(OEMS_ERR_CONFIG, "sample quantity must be E, H or curl H");
+  if (desc->interpolation < OEMS_INTERP_NONE || desc->interpolation > OEMS_INTERP_CELL)
+    return fail(OEMS_ERR_CONFIG, "unknown interpolation");
+  if (count > (uint64_t)1 << 31) return fail(OEMS_ERR_CONFIG, "at most 2^31 queries per call");
+  uint64_t nl_total = 0;
+  OEMS_TRY(check_sample_grid(engine, desc, &nl_total));
+  if (cells)
+    for (uint64_t q = 0; q < count; ++q)
+      if (cells[3 * q] >= (uint64_t)engine->nx || cells[3 * q + 1] >= (uint64_t)engine->ny ||
+          cells[3 * q + 2] >= (uint64_t)engine->nz)
+        return fail(OEMS_ERR_CONFIG, "cell outside the grid");
+  EngineScope guard(engine);
+  // words: lines | queries (3 per) | values (3 per) | snapped cells (3 per)
+  const uint64_t w_q = nl_total, w_v = w_q + 3 * count, w_c = w_v + 3 * count, words = w_c + 3 * count;
+  OEMS_CUDA(engine->d_iface.ensure(words));
+  unsigned long long* base = engine->d_iface.p;
+  SampleArgs a{};
+  OEMS_TRY(upload_sample_grid(engine, desc, base, &a));
+  if (positions) {
+    a.pos = reinterpret_cast<const double*>(base + w_q);
+    OEMS_CUDA(cudaMemcpyAsync(base + w_q, positions, 3 * count * 8, cudaMemcpyHostToDevice, engine->stream));
+  } else {
+    a.cells_in = base + w_q;
+    OEMS_CUDA(cudaMemcpyAsync(base + w_q, cells, 3 * count * 8, cudaMemcpyHostToDevice, engine->stream));
+  }
+  a.count = (long long)count;
+  a.quantity = desc->quantity;
+  a.interp = desc->interpolation;
+  a.out = reinterpret_cast<double*>(base + w_v);
+  a.cells_out = base + w_c;
+  launch_storage<KSample>(engine, a, (int)((count + 127) / 128), 128);
+  OEMS_CUDA(cudaGetLastError());
+  OEMS_CUDA(cudaMemcpyAsync(values, a.out, 3 * count * 8, cudaMemcpyDeviceToHost, engine->stream));
+  if (snapped)
+    OEMS_CUDA(cudaMemcpyAsync(snapped, a.cells_out, 3 * count * 8, cudaMemcpyDeviceToHost, engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  return OEMS_OK;
+}
+
+oems_status oems_engine_integral(oems_engine* engine, const oems_sample_desc* desc, int32_t kind,
+                                 const double start[3], const double stop[3], int32_t normal_dir, double* value) {
+  if (!engine || !desc || !start || !stop || !value) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (kind != 0 && kind != 1) return fail(OEMS_ERR_CONFIG, "integral kind must be 0 (voltage) or 1 (current)");
+  if (normal_dir < 0) return fail(OEMS_ERR_CONFIG, "normal direction must be >= 0");
+  uint64_t nl_total = 0;
+  OEMS_TRY(check_sample_grid(engine, desc, &nl_total));
+  EngineScope guard(engine);
+  OEMS_CUDA(engine->d_iface.ensure(nl_total + 1));
+  unsigned long long* base = engine->d_iface.p;
+  IntegralArgs a{};
+  OEMS_TRY(upload_sample_grid(engine, desc, base, &a.s));
+  for (int ax = 0; ax < 3; ++ax) {
+    a.start[ax] = start[ax];
+    a.stop[ax] = stop[ax];
+  }
+  a.kind = kind;
+  a.normal = normal_dir;
+  a.out = reinterpret_cast<double*>(base + nl_total);
+  launch_storage<KIntegral>(engine, a, 1, 32);
+  OEMS_CUDA(cudaGetLastError());
+  OEMS_CUDA(cudaMemcpyAsync(value, a.out, 8, cudaMemcpyDeviceToHost, engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  return OEMS_OK;
+}
+
+oems_status oems_engine_eval_terms(oems_engine* engine, const oems_probe_term* terms, uint64_t nterms, int32_t mode,
+                                   double* value) {
+  if (!engine || !value || (!terms && nterms)) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (mode != OEMS_PROBE_SUM_F32 && mode != OEMS_PROBE_SUM_F64) return fail(OEMS_ERR_CONFIG, "unknown probe mode");
+  if (nterms > (uint64_t)INT32_MAX) return fail(OEMS_ERR_CONFIG, "too many terms");
+  std::vector<long long> idx(nterms);
+  std::vector<double> w(nterms);
+  std::vector<int> comp(nterms);
+  for (uint64_t t = 0; t < nterms; ++t) {
+    const oems_probe_term& q = terms[t];
+    if (q.component < 0 || q.component > 5) return fail(OEMS_ERR_CONFIG, "term component must be 0..5");
+    if (q.position[0] >= (uint64_t)engine->nx || q.position[1] >= (uint64_t)engine->ny ||
+        q.position[2] >= (uint64_t)engine->nz)
+      return fail(OEMS_ERR_CONFIG, "term position outside the grid");
+    if (!std::isfinite(q.weight)) return fail(OEMS_ERR_CONFIG, "term weight must be finite");
+    idx[t] = ((long long)q.position[0] * engine->ny + (long long)q.position[1]) * engine->g.nzp +
+             (long long)q.position[2];
+    w[t] = q.weight;
+    comp[t] = q.component;
+  }
+  EngineScope guard(engine);
+  // words: idx | w | comp (two per word) | result
+  const uint64_t w_w = nterms, w_c = 2 * nterms, w_o = w_c + (nterms + 1) / 2;
+  OEMS_CUDA(engine->d_iface.ensure(w_o + 1));
+  unsigned long long* base = engine->d_iface.p;
+  TermArgs a{};
+  for (int c = 0; c < 6; ++c) a.f[c] = c < 3 ? engine->E(c) : engine->H(c - 3);
+  a.idx = reinterpret_cast<const long long*>(base);
+  a.w = reinterpret_cast<const double*>(base + w_w);
+  a.comp = reinterpret_cast<const int*>(base + w_c);
+  a.n = (long long)nterms;
+  a.mode = mode;
+  a.h_inv = 1.0f / engine->h_scale;
+  a.out = reinterpret_cast<double*>(base + w_o);
+  if (nterms) {
+    OEMS_CUDA(cudaMemcpyAsync(base, idx.data(), nterms * 8, cudaMemcpyHostToDevice, engine->stream));
+    OEMS_CUDA(cudaMemcpyAsync(base + w_w, w.data(), nterms * 8, cudaMemcpyHostToDevice, engine->stream));
+    OEMS_CUDA(cudaMemcpyAsync(base + w_c, comp.data(), nterms * 4, cudaMemcpyHostToDevice, engine->stream));
+  }
+  launch_storage<KTerms>(engine, a, 1, 32);
+  OEMS_CUDA(cudaGetLastError());
+  OEMS_CUDA(cudaMemcpyAsync(value, a.out, 8, cudaMemcpyDeviceToHost, engine->stream));
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
+  return OEMS_OK;
+}
+
+oems_status oems_engine_set_cells(oems_engine* engine, int32_t field, const uint64_t* cells, const float* values,
+                                  uint64_t count, int32_t add) {
+  if (!engine) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL engine");
+  if (count == 0) return OEMS_OK;
+  if (!cells || !values) return fail(OEMS_ERR_INVALID_ARGUMENT, "NULL cells or values");
+  if (field != 0 && field != 1) return fail(OEMS_ERR_CONFIG, "field must be 0 (E) or 1 (H)");
+  if (count > (uint64_t)1 << 31) return fail(OEMS_ERR_CONFIG, "at most 2^31 writes per call");
+  std::vector<long long> idx(count);
+  for (uint64_t q = 0; q < count; ++q) {
+    const uint64_t* c = cells + 3 * q;
+    if (c[0] >= (uint64_t)engine->nx || c[1] >= (uint64_t)engine->ny || c[2] >= (uint64_t)engine->nz)
+      return fail(OEMS_ERR_CONFIG, "cell outside the grid");
+    idx[q] = ((long long)c[0] * engine->ny + (long long)c[1]) * engine->g.nzp + (long long)c[2];
+  }
+  EngineScope guard(engine);
+  // words: idx | values (3 floats per write)
+  const uint64_t w_v = count, words = w_v + (3 * count + 1) / 2;
+  OEMS_CUDA(engine->d_iface.ensure(words));
+  unsigned long long* base = engine->d_iface.p;
+  SetArgs a{};
+  for (int c = 0; c < 3; ++c) a.f[c] = field == 0 ? engine->E(c) : engine->H(c);
+  a.idx = reinterpret_cast<const long long*>(base);
+  a.v = reinterpret_cast<const float*>(base + w_v);
+  a.n = (long long)count;
+  a.add = add != 0;
+  a.scale = field == 1 ? engine->h_scale : 1.0f;
+  OEMS_CUDA(cudaMemcpyAsync(base, idx.data(), count * 8, cudaMemcpyHostToDevice, engine->stream));
+  OEMS_CUDA(cudaMemcpyAsync(base + w_v, values, 3 * count * 4, cudaMemcpyHostToDevice, engine->stream));
+  launch_storage<KSet>(engine, a, 1, 32);
+  OEMS_CUDA(cudaGetLastError());
+  OEMS_CUDA(cudaStreamSynchronize(engine->stream));
   return OEMS_OK;
 }
 

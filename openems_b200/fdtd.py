@@ -1300,6 +1300,20 @@ class Engine:
         from . import checkpoint
         checkpoint.unpack(self, blob)
 
+    def evaluate_probe(self, probe: "ProbeTerms") -> float:
+        """A probe's value on the present fields, with the probe's arithmetic
+        (VoltageProbe / CurrentProbe::sample, src/processing/probes.rs:98-239,
+        called between steps)."""
+        n = len(probe.terms)
+        arr = (N.ProbeTermC * max(1, n))()
+        for t, (c, pos, w) in enumerate(probe.terms):
+            arr[t].component = c
+            arr[t].position[:] = [int(v) for v in pos]
+            arr[t].weight = w
+        out = N.c_f64()
+        N.check(N.lib().oems_engine_eval_terms(self._h, arr, n, probe.mode, ctypes.byref(out)))
+        return out.value
+
     def energy(self) -> Tuple[float, float]:
         e, h = N.c_f64(), N.c_f64()
         N.check(N.lib().oems_engine_energy(self._h, ctypes.byref(e), ctypes.byref(h)))
