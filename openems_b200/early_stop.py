@@ -20,11 +20,12 @@ same instances.
 """
 from __future__ import annotations
 
+import math
 import os
 import time
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
-from typing import Dict, List, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -111,6 +112,12 @@ class StagePlan:
     max_modes: int = 40
     end_estimate: bool = True
     check: str = "max"  # residual statistic over the band: "max" or "mean" |dB difference|
+    # stage agreement: a stage is accepted only if its prediction is within
+    # agree_db (largest |dB difference| over the band) of the previous
+    # stage's; None leaves it out.  net_slack is added to the network's
+    # threshold when the agreement check is on.
+    agree_db: Optional[float] = None
+    net_slack: float = 0.0
 
     @classmethod
     def dense(cls, **kw) -> "StagePlan":
@@ -208,7 +215,10 @@ def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int
     lock = threading.Lock()
     net_lock = threading.Lock()
 
+    band = plan.band(freqs)
+
     def one(i):
+        prev = None
         for K in plan.stages:
             sw.advance(i, K, batch_steps)
             r = sw.result(i)
@@ -218,19 +228,23 @@ def staged_sweep(instances, freqs: np.ndarray, plan: StagePlan, concurrency: int
             trace = sw.trace(i)
             c = stage_check(trace, r, K, dt, freqs, horizon, decay_db, plan)
             d = c["check_mean"] if plan.check == "mean" else c["check_max"]
+            agree = s11_db_error(c["pred"], prev, band) if prev is not None else math.inf
+            prev = c["pred"]
             if net is not None:
                 x, sc = stage_features(trace, c, K, horizon, plan)
                 with net_lock:  # one forward at a time (the network keeps its activations)
                     score = float(net.predict(x[None], sc[None])[0])
-                ok = score < net.threshold
+                ok = score < net.threshold + (plan.net_slack if plan.agree_db is not None else 0.0)
             else:
                 score, ok = d, d < plan.tau
+            if plan.agree_db is not None:
+                ok = ok and agree < plan.agree_db
             with lock:
                 check_s[0] += time.perf_counter() - tc
             if ok:
                 sw.finish(i)
                 return {"s11": c["pred"], "how": "predicted", "steps": K, "stage": K, "check_db": d,
-                        "score": score, "end": c["end"]}
+                        "score": score, "agree_db": agree, "end": c["end"]}
         sw.advance(i, horizon, batch_steps)
         r = sw.result(i)
         return {"s11": r["s11"], "how": "full", "steps": r["timesteps"], "stage": None}
