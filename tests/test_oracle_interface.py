@@ -160,3 +160,33 @@ def test_snap_quirks():
     assert ref.snap([-1e-6, 0.02, float("nan")]) == (9, 9, 9)
     lines = [np.arange(N + 1) * 1.0] * 3
     assert InterfaceRef(e, h, lines, unit=1e-3).snap([0.0045, 0.0, 0.0]) == (4, 0, 0)
+
+
+# ---- the Python mirror's host-side checks (no library call reached) ----------
+
+class _HostOnlyEngine:
+    """Carries what EngineInterface reads on the host: dims and dt."""
+    dims = (10, 10, 10)
+    dt = 1e-12
+    handle = None
+
+
+def test_mirror_refuses_mismatched_grid_and_bad_shapes():
+    import openems_b200 as oe
+    eng = _HostOnlyEngine()
+    with pytest.raises(oe.ConfigError):
+        oe.EngineInterface(eng, oe.Grid.uniform(9, 10, 10, 0.001))
+    it = oe.EngineInterface(eng, oe.Grid.uniform(10, 10, 10, 0.001))
+    assert it.dt() == 1e-12 and it.dims() == (10, 10, 10) and it.timestep() == 0
+    assert it.with_interpolation(oe.InterpolationType.CellInterpolate) is it
+    with pytest.raises(oe.InvalidArgumentError):
+        it.sample(0, np.zeros((4, 2)))
+    with pytest.raises(oe.InvalidArgumentError):
+        it.with_epsilon(np.ones((3, 10, 10, 9), np.float32))
+    with pytest.raises(oe.ConfigError):
+        it.calc_current_integral([0, 0, 0], [1, 1, 1], -1)
+    m = oe.EngineInterfaceMut(eng, oe.Grid.uniform(10, 10, 10, 0.001))
+    with pytest.raises(oe.InvalidArgumentError):
+        m.set_e_fields([[1, 2, 3], [4, 5, 6]], [[1.0, 2.0, 3.0]])
+    m.set_time(7, 3e-12)
+    assert (m.timestep, m.time, m.dt()) == (7, 3e-12, 1e-12)
