@@ -145,27 +145,34 @@ class Processing:
     def record(self, engine) -> "Processing":
         """Record every probe at each step of the engine's following batches."""
         key = id(engine)
+        # the engine is kept with its probe ids, so its id stays its own
         for p in self.voltage_probes + self.current_probes:
-            p._ids[key] = engine.add_probe(p.terms())
+            p._ids[key] = (engine, engine.add_probe(p.terms()))
         for p in self.field_probes:
-            p._ids[key] = [engine.add_point_probe(c, p.position) for c in range(6)]
+            p._ids[key] = (engine, [engine.add_point_probe(c, p.position) for c in range(6)])
         return self
+
+    @staticmethod
+    def _recorded(p, engine):
+        e = p._ids.get(id(engine))
+        return e[1] if e is not None and e[0] is engine else None
 
     def collect(self, engine) -> int:
         """Append the recorded steps of the engine's most recent batch; returns
         the number of steps."""
-        key = id(engine)
         tr = engine.probe_traces()
         steps = tr.shape[0]
         end = engine.current_timestep()
         times = [(end - steps + 1 + s) * engine.dt for s in range(steps)]
         for p in self.voltage_probes + self.current_probes:
-            if key in p._ids:
+            pid = self._recorded(p, engine)
+            if pid is not None:
                 p.times.extend(times)
-                p.values.extend(tr[:, p._ids[key]].tolist())
+                p.values.extend(tr[:, pid].tolist())
         for p in self.field_probes:
-            if key in p._ids:
-                cols = tr[:, p._ids[key]]
+            pids = self._recorded(p, engine)
+            if pids is not None:
+                cols = tr[:, pids]
                 p.times.extend(times)
                 p.e_values.extend(tuple(r[:3]) for r in cols.tolist())
                 p.h_values.extend(tuple(r[3:]) for r in cols.tolist())

@@ -58,3 +58,48 @@ def test_bin_rounding():
     assert _bin(0.49999999999999994, 1, 1.0) == 0
     assert _bin(-3.0, 1, 1.0) == 0 and _bin(float("nan"), 1, 1.0) == 0
     assert _bin(float("inf"), 1, 1.0) >= 1 << 63
+
+
+class _FakeEngine:
+    """Records probe registrations and serves fixed traces (host logic only)."""
+
+    def __init__(self):
+        self.n, self.dt, self.step = 0, 2e-12, 0
+        self.traces = None
+
+    def add_probe(self, terms):
+        self.n += 1
+        return self.n - 1
+
+    def add_point_probe(self, c, pos):
+        self.n += 1
+        return self.n - 1
+
+    def probe_traces(self):
+        return self.traces
+
+    def current_timestep(self):
+        return self.step
+
+
+def test_record_and_collect_columns_and_times():
+    """record registers the probes in order (a field probe takes six columns);
+    collect appends each probe's column with time = step count x dt, and
+    only for the engine it was recorded on."""
+    p = Processing()
+    p.add_voltage_probe(VoltageProbe("v", (0, 0, 0), (0, 0, 3), 2))
+    p.add_field_probe(FieldProbe("f", (1, 1, 1)))
+    p.add_current_probe(CurrentProbe("i", (0, 0, 1), (2, 2, 1), 2))
+    eng, other = _FakeEngine(), _FakeEngine()
+    p.record(eng)
+    assert eng.n == 1 + 1 + 6
+    eng.traces = np.arange(3 * 8, dtype=np.float64).reshape(3, 8)
+    eng.step = 10
+    assert p.collect(eng) == 3
+    v, i, f = p.voltage_probes[0], p.current_probes[0], p.field_probes[0]
+    assert v.values == [0.0, 8.0, 16.0] and i.values == [1.0, 9.0, 17.0]
+    assert f.e_values[0] == (2.0, 3.0, 4.0) and f.h_values[2] == (21.0, 22.0, 23.0)
+    assert v.times == [8 * 2e-12, 9 * 2e-12, 10 * 2e-12]
+    other.traces = np.zeros((2, 8))
+    p.collect(other)
+    assert len(v.values) == 3
