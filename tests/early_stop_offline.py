@@ -6,12 +6,14 @@ them (test_gpu_sweep.py::test_sweep_instance_matches_oracle), and keeps
 their port traces, energy samples and full-run S11.  It then replays a
 StagePlan's decisions instance by instance as staged_sweep would.  At each
 stage the engine's port DFTs of the first K steps are rebuilt from the
-trace, and check_instance runs on them.  The result is the step ratio
+trace, and stage_check runs on them.  The result is the step ratio
 against the plain runs and every stopped instance's S11 error.
 
     python tests/early_stop_offline.py --seed 50 --count 80 [--cache DIR]
+        [--net [--agree DB --slack S]]
 
-prints the standard and the dense plan side by side.  The step ratio is an
+prints the standard and the dense plan side by side (with --net: the dense
+plan accepted by the trained network, optionally with stage agreement).  The step ratio is an
 upper bound on the sweep's instances/hour ratio: the GPU sweep also pays for
 pauses and host checks.
 """
@@ -76,22 +78,45 @@ def level_db(rec: dict, K: int) -> float:
     return float(10 * np.log10(tot[-1] / tot.max())) if tot.max() > 0 and tot[-1] > 0 else 0.0
 
 
-def replay(records, plan: ES.StagePlan, limit_db: float = 0.5) -> dict:
+def load_net():
+    """The deployed acceptance network (openems_b200/data/stage_net.npz) as
+    its float64 restatement with bf16 operands, and its threshold."""
+    from oracle.tailnet_ref import StageNetRef
+    d = np.load(os.path.join(ROOT, "openems_b200", "data", "stage_net.npz"))
+    ref = StageNetRef([(d[f"w{k}"], d[f"b{k}"]) for k in range(4)], (d["w4"], d["b4"]), (d["w5"], d["b5"]))
+    return ref, float(np.asarray(d["threshold"]).reshape(-1)[0])
+
+
+def replay(records, plan: ES.StagePlan, limit_db: float = 0.5, net=None) -> dict:
     """staged_sweep's decisions on recorded runs: per instance the steps it
-    runs and, if stopped early, its largest S11 error over the band."""
+    runs and, if stopped early, its largest S11 error over the band.  net:
+    load_net()'s pair, to accept by the network's score as staged_sweep does
+    (with the plan's stage-agreement check and slack when agree_db is set)."""
     band = plan.band(P.FREQS)
     steps, errors, how = [], [], []
     for rec in records:
         tr, dt, full = rec["trace"], rec["dt"], rec["steps"]
         used, err, h = full, 0.0, "full"
+        prev = None
         for K in plan.stages:
             if full <= K:
                 h = "decayed"
                 break
             r = {"uf": P.head_dft(tr[:K, 0], 1, dt, P.FREQS, 0.0), "if": P.head_dft(tr[:K, 1], 1, dt, P.FREQS, 0.5),
                  "final_decay_db": level_db(rec, K)}
-            pred, d, _ = ES.check_instance(tr, r, K, dt, P.FREQS, P.HORIZON, 50.0, plan)
-            if d < plan.tau:
+            c = ES.stage_check(tr, r, K, dt, P.FREQS, P.HORIZON, 50.0, plan)
+            pred = c["pred"]
+            agree = ES.s11_db_error(pred, prev, band) if prev is not None else np.inf
+            prev = pred
+            if net is not None:
+                x, sc = ES.stage_features(tr, c, K, P.HORIZON, plan)
+                score = float(net[0].forward(x[None], sc[None], bf16=True)[0, 0])
+                ok = score < net[1] + (plan.net_slack if plan.agree_db is not None else 0.0)
+            else:
+                ok = (c["check_mean"] if plan.check == "mean" else c["check_max"]) < plan.tau
+            if plan.agree_db is not None:
+                ok = ok and agree < plan.agree_db
+            if ok:
                 used, err, h = K, ES.s11_db_error(pred, rec["s11"], band), "predicted"
                 break
         steps.append(used)
@@ -128,12 +153,18 @@ def main(argv=None):
     ap.add_argument("--count", type=int, default=80)
     ap.add_argument("--cache", default=None, help="keep the oracle runs here (npz per instance)")
     ap.add_argument("--threads", type=int, default=8)
+    ap.add_argument("--net", action="store_true", help="accept by the trained network (dense plan only)")
+    ap.add_argument("--agree", type=float, default=None, help="stage agreement bound in dB (StagePlan.agree_db)")
+    ap.add_argument("--slack", type=float, default=0.0, help="added to the network's threshold with --agree")
     a = ap.parse_args(argv)
     from threadpoolctl import threadpool_limits
     records = load_or_run(a.seed, a.count, a.cache, a.threads)
+    net = load_net() if a.net else None
+    dense = ES.StagePlan.dense(agree_db=a.agree, net_slack=a.slack)
+    plans = (("dense", dense),) if a.net else (("standard (tau 0.05)", ES.StagePlan(tau=0.05)), ("dense", dense))
     with threadpool_limits(a.threads):
-        for name, plan in (("standard (tau 0.05)", ES.StagePlan(tau=0.05)), ("dense", ES.StagePlan.dense())):
-            r = replay(records, plan)
+        for name, plan in plans:
+            r = replay(records, plan, net=net)
             r.pop("steps"), r.pop("errors")
             print(json.dumps({"plan": name, "seed": a.seed, "count": len(records),
                               "full_steps_mean": float(np.mean([x["steps"] for x in records])), **r}))
