@@ -130,7 +130,7 @@ class EngineInterface:
         n = q.shape[0]
         vals = np.empty((n, 3), dtype=np.float64)
         snapped = np.empty((n, 3), dtype=np.uint64)
-        d = self._g.desc
+        d = N.SampleDescC.from_buffer_copy(self._g.desc)  # per call: interfaces may be shared by threads
         d.quantity = int(quantity)
         d.interpolation = int(self._interp if interpolation is None else interpolation)
         qp = q.ctypes.data_as(ctypes.c_void_p)
