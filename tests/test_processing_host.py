@@ -2,6 +2,7 @@
 names, cells, the collection and frequency_response on given samples.
 Sampling on the engine is in tests/test_gpu_processing.py."""
 import numpy as np
+import pytest
 
 from openems_b200.processing import CurrentProbe, FieldProbe, Processing, VoltageProbe, _bin
 
@@ -103,3 +104,112 @@ def test_record_and_collect_columns_and_times():
     other.traces = np.zeros((2, 8))
     p.collect(other)
     assert len(v.values) == 3
+
+
+# ---- field dumps (src/processing/fields_fd.rs tests) over a stand-in engine --
+
+from openems_b200.processing import FdDumpType, FrequencyDomainFieldDump, TimeDomainFieldDump  # noqa: E402
+
+
+class _FdEngine:
+    """add_field_dft / field_dft / state sections of an engine, with
+    accumulators = deterministic complex values on the sub-sampled points."""
+
+    def __init__(self, dims):
+        self.dims, self.dt, self.step = dims, 1e-12, 0
+        self.dumps, self.writes = [], []
+
+    def add_field_dft(self, region, freqs, components, sub_sample, interval):
+        shape = tuple(-(-(region[2 * a + 1] - region[2 * a]) // sub_sample[a]) for a in range(3))
+        self.dumps.append((shape, components, len(freqs)))
+        return len(self.dumps) - 1
+
+    def field_dft(self, dump_id, f, c):
+        shape = self.dumps[dump_id][0]
+        n = int(np.prod(shape))
+        return ((np.arange(n) + 1.0 + 10 * c + 100 * f) * (1 + 1j)).reshape(shape)
+
+    def current_timestep(self):
+        return self.step
+
+    def state_sections(self):
+        return [(1, 64, 0)] + [(8, 16 * (k + 1), 0) for k in range(len(self.dumps))]
+
+    def write_state(self, idx, data, variant):
+        self.writes.append((idx, len(data), variant, set(data)))
+
+
+def test_fd_dump_creation_and_sample_count():
+    """test_fd_dump_creation, test_fd_reset: frequencies, samples counted
+    per interval since creation or reset; reset zeroes the dump's own
+    accumulator section."""
+    eng = _FdEngine((10, 10, 10))
+    eng.step = 7
+    FrequencyDomainFieldDump(eng, [5e9], FdDumpType.HField)
+    d = FrequencyDomainFieldDump(eng, [1e9, 2e9, 3e9], FdDumpType.Both, interval=2)
+    assert d.num_frequencies() == 3 and d.frequencies() == [1e9, 2e9, 3e9]
+    assert d.num_samples() == 0
+    eng.step = 12  # steps 8, 10, 12
+    assert d.num_samples() == 3
+    d.reset()
+    assert eng.writes == [(2, 32, 0, {0})] and d.num_samples() == 0
+    assert eng.dumps[1][1] == 0x3F and eng.dumps[0][1] == 0x38
+
+
+def test_fd_accessors_and_magnitude():
+    """get_e_field / get_h_field by dump type, the full i, j, k layout with
+    sub-sampling, get_e_magnitude, extract_e_magnitude / extract_e_phase
+    (test_extract_magnitude, test_sub_sampling)."""
+    eng = _FdEngine((5, 4, 6))
+    d = FrequencyDomainFieldDump(eng, [1e9, 2e9], FdDumpType.EField, sub_sample=(2, 1, 3))
+    assert d.get_h_field(0) is None and d.get_e_field(2) is None and d.get_h_magnitude(0, 0, 0, 0) == 0.0
+    e = d.get_e_field(1)
+    assert len(e) == 3 and all(a.shape == (5 * 4 * 6,) for a in e)
+    full = e[2].reshape(5, 4, 6)
+    np.testing.assert_array_equal(full[::2, :, ::3], eng.field_dft(0, 1, 2))
+    assert full[1, 0, 0] == 0 and full[0, 0, 1] == 0
+    want = np.sqrt(sum(abs(e[c].reshape(5, 4, 6)[2, 3, 3]) ** 2 for c in range(3)))
+    assert d.get_e_magnitude(1, 2, 3, 3) == pytest.approx(want, rel=1e-15)
+    mag = d.extract_e_magnitude(1)
+    assert mag.dtype == np.float32 and mag.shape == (5, 4, 6) and mag[2, 3, 3] == np.float32(want)
+    ph = d.extract_e_phase(0, 7)
+    assert ph.dtype == np.float32 and ph[0, 0, 0] == np.float32(np.pi / 4)
+    assert FrequencyDomainFieldDump(eng, [1e9], FdDumpType.JField).get_h_field(0) is None
+    assert FrequencyDomainFieldDump(eng, [1e9], FdDumpType.RotH).get_h_field(0) is not None
+
+
+def test_td_dump():
+    """test_td_dump: every 100 steps, names prefix_00000000, ..."""
+    dump = TimeDomainFieldDump(100, "field_dump")
+    assert dump.should_dump(0) and not dump.should_dump(50) and dump.should_dump(100)
+    assert dump.get_filename() == "field_dump_00000000"
+    dump.increment()
+    assert dump.get_filename() == "field_dump_00000001" and dump.file_index() == 1
+    dump.reset()
+    assert dump.file_index() == 0
+    assert not TimeDomainFieldDump(0, "x").should_dump(0)
+
+
+def test_td_dump_writes_the_next_snapshot(tmp_path):
+    """write: the engine's present fields under the next name, VTK pair or
+    the binary container, then the index moves on."""
+    import openems_b200 as oe
+
+    class Fields:
+        dt = 1e-12
+
+        def read_fields(self):
+            e = np.zeros((3, 2, 3, 4), np.float32)
+            e[2, 1, 2, 3] = 1.5
+            return e, np.zeros_like(e)
+
+        def current_timestep(self):
+            return 300
+
+    grid = oe.Grid.uniform(2, 3, 4, 1e-3)
+    dump = TimeDomainFieldDump(100, str(tmp_path / "snap"))
+    name = dump.write(Fields(), grid)
+    assert name.endswith("snap_00000000") and dump.file_index() == 1
+    assert (tmp_path / "snap_00000000_E.vtk").exists() and (tmp_path / "snap_00000000_H.vtk").exists()
+    path = dump.write(Fields(), grid, fmt="oems")
+    assert path.endswith("snap_00000001.h5") and (tmp_path / "snap_00000001.h5").exists()
