@@ -190,3 +190,33 @@ def test_mirror_refuses_mismatched_grid_and_bad_shapes():
         m.set_e_fields([[1, 2, 3], [4, 5, 6]], [[1.0, 2.0, 3.0]])
     m.set_time(7, 3e-12)
     assert (m.timestep, m.time, m.dt()) == (7, 3e-12, 1e-12)
+
+
+def test_integral_terms_agree_with_the_interface_restatement():
+    """The host's integral term lists (recorded per step as f64 probes) and
+    the interface restatement give the same voltage integral bit for bit;
+    the current integrals round each product into the sum, where the
+    reference rounds the cell's difference first, so they agree to a few
+    ulps of the terms."""
+    import openems_b200 as oe
+    rng = np.random.default_rng(4)
+    lines = [np.concatenate([[0.0], np.cumsum(rng.uniform(0.5e-3, 1.5e-3, n))]) for n in (9, 7, 11)]
+    grid = oe.Grid(*lines)
+    op = oe.Operator(grid, oe.BoundaryConditions.all_pec())
+    e = rng.standard_normal((3, 9, 7, 11)).astype(np.float32)
+    h = rng.standard_normal((3, 9, 7, 11)).astype(np.float32)
+    ref = InterfaceRef(e, h, lines, 1.0)
+    centre = lambda c: [0.5 * (lines[a][c[a]] + lines[a][c[a] + 1]) for a in range(3)]
+
+    def f64_sum(t):
+        acc = 0.0
+        for comp, (i, j, k), w in t.terms:
+            acc += w * float((e if comp < 3 else h)[comp % 3, i, j, k])
+        return acc
+
+    for s, t in (((1, 2, 3), (7, 5, 9)), ((8, 0, 10), (0, 6, 0)), ((4, 4, 4), (4, 4, 4))):
+        assert f64_sum(oe.voltage_integral(op, s, t)) == ref.calc_voltage_integral(centre(s), centre(t))
+        for normal in (0, 1, 2):
+            a = f64_sum(oe.current_integral(op, s, t, normal))
+            b = ref.calc_current_integral(centre(s), centre(t), normal)
+            assert abs(a - b) <= 1e-12 * max(1.0, abs(b)) * 64
