@@ -115,3 +115,17 @@ def test_engine_without_gpu_fails_loudly():
     op = oe.Operator(oe.Grid.uniform(4, 4, 4, 1e-3), oe.BoundaryConditions.all_pec())
     with pytest.raises(oe.NoDeviceError):
         oe.Engine(op)
+
+
+def test_interface_entry_points_refuse_null_arguments():
+    """oems_engine_sample / _integral / _eval_terms / _set_cells check their
+    arguments on the host before any device work."""
+    L = N.lib()
+    d = N.SampleDescC()
+    out = N.c_f64()
+    three = (N.c_f64 * 3)(0.0, 0.0, 0.0)
+    assert L.oems_engine_sample(None, ctypes.byref(d), None, None, 1, None, None) == N.ERR_INVALID_ARGUMENT
+    assert L.oems_engine_integral(None, ctypes.byref(d), 0, three, three, 0, ctypes.byref(out)) \
+        == N.ERR_INVALID_ARGUMENT
+    assert L.oems_engine_eval_terms(None, None, 0, 0, ctypes.byref(out)) == N.ERR_INVALID_ARGUMENT
+    assert L.oems_engine_set_cells(None, 0, None, None, 1, 0) == N.ERR_INVALID_ARGUMENT
