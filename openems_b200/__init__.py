@@ -19,5 +19,7 @@ from .fdtd import (Grid, BoundaryCondition, BoundaryConditions, CpmlBoundaries, 
                    PropagationDirection, Polarization, TfsfConfig, Pack, compress_coefficients,
                    waveguide_te10)
 from .engine_interface import EngineInterface, EngineInterfaceMut, InterpolationType  # noqa: F401
+from .processing import (Processing, VoltageProbe, CurrentProbe, FieldProbe,  # noqa: F401
+                         FrequencyDomainFieldDump, TimeDomainFieldDump, FdDumpType)
 
 __all__ = [n for n in dir() if not n.startswith("_")]
