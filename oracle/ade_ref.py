@@ -6,18 +6,22 @@ this project's second-order polarisation recursions, kinds 3 and 4) on one
 value at a time.  This module runs them on a grid, vectorised over each
 material's cells, to pin the order around the field update: kinds 3 and 4
 read E as it is before the E update (after the H update); every material
-then updates its cells after the E update, materials in list order, before
-the excitations.  Used only to cross-check the C++ oracle.
+then updates its cells after the E update, materials in list order, then the
+lumped RLC elements in list order, before the excitations.  Used only to
+cross-check the C++ oracle.
 """
 from __future__ import annotations
 
 import numpy as np
 
-from .numpy_ref import _bwd, _fwd, dispersive_coeffs
+from .numpy_ref import _bwd, _fwd, dispersive_coeffs, rlc_coeffs
 
 
-def run(coeffs12, fields6, num_steps, dt, materials, excitations=()):
-    """materials: [(kind, params, cells (n, 3), eps_inf)]; returns fields."""
+def run(coeffs12, fields6, num_steps, dt, materials, excitations=(), rlc=(), deltas=(1.0, 1.0, 1.0)):
+    """materials: [(kind, params, cells (n, 3), eps_inf)]; rlc: [(pos,
+    direction, type, r, l, c)] elements (LumpedRlc::post_update_e,
+    src/extensions/lumped_rlc.rs:263-286, after the media, in list order;
+    coefficients with the cell size along the element); returns fields."""
     c = [np.asarray(x, dtype=np.float32) for x in coeffs12]
     ca, cb, da, db = c[0:3], c[3:6], c[6:9], c[9:12]
     F = [np.array(f, dtype=np.float32) for f in fields6]
@@ -28,6 +32,8 @@ def run(coeffs12, fields6, num_steps, dt, materials, excitations=()):
         mats.append(dict(kind=kind, co=dispersive_coeffs(kind, params, dt, eps_inf), idx=idx,
                          j=np.zeros((3, n), np.float32), pp=np.zeros((3, n), np.float32),
                          ep=np.zeros((3, n), np.float32)))
+    els = [dict(pos=tuple(pos), d=d, co=rlc_coeffs(t, r, l, cc, deltas[d], dt), i=np.float32(0))
+           for pos, d, t, r, l, cc in rlc]
     inner = (slice(1, None),) * 3
     dtf = np.float32(dt)
     for step in range(num_steps):
@@ -66,6 +72,12 @@ def run(coeffs12, fields6, num_steps, dt, materials, excitations=()):
                     m["pp"][k] = old
                     m["j"][k] = pn
                     E[k][m["idx"]] = e - c2 * (pn - old)
+        for el in els:
+            v_vv, v_il = el["co"]
+            e = E[el["d"]][el["pos"]]
+            en = v_vv * e + v_il * el["i"]
+            el["i"] = el["i"] + e * dtf
+            E[el["d"]][el["pos"]] = en
         F = [ex, ey, ez, hx, hy, hz]
         for pos, dr, soft, samples in excitations:
             if step >= len(samples):
