@@ -9,6 +9,13 @@ is a multiple of `interval` (scale 2 dt interval), E at t = n dt and H at
 twiddle is cos / sin of -2 pi f t from the C library (Python's math module)
 times the scale; real and imaginary parts accumulate as separate f64
 products and sums.  The field update is numpy_ref's Yee step.
+
+It also restates the near-field to far-field recording box (no counterpart
+in the reference engine; python/openEMS/nf2ff.py records the same
+quantities): on each enabled face, at the face's plane p along its normal
+a, the two tangential E components (b = a + 1, c = a + 2 mod 3) at p and
+the two tangential H components averaged in f64 over the planes p - 1 and
+p, with the same twiddles (E at n dt, H at (n - 1/2) dt).
 """
 from __future__ import annotations
 
@@ -19,10 +26,12 @@ import numpy as np
 from .numpy_ref import _bwd, _fwd
 
 
-def run(coeffs12, fields6, num_steps, dt, dumps, excitations=(), t0=0):
+def run(coeffs12, fields6, num_steps, dt, dumps, excitations=(), t0=0, boxes=()):
     """dumps: [(region (i0, i1, j0, j1, k0, k1), sub_sample, comps, freqs,
-    interval)]; returns (fields, per dump an array [freq][comp] of complex
-    accumulators over the sub-sampled region, k fastest)."""
+    interval)]; boxes: [(lo, hi, freqs, directions (6 flags), interval)].
+    Returns (fields, per dump an array [freq][comp] of complex accumulators
+    over the sub-sampled region, k fastest, per box {face: array [freq][4]
+    of (nb, nc) complex accumulators Eb, Ec, Hb, Hc})."""
     c = [np.asarray(x, dtype=np.float32) for x in coeffs12]
     ca, cb, da, db = c[0:3], c[3:6], c[6:9], c[9:12]
     F = [np.array(f, dtype=np.float32) for f in fields6]
@@ -31,6 +40,16 @@ def run(coeffs12, fields6, num_steps, dt, dumps, excitations=(), t0=0):
         sels.append(tuple(slice(region[2 * a], region[2 * a + 1], ss[a]) for a in range(3)))
         shape = F[0][sels[-1]].shape
         accs.append([[(np.zeros(shape), np.zeros(shape)) for _ in comps] for _ in freqs])
+    bacc = []
+    for lo, hi, freqs, dirs, interval in boxes:
+        faces = {}
+        for face in range(6):
+            if dirs[face]:
+                a = face // 2
+                b, c_ = (a + 1) % 3, (a + 2) % 3
+                shape = (hi[b] - lo[b] + 1, hi[c_] - lo[c_] + 1)
+                faces[face] = [[[np.zeros(shape), np.zeros(shape)] for _ in range(4)] for _ in freqs]
+        bacc.append(faces)
     inner = (slice(1, None),) * 3
     t = t0
     for step in range(num_steps):
@@ -66,5 +85,38 @@ def run(coeffs12, fields6, num_steps, dt, dumps, excitations=(), t0=0):
                     x = F[comp][sel].astype(np.float64)
                     re, im = acc[fi][ci]
                     acc[fi][ci] = (re + x * wr, im + x * wi)
+        for (lo, hi, freqs, dirs, interval), faces in zip(boxes, bacc):
+            if t % interval:
+                continue
+            scale = 2.0 * dt * float(interval)
+            for face, acc in faces.items():
+                a = face // 2
+                b, c_ = (a + 1) % 3, (a + 2) % 3
+                p = hi[a] if face & 1 else lo[a]
+                sl = [slice(None)] * 3
+                sl[b] = slice(lo[b], hi[b] + 1)
+                sl[c_] = slice(lo[c_], hi[c_] + 1)
+                at = list(sl)
+                at[a] = p
+                am = list(sl)
+                am[a] = p - 1
+
+                def plane(comp, where):
+                    v = F[comp][tuple(where)].astype(np.float64)
+                    return v if b < c_ else v.T  # (nb, nc) order
+
+                vals = [plane(b, at), plane(c_, at),
+                        0.5 * (plane(3 + b, am) + plane(3 + b, at)), 0.5 * (plane(3 + c_, am) + plane(3 + c_, at))]
+                for fi, f in enumerate(freqs):
+                    tw = []
+                    for tt in (float(t) * dt, (float(t) - 0.5) * dt):
+                        ph = -2.0 * math.pi * f * tt
+                        tw.append((math.cos(ph) * scale, math.sin(ph) * scale))
+                    for k in range(4):
+                        wr, wi = tw[0 if k < 2 else 1]
+                        acc[fi][k][0] = acc[fi][k][0] + vals[k] * wr
+                        acc[fi][k][1] = acc[fi][k][1] + vals[k] * wi
     out = [np.array([[re + 1j * im for re, im in row] for row in acc]) for acc in accs]
-    return np.stack(F), out
+    bout = [{face: np.array([[re + 1j * im for re, im in row] for row in acc]) for face, acc in faces.items()}
+            for faces in bacc]
+    return np.stack(F), out, bout

@@ -29,7 +29,7 @@ def test_field_dft_restatements_agree_bitwise():
     s.add_excitation_sampled(*exc[0][:3], samples[half:])
     s.run_batch(steps - half)
     zero = np.zeros((6,) + dims, np.float32)
-    fields, acc = fd_ref.run(c12, zero, steps, dt, dumps, exc)
+    fields, acc, _ = fd_ref.run(c12, zero, steps, dt, dumps, exc)
     np.testing.assert_array_equal(fields, np.asarray(s.fields(), np.float32).reshape(fields.shape))
     for did, (region, ss, comps, freqs, iv), a in zip(ids, dumps, acc):
         for fi in range(len(freqs)):
@@ -37,3 +37,30 @@ def test_field_dft_restatements_agree_bitwise():
                 got = s.field_dft(did, fi, comp)
                 assert np.abs(got).max() > 0
                 np.testing.assert_array_equal(got, a[fi, ci].reshape(-1))
+
+
+def test_nf2ff_box_restatements_agree_bitwise():
+    """All six faces of a recording box (E on the face, H averaged over the
+    two half-cells), two frequencies, interval 2."""
+    dims = (12, 11, 13)
+    lines = [oracle.uniform_lines(n, d) for n, d in zip(dims, (1.0e-3, 0.8e-3, 1.2e-3))]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*dims, dt, delta)
+    c12 = s.coefficients()
+    steps = 70
+    t = (np.arange(steps) - 15.0) / 5.0
+    exc = [((6, 5, 6), 2, True, np.exp(-t * t).astype(np.float32)),
+           ((5, 6, 7), 0, True, (0.3 * np.exp(-t * t)).astype(np.float32))]
+    for pos, d, soft, smp in exc:
+        s.add_excitation_sampled(pos, d, soft, smp)
+    lo, hi, freqs, dirs = (2, 3, 2), (9, 8, 10), [4e9, 9e9], (1, 1, 1, 0, 1, 1)
+    bid = s.add_nf2ff_box(lo, hi, freqs, dirs, 2)
+    s.run_batch(steps)
+    zero = np.zeros((6,) + dims, np.float32)
+    _, _, boxes = fd_ref.run(c12, zero, steps, dt, [], exc, boxes=[(lo, hi, freqs, dirs, 2)])
+    assert set(boxes[0]) == {0, 1, 2, 4, 5}
+    for face, acc in boxes[0].items():
+        for fi in range(len(freqs)):
+            got = s.nf2ff_face(bid, face, fi, lo, hi)
+            assert np.abs(got).max() > 0
+            np.testing.assert_array_equal(got, acc[fi])
