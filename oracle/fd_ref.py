@@ -120,3 +120,19 @@ def run(coeffs12, fields6, num_steps, dt, dumps, excitations=(), t0=0, boxes=())
     bout = [{face: np.array([[re + 1j * im for re, im in row] for row in acc]) for face, acc in faces.items()}
             for faces in bacc]
     return np.stack(F), out, bout
+
+
+def probe_dft(trace, dt, freqs, half, t0=0):
+    """Running DFT of a recorded probe trace (one value per step, the first
+    after step t0 + 1): X(f) += x exp(-j 2 pi f t) 2 dt with t = (step count
+    after the step - half) dt, half = 1/2 for a probe of H values only."""
+    acc = np.zeros(len(freqs), np.complex128)
+    re, im = np.zeros(len(freqs)), np.zeros(len(freqs))
+    for s, x in enumerate(np.asarray(trace, np.float64)):
+        t = (float(t0 + s + 1) - half) * dt
+        for fi, f in enumerate(freqs):
+            ph = -2.0 * math.pi * f * t
+            re[fi] = re[fi] + x * (math.cos(ph) * (2.0 * dt))
+            im[fi] = im[fi] + x * (math.sin(ph) * (2.0 * dt))
+    acc.real, acc.imag = re, im
+    return acc

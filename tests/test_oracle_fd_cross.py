@@ -64,3 +64,30 @@ def test_nf2ff_box_restatements_agree_bitwise():
             got = s.nf2ff_face(bid, face, fi, lo, hi)
             assert np.abs(got).max() > 0
             np.testing.assert_array_equal(got, acc[fi])
+
+
+def test_probe_dft_restatements_agree_bitwise():
+    """A voltage-style probe of E and a current-style probe of H only (half a
+    step earlier), their running DFTs over two batches against the
+    restatement on the recorded traces."""
+    dims = (10, 9, 11)
+    lines = [oracle.uniform_lines(n, d) for n, d in zip(dims, (1.0e-3, 0.8e-3, 1.2e-3))]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*dims, dt, delta)
+    t = (np.arange(60) - 12.0) / 4.0
+    samples = np.exp(-t * t).astype(np.float32)
+    pe = s.add_probe([(2, (5, 4, k), -1.2e-3) for k in range(3, 8)], 1)
+    ph = s.add_probe([(3, (4, 3, 5), 0.8e-3), (4, (4, 3, 5), -1.0e-3)], 1)
+    freqs = [2e9, 7e9, 13e9]
+    de, dh = s.add_probe_dft(pe, freqs), s.add_probe_dft(ph, freqs)
+    traces = []
+    for part in (samples[:25], samples[25:]):
+        s.clear_excitations()
+        s.add_excitation_sampled((5, 4, 5), 2, True, part)
+        s.run_batch(len(part))
+        traces.append(s.probe_traces())
+    tr = np.concatenate(traces)
+    for did, col, half in ((de, pe, 0.0), (dh, ph, 0.5)):
+        want = fd_ref.probe_dft(tr[:, col], dt, freqs, half)
+        assert np.abs(want).max() > 0
+        np.testing.assert_array_equal(s.probe_dft(did), want)
