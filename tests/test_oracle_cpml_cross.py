@@ -50,3 +50,33 @@ def test_cpml_restatements_agree_bitwise(layers, alpha_max, kappa_max):
     # the slabs act: the same run without them differs
     assert not np.array_equal(fields, numpy_ref.run(c12, zero, steps, exc))
     np.testing.assert_array_equal(fields, np.asarray(ref, np.float32).reshape(fields.shape))
+
+
+from hypothesis import given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=12, deadline=None)
+@given(dims=st.tuples(st.integers(6, 12), st.integers(6, 12), st.integers(6, 12)),
+       layers=st.tuples(*[st.integers(0, 4)] * 6),
+       alpha=st.sampled_from([0.0, 0.02]), kappa=st.sampled_from([1.0, 3.0]))
+def test_cpml_restatements_agree_on_random_layouts(dims, layers, alpha, kappa):
+    """Random grid sizes and per-face layer counts (absent faces included)."""
+    if max(layers) == 0:
+        layers = (1,) + layers[1:]
+    for a in range(3):  # both faces of an axis must fit the axis
+        if layers[2 * a] + layers[2 * a + 1] > dims[a]:
+            layers = layers[:2 * a] + (1, 1) + layers[2 * a + 2:]
+    lines = [oracle.uniform_lines(n, d) for n, d in zip(dims, (1.0e-3, 0.9e-3, 1.1e-3))]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*dims, dt, delta)
+    s.enable_cpml(layers, 3.0, 1e-6, alpha, kappa)
+    c12 = s.coefficients()
+    steps = 30
+    t = (np.arange(steps) - 8.0) / 3.0
+    pos = tuple(n // 2 for n in dims)
+    exc = [(pos, 2, True, np.exp(-t * t).astype(np.float32))]
+    s.add_excitation_sampled(*exc[0][:3], exc[0][3])
+    s.run_batch(steps)
+    zero = np.zeros((6,) + dims, np.float32)
+    fields, _ = cpml_ref.run(c12, zero, steps, dt, delta, layers, 3.0, 1e-6, alpha, kappa, exc)
+    np.testing.assert_array_equal(fields, np.asarray(s.fields(), np.float32).reshape(fields.shape))
