@@ -54,3 +54,26 @@ def test_second_order_interior_changes_the_result():
     a = mur_ref.run(c12, zero, 90, dt, delta, (1,) * 6, 1, 0.0, exc)
     b = mur_ref.run(c12, zero, 90, dt, delta, (1,) * 6, 2, 0.0, exc)
     assert np.abs(a - b).max() > 1e-3
+
+
+from hypothesis import given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=12, deadline=None)
+@given(dims=st.tuples(st.integers(7, 12), st.integers(7, 12), st.integers(7, 12)),
+       enabled=st.tuples(*[st.integers(0, 1)] * 6), order=st.sampled_from([1, 2]))
+def test_mur_restatements_agree_on_random_layouts(dims, enabled, order):
+    """Random grid sizes, enabled faces and order."""
+    lines = [oracle.uniform_lines(n, d) for n, d in zip(dims, (1.0e-3, 0.9e-3, 1.1e-3))]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*dims, dt, delta)
+    s.enable_mur(enabled, order, 0.0)
+    c12 = s.coefficients()
+    steps = 40
+    t = (np.arange(steps) - 8.0) / 3.0
+    exc = [(tuple(n // 2 for n in dims), 1, True, np.exp(-t * t).astype(np.float32))]
+    s.add_excitation_sampled(*exc[0][:3], exc[0][3])
+    s.run_batch(steps)
+    zero = np.zeros((6,) + dims, np.float32)
+    got = mur_ref.run(c12, zero, steps, dt, delta, enabled, order, 0.0, exc)
+    np.testing.assert_array_equal(got, np.asarray(s.fields(), np.float32).reshape(got.shape))
