@@ -218,3 +218,50 @@ class InterfaceRef:
     def add_e_field(self, i, j, k, value):
         for c in range(3):
             self.e[c, i, j, k] = np.float32(self.e[c, i, j, k]) + np.float32(value[c])
+
+
+def snap_vec(lines, unit, dims, pos):
+    """snap_to_grid for an (n, 3) array of positions, vectorised: on
+    non-decreasing lines the scan's cell is the first line pair whose upper
+    line is >= the coordinate (searchsorted), if its lower line is <= it;
+    otherwise (below the first line, past the last, NaN) the last cell."""
+    out = np.empty((len(pos), 3), np.int64)
+    for ax in range(3):
+        l = np.asarray(lines[ax], np.float64)
+        x = np.asarray(pos[:, ax], np.float64) / unit
+        if len(l) < 2:
+            out[:, ax] = 0
+            continue
+        i = np.searchsorted(l[1:], x, side="left")  # first i with x <= l[i + 1]
+        ok = (i < len(l) - 1) & (x >= l[np.minimum(i, len(l) - 2)])
+        cell = np.where(ok, i, len(l) - 2)
+        out[:, ax] = np.minimum(cell, dims[ax] - 1)
+    return out
+
+
+def node_vec(field3, lines, unit, dims, pos):
+    """interpolate_*_field_to_node for an (n, 3) array of positions."""
+    c = snap_vec(lines, unit, dims, pos)
+    fr = []
+    for ax in range(3):
+        l = np.asarray(lines[ax], np.float64)
+        i = c[:, ax]
+        line = np.where(i < len(l), l[np.minimum(i, len(l) - 1)], 0.0) * unit
+        hi = np.minimum(i + 1, len(l) - 1)
+        d = np.where(i + 1 < len(l), (l[hi] - l[i]) * unit, np.where(i > 0, (l[i] - l[np.maximum(i - 1, 0)]) * unit, unit))
+        f = (pos[:, ax] - line) / d
+        fr.append(np.where(f < 0.0, 0.0, np.where(f > 1.0, 1.0, f)))
+    fx, fy, fz = fr
+    i, j, k = c[:, 0], c[:, 1], c[:, 2]
+    i1, j1, k1 = (np.minimum(v + 1, dims[a] - 1) for a, v in enumerate((i, j, k)))
+    out = np.empty((len(pos), 3))
+    for comp in range(3):
+        g = field3[comp].astype(np.float64)
+        c00 = g[i, j, k] * (1.0 - fx) + g[i1, j, k] * fx
+        c01 = g[i, j, k1] * (1.0 - fx) + g[i1, j, k1] * fx
+        c10 = g[i, j1, k] * (1.0 - fx) + g[i1, j1, k] * fx
+        c11 = g[i, j1, k1] * (1.0 - fx) + g[i1, j1, k1] * fx
+        c0 = c00 * (1.0 - fy) + c10 * fy
+        c1 = c01 * (1.0 - fy) + c11 * fy
+        out[:, comp] = c0 * (1.0 - fz) + c1 * fz
+    return out

@@ -220,3 +220,27 @@ def test_integral_terms_agree_with_the_interface_restatement():
             a = f64_sum(oe.current_integral(op, s, t, normal))
             b = ref.calc_current_integral(centre(s), centre(t), normal)
             assert abs(a - b) <= 1e-12 * max(1.0, abs(b)) * 64
+
+
+def test_vectorised_restatement_agrees_with_the_scalar_one():
+    """snap and node interpolation vectorised (searchsorted in place of the
+    scan) against the scalar restatement, bit for bit, on a graded grid with
+    a unit: positions inside, on mesh lines, outside and NaN."""
+    from oracle.interface_ref import node_vec, snap_vec
+    rng = np.random.default_rng(8)
+    dims = (9, 7, 11)
+    lines = [np.concatenate([[0.0], np.cumsum(rng.uniform(0.5, 1.5, n))]) for n in dims]
+    unit = 1e-3
+    e = rng.standard_normal((3,) + dims).astype(np.float32)
+    h = np.zeros_like(e)
+    ref = InterfaceRef(e, h, lines, unit, interp=NODE_INTERPOLATE)
+    hi = np.array([l[-1] for l in lines]) * unit
+    pos = rng.uniform(-0.1 * hi, 1.1 * hi, (400, 3))
+    for ax in range(3):
+        pos[:100, ax] = lines[ax][rng.integers(0, len(lines[ax]), 100)] * unit
+    pos[-2:] = [[np.nan, 0.0, 0.0], [0.0, 0.0, np.nan]]
+    cells = snap_vec(lines, unit, dims, pos)
+    vals = node_vec(e, lines, unit, dims, pos)
+    for n in range(len(pos)):
+        assert tuple(cells[n]) == ref.snap(pos[n]), n
+        np.testing.assert_array_equal(vals[n], ref.get_e_field(pos[n]), err_msg=str(n))
