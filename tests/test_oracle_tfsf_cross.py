@@ -36,3 +36,29 @@ def test_tfsf_restatements_agree_bitwise(kind, direction, polarization, layer, v
     assert np.isfinite(ref).all() and np.abs(ref).max() > 0
     assert not np.array_equal(got, numpy_ref.run(c12, zero, steps))
     np.testing.assert_array_equal(got, ref)
+
+
+from hypothesis import given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=12, deadline=None)
+@given(dims=st.tuples(st.integers(6, 11), st.integers(6, 11), st.integers(6, 11)),
+       direction=st.integers(0, 5), polarization=st.integers(0, 1), kind=st.sampled_from([0, 1]),
+       layer_frac=st.floats(0.2, 0.8))
+def test_tfsf_restatements_agree_on_random_layouts(dims, direction, polarization, kind, layer_frac):
+    """Random grid sizes, directions, polarizations and plane positions
+    (kind 1 takes the forward directions only, as its set-up requires)."""
+    if kind == 1:
+        direction -= direction % 2
+    n = dims[direction // 2]
+    layer = max(1, min(n - 2, int(layer_frac * n)))
+    lines = [oracle.uniform_lines(m, d) for m, d in zip(dims, (1.0e-3, 0.9e-3, 1.1e-3))]
+    dt, delta = oracle.grid_timestep(*lines)
+    s = oracle.OracleSim(*dims, dt, delta)
+    c12 = s.coefficients()
+    s.enable_tfsf(direction, polarization, 15e9, 1.0, layer, 0.0, kind)
+    steps = 35
+    s.run_batch(steps)
+    zero = np.zeros((6,) + dims, np.float32)
+    got = tfsf_ref.run(c12, zero, steps, dt, delta, direction, polarization, 15e9, 1.0, layer, 0.0, kind)
+    np.testing.assert_array_equal(got, np.asarray(s.fields(), np.float32).reshape(got.shape))
